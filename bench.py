@@ -1,0 +1,392 @@
+"""Benchmark: worst-case load solve on the 128x128x64 configuration on one B200.
+
+A step is one worst-case solve of the hot path on the resident design:
+Galerkin coarse-stencil assembly + coarsest factorisation, then the largest
+eigenvalue of the load-space compliance operator P K^-1 P by Lanczos (k=16
+Krylov vectors) whose inner MG-PCG solves run to relative residual 1e-6, then
+the worst-case displacement solve to 1e-6.  ``value`` uses the mixed form (FP32
+V-cycles inside FP64 CG; FP64 residuals, dots, orthogonalisation, Rayleigh
+quotient and coarsest solve); the all-FP64 form is reported beside it.
+
+Input: seeded synthetic density (smoothed Gaussian field, sigmoid map), z=0
+clamped, loadable set = top face; no dataset is read.
+
+``--impl reference`` times the CPU restatement of the reference algorithm
+(oracle/, OpenMP, all host cores) on the same configuration — the reference
+itself cannot be built in this image.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(nx=128, ny=128, nz=64, seed=0, k=16, tol=1e-6)
+METRIC = "worst-case solve (Lanczos k=16, MG-PCG inner solves to rel. residual 1e-6) on 128x128x64"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    lrank = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, lrank
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            p = [x.strip() for x in l.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_problem(rb, configs, ctx, precision):
+    cfg = configs.worst_case_box(WORKLOAD["nx"], WORKLOAD["ny"], WORKLOAD["nz"], seed=WORKLOAD["seed"])
+    params = rb.default_params(mode=cfg["mode"], youngs_modulus=1e6, poisson_ratio=0.4, power_penalty=3.0,
+                               min_rho=1e-3, precision=precision, smoother=rb.SMOOTH_SGS, pre_sweeps=1,
+                               post_sweeps=1)
+    G = rb.HierarchyGrid(ctx, params)
+    G.genFromBox(cfg["eact"])
+    G[0].setRho(cfg["rho"].ravel())
+    G.set_support(cfg["vfix"])
+    G.set_load_nodes(cfg["load_nodes"], cfg["normals"])
+    return cfg, G
+
+
+def step(rb, G, seed):
+    G.update_stencil()
+    lam, info = G.worst_case(rb.WORST_LANCZOS, WORKLOAD["k"], WORKLOAD["tol"], seed=seed)
+    return lam, info
+
+
+def time_steps(rb, ctx, G, steps, seed0=100):
+    """K steps bracketed by synchronize + CUDA events on the library's stream."""
+    import torch
+
+    stream = torch.cuda.ExternalStream(ctx_stream_handle(ctx))
+    ctx.sync()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    l0 = ctx.launches()
+    ev0.record(stream)
+    lams, infos = [], []
+    for s in range(steps):
+        lam, info = step(rb, G, seed0 + s)
+        lams.append(lam)
+        infos.append(info)
+    ev1.record(stream)
+    ev1.synchronize()
+    ctx.sync()
+    return ev0.elapsed_time(ev1), lams, infos, ctx.launches() - l0
+
+
+_STREAMS = {}
+
+
+def ctx_stream_handle(ctx):
+    return _STREAMS[id(ctx)]
+
+
+def make_ctx(rb, device):
+    import torch
+
+    torch.cuda.set_device(device)
+    s = torch.cuda.Stream(device=device)
+    ctx = rb.Context(device, C.c_void_p(s.cuda_stream))
+    _STREAMS[id(ctx)] = s.cuda_stream
+    ctx._torch_stream = s
+    return ctx
+
+
+# algorithmic bytes per launch of the kernels that can dominate (per node of the level,
+# level-0 sizes): u/f/r are 3 components of s bytes, w is 4 B per element, flags 1 B
+def algorithmic_bytes(name, nv, ne, s):
+    if name.startswith("fine_residual") or name.startswith("fine_jacobi"):
+        return nv * (3 * s * 3 + 1 + 1) + ne * 4   # read u, f; write r/unew; vact, vfix; w
+    if name.startswith("fine_applyK"):
+        return nv * (3 * s * 2 + 1 + 1) + ne * 4
+    if name.startswith("fine_gs"):
+        # one colour: read u of all nodes + w, read f / write u of 1/8 of the nodes
+        return nv * (3 * s + 1 + 1) + ne * 4 + nv // 8 * (3 * s * 2)
+    return None
+
+
+def roofline(ctx, stats, G, peaks):
+    # dominant kernel by device time
+    name, (n, ms) = max(stats.items(), key=lambda kv: kv[1][1])
+    nv, ne = G[0].nv, G[0].ne
+    s = 4 if name.endswith("f32") else 8
+    b = algorithmic_bytes(name, nv, ne, s)
+    avg_s = ms / max(n, 1) * 1e-3
+    out = {"kernel": name, "launches": n, "avg_us": avg_s * 1e6, "share": ms / sum(v[1] for v in stats.values())}
+    if b is None:
+        out.update({"bound": "hbm", "achieved": None, "peak": peaks.get("hbm_gbs"), "unit": "GB/s", "frac": None,
+                    "traffic": None})
+        return out
+    ach = b / avg_s / 1e9
+    peak = peaks.get("hbm_gbs", 6650.0)
+    out.update({"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(ach / peak, 4), "traffic": None, "algorithmic_bytes": int(b),
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"})
+    return out
+
+
+def e2e_steps(rb, ctx, G, cfg, steps, seed0=500):
+    """Same step through the public API with host buffers: H2D of the density
+    each step, worst-case solve, D2H of the worst-case load field."""
+    import torch
+
+    rho = np.ascontiguousarray(cfg["rho"].ravel(), np.float32)
+    fout = np.zeros(3 * G[0].nv)
+    stream = torch.cuda.ExternalStream(ctx_stream_handle(ctx))
+    ctx.sync()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for s in range(steps):
+        G[0].setRho(rho)
+        step(rb, G, seed0 + s)
+        fout = G[0].getForce()
+    ev1.record(stream)
+    ev1.synchronize()
+    return ev0.elapsed_time(ev1), rho.nbytes, fout.nbytes
+
+
+def cpu_baseline(gpu_inner_iters, gpu_vcycles, threads):
+    """Oracle (plain FP64, OpenMP) on a bounded sample of the same workload:
+    stencil assembly once + a few PCG iterations, extrapolated to the number of
+    inner PCG iterations one GPU step used."""
+    import oracle as O
+    from robtop_b200 import configs
+
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    cfg = configs.worst_case_box(WORKLOAD["nx"], WORKLOAD["ny"], WORKLOAD["nz"], seed=WORKLOAD["seed"])
+    H = O.Hierarchy(cfg["eact"], cfg["rho"], cfg["vfix"], p=3, E=1e6, nu=0.4)
+    t0 = time.perf_counter()
+    H.update_stencil()
+    t_st = time.perf_counter() - t0
+    nv = H.arrs[0]["u"].size // 3
+    b = np.zeros(3 * nv)
+    b[2 * nv + cfg["load_nodes"]] = 1.0 / np.sqrt(cfg["load_nodes"].size)
+    n_it = 3
+    t0 = time.perf_counter()
+    x, it, rr = H.pcg(b, tol=1e-30, maxit=n_it, smoother=O.SMOOTH_SGS)
+    t_it = (time.perf_counter() - t0) / n_it
+    total = t_st + t_it * gpu_inner_iters
+    return {"value": 1.0 / total, "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"oracle FP64 stencil assembly ({t_st:.2f} s) + {n_it} MG-PCG iterations "
+                      f"({t_it:.3f} s each), extrapolated to the {gpu_inner_iters} PCG iterations of one GPU step",
+            "seconds_per_step": total}
+
+
+def run_reference(args):
+    ws, rank, lrank = dist_env()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    # inner PCG iterations per step of the plain method on this workload (FP64, SGS V-cycle, measured
+    # by the oracle's own Lanczos on a bounded sample: 2 Lanczos steps, extrapolated to k=16)
+    import oracle as O
+    from robtop_b200 import configs
+
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    cfg = configs.worst_case_box(WORKLOAD["nx"], WORKLOAD["ny"], WORKLOAD["nz"], seed=WORKLOAD["seed"])
+    H = O.Hierarchy(cfg["eact"], cfg["rho"], cfg["vfix"], p=3, E=1e6, nu=0.4)
+    nv = H.arrs[0]["u"].size // 3
+    nl = cfg["load_nodes"].size
+    times = []
+    for s in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        H.update_stencil()
+        ksample = 2
+        work = np.zeros((ksample + 1) * 3 * nl + 10 * 3 * nv)
+        lam = np.zeros(1)
+        inner = O.lib().or_lanczos(H.LA, H.nlev, O.ptr(H.KE), O.SMOOTH_SGS, 1, 1, 0.6, nl,
+                                   O.ptr(cfg["load_nodes"]), O.ptr(np.ascontiguousarray(cfg["normals"])), 0, 0, None,
+                                   100 + s, ksample, WORKLOAD["tol"], 500, O.ptr(lam), None, O.ptr(work))
+        dt = time.perf_counter() - t0
+        # the full step runs k Lanczos solves plus the final displacement solve
+        scale_f = (WORKLOAD["k"] + 1) / ksample
+        times.append(dt * scale_f)
+    tt = times[args.warmup:]
+    sec = sum(tt) / len(tt)
+    val = 1.0 / sec
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "worst-case 128x128x64 (z=0 clamped, top-face load set, wsff), Lanczos k=16",
+                       "inner_tol": WORKLOAD["tol"], "threads": threads},
+            "cpu_baseline": {"value": val, "unit": "solves/s", "cores": threads, "kind": "port",
+                             "sample": "CPU restatement of the reference algorithm (the reference needs Eigen/CGAL/"
+                                       "OpenVDB and cannot be built here): stencil assembly + 2 of the 16 Lanczos "
+                                       "inner solves per step, time scaled by 17/2"},
+            "e2e": {"value": val, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    ws, rank, lrank = dist_env()
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(lrank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", lrank))
+
+    import robtop_b200 as rb
+    from robtop_b200 import configs
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+
+    ctx = make_ctx(rb, lrank)
+    cfg, G = build_problem(rb, configs, ctx, rb.FP32)
+    results = {}
+    for prec in (rb.FP64, rb.FP32):
+        p = G.params
+        p.precision = prec
+        G.set_params(p)
+        for w in range(max(args.warmup, 3)):
+            step(rb, G, 10 + w)
+        if dist:
+            dist.barrier()
+        clocks = Clocks(lrank) if prec == rb.FP32 else None
+        if clocks:
+            clocks.start()
+        ms, lams, infos, nlaunch = time_steps(rb, ctx, G, args.steps)
+        clk = clocks.stop() if clocks else None
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        results[prec] = dict(ms=ms, lams=lams, infos=[i.as_dict() for i in infos], launches=nlaunch, clocks=clk)
+
+    # per-kernel device time over the same K steps (CUDA events around every launch; separate pass)
+    ctx.profile(True)
+    ctx.profile_reset()
+    time_steps(rb, ctx, G, args.steps)
+    stats = ctx.profile_stats()
+    ctx.profile(False)
+    stats = {k: v for k, v in stats.items() if v[0] > 0}
+    roof = roofline(ctx, stats, G, peaks)
+    top = sorted(stats.items(), key=lambda kv: -kv[1][1])[:8]
+
+    # end to end through the public API with host buffers
+    e2e_ms, h2d, d2h = e2e_steps(rb, ctx, G, cfg, args.steps)
+
+    r32, r64 = results[rb.FP32], results[rb.FP64]
+    ms_step = r32["ms"] / args.steps
+    value = ws * args.steps / (r32["ms"] * 1e-3)
+    lam32 = float(np.mean(r32["lams"]))
+    lam64 = float(np.mean(r64["lams"]))
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+        "config": {"workload": "worst-case 128x128x64 (smoothed random density, z=0 clamped, top-face load set, "
+                               "wsff), Lanczos k=16, inner MG-PCG to 1e-6, stencil assembly included",
+                   "form": "mixed: FP32 V-cycle (SGS 1/1) inside FP64 flexible CG",
+                   "fp64_ms_per_step": r64["ms"] / args.steps,
+                   "speedup_vs_fp64": r64["ms"] / r32["ms"],
+                   "lambda_mixed": lam32, "lambda_fp64": lam64,
+                   "lambda_rel_diff": abs(lam32 - lam64) / abs(lam64),
+                   "inner_pcg_iterations": r32["infos"][0]["inner_iterations"],
+                   "inner_pcg_iterations_fp64": r64["infos"][0]["inner_iterations"],
+                   "l2": "working set ~0.4 GB of vectors and stencils > 126 MB L2 per step",
+                   "parallelism": f"replicas x{ws}"},
+        "clocks": r32["clocks"],
+        "gpu_launches": r32["launches"],
+        "roofline": roof,
+        "kernel_top": {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in top},
+        "e2e": {"value": ws * args.steps / (e2e_ms * 1e-3), "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(r32["infos"][0]["inner_iterations"], r32["infos"][0]["vcycles"],
+                                            os.cpu_count() or 1)
+    if rank == 0:
+        print(json.dumps(line))
+    G.close()
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

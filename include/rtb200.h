@@ -1,0 +1,203 @@
+/*
+ * rtb200.h — C ABI of the B200-native (sm_100a) robtop solver hot path.
+ *
+ * The library replaces the GPU solver of lavenklau/robtop: the matrix-free
+ * geometric multigrid for SIMP-penalised hex8 elasticity on a voxel grid
+ * (grid/Grid.{h,cpp,cu}), the worst-case-load eigen-solve
+ * (optimization/optimization.cpp:123-261, optimization/projection.*), and the
+ * sensitivity / filter / OC density update (optimization/optimization.cu).
+ *
+ * Conventions
+ *  - Every entry point returns an int status (RT_OK on success); the text of
+ *    the last failure is available from rt_last_error(ctx).  The reference
+ *    printed and continued (culib/cudaCommon.cuh:6-11) or called exit(-1)
+ *    (optimization/optimization.cpp:81,234,254); this ABI never exits.
+ *  - Pointers are plain host pointers unless the argument name ends in _dev.
+ *  - "Dense" node vectors are SoA [3][nv] with nv = (nx+1)(ny+1)(nz+1), x
+ *    fastest; element arrays are [ne] = nx*ny*nz, x fastest.  Level 0 is the
+ *    finest grid.  RT_LAYOUT_REF_GS selects the reference's Gauss-Seidel
+ *    colour-ordered, 32-padded layout (grid/Grid.cpp:2045-2106) instead.
+ *  - A context owns one CUDA stream (or borrows the caller's); every call is
+ *    ordered on it.  Contexts and hierarchies are independent of each other
+ *    (the reference rebinds global __constant__ tables per level,
+ *    grid/Grid.cu:48-75, and is not reentrant).
+ */
+#ifndef RTB200_H
+#define RTB200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum rt_status {
+    RT_OK = 0,
+    RT_EINVAL = 1,    /* bad argument */
+    RT_ECUDA = 2,     /* CUDA runtime error */
+    RT_ENOCONV = 3,   /* iteration cap reached before the tolerance */
+    RT_ENAN = 4,      /* NaN/Inf met in a solve */
+    RT_ETIMEOUT = 5,  /* a bounded device wait gave up */
+    RT_ENOMEM = 6,    /* device allocation failed */
+    RT_ESTATE = 7     /* call out of order (e.g. solve before update_stencil) */
+};
+
+/* robtop's work modes, same order as grid::Mode (grid/Grid.h:139-144) */
+enum rt_mode {
+    RT_MODE_NSCF = 0, /* no support, load direction constrained to the surface normal */
+    RT_MODE_NSFF = 1, /* no support, free load direction */
+    RT_MODE_WSCF = 2, /* with support, constrained direction */
+    RT_MODE_WSFF = 3  /* with support, free direction */
+};
+
+enum rt_smoother { RT_SMOOTH_GS = 0, RT_SMOOTH_SGS = 1, RT_SMOOTH_JACOBI = 2 };
+enum rt_precision { RT_FP64 = 0, RT_FP32 = 1 };
+enum rt_layout { RT_LAYOUT_DENSE = 0, RT_LAYOUT_REF_GS = 1 };
+enum rt_field { RT_FIELD_U = 0, RT_FIELD_F = 1, RT_FIELD_R = 2, RT_FIELD_RHO = 3, RT_FIELD_SENS = 4,
+                RT_FIELD_STENCIL = 5, RT_FIELD_VACT = 6, RT_FIELD_EACT = 7, RT_FIELD_VFIX = 8 };
+enum rt_worst_method { RT_WORST_MODPM = 0, RT_WORST_LANCZOS = 1 };
+
+/* Parameter block: optimization/optimization.h:11-22 plus the solver knobs the
+ * reference hard-codes (GS 1/1 sweeps, optimization/optimization.cpp:169). */
+typedef struct rt_params {
+    float power_penalty;    /* SIMP exponent p */
+    float min_rho;          /* rho_min */
+    float volume_ratio;     /* volume target */
+    float design_step;      /* OC move limit */
+    float damp_ratio;       /* OC damping exponent eta */
+    float filter_radius;    /* sensitivity filter radius (the reference stores an int) */
+    double youngs_modulus;  /* E */
+    double poisson_ratio;   /* nu */
+    double element_length;  /* h */
+    int mode;               /* rt_mode */
+    int skip_layer1;        /* 1: first coarse level is 4x coarser (the reference always sets this) */
+    int smoother;           /* rt_smoother used by rt_pcg's V-cycle preconditioner */
+    int pre_sweeps, post_sweeps;
+    double jacobi_omega;
+    int precision;          /* rt_precision of the V-cycle inside rt_pcg / rt_worst_case */
+} rt_params;
+
+typedef struct rt_solve_info {
+    int iterations;         /* outer iterations (CG steps, power steps, Lanczos steps) */
+    int inner_iterations;   /* CG steps inside Lanczos / refinement */
+    int vcycles;            /* V-cycles applied */
+    int status;             /* rt_status of the solve */
+    double rel_residual;    /* final ||f - K u|| / ||f|| (FP64) */
+    double value;           /* compliance f.u or the eigenvalue */
+    double seconds;         /* device time of the call */
+} rt_solve_info;
+
+typedef struct rt_level_info {
+    int nx, ny, nz;         /* element box of the level */
+    int ratio;              /* 0 on level 0, else coarsening ratio to the next finer level */
+    long long n_nodes;      /* nodes in the box */
+    long long n_active_nodes;
+    long long n_active_elements;
+} rt_level_info;
+
+typedef struct rt_ctx rt_ctx;
+typedef struct rt_hier rt_hier;
+
+/* ---- context ------------------------------------------------------------ */
+int rt_ctx_create(int device, void* cuda_stream /* NULL: own stream */, rt_ctx** out);
+void rt_ctx_destroy(rt_ctx* ctx);
+const char* rt_last_error(rt_ctx* ctx);
+int rt_ctx_sync(rt_ctx* ctx);
+void rt_params_default(rt_params* p);
+/* per-kernel device-time accounting (CUDA events around each launch) */
+int rt_profile_enable(rt_ctx* ctx, int on);
+int rt_profile_query(rt_ctx* ctx, int idx, char* name, int name_len, long long* launches, double* ms);
+int rt_profile_reset(rt_ctx* ctx);
+/* number of kernels this context has launched since creation */
+long long rt_launch_count(rt_ctx* ctx);
+
+/* ---- hierarchy ------------------------------------------------------------
+ * replaces HierarchyGrid::genFromMesh(solid_bit, out_reso) (grid/Grid.cpp:455-712)
+ * and Grid::build (grid/Grid.cpp:1513-1677).  The coarsening stops when at
+ * most 400 elements are solid (grid/Grid.cpp:488). */
+int rt_hier_create(rt_ctx* ctx, const rt_params* p, int nx, int ny, int nz, const uint8_t* eact, rt_hier** out);
+/* solid_bits: cubic reso^3 bit grid, bit x + y*reso + z*reso^2, LSB-first words
+ * (the bit layout genFromMesh(solid_bit, out_reso) takes) */
+int rt_hier_create_from_bits(rt_ctx* ctx, const rt_params* p, int reso, const uint32_t* solid_bits, rt_hier** out);
+void rt_hier_destroy(rt_hier* h);
+int rt_hier_n_levels(rt_hier* h);
+int rt_hier_level_info(rt_hier* h, int level, rt_level_info* out);
+int rt_hier_set_params(rt_hier* h, const rt_params* p);
+int rt_hier_get_params(rt_hier* h, rt_params* p);
+/* element template (element/templateMatrix.cpp:31-124), 24x24 row-major */
+int rt_template_matrix(rt_hier* h, double* KE);
+
+/* occupancy hierarchy on the reference's cubic bit grid, on the device
+ * (cubeGridSetSolidVertices_g, setSolidElementFromFineGrid_g: grid/Grid.cu:2555-2648) */
+int rt_cube_vertex_bits(rt_ctx* ctx, int reso, const uint32_t* ebits, uint32_t* vbits);
+int rt_cube_coarsen_bits(rt_ctx* ctx, int reso, const uint32_t* ebits_fine, uint32_t* ebits_coarse);
+
+/* ---- boundary conditions ------------------------------------------------- */
+/* surface nodes of level 0 (mark_surface_nodes_kernel, grid/Grid.cu:2005-2039), dense node order */
+int rt_surface_nodes(rt_hier* h, uint8_t* surf);
+/* support flags on level-0 nodes (Grid::computeProjectionMatrix, grid/Grid.cpp:1291-1403) */
+int rt_set_support(rt_hier* h, const uint8_t* vfix);
+/* load set: dense level-0 node ids with their outward unit normals [3*nload]
+ * (setLoadNodes, optimization/projection.cpp:129-269) */
+int rt_set_load_nodes(rt_hier* h, int nload, const int* nodes, const double* normals);
+
+/* ---- fields ---------------------------------------------------------------
+ * level-0 density: replaces Grid::init_rho / direct writes into getRho() */
+int rt_init_density(rt_hier* h, float rho);
+int rt_put(rt_hier* h, int field, int level, int layout, const void* src);
+int rt_get(rt_hier* h, int field, int level, int layout, void* dst);
+int rt_put_dev(rt_hier* h, int field, int level, const void* src_dev);
+int rt_get_dev(rt_hier* h, int field, int level, void* dst_dev);
+/* reference GS-order map of a level: vidmap[dense node] = GS slot or -1, and the GS slot count */
+int rt_ref_gs_map(rt_hier* h, int level, int* vidmap, int* n_gs, int* gs_num /*[8]*/);
+
+/* ---- multigrid operators (grid/Grid.cu) ----------------------------------- */
+/* Galerkin coarse stencils + coarsest factorisation: HierarchyGrid::update_stencil (grid/Grid.cpp:2108-2119) */
+int rt_update_stencil(rt_hier* h);
+/* Grid::update_residual (grid/Grid.cu:1644-1678): r = f - K u on a level */
+int rt_update_residual(rt_hier* h, int level);
+/* Grid::gs_relax (grid/Grid.cu:1068-1111) and the other smoothers */
+int rt_smooth(rt_hier* h, int level, int smoother, int sweeps, double omega);
+/* Grid::restrict_residual (grid/Grid.cu:1796-1816): f[level] = P^T r[level-1] */
+int rt_restrict_residual(rt_hier* h, int level);
+/* Grid::prolongate_correction (grid/Grid.cu:1898-1915): u[level] += P u[level+1] */
+int rt_prolongate_correction(rt_hier* h, int level);
+/* Grid::solve_fem_host (grid/Grid.cpp:1981-2043), on the device: u = A^+ f on the coarsest level */
+int rt_coarsest_solve(rt_hier* h);
+/* HierarchyGrid::v_cycle (grid/Grid.cpp:1068-1113) on level-0 u/f; returns ||r||/||f|| */
+int rt_vcycle(rt_hier* h, int pre, int post, double* rel_res);
+/* Grid::applyK (grid/Grid.cu:2519-2532): out = K(rho) u on level 0, dense device vectors */
+int rt_apply_K_dev(rt_hier* h, const double* u_dev, double* out_dev);
+int rt_apply_K(rt_hier* h, const double* u, double* out);
+/* Grid::compliance (grid/Grid.cpp:1976-1979): f.u on level 0 */
+int rt_compliance(rt_hier* h, double* c);
+/* Grid::relative_residual (grid/Grid.cu:1946-1951) */
+int rt_relative_residual(rt_hier* h, double* rel);
+
+/* ---- solvers -------------------------------------------------------------- */
+/* MG-preconditioned CG on level 0: u <- K^-1 f to ||r||/||f|| <= tol (solveFEM's role,
+ * optimization/optimization.cpp:85-91).  Uses the precision/smoother in the params. */
+int rt_pcg(rt_hier* h, double tol, int maxit, rt_solve_info* info);
+/* worst-case load: largest eigenvalue of P K^-1 P on the load set.
+ * RT_WORST_MODPM restates modifiedPM (optimization/optimization.cpp:123-261);
+ * RT_WORST_LANCZOS runs k Lanczos steps with PCG inner solves to inner_tol.
+ * On return level-0 f holds the worst-case load and u = K^-1 f. */
+int rt_worst_case(rt_hier* h, int method, int k, double inner_tol, uint64_t seed, double* lambda,
+                  rt_solve_info* info);
+
+/* ---- optimisation step (optimization/optimization.cu) --------------------- */
+/* computeSensitivity (optimization/optimization.cu:109-133) including the filter */
+int rt_sensitivity(rt_hier* h, int filter);
+/* Grid::filterSensitivity (grid/Grid.cu:2411-2437) alone */
+int rt_filter_sensitivity(rt_hier* h, float radius);
+/* updateDensities (optimization/optimization.cu:164-226); returns the multiplier */
+int rt_oc_update(rt_hier* h, float vgoal, float* lambda_out, int* trials_out);
+/* one OC iteration of optimization() (optimization/optimization.cpp:611-656):
+ * update_stencil, worst-case solve, sensitivity+filter, OC update */
+int rt_oc_iteration(rt_hier* h, int method, int k, double inner_tol, uint64_t seed, float vgoal,
+                    double* compliance_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

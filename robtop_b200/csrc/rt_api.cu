@@ -1,0 +1,1416 @@
+// rt_api.cu — C ABI entry points and host orchestration of the solver.
+//
+// The host side only sequences kernels on the context stream; every
+// arithmetic step of the hot path runs on the GPU.  Host work is limited to
+// set-up bookkeeping (level plan, index maps, load-set rigid basis) and to
+// reading back convergence scalars.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "rt_internal.h"
+
+// ---------------------------------------------------------------------------
+// errors, launch accounting
+// ---------------------------------------------------------------------------
+int rt_fail(rt_ctx* c, int code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+int rt_kernel_id(rt_ctx* c, const char* name) {
+    for (size_t i = 0; i < c->kstats.size(); i++)
+        if (c->kstats[i].name == name) return (int)i;
+    rt_kstat k;
+    k.name = name;
+    c->kstats.push_back(k);
+    return (int)c->kstats.size() - 1;
+}
+
+static cudaEvent_t ev_get(rt_ctx* c) {
+    if (!c->ev_pool.empty()) {
+        cudaEvent_t e = c->ev_pool.back();
+        c->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+
+static void profile_drain(rt_ctx* c) {
+    for (auto& p : c->pending) {
+        float ms = 0;
+        cudaEventSynchronize(p.b);
+        cudaEventElapsedTime(&ms, p.a, p.b);
+        c->kstats[p.kid].ms += ms;
+        c->ev_pool.push_back(p.a);
+        c->ev_pool.push_back(p.b);
+    }
+    c->pending.clear();
+}
+
+void rt_launch_begin(rt_ctx* c, int kid, cudaEvent_t* a) {
+    (void)kid;
+    if (c->profile) {
+        *a = ev_get(c);
+        cudaEventRecord(*a, c->stream);
+    }
+}
+
+int rt_launch_end(rt_ctx* c, int kid, cudaEvent_t a, const char* name) {
+    c->launches++;
+    c->kstats[kid].launches++;
+    cudaError_t e = cudaGetLastError();
+    if (c->profile) {
+        cudaEvent_t b = ev_get(c);
+        cudaEventRecord(b, c->stream);
+        c->pending.push_back({kid, a, b});
+        if (c->pending.size() > 4096) profile_drain(c);
+    }
+    if (e != cudaSuccess) return rt_fail(c, RT_ECUDA, "launch of %s failed: %s", name, cudaGetErrorString(e));
+    return RT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+extern "C" int rt_ctx_create(int device, void* stream, rt_ctx** out) {
+    if (!out) return RT_EINVAL;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return RT_ECUDA;
+    if (device < 0 || device >= ndev) return RT_EINVAL;
+    if (cudaSetDevice(device) != cudaSuccess) return RT_ECUDA;
+    rt_ctx* c = new rt_ctx();
+    c->device = device;
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (stream) {
+        c->stream = (cudaStream_t)stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete c;
+            return RT_ECUDA;
+        }
+        c->own_stream = true;
+    }
+    if (cudaMallocHost(&c->hscal, sizeof(double) * 64) != cudaSuccess) {
+        delete c;
+        return RT_ECUDA;
+    }
+    *out = c;
+    return RT_OK;
+}
+
+extern "C" void rt_ctx_destroy(rt_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    profile_drain(c);
+    for (auto e : c->ev_pool) cudaEventDestroy(e);
+    if (c->hscal) cudaFreeHost(c->hscal);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+extern "C" const char* rt_last_error(rt_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+extern "C" int rt_ctx_sync(rt_ctx* c) {
+    if (!c) return RT_EINVAL;
+    RT_CUDA(c, cudaStreamSynchronize(c->stream));
+    return RT_OK;
+}
+
+extern "C" int rt_profile_enable(rt_ctx* c, int on) {
+    if (!c) return RT_EINVAL;
+    if (!on) {
+        cudaStreamSynchronize(c->stream);
+        profile_drain(c);
+    }
+    c->profile = on != 0;
+    return RT_OK;
+}
+
+extern "C" int rt_profile_reset(rt_ctx* c) {
+    if (!c) return RT_EINVAL;
+    cudaStreamSynchronize(c->stream);
+    profile_drain(c);
+    for (auto& k : c->kstats) { k.launches = 0; k.ms = 0; }
+    return RT_OK;
+}
+
+extern "C" int rt_profile_query(rt_ctx* c, int idx, char* name, int name_len, long long* launches, double* ms) {
+    if (!c) return RT_EINVAL;
+    cudaStreamSynchronize(c->stream);
+    profile_drain(c);
+    if (idx < 0 || idx >= (int)c->kstats.size()) return RT_EINVAL;
+    if (name && name_len > 0) {
+        strncpy(name, c->kstats[idx].name.c_str(), name_len - 1);
+        name[name_len - 1] = 0;
+    }
+    if (launches) *launches = c->kstats[idx].launches;
+    if (ms) *ms = c->kstats[idx].ms;
+    return RT_OK;
+}
+
+extern "C" long long rt_launch_count(rt_ctx* c) { return c ? c->launches : 0; }
+
+extern "C" void rt_params_default(rt_params* p) {
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    p->power_penalty = 3.f;
+    p->min_rho = 1e-3f;
+    p->volume_ratio = 0.4f;
+    p->design_step = 0.03f;
+    p->damp_ratio = 0.5f;
+    p->filter_radius = 2.f;
+    p->youngs_modulus = 1e6;
+    p->poisson_ratio = 0.4;
+    p->element_length = 1.0;
+    p->mode = RT_MODE_WSFF;
+    p->skip_layer1 = 1;
+    p->smoother = RT_SMOOTH_SGS;
+    p->pre_sweeps = 1;
+    p->post_sweeps = 1;
+    p->jacobi_omega = 0.6;
+    p->precision = RT_FP64;
+}
+
+// ---------------------------------------------------------------------------
+// element template: element/templateMatrix.cpp:15-124 (host, once per parameter set)
+// ---------------------------------------------------------------------------
+static void template_matrix(double E, double nu, double h, double* KE) {
+    double D[6][6] = {};
+    const double s = E / ((1 + nu) * (1 - 2 * nu));
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) D[i][j] = s * (i == j ? 1 - nu : nu);
+    for (int i = 3; i < 6; i++) D[i][i] = s * (1 - 2 * nu) / 2;
+    const double p = std::sqrt(3.0) / 3;
+    std::fill(KE, KE + 576, 0.0);
+    for (int g = 0; g < 8; g++) {
+        const double gp[3] = {((2 * (g % 2) - 1) * p + 1) / 2, ((2 * (g / 2 % 2) - 1) * p + 1) / 2,
+                              ((2 * (g / 4) - 1) * p + 1) / 2};
+        double gN[8][3];
+        for (int k = 0; k < 8; k++) {
+            const int id[3] = {k % 2, k / 2 % 2, k / 4};
+            double r[3];
+            for (int a = 0; a < 3; a++) r[a] = id[a] ? gp[a] : 1 - gp[a];
+            for (int a = 0; a < 3; a++) gN[k][a] = (id[a] ? 1.0 / h : -1.0 / h) * r[(a + 1) % 3] * r[(a + 2) % 3];
+        }
+        double B[6][24] = {};
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 8; b++) B[a][3 * b + a] = gN[b][a];
+        for (int b = 0; b < 8; b++) {
+            B[3][3 * b + 1] = gN[b][2]; B[3][3 * b + 2] = gN[b][1];
+            B[4][3 * b + 0] = gN[b][2]; B[4][3 * b + 2] = gN[b][0];
+            B[5][3 * b + 0] = gN[b][1]; B[5][3 * b + 1] = gN[b][0];
+        }
+        for (int i = 0; i < 24; i++)
+            for (int j = 0; j < 24; j++) {
+                double acc = 0;
+                for (int a = 0; a < 6; a++)
+                    for (int b = 0; b < 6; b++) acc += B[a][i] * D[a][b] * B[b][j];
+                KE[i * 24 + j] += acc;
+            }
+    }
+    const double sc = std::pow(h / 2, 3);
+    for (int i = 0; i < 576; i++) KE[i] *= sc;
+}
+
+// ---------------------------------------------------------------------------
+// hierarchy
+// ---------------------------------------------------------------------------
+template <typename T>
+static int dalloc(rt_ctx* c, T** p, size_t n) {
+    if (n == 0) n = 1;
+    if (cudaMalloc((void**)p, sizeof(T) * n) != cudaSuccess) {
+        cudaGetLastError();
+        return rt_fail(c, RT_ENOMEM, "cudaMalloc of %zu bytes failed", sizeof(T) * n);
+    }
+    return RT_OK;
+}
+
+static void free_hier(rt_hier* h) {
+    if (!h) return;
+    for (auto& L : h->L) {
+        cudaFree(L.vact); cudaFree(L.eact); cudaFree(L.u); cudaFree(L.f); cudaFree(L.r);
+        cudaFree(L.u32); cudaFree(L.f32); cudaFree(L.r32); cudaFree(L.st); cudaFree(L.st32);
+        cudaFree(L.aidx); cudaFree(L.ainv); cudaFree(L.ainv32); cudaFree(L.dvec); cudaFree(L.dvec32);
+    }
+    cudaFree(h->KE_dev); cudaFree(h->KE32_dev); cudaFree(h->rho); cudaFree(h->w); cudaFree(h->vfix);
+    cudaFree(h->sens); cudaFree(h->ftmp); cudaFree(h->eshell); cudaFree(h->load_nodes); cudaFree(h->load_normal);
+    cudaFree(h->Rd); cudaFree(h->Ru); cudaFree(h->fs); cudaFree(h->fs_old); cudaFree(h->x); cudaFree(h->rr);
+    cudaFree(h->z); cudaFree(h->p); cudaFree(h->q); cudaFree(h->rold); cudaFree(h->Q); cudaFree(h->partials);
+    cudaFree(h->scal); cudaFree(h->Qgal);
+    delete h;
+}
+
+static int upload_KE(rt_hier* h) {
+    template_matrix(h->P.youngs_modulus, h->P.poisson_ratio, h->P.element_length, h->KE);
+    float ke32[576];
+    for (int i = 0; i < 576; i++) ke32[i] = (float)h->KE[i];
+    RT_CUDA(h->ctx, cudaMemcpyAsync(h->KE_dev, h->KE, sizeof(double) * 576, cudaMemcpyHostToDevice, h->ctx->stream));
+    RT_CUDA(h->ctx, cudaMemcpyAsync(h->KE32_dev, ke32, sizeof(float) * 576, cudaMemcpyHostToDevice, h->ctx->stream));
+    RT_CUDA(h->ctx, cudaStreamSynchronize(h->ctx->stream));
+    if (h->Qgal) { cudaFree(h->Qgal); h->Qgal = nullptr; h->Qgal_ratio = 0; }
+    return RT_OK;
+}
+
+static int build_hier(rt_ctx* c, const rt_params* p, int nx, int ny, int nz, uint8_t* eact_dev, rt_hier** out) {
+    rt_hier* h = new rt_hier();
+    h->ctx = c;
+    h->P = *p;
+    // level chain on the device: halve while more than 400 elements are solid (grid/Grid.cpp:488)
+    struct Chain { int nx, ny, nz; uint8_t* e; long cnt; };
+    std::vector<Chain> chain;
+    double* dcnt = nullptr;
+    RT_CUDA(c, cudaMalloc(&dcnt, sizeof(double)));
+    chain.push_back({nx, ny, nz, eact_dev, 0});
+    for (;;) {
+        Chain& last = chain.back();
+        long ne = (long)last.nx * last.ny * last.nz;
+        RT_CHECK(rtk::count_u8(c, ne, last.e, dcnt));
+        double hc = 0;
+        RT_CUDA(c, cudaMemcpyAsync(&hc, dcnt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        RT_CUDA(c, cudaStreamSynchronize(c->stream));
+        last.cnt = (long)hc;
+        if (last.cnt <= 400 || (last.nx <= 1 && last.ny <= 1 && last.nz <= 1)) break;
+        Chain nxt{(last.nx + 1) / 2, (last.ny + 1) / 2, (last.nz + 1) / 2, nullptr, 0};
+        RT_CHECK(dalloc(c, &nxt.e, (size_t)nxt.nx * nxt.ny * nxt.nz));
+        RT_CHECK(rtk::coarsen_elements(c, last.nx, last.ny, last.nz, 2, last.e, nxt.e));
+        chain.push_back(nxt);
+    }
+    cudaFree(dcnt);
+    std::vector<int> idx, ratio;
+    if (p->skip_layer1 && chain.size() >= 3) {
+        idx.push_back(0); ratio.push_back(0);
+        idx.push_back(2); ratio.push_back(4);
+        for (size_t i = 3; i < chain.size(); i++) { idx.push_back((int)i); ratio.push_back(2); }
+    } else {
+        for (size_t i = 0; i < chain.size(); i++) { idx.push_back((int)i); ratio.push_back(i ? 2 : 0); }
+    }
+    if (chain.size() == 1) return rt_fail(c, RT_EINVAL, "grid too small for multigrid (<= 400 solid elements)");
+    for (size_t k = 0; k < idx.size(); k++) {
+        Chain& ch = chain[idx[k]];
+        rt_level L;
+        L.nx = ch.nx; L.ny = ch.ny; L.nz = ch.nz;
+        L.vx = L.nx + 1; L.vy = L.ny + 1; L.vz = L.nz + 1;
+        L.nv = (long)L.vx * L.vy * L.vz;
+        L.ne = (long)L.nx * L.ny * L.nz;
+        L.ratio = ratio[k];
+        L.n_act_elems = ch.cnt;
+        L.eact = ch.e;
+        ch.e = nullptr;
+        h->L.push_back(L);
+    }
+    for (auto& ch : chain) if (ch.e) cudaFree(ch.e);
+    for (size_t k = 0; k < h->L.size(); k++) {
+        rt_level& L = h->L[k];
+        if ((double)L.nv * 243.0 >= 2147483647.0 && k > 0) return rt_fail(c, RT_EINVAL, "coarse level too large");
+        RT_CHECK(dalloc(c, &L.vact, L.nv));
+        RT_CHECK(rtk::node_active(c, L.nx, L.ny, L.nz, L.eact, L.vact));
+        RT_CHECK(dalloc(c, &L.u, 3 * L.nv)); RT_CHECK(dalloc(c, &L.f, 3 * L.nv)); RT_CHECK(dalloc(c, &L.r, 3 * L.nv));
+        RT_CHECK(dalloc(c, &L.u32, 3 * L.nv)); RT_CHECK(dalloc(c, &L.f32, 3 * L.nv)); RT_CHECK(dalloc(c, &L.r32, 3 * L.nv));
+        RT_CUDA(c, cudaMemsetAsync(L.u, 0, sizeof(double) * 3 * L.nv, c->stream));
+        RT_CUDA(c, cudaMemsetAsync(L.f, 0, sizeof(double) * 3 * L.nv, c->stream));
+        RT_CUDA(c, cudaMemsetAsync(L.r, 0, sizeof(double) * 3 * L.nv, c->stream));
+        if (k > 0) {
+            RT_CHECK(dalloc(c, &L.st, 243 * L.nv));
+            RT_CHECK(dalloc(c, &L.st32, 243 * L.nv));
+            RT_CUDA(c, cudaMemsetAsync(L.st, 0, sizeof(double) * 243 * L.nv, c->stream));
+        }
+        std::vector<uint8_t> va(L.nv);
+        RT_CUDA(c, cudaMemcpyAsync(va.data(), L.vact, L.nv, cudaMemcpyDeviceToHost, c->stream));
+        RT_CUDA(c, cudaStreamSynchronize(c->stream));
+        long na = 0;
+        for (long v = 0; v < L.nv; v++) na += va[v];
+        L.n_act_nodes = na;
+        if (k + 1 == h->L.size()) {
+            std::vector<int> aidx;
+            for (long v = 0; v < L.nv; v++)
+                if (va[v]) aidx.push_back((int)v);
+            L.na = (int)aidx.size();
+            const size_t n = 3 * (size_t)L.na;
+            if (n > 6000) return rt_fail(c, RT_EINVAL, "coarsest level too large for the dense solve (%zu DOF)", n);
+            RT_CHECK(dalloc(c, &L.aidx, L.na));
+            RT_CUDA(c, cudaMemcpyAsync(L.aidx, aidx.data(), sizeof(int) * L.na, cudaMemcpyHostToDevice, c->stream));
+            RT_CHECK(dalloc(c, &L.ainv, n * n));
+            RT_CHECK(dalloc(c, &L.ainv32, n * n));
+            RT_CHECK(dalloc(c, &L.dvec, n));
+            RT_CHECK(dalloc(c, &L.dvec32, n));
+            RT_CUDA(c, cudaStreamSynchronize(c->stream));
+        }
+    }
+    rt_level& L0 = h->L[0];
+    RT_CHECK(dalloc(c, &h->KE_dev, 576));
+    RT_CHECK(dalloc(c, &h->KE32_dev, 576));
+    RT_CHECK(dalloc(c, &h->rho, L0.ne));
+    RT_CHECK(dalloc(c, &h->w, L0.ne));
+    RT_CHECK(dalloc(c, &h->vfix, L0.nv));
+    RT_CHECK(dalloc(c, &h->sens, L0.ne));
+    RT_CHECK(dalloc(c, &h->ftmp, L0.ne));
+    RT_CUDA(c, cudaMemsetAsync(h->vfix, 0, L0.nv, c->stream));
+    RT_CUDA(c, cudaMemsetAsync(h->sens, 0, sizeof(float) * L0.ne, c->stream));
+    const size_t n3 = 3 * (size_t)L0.nv;
+    RT_CHECK(dalloc(c, &h->x, n3)); RT_CHECK(dalloc(c, &h->rr, n3)); RT_CHECK(dalloc(c, &h->z, n3));
+    RT_CHECK(dalloc(c, &h->p, n3)); RT_CHECK(dalloc(c, &h->q, n3)); RT_CHECK(dalloc(c, &h->rold, n3));
+    RT_CHECK(dalloc(c, &h->partials, RT_PARTIALS));
+    RT_CHECK(dalloc(c, &h->scal, RT_NSCAL));
+    RT_CUDA(c, cudaMemsetAsync(h->scal, 0, sizeof(double) * RT_NSCAL, c->stream));
+    RT_CHECK(upload_KE(h));
+    *out = h;
+    return RT_OK;
+}
+
+extern "C" int rt_hier_create(rt_ctx* c, const rt_params* p, int nx, int ny, int nz, const uint8_t* eact,
+                              rt_hier** out) {
+    if (!c || !p || !eact || !out || nx <= 0 || ny <= 0 || nz <= 0) return RT_EINVAL;
+    *out = nullptr;
+    RT_CUDA(c, cudaSetDevice(c->device));
+    uint8_t* e = nullptr;
+    const size_t ne = (size_t)nx * ny * nz;
+    RT_CHECK(dalloc(c, &e, ne));
+    RT_CUDA(c, cudaMemcpyAsync(e, eact, ne, cudaMemcpyHostToDevice, c->stream));
+    rt_hier* h = nullptr;
+    int s = build_hier(c, p, nx, ny, nz, e, &h);
+    if (s != RT_OK) {
+        if (h) free_hier(h);
+        return s;
+    }
+    *out = h;
+    return RT_OK;
+}
+
+// genFromMesh(solid_bit, out_reso) takes a cubic reso^3 bit grid; the dense box is
+// the solid's extent from the origin (coarsening stays aligned with the cube's).
+extern "C" int rt_hier_create_from_bits(rt_ctx* c, const rt_params* p, int reso, const uint32_t* bits, rt_hier** out) {
+    if (!c || !p || !bits || !out || reso <= 0) return RT_EINVAL;
+    int mx = 0, my = 0, mz = 0;
+    const long nb = (long)reso * reso * reso;
+    for (long t = 0; t < nb; t++)
+        if ((bits[t >> 5] >> (t & 31)) & 1u) {
+            mx = std::max(mx, (int)(t % reso) + 1);
+            my = std::max(my, (int)((t / reso) % reso) + 1);
+            mz = std::max(mz, (int)(t / ((long)reso * reso)) + 1);
+        }
+    if (mx == 0) return rt_fail(c, RT_EINVAL, "empty solid");
+    std::vector<uint8_t> e((size_t)mx * my * mz, 0);
+    for (int z = 0; z < mz; z++)
+        for (int y = 0; y < my; y++)
+            for (int x = 0; x < mx; x++) {
+                long t = x + (long)reso * (y + (long)reso * z);
+                e[x + (size_t)mx * (y + (size_t)my * z)] = (bits[t >> 5] >> (t & 31)) & 1u;
+            }
+    return rt_hier_create(c, p, mx, my, mz, e.data(), out);
+}
+
+extern "C" void rt_hier_destroy(rt_hier* h) {
+    if (!h) return;
+    cudaSetDevice(h->ctx->device);
+    cudaStreamSynchronize(h->ctx->stream);
+    free_hier(h);
+}
+
+extern "C" int rt_hier_n_levels(rt_hier* h) { return h ? (int)h->L.size() : 0; }
+
+extern "C" int rt_hier_level_info(rt_hier* h, int lvl, rt_level_info* out) {
+    if (!h || !out || lvl < 0 || lvl >= (int)h->L.size()) return RT_EINVAL;
+    rt_level& L = h->L[lvl];
+    out->nx = L.nx; out->ny = L.ny; out->nz = L.nz; out->ratio = L.ratio;
+    out->n_nodes = L.nv; out->n_active_nodes = L.n_act_nodes; out->n_active_elements = L.n_act_elems;
+    return RT_OK;
+}
+
+extern "C" int rt_hier_get_params(rt_hier* h, rt_params* p) {
+    if (!h || !p) return RT_EINVAL;
+    *p = h->P;
+    return RT_OK;
+}
+
+extern "C" int rt_hier_set_params(rt_hier* h, const rt_params* p) {
+    if (!h || !p) return RT_EINVAL;
+    const bool ke = p->youngs_modulus != h->P.youngs_modulus || p->poisson_ratio != h->P.poisson_ratio ||
+                    p->element_length != h->P.element_length;
+    if (p->skip_layer1 != h->P.skip_layer1)
+        return rt_fail(h->ctx, RT_EINVAL, "skip_layer1 is fixed when the hierarchy is built");
+    h->P = *p;
+    if (ke) RT_CHECK(upload_KE(h));
+    h->stencil_ready = false;
+    return RT_OK;
+}
+
+extern "C" int rt_template_matrix(rt_hier* h, double* KE) {
+    if (!h || !KE) return RT_EINVAL;
+    memcpy(KE, h->KE, sizeof(double) * 576);
+    return RT_OK;
+}
+
+extern "C" int rt_cube_vertex_bits(rt_ctx* c, int reso, const uint32_t* eb, uint32_t* vb) {
+    if (!c || !eb || !vb || reso <= 0) return RT_EINVAL;
+    const size_t ne = ((size_t)reso * reso * reso + 31) / 32, nv = ((size_t)(reso + 1) * (reso + 1) * (reso + 1) + 31) / 32;
+    uint32_t *de = nullptr, *dv = nullptr;
+    RT_CHECK(dalloc(c, &de, ne));
+    RT_CHECK(dalloc(c, &dv, nv));
+    RT_CUDA(c, cudaMemcpyAsync(de, eb, ne * 4, cudaMemcpyHostToDevice, c->stream));
+    int s = rtk::cube_vbits(c, reso, de, dv);
+    if (s == RT_OK) {
+        cudaMemcpyAsync(vb, dv, nv * 4, cudaMemcpyDeviceToHost, c->stream);
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess) s = RT_ECUDA;
+    }
+    cudaFree(de);
+    cudaFree(dv);
+    return s;
+}
+
+extern "C" int rt_cube_coarsen_bits(rt_ctx* c, int reso, const uint32_t* ef, uint32_t* ec) {
+    if (!c || !ef || !ec || reso < 2) return RT_EINVAL;
+    const int rc = reso / 2;
+    const size_t nf = ((size_t)reso * reso * reso + 31) / 32, ncw = ((size_t)rc * rc * rc + 31) / 32;
+    uint32_t *df = nullptr, *dc = nullptr;
+    RT_CHECK(dalloc(c, &df, nf));
+    RT_CHECK(dalloc(c, &dc, ncw));
+    RT_CUDA(c, cudaMemcpyAsync(df, ef, nf * 4, cudaMemcpyHostToDevice, c->stream));
+    int s = rtk::cube_coarsen(c, reso, df, dc);
+    if (s == RT_OK) {
+        cudaMemcpyAsync(ec, dc, ncw * 4, cudaMemcpyDeviceToHost, c->stream);
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess) s = RT_ECUDA;
+    }
+    cudaFree(df);
+    cudaFree(dc);
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// boundary conditions
+// ---------------------------------------------------------------------------
+extern "C" int rt_surface_nodes(rt_hier* h, uint8_t* surf) {
+    if (!h || !surf) return RT_EINVAL;
+    rt_level& L = h->L[0];
+    uint8_t* d = nullptr;
+    RT_CHECK(dalloc(h->ctx, &d, L.nv));
+    int s = rtk::surface_nodes(h, d);
+    if (s == RT_OK) {
+        cudaMemcpyAsync(surf, d, L.nv, cudaMemcpyDeviceToHost, h->ctx->stream);
+        if (cudaStreamSynchronize(h->ctx->stream) != cudaSuccess) s = RT_ECUDA;
+    }
+    cudaFree(d);
+    return s;
+}
+
+extern "C" int rt_set_support(rt_hier* h, const uint8_t* vfix) {
+    if (!h || !vfix) return RT_EINVAL;
+    rt_level& L = h->L[0];
+    long cnt = 0;
+    for (long v = 0; v < L.nv; v++) cnt += vfix[v] != 0;
+    RT_CUDA(h->ctx, cudaMemcpyAsync(h->vfix, vfix, L.nv, cudaMemcpyHostToDevice, h->ctx->stream));
+    RT_CUDA(h->ctx, cudaStreamSynchronize(h->ctx->stream));
+    h->has_support = cnt > 0;
+    h->stencil_ready = false;
+    return RT_OK;
+}
+
+// setLoadNodes (optimization/projection.cpp:129-269): rigid modes on the load set,
+// normal part only when the direction is constrained, Gram-Schmidt, degenerate dropped
+static int load_rigid_basis(rt_hier* h, const int* nodes, const double* normals) {
+    const int nl = h->nload;
+    const size_t n = 3 * (size_t)nl;
+    rt_level& L = h->L[0];
+    const bool constrain = (h->P.mode == RT_MODE_NSCF || h->P.mode == RT_MODE_WSCF);
+    const bool no_support = (h->P.mode == RT_MODE_NSCF || h->P.mode == RT_MODE_NSFF);
+    h->nrig = 0;
+    if (!no_support || nl == 0) return RT_OK;
+    std::vector<double> R(6 * n, 0.0);
+    for (int i = 0; i < nl; i++) {
+        const long v = nodes[i];
+        const double pz = (double)(v / ((long)L.vx * L.vy)), py = (double)((v / L.vx) % L.vy), px = (double)(v % L.vx);
+        const double ph[3][3] = {{0, -pz, py}, {pz, 0, -px}, {-py, px, 0}};
+        for (int t = 0; t < 3; t++) R[t * n + 3 * i + t] = 1.0;
+        for (int k = 0; k < 3; k++)
+            for (int t = 0; t < 3; t++) R[(3 + k) * n + 3 * i + t] = ph[t][k];
+    }
+    if (constrain)
+        for (int k = 0; k < 6; k++)
+            for (int i = 0; i < nl; i++) {
+                const double* nn = normals + 3 * i;
+                double* vv = &R[k * n + 3 * i];
+                const double d = vv[0] * nn[0] + vv[1] * nn[1] + vv[2] * nn[2];
+                for (int t = 0; t < 3; t++) vv[t] = d * nn[t];
+            }
+    bool invalid[6] = {false};
+    for (int k = 0; k < 6; k++) {
+        double* ck = &R[k * n];
+        double old = 0;
+        for (size_t q = 0; q < n; q++) old += ck[q] * ck[q];
+        old = std::sqrt(old);
+        for (int j = 0; j < k; j++) {
+            if (invalid[j]) continue;
+            double w = 0;
+            for (size_t q = 0; q < n; q++) w += ck[q] * R[j * n + q];
+            for (size_t q = 0; q < n; q++) ck[q] -= w * R[j * n + q];
+        }
+        double res = 0;
+        for (size_t q = 0; q < n; q++) res += ck[q] * ck[q];
+        res = std::sqrt(res);
+        if (res / old < 1e-6 || old < 1e-6) invalid[k] = true;
+        for (size_t q = 0; q < n; q++) ck[q] /= res;
+    }
+    std::vector<double> Rv;
+    for (int k = 0; k < 6; k++)
+        if (!invalid[k]) Rv.insert(Rv.end(), R.begin() + k * n, R.begin() + (k + 1) * n);
+    h->nrig = (int)(Rv.size() / std::max<size_t>(n, 1));
+    if (h->nrig > 0)
+        RT_CUDA(h->ctx, cudaMemcpyAsync(h->Rd, Rv.data(), sizeof(double) * Rv.size(), cudaMemcpyHostToDevice,
+                                        h->ctx->stream));
+    return RT_OK;
+}
+
+extern "C" int rt_set_load_nodes(rt_hier* h, int nload, const int* nodes, const double* normals) {
+    if (!h || nload < 0 || (nload > 0 && (!nodes || !normals))) return RT_EINVAL;
+    rt_ctx* c = h->ctx;
+    rt_level& L = h->L[0];
+    for (int i = 0; i < nload; i++)
+        if (nodes[i] < 0 || nodes[i] >= L.nv) return rt_fail(c, RT_EINVAL, "load node %d out of range", nodes[i]);
+    // keep load nodes sorted (setLoadNodes sorts them, optimization/projection.cpp:139-143)
+    std::vector<int> perm(nload);
+    for (int i = 0; i < nload; i++) perm[i] = i;
+    std::sort(perm.begin(), perm.end(), [&](int a, int b) { return nodes[a] < nodes[b]; });
+    std::vector<int> sn(nload);
+    std::vector<double> sN(3 * (size_t)nload);
+    for (int i = 0; i < nload; i++) {
+        sn[i] = nodes[perm[i]];
+        for (int t = 0; t < 3; t++) sN[3 * i + t] = normals[3 * perm[i] + t];
+    }
+    cudaFree(h->load_nodes); cudaFree(h->load_normal); cudaFree(h->Rd); cudaFree(h->fs); cudaFree(h->fs_old);
+    h->load_nodes = nullptr; h->load_normal = nullptr; h->Rd = nullptr; h->fs = nullptr; h->fs_old = nullptr;
+    h->nload = nload;
+    RT_CHECK(dalloc(c, &h->load_nodes, nload));
+    RT_CHECK(dalloc(c, &h->load_normal, 3 * (size_t)nload));
+    RT_CHECK(dalloc(c, &h->Rd, 6 * 3 * (size_t)nload));
+    RT_CHECK(dalloc(c, &h->fs, 3 * (size_t)nload));
+    RT_CHECK(dalloc(c, &h->fs_old, 3 * (size_t)nload));
+    if (nload > 0) {
+        RT_CUDA(c, cudaMemcpyAsync(h->load_nodes, sn.data(), sizeof(int) * nload, cudaMemcpyHostToDevice, c->stream));
+        RT_CUDA(c, cudaMemcpyAsync(h->load_normal, sN.data(), sizeof(double) * 3 * nload, cudaMemcpyHostToDevice,
+                                   c->stream));
+    }
+    RT_CHECK(load_rigid_basis(h, sn.data(), sN.data()));
+    RT_CUDA(c, cudaStreamSynchronize(c->stream));
+    return RT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// fields
+// ---------------------------------------------------------------------------
+static int field_ptr(rt_hier* h, int field, int lvl, void** ptr, size_t* bytes) {
+    if (lvl < 0 || lvl >= (int)h->L.size()) return RT_EINVAL;
+    rt_level& L = h->L[lvl];
+    switch (field) {
+        case RT_FIELD_U: *ptr = L.u; *bytes = sizeof(double) * 3 * L.nv; return RT_OK;
+        case RT_FIELD_F: *ptr = L.f; *bytes = sizeof(double) * 3 * L.nv; return RT_OK;
+        case RT_FIELD_R: *ptr = L.r; *bytes = sizeof(double) * 3 * L.nv; return RT_OK;
+        case RT_FIELD_STENCIL:
+            if (lvl == 0) return RT_EINVAL;
+            *ptr = L.st; *bytes = sizeof(double) * 243 * L.nv; return RT_OK;
+        case RT_FIELD_VACT: *ptr = L.vact; *bytes = L.nv; return RT_OK;
+        case RT_FIELD_EACT: *ptr = L.eact; *bytes = L.ne; return RT_OK;
+        case RT_FIELD_RHO: if (lvl) return RT_EINVAL; *ptr = h->rho; *bytes = sizeof(float) * L.ne; return RT_OK;
+        case RT_FIELD_SENS: if (lvl) return RT_EINVAL; *ptr = h->sens; *bytes = sizeof(float) * L.ne; return RT_OK;
+        case RT_FIELD_VFIX: if (lvl) return RT_EINVAL; *ptr = h->vfix; *bytes = L.nv; return RT_OK;
+    }
+    return RT_EINVAL;
+}
+
+// reference GS colour order of a level (grid/Grid.cpp:2045-2106): vertices by colour
+// x%2 + 2(y%2) + 4(z%2), bit order within a colour, each colour padded to 32
+static void ref_gs_order(int vx, int vy, int vz, const std::vector<uint8_t>& act, std::vector<int>& map, int& ngs,
+                         int gs_num[8]) {
+    long nv = (long)vx * vy * vz;
+    int cnt[8] = {0};
+    for (long v = 0; v < nv; v++)
+        if (act[v]) {
+            int x = v % vx, y = (v / vx) % vy, z = v / ((long)vx * vy);
+            cnt[(x & 1) + 2 * (y & 1) + 4 * (z & 1)]++;
+        }
+    int off[8], tot = 0;
+    for (int c = 0; c < 8; c++) {
+        gs_num[c] = (cnt[c] + 31) / 32 * 32;
+        off[c] = tot;
+        tot += gs_num[c];
+    }
+    map.assign(nv, -1);
+    int acc[8] = {0};
+    for (long v = 0; v < nv; v++)
+        if (act[v]) {
+            int x = v % vx, y = (v / vx) % vy, z = v / ((long)vx * vy);
+            int c = (x & 1) + 2 * (y & 1) + 4 * (z & 1);
+            map[v] = off[c] + acc[c]++;
+        }
+    ngs = tot;
+}
+
+extern "C" int rt_ref_gs_map(rt_hier* h, int lvl, int* vidmap, int* n_gs, int* gs_num) {
+    if (!h || lvl < 0 || lvl >= (int)h->L.size()) return RT_EINVAL;
+    rt_level& L = h->L[lvl];
+    std::vector<uint8_t> act(L.nv);
+    RT_CUDA(h->ctx, cudaMemcpyAsync(act.data(), L.vact, L.nv, cudaMemcpyDeviceToHost, h->ctx->stream));
+    RT_CUDA(h->ctx, cudaStreamSynchronize(h->ctx->stream));
+    std::vector<int> map;
+    int ngs, gn[8];
+    ref_gs_order(L.vx, L.vy, L.vz, act, map, ngs, gn);
+    if (vidmap) memcpy(vidmap, map.data(), sizeof(int) * L.nv);
+    if (n_gs) *n_gs = ngs;
+    if (gs_num) memcpy(gs_num, gn, sizeof(gn));
+    return RT_OK;
+}
+
+// element GS order (colour of the element position, grid/Grid.cu:583-600)
+static void ref_gs_order_elems(int nx, int ny, int nz, const std::vector<uint8_t>& act, std::vector<int>& map, int& ngs) {
+    int gn[8];
+    // element colour uses the same parity rule as vertices
+    long ne = (long)nx * ny * nz;
+    int cnt[8] = {0};
+    for (long e = 0; e < ne; e++)
+        if (act[e]) cnt[(e % nx & 1) + 2 * ((e / nx) % ny & 1) + 4 * ((e / ((long)nx * ny)) & 1)]++;
+    int off[8], tot = 0;
+    for (int c = 0; c < 8; c++) { gn[c] = (cnt[c] + 31) / 32 * 32; off[c] = tot; tot += gn[c]; }
+    map.assign(ne, -1);
+    int acc[8] = {0};
+    for (long e = 0; e < ne; e++)
+        if (act[e]) {
+            int c = (e % nx & 1) + 2 * ((e / nx) % ny & 1) + 4 * ((e / ((long)nx * ny)) & 1);
+            map[e] = off[c] + acc[c]++;
+        }
+    ngs = tot;
+}
+
+static int convert_layout(rt_hier* h, int field, int lvl, bool to_ref, const void* src, void* dst, size_t bytes) {
+    rt_level& L = h->L[lvl];
+    const bool elem = field == RT_FIELD_RHO || field == RT_FIELD_SENS;
+    std::vector<uint8_t> act(elem ? L.ne : L.nv);
+    RT_CUDA(h->ctx, cudaMemcpyAsync(act.data(), elem ? L.eact : L.vact, act.size(), cudaMemcpyDeviceToHost, h->ctx->stream));
+    RT_CUDA(h->ctx, cudaStreamSynchronize(h->ctx->stream));
+    std::vector<int> map;
+    int ngs, gn[8];
+    if (elem) ref_gs_order_elems(L.nx, L.ny, L.nz, act, map, ngs);
+    else ref_gs_order(L.vx, L.vy, L.vz, act, map, ngs, gn);
+    if (field == RT_FIELD_U || field == RT_FIELD_F || field == RT_FIELD_R) {
+        const double* s = (const double*)src;
+        double* d = (double*)dst;
+        if (to_ref) {
+            std::fill(d, d + 3 * (size_t)ngs, 0.0);
+            for (long v = 0; v < L.nv; v++)
+                if (map[v] >= 0)
+                    for (int c = 0; c < 3; c++) d[(size_t)c * ngs + map[v]] = s[c * L.nv + v];
+        } else {
+            std::fill(d, d + 3 * L.nv, 0.0);
+            for (long v = 0; v < L.nv; v++)
+                if (map[v] >= 0)
+                    for (int c = 0; c < 3; c++) d[c * L.nv + v] = s[(size_t)c * ngs + map[v]];
+        }
+        return RT_OK;
+    }
+    if (elem) {
+        const float* s = (const float*)src;
+        float* d = (float*)dst;
+        if (to_ref) {
+            std::fill(d, d + ngs, 0.f);
+            for (long e = 0; e < L.ne; e++) if (map[e] >= 0) d[map[e]] = s[e];
+        } else {
+            std::fill(d, d + L.ne, 0.f);
+            for (long e = 0; e < L.ne; e++) if (map[e] >= 0) d[e] = s[map[e]];
+        }
+        return RT_OK;
+    }
+    (void)bytes;
+    return rt_fail(h->ctx, RT_EINVAL, "field has no reference-order layout");
+}
+
+extern "C" int rt_put(rt_hier* h, int field, int lvl, int layout, const void* src) {
+    if (!h || !src) return RT_EINVAL;
+    void* d;
+    size_t bytes;
+    RT_CHECK(field_ptr(h, field, lvl, &d, &bytes));
+    if (layout == RT_LAYOUT_REF_GS) {
+        std::vector<char> tmp(bytes);
+        RT_CHECK(convert_layout(h, field, lvl, false, src, tmp.data(), bytes));
+        RT_CUDA(h->ctx, cudaMemcpyAsync(d, tmp.data(), bytes, cudaMemcpyHostToDevice, h->ctx->stream));
+        RT_CUDA(h->ctx, cudaStreamSynchronize(h->ctx->stream));
+    } else {
+        RT_CUDA(h->ctx, cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, h->ctx->stream));
+        RT_CUDA(h->ctx, cudaStreamSynchronize(h->ctx->stream));
+    }
+    if (field == RT_FIELD_RHO || field == RT_FIELD_VFIX || field == RT_FIELD_STENCIL) h->stencil_ready = false;
+    return RT_OK;
+}
+
+extern "C" int rt_get(rt_hier* h, int field, int lvl, int layout, void* dst) {
+    if (!h || !dst) return RT_EINVAL;
+    void* d;
+    size_t bytes;
+    RT_CHECK(field_ptr(h, field, lvl, &d, &bytes));
+    if (layout == RT_LAYOUT_REF_GS) {
+        std::vector<char> tmp(bytes);
+        RT_CUDA(h->ctx, cudaMemcpyAsync(tmp.data(), d, bytes, cudaMemcpyDeviceToHost, h->ctx->stream));
+        RT_CUDA(h->ctx, cudaStreamSynchronize(h->ctx->stream));
+        return convert_layout(h, field, lvl, true, tmp.data(), dst, bytes);
+    }
+    RT_CUDA(h->ctx, cudaMemcpyAsync(dst, d, bytes, cudaMemcpyDeviceToHost, h->ctx->stream));
+    RT_CUDA(h->ctx, cudaStreamSynchronize(h->ctx->stream));
+    return RT_OK;
+}
+
+extern "C" int rt_put_dev(rt_hier* h, int field, int lvl, const void* src) {
+    if (!h || !src) return RT_EINVAL;
+    void* d;
+    size_t bytes;
+    RT_CHECK(field_ptr(h, field, lvl, &d, &bytes));
+    RT_CUDA(h->ctx, cudaMemcpyAsync(d, src, bytes, cudaMemcpyDeviceToDevice, h->ctx->stream));
+    if (field == RT_FIELD_RHO || field == RT_FIELD_VFIX) h->stencil_ready = false;
+    return RT_OK;
+}
+
+extern "C" int rt_get_dev(rt_hier* h, int field, int lvl, void* dst) {
+    if (!h || !dst) return RT_EINVAL;
+    void* d;
+    size_t bytes;
+    RT_CHECK(field_ptr(h, field, lvl, &d, &bytes));
+    RT_CUDA(h->ctx, cudaMemcpyAsync(dst, d, bytes, cudaMemcpyDeviceToDevice, h->ctx->stream));
+    return RT_OK;
+}
+
+__global__ void k_fill_rho(long ne, const uint8_t* __restrict__ eact, float v, float* __restrict__ rho) {
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < ne; e += (long)gridDim.x * blockDim.x)
+        rho[e] = eact[e] ? v : 0.f;
+}
+
+extern "C" int rt_init_density(rt_hier* h, float rho) {
+    if (!h) return RT_EINVAL;
+    rt_level& L = h->L[0];
+    h->stencil_ready = false;
+    return rt_launch(h->ctx, "init_density", [&] {
+        k_fill_rho<<<(unsigned)std::min<long>((L.ne + 255) / 256, 148 * 16), 256, 0, h->ctx->stream>>>(L.ne, L.eact,
+                                                                                                       rho, h->rho);
+    });
+}
+
+// ---------------------------------------------------------------------------
+// multigrid
+// ---------------------------------------------------------------------------
+extern "C" int rt_update_stencil(rt_hier* h) {
+    if (!h) return RT_EINVAL;
+    RT_CUDA(h->ctx, cudaSetDevice(h->ctx->device));
+    RT_CHECK(rtk::penalty_weights(h));
+    const int nl = (int)h->L.size();
+    for (int i = 1; i < nl; i++) {
+        if (i == 1) RT_CHECK(rtk::galerkin_from_elements(h));
+        else RT_CHECK(rtk::galerkin_from_stencil(h, i));
+        RT_CHECK(rtk::d2f(h, 243 * h->L[i].nv, h->L[i].st, h->L[i].st32));
+    }
+    RT_CHECK(rtk::coarsest_setup(h));
+    h->stencil_ready = true;
+    return RT_OK;
+}
+
+template <typename T>
+struct LvlVec;
+template <>
+struct LvlVec<double> {
+    static double* u(rt_level& L) { return L.u; }
+    static double* f(rt_level& L) { return L.f; }
+    static double* r(rt_level& L) { return L.r; }
+};
+template <>
+struct LvlVec<float> {
+    static float* u(rt_level& L) { return L.u32; }
+    static float* f(rt_level& L) { return L.f32; }
+    static float* r(rt_level& L) { return L.r32; }
+};
+
+template <typename T>
+static int level_residual(rt_hier* h, int lvl) {
+    rt_level& L = h->L[lvl];
+    if (lvl == 0) return rtk::fine_residual<T>(h, LvlVec<T>::u(L), LvlVec<T>::f(L), LvlVec<T>::r(L));
+    return rtk::st_residual<T>(h, lvl, LvlVec<T>::u(L), LvlVec<T>::f(L), LvlVec<T>::r(L));
+}
+
+template <typename T>
+static int level_smooth(rt_hier* h, int lvl, int smoother, int sweeps, double omega, bool backward) {
+    rt_level& L = h->L[lvl];
+    T* u = LvlVec<T>::u(L);
+    T* f = LvlVec<T>::f(L);
+    T* tmp = LvlVec<T>::r(L);
+    for (int s = 0; s < sweeps; s++) {
+        if (smoother == RT_SMOOTH_JACOBI) {
+            // ping-pong u -> tmp -> u
+            const T* src = (s % 2 == 0) ? u : tmp;
+            T* dst = (s % 2 == 0) ? tmp : u;
+            if (lvl == 0) RT_CHECK(rtk::fine_jacobi<T>(h, src, f, dst, omega));
+            else RT_CHECK(rtk::st_jacobi<T>(h, lvl, src, f, dst, omega));
+        } else {
+            if (lvl == 0) RT_CHECK(rtk::fine_gs<T>(h, u, f, backward));
+            else RT_CHECK(rtk::st_gs<T>(h, lvl, u, f, backward));
+        }
+    }
+    if (smoother == RT_SMOOTH_JACOBI && (sweeps % 2) == 1)
+        RT_CUDA(h->ctx, cudaMemcpyAsync(u, tmp, sizeof(T) * 3 * L.nv, cudaMemcpyDeviceToDevice, h->ctx->stream));
+    return RT_OK;
+}
+
+// HierarchyGrid::v_cycle (grid/Grid.cpp:1068-1113) over the real levels
+template <typename T>
+static int vcycle_T(rt_hier* h, int smoother, int pre, int post, double omega) {
+    const int nl = (int)h->L.size();
+    for (int i = 0; i < nl; i++) {
+        if (i > 0) {
+            RT_CHECK(level_residual<T>(h, i - 1));
+            RT_CHECK(rtk::restrict_<T>(h, i, LvlVec<T>::r(h->L[i - 1]), LvlVec<T>::f(h->L[i])));
+        }
+        if (i < nl - 1) {
+            if (i > 0)
+                RT_CUDA(h->ctx, cudaMemsetAsync(LvlVec<T>::u(h->L[i]), 0, sizeof(T) * 3 * h->L[i].nv, h->ctx->stream));
+            RT_CHECK(level_smooth<T>(h, i, smoother, pre, omega, false));
+        } else {
+            RT_CHECK(rtk::coarsest_solve<T>(h, LvlVec<T>::f(h->L[i]), LvlVec<T>::u(h->L[i])));
+        }
+    }
+    for (int i = nl - 2; i >= 0; i--) {
+        RT_CHECK(rtk::prolong_add<T>(h, i, LvlVec<T>::u(h->L[i + 1]), LvlVec<T>::u(h->L[i])));
+        RT_CHECK(level_smooth<T>(h, i, smoother, post, omega, smoother == RT_SMOOTH_SGS));
+    }
+    return RT_OK;
+}
+
+static int read_scalars(rt_hier* h, int first, int count, double* out) {
+    rt_ctx* c = h->ctx;
+    RT_CUDA(c, cudaMemcpyAsync(c->hscal, h->scal + first, sizeof(double) * count, cudaMemcpyDeviceToHost, c->stream));
+    RT_CUDA(c, cudaStreamSynchronize(c->stream));
+    memcpy(out, c->hscal, sizeof(double) * count);
+    return RT_OK;
+}
+
+static int need_stencil(rt_hier* h) {
+    if (!h->stencil_ready) return rt_fail(h->ctx, RT_ESTATE, "rt_update_stencil must run after the density or supports change");
+    return RT_OK;
+}
+
+extern "C" int rt_vcycle(rt_hier* h, int pre, int post, double* rel_res) {
+    if (!h || pre < 0 || post < 0) return RT_EINVAL;
+    RT_CHECK(need_stencil(h));
+    RT_CHECK(vcycle_T<double>(h, RT_SMOOTH_GS, pre, post, h->P.jacobi_omega));
+    rt_level& L = h->L[0];
+    RT_CHECK(rtk::fine_residual<double>(h, L.u, L.f, L.r));
+    if (rel_res) {
+        RT_CHECK(rtk::dot(h, 3 * L.nv, L.r, L.r, h->scal + 0));
+        RT_CHECK(rtk::dot(h, 3 * L.nv, L.f, L.f, h->scal + 1));
+        double s[2];
+        RT_CHECK(read_scalars(h, 0, 2, s));
+        *rel_res = std::sqrt(s[0]) / std::sqrt(s[1]);
+    }
+    return RT_OK;
+}
+
+extern "C" int rt_update_residual(rt_hier* h, int lvl) {
+    if (!h || lvl < 0 || lvl >= (int)h->L.size()) return RT_EINVAL;
+    if (lvl > 0) RT_CHECK(need_stencil(h));
+    else RT_CHECK(rtk::penalty_weights(h));
+    return level_residual<double>(h, lvl);
+}
+
+extern "C" int rt_smooth(rt_hier* h, int lvl, int smoother, int sweeps, double omega) {
+    if (!h || lvl < 0 || lvl >= (int)h->L.size() || sweeps < 0) return RT_EINVAL;
+    if (lvl > 0) RT_CHECK(need_stencil(h));
+    else RT_CHECK(rtk::penalty_weights(h));
+    return level_smooth<double>(h, lvl, smoother, sweeps, omega, smoother == RT_SMOOTH_SGS);
+}
+
+extern "C" int rt_restrict_residual(rt_hier* h, int lvl) {
+    if (!h || lvl < 1 || lvl >= (int)h->L.size()) return RT_EINVAL;
+    return rtk::restrict_<double>(h, lvl, h->L[lvl - 1].r, h->L[lvl].f);
+}
+
+extern "C" int rt_prolongate_correction(rt_hier* h, int lvl) {
+    if (!h || lvl < 0 || lvl + 1 >= (int)h->L.size()) return RT_EINVAL;
+    return rtk::prolong_add<double>(h, lvl, h->L[lvl + 1].u, h->L[lvl].u);
+}
+
+extern "C" int rt_coarsest_solve(rt_hier* h) {
+    if (!h) return RT_EINVAL;
+    RT_CHECK(need_stencil(h));
+    rt_level& L = h->L.back();
+    return rtk::coarsest_solve<double>(h, L.f, L.u);
+}
+
+extern "C" int rt_apply_K_dev(rt_hier* h, const double* u, double* out) {
+    if (!h || !u || !out) return RT_EINVAL;
+    RT_CHECK(rtk::penalty_weights(h));
+    return rtk::fine_applyK<double>(h, u, out);
+}
+
+extern "C" int rt_apply_K(rt_hier* h, const double* u, double* out) {
+    if (!h || !u || !out) return RT_EINVAL;
+    rt_level& L = h->L[0];
+    const size_t b = sizeof(double) * 3 * L.nv;
+    RT_CUDA(h->ctx, cudaMemcpyAsync(h->x, u, b, cudaMemcpyHostToDevice, h->ctx->stream));
+    RT_CHECK(rt_apply_K_dev(h, h->x, h->q));
+    RT_CUDA(h->ctx, cudaMemcpyAsync(out, h->q, b, cudaMemcpyDeviceToHost, h->ctx->stream));
+    RT_CUDA(h->ctx, cudaStreamSynchronize(h->ctx->stream));
+    return RT_OK;
+}
+
+extern "C" int rt_compliance(rt_hier* h, double* cpl) {
+    if (!h || !cpl) return RT_EINVAL;
+    rt_level& L = h->L[0];
+    RT_CHECK(rtk::dot(h, 3 * L.nv, L.f, L.u, h->scal + 2));
+    return read_scalars(h, 2, 1, cpl);
+}
+
+extern "C" int rt_relative_residual(rt_hier* h, double* rel) {
+    if (!h || !rel) return RT_EINVAL;
+    rt_level& L = h->L[0];
+    RT_CHECK(rtk::dot(h, 3 * L.nv, L.r, L.r, h->scal + 0));
+    RT_CHECK(rtk::dot(h, 3 * L.nv, L.f, L.f, h->scal + 1));
+    double s[2];
+    RT_CHECK(read_scalars(h, 0, 2, s));
+    *rel = std::sqrt(s[0]) / std::sqrt(s[1]);
+    return RT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// MG-preconditioned flexible CG on level 0: x = L0.u (initial guess), b = L0.f
+// scal slots: 10..13 r.z / rold.z (two parities), 20 p.q, 21 r.r, 22 b.b
+// ---------------------------------------------------------------------------
+static int precondition(rt_hier* h, const double* r, double* z, const double* rr_dev) {
+    rt_level& L = h->L[0];
+    const long n = 3 * L.nv;
+    if (h->P.precision == RT_FP32) {
+        RT_CHECK(rtk::d2f_scaled(h, n, r, L.f32, rr_dev));
+        RT_CUDA(h->ctx, cudaMemsetAsync(L.u32, 0, sizeof(float) * n, h->ctx->stream));
+        RT_CHECK(vcycle_T<float>(h, h->P.smoother, h->P.pre_sweeps, h->P.post_sweeps, h->P.jacobi_omega));
+        RT_CHECK(rtk::f2d_scaled(h, n, L.u32, z, rr_dev));
+    } else {
+        // run the FP64 V-cycle on level-0 f/u, using r/z as the level-0 vectors
+        double* saved_f = L.f;
+        double* saved_u = L.u;
+        L.f = const_cast<double*>(r);
+        L.u = z;
+        RT_CUDA(h->ctx, cudaMemsetAsync(z, 0, sizeof(double) * n, h->ctx->stream));
+        int s = vcycle_T<double>(h, h->P.smoother, h->P.pre_sweeps, h->P.post_sweeps, h->P.jacobi_omega);
+        L.f = saved_f;
+        L.u = saved_u;
+        RT_CHECK(s);
+    }
+    return RT_OK;
+}
+
+static int pcg_core(rt_hier* h, double* x, const double* b, double tol, int maxit, rt_solve_info* info, int* vcycles) {
+    rt_level& L = h->L[0];
+    const long n = 3 * L.nv;
+    double* r = h->rr;
+    // r = b - K x (identity rows on supports), rold = 0
+    RT_CHECK(rtk::fine_applyK<double>(h, x, h->q));
+    RT_CUDA(h->ctx, cudaMemcpyAsync(r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->ctx->stream));
+    RT_CHECK(rtk::axpy(h, n, -1.0, h->q, r));
+    RT_CHECK(rtk::mask_copy(h, n, r, r));
+    RT_CUDA(h->ctx, cudaMemsetAsync(h->rold, 0, sizeof(double) * n, h->ctx->stream));
+    RT_CHECK(rtk::dot(h, n, b, b, h->scal + 22));
+    RT_CHECK(rtk::dot(h, n, r, r, h->scal + 21));
+    double s[2];
+    RT_CHECK(read_scalars(h, 21, 2, s));
+    const double bn = std::sqrt(s[1]) > 0 ? std::sqrt(s[1]) : 1.0;
+    double rel = std::sqrt(s[0]) / bn;
+    int it = 0;
+    while (rel > tol && it < maxit) {
+        RT_CHECK(precondition(h, r, h->z, h->scal + 21));
+        (*vcycles)++;
+        double* rz = h->scal + 10 + 2 * (it & 1);
+        double* rz_prev = h->scal + 10 + 2 * ((it + 1) & 1);
+        RT_CHECK(rtk::dot2(h, n, h->z, r, h->rold, rz));  // rz[0] = z.r, rz[1] = z.rold
+        RT_CHECK(rtk::pcg_update_p(h, n, rz, rz_prev, h->p, h->z, it == 0));
+        RT_CHECK(rtk::fine_applyK<double>(h, h->p, h->q));
+        RT_CHECK(rtk::dot(h, n, h->p, h->q, h->scal + 20));
+        RT_CHECK(rtk::pcg_update_xr(h, n, rz, h->scal + 20, x, r, h->p, h->q, h->rold));
+        RT_CHECK(rtk::dot(h, n, r, r, h->scal + 21));
+        double rr2;
+        RT_CHECK(read_scalars(h, 21, 1, &rr2));
+        if (!std::isfinite(rr2)) {
+            if (info) { info->status = RT_ENAN; info->iterations = it + 1; }
+            return rt_fail(h->ctx, RT_ENAN, "NaN in PCG at iteration %d", it + 1);
+        }
+        rel = std::sqrt(rr2) / bn;
+        it++;
+    }
+    if (info) {
+        info->iterations = it;
+        info->rel_residual = rel;
+        info->status = rel <= tol ? RT_OK : RT_ENOCONV;
+    }
+    return RT_OK;
+}
+
+extern "C" int rt_pcg(rt_hier* h, double tol, int maxit, rt_solve_info* info) {
+    if (!h || tol <= 0 || maxit < 0) return RT_EINVAL;
+    RT_CHECK(need_stencil(h));
+    rt_solve_info loc;
+    memset(&loc, 0, sizeof(loc));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, h->ctx->stream);
+    rt_level& L = h->L[0];
+    int vc = 0;
+    int s = pcg_core(h, L.u, L.f, tol, maxit, &loc, &vc);
+    cudaEventRecord(b, h->ctx->stream);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    loc.vcycles = vc;
+    loc.seconds = ms * 1e-3;
+    if (s == RT_OK) {
+        RT_CHECK(rtk::dot(h, 3 * L.nv, L.f, L.u, h->scal + 2));
+        RT_CHECK(read_scalars(h, 2, 1, &loc.value));
+    }
+    if (info) *info = loc;
+    if (s != RT_OK) return s;
+    return loc.status == RT_OK ? RT_OK : RT_ENOCONV;
+}
+
+// ---------------------------------------------------------------------------
+// worst-case load
+// ---------------------------------------------------------------------------
+__global__ void k_multidot(long n, int m, const double* __restrict__ Q, const double* __restrict__ w,
+                           double* __restrict__ partials) {
+    // m <= 64 dots of w against the rows of Q; block partials [block][64]
+    __shared__ double sh[64][8];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int k = 0; k < m; k++) {
+        double s = 0;
+        for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+            s += Q[(long)k * n + i] * w[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) sh[k][warp] = s;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < m; k += blockDim.x) {
+        double s = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) s += sh[k][q];
+        partials[blockIdx.x * 64 + k] = s;
+    }
+}
+__global__ void k_multidot_final(int nblocks, int m, const double* __restrict__ partials, double* __restrict__ out) {
+    for (int k = threadIdx.x; k < m; k += blockDim.x) {
+        double s = 0;
+        for (int b = 0; b < nblocks; b++) s += partials[b * 64 + k];
+        out[k] = s;
+    }
+}
+__global__ void k_sub_multi(long n, int m, const double* __restrict__ Q, const double* __restrict__ hcoef,
+                            double* __restrict__ w) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        double s = w[i];
+        for (int k = 0; k < m; k++) s -= hcoef[k] * Q[(long)k * n + i];
+        w[i] = s;
+    }
+}
+__global__ void k_combine(long n, int m, const double* __restrict__ Q, const double* __restrict__ y,
+                          double* __restrict__ out) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        double s = 0;
+        for (int k = 0; k < m; k++) s += y[k] * Q[(long)k * n + i];
+        out[i] = s;
+    }
+}
+// store alpha_j = a and beta_j = sqrt(bb); w /= beta_j done by k_scale with the same slot
+__global__ void k_store_ab(const double* __restrict__ adot, const double* __restrict__ bb, double* __restrict__ alpha,
+                           double* __restrict__ beta, int j) {
+    if (threadIdx.x == 0) {
+        alpha[j] = adot[0];
+        beta[j] = sqrt(bb[0]);
+    }
+}
+// Ritz vector of the largest eigenvalue of T_k by three steps of inverse iteration
+__global__ void k_tridiag_ritz(int k, const double* __restrict__ alpha, const double* __restrict__ beta,
+                               const double* __restrict__ lam, double* __restrict__ y) {
+    if (threadIdx.x != 0) return;
+    double yy[64], cp[64], dp[64];
+    for (int i = 0; i < k; i++) yy[i] = 1.0;
+    const double shift = lam[0] * (1 + 1e-12) + 1e-300;
+    for (int it = 0; it < 3; it++) {
+        for (int i = 0; i < k; i++) {
+            const double a = i > 0 ? beta[i - 1] : 0, b = alpha[i] - shift, c = i < k - 1 ? beta[i] : 0;
+            const double den = b - (i > 0 ? a * cp[i - 1] : 0);
+            cp[i] = c / den;
+            dp[i] = (yy[i] - (i > 0 ? a * dp[i - 1] : 0)) / den;
+        }
+        double nrm = 0;
+        for (int i = k - 1; i >= 0; i--) {
+            yy[i] = dp[i] - (i < k - 1 ? cp[i] * yy[i + 1] : 0);
+        }
+        for (int i = 0; i < k; i++) nrm += yy[i] * yy[i];
+        nrm = sqrt(nrm);
+        for (int i = 0; i < k; i++) yy[i] /= nrm;
+    }
+    for (int i = 0; i < k; i++) y[i] = yy[i];
+}
+__global__ void k_diffnorm(long n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ partials) {
+    __shared__ double sh[2][8];
+    double s0 = 0, s1 = 0;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const double d = a[i] - b[i];
+        s0 += d * d;
+        s1 += b[i] * b[i];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_down_sync(0xffffffffu, s0, o);
+        s1 += __shfl_down_sync(0xffffffffu, s1, o);
+    }
+    if ((threadIdx.x & 31) == 0) { sh[0][threadIdx.x >> 5] = s0; sh[1][threadIdx.x >> 5] = s1; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a0 = 0, a1 = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) { a0 += sh[0][q]; a1 += sh[1][q]; }
+        partials[blockIdx.x * 2] = a0;
+        partials[blockIdx.x * 2 + 1] = a1;
+    }
+}
+__global__ void k_final2(int nb, const double* __restrict__ partials, double* __restrict__ out) {
+    if (threadIdx.x == 0) {
+        double a0 = 0, a1 = 0;
+        for (int b = 0; b < nb; b++) { a0 += partials[2 * b]; a1 += partials[2 * b + 1]; }
+        out[0] = a0;
+        out[1] = a1;
+    }
+}
+
+static int multidot(rt_hier* h, long n, int m, const double* Q, const double* w, double* out) {
+    RT_CHECK(rt_launch(h->ctx, "lanczos_multidot", [&] {
+        k_multidot<<<RT_RED_BLOCKS / 2, 256, 0, h->ctx->stream>>>(n, m, Q, w, h->partials);
+    }));
+    return rt_launch(h->ctx, "lanczos_multidot_final", [&] {
+        k_multidot_final<<<1, 64, 0, h->ctx->stream>>>(RT_RED_BLOCKS / 2, m, h->partials, out);
+    });
+}
+
+static int lanczos(rt_hier* h, int k, double inner_tol, uint64_t seed, double* lambda, rt_solve_info* info) {
+    rt_ctx* c = h->ctx;
+    rt_level& L = h->L[0];
+    const long n = 3 * L.nv, nl = 3L * h->nload;
+    if (h->nload == 0) return rt_fail(c, RT_ESTATE, "no load nodes");
+    if (k < 1 || k > 60) return rt_fail(c, RT_EINVAL, "Lanczos k must be in [1, 60]");
+    if (h->Qcap < k + 1) {
+        cudaFree(h->Q);
+        h->Q = nullptr;
+        RT_CHECK(dalloc(c, &h->Q, (size_t)(k + 1) * nl));
+        h->Qcap = k + 1;
+    }
+    double* alpha = h->scal + 100;  // [64]
+    double* beta = h->scal + 164;   // [64]
+    double* hc = h->scal + 240;     // [64] re-orthogonalisation coefficients, then the Ritz vector
+    double* Q = h->Q;
+    RT_CHECK(rtk::rng_uniform(h, seed, n, L.f));
+    RT_CHECK(rtk::project_load(h, L.f));
+    RT_CHECK(rtk::gather_load(h, L.f, Q));
+    RT_CHECK(rtk::dot(h, nl, Q, Q, h->scal + 30));
+    RT_CHECK(rtk::scale(h, nl, Q, h->scal + 30, true));
+    int inner = 0, vcycles = 0, steps = 0;
+    for (int j = 0; j < k; j++) {
+        double* qj = Q + (long)j * nl;
+        double* w = Q + (long)(j + 1) * nl;
+        RT_CUDA(c, cudaMemsetAsync(L.f, 0, sizeof(double) * n, c->stream));
+        RT_CHECK(rtk::scatter_load(h, qj, L.f));
+        RT_CUDA(c, cudaMemsetAsync(L.u, 0, sizeof(double) * n, c->stream));
+        rt_solve_info si;
+        memset(&si, 0, sizeof(si));
+        RT_CHECK(pcg_core(h, L.u, L.f, inner_tol, 500, &si, &vcycles));
+        inner += si.iterations;
+        // w = P S u
+        RT_CUDA(c, cudaMemcpyAsync(h->z, L.u, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+        RT_CHECK(rtk::project_load(h, h->z));
+        RT_CHECK(rtk::gather_load(h, h->z, w));
+        RT_CHECK(rtk::dot(h, nl, w, qj, h->scal + 31));
+        // CGS2 full re-orthogonalisation against q_0..q_j
+        for (int pass = 0; pass < 2; pass++) {
+            RT_CHECK(multidot(h, nl, j + 1, Q, w, hc));
+            RT_CHECK(rt_launch(c, "lanczos_sub", [&] {
+                k_sub_multi<<<(unsigned)std::min<long>((nl + 255) / 256, c->sm_count * 8), 256, 0, c->stream>>>(
+                    nl, j + 1, Q, hc, w);
+            }));
+        }
+        RT_CHECK(rtk::dot(h, nl, w, w, h->scal + 32));
+        RT_CHECK(rt_launch(c, "lanczos_store_ab",
+                           [&] { k_store_ab<<<1, 32, 0, c->stream>>>(h->scal + 31, h->scal + 32, alpha, beta, j); }));
+        RT_CHECK(rtk::scale(h, nl, w, h->scal + 32, true));
+        steps = j + 1;
+        double ab[2];
+        RT_CUDA(c, cudaMemcpyAsync(c->hscal, alpha + j, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        RT_CUDA(c, cudaMemcpyAsync(c->hscal + 1, beta + j, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        RT_CUDA(c, cudaStreamSynchronize(c->stream));
+        ab[0] = c->hscal[0];
+        ab[1] = c->hscal[1];
+        if (!std::isfinite(ab[0]) || !std::isfinite(ab[1])) return rt_fail(c, RT_ENAN, "NaN in Lanczos");
+        if (ab[1] < 1e-13 * std::fabs(ab[0])) break;
+    }
+    RT_CHECK(rtk::tridiag_max_eig(h, steps, alpha, beta, h->scal + 33));
+    RT_CHECK(rt_launch(c, "lanczos_ritz", [&] { k_tridiag_ritz<<<1, 32, 0, c->stream>>>(steps, alpha, beta, h->scal + 33, hc); }));
+    // worst-case load f = Q y on the load set, u = K^-1 f
+    RT_CHECK(rt_launch(c, "lanczos_combine", [&] {
+        k_combine<<<(unsigned)std::min<long>((nl + 255) / 256, c->sm_count * 8), 256, 0, c->stream>>>(nl, steps, Q, hc, h->fs_old);
+    }));
+    RT_CUDA(c, cudaMemsetAsync(L.f, 0, sizeof(double) * n, c->stream));
+    RT_CHECK(rtk::scatter_load(h, h->fs_old, L.f));
+    RT_CUDA(c, cudaMemsetAsync(L.u, 0, sizeof(double) * n, c->stream));
+    rt_solve_info si;
+    memset(&si, 0, sizeof(si));
+    RT_CHECK(pcg_core(h, L.u, L.f, inner_tol, 500, &si, &vcycles));
+    inner += si.iterations;
+    RT_CHECK(read_scalars(h, 33, 1, lambda));
+    if (info) {
+        info->iterations = steps;
+        info->inner_iterations = inner;
+        info->vcycles = vcycles;
+        info->rel_residual = si.rel_residual;
+        info->value = *lambda;
+        info->status = RT_OK;
+    }
+    return RT_OK;
+}
+
+// modifiedPM (optimization/optimization.cpp:123-261)
+static int modified_pm(rt_hier* h, int maxit, uint64_t seed, double* lambda, rt_solve_info* info) {
+    rt_ctx* c = h->ctx;
+    rt_level& L = h->L[0];
+    const long n = 3 * L.nv, nl = 3L * h->nload;
+    if (h->nload == 0) return rt_fail(c, RT_ESTATE, "no load nodes");
+    const bool no_support = (h->P.mode == RT_MODE_NSCF || h->P.mode == RT_MODE_NSFF);
+    if (no_support && h->Ru == nullptr) RT_CHECK(rtk::rigid_nodes(h));
+    RT_CHECK(rtk::rng_uniform(h, seed, n, L.f));
+    RT_CHECK(rtk::project_load(h, L.f));
+    RT_CHECK(rtk::dot(h, n, L.f, L.f, h->scal + 30));
+    RT_CHECK(rtk::scale(h, n, L.f, h->scal + 30, true));
+    RT_CUDA(c, cudaMemsetAsync(L.u, 0, sizeof(double) * n, c->stream));
+    RT_CHECK(rtk::gather_load(h, L.f, h->fs_old));
+    double fch = 1, rel = 1;
+    int itn = 0;
+    while (itn++ < maxit && (fch > 1e-4 || rel > 1e-2)) {
+        RT_CHECK(vcycle_T<double>(h, RT_SMOOTH_GS, 1, 1, h->P.jacobi_omega));
+        RT_CHECK(rtk::fine_residual<double>(h, L.u, L.f, L.r));
+        RT_CHECK(rtk::dot(h, n, L.r, L.r, h->scal + 0));
+        RT_CHECK(rtk::dot(h, n, L.f, L.f, h->scal + 1));
+        if (no_support) RT_CHECK(rtk::displacement_project(h, L.u));
+        RT_CUDA(c, cudaMemcpyAsync(L.f, L.u, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+        RT_CHECK(rtk::project_load(h, L.f));
+        RT_CHECK(rtk::dot(h, n, L.f, L.f, h->scal + 30));
+        RT_CHECK(rtk::scale(h, n, L.f, h->scal + 30, true));
+        RT_CHECK(rtk::gather_load(h, L.f, h->fs));
+        RT_CHECK(rt_launch(c, "pm_diffnorm", [&] { k_diffnorm<<<64, 256, 0, c->stream>>>(nl, h->fs, h->fs_old, h->partials); }));
+        RT_CHECK(rt_launch(c, "pm_diffnorm_final", [&] { k_final2<<<1, 32, 0, c->stream>>>(64, h->partials, h->scal + 3); }));
+        RT_CUDA(c, cudaMemcpyAsync(h->fs_old, h->fs, sizeof(double) * nl, cudaMemcpyDeviceToDevice, c->stream));
+        double s[5];
+        RT_CHECK(read_scalars(h, 0, 5, s));
+        rel = std::sqrt(s[0]) / std::sqrt(s[1]);
+        fch = std::sqrt(s[3]) / std::sqrt(s[4]);
+        if (!(rel <= 1e4)) return rt_fail(c, RT_ENAN, "modified power method diverged (rel_res %g)", rel);
+    }
+    RT_CHECK(rtk::dot(h, n, L.f, L.u, h->scal + 2));
+    RT_CHECK(read_scalars(h, 2, 1, lambda));
+    if (info) {
+        info->iterations = itn - 1;
+        info->vcycles = itn - 1;
+        info->rel_residual = rel;
+        info->value = *lambda;
+        info->status = (fch <= 1e-4 && rel <= 1e-2) ? RT_OK : RT_ENOCONV;
+    }
+    return RT_OK;
+}
+
+extern "C" int rt_worst_case(rt_hier* h, int method, int k, double inner_tol, uint64_t seed, double* lambda,
+                             rt_solve_info* info) {
+    if (!h || !lambda) return RT_EINVAL;
+    RT_CHECK(need_stencil(h));
+    rt_solve_info loc;
+    memset(&loc, 0, sizeof(loc));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, h->ctx->stream);
+    int s;
+    if (method == RT_WORST_LANCZOS) s = lanczos(h, k, inner_tol, seed, lambda, &loc);
+    else if (method == RT_WORST_MODPM) s = modified_pm(h, k > 0 ? k : 500, seed, lambda, &loc);
+    else s = RT_EINVAL;
+    cudaEventRecord(b, h->ctx->stream);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    loc.seconds = ms * 1e-3;
+    if (info) *info = loc;
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// optimisation step
+// ---------------------------------------------------------------------------
+extern "C" int rt_filter_sensitivity(rt_hier* h, float radius) {
+    if (!h || radius <= 0) return RT_EINVAL;
+    return rtk::filter(h, radius);
+}
+
+extern "C" int rt_sensitivity(rt_hier* h, int filt) {
+    if (!h) return RT_EINVAL;
+    RT_CHECK(rtk::sensitivity(h, h->L[0].u));
+    if (filt) RT_CHECK(rtk::filter(h, h->P.filter_radius));
+    return RT_OK;
+}
+
+extern "C" int rt_oc_update(rt_hier* h, float vgoal, float* lambda_out, int* trials_out) {
+    if (!h) return RT_EINVAL;
+    rt_level& L = h->L[0];
+    RT_CHECK(rtk::oc_maxabs(h, nullptr));
+    double gmax;
+    RT_CHECK(read_scalars(h, 50, 1, &gmax));
+    float lo = 0, hi = (float)gmax, thr = (lo + hi) / 2, V = 2;
+    const double nact = (double)L.n_act_elems;
+    int itn = 0, trials = 0;
+    do {
+        thr = (lo + hi) / 2;
+        RT_CHECK(rtk::oc_try(h, thr, h->ftmp, h->scal + 51));
+        double vs;
+        RT_CHECK(read_scalars(h, 51, 1, &vs));
+        V = (float)(vs / nact);
+        trials++;
+        if (V > vgoal) lo = thr;
+        else if (V < vgoal) hi = thr;
+    } while (std::fabs(V - vgoal) > 1e-4f && itn++ < 30);
+    RT_CHECK(rtk::oc_try(h, thr, h->rho, h->scal + 51));
+    h->stencil_ready = false;
+    if (lambda_out) *lambda_out = thr;
+    if (trials_out) *trials_out = trials;
+    return RT_OK;
+}
+
+extern "C" int rt_oc_iteration(rt_hier* h, int method, int k, double inner_tol, uint64_t seed, float vgoal,
+                               double* compliance_out) {
+    if (!h) return RT_EINVAL;
+    RT_CHECK(rt_update_stencil(h));
+    double lam = 0;
+    rt_solve_info info;
+    RT_CHECK(rt_worst_case(h, method, k, inner_tol, seed, &lam, &info));
+    RT_CHECK(rt_sensitivity(h, 1));
+    RT_CHECK(rt_oc_update(h, vgoal, nullptr, nullptr));
+    if (compliance_out) *compliance_out = lam;
+    return RT_OK;
+}

@@ -1,0 +1,542 @@
+// rt_coarse.cu — assembled-stencil levels, grid transfers and Galerkin assembly.
+//
+// Restates:
+//   update_residual_kernel_1               grid/Grid.cu:1350-1448
+//   gs_relax_kernel                        grid/Grid.cu:678-790
+//   restrict_residual{,_nondyadic}_kernel  grid/Grid.cu:1680-1794
+//   prolongate_correction{,_nondyadic}_kernel grid/Grid.cu:1818-1895
+//   restrict_stencil_nondyadic_OTFA_{NS,WS}_kernel grid/Grid.cu:296-506
+//   restrict_stencil_dyadic_kernel         grid/Grid.cu:120-177
+// Stencils are [27*9][nv]: entry (k*9 + 3*row + col)*nv + v couples node v to
+// neighbour v + d(k), d(k) = (k%3-1, k/3%3-1, k/9-1) — the reference's
+// GraftArray<double,27,9> layout over a dense node box.
+#include <cuda_runtime.h>
+
+#include "rt_internal.h"
+
+namespace {
+
+constexpr int ST_BS = 256;
+
+unsigned grid_for(rt_ctx* c, long n, int bs) {
+    long b = rt_blocks(n, bs);
+    long cap = (long)c->sm_count * 16;
+    return (unsigned)(b < cap ? b : cap);
+}
+
+template <typename T, bool SKIPSELF>
+__device__ __forceinline__ void st_node_sum(int x, int y, int z, int vx, int vy, int vz, long nv,
+                                            const uint8_t* __restrict__ vact, const T* __restrict__ st,
+                                            const T* __restrict__ u, long v, T Au[3]) {
+    Au[0] = Au[1] = Au[2] = T(0);
+#pragma unroll
+    for (int k = 0; k < 27; k++) {
+        if (SKIPSELF && k == 13) continue;
+        const int jx = x + k % 3 - 1, jy = y + (k / 3) % 3 - 1, jz = z + k / 9 - 1;
+        if (jx < 0 || jy < 0 || jz < 0 || jx >= vx || jy >= vy || jz >= vz) continue;
+        const long nj = jx + (long)vx * (jy + (long)vy * jz);
+        const T u0 = u[nj], u1 = u[nv + nj], u2 = u[2 * nv + nj];
+        const T* s = st + (long)(k * 9) * nv + v;
+#pragma unroll
+        for (int r = 0; r < 3; r++) Au[r] += s[(3 * r) * nv] * u0 + s[(3 * r + 1) * nv] * u1 + s[(3 * r + 2) * nv] * u2;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(ST_BS) k_st_residual(int nx, int ny, int nz, const uint8_t* __restrict__ vact,
+                                                        const T* __restrict__ st, const T* __restrict__ u,
+                                                        const T* __restrict__ f, T* __restrict__ r) {
+    const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
+    const long nv = (long)vx * vy * vz;
+    for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < nv; v += (long)gridDim.x * blockDim.x) {
+        const int x = (int)(v % vx), y = (int)((v / vx) % vy), z = (int)(v / ((long)vx * vy));
+        T Au[3] = {T(0), T(0), T(0)};
+        const bool act = vact[v];
+        if (act) st_node_sum<T, false>(x, y, z, vx, vy, vz, nv, vact, st, u, v, Au);
+#pragma unroll
+        for (int c = 0; c < 3; c++) r[c * nv + v] = act ? f[c * nv + v] - Au[c] : T(0);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(ST_BS) k_st_gs(int nx, int ny, int nz, int color, bool backward,
+                                                  const uint8_t* __restrict__ vact, const T* __restrict__ st,
+                                                  T* __restrict__ u, const T* __restrict__ f) {
+    const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
+    const long nv = (long)vx * vy * vz;
+    const int px = color & 1, py = (color >> 1) & 1, pz = (color >> 2) & 1;
+    const int cx = (vx - px + 1) / 2, cy = (vy - py + 1) / 2, cz = (vz - pz + 1) / 2;
+    const long nc = (long)cx * cy * cz;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nc; t += (long)gridDim.x * blockDim.x) {
+        const int x = px + 2 * (int)(t % cx), y = py + 2 * (int)((t / cx) % cy), z = pz + 2 * (int)(t / ((long)cx * cy));
+        const long v = x + (long)vx * (y + (long)vy * z);
+        if (!vact[v]) continue;
+        T Au[3];
+        st_node_sum<T, true>(x, y, z, vx, vy, vz, nv, vact, st, u, v, Au);
+        T S[9];
+#pragma unroll
+        for (int i = 0; i < 9; i++) S[i] = st[(long)(13 * 9 + i) * nv + v];
+        const T F[3] = {f[v], f[nv + v], f[2 * nv + v]};
+        T uu[3] = {u[v], u[nv + v], u[2 * nv + v]};
+        if (!backward) {
+            uu[0] = (F[0] - S[1] * uu[1] - S[2] * uu[2] - Au[0]) / S[0];
+            uu[1] = (F[1] - S[3] * uu[0] - S[5] * uu[2] - Au[1]) / S[4];
+            uu[2] = (F[2] - S[6] * uu[0] - S[7] * uu[1] - Au[2]) / S[8];
+        } else {
+            uu[2] = (F[2] - S[6] * uu[0] - S[7] * uu[1] - Au[2]) / S[8];
+            uu[1] = (F[1] - S[3] * uu[0] - S[5] * uu[2] - Au[1]) / S[4];
+            uu[0] = (F[0] - S[1] * uu[1] - S[2] * uu[2] - Au[0]) / S[0];
+        }
+        u[v] = uu[0]; u[nv + v] = uu[1]; u[2 * nv + v] = uu[2];
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(ST_BS) k_st_jacobi(int nx, int ny, int nz, T omega,
+                                                      const uint8_t* __restrict__ vact, const T* __restrict__ st,
+                                                      const T* __restrict__ u, const T* __restrict__ f,
+                                                      T* __restrict__ unew) {
+    const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
+    const long nv = (long)vx * vy * vz;
+    for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < nv; v += (long)gridDim.x * blockDim.x) {
+        const int x = (int)(v % vx), y = (int)((v / vx) % vy), z = (int)(v / ((long)vx * vy));
+        T nu[3] = {T(0), T(0), T(0)};
+        if (vact[v]) {
+            T Au[3];
+            st_node_sum<T, false>(x, y, z, vx, vy, vz, nv, vact, st, u, v, Au);
+            T S[9], I[9];
+#pragma unroll
+            for (int i = 0; i < 9; i++) S[i] = st[(long)(13 * 9 + i) * nv + v];
+            const T a = S[0], b = S[1], c = S[2], d = S[3], e = S[4], ff = S[5], g = S[6], hh = S[7], k = S[8];
+            const T A = e * k - ff * hh, B = -(d * k - ff * g), Cc = d * hh - e * g;
+            const T id = T(1) / (a * A + b * B + c * Cc);
+            I[0] = A * id; I[1] = -(b * k - c * hh) * id; I[2] = (b * ff - c * e) * id;
+            I[3] = B * id; I[4] = (a * k - c * g) * id; I[5] = -(a * ff - c * d) * id;
+            I[6] = Cc * id; I[7] = -(a * hh - b * g) * id; I[8] = (a * e - b * d) * id;
+            T rr[3];
+#pragma unroll
+            for (int q = 0; q < 3; q++) rr[q] = f[q * nv + v] - Au[q];
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+                nu[q] = u[q * nv + v] + omega * (I[q * 3] * rr[0] + I[q * 3 + 1] * rr[1] + I[q * 3 + 2] * rr[2]);
+        }
+#pragma unroll
+        for (int q = 0; q < 3; q++) unew[q * nv + v] = nu[q];
+    }
+}
+
+// f_c(X) = sum_{|d| < r} prod (r - |d|)/r * r_f(rX + d)
+template <typename T, int R>
+__global__ void __launch_bounds__(ST_BS) k_restrict(int fnx, int fny, int fnz, int cnx, int cny, int cnz,
+                                                     const uint8_t* __restrict__ cvact, const T* __restrict__ rf,
+                                                     T* __restrict__ fc) {
+    const int fvx = fnx + 1, fvy = fny + 1, fvz = fnz + 1;
+    const int cvx = cnx + 1, cvy = cny + 1, cvz = cnz + 1;
+    const long nvf = (long)fvx * fvy * fvz, nvc = (long)cvx * cvy * cvz;
+    for (long vc = blockIdx.x * (long)blockDim.x + threadIdx.x; vc < nvc; vc += (long)gridDim.x * blockDim.x) {
+        const int X = (int)(vc % cvx), Y = (int)((vc / cvx) % cvy), Z = (int)(vc / ((long)cvx * cvy));
+        T s[3] = {T(0), T(0), T(0)};
+        if (cvact[vc]) {
+            for (int dz = -(R - 1); dz <= R - 1; dz++) {
+                const int z = R * Z + dz;
+                if (z < 0 || z >= fvz) continue;
+                const T wz = T(R - abs(dz));
+                for (int dy = -(R - 1); dy <= R - 1; dy++) {
+                    const int y = R * Y + dy;
+                    if (y < 0 || y >= fvy) continue;
+                    const T wyz = wz * T(R - abs(dy));
+#pragma unroll
+                    for (int dx = -(R - 1); dx <= R - 1; dx++) {
+                        const int x = R * X + dx;
+                        if (x < 0 || x >= fvx) continue;
+                        const long vf = x + (long)fvx * (y + (long)fvy * z);
+                        const T wgt = wyz * T(R - abs(dx)) * (T(1) / T(R * R * R));
+                        s[0] += wgt * rf[vf];
+                        s[1] += wgt * rf[nvf + vf];
+                        s[2] += wgt * rf[2 * nvf + vf];
+                    }
+                }
+            }
+        }
+        fc[vc] = s[0]; fc[nvc + vc] = s[1]; fc[2 * nvc + vc] = s[2];
+    }
+}
+
+// u_f(x) += sum over the 8 corners of the coarse cell containing x of trilinear weights * u_c
+template <typename T, int R>
+__global__ void __launch_bounds__(ST_BS) k_prolong(int fnx, int fny, int fnz, int cnx, int cny, int cnz,
+                                                    const uint8_t* __restrict__ fvact, const T* __restrict__ uc,
+                                                    T* __restrict__ uf) {
+    const int fvx = fnx + 1, fvy = fny + 1, fvz = fnz + 1;
+    const int cvx = cnx + 1, cvy = cny + 1, cvz = cnz + 1;
+    const long nvf = (long)fvx * fvy * fvz, nvc = (long)cvx * cvy * cvz;
+    for (long vf = blockIdx.x * (long)blockDim.x + threadIdx.x; vf < nvf; vf += (long)gridDim.x * blockDim.x) {
+        if (!fvact[vf]) continue;
+        const int x = (int)(vf % fvx), y = (int)((vf / fvx) % fvy), z = (int)(vf / ((long)fvx * fvy));
+        const int X0 = x / R, Y0 = y / R, Z0 = z / R;
+        const int ox = x - R * X0, oy = y - R * Y0, oz = z - R * Z0;
+        T s[3] = {T(0), T(0), T(0)};
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int a = i & 1, b = (i >> 1) & 1, c = i >> 2;
+            const int wx = a ? ox : R - ox, wy = b ? oy : R - oy, wz = c ? oz : R - oz;
+            if (wx == 0 || wy == 0 || wz == 0) continue;
+            const long vc = (X0 + a) + (long)cvx * ((Y0 + b) + (long)cvy * (Z0 + c));
+            const T wgt = T(wx * wy * wz) * (T(1) / T(R * R * R));
+            s[0] += wgt * uc[vc];
+            s[1] += wgt * uc[nvc + vc];
+            s[2] += wgt * uc[2 * nvc + vc];
+        }
+        uf[vf] += s[0]; uf[nvf + vf] += s[1]; uf[2 * nvf + vf] += s[2];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Galerkin assembly of the first coarse level directly from the elements:
+// for every coarse cell M = sum_e rho_e^p Q_pos(e), Q_pos = P_pos^T KE P_pos,
+// then M's 3x3 blocks are added into the 8 corner nodes' stencils.  Cells are
+// processed in 8 parity colours so no two cells of one launch share a node
+// (deterministic, no atomics).  Elements touching a fixed node take the
+// Dirichlet form of grid/Grid.cu:465-490 and are computed explicitly.
+// ---------------------------------------------------------------------------
+constexpr int GAL_CELLS = 8;
+constexpr int GAL_BS = 288;  // 2 entries of the 576-entry cell matrix per thread
+
+__device__ __forceinline__ double interp_w(int off, int corner, int R) {
+    return (double)(R - abs(off - R * corner)) / (double)R;
+}
+
+template <int R>
+__global__ void __launch_bounds__(GAL_BS) k_galerkin_cells(int fnx, int fny, int fnz, int cnx, int cny, int cnz,
+                                                           int color, const uint8_t* __restrict__ ceact,
+                                                           const float* __restrict__ w,
+                                                           const uint8_t* __restrict__ vfix,
+                                                           const double* __restrict__ Q, const double* __restrict__ KEg,
+                                                           double* __restrict__ st) {
+    constexpr int NP = R * R * R;
+    __shared__ double sw[GAL_CELLS][NP];
+    __shared__ int scell[GAL_CELLS];
+    __shared__ int sfixed[GAL_CELLS];
+    const int fvx = fnx + 1, fvy = fny + 1;
+    const int cvx = cnx + 1, cvy = cny + 1, cvz = cnz + 1;
+    const long nvc = (long)cvx * cvy * cvz;
+    const int px = color & 1, py = (color >> 1) & 1, pz = (color >> 2) & 1;
+    const int ccx = (cnx - px + 1) / 2, ccy = (cny - py + 1) / 2, ccz = (cnz - pz + 1) / 2;
+    const long ncells = (long)ccx * ccy * ccz;
+    const long ngroups = (ncells + GAL_CELLS - 1) / GAL_CELLS;
+    for (long g = blockIdx.x; g < ngroups; g += gridDim.x) {
+        __syncthreads();
+        if (threadIdx.x < GAL_CELLS) {
+            long t = g * GAL_CELLS + threadIdx.x;
+            int cid = -1;
+            if (t < ncells) {
+                int X = px + 2 * (int)(t % ccx), Y = py + 2 * (int)((t / ccx) % ccy), Z = pz + 2 * (int)(t / ((long)ccx * ccy));
+                if (ceact[X + (long)cnx * (Y + (long)cny * Z)]) cid = X + cnx * (Y + cny * Z);
+            }
+            scell[threadIdx.x] = cid;
+            sfixed[threadIdx.x] = 0;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < GAL_CELLS * NP; i += blockDim.x) {
+            const int c = i / NP, pos = i % NP;
+            double wv = 0;
+            const int cid = scell[c];
+            if (cid >= 0) {
+                const int X = cid % cnx, Y = (cid / cnx) % cny, Z = cid / (cnx * cny);
+                const int a = pos % R, b = (pos / R) % R, cc = pos / (R * R);
+                const int ex = R * X + a, ey = R * Y + b, ez = R * Z + cc;
+                if (ex < fnx && ey < fny && ez < fnz) {
+                    wv = w[ex + (long)fnx * (ey + (long)fny * ez)];
+                    if (vfix != nullptr && wv != 0) {
+                        bool fx = false;
+                        for (int j = 0; j < 8; j++)
+                            fx |= vfix[(ex + (j & 1)) + (long)fvx * ((ey + ((j >> 1) & 1)) + (long)fvy * (ez + (j >> 2)))] != 0;
+                        if (fx) { sfixed[c] = 1; wv = -1.0 - wv; }  // marker: handled explicitly below
+                    }
+                }
+            }
+            sw[c][pos] = wv;
+        }
+        __syncthreads();
+        // dense part: M[c][t] = sum_pos w[c][pos] Q[pos][t] over non-fixed elements
+        double acc[GAL_CELLS][2];
+#pragma unroll
+        for (int c = 0; c < GAL_CELLS; c++) acc[c][0] = acc[c][1] = 0;
+        const int t0 = threadIdx.x, t1 = threadIdx.x + GAL_BS;
+        for (int pos = 0; pos < NP; pos++) {
+            const double q0 = Q[(long)pos * 576 + t0], q1 = Q[(long)pos * 576 + t1];
+#pragma unroll
+            for (int c = 0; c < GAL_CELLS; c++) {
+                const double wv = sw[c][pos] > 0 ? sw[c][pos] : 0.0;
+                acc[c][0] += wv * q0;
+                acc[c][1] += wv * q1;
+            }
+        }
+        // elements with fixed nodes: rows/cols dropped, 1e6 * P^T P diagonal
+        for (int c = 0; c < GAL_CELLS; c++) {
+            if (!sfixed[c]) continue;
+            const int cid = scell[c];
+            const int X = cid % cnx, Y = (cid / cnx) % cny, Z = cid / (cnx * cny);
+            for (int pos = 0; pos < NP; pos++) {
+                const double wm = sw[c][pos];
+                if (wm >= 0) continue;
+                const double pen = -1.0 - wm;
+                const int a = pos % R, b = (pos / R) % R, cc = pos / (R * R);
+                const int ex = R * X + a, ey = R * Y + b, ez = R * Z + cc;
+#pragma unroll
+                for (int half = 0; half < 2; half++) {
+                    const int t = half ? t1 : t0;
+                    const int mrow = t / 24, ncol = t % 24;
+                    const int m = mrow / 3, row = mrow % 3, n = ncol / 3, col = ncol % 3;
+                    double s = 0;
+                    for (int j = 0; j < 8; j++) {
+                        const int oj[3] = {a + (j & 1), b + ((j >> 1) & 1), cc + (j >> 2)};
+                        const double pj = interp_w(oj[0], m & 1, R) * interp_w(oj[1], (m >> 1) & 1, R) *
+                                          interp_w(oj[2], m >> 2, R);
+                        if (pj == 0) continue;
+                        const bool fj = vfix[(ex + (j & 1)) + (long)fvx * ((ey + ((j >> 1) & 1)) + (long)fvy * (ez + (j >> 2)))];
+                        for (int k = 0; k < 8; k++) {
+                            const int ok[3] = {a + (k & 1), b + ((k >> 1) & 1), cc + (k >> 2)};
+                            const double pk = interp_w(ok[0], n & 1, R) * interp_w(ok[1], (n >> 1) & 1, R) *
+                                              interp_w(ok[2], n >> 2, R);
+                            if (pk == 0) continue;
+                            const bool fk = vfix[(ex + (k & 1)) + (long)fvx * ((ey + ((k >> 1) & 1)) + (long)fvy * (ez + (k >> 2)))];
+                            double kk;
+                            if (fj || fk) kk = (j == k && row == col) ? 1e6 : 0.0;
+                            else kk = pen * KEg[(3 * j + row) * 24 + 3 * k + col];
+                            s += pj * kk * pk;
+                        }
+                    }
+                    acc[c][half] += s;
+                }
+            }
+        }
+        // scatter: entry t = (3m+row)*24 + 3n+col -> node corner m, neighbour k(n-m)
+#pragma unroll
+        for (int c = 0; c < GAL_CELLS; c++) {
+            const int cid = scell[c];
+            if (cid < 0) continue;
+            const int X = cid % cnx, Y = (cid / cnx) % cny, Z = cid / (cnx * cny);
+#pragma unroll
+            for (int half = 0; half < 2; half++) {
+                const int t = half ? t1 : t0;
+                const int mrow = t / 24, ncol = t % 24;
+                const int m = mrow / 3, row = mrow % 3, n = ncol / 3, col = ncol % 3;
+                const int dx = (n & 1) - (m & 1), dy = ((n >> 1) & 1) - ((m >> 1) & 1), dz = (n >> 2) - (m >> 2);
+                const int k = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1);
+                const long vc = (X + (m & 1)) + (long)cvx * ((Y + ((m >> 1) & 1)) + (long)cvy * (Z + (m >> 2)));
+                st[(long)(k * 9 + row * 3 + col) * nvc + vc] += acc[c][half];
+            }
+        }
+    }
+}
+
+// A_c = P^T A_f P for a dyadic (ratio 2) level from the finer stencil
+__global__ void __launch_bounds__(ST_BS) k_galerkin_dyadic(int fnx, int fny, int fnz, int cnx, int cny, int cnz,
+                                                           const uint8_t* __restrict__ fvact,
+                                                           const uint8_t* __restrict__ cvact,
+                                                           const double* __restrict__ stf, double* __restrict__ stc) {
+    const int fvx = fnx + 1, fvy = fny + 1, fvz = fnz + 1;
+    const int cvx = cnx + 1, cvy = cny + 1, cvz = cnz + 1;
+    const long nvf = (long)fvx * fvy * fvz, nvc = (long)cvx * cvy * cvz;
+    const double wtab[4] = {1.0, 0.5, 0.25, 0.125};
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nvc * 9; t += (long)gridDim.x * blockDim.x) {
+        const long vc = t % nvc;
+        const int rc = (int)(t / nvc);
+        const int X = (int)(vc % cvx), Y = (int)((vc / cvx) % cvy), Z = (int)(vc / ((long)cvx * cvy));
+        double acc[27];
+#pragma unroll
+        for (int s = 0; s < 27; s++) acc[s] = 0;
+        if (cvact[vc]) {
+            for (int i = 0; i < 27; i++) {
+                const int dx = i % 3 - 1, dy = (i / 3) % 3 - 1, dz = i / 9 - 1;
+                const int x = 2 * X + dx, y = 2 * Y + dy, z = 2 * Z + dz;
+                if (x < 0 || y < 0 || z < 0 || x >= fvx || y >= fvy || z >= fvz) continue;
+                const long vn = x + (long)fvx * (y + (long)fvy * z);
+                if (!fvact[vn]) continue;
+                const double wi = wtab[abs(dx) + abs(dy) + abs(dz)];
+                for (int j = 0; j < 27; j++) {
+                    const int mx = x + j % 3 - 1, my = y + (j / 3) % 3 - 1, mz = z + j / 9 - 1;
+                    if (mx < 0 || my < 0 || mz < 0 || mx >= fvx || my >= fvy || mz >= fvz) continue;
+                    const double kij = stf[(long)(j * 9 + rc) * nvf + vn] * wi;
+                    if (kij == 0) continue;
+#pragma unroll
+                    for (int s = 0; s < 27; s++) {
+                        const int ax = abs(2 * (X + s % 3 - 1) - mx), ay = abs(2 * (Y + (s / 3) % 3 - 1) - my),
+                                  az = abs(2 * (Z + s / 9 - 1) - mz);
+                        if (ax >= 2 || ay >= 2 || az >= 2) continue;
+                        acc[s] += wtab[ax + ay + az] * kij;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < 27; s++) stc[(long)(s * 9 + rc) * nvc + vc] = acc[s];
+    }
+}
+
+__global__ void k_d2f(long n, const double* __restrict__ a, float* __restrict__ b) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) b[i] = (float)a[i];
+}
+
+}  // namespace
+
+namespace rtk {
+
+template <typename T>
+static const T* stp(rt_level& L);
+template <>
+const double* stp<double>(rt_level& L) { return L.st; }
+template <>
+const float* stp<float>(rt_level& L) { return L.st32; }
+
+template <typename T>
+int st_residual(rt_hier* h, int lvl, const T* u, const T* f, T* r) {
+    rt_level& L = h->L[lvl];
+    return rt_launch(h->ctx, sizeof(T) == 8 ? "st_residual_f64" : "st_residual_f32", [&] {
+        k_st_residual<T><<<grid_for(h->ctx, L.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(L.nx, L.ny, L.nz, L.vact,
+                                                                                      stp<T>(L), u, f, r);
+    });
+}
+
+template <typename T>
+int st_gs(rt_hier* h, int lvl, T* u, const T* f, bool backward) {
+    rt_level& L = h->L[lvl];
+    for (int cc = 0; cc < 8; cc++) {
+        int col = backward ? 7 - cc : cc;
+        long ncol = (long)((L.vx - (col & 1) + 1) / 2) * ((L.vy - ((col >> 1) & 1) + 1) / 2) *
+                    ((L.vz - ((col >> 2) & 1) + 1) / 2);
+        RT_CHECK(rt_launch(h->ctx, sizeof(T) == 8 ? "st_gs_f64" : "st_gs_f32", [&] {
+            k_st_gs<T><<<grid_for(h->ctx, ncol, ST_BS), ST_BS, 0, h->ctx->stream>>>(L.nx, L.ny, L.nz, col, backward,
+                                                                                    L.vact, stp<T>(L), u, f);
+        }));
+    }
+    return RT_OK;
+}
+
+template <typename T>
+int st_jacobi(rt_hier* h, int lvl, const T* u, const T* f, T* unew, double omega) {
+    rt_level& L = h->L[lvl];
+    return rt_launch(h->ctx, sizeof(T) == 8 ? "st_jacobi_f64" : "st_jacobi_f32", [&] {
+        k_st_jacobi<T><<<grid_for(h->ctx, L.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(L.nx, L.ny, L.nz, (T)omega, L.vact,
+                                                                                    stp<T>(L), u, f, unew);
+    });
+}
+
+template <typename T>
+int restrict_(rt_hier* h, int lvl, const T* rf, T* fc) {
+    rt_level& F = h->L[lvl - 1];
+    rt_level& Cc = h->L[lvl];
+    return rt_launch(h->ctx, sizeof(T) == 8 ? "restrict_f64" : "restrict_f32", [&] {
+        unsigned g = grid_for(h->ctx, Cc.nv, ST_BS);
+        if (Cc.ratio == 4)
+            k_restrict<T, 4><<<g, ST_BS, 0, h->ctx->stream>>>(F.nx, F.ny, F.nz, Cc.nx, Cc.ny, Cc.nz, Cc.vact, rf, fc);
+        else
+            k_restrict<T, 2><<<g, ST_BS, 0, h->ctx->stream>>>(F.nx, F.ny, F.nz, Cc.nx, Cc.ny, Cc.nz, Cc.vact, rf, fc);
+    });
+}
+
+template <typename T>
+int prolong_add(rt_hier* h, int lvl, const T* uc, T* uf) {
+    rt_level& F = h->L[lvl];
+    rt_level& Cc = h->L[lvl + 1];
+    return rt_launch(h->ctx, sizeof(T) == 8 ? "prolong_f64" : "prolong_f32", [&] {
+        unsigned g = grid_for(h->ctx, F.nv, ST_BS);
+        if (Cc.ratio == 4)
+            k_prolong<T, 4><<<g, ST_BS, 0, h->ctx->stream>>>(F.nx, F.ny, F.nz, Cc.nx, Cc.ny, Cc.nz, F.vact, uc, uf);
+        else
+            k_prolong<T, 2><<<g, ST_BS, 0, h->ctx->stream>>>(F.nx, F.ny, F.nz, Cc.nx, Cc.ny, Cc.nz, F.vact, uc, uf);
+    });
+}
+
+// Q_pos = P_pos^T KE P_pos for every element position in a coarse cell
+static int build_Q(rt_hier* h, int R, double** Qdev) {
+    const int NP = R * R * R;
+    std::vector<double> Qh((size_t)NP * 576);
+    for (int pos = 0; pos < NP; pos++) {
+        int a = pos % R, b = (pos / R) % R, c = pos / (R * R);
+        double P[8][8];
+        for (int j = 0; j < 8; j++) {
+            int o[3] = {a + (j & 1), b + ((j >> 1) & 1), c + (j >> 2)};
+            for (int m = 0; m < 8; m++) {
+                int mm[3] = {m & 1, (m >> 1) & 1, m >> 2};
+                double wv = 1;
+                for (int t = 0; t < 3; t++) wv *= (double)(R - abs(o[t] - R * mm[t])) / R;
+                P[j][m] = wv;
+            }
+        }
+        for (int m = 0; m < 8; m++)
+            for (int row = 0; row < 3; row++)
+                for (int n = 0; n < 8; n++)
+                    for (int col = 0; col < 3; col++) {
+                        double s = 0;
+                        for (int j = 0; j < 8; j++) {
+                            if (P[j][m] == 0) continue;
+                            for (int k = 0; k < 8; k++)
+                                s += P[j][m] * h->KE[(3 * j + row) * 24 + 3 * k + col] * P[k][n];
+                        }
+                        Qh[(size_t)pos * 576 + (3 * m + row) * 24 + 3 * n + col] = s;
+                    }
+    }
+    RT_CUDA(h->ctx, cudaMalloc(Qdev, sizeof(double) * Qh.size()));
+    RT_CUDA(h->ctx, cudaMemcpyAsync(*Qdev, Qh.data(), sizeof(double) * Qh.size(), cudaMemcpyHostToDevice,
+                                    h->ctx->stream));
+    return RT_OK;
+}
+
+int galerkin_from_elements(rt_hier* h) {
+    rt_level& F = h->L[0];
+    rt_level& Cc = h->L[1];
+    const int R = Cc.ratio;
+    if (h->Qgal == nullptr || h->Qgal_ratio != R) {
+        if (h->Qgal) cudaFree(h->Qgal);
+        h->Qgal = nullptr;
+        RT_CHECK(build_Q(h, R, &h->Qgal));
+        h->Qgal_ratio = R;
+    }
+    const double* Q = h->Qgal;
+    RT_CUDA(h->ctx, cudaMemsetAsync(Cc.st, 0, sizeof(double) * 243 * Cc.nv, h->ctx->stream));
+    for (int color = 0; color < 8; color++) {
+        long ccells = (long)((Cc.nx - (color & 1) + 1) / 2) * ((Cc.ny - ((color >> 1) & 1) + 1) / 2) *
+                      ((Cc.nz - (color >> 2) + 1) / 2);
+        long groups = (ccells + GAL_CELLS - 1) / GAL_CELLS;
+        if (groups == 0) continue;
+        unsigned g = (unsigned)(groups < (long)h->ctx->sm_count * 8 ? groups : (long)h->ctx->sm_count * 8);
+        RT_CHECK(rt_launch(h->ctx, "galerkin_cells", [&] {
+            const uint8_t* vf = h->has_support ? h->vfix : nullptr;
+            if (R == 4)
+                k_galerkin_cells<4><<<g, GAL_BS, 0, h->ctx->stream>>>(F.nx, F.ny, F.nz, Cc.nx, Cc.ny, Cc.nz, color,
+                                                                      Cc.eact, h->w, vf, Q, h->KE_dev, Cc.st);
+            else
+                k_galerkin_cells<2><<<g, GAL_BS, 0, h->ctx->stream>>>(F.nx, F.ny, F.nz, Cc.nx, Cc.ny, Cc.nz, color,
+                                                                      Cc.eact, h->w, vf, Q, h->KE_dev, Cc.st);
+        }));
+    }
+    return RT_OK;
+}
+
+int galerkin_from_stencil(rt_hier* h, int lvl) {
+    rt_level& F = h->L[lvl - 1];
+    rt_level& Cc = h->L[lvl];
+    return rt_launch(h->ctx, "galerkin_dyadic", [&] {
+        k_galerkin_dyadic<<<grid_for(h->ctx, Cc.nv * 9, ST_BS), ST_BS, 0, h->ctx->stream>>>(
+            F.nx, F.ny, F.nz, Cc.nx, Cc.ny, Cc.nz, F.vact, Cc.vact, F.st, Cc.st);
+    });
+}
+
+int d2f(rt_hier* h, long n, const double* a, float* b) {
+    return rt_launch(h->ctx, "d2f", [&] { k_d2f<<<grid_for(h->ctx, n, 256), 256, 0, h->ctx->stream>>>(n, a, b); });
+}
+
+template int st_residual<double>(rt_hier*, int, const double*, const double*, double*);
+template int st_residual<float>(rt_hier*, int, const float*, const float*, float*);
+template int st_gs<double>(rt_hier*, int, double*, const double*, bool);
+template int st_gs<float>(rt_hier*, int, float*, const float*, bool);
+template int st_jacobi<double>(rt_hier*, int, const double*, const double*, double*, double);
+template int st_jacobi<float>(rt_hier*, int, const float*, const float*, float*, double);
+template int restrict_<double>(rt_hier*, int, const double*, double*);
+template int restrict_<float>(rt_hier*, int, const float*, float*);
+template int prolong_add<double>(rt_hier*, int, const double*, double*);
+template int prolong_add<float>(rt_hier*, int, const float*, float*);
+
+}  // namespace rtk

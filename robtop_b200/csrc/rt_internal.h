@@ -1,0 +1,195 @@
+// rt_internal.h — internal state of the B200 solver library (not part of the ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/rtb200.h"
+
+#define RT_KERNEL_NAMES_MAX 64
+
+struct rt_kstat {
+    std::string name;
+    long long launches = 0;
+    double ms = 0;
+};
+
+struct rt_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+    int sm_count = 148;
+    long long launches = 0;
+    // profiling
+    bool profile = false;
+    std::vector<rt_kstat> kstats;
+    std::vector<cudaEvent_t> ev_pool;
+    struct Pending { int kid; cudaEvent_t a, b; };
+    std::vector<Pending> pending;
+    // host-pinned scalar mailbox
+    double* hscal = nullptr;
+};
+
+struct rt_level {
+    int nx = 0, ny = 0, nz = 0, vx = 0, vy = 0, vz = 0;
+    long nv = 0, ne = 0;
+    int ratio = 0;
+    long n_act_nodes = 0, n_act_elems = 0;
+    uint8_t* vact = nullptr;
+    uint8_t* eact = nullptr;
+    double *u = nullptr, *f = nullptr, *r = nullptr;
+    float *u32 = nullptr, *f32 = nullptr, *r32 = nullptr;
+    double* st = nullptr;   // [243][nv]
+    float* st32 = nullptr;  // [243][nv]
+    // coarsest level
+    int na = 0;
+    int* aidx = nullptr;
+    double* ainv = nullptr;  // [3na][3na]
+    float* ainv32 = nullptr;
+    double* dvec = nullptr;  // [3na] gather buffer
+    float* dvec32 = nullptr;
+};
+
+struct rt_hier {
+    rt_ctx* ctx = nullptr;
+    rt_params P;
+    std::vector<rt_level> L;
+    double KE[576];
+    double* KE_dev = nullptr;
+    float* KE32_dev = nullptr;
+    // level-0 design data
+    float* rho = nullptr;
+    float* w = nullptr;       // powf(rho, p) or 0
+    uint8_t* vfix = nullptr;  // support flags
+    bool has_support = false;
+    float* sens = nullptr;
+    float* ftmp = nullptr;    // element scratch (filter copy / OC trial)
+    uint8_t* eshell = nullptr;
+    // load set
+    int nload = 0;
+    int* load_nodes = nullptr;
+    double* load_normal = nullptr;  // [3*nload]
+    double* Rd = nullptr;           // [6][3*nload]
+    int nrig = 0;
+    double* Ru = nullptr;           // [6][3*nv] rigid modes over active nodes (no-support modes)
+    double* fs = nullptr;           // [3*nload] gather buffer
+    double* fs_old = nullptr;       // [3*nload]
+    // solver work vectors (3*nv doubles each)
+    double *x = nullptr, *rr = nullptr, *z = nullptr, *p = nullptr, *q = nullptr, *rold = nullptr;
+    // Lanczos basis
+    double* Q = nullptr;
+    int Qcap = 0;
+    // reductions
+    double* partials = nullptr;  // [RT_RED_BLOCKS * 8]
+    double* scal = nullptr;      // [64] device scalars
+    bool stencil_ready = false;
+    double* Qgal = nullptr;  // [R^3][576] cell Galerkin blocks P^T KE P (rebuilt when KE changes)
+    int Qgal_ratio = 0;
+};
+
+#define RT_RED_BLOCKS 296
+#define RT_PARTIALS (148 * 64)  // block partial sums: up to 64 values from 148 blocks
+#define RT_NSCAL 512            // device scalar slots
+
+// error helpers -------------------------------------------------------------
+int rt_fail(rt_ctx* c, int code, const char* fmt, ...);
+#define RT_CUDA(c, call)                                                                    \
+    do {                                                                                    \
+        cudaError_t _e = (call);                                                            \
+        if (_e != cudaSuccess)                                                              \
+            return rt_fail((c), RT_ECUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call,        \
+                           cudaGetErrorString(_e));                                         \
+    } while (0)
+#define RT_CHECK(x)                     \
+    do {                                \
+        int _s = (x);                   \
+        if (_s != RT_OK) return _s;     \
+    } while (0)
+
+// launch accounting ------------------------------------------------------------
+int rt_kernel_id(rt_ctx* c, const char* name);
+void rt_launch_begin(rt_ctx* c, int kid, cudaEvent_t* a);
+int rt_launch_end(rt_ctx* c, int kid, cudaEvent_t a, const char* name);
+
+template <typename F>
+inline int rt_launch(rt_ctx* c, const char* name, F&& f) {
+    static thread_local int cached_kid = -1;
+    static thread_local rt_ctx* cached_ctx = nullptr;
+    if (cached_ctx != c) { cached_kid = rt_kernel_id(c, name); cached_ctx = c; }
+    cudaEvent_t a = nullptr;
+    rt_launch_begin(c, cached_kid, &a);
+    f();
+    return rt_launch_end(c, cached_kid, a, name);
+}
+
+static inline unsigned rt_blocks(long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+// kernels (each returns RT_OK or an error code) -------------------------------
+namespace rtk {
+// fine level
+template <typename T>
+int fine_residual(rt_hier* h, const T* u, const T* f, T* r);
+template <typename T>
+int fine_applyK(rt_hier* h, const T* u, T* out);
+template <typename T>
+int fine_gs(rt_hier* h, T* u, const T* f, bool backward);
+template <typename T>
+int fine_jacobi(rt_hier* h, const T* u, const T* f, T* unew, double omega);
+int penalty_weights(rt_hier* h);
+// stencil levels
+template <typename T>
+int st_residual(rt_hier* h, int lvl, const T* u, const T* f, T* r);
+template <typename T>
+int st_gs(rt_hier* h, int lvl, T* u, const T* f, bool backward);
+template <typename T>
+int st_jacobi(rt_hier* h, int lvl, const T* u, const T* f, T* unew, double omega);
+int galerkin_from_elements(rt_hier* h);
+int galerkin_from_stencil(rt_hier* h, int lvl);
+// transfers
+template <typename T>
+int restrict_(rt_hier* h, int lvl, const T* rf, T* fc);
+template <typename T>
+int prolong_add(rt_hier* h, int lvl, const T* uc, T* uf);
+// coarsest
+int coarsest_setup(rt_hier* h);
+template <typename T>
+int coarsest_solve(rt_hier* h, const T* f, T* u);
+// BLAS-1 / reductions
+int dot(rt_hier* h, long n, const double* a, const double* b, double* out_dev);
+int dot2(rt_hier* h, long n, const double* a, const double* b, const double* c, double* out_dev);
+int axpy(rt_hier* h, long n, double a, const double* x, double* y);
+int d2f(rt_hier* h, long n, const double* a, float* b);
+int f2d(rt_hier* h, long n, const float* a, double* b);
+int d2f_scaled(rt_hier* h, long n, const double* a, float* b, const double* s_dev);
+int f2d_scaled(rt_hier* h, long n, const float* a, double* b, const double* s_dev);
+int pcg_update_xr(rt_hier* h, long n, const double* scal_alpha_num, const double* scal_alpha_den, double* x,
+                  double* r, const double* p, const double* q, double* rold);
+int pcg_update_p(rt_hier* h, long n, const double* s_num, const double* s_den, double* p, const double* z,
+                 bool first);
+int mask_copy(rt_hier* h, long n, const double* src, double* dst);
+// worst case
+int rng_uniform(rt_hier* h, uint64_t seed, long n, double* out);
+int project_load(rt_hier* h, double* f);
+int gather_load(rt_hier* h, const double* f, double* fs);
+int scatter_load(rt_hier* h, const double* fs, double* f);
+int rigid_basis(rt_hier* h);
+int rigid_nodes(rt_hier* h);
+int displacement_project(rt_hier* h, double* u);
+int scale(rt_hier* h, long n, double* x, const double* s_dev, bool inverse_sqrt);
+int tridiag_max_eig(rt_hier* h, int k, const double* alpha_dev, const double* beta_dev, double* out_dev);
+// optimisation
+int sensitivity(rt_hier* h, const double* u);
+int filter(rt_hier* h, float radius);
+int oc_try(rt_hier* h, float thr, float* out, double* vol_dev);
+int oc_maxabs(rt_hier* h, float* out_dev);
+// setup
+int node_active(rt_ctx* c, int nx, int ny, int nz, const uint8_t* eact, uint8_t* vact);
+int coarsen_elements(rt_ctx* c, int nx, int ny, int nz, int ratio, const uint8_t* ef, uint8_t* ec);
+int surface_nodes(rt_hier* h, uint8_t* surf_dev);
+int cube_vbits(rt_ctx* c, int R, const uint32_t* eb, uint32_t* vb);
+int cube_coarsen(rt_ctx* c, int R, const uint32_t* ef, uint32_t* ec);
+int count_u8(rt_ctx* c, long n, const uint8_t* a, double* out_dev);
+}  // namespace rtk

@@ -1,0 +1,337 @@
+"""Host-side mirror of robtop's ``grid::HierarchyGrid`` / ``grid::Grid`` API.
+
+Same method names and argument meaning as ``grid/Grid.h:172-692`` of the
+reference; every call goes through the C ABI in ``librtb200.so``.  Vectors are
+exchanged as numpy arrays in the dense layout (SoA ``[3][nv]``, x fastest) or,
+with ``layout=LAYOUT_REF_GS``, in the reference's GS-colour-ordered padded
+layout (``grid/Grid.cpp:2045-2106``).  Errors raise ``RTError`` instead of the
+reference's print-and-continue / ``exit(-1)``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi as A
+from ._capi import check
+
+
+def _p(a):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data
+
+
+class Context:
+    """One device + one CUDA stream (``stream`` may be a caller's cudaStream_t handle)."""
+
+    def __init__(self, device=0, stream=None):
+        self._h = C.c_void_p()
+        check(A.lib().rt_ctx_create(device, stream, C.byref(self._h)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def sync(self):
+        check(A.lib().rt_ctx_sync(self._h), self._h)
+
+    def last_error(self):
+        return A.lib().rt_last_error(self._h).decode()
+
+    def launches(self):
+        return int(A.lib().rt_launch_count(self._h))
+
+    def profile(self, on=True):
+        check(A.lib().rt_profile_enable(self._h, 1 if on else 0), self._h)
+
+    def profile_reset(self):
+        check(A.lib().rt_profile_reset(self._h), self._h)
+
+    def profile_stats(self):
+        out = {}
+        i = 0
+        name = C.create_string_buffer(128)
+        n = C.c_longlong()
+        ms = C.c_double()
+        while A.lib().rt_profile_query(self._h, i, name, 128, C.byref(n), C.byref(ms)) == A.RT_OK:
+            out[name.value.decode()] = (int(n.value), float(ms.value))
+            i += 1
+        return out
+
+    def close(self):
+        if self._h:
+            A.lib().rt_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def default_params(**kw):
+    p = A.Params()
+    A.lib().rt_params_default(C.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise AttributeError(k)
+        setattr(p, k, v)
+    return p
+
+
+class Grid:
+    """One level of the hierarchy (``grid::Grid``, grid/Grid.h:172-532)."""
+
+    def __init__(self, hier, level):
+        self._H = hier
+        self._layer = level
+        info = A.LevelInfo()
+        check(A.lib().rt_hier_level_info(hier.handle, level, C.byref(info)), hier.ctx.handle)
+        self.nx, self.ny, self.nz, self.ratio = info.nx, info.ny, info.nz, info.ratio
+        self.n_box_nodes = int(info.n_nodes)
+        self.n_vertices = int(info.n_active_nodes)
+        self.n_elements = int(info.n_active_elements)
+
+    # sizes ---------------------------------------------------------------
+    @property
+    def nv(self):
+        return self.n_box_nodes
+
+    @property
+    def ne(self):
+        return self.nx * self.ny * self.nz
+
+    def n_nodes(self):
+        return self.n_vertices
+
+    def n_valid_elements(self):
+        return self.n_elements
+
+    # operators (grid/Grid.cu) --------------------------------------------
+    def update_residual(self):
+        self._H._c(A.lib().rt_update_residual(self._H.handle, self._layer))
+
+    def gs_relax(self, n_times=1):
+        self._H._c(A.lib().rt_smooth(self._H.handle, self._layer, A.SMOOTH_GS, n_times, 1.0))
+
+    def smooth(self, smoother, sweeps=1, omega=0.6):
+        self._H._c(A.lib().rt_smooth(self._H.handle, self._layer, smoother, sweeps, omega))
+
+    def restrict_residual(self):
+        self._H._c(A.lib().rt_restrict_residual(self._H.handle, self._layer))
+
+    def prolongate_correction(self):
+        self._H._c(A.lib().rt_prolongate_correction(self._H.handle, self._layer))
+
+    def solve_fem_host(self):
+        """Coarsest direct solve (on the device, despite the reference's name)."""
+        self._H._c(A.lib().rt_coarsest_solve(self._H.handle))
+
+    def applyK(self, u):
+        assert self._layer == 0
+        u = np.ascontiguousarray(u, np.float64)
+        out = np.zeros_like(u)
+        self._H._c(A.lib().rt_apply_K(self._H.handle, _p(u), _p(out)))
+        return out
+
+    def compliance(self):
+        c = C.c_double()
+        self._H._c(A.lib().rt_compliance(self._H.handle, C.byref(c)))
+        return c.value
+
+    def relative_residual(self):
+        c = C.c_double()
+        self._H._c(A.lib().rt_relative_residual(self._H.handle, C.byref(c)))
+        return c.value
+
+    def filterSensitivity(self, radii):
+        self._H._c(A.lib().rt_filter_sensitivity(self._H.handle, float(radii)))
+
+    def init_rho(self, rh0):
+        self._H._c(A.lib().rt_init_density(self._H.handle, float(rh0)))
+
+    # fields ---------------------------------------------------------------
+    def _get(self, field, layout, shape, dtype):
+        out = np.zeros(shape, dtype)
+        self._H._c(A.lib().rt_get(self._H.handle, field, self._layer, layout, _p(out)))
+        return out
+
+    def _put(self, field, layout, arr, dtype):
+        arr = np.ascontiguousarray(arr, dtype)
+        self._H._c(A.lib().rt_put(self._H.handle, field, self._layer, layout, _p(arr)))
+
+    def ref_gs_map(self):
+        vm = np.zeros(self.nv, np.int32)
+        ngs = C.c_int()
+        gsn = np.zeros(8, np.int32)
+        self._H._c(A.lib().rt_ref_gs_map(self._H.handle, self._layer, _p(vm), C.byref(ngs), _p(gsn)))
+        return vm, int(ngs.value), gsn
+
+    def _vec_shape(self, layout):
+        if layout == A.LAYOUT_REF_GS:
+            return 3 * self.ref_gs_map()[1]
+        return 3 * self.nv
+
+    def getDisplacement(self, layout=A.LAYOUT_DENSE):
+        return self._get(A.FIELD_U, layout, self._vec_shape(layout), np.float64)
+
+    def getForce(self, layout=A.LAYOUT_DENSE):
+        return self._get(A.FIELD_F, layout, self._vec_shape(layout), np.float64)
+
+    def getResidual(self, layout=A.LAYOUT_DENSE):
+        return self._get(A.FIELD_R, layout, self._vec_shape(layout), np.float64)
+
+    def setDisplacement(self, u, layout=A.LAYOUT_DENSE):
+        self._put(A.FIELD_U, layout, u, np.float64)
+
+    def setForce(self, f, layout=A.LAYOUT_DENSE):
+        self._put(A.FIELD_F, layout, f, np.float64)
+
+    def setResidual(self, r, layout=A.LAYOUT_DENSE):
+        self._put(A.FIELD_R, layout, r, np.float64)
+
+    def getRho(self):
+        return self._get(A.FIELD_RHO, A.LAYOUT_DENSE, self.ne, np.float32)
+
+    def setRho(self, rho):
+        self._put(A.FIELD_RHO, A.LAYOUT_DENSE, rho, np.float32)
+
+    def getSens(self):
+        return self._get(A.FIELD_SENS, A.LAYOUT_DENSE, self.ne, np.float32)
+
+    def setSens(self, s):
+        self._put(A.FIELD_SENS, A.LAYOUT_DENSE, s, np.float32)
+
+    def getStencil(self):
+        return self._get(A.FIELD_STENCIL, A.LAYOUT_DENSE, 243 * self.nv, np.float64)
+
+    def setStencil(self, st):
+        self._put(A.FIELD_STENCIL, A.LAYOUT_DENSE, st, np.float64)
+
+    def getVact(self):
+        return self._get(A.FIELD_VACT, A.LAYOUT_DENSE, self.nv, np.uint8)
+
+    def getEact(self):
+        return self._get(A.FIELD_EACT, A.LAYOUT_DENSE, self.ne, np.uint8)
+
+    def reset_displacement(self):
+        self.setDisplacement(np.zeros(3 * self.nv))
+
+    def reset_force(self):
+        self.setForce(np.zeros(3 * self.nv))
+
+    def reset_residual(self):
+        self.setResidual(np.zeros(3 * self.nv))
+
+
+class HierarchyGrid:
+    """``grid::HierarchyGrid`` (grid/Grid.h:534-692) on the device."""
+
+    def __init__(self, ctx: Context, params=None):
+        self.ctx = ctx
+        self.params = params if params is not None else default_params()
+        self._h = C.c_void_p()
+        self._grids = []
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _c(self, status):
+        return check(status, self.ctx.handle)
+
+    # construction (grid/Grid.cpp:455-712) --------------------------------
+    def genFromMesh(self, solid_bit, out_reso):
+        """Cubic ``out_reso[0]^3`` bit grid (LSB-first words, bit x + y R + z R^2)."""
+        reso = int(out_reso[0]) if np.ndim(out_reso) else int(out_reso)
+        bits = np.ascontiguousarray(solid_bit, np.uint32)
+        self._c(A.lib().rt_hier_create_from_bits(self.ctx.handle, C.byref(self.params), reso, _p(bits),
+                                                 C.byref(self._h)))
+        self._init_levels()
+
+    def genFromBox(self, eact):
+        """Dense element-activity box ``eact[nz, ny, nx]`` (x fastest)."""
+        eact = np.ascontiguousarray(eact, np.uint8)
+        nz, ny, nx = eact.shape
+        self._c(A.lib().rt_hier_create(self.ctx.handle, C.byref(self.params), nx, ny, nz, _p(eact),
+                                       C.byref(self._h)))
+        self._init_levels()
+
+    def _init_levels(self):
+        n = A.lib().rt_hier_n_levels(self._h)
+        self._grids = [Grid(self, i) for i in range(n)]
+
+    def __getitem__(self, i):
+        return self._grids[i]
+
+    def n_grid(self):
+        return len(self._grids)
+
+    def setMode(self, mode):
+        self.params.mode = mode
+        self.set_params(self.params)
+
+    def set_params(self, params):
+        self.params = params
+        self._c(A.lib().rt_hier_set_params(self._h, C.byref(params)))
+
+    def isForceFree(self):
+        return self.params.mode in (A.MODE_NSFF, A.MODE_WSFF)
+
+    def hasSupport(self):
+        return self.params.mode in (A.MODE_WSCF, A.MODE_WSFF)
+
+    def template_matrix(self):
+        KE = np.zeros((24, 24))
+        self._c(A.lib().rt_template_matrix(self._h, _p(KE)))
+        return KE
+
+    # boundary conditions ---------------------------------------------------
+    def surface_nodes(self):
+        s = np.zeros(self[0].nv, np.uint8)
+        self._c(A.lib().rt_surface_nodes(self._h, _p(s)))
+        return s
+
+    def set_support(self, vfix):
+        vfix = np.ascontiguousarray(vfix, np.uint8).ravel()
+        self._c(A.lib().rt_set_support(self._h, _p(vfix)))
+
+    def set_load_nodes(self, nodes, normals):
+        nodes = np.ascontiguousarray(nodes, np.int32)
+        normals = np.ascontiguousarray(normals, np.float64).reshape(-1)
+        self._c(A.lib().rt_set_load_nodes(self._h, int(nodes.size), _p(nodes), _p(normals)))
+
+    # multigrid -----------------------------------------------------------------
+    def update_stencil(self):
+        self._c(A.lib().rt_update_stencil(self._h))
+
+    def v_cycle(self, pre_relax=1, post_relax=1):
+        r = C.c_double()
+        self._c(A.lib().rt_vcycle(self._h, pre_relax, post_relax, C.byref(r)))
+        return r.value
+
+    def pcg(self, tol=1e-6, maxit=200):
+        info = A.SolveInfo()
+        st = A.lib().rt_pcg(self._h, tol, maxit, C.byref(info))
+        if st not in (A.RT_OK, A.RT_ENOCONV):
+            self._c(st)
+        return info
+
+    def worst_case(self, method=A.WORST_LANCZOS, k=16, inner_tol=1e-8, seed=0):
+        lam = C.c_double()
+        info = A.SolveInfo()
+        self._c(A.lib().rt_worst_case(self._h, method, k, inner_tol, seed, C.byref(lam), C.byref(info)))
+        return lam.value, info
+
+    def close(self):
+        if self._h:
+            A.lib().rt_hier_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
