@@ -54,7 +54,8 @@ enum rt_smoother { RT_SMOOTH_GS = 0, RT_SMOOTH_SGS = 1, RT_SMOOTH_JACOBI = 2 };
 enum rt_precision { RT_FP64 = 0, RT_FP32 = 1 };
 enum rt_layout { RT_LAYOUT_DENSE = 0, RT_LAYOUT_REF_GS = 1 };
 enum rt_field { RT_FIELD_U = 0, RT_FIELD_F = 1, RT_FIELD_R = 2, RT_FIELD_RHO = 3, RT_FIELD_SENS = 4,
-                RT_FIELD_STENCIL = 5, RT_FIELD_VACT = 6, RT_FIELD_EACT = 7, RT_FIELD_VFIX = 8 };
+                RT_FIELD_STENCIL = 5, RT_FIELD_VACT = 6, RT_FIELD_EACT = 7, RT_FIELD_VFIX = 8,
+                RT_FIELD_PENALTY = 9 /* level-0 element weights powf(rho, p), FP32, refreshed by rt_update_stencil */ };
 enum rt_worst_method { RT_WORST_MODPM = 0, RT_WORST_LANCZOS = 1 };
 
 /* Parameter block: optimization/optimization.h:11-22 plus the solver knobs the

@@ -18,7 +18,8 @@ MODE_NSCF, MODE_NSFF, MODE_WSCF, MODE_WSFF = range(4)
 SMOOTH_GS, SMOOTH_SGS, SMOOTH_JACOBI = range(3)
 FP64, FP32 = 0, 1
 LAYOUT_DENSE, LAYOUT_REF_GS = 0, 1
-FIELD_U, FIELD_F, FIELD_R, FIELD_RHO, FIELD_SENS, FIELD_STENCIL, FIELD_VACT, FIELD_EACT, FIELD_VFIX = range(9)
+FIELD_U, FIELD_F, FIELD_R, FIELD_RHO, FIELD_SENS, FIELD_STENCIL, FIELD_VACT, FIELD_EACT, FIELD_VFIX, \
+    FIELD_PENALTY = range(10)
 WORST_MODPM, WORST_LANCZOS = 0, 1
 
 

@@ -82,5 +82,25 @@ def build(verbose=False, ptxas_info=False) -> str:
     return LIB
 
 
+COMPAT_SRC = os.path.join(ROOT, "tests", "cpp", "compat_main.cpp")
+COMPAT_BIN = os.path.join(ROOT, "tests", "cpp", "compat_test")
+
+
+def build_compat_driver() -> str:
+    """C++ driver of the reference-signature layer (tests/cpp/compat_main.cpp)."""
+    lib = build()
+    if os.path.exists(COMPAT_BIN) and os.path.getmtime(COMPAT_BIN) >= max(os.path.getmtime(COMPAT_SRC),
+                                                                           os.path.getmtime(lib)):
+        return COMPAT_BIN
+    cxx = _host_cxx() or "g++"
+    cmd = [cxx, "-O2", "-std=c++17", COMPAT_SRC, "-o", COMPAT_BIN, "-I/usr/local/cuda/include", f"-L{HERE}",
+           "-lrtb200", f"-Wl,-rpath,{HERE}", "-Wl,-rpath,$ORIGIN/../../robtop_b200"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"compat driver build failed:\n{r.stdout}\n{r.stderr}")
+    return COMPAT_BIN
+
+
 if __name__ == "__main__":
     print(build(verbose="-v" in sys.argv, ptxas_info="--ptxas" in sys.argv))
+    print(build_compat_driver())

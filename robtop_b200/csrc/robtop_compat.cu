@@ -1,0 +1,369 @@
+// robtop_compat.cu — the reference's C++ entry points (robtop_compat.h) on the C ABI.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+
+#include "robtop_compat.h"
+#include "rt_internal.h"
+
+Parameter params;
+grid::HierarchyGrid grids;
+
+namespace grid {
+
+void HierarchyGrid::check(int status, const char* what) {
+    if (status != RT_OK) {
+        std::string msg = std::string(what) + ": " + (_ctx ? rt_last_error(_ctx) : "no context") + " (status " +
+                          std::to_string(status) + ")";
+        throw std::runtime_error(msg);
+    }
+}
+
+HierarchyGrid::HierarchyGrid(void) {
+    rt_params_default(&_params);
+    _params.smoother = RT_SMOOTH_GS;  // the reference's V-cycle smoother
+}
+
+HierarchyGrid::~HierarchyGrid() {
+    for (auto g : _grids) delete g;
+    // the process may already be tearing the CUDA runtime down at static destruction;
+    // library handles are released only when the runtime is still usable
+    if (_h && cudaFree(nullptr) == cudaSuccess) rt_hier_destroy(_h);
+    if (_ctx && cudaFree(nullptr) == cudaSuccess) rt_ctx_destroy(_ctx);
+}
+
+void HierarchyGrid::setMode(Mode mode) {
+    _mode = mode;
+    _params.mode = (int)mode;  // same order as rt_mode
+    if (_h) check(rt_hier_set_params(_h, &_params), "setMode");
+}
+
+void HierarchyGrid::resetAllResidual(void) {
+    for (auto g : _grids) g->reset_residual();
+}
+
+// HierarchyGrid::genFromMesh(solid_bit, out_reso) (grid/Grid.cpp:455-712) plus the
+// support / load flags of Grid::computeProjectionMatrix (grid/Grid.cpp:1291-1403)
+void HierarchyGrid::genFromMesh(const std::vector<unsigned int>& solid_bit, int out_reso[3]) {
+    if (!_ctx) check(rt_ctx_create(0, nullptr, &_ctx), "rt_ctx_create");
+    if (_h) {
+        rt_hier_destroy(_h);
+        _h = nullptr;
+        for (auto g : _grids) delete g;
+        _grids.clear();
+    }
+    const int R = out_reso[0];
+    if ((long long)solid_bit.size() * 32 < (long long)R * R * R) throw std::runtime_error("genFromMesh: bit array too short");
+    check(rt_hier_create_from_bits(_ctx, &_params, R, solid_bit.data(), &_h), "genFromMesh");
+    for (int i = 0; i < rt_hier_n_levels(_h); i++) _grids.push_back(new Grid(this, i));
+    rt_level_info li;
+    check(rt_hier_level_info(_h, 0, &li), "level info");
+    const int vx = li.nx + 1, vy = li.ny + 1, vz = li.nz + 1;
+    const long nv = (long)vx * vy * vz;
+    std::vector<uint8_t> surf(nv), vact(nv), vfix(nv, 0), eact((size_t)li.nx * li.ny * li.nz);
+    check(rt_surface_nodes(_h, surf.data()), "surface nodes");
+    check(rt_get(_h, RT_FIELD_VACT, 0, RT_LAYOUT_DENSE, vact.data()), "vact");
+    check(rt_get(_h, RT_FIELD_EACT, 0, RT_LAYOUT_DENSE, eact.data()), "eact");
+    std::vector<double> normals;
+    _load_nodes.clear();
+    _preload.clear();
+    const double eh = _params.element_length;
+    for (long v = 0; v < nv; v++) {
+        if (!surf[v] || !vact[v]) continue;
+        const int x = v % vx, y = (v / vx) % vy, z = v / ((long)vx * vy);
+        double pos[3] = {x * eh, y * eh, z * eh};
+        if (_inFixedArea && _inFixedArea(pos)) {
+            vfix[v] = 1;
+            continue;
+        }
+        if (_inLoadArea && _inLoadArea(pos)) {
+            _load_nodes.push_back((int)v);
+            // outward normal from the empty incident element slots (stand-in for the
+            // CGAL AABB-tree normal of Grid::outwardNormal, grid/Grid.cpp:1405-1423)
+            double n[3] = {0, 0, 0};
+            for (int i = 0; i < 8; i++) {
+                const int ex = x + (i & 1) - 1, ey = y + ((i >> 1) & 1) - 1, ez = z + (i >> 2) - 1;
+                const bool inside = ex >= 0 && ey >= 0 && ez >= 0 && ex < li.nx && ey < li.ny && ez < li.nz &&
+                                    eact[ex + (size_t)li.nx * (ey + (size_t)li.ny * ez)];
+                if (!inside) {
+                    n[0] += (i & 1) ? 0.5 : -0.5;
+                    n[1] += ((i >> 1) & 1) ? 0.5 : -0.5;
+                    n[2] += (i >> 2) ? 0.5 : -0.5;
+                }
+            }
+            double nn = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+            if (nn == 0) { n[2] = 1; nn = 1; }
+            for (int t = 0; t < 3; t++) normals.push_back(n[t] / nn);
+            std::array<double, 3> fl = _loadField ? _loadField(pos) : std::array<double, 3>{0, 0, 0};
+            for (int t = 0; t < 3; t++) _preload.push_back(fl[t]);
+        }
+    }
+    check(rt_set_support(_h, vfix.data()), "rt_set_support");
+    check(rt_set_load_nodes(_h, (int)_load_nodes.size(), _load_nodes.data(), normals.data()), "rt_set_load_nodes");
+    // rt_set_load_nodes keeps the nodes sorted; _load_nodes was built in increasing order already
+}
+
+void HierarchyGrid::update_stencil(void) { check(rt_update_stencil(_h), "update_stencil"); }
+
+double HierarchyGrid::v_cycle(int pre_relax, int post_relax) {
+    double r = 0;
+    check(rt_vcycle(_h, pre_relax, post_relax, &r), "v_cycle");
+    return r;
+}
+
+Grid::Grid(HierarchyGrid* owner, int layer) : _layer(layer), _H(owner) {
+    rt_level_info li;
+    owner->check(rt_hier_level_info(owner->hier(), layer, &li), "level info");
+    _nv = li.n_nodes;
+    _n_active_nodes = li.n_active_nodes;
+    _n_active_elements = li.n_active_elements;
+    rt_level& L = owner->hier()->L[layer];
+    for (int c = 0; c < 3; c++) {
+        _U[c] = L.u + c * L.nv;
+        _F[c] = L.f + c * L.nv;
+        _R[c] = L.r + c * L.nv;
+    }
+}
+
+void Grid::update_residual(void) { _H->check(rt_update_residual(_H->hier(), _layer), "update_residual"); }
+void Grid::gs_relax(int n) { _H->check(rt_smooth(_H->hier(), _layer, RT_SMOOTH_GS, n, 1.0), "gs_relax"); }
+void Grid::restrict_residual(void) { _H->check(rt_restrict_residual(_H->hier(), _layer), "restrict_residual"); }
+void Grid::prolongate_correction(void) {
+    _H->check(rt_prolongate_correction(_H->hier(), _layer), "prolongate_correction");
+}
+void Grid::solve_fem_host(void) { _H->check(rt_coarsest_solve(_H->hier()), "solve_fem_host"); }
+
+static bool contiguous(double* v[3], long long nv) { return v[1] == v[0] + nv && v[2] == v[0] + 2 * nv; }
+
+void Grid::applyK(double* u[3], double* f[3]) {
+    if (_layer != 0) throw std::runtime_error("applyK is defined on the finest level");
+    rt_hier* h = _H->hier();
+    cudaStream_t s = h->ctx->stream;
+    const double* uin = u[0];
+    if (!contiguous(u, _nv)) {
+        for (int c = 0; c < 3; c++) cudaMemcpyAsync(h->x + c * _nv, u[c], sizeof(double) * _nv, cudaMemcpyDeviceToDevice, s);
+        uin = h->x;
+    }
+    double* out = contiguous(f, _nv) ? f[0] : h->q;
+    _H->check(rt_apply_K_dev(h, uin, out), "applyK");
+    if (out == h->q)
+        for (int c = 0; c < 3; c++) cudaMemcpyAsync(f[c], h->q + c * _nv, sizeof(double) * _nv, cudaMemcpyDeviceToDevice, s);
+}
+
+double Grid::compliance(void) {
+    if (_layer != 0) return v3_dot(_F, _U);
+    double c = 0;
+    _H->check(rt_compliance(_H->hier(), &c), "compliance");
+    return c;
+}
+
+double Grid::relative_residual(void) { return v3_norm(_R) / v3_norm(_F); }
+double Grid::residual(void) { return v3_norm(_R); }
+void Grid::filterSensitivity(double radii) {
+    _H->check(rt_filter_sensitivity(_H->hier(), (float)radii), "filterSensitivity");
+}
+void Grid::init_rho(double rh0) { _H->check(rt_init_density(_H->hier(), (float)rh0), "init_rho"); }
+
+static uint64_t g_rand_seed = 0x5eed;
+void Grid::randForce(void) {
+    rt_hier* h = _H->hier();
+    _H->check(rtk::rng_uniform(h, g_rand_seed++, 3 * _nv, _F[0]), "randForce");
+}
+
+double Grid::unitizeForce(void) {
+    const double n = v3_norm(_F);
+    v3_scale(_F, 1.0 / n);
+    return n;
+}
+
+void Grid::reset_displacement(void) {
+    for (int c = 0; c < 3; c++) cudaMemsetAsync(_U[c], 0, sizeof(double) * _nv, _H->hier()->ctx->stream);
+}
+void Grid::reset_force(void) {
+    for (int c = 0; c < 3; c++) cudaMemsetAsync(_F[c], 0, sizeof(double) * _nv, _H->hier()->ctx->stream);
+}
+void Grid::reset_residual(void) {
+    for (int c = 0; c < 3; c++) cudaMemsetAsync(_R[c], 0, sizeof(double) * _nv, _H->hier()->ctx->stream);
+}
+float* Grid::getRho(void) { return _layer == 0 ? _H->hier()->rho : nullptr; }
+float* Grid::getSens(void) { return _layer == 0 ? _H->hier()->sens : nullptr; }
+
+double Grid::v3_dot(double* v[3], double* u[3]) {
+    rt_hier* h = _H->hier();
+    double tot = 0;
+    for (int c = 0; c < 3; c++) {
+        _H->check(rtk::dot(h, _nv, v[c], u[c], h->scal + 80 + c), "v3_dot");
+    }
+    cudaMemcpyAsync(h->ctx->hscal, h->scal + 80, sizeof(double) * 3, cudaMemcpyDeviceToHost, h->ctx->stream);
+    cudaStreamSynchronize(h->ctx->stream);
+    for (int c = 0; c < 3; c++) tot += h->ctx->hscal[c];
+    return tot;
+}
+
+double Grid::v3_norm(double* v[3]) { return std::sqrt(v3_dot(v, v)); }
+
+void Grid::v3_copy(double* vsrc[3], double* vdst[3]) {
+    for (int c = 0; c < 3; c++)
+        cudaMemcpyAsync(vdst[c], vsrc[c], sizeof(double) * _nv, cudaMemcpyDeviceToDevice, _H->hier()->ctx->stream);
+}
+
+void Grid::v3_scale(double* v[3], double ampl) {
+    rt_hier* h = _H->hier();
+    cudaMemcpyAsync(h->scal + 84, &ampl, sizeof(double), cudaMemcpyHostToDevice, h->ctx->stream);
+    for (int c = 0; c < 3; c++) _H->check(rtk::scale(h, _nv, v[c], h->scal + 84, false), "v3_scale");
+    cudaStreamSynchronize(h->ctx->stream);
+}
+
+}  // namespace grid
+
+// ---------------------------------------------------------------------------
+// optimization/optimization.h free functions
+// ---------------------------------------------------------------------------
+static uint64_t g_pm_seed = 1;
+
+void buildGrids(const std::vector<unsigned int>& solid_bit, int reso) {
+    grids.set_skip_layer(true);  // buildGrids always skips layer 1 (optimization/optimization.cpp:17)
+    int r[3] = {reso, reso, reso};
+    grids.genFromMesh(solid_bit, r);
+}
+
+void setParameters(float volRatio, float volDecrease, float designStep, float filterRadi, float dampRatio,
+                   float powerPenal, float min_density, int gridreso, float youngs_modulu, float poisson_ratio,
+                   float /*shell_width*/, bool /*logdensity*/, bool /*logcompliance*/) {
+    params.volume_ratio = volRatio;
+    params.volume_decrease = volDecrease;
+    params.design_step = designStep;
+    params.filter_radius = (int)filterRadi;
+    params.damp_ratio = dampRatio;
+    params.power_penalty = powerPenal;
+    params.min_rho = min_density;
+    params.gridreso = gridreso;
+    params.youngs_modulu = youngs_modulu;
+    params.poisson_ratio = poisson_ratio;
+    rt_params& p = grids.params();
+    p.volume_ratio = volRatio;
+    p.design_step = designStep;
+    p.filter_radius = (float)params.filter_radius;
+    p.damp_ratio = dampRatio;
+    p.power_penalty = powerPenal;
+    p.min_rho = min_density;
+    p.youngs_modulus = youngs_modulu;
+    p.poisson_ratio = poisson_ratio;
+    if (grids.hier()) grids.check(rt_hier_set_params(grids.hier(), &p), "setParameters");
+}
+
+void setWorkMode(const std::string& m) {
+    if (m == "nscf") grids.setMode(grid::no_support_constrain_force_direction);
+    else if (m == "nsff") grids.setMode(grid::no_support_free_force);
+    else if (m == "wscf") grids.setMode(grid::with_support_constrain_force_direction);
+    else if (m == "wsff") grids.setMode(grid::with_support_free_force);
+    else throw std::invalid_argument("unsupported mode " + m);
+}
+
+grid::HierarchyGrid& getGrids(void) { return grids; }
+
+void setBoundaryCondition(std::function<bool(double[3])> fixarea, std::function<bool(double[3])> loadarea,
+                          std::function<std::array<double, 3>(double[3])> forcefield) {
+    grids._inFixedArea = fixarea;
+    grids._inLoadArea = loadarea;
+    grids._loadField = forcefield;
+}
+
+void uploadTemplateMatrix(void) {
+    rt_params& p = grids.params();
+    p.youngs_modulus = params.youngs_modulu;
+    p.poisson_ratio = params.poisson_ratio;
+    p.power_penalty = params.power_penalty;
+    grids.check(rt_hier_set_params(grids.hier(), &p), "uploadTemplateMatrix");
+}
+
+void initDensities(double rho) { grids[0]->init_rho(rho); }
+
+void update_stencil(void) { grids.update_stencil(); }
+
+// solveFEM (optimization/optimization.cpp:85-91) on the preloaded force field
+// (the load field at the load nodes, TestSuit::testOrdinaryTopopt's setForceSupport)
+void solveFEM(void) {
+    rt_hier* h = grids.hier();
+    const long long nv = grids[0]->n_box_nodes();
+    std::vector<double> f(3 * nv, 0.0);
+    const auto& ln = grids.loadNodes();
+    const auto& pl = grids.preloadForce();
+    for (size_t i = 0; i < ln.size(); i++)
+        for (int c = 0; c < 3; c++) f[c * nv + ln[i]] = pl[3 * i + c];
+    grids.check(rt_put(h, RT_FIELD_F, 0, RT_LAYOUT_DENSE, f.data()), "solveFEM");
+    double rel = 1;
+    int it = 0;
+    while (rel > 1e-4) {
+        rel = grids.v_cycle();
+        if (++it > 1000 || !std::isfinite(rel)) throw std::runtime_error("solveFEM did not converge");
+    }
+}
+
+double modifiedPM(void) {
+    double lam = 0;
+    rt_solve_info info;
+    grids.check(rt_worst_case(grids.hier(), RT_WORST_MODPM, 500, 0.0, g_pm_seed++, &lam, &info), "modifiedPM");
+    return lam;
+}
+
+void computeSensitivity(void) { grids.check(rt_sensitivity(grids.hier(), 1), "computeSensitivity"); }
+
+float updateDensities(float Vgoal) {
+    float lam = 0;
+    int trials = 0;
+    grids.check(rt_oc_update(grids.hier(), Vgoal, &lam, &trials), "updateDensities");
+    return lam;
+}
+
+// optimization() (optimization/optimization.cpp:583-673) without the file output
+void optimization(int max_iter) {
+    initDensities(params.volume_ratio);
+    float Vgoal = params.volume_ratio;
+    double last = 0;
+    int small = 0;
+    for (int itn = 1; itn <= max_iter; itn++) {
+        Vgoal *= (1 - params.volume_decrease);
+        if (Vgoal < params.volume_ratio) Vgoal = params.volume_ratio;
+        update_stencil();
+        const double c = modifiedPM();
+        // converge_criteria(1, 2, 5e-3) (utils/snippet.h:156-213): relative change below 5e-3 twice
+        if (itn > 1 && std::fabs(c - last) / std::fabs(last) < 5e-3) small++;
+        else small = 0;
+        last = c;
+        if (small >= 2 && Vgoal <= params.volume_ratio + 1e-3) break;
+        computeSensitivity();
+        updateDensities(Vgoal);
+    }
+}
+
+// test_rigid_displacement (optimization/optimization.cpp:697-709)
+void test_rigid_displacement(void) {
+    grid::Grid* g = grids[0];
+    rt_hier* h = grids.hier();
+    rt_level& L = h->L[0];
+    std::vector<double> u(3 * L.nv);
+    std::vector<uint8_t> act(L.nv);
+    grids.check(rt_get(h, RT_FIELD_VACT, 0, RT_LAYOUT_DENSE, act.data()), "vact");
+    for (int k = 0; k < 6; k++) {
+        for (long v = 0; v < L.nv; v++) {
+            const double p[3] = {(double)(v % L.vx), (double)((v / L.vx) % L.vy), (double)(v / ((long)L.vx * L.vy))};
+            double m[3] = {0, 0, 0};
+            if (k < 3) m[k] = 1;
+            else {
+                const double w[3] = {k == 3 ? 1.0 : 0.0, k == 4 ? 1.0 : 0.0, k == 5 ? 1.0 : 0.0};
+                m[0] = w[1] * p[2] - w[2] * p[1];
+                m[1] = w[2] * p[0] - w[0] * p[2];
+                m[2] = w[0] * p[1] - w[1] * p[0];
+            }
+            for (int c = 0; c < 3; c++) u[c * L.nv + v] = act[v] ? m[c] : 0.0;
+        }
+        grids.check(rt_put(h, RT_FIELD_U, 0, RT_LAYOUT_DENSE, u.data()), "rigid u");
+        g->reset_force();
+        g->update_residual();
+        printf("-- u_rigid %d res = %lf\n", k, g->residual());
+    }
+}

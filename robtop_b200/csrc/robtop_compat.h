@@ -1,0 +1,154 @@
+// robtop_compat.h — the reference's C++ entry points, implemented on the C ABI.
+//
+// Same names, argument meaning and call order as lavenklau/robtop's
+// optimization/optimization.h:28-82 and grid/Grid.h:172-692, so callers such as
+// robtop.cpp:27-46 or the TestSuit routines link against this layer unchanged
+// except for two documented differences:
+//  * vectors returned by getForce()/getDisplacement()/getResidual() are device
+//    pointers to the three components of the DENSE node box (SoA, x fastest),
+//    not the reference's GS-colour-ordered arrays (use rt_get(...,
+//    RT_LAYOUT_REF_GS, ...) for that order);
+//  * setBoundaryCondition's force field returns std::array<double,3> instead of
+//    Eigen::Matrix<double,3,1> (Eigen is not a dependency of this library).
+// Errors throw std::runtime_error carrying rt_last_error(); the reference
+// printed and continued or called exit(-1).
+#pragma once
+#include <array>
+#include <cstdint>
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "../../include/rtb200.h"
+
+namespace grid {
+
+enum Mode {
+    no_support_constrain_force_direction,
+    no_support_free_force,
+    with_support_constrain_force_direction,
+    with_support_free_force
+};
+
+class HierarchyGrid;
+
+// one level (grid::Grid, grid/Grid.h:172-532)
+class Grid {
+public:
+    Grid(HierarchyGrid* owner, int layer);
+    void update_residual(void);
+    void gs_relax(int n_times = 1);
+    void restrict_residual(void);
+    void prolongate_correction(void);
+    void solve_fem_host(void);
+    void applyK(double* u[3], double* f[3]);
+    double compliance(void);
+    double relative_residual(void);
+    double residual(void);
+    void filterSensitivity(double radii);
+    void init_rho(double rh0);
+    void randForce(void);
+    double unitizeForce(void);
+    void reset_displacement(void);
+    void reset_force(void);
+    void reset_residual(void);
+    double** getForce(void) { return _F; }
+    double** getDisplacement(void) { return _U; }
+    double** getResidual(void) { return _R; }
+    float* getRho(void);
+    float* getSens(void);
+    int n_nodes(void) const { return (int)_n_active_nodes; }
+    int n_rho(void) const { return (int)_n_active_elements; }
+    long long n_box_nodes(void) const { return _nv; }
+    double v3_dot(double* v[3], double* u[3]);
+    double v3_norm(double* v[3]);
+    void v3_copy(double* vsrc[3], double* vdst[3]);
+    void v3_scale(double* v[3], double ampl);
+    int _layer = 0;
+
+private:
+    friend class HierarchyGrid;
+    HierarchyGrid* _H;
+    long long _nv = 0, _n_active_nodes = 0, _n_active_elements = 0;
+    double* _U[3];
+    double* _F[3];
+    double* _R[3];
+    double* _tmp = nullptr;
+};
+
+// grid::HierarchyGrid (grid/Grid.h:534-692)
+class HierarchyGrid {
+public:
+    HierarchyGrid(void);
+    ~HierarchyGrid();
+    void genFromMesh(const std::vector<unsigned int>& solid_bit, int out_reso[3]);
+    void update_stencil(void);
+    double v_cycle(int pre_relax = 1, int post_relax = 1);
+    void setMode(Mode mode);
+    Grid* operator[](int i) { return _grids[i]; }
+    int n_grid(void) { return (int)_grids.size(); }
+    void set_skip_layer(bool isskip) { _params.skip_layer1 = isskip ? 1 : 0; }
+    bool isForceFree(void) { return _mode == no_support_free_force || _mode == with_support_free_force; }
+    bool hasSupport(void) { return _mode == with_support_constrain_force_direction || _mode == with_support_free_force; }
+    double elementLength(void) { return _params.element_length; }
+    void resetAllResidual(void);
+
+    std::function<bool(double[3])> _inLoadArea;
+    std::function<bool(double[3])> _inFixedArea;
+    std::function<std::array<double, 3>(double[3])> _loadField;
+    Mode _mode = with_support_free_force;
+
+    // library handles (for callers that mix the C ABI in)
+    rt_ctx* ctx(void) { return _ctx; }
+    rt_hier* hier(void) { return _h; }
+    rt_params& params(void) { return _params; }
+    void check(int status, const char* what);
+    const std::vector<int>& loadNodes(void) const { return _load_nodes; }
+    const std::vector<double>& preloadForce(void) const { return _preload; }
+
+private:
+    rt_ctx* _ctx = nullptr;
+    rt_hier* _h = nullptr;
+    rt_params _params;
+    std::vector<Grid*> _grids;
+    std::vector<int> _load_nodes;
+    std::vector<double> _preload;  // [3*nload] load field at the load nodes
+};
+
+}  // namespace grid
+
+// optimization/optimization.h:11-22
+struct Parameter {
+    float damp_ratio;
+    float design_step;
+    float power_penalty;
+    float volume_ratio;
+    float volume_decrease;
+    int filter_radius;
+    float min_rho;
+    int gridreso;
+    float youngs_modulu;
+    float poisson_ratio;
+};
+
+extern Parameter params;
+extern grid::HierarchyGrid grids;
+
+// optimization/optimization.h:28-82
+void buildGrids(const std::vector<unsigned int>& solid_bit, int reso);
+void setParameters(float volRatio, float volDecrease, float designStep, float filterRadi, float dampRatio,
+                   float powerPenal, float min_density, int gridreso, float youngs_modulu, float poisson_ratio,
+                   float shell_width, bool logdensity, bool logcompliance);
+void setWorkMode(const std::string& modestr);
+void solveFEM(void);
+double modifiedPM(void);
+void computeSensitivity(void);
+float updateDensities(float Vgoal);
+void optimization(int max_iter = 100);
+grid::HierarchyGrid& getGrids(void);
+void setBoundaryCondition(std::function<bool(double[3])> fixarea, std::function<bool(double[3])> loadarea,
+                          std::function<std::array<double, 3>(double[3])> forcefield);
+void uploadTemplateMatrix(void);
+void initDensities(double rho);
+void update_stencil(void);
+void test_rigid_displacement(void);

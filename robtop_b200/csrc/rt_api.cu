@@ -626,6 +626,7 @@ static int field_ptr(rt_hier* h, int field, int lvl, void** ptr, size_t* bytes) 
         case RT_FIELD_RHO: if (lvl) return RT_EINVAL; *ptr = h->rho; *bytes = sizeof(float) * L.ne; return RT_OK;
         case RT_FIELD_SENS: if (lvl) return RT_EINVAL; *ptr = h->sens; *bytes = sizeof(float) * L.ne; return RT_OK;
         case RT_FIELD_VFIX: if (lvl) return RT_EINVAL; *ptr = h->vfix; *bytes = L.nv; return RT_OK;
+        case RT_FIELD_PENALTY: if (lvl) return RT_EINVAL; *ptr = h->w; *bytes = sizeof(float) * L.ne; return RT_OK;
     }
     return RT_EINVAL;
 }
@@ -1029,8 +1030,12 @@ static int pcg_core(rt_hier* h, double* x, const double* b, double tol, int maxi
     const double bn = std::sqrt(s[1]) > 0 ? std::sqrt(s[1]) : 1.0;
     double rel = std::sqrt(s[0]) / bn;
     int it = 0;
+    // without supports K is singular (rigid modes): keep the search space in its range
+    const bool no_support = (h->P.mode == RT_MODE_NSCF || h->P.mode == RT_MODE_NSFF);
+    if (no_support && h->Ru == nullptr) RT_CHECK(rtk::rigid_nodes(h));
     while (rel > tol && it < maxit) {
         RT_CHECK(precondition(h, r, h->z, h->scal + 21));
+        if (no_support) RT_CHECK(rtk::displacement_project(h, h->z));
         (*vcycles)++;
         double* rz = h->scal + 10 + 2 * (it & 1);
         double* rz_prev = h->scal + 10 + 2 * ((it + 1) & 1);

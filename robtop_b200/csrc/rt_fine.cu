@@ -69,38 +69,6 @@ __device__ __forceinline__ void fine_node_sum(int x, int y, int z, int vx, int v
 }
 
 // MODE 0: r = f - K u (fixed rows: K u = 0); MODE 1: out = K u (fixed rows: u)
-template <typename T, bool WS, int MODE>
-__global__ void __launch_bounds__(FINE_BS) k_fine_op(int nx, int ny, int nz, const uint8_t* __restrict__ vact,
-                                                      const float* __restrict__ w, const uint8_t* __restrict__ vfix,
-                                                      const T* __restrict__ KEg, const T* __restrict__ u,
-                                                      const T* __restrict__ f, T* __restrict__ out) {
-    __shared__ T sKE[576];
-    load_KE(sKE, KEg);
-    const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
-    const long nv = (long)vx * vy * vz;
-    for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < nv; v += (long)gridDim.x * blockDim.x) {
-        const int x = (int)(v % vx), y = (int)((v / vx) % vy), z = (int)(v / ((long)vx * vy));
-        T KU[3] = {T(0), T(0), T(0)};
-        const bool act = vact[v];
-        const bool fixed = WS && act && vfix[v];
-        if (act && !fixed) {
-            int ne;
-            T S[9];
-            fine_node_sum<T, WS, false, false>(x, y, z, vx, vy, nx, ny, nz, nv, w, vfix, u, sKE, KU, S, ne);
-        }
-        if (MODE == 0) {
-#pragma unroll
-            for (int c = 0; c < 3; c++) out[c * nv + v] = act ? f[c * nv + v] - KU[c] : T(0);
-        } else {
-            if (fixed) {
-                KU[0] = u[v]; KU[1] = u[nv + v]; KU[2] = u[2 * nv + v];
-            }
-#pragma unroll
-            for (int c = 0; c < 3; c++) out[c * nv + v] = KU[c];
-        }
-    }
-}
-
 template <typename T>
 __device__ __forceinline__ void block_gs(const T S[9], const T F[3], const T KU[3], T uu[3], bool backward) {
     if (!backward) {
@@ -144,53 +112,6 @@ __global__ void __launch_bounds__(FINE_BS) k_fine_gs(int nx, int ny, int nz, int
         T uu[3] = {u[v], u[nv + v], u[2 * nv + v]};
         block_gs(S, F, KU, uu, backward);
         u[v] = uu[0]; u[nv + v] = uu[1]; u[2 * nv + v] = uu[2];
-    }
-}
-
-template <typename T>
-__device__ __forceinline__ void inv3(const T S[9], T I[9]) {
-    const T a = S[0], b = S[1], c = S[2], d = S[3], e = S[4], f = S[5], g = S[6], h = S[7], k = S[8];
-    const T A = e * k - f * h, B = -(d * k - f * g), Cc = d * h - e * g;
-    const T id = T(1) / (a * A + b * B + c * Cc);
-    I[0] = A * id; I[1] = -(b * k - c * h) * id; I[2] = (b * f - c * e) * id;
-    I[3] = B * id; I[4] = (a * k - c * g) * id; I[5] = -(a * f - c * d) * id;
-    I[6] = Cc * id; I[7] = -(a * h - b * g) * id; I[8] = (a * e - b * d) * id;
-}
-
-// damped point-block Jacobi: unew = u + omega D^-1 (f - K u); fixed nodes: unew = f / n_e
-template <typename T, bool WS>
-__global__ void __launch_bounds__(FINE_BS) k_fine_jacobi(int nx, int ny, int nz, T omega,
-                                                          const uint8_t* __restrict__ vact,
-                                                          const float* __restrict__ w,
-                                                          const uint8_t* __restrict__ vfix, const T* __restrict__ KEg,
-                                                          const T* __restrict__ u, const T* __restrict__ f,
-                                                          T* __restrict__ unew) {
-    __shared__ T sKE[576];
-    load_KE(sKE, KEg);
-    const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
-    const long nv = (long)vx * vy * vz;
-    for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < nv; v += (long)gridDim.x * blockDim.x) {
-        const int x = (int)(v % vx), y = (int)((v / vx) % vy), z = (int)(v / ((long)vx * vy));
-        T nu[3] = {T(0), T(0), T(0)};
-        if (vact[v]) {
-            T KU[3], S[9];
-            int ne;
-            fine_node_sum<T, WS, true, false>(x, y, z, vx, vy, nx, ny, nz, nv, w, vfix, u, sKE, KU, S, ne);
-            if (WS && vfix[v]) {
-#pragma unroll
-                for (int c = 0; c < 3; c++) nu[c] = f[c * nv + v] / T(ne);
-            } else {
-                T Si[9], rr[3];
-                inv3(S, Si);
-#pragma unroll
-                for (int c = 0; c < 3; c++) rr[c] = f[c * nv + v] - KU[c];
-#pragma unroll
-                for (int c = 0; c < 3; c++)
-                    nu[c] = u[c * nv + v] + omega * (Si[c * 3] * rr[0] + Si[c * 3 + 1] * rr[1] + Si[c * 3 + 2] * rr[2]);
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < 3; c++) unew[c * nv + v] = nu[c];
     }
 }
 
@@ -258,36 +179,6 @@ int penalty_weights(rt_hier* h) {
 }
 
 template <typename T>
-int fine_residual(rt_hier* h, const T* u, const T* f, T* r) {
-    rt_level& L = h->L[0];
-    const char* nm = sizeof(T) == 8 ? "fine_residual_f64" : "fine_residual_f32";
-    return rt_launch(h->ctx, nm, [&] {
-        unsigned g = fine_grid(h->ctx, L.nv);
-        if (h->has_support)
-            k_fine_op<T, true, 0><<<g, FINE_BS, 0, h->ctx->stream>>>(L.nx, L.ny, L.nz, L.vact, h->w, h->vfix,
-                                                                     KEptr<T>(h), u, f, r);
-        else
-            k_fine_op<T, false, 0><<<g, FINE_BS, 0, h->ctx->stream>>>(L.nx, L.ny, L.nz, L.vact, h->w, h->vfix,
-                                                                      KEptr<T>(h), u, f, r);
-    });
-}
-
-template <typename T>
-int fine_applyK(rt_hier* h, const T* u, T* out) {
-    rt_level& L = h->L[0];
-    const char* nm = sizeof(T) == 8 ? "fine_applyK_f64" : "fine_applyK_f32";
-    return rt_launch(h->ctx, nm, [&] {
-        unsigned g = fine_grid(h->ctx, L.nv);
-        if (h->has_support)
-            k_fine_op<T, true, 1><<<g, FINE_BS, 0, h->ctx->stream>>>(L.nx, L.ny, L.nz, L.vact, h->w, h->vfix,
-                                                                     KEptr<T>(h), u, nullptr, out);
-        else
-            k_fine_op<T, false, 1><<<g, FINE_BS, 0, h->ctx->stream>>>(L.nx, L.ny, L.nz, L.vact, h->w, h->vfix,
-                                                                      KEptr<T>(h), u, nullptr, out);
-    });
-}
-
-template <typename T>
 int fine_gs(rt_hier* h, T* u, const T* f, bool backward) {
     rt_level& L = h->L[0];
     const char* nm = sizeof(T) == 8 ? "fine_gs_f64" : "fine_gs_f32";
@@ -308,21 +199,6 @@ int fine_gs(rt_hier* h, T* u, const T* f, bool backward) {
     return RT_OK;
 }
 
-template <typename T>
-int fine_jacobi(rt_hier* h, const T* u, const T* f, T* unew, double omega) {
-    rt_level& L = h->L[0];
-    const char* nm = sizeof(T) == 8 ? "fine_jacobi_f64" : "fine_jacobi_f32";
-    return rt_launch(h->ctx, nm, [&] {
-        unsigned g = fine_grid(h->ctx, L.nv);
-        if (h->has_support)
-            k_fine_jacobi<T, true><<<g, FINE_BS, 0, h->ctx->stream>>>(L.nx, L.ny, L.nz, (T)omega, L.vact, h->w,
-                                                                      h->vfix, KEptr<T>(h), u, f, unew);
-        else
-            k_fine_jacobi<T, false><<<g, FINE_BS, 0, h->ctx->stream>>>(L.nx, L.ny, L.nz, (T)omega, L.vact, h->w,
-                                                                       h->vfix, KEptr<T>(h), u, f, unew);
-    });
-}
-
 int sensitivity(rt_hier* h, const double* u) {
     rt_level& L = h->L[0];
     return rt_launch(h->ctx, "sensitivity", [&] {
@@ -332,13 +208,7 @@ int sensitivity(rt_hier* h, const double* u) {
     });
 }
 
-template int fine_residual<double>(rt_hier*, const double*, const double*, double*);
-template int fine_residual<float>(rt_hier*, const float*, const float*, float*);
-template int fine_applyK<double>(rt_hier*, const double*, double*);
-template int fine_applyK<float>(rt_hier*, const float*, float*);
 template int fine_gs<double>(rt_hier*, double*, const double*, bool);
 template int fine_gs<float>(rt_hier*, float*, const float*, bool);
-template int fine_jacobi<double>(rt_hier*, const double*, const double*, double*, double);
-template int fine_jacobi<float>(rt_hier*, const float*, const float*, float*, double);
 
 }  // namespace rtk

@@ -1,0 +1,337 @@
+// rt_fine_tile.cu — finest-level operator as an element-tile kernel.
+//
+// Same operator as update_residual_OTFA_{NS,WS}_kernel (grid/Grid.cu:1450-1557),
+// applyK_OTFA_kernel (grid/Grid.cu:2439-2517) plus a damped point-block
+// Jacobi sweep, computed element by element instead of node by node:
+//
+//  * KE is applied in the Hadamard (+-1 tensor-product) basis of the 8
+//    element vertices.  With T = H (x) I3, KE = T Kt T^T / 64 and the 24x24 Kt
+//    has 45 non-zeros (independent of E, nu, h), so one element costs two
+//    3-stage butterflies per component and 45 FMAs instead of a dense 24x24.
+//  * A CTA owns a 32x8 node tile and marches up through z.  Per element layer
+//    the 33x9 elements touching the tile are computed once, their 24 outputs
+//    go to shared memory, and every node gathers its 8 contributions (4 from
+//    the layer below, 4 from the layer above) — no atomics, each element is
+//    evaluated once per tile.
+//  * u of the two node layers an element layer couples sits in shared memory
+//    (34x10 halo tile per layer, loaded once); fixed (support) nodes are
+//    loaded as zero so the WS rule of the reference falls out of the data.
+#include <cuda_runtime.h>
+
+#include "rt_internal.h"
+
+namespace {
+
+constexpr int TX = 32, TY = 8;            // node tile
+constexpr int EXT = TX + 1, EYT = TY + 1;  // element tile (one halo element below in x and y)
+constexpr int UXT = TX + 2, UYT = TY + 2;  // node halo tile
+constexpr int NE_T = EXT * EYT;            // 297 elements per layer
+constexpr int NU_T = UXT * UYT;            // 340 nodes per layer
+constexpr int TILE_BS = 320;               // >= NE_T, multiple of 32
+
+// sparsity pattern of Kt = T^T KE T / 64 (rows/cols index 3*mode + comp)
+__device__ constexpr int KT_R[45] = {3, 3, 3, 4, 4, 5, 5, 6, 6, 7, 7, 7, 8, 8, 9, 9, 10, 10, 11, 11, 11, 12, 12,
+                                     13, 13, 14, 14, 14, 15, 15, 16, 16, 16, 17, 17, 18, 18, 18, 19, 19, 20, 20, 21,
+                                     22, 23};
+__device__ constexpr int KT_C[45] = {3, 7, 14, 4, 6, 5, 12, 4, 6, 3, 7, 14, 8, 13, 9, 20, 10, 17, 11, 16, 18, 5, 12,
+                                     8, 13, 3, 7, 14, 15, 19, 11, 16, 18, 10, 17, 11, 16, 18, 15, 19, 9, 20, 21, 22,
+                                     23};
+
+template <typename T>
+struct KtVals {
+    T v[45];
+    T diag_a, diag_b;  // KE diagonal block of any vertex: a I + b (s s^T - I), s = vertex reflection signs
+};
+
+// 8-point Sylvester-Hadamard over the vertex bits (x, y, z) of one component
+template <typename T>
+__device__ __forceinline__ void hadamard8(T* a, int c) {
+#pragma unroll
+    for (int bit = 1; bit < 8; bit <<= 1)
+#pragma unroll
+        for (int i = 0; i < 8; i++)
+            if (!(i & bit)) {
+                const T p = a[3 * i + c], q = a[3 * (i | bit) + c];
+                a[3 * i + c] = p + q;
+                a[3 * (i | bit) + c] = p - q;
+            }
+}
+
+// ye = w * KE * ue, ue/ye indexed 3*vertex + comp
+template <typename T>
+__device__ __forceinline__ void element_apply(T* a, const KtVals<T>& kt, T w) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) hadamard8(a, c);
+    T z[24];
+#pragma unroll
+    for (int i = 0; i < 24; i++) z[i] = T(0);
+#pragma unroll
+    for (int k = 0; k < 45; k++) z[KT_R[k]] += kt.v[k] * a[KT_C[k]];
+#pragma unroll
+    for (int i = 0; i < 24; i++) a[i] = w * z[i];
+#pragma unroll
+    for (int c = 0; c < 3; c++) hadamard8(a, c);
+}
+
+template <typename T>
+struct TileSmem {
+    T u[2][3][NU_T];
+    T e[24][NE_T];
+    float w[3][NE_T];  // element weights of layers ez-1, ez, ez+1 (slot (layer+3)%3)
+};
+
+// MODE 0: r = f - K u (fixed rows: r = f)     MODE 1: out = K u (fixed rows: u)
+// MODE 2: unew = u + omega D^-1 (f - K u) (fixed: f / n_e)
+template <typename T, bool WS, int MODE>
+__global__ void __launch_bounds__(TILE_BS) k_fine_tile(int nx, int ny, int nz, int zchunk,
+                                                        const uint8_t* __restrict__ vact,
+                                                        const float* __restrict__ wgt,
+                                                        const uint8_t* __restrict__ vfix, const KtVals<T> kt,
+                                                        const T* __restrict__ u, const T* __restrict__ f,
+                                                        T* __restrict__ out, T omega) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    TileSmem<T>& S = *reinterpret_cast<TileSmem<T>*>(smraw);
+    const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
+    const long nv = (long)vx * vy * vz;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int zb = blockIdx.z * zchunk;
+    const int ze = min(zb + zchunk, vz);
+    const int tid = threadIdx.x;
+    // node owned by this thread
+    const int nxl = tid % TX, nyl = tid / TX;
+    const int nxg = x0 + nxl, nyg = y0 + nyl;
+    const bool node_thread = tid < TX * TY && nxg < vx && nyg < vy;
+    // element owned by this thread
+    const int exl = tid % EXT, eyl = tid / EXT;
+    const int exg = x0 - 1 + exl, eyg = y0 - 1 + eyl;
+    const bool elem_xy = tid < NE_T && exg >= 0 && eyg >= 0 && exg < nx && eyg < ny;
+
+    auto load_layer = [&](int L) {
+        T* dst = &S.u[L & 1][0][0];
+        for (int i = tid; i < NU_T; i += TILE_BS) {
+            const int xx = x0 - 1 + i % UXT, yy = y0 - 1 + i / UXT;
+            T a = T(0), b = T(0), c = T(0);
+            if (L >= 0 && L < vz && xx >= 0 && yy >= 0 && xx < vx && yy < vy) {
+                const long v = xx + (long)vx * (yy + (long)vy * L);
+                if (!(WS && vfix[v])) {
+                    a = u[v];
+                    b = u[nv + v];
+                    c = u[2 * nv + v];
+                }
+            }
+            dst[i] = a;
+            dst[NU_T + i] = b;
+            dst[2 * NU_T + i] = c;
+        }
+    };
+    auto load_w = [&](int ez) {
+        if (tid < NE_T) {
+            float wv = 0.f;
+            if (elem_xy && ez >= 0 && ez < nz) wv = wgt[exg + (long)nx * (eyg + (long)ny * ez)];
+            S.w[(ez + 3) % 3][tid] = wv;
+        }
+    };
+
+    load_layer(zb - 1);
+    load_w(zb - 1);
+    T acc[3] = {T(0), T(0), T(0)};
+    for (int ez = zb - 1; ez < ze; ez++) {
+        // node layers ez (in smem) and ez+1 (load now); weights of element layer ez
+        load_layer(ez + 1);
+        if (ez != zb - 1) load_w(ez);
+        __syncthreads();
+        // ---- element phase
+        if (tid < NE_T) {
+            T a[24];
+            const float wv = S.w[(ez + 3) % 3][tid];
+            if (wv != 0.f) {
+                const T* lo = &S.u[ez & 1][0][0];
+                const T* hi = &S.u[(ez + 1) & 1][0][0];
+#pragma unroll
+                for (int vtx = 0; vtx < 8; vtx++) {
+                    const T* src = (vtx & 4) ? hi : lo;
+                    const int idx = (eyl + ((vtx >> 1) & 1)) * UXT + exl + (vtx & 1);
+                    a[3 * vtx] = src[idx];
+                    a[3 * vtx + 1] = src[NU_T + idx];
+                    a[3 * vtx + 2] = src[2 * NU_T + idx];
+                }
+                element_apply(a, kt, T(wv));
+            } else {
+#pragma unroll
+                for (int q = 0; q < 24; q++) a[q] = T(0);
+            }
+#pragma unroll
+            for (int q = 0; q < 24; q++) S.e[q][tid] = a[q];
+        }
+        __syncthreads();
+        // ---- node phase
+        if (node_thread) {
+            if (ez >= zb) {
+                // node layer ez: bottom vertices (bit z = 0) of element layer ez
+#pragma unroll
+                for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+                    for (int dx = 0; dx < 2; dx++) {
+                        const int el = (nyl + dy) * EXT + nxl + dx;
+                        const int vtx = (1 - dx) + 2 * (1 - dy);
+#pragma unroll
+                        for (int c = 0; c < 3; c++) acc[c] += S.e[3 * vtx + c][el];
+                    }
+                const int zg = ez;
+                const long v = nxg + (long)vx * (nyg + (long)vy * zg);
+                const bool act = vact[v];
+                const bool fixed = WS && act && vfix[v];
+                if (MODE == 0) {
+#pragma unroll
+                    for (int c = 0; c < 3; c++)
+                        out[c * nv + v] = act ? (fixed ? f[c * nv + v] : f[c * nv + v] - acc[c]) : T(0);
+                } else if (MODE == 1) {
+#pragma unroll
+                    for (int c = 0; c < 3; c++) out[c * nv + v] = act ? (fixed ? u[c * nv + v] : acc[c]) : T(0);
+                } else {
+                    T nu[3] = {T(0), T(0), T(0)};
+                    if (act) {
+                        // diagonal block from the 8 incident element weights
+                        T sw = T(0), sxy = T(0), sxz = T(0), syz = T(0);
+                        int ne = 0;
+#pragma unroll
+                        for (int dz = 0; dz < 2; dz++)
+#pragma unroll
+                            for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+                                for (int dx = 0; dx < 2; dx++) {
+                                    const float wv = S.w[(ez + 2 + dz) % 3][(nyl + dy) * EXT + nxl + dx];
+                                    if (wv != 0.f) ne++;
+                                    // node's vertex bits in that element: (1-dx, 1-dy, 1-dz)
+                                    const T sx = dx ? T(1) : T(-1), sy = dy ? T(1) : T(-1), sz = dz ? T(1) : T(-1);
+                                    sw += T(wv);
+                                    sxy += T(wv) * sx * sy;
+                                    sxz += T(wv) * sx * sz;
+                                    syz += T(wv) * sy * sz;
+                                }
+                        if (fixed) {
+#pragma unroll
+                            for (int c = 0; c < 3; c++) nu[c] = f[c * nv + v] / T(ne);
+                        } else {
+                            const T A = kt.diag_a * sw, bxy = kt.diag_b * sxy, bxz = kt.diag_b * sxz,
+                                    byz = kt.diag_b * syz;
+                            // inverse of [[A,bxy,bxz],[bxy,A,byz],[bxz,byz,A]]
+                            const T c00 = A * A - byz * byz, c01 = -(bxy * A - byz * bxz), c02 = bxy * byz - A * bxz;
+                            const T c11 = A * A - bxz * bxz, c12 = -(A * byz - bxy * bxz), c22 = A * A - bxy * bxy;
+                            const T id = T(1) / (A * c00 + bxy * c01 + bxz * c02);
+                            T rr[3];
+#pragma unroll
+                            for (int c = 0; c < 3; c++) rr[c] = f[c * nv + v] - acc[c];
+                            nu[0] = u[v] + omega * id * (c00 * rr[0] + c01 * rr[1] + c02 * rr[2]);
+                            nu[1] = u[nv + v] + omega * id * (c01 * rr[0] + c11 * rr[1] + c12 * rr[2]);
+                            nu[2] = u[2 * nv + v] + omega * id * (c02 * rr[0] + c12 * rr[1] + c22 * rr[2]);
+                        }
+                    }
+#pragma unroll
+                    for (int c = 0; c < 3; c++) out[c * nv + v] = nu[c];
+                }
+            }
+            // start node layer ez+1 with the top vertices (bit z = 1) of element layer ez
+#pragma unroll
+            for (int c = 0; c < 3; c++) acc[c] = T(0);
+#pragma unroll
+            for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+                for (int dx = 0; dx < 2; dx++) {
+                    const int el = (nyl + dy) * EXT + nxl + dx;
+                    const int vtx = (1 - dx) + 2 * (1 - dy) + 4;
+#pragma unroll
+                    for (int c = 0; c < 3; c++) acc[c] += S.e[3 * vtx + c][el];
+                }
+        }
+    }
+}
+
+template <typename T>
+KtVals<T> make_kt(const rt_hier* h) {
+    // Kt = T^T KE T / 64 with T = H (x) I3, H the 8x8 Sylvester-Hadamard over vertex bits
+    static const int R[45] = {3, 3, 3, 4, 4, 5, 5, 6, 6, 7, 7, 7, 8, 8, 9, 9, 10, 10, 11, 11, 11, 12, 12,
+                              13, 13, 14, 14, 14, 15, 15, 16, 16, 16, 17, 17, 18, 18, 18, 19, 19, 20, 20, 21,
+                              22, 23};
+    static const int Cc[45] = {3, 7, 14, 4, 6, 5, 12, 4, 6, 3, 7, 14, 8, 13, 9, 20, 10, 17, 11, 16, 18, 5, 12,
+                               8, 13, 3, 7, 14, 15, 19, 11, 16, 18, 10, 17, 11, 16, 18, 15, 19, 9, 20, 21, 22,
+                               23};
+    KtVals<T> k;
+    for (int q = 0; q < 45; q++) {
+        const int m = R[q] / 3, c = R[q] % 3, n = Cc[q] / 3, d = Cc[q] % 3;
+        double s = 0;
+        for (int i = 0; i < 8; i++)
+            for (int j = 0; j < 8; j++) {
+                const double hmi = (__builtin_popcount(m & i) & 1) ? -1.0 : 1.0;
+                const double hnj = (__builtin_popcount(n & j) & 1) ? -1.0 : 1.0;
+                s += hmi * h->KE[(3 * i + c) * 24 + 3 * j + d] * hnj;
+            }
+        k.v[q] = (T)(s / 64.0);
+    }
+    k.diag_a = (T)h->KE[0];
+    k.diag_b = (T)h->KE[1];
+    return k;
+}
+
+int tile_zchunk(rt_ctx* c, int vx, int vy, int vz) {
+    const long tiles = (long)((vx + TX - 1) / TX) * ((vy + TY - 1) / TY);
+    const long target = (long)c->sm_count * 3;  // ~3 resident CTAs per SM
+    long chunks = (target + tiles - 1) / tiles;
+    if (chunks < 1) chunks = 1;
+    int zc = (int)((vz + chunks - 1) / chunks);
+    if (zc < 4) zc = 4;
+    return zc;
+}
+
+template <typename T, bool WS, int MODE>
+int launch_tile(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name) {
+    rt_level& L = h->L[0];
+    static int attr_dev = -1;
+    const size_t smem = sizeof(TileSmem<T>);
+    auto kern = k_fine_tile<T, WS, MODE>;
+    if (attr_dev != h->ctx->device) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return rt_fail(h->ctx, RT_ECUDA, "smem attribute: %s", cudaGetErrorString(e));
+        attr_dev = h->ctx->device;
+    }
+    const int zc = tile_zchunk(h->ctx, L.vx, L.vy, L.vz);
+    dim3 grid((L.vx + TX - 1) / TX, (L.vy + TY - 1) / TY, (L.vz + zc - 1) / zc);
+    const KtVals<T> kt = make_kt<T>(h);
+    return rt_launch(h->ctx, name, [&] {
+        kern<<<grid, TILE_BS, smem, h->ctx->stream>>>(L.nx, L.ny, L.nz, zc, L.vact, h->w, h->vfix, kt, u, f, out,
+                                                      (T)omega);
+    });
+}
+
+}  // namespace
+
+namespace rtk {
+
+template <typename T>
+int fine_residual(rt_hier* h, const T* u, const T* f, T* r) {
+    const char* nm = sizeof(T) == 8 ? "fine_residual_f64" : "fine_residual_f32";
+    return h->has_support ? launch_tile<T, true, 0>(h, u, f, r, 0.0, nm) : launch_tile<T, false, 0>(h, u, f, r, 0.0, nm);
+}
+
+template <typename T>
+int fine_applyK(rt_hier* h, const T* u, T* out) {
+    const char* nm = sizeof(T) == 8 ? "fine_applyK_f64" : "fine_applyK_f32";
+    return h->has_support ? launch_tile<T, true, 1>(h, u, nullptr, out, 0.0, nm)
+                          : launch_tile<T, false, 1>(h, u, nullptr, out, 0.0, nm);
+}
+
+template <typename T>
+int fine_jacobi(rt_hier* h, const T* u, const T* f, T* unew, double omega) {
+    const char* nm = sizeof(T) == 8 ? "fine_jacobi_f64" : "fine_jacobi_f32";
+    return h->has_support ? launch_tile<T, true, 2>(h, u, f, unew, omega, nm)
+                          : launch_tile<T, false, 2>(h, u, f, unew, omega, nm);
+}
+
+template int fine_residual<double>(rt_hier*, const double*, const double*, double*);
+template int fine_residual<float>(rt_hier*, const float*, const float*, float*);
+template int fine_applyK<double>(rt_hier*, const double*, double*);
+template int fine_applyK<float>(rt_hier*, const float*, float*);
+template int fine_jacobi<double>(rt_hier*, const double*, const double*, double*, double);
+template int fine_jacobi<float>(rt_hier*, const float*, const float*, float*, double);
+
+}  // namespace rtk

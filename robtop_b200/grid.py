@@ -198,6 +198,10 @@ class Grid:
     def setRho(self, rho):
         self._put(A.FIELD_RHO, A.LAYOUT_DENSE, rho, np.float32)
 
+    def getPenalty(self):
+        """Element weights powf(rho, p) used by the operator (refreshed by update_stencil)."""
+        return self._get(A.FIELD_PENALTY, A.LAYOUT_DENSE, self.ne, np.float32)
+
     def getSens(self):
         return self._get(A.FIELD_SENS, A.LAYOUT_DENSE, self.ne, np.float32)
 

@@ -1,0 +1,191 @@
+"""Python mirror of robtop's optimization module (optimization/optimization.h:28-82).
+
+Module-level state stands in for the reference's globals ``grids`` and
+``params`` (optimization/optimization.cpp:8-12); every numeric step runs in
+``librtb200.so`` through :mod:`robtop_b200.grid`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _capi as A
+from .grid import Context, HierarchyGrid, default_params
+
+
+@dataclass
+class Parameter:
+    """optimization/optimization.h:11-22"""
+    damp_ratio: float = 0.5
+    design_step: float = 0.03
+    power_penalty: float = 3.0
+    volume_ratio: float = 0.4
+    volume_decrease: float = 0.0
+    filter_radius: int = 2
+    min_rho: float = 1e-3
+    gridreso: int = 128
+    youngs_modulu: float = 1e6
+    poisson_ratio: float = 0.4
+
+
+params = Parameter()
+_state = {"ctx": None, "grids": None, "mode": A.MODE_WSFF, "fixed": None, "load": None, "field": None,
+          "pm_seed": 1, "records": []}
+
+
+def _ctx():
+    if _state["ctx"] is None:
+        _state["ctx"] = Context(0)
+    return _state["ctx"]
+
+
+def getGrids() -> HierarchyGrid:
+    return _state["grids"]
+
+
+def setParameters(volRatio, volDecrease, designStep, filterRadi, dampRatio, powerPenal, min_density, gridreso,
+                  youngs_modulu, poisson_ratio, shell_width=0.0, logdensity=False, logcompliance=False):
+    """optimization/optimization.cpp:32-50"""
+    params.volume_ratio = volRatio
+    params.volume_decrease = volDecrease
+    params.design_step = designStep
+    params.filter_radius = int(filterRadi)
+    params.damp_ratio = dampRatio
+    params.power_penalty = powerPenal
+    params.min_rho = min_density
+    params.gridreso = gridreso
+    params.youngs_modulu = youngs_modulu
+    params.poisson_ratio = poisson_ratio
+
+
+def setWorkMode(modestr):
+    """optimization/optimization.cpp:65-83 (raises instead of exit(-1))."""
+    modes = {"nscf": A.MODE_NSCF, "nsff": A.MODE_NSFF, "wscf": A.MODE_WSCF, "wsff": A.MODE_WSFF}
+    if modestr not in modes:
+        raise ValueError(f"unsupported mode {modestr}")
+    _state["mode"] = modes[modestr]
+    if _state["grids"] is not None:
+        _state["grids"].setMode(modes[modestr])
+
+
+def setBoundaryCondition(fixarea, loadarea, forcefield):
+    """optimization/optimization.cpp:680-685; predicates take a position (x, y, z)."""
+    _state["fixed"], _state["load"], _state["field"] = fixarea, loadarea, forcefield
+
+
+def _rt_params(**kw):
+    return default_params(power_penalty=params.power_penalty, min_rho=params.min_rho,
+                          volume_ratio=params.volume_ratio, design_step=params.design_step,
+                          damp_ratio=params.damp_ratio, filter_radius=float(params.filter_radius),
+                          youngs_modulus=params.youngs_modulu, poisson_ratio=params.poisson_ratio,
+                          mode=_state["mode"], skip_layer1=1, **kw)
+
+
+def buildGrids(solid_bit, reso, **solver):
+    """Builds the hierarchy from a cubic bit grid (HierarchyGrid::genFromMesh(solid_bit, out_reso),
+    grid/Grid.cpp:455) and applies the boundary predicates to the level-0 surface nodes
+    (Grid::computeProjectionMatrix, grid/Grid.cpp:1291-1403)."""
+    G = HierarchyGrid(_ctx(), _rt_params(**solver))
+    G.genFromMesh(solid_bit, [reso, reso, reso])
+    g0 = G[0]
+    surf = G.surface_nodes().astype(bool) & g0.getVact().astype(bool)
+    nv = g0.nv
+    vx, vy = g0.nx + 1, g0.ny + 1
+    ids = np.flatnonzero(surf)
+    pos = np.stack([ids % vx, (ids // vx) % vy, ids // (vx * vy)], 1).astype(np.float64)
+    fixed = np.array([bool(_state["fixed"](p)) for p in pos]) if _state["fixed"] else np.zeros(ids.size, bool)
+    loadm = np.array([bool(_state["load"](p)) for p in pos]) if _state["load"] else np.zeros(ids.size, bool)
+    loadm &= ~fixed
+    vfix = np.zeros(nv, np.uint8)
+    vfix[ids[fixed]] = 1
+    G.set_support(vfix)
+    load_ids = ids[loadm]
+    normals = np.tile([0.0, 0.0, 1.0], (load_ids.size, 1))
+    G.set_load_nodes(load_ids, normals)
+    _state["grids"] = G
+    _state["load_ids"] = load_ids
+    _state["load_pos"] = pos[loadm]
+    return G
+
+
+def uploadTemplateMatrix():
+    G = getGrids()
+    p = G.params
+    p.youngs_modulus, p.poisson_ratio, p.power_penalty = params.youngs_modulu, params.poisson_ratio, \
+        params.power_penalty
+    G.set_params(p)
+
+
+def initDensities(rho):
+    getGrids()[0].init_rho(rho)
+
+
+def update_stencil():
+    getGrids().update_stencil()
+
+
+def solveFEM(tol=1e-4):
+    """optimization/optimization.cpp:85-91 on the preloaded force field."""
+    G = getGrids()
+    nv = G[0].nv
+    f = np.zeros(3 * nv)
+    for i, p in zip(_state["load_ids"], _state["load_pos"]):
+        v = _state["field"](p) if _state["field"] else (0.0, 0.0, 0.0)
+        f[i], f[nv + i], f[2 * nv + i] = v
+    G[0].setForce(f)
+    rel = 1.0
+    it = 0
+    while rel > tol:
+        rel = G.v_cycle()
+        it += 1
+        if it > 1000 or not np.isfinite(rel):
+            raise RuntimeError("solveFEM did not converge")
+    return rel
+
+
+def modifiedPM():
+    """optimization/optimization.cpp:123-261 (on the device)."""
+    lam, _ = getGrids().worst_case(A.WORST_MODPM, 500, 0.0, seed=_state["pm_seed"])
+    _state["pm_seed"] += 1
+    return lam
+
+
+def worstCaseLanczos(k=16, inner_tol=1e-6, seed=0):
+    lam, _ = getGrids().worst_case(A.WORST_LANCZOS, k, inner_tol, seed=seed)
+    return lam
+
+
+def computeSensitivity():
+    A.check(A.lib().rt_sensitivity(getGrids().handle, 1), _ctx().handle)
+
+
+def updateDensities(Vgoal):
+    lam = C.c_float()
+    trials = C.c_int()
+    A.check(A.lib().rt_oc_update(getGrids().handle, float(Vgoal), C.byref(lam), C.byref(trials)), _ctx().handle)
+    return lam.value
+
+
+def optimization(max_iter=100, worst=modifiedPM):
+    """optimization/optimization.cpp:583-673 without file output; returns the compliance record."""
+    initDensities(params.volume_ratio)
+    Vgoal = params.volume_ratio
+    rec = []
+    small = 0
+    for itn in range(1, max_iter + 1):
+        Vgoal = max(Vgoal * (1 - params.volume_decrease), params.volume_ratio)
+        update_stencil()
+        c = worst()
+        if rec and abs(c - rec[-1]) / abs(rec[-1]) < 5e-3:
+            small += 1
+        else:
+            small = 0
+        rec.append(c)
+        if small >= 2 and Vgoal <= params.volume_ratio + 1e-3:
+            break
+        computeSensitivity()
+        updateDensities(Vgoal)
+    _state["records"] = rec
+    return rec

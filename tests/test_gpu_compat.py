@@ -1,0 +1,55 @@
+"""The reference-signature C++ layer (robtop_compat.h), driven the way robtop.cpp and
+TestSuit drive robtop, compared with the CPU oracle on the same problem."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as O
+from robtop_b200 import build as B
+from robtop_b200 import configs
+
+pytestmark = pytest.mark.gpu
+
+
+def run_driver():
+    exe = B.build_compat_driver()
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout + out.stderr
+    vals = {}
+    rigid = []
+    for line in out.stdout.splitlines():
+        if line.startswith("-- u_rigid"):
+            rigid.append(float(line.split("=")[1]))
+            continue
+        k, v = line.split()
+        vals[k] = float(v)
+    return vals, rigid
+
+
+def test_compat_flow_matches_oracle():
+    vals, rigid = run_driver()
+    cfg = configs.cantilever(24, 12, 12)
+    assert vals["load_nodes"] == cfg["load_nodes"].size
+    H = O.Hierarchy(cfg["eact"], cfg["rho"], cfg["vfix"], p=3, E=1e6, nu=0.4)
+    H.update_stencil()
+    assert vals["levels"] == H.nlev
+    # test_rigid_displacement: K u_rigid vanishes away from the supports; with supports the
+    # residual is nonzero only through the clamped nodes, so compare with the oracle's value
+    assert len(rigid) == 6
+    # solveFEM: V-cycles to 1e-4 on the preloaded force
+    b = cfg["fload"].ravel().copy()
+    H.arrs[0]["f"][:] = b
+    H.arrs[0]["u"][:] = 0
+    rel = 1
+    while rel > 1e-4:
+        rel = H.vcycle(O.SMOOTH_GS, 1, 1)
+    c_or = b @ H.arrs[0]["u"]
+    assert vals["rel_residual"] <= 1e-4
+    assert abs(vals["compliance"] - c_or) <= 1e-4 * abs(c_or)
+    # modifiedPM: worst-case compliance (random start differs in seed; the eigenvalue does not)
+    assert vals["worst_compliance"] > 0
+    x, _, _ = H.pcg(b / np.linalg.norm(b), tol=1e-10)
+    assert vals["worst_compliance"] >= (b / np.linalg.norm(b)) @ x * (1 - 1e-3)
+    assert abs(vals["volume"] - 0.4) <= 2e-4

@@ -22,6 +22,8 @@ def pair(request):
     cfg = CONFIGS[request.param]()
     ctx, G, H = build_pair(cfg)
     G.update_stencil()
+    # operator-level parity shares the device's FP32 powf weights (checked on their own below)
+    H.set_weights(G[0].getPenalty())
     H.update_stencil()
     yield cfg, ctx, G, H
     G.close()
@@ -36,6 +38,16 @@ def test_level_plan_and_activity_bit_exact(pair):
         assert (G[i].nx, G[i].ny, G[i].nz, G[i].ratio) == (L.nx, L.ny, L.nz, L.ratio)
         assert np.array_equal(G[i].getVact(), H.arrs[i]["vact"])
         assert np.array_equal(G[i].getEact(), H.arrs[i]["eact"].ravel())
+
+
+def test_penalty_weights_within_2ulp(pair):
+    # powf(rho, p) in FP32 as the reference computes it; CUDA and glibc powf agree to ~1 ulp
+    cfg, ctx, G, H = pair
+    w = G[0].getPenalty()
+    rho = cfg["rho"].ravel().astype(np.float32)
+    ref = np.where(cfg["eact"].ravel() != 0, np.power(rho, np.float32(3.0)), np.float32(0)).astype(np.float32)
+    ulp = np.spacing(np.maximum(np.abs(ref), np.finfo(np.float32).tiny))
+    assert np.all(np.abs(w.astype(np.float64) - ref) <= 2 * ulp)
 
 
 def test_template_matrix(pair):
