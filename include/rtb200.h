@@ -174,6 +174,20 @@ int rt_apply_K(rt_hier* h, const double* u, double* out);
 int rt_compliance(rt_hier* h, double* c);
 /* Grid::relative_residual (grid/Grid.cu:1946-1951) */
 int rt_relative_residual(rt_hier* h, double* rel);
+/* Compliance f.u of two caller-owned FP64 device vectors of length n, written to
+ * out_dev[0], without allocating any device memory: for callers that cannot call
+ * cudaMalloc (all device memory handed to their own pool, or no allocation
+ * allowed once their solve loop runs).  No counterpart in the reference.
+ * The scratch is a fixed 512 KiB device array inside the library (held by every
+ * GPU that loads it until exit); n must not exceed RT_NOALLOC_MAX_N, larger n is
+ * rejected with RT_EINVAL and a message on stderr.  The array's address is looked
+ * up on the first call per device (make that call before any stream capture).
+ * All calls share the array: calls that overlap on the GPU race.  Runs on
+ * cuda_stream (NULL: the legacy default stream) of the current device. */
+#define RT_NOALLOC_MAX_PARTIALS 65536
+#define RT_NOALLOC_MAX_N (65536LL * 4096LL)
+int rt_compliance_noalloc(const double* f_dev, const double* u_dev, long long n, double* out_dev,
+                          void* cuda_stream);
 
 /* ---- solvers -------------------------------------------------------------- */
 /* MG-preconditioned CG on level 0: u <- K^-1 f to ||r||/||f|| <= tol (solveFEM's role,

@@ -97,6 +97,7 @@ SIGNATURES = {
     "rt_apply_K": (I, [P, P, P]),
     "rt_compliance": (I, [P, C.POINTER(D)]),
     "rt_relative_residual": (I, [P, C.POINTER(D)]),
+    "rt_compliance_noalloc": (I, [P, P, C.c_longlong, P, P]),
     "rt_pcg": (I, [P, D, I, C.POINTER(SolveInfo)]),
     "rt_worst_case": (I, [P, I, I, D, C.c_uint64, C.POINTER(D), C.POINTER(SolveInfo)]),
     "rt_sensitivity": (I, [P, I]),
