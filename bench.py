@@ -33,6 +33,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = dict(nx=128, ny=128, nz=64, seed=0, k=16, tol=1e-6)
+# plain: the reference's V-cycle made symmetric (8-colour GS, forward pre / backward post), all FP64
+# mixed: FP32 V-cycle with Chebyshev(4) smoothing inside FP64 flexible CG
+FORMS = {"plain": dict(precision="FP64", smoother="SMOOTH_SGS", sweeps=1),
+         "mixed": dict(precision="FP32", smoother="SMOOTH_CHEBY", sweeps=4)}
 METRIC = "worst-case solve (Lanczos k=16, MG-PCG inner solves to rel. residual 1e-6) on 128x128x64"
 
 
@@ -281,6 +285,37 @@ def run_reference(args):
     return 0
 
 
+def run_kernel(args):
+    """Repeat one hot operator of the path on the bench workload (short command for
+    ncu captures): fine_residual = rt_update_residual(level 0), fine_jacobi =
+    rt_smooth(level 0, Jacobi), st_residual = rt_update_residual(level 1)."""
+    import robtop_b200 as rb
+    from robtop_b200 import configs
+
+    ctx = rb.Context(0)
+    cfg, G = build_problem(rb, configs, ctx, rb.FP64)
+    G.update_stencil()
+    u = np.random.default_rng(0).standard_normal(3 * G[0].nv) * np.tile(G[0].getVact(), 3)
+    G[0].setDisplacement(u)
+    G[0].setForce(u[::-1].copy())
+    ops = {"fine_residual": lambda: G[0].update_residual(),
+           "fine_jacobi": lambda: G[0].smooth(rb.SMOOTH_JACOBI, 1, 0.6),
+           "st_residual": lambda: G[1].update_residual()}
+    op = ops[args.kernel]
+    for _ in range(args.warmup):
+        op()
+    ctx.sync()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        op()
+    ctx.sync()
+    dt = (time.perf_counter() - t0) / args.steps
+    print(json.dumps({"kernel": args.kernel, "us_per_call": dt * 1e6, "nodes": G[0].nv}))
+    G.close()
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -288,9 +323,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel", default=None, choices=["fine_residual", "fine_jacobi", "st_residual"])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.kernel:
+        return run_kernel(args)
 
     import torch
 
@@ -317,8 +355,11 @@ def main():
     cfg, G = build_problem(rb, configs, ctx, rb.FP32)
     results = {}
     for prec in (rb.FP64, rb.FP32):
+        form = FORMS["plain" if prec == rb.FP64 else "mixed"]
         p = G.params
         p.precision = prec
+        p.smoother = getattr(rb, form["smoother"])
+        p.pre_sweeps = p.post_sweeps = form["sweeps"]
         G.set_params(p)
         for w in range(max(args.warmup, 3)):
             step(rb, G, 10 + w)
@@ -359,7 +400,8 @@ def main():
         "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
         "config": {"workload": "worst-case 128x128x64 (smoothed random density, z=0 clamped, top-face load set, "
                                "wsff), Lanczos k=16, inner MG-PCG to 1e-6, stencil assembly included",
-                   "form": "mixed: FP32 V-cycle (SGS 1/1) inside FP64 flexible CG",
+                   "form": "mixed: FP32 V-cycle (Chebyshev(4) smoothing) inside FP64 flexible CG, one CUDA "
+                           "graph per solve; plain (fp64_ms_per_step): FP64 symmetric-GS V-cycle",
                    "fp64_ms_per_step": r64["ms"] / args.steps,
                    "speedup_vs_fp64": r64["ms"] / r32["ms"],
                    "lambda_mixed": lam32, "lambda_fp64": lam64,

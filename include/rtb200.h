@@ -50,7 +50,12 @@ enum rt_mode {
     RT_MODE_WSFF = 3  /* with support, free direction */
 };
 
-enum rt_smoother { RT_SMOOTH_GS = 0, RT_SMOOTH_SGS = 1, RT_SMOOTH_JACOBI = 2 };
+/* GS: the reference's 8-colour point-block Gauss-Seidel (forward in pre and post
+ * smoothing, grid/Grid.cu:1068-1111); SGS: forward pre, backward post (symmetric
+ * V-cycle); JACOBI: damped point-block Jacobi; CHEBY: Chebyshev polynomial in
+ * D^-1 A of degree pre/post_sweeps on [lmax/30, 1.1 lmax], lmax estimated per
+ * level by rt_update_stencil (one fused element-tile / stencil kernel per step). */
+enum rt_smoother { RT_SMOOTH_GS = 0, RT_SMOOTH_SGS = 1, RT_SMOOTH_JACOBI = 2, RT_SMOOTH_CHEBY = 3 };
 enum rt_precision { RT_FP64 = 0, RT_FP32 = 1 };
 enum rt_layout { RT_LAYOUT_DENSE = 0, RT_LAYOUT_REF_GS = 1 };
 enum rt_field { RT_FIELD_U = 0, RT_FIELD_F = 1, RT_FIELD_R = 2, RT_FIELD_RHO = 3, RT_FIELD_SENS = 4,
@@ -155,6 +160,9 @@ int rt_ref_gs_map(rt_hier* h, int level, int* vidmap, int* n_gs, int* gs_num /*[
 /* ---- multigrid operators (grid/Grid.cu) ----------------------------------- */
 /* Galerkin coarse stencils + coarsest factorisation: HierarchyGrid::update_stencil (grid/Grid.cpp:2108-2119) */
 int rt_update_stencil(rt_hier* h);
+/* largest eigenvalue estimate of D^-1 A on a smoothed level (set by rt_update_stencil);
+ * no counterpart in the reference (its GS smoother needs none) */
+int rt_smoother_lmax(rt_hier* h, int level, double* lmax);
 /* Grid::update_residual (grid/Grid.cu:1644-1678): r = f - K u on a level */
 int rt_update_residual(rt_hier* h, int level);
 /* Grid::gs_relax (grid/Grid.cu:1068-1111) and the other smoothers */

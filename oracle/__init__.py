@@ -20,7 +20,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "liboracle.so")
 
-SMOOTH_GS, SMOOTH_SGS, SMOOTH_JACOBI = 0, 1, 2
+SMOOTH_GS, SMOOTH_SGS, SMOOTH_JACOBI, SMOOTH_CHEBY = 0, 1, 2, 3
 
 
 def build() -> str:
@@ -36,7 +36,7 @@ class Level(C.Structure):
         ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("ratio", C.c_int),
         ("eact", C.c_void_p), ("vact", C.c_void_p), ("vfix", C.c_void_p), ("w", C.c_void_p),
         ("st", C.c_void_p), ("u", C.c_void_p), ("f", C.c_void_p), ("r", C.c_void_p),
-        ("ainv", C.c_void_p), ("aidx", C.c_void_p), ("na", C.c_int),
+        ("ainv", C.c_void_p), ("aidx", C.c_void_p), ("na", C.c_int), ("lmax", C.c_double), ("d", C.c_void_p),
     ]
 
 
@@ -88,6 +88,10 @@ def lib():
             "or_lanczos": (C.c_int, [P, C.c_int, P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, P, P,
                                      C.c_int, C.c_int, P, C.c_uint64, C.c_int, C.c_double, C.c_int, P, P, P]),
             "or_tridiag_max_eig": (C.c_double, [C.c_int, P, P]),
+            "or_cheby_coef": (None, [C.c_double, C.c_int, P, P]),
+            "or_fine_cheby": (None, [P, P, P, P, P, P, C.c_int]),
+            "or_st_cheby": (None, [P, P, P, P, P, C.c_int]),
+            "or_lambda_max": (C.c_double, [P, C.c_int, P, C.c_uint64, C.c_int, P]),
             "or_sensitivity": (None, [C.c_int, C.c_int, C.c_int, P, P, C.c_float, P, P, P]),
             "or_filter": (None, [C.c_int, C.c_int, C.c_int, P, C.c_float, P, P]),
             "or_oc_try": (None, [C.c_long, P, P, P, P, C.c_float, C.c_float, C.c_float, C.c_float, P]),
@@ -224,6 +228,7 @@ class Hierarchy:
             d["u"] = np.zeros(3 * nv)
             d["f"] = np.zeros(3 * nv)
             d["r"] = np.zeros(3 * nv)
+            d["d"] = np.zeros(3 * nv)
             if i == 0:
                 d["rho"] = np.ascontiguousarray(rho, np.float32).ravel().copy()
                 d["w"] = np.zeros(nx * ny * nz)
@@ -250,6 +255,7 @@ class Hierarchy:
             L.w = ptr(d.get("w"))
             L.st = ptr(d.get("st"))
             L.u, L.f, L.r = ptr(d["u"]), ptr(d["f"]), ptr(d["r"])
+            L.d = ptr(d["d"])
             L.ainv = ptr(d.get("ainv"))
             L.aidx = ptr(d.get("aidx"))
 
@@ -269,6 +275,12 @@ class Hierarchy:
             return
         lib().or_penalty_weights(d["w"].size, ptr(d["eact"]), ptr(d["rho"]), self.p, ptr(d["w"]))
 
+    def set_lmax(self, values):
+        """Chebyshev bounds per smoothed level (e.g. the device's estimates, for parity)."""
+        for i, v in enumerate(values):
+            self.LA[i].lmax = float(v)
+        self._lmax_fixed = True
+
     def set_weights(self, w):
         """Use given element weights rho^p instead of this library's powf.  The
         reference evaluates powf in FP32; C and CUDA powf may differ by an ulp, so
@@ -286,6 +298,11 @@ class Hierarchy:
             else:
                 lib().or_galerkin_from_stencil(self.lv(i - 1), self.lv(i))
         rc = lib().or_coarsest_setup(self.lv(self.nlev - 1), 1 if self.no_support else 0)
+        if not getattr(self, "_lmax_fixed", False):
+            for i in range(self.nlev - 1):
+                work = np.zeros(3 * self.arrs[i]["u"].size)
+                self.LA[i].lmax = lib().or_lambda_max(self.lv(i), 1 if i == 0 else 0, ptr(self.KE), 0x51AB + i, 15,
+                                                      ptr(work))
         if rc != 0:
             raise RuntimeError("coarsest factorisation failed")
 

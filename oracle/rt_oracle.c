@@ -469,6 +469,57 @@ void or_st_jacobi(const or_level* L, double* u, const double* f, double omega, d
 }
 
 /* ------------------------------------------------------------------------ */
+/* Chebyshev smoothing (not in the reference)                               */
+/* ------------------------------------------------------------------------ */
+void or_cheby_coef(double lmax, int k, double* a, double* b) {
+    double hi = 1.1 * lmax, lo = lmax / 30.0;
+    double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+    double rho = 1.0 / sigma;
+    *a = 0.0;
+    *b = 1.0 / theta;
+    for (int i = 1; i <= k; i++) {
+        double rn = 1.0 / (2.0 * sigma - rho);
+        *a = rn * rho;
+        *b = 2.0 * rn / delta;
+        rho = rn;
+    }
+}
+
+/* d = a_k d + b_k D^-1 (f - K u), unew = u + d; fixed nodes: unew = f / n_e, d = 0 */
+void or_fine_cheby(const or_level* L, const double* KE, const double* u, const double* f, double* unew, double* d,
+                   int k) {
+    int vx = L->nx + 1, vy = L->ny + 1, vz = L->nz + 1;
+    long nv = (long)vx * vy * vz;
+    double ca, cb;
+    or_cheby_coef(L->lmax, k, &ca, &cb);
+#pragma omp parallel for collapse(2)
+    for (int z = 0; z < vz; z++)
+        for (int y = 0; y < vy; y++)
+            for (int x = 0; x < vx; x++) {
+                long v = NODE(x, y, z, vx, vy);
+                double nu[3] = {0, 0, 0}, dn[3] = {0, 0, 0};
+                if (L->vact[v]) {
+                    double KU[3], S[9];
+                    int ne;
+                    fine_node_sum(L, KE, u, x, y, z, 0, KU, S, &ne);
+                    if (L->vfix && L->vfix[v]) {
+                        for (int c = 0; c < 3; c++) nu[c] = f[c * nv + v] / ne;
+                    } else {
+                        double Si[9], rr[3];
+                        inv3(S, Si);
+                        for (int c = 0; c < 3; c++) rr[c] = f[c * nv + v] - KU[c];
+                        for (int c = 0; c < 3; c++) {
+                            double zc = Si[c * 3] * rr[0] + Si[c * 3 + 1] * rr[1] + Si[c * 3 + 2] * rr[2];
+                            dn[c] = (k == 0 ? 0.0 : ca * d[c * nv + v]) + cb * zc;
+                            nu[c] = u[c * nv + v] + dn[c];
+                        }
+                    }
+                }
+                for (int c = 0; c < 3; c++) { unew[c * nv + v] = nu[c]; d[c * nv + v] = dn[c]; }
+            }
+}
+
+/* ------------------------------------------------------------------------ */
 /* transfers: trilinear P with weights prod (r-|d|)/r, restriction = P^T    */
 /* restrict_residual{,_nondyadic}_kernel (grid/Grid.cu:1680-1794),          */
 /* prolongate_correction{,_nondyadic}_kernel (grid/Grid.cu:1818-1895)        */
@@ -530,6 +581,51 @@ void or_prolong_add(const or_level* fine, const or_level* coarse, const double* 
                 }
                 for (int c = 0; c < 3; c++) uf[c * nvf + vf] += s[c];
             }
+}
+
+void or_st_cheby(const or_level* L, const double* u, const double* f, double* unew, double* d, int k) {
+    int vx = L->nx + 1, vy = L->ny + 1, vz = L->nz + 1;
+    long nv = (long)vx * vy * vz;
+    double ca, cb;
+    or_cheby_coef(L->lmax, k, &ca, &cb);
+#pragma omp parallel for collapse(2)
+    for (int z = 0; z < vz; z++)
+        for (int y = 0; y < vy; y++)
+            for (int x = 0; x < vx; x++) {
+                long v = NODE(x, y, z, vx, vy);
+                double nu[3] = {0, 0, 0}, dn[3] = {0, 0, 0};
+                if (L->vact[v]) {
+                    double Au[3], S[9], Si[9], rr[3];
+                    st_node_sum(L, u, x, y, z, 0, Au);
+                    for (int i = 0; i < 9; i++) S[i] = L->st[(long)(13 * 9 + i) * nv + v];
+                    inv3(S, Si);
+                    for (int c = 0; c < 3; c++) rr[c] = f[c * nv + v] - Au[c];
+                    for (int c = 0; c < 3; c++) {
+                        double zc = Si[c * 3] * rr[0] + Si[c * 3 + 1] * rr[1] + Si[c * 3 + 2] * rr[2];
+                        dn[c] = (k == 0 ? 0.0 : ca * d[c * nv + v]) + cb * zc;
+                        nu[c] = u[c * nv + v] + dn[c];
+                    }
+                }
+                for (int c = 0; c < 3; c++) { unew[c * nv + v] = nu[c]; d[c * nv + v] = dn[c]; }
+            }
+}
+
+/* largest eigenvalue of D^-1 A by power steps (D^-1 A v = v - jacobi(v; f = 0, omega = 1)) */
+double or_lambda_max(or_level* L, int is_fine, const double* KE, uint64_t seed, int iters, double* work) {
+    long nv = (long)(L->nx + 1) * (L->ny + 1) * (L->nz + 1), n = 3 * nv;
+    double *x = work, *z = work + n, *zero = work + 2 * n;
+    memset(zero, 0, sizeof(double) * n);
+    or_rng_uniform(seed, n, x);
+    for (int it = 0; it < iters; it++) {
+        double nn = sqrt(or_dot(n, x, x));
+        for (long i = 0; i < n; i++) x[i] /= nn;
+        memcpy(z, x, sizeof(double) * n);
+        double* tmp = L->r;
+        if (is_fine) or_fine_jacobi(L, KE, z, zero, 1.0, tmp);
+        else or_st_jacobi(L, z, zero, 1.0, tmp);
+        for (long i = 0; i < n; i++) x[i] -= z[i];
+    }
+    return sqrt(or_dot(n, x, x));
 }
 
 /* ------------------------------------------------------------------------ */
@@ -808,7 +904,13 @@ double or_dot(long n, const double* a, const double* b) {
 static long lvl_nv(const or_level* L) { return (long)(L->nx + 1) * (L->ny + 1) * (L->nz + 1); }
 
 static void smooth(or_level* L, int is_fine, const double* KE, int smoother, int backward, double omega) {
-    if (smoother == OR_SMOOTH_JACOBI) {
+    if (smoother == OR_SMOOTH_CHEBY) {
+        /* one step of degree 1 (callers use smooth_n for higher degree) */
+        double* tmp = L->r;
+        if (is_fine) or_fine_cheby(L, KE, L->u, L->f, tmp, L->d, 0);
+        else or_st_cheby(L, L->u, L->f, tmp, L->d, 0);
+        memcpy(L->u, tmp, sizeof(double) * 3 * lvl_nv(L));
+    } else if (smoother == OR_SMOOTH_JACOBI) {
         double* tmp = L->r; /* r is free scratch while smoothing */
         if (is_fine) or_fine_jacobi(L, KE, L->u, L->f, omega, tmp);
         else or_st_jacobi(L, L->u, L->f, omega, tmp);
@@ -816,6 +918,21 @@ static void smooth(or_level* L, int is_fine, const double* KE, int smoother, int
         if (is_fine) or_fine_gs(L, KE, L->u, L->f, backward);
         else or_st_gs(L, L->u, L->f, backward);
     }
+}
+
+static void smooth_n(or_level* L, int is_fine, const double* KE, int smoother, int n, int backward, double omega) {
+    if (smoother != OR_SMOOTH_CHEBY) {
+        for (int s = 0; s < n; s++) smooth(L, is_fine, KE, smoother, backward, omega);
+        return;
+    }
+    long nn = 3 * lvl_nv(L);
+    for (int s = 0; s < n; s++) {
+        double* src = (s % 2 == 0) ? L->u : L->r;
+        double* dst = (s % 2 == 0) ? L->r : L->u;
+        if (is_fine) or_fine_cheby(L, KE, src, L->f, dst, L->d, s);
+        else or_st_cheby(L, src, L->f, dst, L->d, s);
+    }
+    if (n % 2 == 1) memcpy(L->u, L->r, sizeof(double) * nn);
 }
 
 double or_vcycle(or_level* lv, int nlev, const double* KE, int smoother, int npre, int npost, double omega,
@@ -828,14 +945,14 @@ double or_vcycle(or_level* lv, int nlev, const double* KE, int smoother, int npr
             memset(lv[i].u, 0, sizeof(double) * 3 * lvl_nv(&lv[i]));
         }
         if (i < nlev - 1) {
-            for (int s = 0; s < npre; s++) smooth(&lv[i], i == 0, KE, smoother, 0, omega);
+            smooth_n(&lv[i], i == 0, KE, smoother, npre, 0, omega);
         } else {
             or_coarsest_solve(&lv[i]);
         }
     }
     for (int i = nlev - 2; i >= 0; i--) {
         or_prolong_add(&lv[i], &lv[i + 1], lv[i + 1].u, lv[i].u);
-        for (int s = 0; s < npost; s++) smooth(&lv[i], i == 0, KE, smoother, smoother == OR_SMOOTH_SGS, omega);
+        smooth_n(&lv[i], i == 0, KE, smoother, npost, smoother == OR_SMOOTH_SGS, omega);
     }
     if (precond_mode) return 0;
     or_fine_residual(&lv[0], KE, lv[0].u, lv[0].f, lv[0].r);

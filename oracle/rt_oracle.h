@@ -43,9 +43,18 @@ typedef struct {
     double* ainv;         /* coarsest level only: dense (pseudo-)inverse [3na][3na] */
     int* aidx;            /* coarsest level only: active-node index -> node id [na] */
     int na;               /* coarsest level only: number of active nodes */
+    double lmax;          /* smoothed levels: largest eigenvalue estimate of D^-1 A (Chebyshev) */
+    double* d;            /* smoothed levels: Chebyshev direction [3][nv] */
 } or_level;
 
-enum { OR_SMOOTH_GS = 0, OR_SMOOTH_SGS = 1, OR_SMOOTH_JACOBI = 2 };
+enum { OR_SMOOTH_GS = 0, OR_SMOOTH_SGS = 1, OR_SMOOTH_JACOBI = 2, OR_SMOOTH_CHEBY = 3 };
+
+/* Chebyshev smoothing on [lmax/30, 1.1 lmax] (not in the reference) */
+void or_cheby_coef(double lmax, int k, double* a, double* b);
+void or_fine_cheby(const or_level* L, const double* KE, const double* u, const double* f, double* unew, double* d,
+                   int k);
+void or_st_cheby(const or_level* L, const double* u, const double* f, double* unew, double* d, int k);
+double or_lambda_max(or_level* L, int is_fine, const double* KE, uint64_t seed, int iters, double* work /*[3][3nv]*/);
 
 /* element template (element/templateMatrix.cpp:15-124) */
 void or_template_matrix(double E, double nu, double h, double* KE /* [576] row-major */);

@@ -15,7 +15,7 @@ RT_OK, RT_EINVAL, RT_ECUDA, RT_ENOCONV, RT_ENAN, RT_ETIMEOUT, RT_ENOMEM, RT_ESTA
 STATUS_NAMES = {0: "RT_OK", 1: "RT_EINVAL", 2: "RT_ECUDA", 3: "RT_ENOCONV", 4: "RT_ENAN", 5: "RT_ETIMEOUT",
                 6: "RT_ENOMEM", 7: "RT_ESTATE"}
 MODE_NSCF, MODE_NSFF, MODE_WSCF, MODE_WSFF = range(4)
-SMOOTH_GS, SMOOTH_SGS, SMOOTH_JACOBI = range(3)
+SMOOTH_GS, SMOOTH_SGS, SMOOTH_JACOBI, SMOOTH_CHEBY = range(4)
 FP64, FP32 = 0, 1
 LAYOUT_DENSE, LAYOUT_REF_GS = 0, 1
 FIELD_U, FIELD_F, FIELD_R, FIELD_RHO, FIELD_SENS, FIELD_STENCIL, FIELD_VACT, FIELD_EACT, FIELD_VFIX, \
@@ -88,6 +88,7 @@ SIGNATURES = {
     "rt_ref_gs_map": (I, [P, I, P, P, P]),
     "rt_update_stencil": (I, [P]),
     "rt_update_residual": (I, [P, I]),
+    "rt_smoother_lmax": (I, [P, I, C.POINTER(D)]),
     "rt_smooth": (I, [P, I, I, I, D]),
     "rt_restrict_residual": (I, [P, I]),
     "rt_prolongate_correction": (I, [P, I]),

@@ -245,6 +245,7 @@ static void free_hier(rt_hier* h) {
     for (auto& L : h->L) {
         cudaFree(L.vact); cudaFree(L.eact); cudaFree(L.u); cudaFree(L.f); cudaFree(L.r);
         cudaFree(L.u32); cudaFree(L.f32); cudaFree(L.r32); cudaFree(L.st); cudaFree(L.st32);
+        cudaFree(L.d); cudaFree(L.d32);
         cudaFree(L.aidx); cudaFree(L.ainv); cudaFree(L.ainv32); cudaFree(L.dvec); cudaFree(L.dvec32);
     }
     cudaFree(h->KE_dev); cudaFree(h->KE32_dev); cudaFree(h->rho); cudaFree(h->w); cudaFree(h->vfix);
@@ -252,6 +253,8 @@ static void free_hier(rt_hier* h) {
     cudaFree(h->Rd); cudaFree(h->Ru); cudaFree(h->fs); cudaFree(h->fs_old); cudaFree(h->x); cudaFree(h->rr);
     cudaFree(h->z); cudaFree(h->p); cudaFree(h->q); cudaFree(h->rold); cudaFree(h->Q); cudaFree(h->partials);
     cudaFree(h->scal); cudaFree(h->Qgal);
+    if (h->pcg_exec) cudaGraphExecDestroy(h->pcg_exec);
+    if (h->pcg_graph) cudaGraphDestroy(h->pcg_graph);
     delete h;
 }
 
@@ -263,6 +266,7 @@ static int upload_KE(rt_hier* h) {
     RT_CUDA(h->ctx, cudaMemcpyAsync(h->KE32_dev, ke32, sizeof(float) * 576, cudaMemcpyHostToDevice, h->ctx->stream));
     RT_CUDA(h->ctx, cudaStreamSynchronize(h->ctx->stream));
     if (h->Qgal) { cudaFree(h->Qgal); h->Qgal = nullptr; h->Qgal_ratio = 0; }
+    h->graph_epoch++;  // the element operator's Hadamard-domain values are kernel parameters
     return RT_OK;
 }
 
@@ -321,6 +325,7 @@ static int build_hier(rt_ctx* c, const rt_params* p, int nx, int ny, int nz, uin
         RT_CHECK(rtk::node_active(c, L.nx, L.ny, L.nz, L.eact, L.vact));
         RT_CHECK(dalloc(c, &L.u, 3 * L.nv)); RT_CHECK(dalloc(c, &L.f, 3 * L.nv)); RT_CHECK(dalloc(c, &L.r, 3 * L.nv));
         RT_CHECK(dalloc(c, &L.u32, 3 * L.nv)); RT_CHECK(dalloc(c, &L.f32, 3 * L.nv)); RT_CHECK(dalloc(c, &L.r32, 3 * L.nv));
+        RT_CHECK(dalloc(c, &L.d, 3 * L.nv)); RT_CHECK(dalloc(c, &L.d32, 3 * L.nv));
         RT_CUDA(c, cudaMemsetAsync(L.u, 0, sizeof(double) * 3 * L.nv, c->stream));
         RT_CUDA(c, cudaMemsetAsync(L.f, 0, sizeof(double) * 3 * L.nv, c->stream));
         RT_CUDA(c, cudaMemsetAsync(L.r, 0, sizeof(double) * 3 * L.nv, c->stream));
@@ -368,6 +373,7 @@ static int build_hier(rt_ctx* c, const rt_params* p, int nx, int ny, int nz, uin
     RT_CHECK(dalloc(c, &h->scal, RT_NSCAL));
     RT_CUDA(c, cudaMemsetAsync(h->scal, 0, sizeof(double) * RT_NSCAL, c->stream));
     RT_CHECK(upload_KE(h));
+    RT_CHECK(rtk::init_tile_kernels(c));
     *out = h;
     return RT_OK;
 }
@@ -515,6 +521,7 @@ extern "C" int rt_set_support(rt_hier* h, const uint8_t* vfix) {
     RT_CUDA(h->ctx, cudaMemcpyAsync(h->vfix, vfix, L.nv, cudaMemcpyHostToDevice, h->ctx->stream));
     RT_CUDA(h->ctx, cudaStreamSynchronize(h->ctx->stream));
     h->has_support = cnt > 0;
+    h->graph_epoch++;  // kernel variants depend on whether supports exist
     h->stencil_ready = false;
     return RT_OK;
 }
@@ -807,6 +814,8 @@ extern "C" int rt_init_density(rt_hier* h, float rho) {
 // ---------------------------------------------------------------------------
 // multigrid
 // ---------------------------------------------------------------------------
+static int estimate_lmax(rt_hier* h, int lvl);
+
 extern "C" int rt_update_stencil(rt_hier* h) {
     if (!h) return RT_EINVAL;
     RT_CUDA(h->ctx, cudaSetDevice(h->ctx->device));
@@ -818,7 +827,19 @@ extern "C" int rt_update_stencil(rt_hier* h) {
         RT_CHECK(rtk::d2f(h, 243 * h->L[i].nv, h->L[i].st, h->L[i].st32));
     }
     RT_CHECK(rtk::coarsest_setup(h));
+    // spectral bound of D^-1 A per smoothed level, for the Chebyshev smoother
+    for (int i = 0; i + 1 < nl; i++) RT_CHECK(estimate_lmax(h, i));
     h->stencil_ready = true;
+    return RT_OK;
+}
+
+extern "C" int rt_smoother_lmax(rt_hier* h, int lvl, double* lmax) {
+    if (!h || !lmax || lvl < 0 || lvl + 1 >= (int)h->L.size()) return RT_EINVAL;
+    if (!h->stencil_ready) return rt_fail(h->ctx, RT_ESTATE, "rt_update_stencil has not run");
+    RT_CUDA(h->ctx, cudaMemcpyAsync(h->ctx->hscal, h->scal + RT_SCAL_LMAX + lvl, sizeof(double),
+                                    cudaMemcpyDeviceToHost, h->ctx->stream));
+    RT_CUDA(h->ctx, cudaStreamSynchronize(h->ctx->stream));
+    *lmax = h->ctx->hscal[0];
     return RT_OK;
 }
 
@@ -829,13 +850,40 @@ struct LvlVec<double> {
     static double* u(rt_level& L) { return L.u; }
     static double* f(rt_level& L) { return L.f; }
     static double* r(rt_level& L) { return L.r; }
+    static double* d(rt_level& L) { return L.d; }
 };
 template <>
 struct LvlVec<float> {
     static float* u(rt_level& L) { return L.u32; }
     static float* f(rt_level& L) { return L.f32; }
     static float* r(rt_level& L) { return L.r32; }
+    static float* d(rt_level& L) { return L.d32; }
 };
+
+__global__ void k_sqrt_slot(const double* __restrict__ src, double* __restrict__ dst) {
+    if (threadIdx.x == 0) dst[0] = sqrt(src[0]);
+}
+
+// lmax(D^-1 A) of a level by 15 power steps (D^-1 A v = v - jacobi(v; f = 0, omega = 1)),
+// left on the device for the Chebyshev kernels
+static int estimate_lmax(rt_hier* h, int lvl) {
+    rt_level& L = h->L[lvl];
+    const long n = 3 * L.nv;
+    double *x = h->x, *z = h->z, *zero = h->q;
+    RT_CUDA(h->ctx, cudaMemsetAsync(zero, 0, sizeof(double) * n, h->ctx->stream));
+    RT_CHECK(rtk::rng_uniform(h, 0x51ab + lvl, n, x));
+    for (int it = 0; it < 15; it++) {
+        RT_CHECK(rtk::dot(h, n, x, x, h->scal + 290));
+        RT_CHECK(rtk::scale(h, n, x, h->scal + 290, true));
+        if (lvl == 0) RT_CHECK(rtk::fine_jacobi<double>(h, x, zero, z, 1.0));
+        else RT_CHECK(rtk::st_jacobi<double>(h, lvl, x, zero, z, 1.0));
+        RT_CHECK(rtk::axpy(h, n, -1.0, z, x));
+    }
+    RT_CHECK(rtk::dot(h, n, x, x, h->scal + 291));
+    return rt_launch(h->ctx, "lmax_sqrt", [&] {
+        k_sqrt_slot<<<1, 32, 0, h->ctx->stream>>>(h->scal + 291, h->scal + RT_SCAL_LMAX + lvl);
+    });
+}
 
 template <typename T>
 static int level_residual(rt_hier* h, int lvl) {
@@ -850,19 +898,26 @@ static int level_smooth(rt_hier* h, int lvl, int smoother, int sweeps, double om
     T* u = LvlVec<T>::u(L);
     T* f = LvlVec<T>::f(L);
     T* tmp = LvlVec<T>::r(L);
+    const double* lmax = h->scal + RT_SCAL_LMAX + lvl;
     for (int s = 0; s < sweeps; s++) {
-        if (smoother == RT_SMOOTH_JACOBI) {
+        if (smoother == RT_SMOOTH_JACOBI || smoother == RT_SMOOTH_CHEBY) {
             // ping-pong u -> tmp -> u
             const T* src = (s % 2 == 0) ? u : tmp;
             T* dst = (s % 2 == 0) ? tmp : u;
-            if (lvl == 0) RT_CHECK(rtk::fine_jacobi<T>(h, src, f, dst, omega));
-            else RT_CHECK(rtk::st_jacobi<T>(h, lvl, src, f, dst, omega));
+            if (smoother == RT_SMOOTH_CHEBY) {
+                T* d = LvlVec<T>::d(L);
+                if (lvl == 0) RT_CHECK(rtk::fine_cheby<T>(h, src, f, dst, d, lmax, s));
+                else RT_CHECK(rtk::st_cheby<T>(h, lvl, src, f, dst, d, lmax, s));
+            } else {
+                if (lvl == 0) RT_CHECK(rtk::fine_jacobi<T>(h, src, f, dst, omega));
+                else RT_CHECK(rtk::st_jacobi<T>(h, lvl, src, f, dst, omega));
+            }
         } else {
             if (lvl == 0) RT_CHECK(rtk::fine_gs<T>(h, u, f, backward));
             else RT_CHECK(rtk::st_gs<T>(h, lvl, u, f, backward));
         }
     }
-    if (smoother == RT_SMOOTH_JACOBI && (sweeps % 2) == 1)
+    if ((smoother == RT_SMOOTH_JACOBI || smoother == RT_SMOOTH_CHEBY) && (sweeps % 2) == 1)
         RT_CUDA(h->ctx, cudaMemcpyAsync(u, tmp, sizeof(T) * 3 * L.nv, cudaMemcpyDeviceToDevice, h->ctx->stream));
     return RT_OK;
 }
@@ -1013,6 +1068,97 @@ static int precondition(rt_hier* h, const double* r, double* z, const double* rr
     return RT_OK;
 }
 
+// p = z + beta p, flexible beta = (z.r - z.rold) / rz_prev; beta = 0 on the first iteration
+__global__ void k_pcg_p_it(long n, const double* __restrict__ s, const double* __restrict__ it, double* __restrict__ p,
+                           const double* __restrict__ z) {
+    const bool first = it[0] == 0.0;
+    const double den = s[2];
+    const double beta = (first || den == 0.0) ? 0.0 : (s[0] - s[1]) / den;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        p[i] = first ? z[i] : z[i] + beta * p[i];
+}
+
+// end of an iteration: it += 1, rz_prev = rz; optionally set the WHILE condition of the graph
+__global__ void k_pcg_tail(double* __restrict__ scal, cudaGraphConditionalHandle cond, int use_cond) {
+    if (threadIdx.x != 0) return;
+    const double it = scal[24] + 1.0;
+    scal[24] = it;
+    scal[12] = scal[10];
+    if (use_cond) {
+        const double rr = scal[21], bb = scal[22] > 0 ? scal[22] : 1.0;
+        const bool go = isfinite(rr) && sqrt(rr) > scal[25] * sqrt(bb) && it < scal[26];
+        cudaGraphSetConditional(cond, go ? 1u : 0u);
+    }
+}
+
+// one MG-PCG iteration, all scalars on the device (graph-capturable):
+// scal[10] z.r, [11] z.rold, [12] previous z.r, [20] p.q, [21] r.r, [24] iteration
+static int pcg_body(rt_hier* h, double* x, double* r, bool no_support, cudaGraphConditionalHandle cond,
+                    int use_cond = 0) {
+    rt_level& L = h->L[0];
+    const long n = 3 * L.nv;
+    rt_ctx* c = h->ctx;
+    RT_CHECK(precondition(h, r, h->z, h->scal + 21));
+    if (no_support) RT_CHECK(rtk::displacement_project(h, h->z));
+    RT_CHECK(rtk::dot2(h, n, h->z, r, h->rold, h->scal + 10));
+    RT_CHECK(rt_launch(c, "pcg_update_p", [&] {
+        k_pcg_p_it<<<(unsigned)std::min<long>((n + 255) / 256, (long)c->sm_count * 16), 256, 0, c->stream>>>(
+            n, h->scal + 10, h->scal + 24, h->p, h->z);
+    }));
+    RT_CHECK(rtk::fine_applyK<double>(h, h->p, h->q));
+    RT_CHECK(rtk::dot(h, n, h->p, h->q, h->scal + 20));
+    RT_CHECK(rtk::pcg_update_xr(h, n, h->scal + 10, h->scal + 20, x, r, h->p, h->q, h->rold));
+    RT_CHECK(rtk::dot(h, n, r, r, h->scal + 21));
+    return rt_launch(c, "pcg_tail", [&] { k_pcg_tail<<<1, 32, 0, c->stream>>>(h->scal, cond, use_cond); });
+}
+
+// the whole iteration loop as one graph: a WHILE conditional node whose body is one
+// captured iteration; the body's last kernel decides whether to run again
+static int pcg_graph_run(rt_hier* h, double* x, double* r, bool no_support) {
+    rt_ctx* c = h->ctx;
+    const uint64_t key = ((uint64_t)(uintptr_t)x * 1315423911ull) ^ ((uint64_t)h->P.precision << 1) ^
+                         ((uint64_t)h->P.smoother << 3) ^ ((uint64_t)h->P.pre_sweeps << 6) ^
+                         ((uint64_t)h->P.post_sweeps << 11) ^ ((uint64_t)no_support << 16) ^
+                         ((uint64_t)(h->P.jacobi_omega * 1e6) << 20) ^ ((uint64_t)h->graph_epoch << 40);
+    if (!h->pcg_exec || h->pcg_key != key) {
+        if (h->pcg_exec) { cudaGraphExecDestroy(h->pcg_exec); h->pcg_exec = nullptr; }
+        if (h->pcg_graph) { cudaGraphDestroy(h->pcg_graph); h->pcg_graph = nullptr; }
+        cudaGraph_t g;
+        RT_CUDA(c, cudaGraphCreate(&g, 0));
+        cudaGraphConditionalHandle cond;
+        RT_CUDA(c, cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cond;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        RT_CUDA(c, cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        RT_CUDA(c, cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        int s = pcg_body(h, x, r, no_support, cond, 1);
+        cudaGraph_t captured = nullptr;
+        cudaError_t e = cudaStreamEndCapture(c->stream, &captured);
+        if (s != RT_OK) { cudaGraphDestroy(g); return s; }
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(g);
+            return rt_fail(c, RT_ECUDA, "PCG graph capture failed: %s", cudaGetErrorString(e));
+        }
+        cudaGraphExec_t exec;
+        e = cudaGraphInstantiate(&exec, g, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(g);
+            return rt_fail(c, RT_ECUDA, "PCG graph instantiation failed: %s", cudaGetErrorString(e));
+        }
+        h->pcg_graph = g;
+        h->pcg_exec = exec;
+        h->pcg_key = key;
+    }
+    RT_CUDA(c, cudaGraphLaunch(h->pcg_exec, c->stream));
+    c->launches += 1;
+    return RT_OK;
+}
+
 static int pcg_core(rt_hier* h, double* x, const double* b, double tol, int maxit, rt_solve_info* info, int* vcycles) {
     rt_level& L = h->L[0];
     const long n = 3 * L.nv;
@@ -1033,27 +1179,32 @@ static int pcg_core(rt_hier* h, double* x, const double* b, double tol, int maxi
     // without supports K is singular (rigid modes): keep the search space in its range
     const bool no_support = (h->P.mode == RT_MODE_NSCF || h->P.mode == RT_MODE_NSFF);
     if (no_support && h->Ru == nullptr) RT_CHECK(rtk::rigid_nodes(h));
-    while (rel > tol && it < maxit) {
-        RT_CHECK(precondition(h, r, h->z, h->scal + 21));
-        if (no_support) RT_CHECK(rtk::displacement_project(h, h->z));
-        (*vcycles)++;
-        double* rz = h->scal + 10 + 2 * (it & 1);
-        double* rz_prev = h->scal + 10 + 2 * ((it + 1) & 1);
-        RT_CHECK(rtk::dot2(h, n, h->z, r, h->rold, rz));  // rz[0] = z.r, rz[1] = z.rold
-        RT_CHECK(rtk::pcg_update_p(h, n, rz, rz_prev, h->p, h->z, it == 0));
-        RT_CHECK(rtk::fine_applyK<double>(h, h->p, h->q));
-        RT_CHECK(rtk::dot(h, n, h->p, h->q, h->scal + 20));
-        RT_CHECK(rtk::pcg_update_xr(h, n, rz, h->scal + 20, x, r, h->p, h->q, h->rold));
-        RT_CHECK(rtk::dot(h, n, r, r, h->scal + 21));
-        double rr2;
-        RT_CHECK(read_scalars(h, 21, 1, &rr2));
-        if (!std::isfinite(rr2)) {
-            if (info) { info->status = RT_ENAN; info->iterations = it + 1; }
-            return rt_fail(h->ctx, RT_ENAN, "NaN in PCG at iteration %d", it + 1);
+    if (rel > tol && maxit > 0) {
+        // loop state on the device: scal[24] iteration count, scal[25] tol, scal[26] maxit
+        double st[3] = {0.0, tol, (double)maxit};
+        memcpy(h->ctx->hscal + 8, st, sizeof(st));
+        RT_CUDA(h->ctx, cudaMemcpyAsync(h->scal + 24, h->ctx->hscal + 8, sizeof(st), cudaMemcpyHostToDevice,
+                                        h->ctx->stream));
+        if (h->use_graphs && !h->ctx->profile) {
+            RT_CHECK(pcg_graph_run(h, x, r, no_support));
+        } else {
+            for (int k = 0; k < maxit; k++) {
+                RT_CHECK(pcg_body(h, x, r, no_support, 0));
+                double s2[4];
+                RT_CHECK(read_scalars(h, 21, 4, s2));
+                if (!std::isfinite(s2[0]) || std::sqrt(s2[0]) / bn <= tol) break;
+            }
         }
-        rel = std::sqrt(rr2) / bn;
-        it++;
+        double s3[4];
+        RT_CHECK(read_scalars(h, 21, 4, s3));  // rr, bb, (unused), it
+        if (!std::isfinite(s3[0])) {
+            if (info) { info->status = RT_ENAN; info->iterations = (int)s3[3]; }
+            return rt_fail(h->ctx, RT_ENAN, "NaN in PCG at iteration %d", (int)s3[3]);
+        }
+        rel = std::sqrt(s3[0]) / bn;
+        it = (int)s3[3];
     }
+    *vcycles += it;
     if (info) {
         info->iterations = it;
         info->rel_residual = rel;

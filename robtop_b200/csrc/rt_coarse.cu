@@ -125,6 +125,181 @@ __global__ void __launch_bounds__(ST_BS) k_st_jacobi(int nx, int ny, int nz, T o
     }
 }
 
+// ---------------------------------------------------------------------------
+// Lane-split stencil kernels: 4 lanes per node, lane q sums neighbours
+// k = q, q+4, ..., then the three row sums are combined with shuffles.  Coarse
+// levels are small (the first coarse level of 128x128x64 has 18.5k nodes), so
+// a thread per node leaves most of the GPU idle on long dependent load chains.
+// MODE 0: r = f - A u;  MODE 2: Jacobi;  MODE 3: Chebyshev step.
+// ---------------------------------------------------------------------------
+template <typename T, int MODE>
+__global__ void __launch_bounds__(ST_BS) k_st_split4(int nx, int ny, int nz, const uint8_t* __restrict__ vact,
+                                                      const T* __restrict__ st, const T* __restrict__ u,
+                                                      const T* __restrict__ f, T* __restrict__ out,
+                                                      T* __restrict__ d, T omega, const double* __restrict__ lmax,
+                                                      int kstep) {
+    T ca = T(0), cb = T(0);
+    if (MODE == 3) {
+        double a_, b_;
+        rt_cheby_coef(lmax[0], kstep, a_, b_);
+        ca = (T)a_;
+        cb = (T)b_;
+    }
+    const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
+    const long nv = (long)vx * vy * vz;
+    const int q = threadIdx.x & 3;
+    const long ngroups = (long)gridDim.x * (blockDim.x >> 2);
+    // every lane runs the same number of trips (the shuffles below use the full mask)
+    const long vend = ((nv + ngroups - 1) / ngroups) * ngroups;
+    for (long v = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 2; v < vend; v += ngroups) {
+        const bool inb = v < nv;
+        const bool act = inb && vact[v];
+        T Au[3] = {T(0), T(0), T(0)};
+        if (act) {
+            const int x = (int)(v % vx), y = (int)((v / vx) % vy), z = (int)(v / ((long)vx * vy));
+#pragma unroll
+            for (int kk = 0; kk < 7; kk++) {
+                const int k = q + 4 * kk;
+                if (k >= 27) break;
+                const int jx = x + k % 3 - 1, jy = y + (k / 3) % 3 - 1, jz = z + k / 9 - 1;
+                if (jx < 0 || jy < 0 || jz < 0 || jx >= vx || jy >= vy || jz >= vz) continue;
+                const long nj = jx + (long)vx * (jy + (long)vy * jz);
+                const T u0 = u[nj], u1 = u[nv + nj], u2 = u[2 * nv + nj];
+                const T* s = st + (long)(k * 9) * nv + v;
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+                    Au[r] += s[(3 * r) * nv] * u0 + s[(3 * r + 1) * nv] * u1 + s[(3 * r + 2) * nv] * u2;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            Au[r] += __shfl_xor_sync(0xffffffffu, Au[r], 1);
+            Au[r] += __shfl_xor_sync(0xffffffffu, Au[r], 2);
+        }
+        if (!inb || q == 3) continue;
+        // lane q (0..2) owns component q
+        const long oq = (long)q * nv + v;
+        if (MODE == 0) {
+            out[oq] = act ? f[oq] - Au[q] : T(0);
+            continue;
+        }
+        T res = T(0), dn = T(0);
+        if (act) {
+            T S[9], I[9];
+#pragma unroll
+            for (int i = 0; i < 9; i++) S[i] = st[(long)(13 * 9 + i) * nv + v];
+            const T a0 = S[0], b0 = S[1], c0 = S[2], d0 = S[3], e0 = S[4], f0 = S[5], g0 = S[6], h0 = S[7], k0 = S[8];
+            const T A = e0 * k0 - f0 * h0, B = -(d0 * k0 - f0 * g0), Cc = d0 * h0 - e0 * g0;
+            const T id = T(1) / (a0 * A + b0 * B + c0 * Cc);
+            I[0] = A * id; I[1] = -(b0 * k0 - c0 * h0) * id; I[2] = (b0 * f0 - c0 * e0) * id;
+            I[3] = B * id; I[4] = (a0 * k0 - c0 * g0) * id; I[5] = -(a0 * f0 - c0 * d0) * id;
+            I[6] = Cc * id; I[7] = -(a0 * h0 - b0 * g0) * id; I[8] = (a0 * e0 - b0 * d0) * id;
+            const T r0 = f[v] - Au[0], r1 = f[nv + v] - Au[1], r2 = f[2 * nv + v] - Au[2];
+            const T zq = I[q * 3] * r0 + I[q * 3 + 1] * r1 + I[q * 3 + 2] * r2;
+            if (MODE == 2) {
+                res = u[oq] + omega * zq;
+            } else {
+                dn = (kstep == 0 ? T(0) : ca * d[oq]) + cb * zq;
+                res = u[oq] + dn;
+            }
+        }
+        out[oq] = res;
+        if (MODE == 3) d[oq] = dn;
+    }
+}
+
+// ratio-4 restriction, 8 lanes per coarse node: lane t sums the fine plane dz = t - 3
+template <typename T>
+__global__ void __launch_bounds__(ST_BS) k_restrict4_split8(int fnx, int fny, int fnz, int cnx, int cny, int cnz,
+                                                            const uint8_t* __restrict__ cvact,
+                                                            const T* __restrict__ rf, T* __restrict__ fc) {
+    constexpr int R = 4;
+    const int fvx = fnx + 1, fvy = fny + 1, fvz = fnz + 1;
+    const int cvx = cnx + 1, cvy = cny + 1, cvz = cnz + 1;
+    const long nvf = (long)fvx * fvy * fvz, nvc = (long)cvx * cvy * cvz;
+    const int t = threadIdx.x & 7;
+    const long ngroups = (long)gridDim.x * (blockDim.x >> 3);
+    const long vend = ((nvc + ngroups - 1) / ngroups) * ngroups;
+    for (long vc = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 3; vc < vend; vc += ngroups) {
+        T s[3] = {T(0), T(0), T(0)};
+        const bool inb = vc < nvc;
+        if (inb && t < 7 && cvact[vc]) {
+            const int X = (int)(vc % cvx), Y = (int)((vc / cvx) % cvy), Z = (int)(vc / ((long)cvx * cvy));
+            const int dz = t - 3;
+            const int z = R * Z + dz;
+            if (z >= 0 && z < fvz) {
+                const T wz = T(R - abs(dz));
+                for (int dy = -(R - 1); dy <= R - 1; dy++) {
+                    const int y = R * Y + dy;
+                    if (y < 0 || y >= fvy) continue;
+                    const T wyz = wz * T(R - abs(dy));
+#pragma unroll
+                    for (int dx = -(R - 1); dx <= R - 1; dx++) {
+                        const int x = R * X + dx;
+                        if (x < 0 || x >= fvx) continue;
+                        const long vf = x + (long)fvx * (y + (long)fvy * z);
+                        const T wgt = wyz * T(R - abs(dx)) * (T(1) / T(R * R * R));
+                        s[0] += wgt * rf[vf];
+                        s[1] += wgt * rf[nvf + vf];
+                        s[2] += wgt * rf[2 * nvf + vf];
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            s[c] += __shfl_xor_sync(0xffffffffu, s[c], 1);
+            s[c] += __shfl_xor_sync(0xffffffffu, s[c], 2);
+            s[c] += __shfl_xor_sync(0xffffffffu, s[c], 4);
+        }
+        if (inb && t < 3) fc[(long)t * nvc + vc] = s[t];
+    }
+}
+
+// Chebyshev step on an assembled-stencil level (see rt_cheby_coef)
+template <typename T>
+__global__ void __launch_bounds__(ST_BS) k_st_cheby(int nx, int ny, int nz, const uint8_t* __restrict__ vact,
+                                                     const T* __restrict__ st, const T* __restrict__ u,
+                                                     const T* __restrict__ f, T* __restrict__ unew,
+                                                     T* __restrict__ d, const double* __restrict__ lmax, int kstep) {
+    double ca, cb;
+    rt_cheby_coef(lmax[0], kstep, ca, cb);
+    const T a = (T)ca, b = (T)cb;
+    const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
+    const long nv = (long)vx * vy * vz;
+    for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < nv; v += (long)gridDim.x * blockDim.x) {
+        const int x = (int)(v % vx), y = (int)((v / vx) % vy), z = (int)(v / ((long)vx * vy));
+        T nu[3] = {T(0), T(0), T(0)}, dn[3] = {T(0), T(0), T(0)};
+        if (vact[v]) {
+            T Au[3];
+            st_node_sum<T, false>(x, y, z, vx, vy, vz, nv, vact, st, u, v, Au);
+            T S[9], I[9];
+#pragma unroll
+            for (int i = 0; i < 9; i++) S[i] = st[(long)(13 * 9 + i) * nv + v];
+            const T a0 = S[0], b0 = S[1], c0 = S[2], d0 = S[3], e0 = S[4], f0 = S[5], g0 = S[6], h0 = S[7], k0 = S[8];
+            const T A = e0 * k0 - f0 * h0, B = -(d0 * k0 - f0 * g0), Cc = d0 * h0 - e0 * g0;
+            const T id = T(1) / (a0 * A + b0 * B + c0 * Cc);
+            I[0] = A * id; I[1] = -(b0 * k0 - c0 * h0) * id; I[2] = (b0 * f0 - c0 * e0) * id;
+            I[3] = B * id; I[4] = (a0 * k0 - c0 * g0) * id; I[5] = -(a0 * f0 - c0 * d0) * id;
+            I[6] = Cc * id; I[7] = -(a0 * h0 - b0 * g0) * id; I[8] = (a0 * e0 - b0 * d0) * id;
+            T rr[3];
+#pragma unroll
+            for (int q = 0; q < 3; q++) rr[q] = f[q * nv + v] - Au[q];
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                const T zq = I[q * 3] * rr[0] + I[q * 3 + 1] * rr[1] + I[q * 3 + 2] * rr[2];
+                dn[q] = (kstep == 0 ? T(0) : a * d[q * nv + v]) + b * zq;
+                nu[q] = u[q * nv + v] + dn[q];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            unew[q * nv + v] = nu[q];
+            d[q * nv + v] = dn[q];
+        }
+    }
+}
+
 // f_c(X) = sum_{|d| < r} prod (r - |d|)/r * r_f(rX + d)
 template <typename T, int R>
 __global__ void __launch_bounds__(ST_BS) k_restrict(int fnx, int fny, int fnz, int cnx, int cny, int cnz,
@@ -394,8 +569,8 @@ template <typename T>
 int st_residual(rt_hier* h, int lvl, const T* u, const T* f, T* r) {
     rt_level& L = h->L[lvl];
     return rt_launch(h->ctx, sizeof(T) == 8 ? "st_residual_f64" : "st_residual_f32", [&] {
-        k_st_residual<T><<<grid_for(h->ctx, L.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(L.nx, L.ny, L.nz, L.vact,
-                                                                                      stp<T>(L), u, f, r);
+        k_st_split4<T, 0><<<grid_for(h->ctx, 4 * L.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(
+            L.nx, L.ny, L.nz, L.vact, stp<T>(L), u, f, r, nullptr, T(0), nullptr, 0);
     });
 }
 
@@ -418,10 +593,21 @@ template <typename T>
 int st_jacobi(rt_hier* h, int lvl, const T* u, const T* f, T* unew, double omega) {
     rt_level& L = h->L[lvl];
     return rt_launch(h->ctx, sizeof(T) == 8 ? "st_jacobi_f64" : "st_jacobi_f32", [&] {
-        k_st_jacobi<T><<<grid_for(h->ctx, L.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(L.nx, L.ny, L.nz, (T)omega, L.vact,
-                                                                                    stp<T>(L), u, f, unew);
+        k_st_split4<T, 2><<<grid_for(h->ctx, 4 * L.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(
+            L.nx, L.ny, L.nz, L.vact, stp<T>(L), u, f, unew, nullptr, (T)omega, nullptr, 0);
     });
 }
+
+template <typename T>
+int st_cheby(rt_hier* h, int lvl, const T* u, const T* f, T* unew, T* d, const double* lmax, int kstep) {
+    rt_level& L = h->L[lvl];
+    return rt_launch(h->ctx, sizeof(T) == 8 ? "st_cheby_f64" : "st_cheby_f32", [&] {
+        k_st_split4<T, 3><<<grid_for(h->ctx, 4 * L.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(
+            L.nx, L.ny, L.nz, L.vact, stp<T>(L), u, f, unew, d, T(0), lmax, kstep);
+    });
+}
+template int st_cheby<double>(rt_hier*, int, const double*, const double*, double*, double*, const double*, int);
+template int st_cheby<float>(rt_hier*, int, const float*, const float*, float*, float*, const double*, int);
 
 template <typename T>
 int restrict_(rt_hier* h, int lvl, const T* rf, T* fc) {
@@ -430,7 +616,8 @@ int restrict_(rt_hier* h, int lvl, const T* rf, T* fc) {
     return rt_launch(h->ctx, sizeof(T) == 8 ? "restrict_f64" : "restrict_f32", [&] {
         unsigned g = grid_for(h->ctx, Cc.nv, ST_BS);
         if (Cc.ratio == 4)
-            k_restrict<T, 4><<<g, ST_BS, 0, h->ctx->stream>>>(F.nx, F.ny, F.nz, Cc.nx, Cc.ny, Cc.nz, Cc.vact, rf, fc);
+            k_restrict4_split8<T><<<grid_for(h->ctx, 8 * Cc.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(
+                F.nx, F.ny, F.nz, Cc.nx, Cc.ny, Cc.nz, Cc.vact, rf, fc);
         else
             k_restrict<T, 2><<<g, ST_BS, 0, h->ctx->stream>>>(F.nx, F.ny, F.nz, Cc.nx, Cc.ny, Cc.nz, Cc.vact, rf, fc);
     });

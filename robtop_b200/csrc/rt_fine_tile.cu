@@ -1,33 +1,37 @@
 // rt_fine_tile.cu — finest-level operator as an element-tile kernel.
 //
 // Same operator as update_residual_OTFA_{NS,WS}_kernel (grid/Grid.cu:1450-1557),
-// applyK_OTFA_kernel (grid/Grid.cu:2439-2517) plus a damped point-block
-// Jacobi sweep, computed element by element instead of node by node:
+// applyK_OTFA_kernel (grid/Grid.cu:2439-2517) plus damped point-block Jacobi
+// and Chebyshev smoothing steps, computed element by element instead of node
+// by node:
 //
 //  * KE is applied in the Hadamard (+-1 tensor-product) basis of the 8
 //    element vertices.  With T = H (x) I3, KE = T Kt T^T / 64 and the 24x24 Kt
 //    has 45 non-zeros (independent of E, nu, h), so one element costs two
 //    3-stage butterflies per component and 45 FMAs instead of a dense 24x24.
-//  * A CTA owns a 32x8 node tile and marches up through z.  Per element layer
-//    the 33x9 elements touching the tile are computed once, their 24 outputs
-//    go to shared memory, and every node gathers its 8 contributions (4 from
-//    the layer below, 4 from the layer above) — no atomics, each element is
-//    evaluated once per tile.
-//  * u of the two node layers an element layer couples sits in shared memory
-//    (34x10 halo tile per layer, loaded once); fixed (support) nodes are
-//    loaded as zero so the WS rule of the reference falls out of the data.
+//  * A CTA owns a 32 x TY node tile and marches up through z.  Per element
+//    layer the (33 x (TY+1)) elements touching the tile are computed once,
+//    their 24 outputs go to shared memory, and every node gathers its 8
+//    contributions (4 from the layer below, 4 from the layer above) — no
+//    atomics, each element is evaluated once per tile.
+//  * The loop is software-pipelined: while layer ez is computed, the u values
+//    of node layer ez+2, the weights of element layer ez+1 and the node-phase
+//    inputs (f, own u, flags) are already in flight into registers.
+//  * Fixed (support) nodes are stored as zero in the shared u tile, so the WS
+//    rule of the reference falls out of the data.
 #include <cuda_runtime.h>
 
 #include "rt_internal.h"
 
 namespace {
 
-constexpr int TX = 32, TY = 8;            // node tile
+constexpr int TX = 32, TY = 4;             // node tile
 constexpr int EXT = TX + 1, EYT = TY + 1;  // element tile (one halo element below in x and y)
 constexpr int UXT = TX + 2, UYT = TY + 2;  // node halo tile
-constexpr int NE_T = EXT * EYT;            // 297 elements per layer
-constexpr int NU_T = UXT * UYT;            // 340 nodes per layer
-constexpr int TILE_BS = 320;               // >= NE_T, multiple of 32
+constexpr int NE_T = EXT * EYT;            // 165 elements per layer
+constexpr int NU_T = UXT * UYT;            // 204 nodes per layer
+constexpr int TILE_BS = 192;               // >= NE_T, multiple of 32
+constexpr int U_PER_T = (NU_T + TILE_BS - 1) / TILE_BS;  // halo nodes loaded per thread (2)
 
 // sparsity pattern of Kt = T^T KE T / 64 (rows/cols index 3*mode + comp)
 __device__ constexpr int KT_R[45] = {3, 3, 3, 4, 4, 5, 5, 6, 6, 7, 7, 7, 8, 8, 9, 9, 10, 10, 11, 11, 11, 12, 12,
@@ -75,24 +79,34 @@ __device__ __forceinline__ void element_apply(T* a, const KtVals<T>& kt, T w) {
 
 template <typename T>
 struct TileSmem {
-    T u[2][3][NU_T];
-    T e[24][NE_T];
+    T u[2][3][NU_T];   // node layers ez, ez+1 (slot layer & 1)
+    T e[24][NE_T];     // element outputs of the current layer
     float w[3][NE_T];  // element weights of layers ez-1, ez, ez+1 (slot (layer+3)%3)
 };
 
 // MODE 0: r = f - K u (fixed rows: r = f)     MODE 1: out = K u (fixed rows: u)
 // MODE 2: unew = u + omega D^-1 (f - K u) (fixed: f / n_e)
+// MODE 3: Chebyshev step kstep: d = a_k d + b_k D^-1 (f - K u), unew = u + d (fixed: f / n_e)
 template <typename T, bool WS, int MODE>
-__global__ void __launch_bounds__(TILE_BS) k_fine_tile(int nx, int ny, int nz, int zchunk,
+__global__ void __launch_bounds__(TILE_BS, sizeof(T) == 8 ? 2 : 4) k_fine_tile(int nx, int ny, int nz, int zchunk,
                                                         const uint8_t* __restrict__ vact,
                                                         const float* __restrict__ wgt,
                                                         const uint8_t* __restrict__ vfix, const KtVals<T> kt,
                                                         const T* __restrict__ u, const T* __restrict__ f,
-                                                        T* __restrict__ out, T omega) {
+                                                        T* __restrict__ out, T omega, T* __restrict__ dvec,
+                                                        const double* __restrict__ lmax, int kstep) {
     extern __shared__ __align__(16) unsigned char smraw[];
     TileSmem<T>& S = *reinterpret_cast<TileSmem<T>*>(smraw);
+    T cheb_a = T(0), cheb_b = T(0);
+    if (MODE == 3) {
+        double ca, cb;
+        rt_cheby_coef(lmax[0], kstep, ca, cb);
+        cheb_a = (T)ca;
+        cheb_b = (T)cb;
+    }
     const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
     const long nv = (long)vx * vy * vz;
+    const long plane = (long)vx * vy;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int zb = blockIdx.z * zchunk;
     const int ze = min(zb + zchunk, vz);
@@ -101,46 +115,104 @@ __global__ void __launch_bounds__(TILE_BS) k_fine_tile(int nx, int ny, int nz, i
     const int nxl = tid % TX, nyl = tid / TX;
     const int nxg = x0 + nxl, nyg = y0 + nyl;
     const bool node_thread = tid < TX * TY && nxg < vx && nyg < vy;
+    const long vxy = node_thread ? nxg + (long)vx * nyg : 0;
     // element owned by this thread
     const int exl = tid % EXT, eyl = tid / EXT;
     const int exg = x0 - 1 + exl, eyg = y0 - 1 + eyl;
     const bool elem_xy = tid < NE_T && exg >= 0 && eyg >= 0 && exg < nx && eyg < ny;
+    const long exy = elem_xy ? exg + (long)nx * eyg : 0;
+    // halo nodes this thread loads (columns of the 34 x (TY+2) tile)
+    long hxy[U_PER_T];
+    bool hok[U_PER_T];
+#pragma unroll
+    for (int j = 0; j < U_PER_T; j++) {
+        const int i = tid + j * TILE_BS;
+        const int xx = x0 - 1 + i % UXT, yy = y0 - 1 + i / UXT;
+        hok[j] = i < NU_T && xx >= 0 && yy >= 0 && xx < vx && yy < vy;
+        hxy[j] = hok[j] ? xx + (long)vx * yy : 0;
+    }
 
-    auto load_layer = [&](int L) {
-        T* dst = &S.u[L & 1][0][0];
-        for (int i = tid; i < NU_T; i += TILE_BS) {
-            const int xx = x0 - 1 + i % UXT, yy = y0 - 1 + i / UXT;
+    // register stage for one node layer of the halo tile + one element layer of weights
+    T pu[U_PER_T][3];
+    float pw = 0.f;
+    auto fetch_layer = [&](int L) {
+#pragma unroll
+        for (int j = 0; j < U_PER_T; j++) {
             T a = T(0), b = T(0), c = T(0);
-            if (L >= 0 && L < vz && xx >= 0 && yy >= 0 && xx < vx && yy < vy) {
-                const long v = xx + (long)vx * (yy + (long)vy * L);
+            if (hok[j] && L >= 0 && L < vz) {
+                const long v = hxy[j] + plane * L;
                 if (!(WS && vfix[v])) {
                     a = u[v];
                     b = u[nv + v];
                     c = u[2 * nv + v];
                 }
             }
-            dst[i] = a;
-            dst[NU_T + i] = b;
-            dst[2 * NU_T + i] = c;
+            pu[j][0] = a;
+            pu[j][1] = b;
+            pu[j][2] = c;
         }
     };
-    auto load_w = [&](int ez) {
-        if (tid < NE_T) {
-            float wv = 0.f;
-            if (elem_xy && ez >= 0 && ez < nz) wv = wgt[exg + (long)nx * (eyg + (long)ny * ez)];
-            S.w[(ez + 3) % 3][tid] = wv;
+    auto stash_layer = [&](int L) {
+        T* dst = &S.u[L & 1][0][0];
+#pragma unroll
+        for (int j = 0; j < U_PER_T; j++) {
+            const int i = tid + j * TILE_BS;
+            if (i < NU_T) {
+                dst[i] = pu[j][0];
+                dst[NU_T + i] = pu[j][1];
+                dst[2 * NU_T + i] = pu[j][2];
+            }
         }
+    };
+    auto fetch_w = [&](int ez) {
+        pw = (elem_xy && ez >= 0 && ez < nz) ? wgt[exy + (long)nx * ny * ez] : 0.f;
+    };
+    auto stash_w = [&](int ez) {
+        if (tid < NE_T) S.w[(ez + 3) % 3][tid] = pw;
     };
 
-    load_layer(zb - 1);
-    load_w(zb - 1);
+    // prologue: node layer zb-1 and element weights of layer zb-1 into shared memory,
+    // node layer zb in registers
+    fetch_layer(zb - 1);
+    fetch_w(zb - 1);
+    stash_layer(zb - 1);
+    stash_w(zb - 1);
+    fetch_layer(zb);
+    fetch_w(zb);
+
     T acc[3] = {T(0), T(0), T(0)};
     for (int ez = zb - 1; ez < ze; ez++) {
-        // node layers ez (in smem) and ez+1 (load now); weights of element layer ez
-        load_layer(ez + 1);
-        if (ez != zb - 1) load_w(ez);
+        // registers hold node layer ez+1 and the weights of element layer ez+1.  The u slot of
+        // layer ez+1 was last read by the element phase of iteration ez-1 (behind its second
+        // barrier); the weight slot (ez+1)%3 held layer ez-2, read by the node phase of
+        // iteration ez-1, so it is only written after the barrier below.
+        stash_layer(ez + 1);
         __syncthreads();
-        // ---- element phase
+        if (ez + 1 < ze) stash_w(ez + 1);
+        // start the loads for the next iteration and for this iteration's node phase
+        if (ez + 2 <= ze) {
+            fetch_layer(ez + 2);
+            fetch_w(ez + 2);
+        }
+        const bool out_layer = ez >= zb;
+        T fv[3] = {T(0), T(0), T(0)}, uo[3] = {T(0), T(0), T(0)}, dv[3] = {T(0), T(0), T(0)};
+        bool act = false, fixed = false;
+        long vout = 0;
+        if (node_thread && out_layer) {
+            vout = vxy + plane * ez;
+            act = vact[vout];
+            fixed = WS && act && vfix[vout];
+            if (MODE != 1)
+#pragma unroll
+                for (int c = 0; c < 3; c++) fv[c] = f[c * nv + vout];
+            if (MODE >= 1)
+#pragma unroll
+                for (int c = 0; c < 3; c++) uo[c] = u[c * nv + vout];
+            if (MODE == 3 && kstep > 0)
+#pragma unroll
+                for (int c = 0; c < 3; c++) dv[c] = dvec[c * nv + vout];
+        }
+        // ---- element phase (element layer ez couples node layers ez and ez+1)
         if (tid < NE_T) {
             T a[24];
             const float wv = S.w[(ez + 3) % 3][tid];
@@ -166,7 +238,7 @@ __global__ void __launch_bounds__(TILE_BS) k_fine_tile(int nx, int ny, int nz, i
         __syncthreads();
         // ---- node phase
         if (node_thread) {
-            if (ez >= zb) {
+            if (out_layer) {
                 // node layer ez: bottom vertices (bit z = 0) of element layer ez
 #pragma unroll
                 for (int dy = 0; dy < 2; dy++)
@@ -177,19 +249,16 @@ __global__ void __launch_bounds__(TILE_BS) k_fine_tile(int nx, int ny, int nz, i
 #pragma unroll
                         for (int c = 0; c < 3; c++) acc[c] += S.e[3 * vtx + c][el];
                     }
-                const int zg = ez;
-                const long v = nxg + (long)vx * (nyg + (long)vy * zg);
-                const bool act = vact[v];
-                const bool fixed = WS && act && vfix[v];
+                const long v = vout;
                 if (MODE == 0) {
 #pragma unroll
-                    for (int c = 0; c < 3; c++)
-                        out[c * nv + v] = act ? (fixed ? f[c * nv + v] : f[c * nv + v] - acc[c]) : T(0);
+                    for (int c = 0; c < 3; c++) out[c * nv + v] = act ? (fixed ? fv[c] : fv[c] - acc[c]) : T(0);
                 } else if (MODE == 1) {
 #pragma unroll
-                    for (int c = 0; c < 3; c++) out[c * nv + v] = act ? (fixed ? u[c * nv + v] : acc[c]) : T(0);
+                    for (int c = 0; c < 3; c++) out[c * nv + v] = act ? (fixed ? uo[c] : acc[c]) : T(0);
                 } else {
                     T nu[3] = {T(0), T(0), T(0)};
+                    T dn[3] = {T(0), T(0), T(0)};
                     if (act) {
                         // diagonal block from the 8 incident element weights
                         T sw = T(0), sxy = T(0), sxz = T(0), syz = T(0);
@@ -211,7 +280,7 @@ __global__ void __launch_bounds__(TILE_BS) k_fine_tile(int nx, int ny, int nz, i
                                 }
                         if (fixed) {
 #pragma unroll
-                            for (int c = 0; c < 3; c++) nu[c] = f[c * nv + v] / T(ne);
+                            for (int c = 0; c < 3; c++) nu[c] = fv[c] / T(ne);
                         } else {
                             const T A = kt.diag_a * sw, bxy = kt.diag_b * sxy, bxz = kt.diag_b * sxz,
                                     byz = kt.diag_b * syz;
@@ -221,14 +290,29 @@ __global__ void __launch_bounds__(TILE_BS) k_fine_tile(int nx, int ny, int nz, i
                             const T id = T(1) / (A * c00 + bxy * c01 + bxz * c02);
                             T rr[3];
 #pragma unroll
-                            for (int c = 0; c < 3; c++) rr[c] = f[c * nv + v] - acc[c];
-                            nu[0] = u[v] + omega * id * (c00 * rr[0] + c01 * rr[1] + c02 * rr[2]);
-                            nu[1] = u[nv + v] + omega * id * (c01 * rr[0] + c11 * rr[1] + c12 * rr[2]);
-                            nu[2] = u[2 * nv + v] + omega * id * (c02 * rr[0] + c12 * rr[1] + c22 * rr[2]);
+                            for (int c = 0; c < 3; c++) rr[c] = fv[c] - acc[c];
+                            T zz[3];
+                            zz[0] = id * (c00 * rr[0] + c01 * rr[1] + c02 * rr[2]);
+                            zz[1] = id * (c01 * rr[0] + c11 * rr[1] + c12 * rr[2]);
+                            zz[2] = id * (c02 * rr[0] + c12 * rr[1] + c22 * rr[2]);
+                            if (MODE == 2) {
+#pragma unroll
+                                for (int c = 0; c < 3; c++) nu[c] = uo[c] + omega * zz[c];
+                            } else {
+                                // Chebyshev step: d = ca d + cb D^-1 r, u += d
+#pragma unroll
+                                for (int c = 0; c < 3; c++) {
+                                    dn[c] = (kstep == 0 ? T(0) : cheb_a * dv[c]) + cheb_b * zz[c];
+                                    nu[c] = uo[c] + dn[c];
+                                }
+                            }
                         }
                     }
 #pragma unroll
                     for (int c = 0; c < 3; c++) out[c * nv + v] = nu[c];
+                    if (MODE == 3)
+#pragma unroll
+                        for (int c = 0; c < 3; c++) dvec[c * nv + v] = dn[c];
                 }
             }
             // start node layer ez+1 with the top vertices (bit z = 1) of element layer ez
@@ -275,37 +359,59 @@ KtVals<T> make_kt(const rt_hier* h) {
 
 int tile_zchunk(rt_ctx* c, int vx, int vy, int vz) {
     const long tiles = (long)((vx + TX - 1) / TX) * ((vy + TY - 1) / TY);
-    const long target = (long)c->sm_count * 3;  // ~3 resident CTAs per SM
+    const long target = (long)c->sm_count * 4;  // ~4 resident CTAs per SM
     long chunks = (target + tiles - 1) / tiles;
     if (chunks < 1) chunks = 1;
     int zc = (int)((vz + chunks - 1) / chunks);
-    if (zc < 4) zc = 4;
+    if (zc < 8) zc = 8;
     return zc;
 }
 
 template <typename T, bool WS, int MODE>
-int launch_tile(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name) {
+int launch_tile(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name, T* dvec = nullptr,
+                const double* lmax = nullptr, int kstep = 0) {
     rt_level& L = h->L[0];
-    static int attr_dev = -1;
     const size_t smem = sizeof(TileSmem<T>);
     auto kern = k_fine_tile<T, WS, MODE>;
-    if (attr_dev != h->ctx->device) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return rt_fail(h->ctx, RT_ECUDA, "smem attribute: %s", cudaGetErrorString(e));
-        attr_dev = h->ctx->device;
-    }
     const int zc = tile_zchunk(h->ctx, L.vx, L.vy, L.vz);
     dim3 grid((L.vx + TX - 1) / TX, (L.vy + TY - 1) / TY, (L.vz + zc - 1) / zc);
     const KtVals<T> kt = make_kt<T>(h);
     return rt_launch(h->ctx, name, [&] {
         kern<<<grid, TILE_BS, smem, h->ctx->stream>>>(L.nx, L.ny, L.nz, zc, L.vact, h->w, h->vfix, kt, u, f, out,
-                                                      (T)omega);
+                                                      (T)omega, dvec, lmax, kstep);
     });
+}
+
+template <typename T, bool WS, int MODE>
+cudaError_t set_attr() {
+    return cudaFuncSetAttribute(k_fine_tile<T, WS, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(TileSmem<T>));
+}
+
+template <typename T>
+cudaError_t set_attrs_T() {
+    cudaError_t e = cudaSuccess;
+    cudaError_t r[8] = {set_attr<T, false, 0>(), set_attr<T, false, 1>(), set_attr<T, false, 2>(),
+                        set_attr<T, false, 3>(), set_attr<T, true, 0>(),  set_attr<T, true, 1>(),
+                        set_attr<T, true, 2>(),  set_attr<T, true, 3>()};
+    for (auto x : r)
+        if (x != cudaSuccess) e = x;
+    return e;
 }
 
 }  // namespace
 
 namespace rtk {
+
+// dynamic shared-memory limits of every tile-kernel variant, set once per device
+// (before any stream capture can include a launch)
+int init_tile_kernels(rt_ctx* c) {
+    cudaError_t e1 = set_attrs_T<double>(), e2 = set_attrs_T<float>();
+    if (e1 != cudaSuccess || e2 != cudaSuccess)
+        return rt_fail(c, RT_ECUDA, "tile kernel attributes: %s",
+                       cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+    return RT_OK;
+}
 
 template <typename T>
 int fine_residual(rt_hier* h, const T* u, const T* f, T* r) {
@@ -327,6 +433,15 @@ int fine_jacobi(rt_hier* h, const T* u, const T* f, T* unew, double omega) {
                           : launch_tile<T, false, 2>(h, u, f, unew, omega, nm);
 }
 
+template <typename T>
+int fine_cheby(rt_hier* h, const T* u, const T* f, T* unew, T* d, const double* lmax, int kstep) {
+    const char* nm = sizeof(T) == 8 ? "fine_cheby_f64" : "fine_cheby_f32";
+    return h->has_support ? launch_tile<T, true, 3>(h, u, f, unew, 0.0, nm, d, lmax, kstep)
+                          : launch_tile<T, false, 3>(h, u, f, unew, 0.0, nm, d, lmax, kstep);
+}
+
+template int fine_cheby<double>(rt_hier*, const double*, const double*, double*, double*, const double*, int);
+template int fine_cheby<float>(rt_hier*, const float*, const float*, float*, float*, const double*, int);
 template int fine_residual<double>(rt_hier*, const double*, const double*, double*);
 template int fine_residual<float>(rt_hier*, const float*, const float*, float*);
 template int fine_applyK<double>(rt_hier*, const double*, double*);

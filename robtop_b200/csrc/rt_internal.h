@@ -42,6 +42,8 @@ struct rt_level {
     uint8_t* eact = nullptr;
     double *u = nullptr, *f = nullptr, *r = nullptr;
     float *u32 = nullptr, *f32 = nullptr, *r32 = nullptr;
+    double* d = nullptr;  // Chebyshev direction
+    float* d32 = nullptr;
     double* st = nullptr;   // [243][nv]
     float* st32 = nullptr;  // [243][nv]
     // coarsest level
@@ -88,6 +90,12 @@ struct rt_hier {
     bool stencil_ready = false;
     double* Qgal = nullptr;  // [R^3][576] cell Galerkin blocks P^T KE P (rebuilt when KE changes)
     int Qgal_ratio = 0;
+    // MG-PCG loop captured as one CUDA graph (WHILE conditional node)
+    bool use_graphs = true;
+    cudaGraph_t pcg_graph = nullptr;
+    cudaGraphExec_t pcg_exec = nullptr;
+    uint64_t pcg_key = 0;
+    uint64_t graph_epoch = 0;  // bumped whenever captured pointers may change
 };
 
 #define RT_RED_BLOCKS 296
@@ -127,6 +135,28 @@ inline int rt_launch(rt_ctx* c, const char* name, F&& f) {
 
 static inline unsigned rt_blocks(long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
+// Chebyshev smoother on the interval [lmax / 30, 1.1 lmax] of D^-1 A (lmax from a
+// power iteration at stencil set-up).  Step k of the three-term recurrence
+//   d_0 = D^-1 r_0 / theta,   d_k = a_k d_{k-1} + b_k D^-1 r_k,   u += d_k
+// with theta = (hi+lo)/2, delta = (hi-lo)/2, sigma = theta/delta, rho_0 = 1/sigma,
+// rho_k = 1/(2 sigma - rho_{k-1}), a_k = rho_k rho_{k-1}, b_k = 2 rho_k / delta.
+#define RT_CHEBY_LO_FRAC (1.0 / 30.0)
+#define RT_CHEBY_HI_FRAC 1.1
+#define RT_SCAL_LMAX 300  // device scalar slots holding lmax(D^-1 A) per level
+__host__ __device__ inline void rt_cheby_coef(double lmax, int k, double& a, double& b) {
+    const double hi = RT_CHEBY_HI_FRAC * lmax, lo = RT_CHEBY_LO_FRAC * lmax;
+    const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+    double rho = 1.0 / sigma;
+    a = 0.0;
+    b = 1.0 / theta;
+    for (int i = 1; i <= k; i++) {
+        const double rn = 1.0 / (2.0 * sigma - rho);
+        a = rn * rho;
+        b = 2.0 * rn / delta;
+        rho = rn;
+    }
+}
+
 // kernels (each returns RT_OK or an error code) -------------------------------
 namespace rtk {
 // fine level
@@ -138,7 +168,12 @@ template <typename T>
 int fine_gs(rt_hier* h, T* u, const T* f, bool backward);
 template <typename T>
 int fine_jacobi(rt_hier* h, const T* u, const T* f, T* unew, double omega);
+template <typename T>
+int fine_cheby(rt_hier* h, const T* u, const T* f, T* unew, T* d, const double* lmax, int kstep);
+template <typename T>
+int st_cheby(rt_hier* h, int lvl, const T* u, const T* f, T* unew, T* d, const double* lmax, int kstep);
 int penalty_weights(rt_hier* h);
+int init_tile_kernels(rt_ctx* c);
 // stencil levels
 template <typename T>
 int st_residual(rt_hier* h, int lvl, const T* u, const T* f, T* r);

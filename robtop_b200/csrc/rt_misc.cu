@@ -107,7 +107,7 @@ __global__ void k_f2d_scaled(long n, const float* __restrict__ a, double* __rest
 __global__ void k_pcg_xr(long n, const double* __restrict__ num, const double* __restrict__ den, double* __restrict__ x,
                          double* __restrict__ r, const double* __restrict__ p, const double* __restrict__ q,
                          double* __restrict__ rold) {
-    const double alpha = num[0] / den[0];
+    const double alpha = den[0] != 0.0 ? num[0] / den[0] : 0.0;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
         const double ri = r[i];
         rold[i] = ri;

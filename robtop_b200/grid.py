@@ -311,6 +311,11 @@ class HierarchyGrid:
     def update_stencil(self):
         self._c(A.lib().rt_update_stencil(self._h))
 
+    def smoother_lmax(self, level):
+        v = C.c_double()
+        self._c(A.lib().rt_smoother_lmax(self._h, level, C.byref(v)))
+        return v.value
+
     def v_cycle(self, pre_relax=1, post_relax=1):
         r = C.c_double()
         self._c(A.lib().rt_vcycle(self._h, pre_relax, post_relax, C.byref(r)))

@@ -133,7 +133,31 @@ def test_coarse_level_ops(pair):
         G[i].gs_relax(1)
         uo = u.copy()
         O.lib().or_st_gs(H.lv(i), O.ptr(uo), O.ptr(f), 0)
-        assert rel_err(G[i].getDisplacement(), uo) < 1e-10
+        # the block division amplifies FP64 rounding on the 1e9-contrast stencils
+        assert rel_err(G[i].getDisplacement(), uo) < 1e-9
+
+
+def test_chebyshev_bounds_and_steps(pair):
+    cfg, ctx, G, H = pair
+    lm = [G.smoother_lmax(i) for i in range(H.nlev - 1)]
+    # device power iteration vs the oracle's own estimate (different rounding, same start vector)
+    for i in range(H.nlev - 1):
+        assert abs(lm[i] - H.LA[i].lmax) <= 1e-6 * H.LA[i].lmax
+    H.set_lmax(lm)
+    for i in range(H.nlev - 1):
+        u, f = _rand_vec(G, i, 110 + i), _rand_vec(G, i, 120 + i)
+        G[i].setDisplacement(u)
+        G[i].setForce(f)
+        G[i].smooth(rb.SMOOTH_CHEBY, 3)
+        uo, un = u.copy(), np.zeros_like(u)
+        d = np.zeros_like(u)
+        for k in range(3):
+            if i == 0:
+                O.lib().or_fine_cheby(H.lv(0), O.ptr(H.KE), O.ptr(uo), O.ptr(f), O.ptr(un), O.ptr(d), k)
+            else:
+                O.lib().or_st_cheby(H.lv(i), O.ptr(uo), O.ptr(f), O.ptr(un), O.ptr(d), k)
+            uo, un = un, uo
+        assert rel_err(G[i].getDisplacement(), uo) < 1e-9, f"level {i}"
 
 
 def test_coarsest_solve(pair):
@@ -161,8 +185,10 @@ def test_vcycle_sequence(pair):
     assert rel_err(G[0].getDisplacement(), H.arrs[0]["u"]) < 1e-8
 
 
-@pytest.mark.parametrize("precision", [rb.FP64, rb.FP32])
-def test_pcg_to_1e6(pair, precision):
+@pytest.mark.parametrize("precision,smoother,sweeps", [(rb.FP64, rb.SMOOTH_SGS, 1), (rb.FP32, rb.SMOOTH_SGS, 1),
+                                                       (rb.FP32, rb.SMOOTH_CHEBY, 4),
+                                                       (rb.FP64, rb.SMOOTH_JACOBI, 2)])
+def test_pcg_to_1e6(pair, precision, smoother, sweeps):
     cfg, ctx, G, H = pair
     b = _rand_vec(G, 0, 80)
     if cfg["mode"] in (rb.MODE_WSCF, rb.MODE_WSFF):
@@ -174,11 +200,14 @@ def test_pcg_to_1e6(pair, precision):
         O.lib().or_displacement_project(b.size // 3, O.ptr(Ru), O.ptr(b))
     params = G.params
     params.precision = precision
+    params.smoother = smoother
+    params.pre_sweeps = params.post_sweeps = sweeps
+    params.jacobi_omega = 0.5
     G.set_params(params)
     G.update_stencil()
     G[0].setForce(b)
     G[0].reset_displacement()
-    info = G.pcg(1e-6, 200)
+    info = G.pcg(1e-6, 1000)
     assert info.status == 0 and info.rel_residual <= 1e-6
     x = G[0].getDisplacement()
     # FP64 residual check of the returned solution with the oracle operator
@@ -188,6 +217,8 @@ def test_pcg_to_1e6(pair, precision):
     xo, ito, rro = H.pcg(b, tol=1e-6, smoother=O.SMOOTH_SGS)
     assert abs(b @ x - b @ xo) <= 1e-5 * abs(b @ xo)
     params.precision = rb.FP64
+    params.smoother = rb.SMOOTH_SGS
+    params.pre_sweeps = params.post_sweeps = 1
     G.set_params(params)
     G.update_stencil()
 
