@@ -29,12 +29,19 @@ int rt_fail(rt_ctx* c, int code, const char* fmt, ...) {
 }
 
 int rt_kernel_id(rt_ctx* c, const char* name) {
-    for (size_t i = 0; i < c->kstats.size(); i++)
-        if (c->kstats[i].name == name) return (int)i;
-    rt_kstat k;
-    k.name = name;
-    c->kstats.push_back(k);
-    return (int)c->kstats.size() - 1;
+    auto it = c->kid_by_name.find(name);
+    if (it != c->kid_by_name.end()) return it->second;
+    int id = -1;
+    for (size_t i = 0; i < c->kstats.size(); i++)  // same name from another literal
+        if (c->kstats[i].name == name) id = (int)i;
+    if (id < 0) {
+        rt_kstat k;
+        k.name = name;
+        c->kstats.push_back(k);
+        id = (int)c->kstats.size() - 1;
+    }
+    c->kid_by_name[name] = id;
+    return id;
 }
 
 static cudaEvent_t ev_get(rt_ctx* c) {
@@ -274,6 +281,7 @@ static int build_hier(rt_ctx* c, const rt_params* p, int nx, int ny, int nz, uin
     rt_hier* h = new rt_hier();
     h->ctx = c;
     h->P = *p;
+    *out = h;  // the caller releases a partially built hierarchy on failure
     // level chain on the device: halve while more than 400 elements are solid (grid/Grid.cpp:488)
     struct Chain { int nx, ny, nz; uint8_t* e; long cnt; };
     std::vector<Chain> chain;
@@ -303,7 +311,10 @@ static int build_hier(rt_ctx* c, const rt_params* p, int nx, int ny, int nz, uin
     } else {
         for (size_t i = 0; i < chain.size(); i++) { idx.push_back((int)i); ratio.push_back(i ? 2 : 0); }
     }
-    if (chain.size() == 1) return rt_fail(c, RT_EINVAL, "grid too small for multigrid (<= 400 solid elements)");
+    if (chain.size() == 1) {
+        cudaFree(chain[0].e);
+        return rt_fail(c, RT_EINVAL, "grid too small for multigrid (<= 400 solid elements)");
+    }
     for (size_t k = 0; k < idx.size(); k++) {
         Chain& ch = chain[idx[k]];
         rt_level L;

@@ -4,6 +4,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/rtb200.h"
@@ -26,6 +27,7 @@ struct rt_ctx {
     // profiling
     bool profile = false;
     std::vector<rt_kstat> kstats;
+    std::unordered_map<const void*, int> kid_by_name;  // kernel-name literal -> kstats index
     std::vector<cudaEvent_t> ev_pool;
     struct Pending { int kid; cudaEvent_t a, b; };
     std::vector<Pending> pending;
@@ -122,15 +124,15 @@ int rt_kernel_id(rt_ctx* c, const char* name);
 void rt_launch_begin(rt_ctx* c, int kid, cudaEvent_t* a);
 int rt_launch_end(rt_ctx* c, int kid, cudaEvent_t a, const char* name);
 
+// every kernel launch of the library goes through here: per-context launch counts
+// and, when profiling is on, CUDA events around the launch
 template <typename F>
 inline int rt_launch(rt_ctx* c, const char* name, F&& f) {
-    static thread_local int cached_kid = -1;
-    static thread_local rt_ctx* cached_ctx = nullptr;
-    if (cached_ctx != c) { cached_kid = rt_kernel_id(c, name); cached_ctx = c; }
+    const int kid = rt_kernel_id(c, name);
     cudaEvent_t a = nullptr;
-    rt_launch_begin(c, cached_kid, &a);
+    rt_launch_begin(c, kid, &a);
     f();
-    return rt_launch_end(c, cached_kid, a, name);
+    return rt_launch_end(c, kid, a, name);
 }
 
 static inline unsigned rt_blocks(long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
