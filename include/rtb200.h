@@ -197,6 +197,17 @@ int rt_relative_residual(rt_hier* h, double* rel);
 int rt_compliance_noalloc(const double* f_dev, const double* u_dev, long long n, double* out_dev,
                           void* cuda_stream);
 
+/* Launch-shape autotuner (no counterpart in the reference): times every
+ * finest-level kernel (residual, applyK, Jacobi, Chebyshev; FP32 and FP64) over
+ * candidate tile shapes with CUDA events on the context stream and keeps the
+ * fastest.  reps: timed launches per candidate (<= 0: 5). */
+int rt_autotune(rt_hier* h, int reps);
+/* chosen shape of a finest-level kernel; mode 0 residual, 1 applyK, 2 Jacobi, 3 Chebyshev;
+ * variant 0 shared-memory element tile, 1 register-marching element kernel */
+int rt_tuning_info(rt_hier* h, int precision, int mode, int* variant, int* ty, int* zchunk, double* us);
+/* set a finest-level kernel's launch shape explicitly (ty: 2, 4 or 8 rows for variant 1) */
+int rt_set_tuning(rt_hier* h, int precision, int mode, int variant, int ty, int zchunk);
+
 /* ---- solvers -------------------------------------------------------------- */
 /* MG-preconditioned CG on level 0: u <- K^-1 f to ||r||/||f|| <= tol (solveFEM's role,
  * optimization/optimization.cpp:85-91).  Uses the precision/smoother in the params. */

@@ -99,6 +99,9 @@ SIGNATURES = {
     "rt_compliance": (I, [P, C.POINTER(D)]),
     "rt_relative_residual": (I, [P, C.POINTER(D)]),
     "rt_compliance_noalloc": (I, [P, P, C.c_longlong, P, P]),
+    "rt_autotune": (I, [P, I]),
+    "rt_tuning_info": (I, [P, I, I, C.POINTER(I), C.POINTER(I), C.POINTER(I), C.POINTER(D)]),
+    "rt_set_tuning": (I, [P, I, I, I, I, I]),
     "rt_pcg": (I, [P, D, I, C.POINTER(SolveInfo)]),
     "rt_worst_case": (I, [P, I, I, D, C.c_uint64, C.POINTER(D), C.POINTER(SolveInfo)]),
     "rt_sensitivity": (I, [P, I]),

@@ -259,7 +259,7 @@ static void free_hier(rt_hier* h) {
     cudaFree(h->sens); cudaFree(h->ftmp); cudaFree(h->eshell); cudaFree(h->load_nodes); cudaFree(h->load_normal);
     cudaFree(h->Rd); cudaFree(h->Ru); cudaFree(h->fs); cudaFree(h->fs_old); cudaFree(h->x); cudaFree(h->rr);
     cudaFree(h->z); cudaFree(h->p); cudaFree(h->q); cudaFree(h->rold); cudaFree(h->Q); cudaFree(h->partials);
-    cudaFree(h->scal); cudaFree(h->Qgal);
+    cudaFree(h->scal); cudaFree(h->Qgal); cudaFree(h->dinv64); cudaFree(h->dinv32);
     if (h->pcg_exec) cudaGraphExecDestroy(h->pcg_exec);
     if (h->pcg_graph) cudaGraphDestroy(h->pcg_graph);
     delete h;
@@ -370,6 +370,13 @@ static int build_hier(rt_ctx* c, const rt_params* p, int nx, int ny, int nz, uin
     rt_level& L0 = h->L[0];
     RT_CHECK(dalloc(c, &h->KE_dev, 576));
     RT_CHECK(dalloc(c, &h->KE32_dev, 576));
+    RT_CHECK(dalloc(c, &h->dinv64, 6 * (size_t)L0.nv));
+    RT_CHECK(dalloc(c, &h->dinv32, 6 * (size_t)L0.nv));
+    {
+        const int zc = rtk::tile_zchunk_default(c, L0.vx, L0.vy, L0.vz);
+        for (int pr = 0; pr < 2; pr++)
+            for (int m = 0; m < 4; m++) h->tune[pr][m] = rt_tile_cfg{1, 4, zc};
+    }
     RT_CHECK(dalloc(c, &h->rho, L0.ne));
     RT_CHECK(dalloc(c, &h->w, L0.ne));
     RT_CHECK(dalloc(c, &h->vfix, L0.nv));
@@ -827,10 +834,16 @@ extern "C" int rt_init_density(rt_hier* h, float rho) {
 // ---------------------------------------------------------------------------
 static int estimate_lmax(rt_hier* h, int lvl);
 
+// element weights rho^p and the inverted diagonal blocks of the finest level
+static int refresh_fine(rt_hier* h) {
+    RT_CHECK(rtk::penalty_weights(h));
+    return rtk::fine_dinv(h);
+}
+
 extern "C" int rt_update_stencil(rt_hier* h) {
     if (!h) return RT_EINVAL;
     RT_CUDA(h->ctx, cudaSetDevice(h->ctx->device));
-    RT_CHECK(rtk::penalty_weights(h));
+    RT_CHECK(refresh_fine(h));
     const int nl = (int)h->L.size();
     for (int i = 1; i < nl; i++) {
         if (i == 1) RT_CHECK(rtk::galerkin_from_elements(h));
@@ -989,14 +1002,14 @@ extern "C" int rt_vcycle(rt_hier* h, int pre, int post, double* rel_res) {
 extern "C" int rt_update_residual(rt_hier* h, int lvl) {
     if (!h || lvl < 0 || lvl >= (int)h->L.size()) return RT_EINVAL;
     if (lvl > 0) RT_CHECK(need_stencil(h));
-    else RT_CHECK(rtk::penalty_weights(h));
+    else RT_CHECK(refresh_fine(h));
     return level_residual<double>(h, lvl);
 }
 
 extern "C" int rt_smooth(rt_hier* h, int lvl, int smoother, int sweeps, double omega) {
     if (!h || lvl < 0 || lvl >= (int)h->L.size() || sweeps < 0) return RT_EINVAL;
     if (lvl > 0) RT_CHECK(need_stencil(h));
-    else RT_CHECK(rtk::penalty_weights(h));
+    else RT_CHECK(refresh_fine(h));
     return level_smooth<double>(h, lvl, smoother, sweeps, omega, smoother == RT_SMOOTH_SGS);
 }
 
@@ -1019,7 +1032,7 @@ extern "C" int rt_coarsest_solve(rt_hier* h) {
 
 extern "C" int rt_apply_K_dev(rt_hier* h, const double* u, double* out) {
     if (!h || !u || !out) return RT_EINVAL;
-    RT_CHECK(rtk::penalty_weights(h));
+    RT_CHECK(refresh_fine(h));
     return rtk::fine_applyK<double>(h, u, out);
 }
 
@@ -1579,5 +1592,113 @@ extern "C" int rt_oc_iteration(rt_hier* h, int method, int k, double inner_tol, 
     RT_CHECK(rt_sensitivity(h, 1));
     RT_CHECK(rt_oc_update(h, vgoal, nullptr, nullptr));
     if (compliance_out) *compliance_out = lam;
+    return RT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// launch-shape autotuner for the finest-level kernels
+// ---------------------------------------------------------------------------
+static double time_fine_kernel(rt_hier* h, int prec, int mode, int reps) {
+    rt_ctx* c = h->ctx;
+    rt_level& L = h->L[0];
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const double* lmax = h->stencil_ready ? h->scal + RT_SCAL_LMAX : h->scal + 299;
+    auto run = [&]() -> int {
+        if (prec == 1) {
+            double *u = h->x, *f = h->q, *o = h->z, *d = h->p;
+            switch (mode) {
+                case 0: return rtk::fine_residual<double>(h, u, f, o);
+                case 1: return rtk::fine_applyK<double>(h, u, o);
+                case 2: return rtk::fine_jacobi<double>(h, u, f, o, 0.6);
+                default: return rtk::fine_cheby<double>(h, u, f, o, d, lmax, 1);
+            }
+        }
+        float *u = L.u32, *f = L.f32, *o = L.r32, *d = L.d32;
+        switch (mode) {
+            case 0: return rtk::fine_residual<float>(h, u, f, o);
+            case 1: return rtk::fine_applyK<float>(h, u, o);
+            case 2: return rtk::fine_jacobi<float>(h, u, f, o, 0.6);
+            default: return rtk::fine_cheby<float>(h, u, f, o, d, lmax, 1);
+        }
+    };
+    double best = 1e30;
+    if (run() == RT_OK) {  // warm-up
+        cudaEventRecord(a, c->stream);
+        bool ok = true;
+        for (int i = 0; i < reps && ok; i++) ok = run() == RT_OK;
+        cudaEventRecord(b, c->stream);
+        cudaEventSynchronize(b);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        if (ok) best = ms * 1e3 / reps;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return best;
+}
+
+extern "C" int rt_autotune(rt_hier* h, int reps) {
+    if (!h) return RT_EINVAL;
+    if (reps <= 0) reps = 5;
+    rt_ctx* c = h->ctx;
+    rt_level& L = h->L[0];
+    const long n = 3 * L.nv;
+    const bool was_profiling = c->profile;
+    c->profile = false;
+    // inputs: random u, f on the solver's scratch vectors (their contents do not persist across calls)
+    RT_CHECK(refresh_fine(h));
+    RT_CHECK(rtk::rng_uniform(h, 0xa770, n, h->x));
+    RT_CHECK(rtk::rng_uniform(h, 0xa771, n, h->q));
+    RT_CHECK(rtk::d2f(h, n, h->x, L.u32));
+    RT_CHECK(rtk::d2f(h, n, h->q, L.f32));
+    RT_CUDA(c, cudaMemsetAsync(h->p, 0, sizeof(double) * n, c->stream));
+    RT_CUDA(c, cudaMemsetAsync(L.d32, 0, sizeof(float) * n, c->stream));
+    if (!h->stencil_ready) {
+        const double one = 2.0;
+        RT_CUDA(c, cudaMemcpyAsync(h->scal + 299, &one, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    }
+    std::vector<rt_tile_cfg> cands;
+    for (int ty : {2, 4, 8})
+        for (int zc : {4, 8, 16, 32, 64}) cands.push_back(rt_tile_cfg{1, ty, zc});
+    for (int zc : {8, 16, 32}) cands.push_back(rt_tile_cfg{0, 4, zc});
+    for (int prec = 0; prec < 2; prec++)
+        for (int mode = 0; mode < 4; mode++) {
+            rt_tile_cfg best_cfg = h->tune[prec][mode];
+            double best = 1e30;
+            for (const rt_tile_cfg& cfg : cands) {
+                if (cfg.zchunk > 2 * L.vz && cfg.zchunk != 4) continue;
+                h->tune[prec][mode] = cfg;
+                const double t = time_fine_kernel(h, prec, mode, reps);
+                if (t < best) { best = t; best_cfg = cfg; }
+            }
+            h->tune[prec][mode] = best_cfg;
+            h->tune_us[prec][mode] = best;
+        }
+    cudaGetLastError();
+    h->graph_epoch++;  // launch shapes are baked into captured graphs
+    c->profile = was_profiling;
+    return RT_OK;
+}
+
+extern "C" int rt_tuning_info(rt_hier* h, int precision, int mode, int* variant, int* ty, int* zchunk, double* us) {
+    if (!h || precision < 0 || precision > 1 || mode < 0 || mode > 3) return RT_EINVAL;
+    const int pr = precision == RT_FP64 ? 1 : 0;
+    const rt_tile_cfg& t = h->tune[pr][mode];
+    if (variant) *variant = t.variant;
+    if (ty) *ty = t.ty;
+    if (zchunk) *zchunk = t.zchunk;
+    if (us) *us = h->tune_us[pr][mode];
+    return RT_OK;
+}
+
+extern "C" int rt_set_tuning(rt_hier* h, int precision, int mode, int variant, int ty, int zchunk) {
+    if (!h || precision < 0 || precision > 1 || mode < 0 || mode > 3 || variant < 0 || variant > 1 || zchunk < 1)
+        return RT_EINVAL;
+    if (variant == 1 && ty != 2 && ty != 4 && ty != 8) return rt_fail(h->ctx, RT_EINVAL, "rows per tile must be 2, 4 or 8");
+    const int pr = precision == RT_FP64 ? 1 : 0;
+    h->tune[pr][mode] = rt_tile_cfg{variant, variant == 1 ? ty : 4, zchunk};
+    h->graph_epoch++;
     return RT_OK;
 }

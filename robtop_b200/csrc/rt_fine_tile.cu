@@ -21,6 +21,7 @@
 //    rule of the reference falls out of the data.
 #include <cuda_runtime.h>
 
+#include "rt_element.cuh"
 #include "rt_internal.h"
 
 namespace {
@@ -32,50 +33,6 @@ constexpr int NE_T = EXT * EYT;            // 165 elements per layer
 constexpr int NU_T = UXT * UYT;            // 204 nodes per layer
 constexpr int TILE_BS = 192;               // >= NE_T, multiple of 32
 constexpr int U_PER_T = (NU_T + TILE_BS - 1) / TILE_BS;  // halo nodes loaded per thread (2)
-
-// sparsity pattern of Kt = T^T KE T / 64 (rows/cols index 3*mode + comp)
-__device__ constexpr int KT_R[45] = {3, 3, 3, 4, 4, 5, 5, 6, 6, 7, 7, 7, 8, 8, 9, 9, 10, 10, 11, 11, 11, 12, 12,
-                                     13, 13, 14, 14, 14, 15, 15, 16, 16, 16, 17, 17, 18, 18, 18, 19, 19, 20, 20, 21,
-                                     22, 23};
-__device__ constexpr int KT_C[45] = {3, 7, 14, 4, 6, 5, 12, 4, 6, 3, 7, 14, 8, 13, 9, 20, 10, 17, 11, 16, 18, 5, 12,
-                                     8, 13, 3, 7, 14, 15, 19, 11, 16, 18, 10, 17, 11, 16, 18, 15, 19, 9, 20, 21, 22,
-                                     23};
-
-template <typename T>
-struct KtVals {
-    T v[45];
-    T diag_a, diag_b;  // KE diagonal block of any vertex: a I + b (s s^T - I), s = vertex reflection signs
-};
-
-// 8-point Sylvester-Hadamard over the vertex bits (x, y, z) of one component
-template <typename T>
-__device__ __forceinline__ void hadamard8(T* a, int c) {
-#pragma unroll
-    for (int bit = 1; bit < 8; bit <<= 1)
-#pragma unroll
-        for (int i = 0; i < 8; i++)
-            if (!(i & bit)) {
-                const T p = a[3 * i + c], q = a[3 * (i | bit) + c];
-                a[3 * i + c] = p + q;
-                a[3 * (i | bit) + c] = p - q;
-            }
-}
-
-// ye = w * KE * ue, ue/ye indexed 3*vertex + comp
-template <typename T>
-__device__ __forceinline__ void element_apply(T* a, const KtVals<T>& kt, T w) {
-#pragma unroll
-    for (int c = 0; c < 3; c++) hadamard8(a, c);
-    T z[24];
-#pragma unroll
-    for (int i = 0; i < 24; i++) z[i] = T(0);
-#pragma unroll
-    for (int k = 0; k < 45; k++) z[KT_R[k]] += kt.v[k] * a[KT_C[k]];
-#pragma unroll
-    for (int i = 0; i < 24; i++) a[i] = w * z[i];
-#pragma unroll
-    for (int c = 0; c < 3; c++) hadamard8(a, c);
-}
 
 template <typename T>
 struct TileSmem {
@@ -91,7 +48,7 @@ template <typename T, bool WS, int MODE>
 __global__ void __launch_bounds__(TILE_BS, sizeof(T) == 8 ? 2 : 4) k_fine_tile(int nx, int ny, int nz, int zchunk,
                                                         const uint8_t* __restrict__ vact,
                                                         const float* __restrict__ wgt,
-                                                        const uint8_t* __restrict__ vfix, const KtVals<T> kt,
+                                                        const uint8_t* __restrict__ vfix, const rte::KtVals<T> kt,
                                                         const T* __restrict__ u, const T* __restrict__ f,
                                                         T* __restrict__ out, T omega, T* __restrict__ dvec,
                                                         const double* __restrict__ lmax, int kstep) {
@@ -227,7 +184,7 @@ __global__ void __launch_bounds__(TILE_BS, sizeof(T) == 8 ? 2 : 4) k_fine_tile(i
                     a[3 * vtx + 1] = src[NU_T + idx];
                     a[3 * vtx + 2] = src[2 * NU_T + idx];
                 }
-                element_apply(a, kt, T(wv));
+                rte::element_apply(a, kt, T(wv));
             } else {
 #pragma unroll
                 for (int q = 0; q < 24; q++) a[q] = T(0);
@@ -331,41 +288,6 @@ __global__ void __launch_bounds__(TILE_BS, sizeof(T) == 8 ? 2 : 4) k_fine_tile(i
     }
 }
 
-template <typename T>
-KtVals<T> make_kt(const rt_hier* h) {
-    // Kt = T^T KE T / 64 with T = H (x) I3, H the 8x8 Sylvester-Hadamard over vertex bits
-    static const int R[45] = {3, 3, 3, 4, 4, 5, 5, 6, 6, 7, 7, 7, 8, 8, 9, 9, 10, 10, 11, 11, 11, 12, 12,
-                              13, 13, 14, 14, 14, 15, 15, 16, 16, 16, 17, 17, 18, 18, 18, 19, 19, 20, 20, 21,
-                              22, 23};
-    static const int Cc[45] = {3, 7, 14, 4, 6, 5, 12, 4, 6, 3, 7, 14, 8, 13, 9, 20, 10, 17, 11, 16, 18, 5, 12,
-                               8, 13, 3, 7, 14, 15, 19, 11, 16, 18, 10, 17, 11, 16, 18, 15, 19, 9, 20, 21, 22,
-                               23};
-    KtVals<T> k;
-    for (int q = 0; q < 45; q++) {
-        const int m = R[q] / 3, c = R[q] % 3, n = Cc[q] / 3, d = Cc[q] % 3;
-        double s = 0;
-        for (int i = 0; i < 8; i++)
-            for (int j = 0; j < 8; j++) {
-                const double hmi = (__builtin_popcount(m & i) & 1) ? -1.0 : 1.0;
-                const double hnj = (__builtin_popcount(n & j) & 1) ? -1.0 : 1.0;
-                s += hmi * h->KE[(3 * i + c) * 24 + 3 * j + d] * hnj;
-            }
-        k.v[q] = (T)(s / 64.0);
-    }
-    k.diag_a = (T)h->KE[0];
-    k.diag_b = (T)h->KE[1];
-    return k;
-}
-
-int tile_zchunk(rt_ctx* c, int vx, int vy, int vz) {
-    const long tiles = (long)((vx + TX - 1) / TX) * ((vy + TY - 1) / TY);
-    const long target = (long)c->sm_count * 4;  // ~4 resident CTAs per SM
-    long chunks = (target + tiles - 1) / tiles;
-    if (chunks < 1) chunks = 1;
-    int zc = (int)((vz + chunks - 1) / chunks);
-    if (zc < 8) zc = 8;
-    return zc;
-}
 
 template <typename T, bool WS, int MODE>
 int launch_tile(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name, T* dvec = nullptr,
@@ -373,9 +295,9 @@ int launch_tile(rt_hier* h, const T* u, const T* f, T* out, double omega, const 
     rt_level& L = h->L[0];
     const size_t smem = sizeof(TileSmem<T>);
     auto kern = k_fine_tile<T, WS, MODE>;
-    const int zc = tile_zchunk(h->ctx, L.vx, L.vy, L.vz);
+    const int zc = h->tune[sizeof(T) == 8 ? 1 : 0][MODE].zchunk;
     dim3 grid((L.vx + TX - 1) / TX, (L.vy + TY - 1) / TY, (L.vz + zc - 1) / zc);
-    const KtVals<T> kt = make_kt<T>(h);
+    const rte::KtVals<T> kt = rte::make_kt<T>(h);
     return rt_launch(h->ctx, name, [&] {
         kern<<<grid, TILE_BS, smem, h->ctx->stream>>>(L.nx, L.ny, L.nz, zc, L.vact, h->w, h->vfix, kt, u, f, out,
                                                       (T)omega, dvec, lmax, kstep);
@@ -413,14 +335,31 @@ int init_tile_kernels(rt_ctx* c) {
     return RT_OK;
 }
 
+// default launch shape (rt_autotune refines it): enough z-chunks for ~4 tiles per SM
+int tile_zchunk_default(rt_ctx* c, int vx, int vy, int vz) {
+    const long tiles = (long)((vx + 29) / 30) * ((vy + 3) / 4);
+    const long target = (long)c->sm_count * 16;  // marching kernel: 4 warps per CTA, ~16 warps per SM
+    long chunks = (target + tiles - 1) / tiles;
+    if (chunks < 1) chunks = 1;
+    int zc = (int)((vz + chunks - 1) / chunks);
+    return zc < 8 ? 8 : zc;
+}
+
+template <typename T>
+static bool use_march(rt_hier* h, int mode) {
+    return h->tune[sizeof(T) == 8 ? 1 : 0][mode].variant == 1;
+}
+
 template <typename T>
 int fine_residual(rt_hier* h, const T* u, const T* f, T* r) {
+    if (use_march<T>(h, 0)) return fine_march<T, 0>(h, u, f, r, 0.0, nullptr, nullptr, 0);
     const char* nm = sizeof(T) == 8 ? "fine_residual_f64" : "fine_residual_f32";
     return h->has_support ? launch_tile<T, true, 0>(h, u, f, r, 0.0, nm) : launch_tile<T, false, 0>(h, u, f, r, 0.0, nm);
 }
 
 template <typename T>
 int fine_applyK(rt_hier* h, const T* u, T* out) {
+    if (use_march<T>(h, 1)) return fine_march<T, 1>(h, u, nullptr, out, 0.0, nullptr, nullptr, 0);
     const char* nm = sizeof(T) == 8 ? "fine_applyK_f64" : "fine_applyK_f32";
     return h->has_support ? launch_tile<T, true, 1>(h, u, nullptr, out, 0.0, nm)
                           : launch_tile<T, false, 1>(h, u, nullptr, out, 0.0, nm);
@@ -428,6 +367,7 @@ int fine_applyK(rt_hier* h, const T* u, T* out) {
 
 template <typename T>
 int fine_jacobi(rt_hier* h, const T* u, const T* f, T* unew, double omega) {
+    if (use_march<T>(h, 2)) return fine_march<T, 2>(h, u, f, unew, omega, nullptr, nullptr, 0);
     const char* nm = sizeof(T) == 8 ? "fine_jacobi_f64" : "fine_jacobi_f32";
     return h->has_support ? launch_tile<T, true, 2>(h, u, f, unew, omega, nm)
                           : launch_tile<T, false, 2>(h, u, f, unew, omega, nm);
@@ -435,6 +375,7 @@ int fine_jacobi(rt_hier* h, const T* u, const T* f, T* unew, double omega) {
 
 template <typename T>
 int fine_cheby(rt_hier* h, const T* u, const T* f, T* unew, T* d, const double* lmax, int kstep) {
+    if (use_march<T>(h, 3)) return fine_march<T, 3>(h, u, f, unew, 0.0, d, lmax, kstep);
     const char* nm = sizeof(T) == 8 ? "fine_cheby_f64" : "fine_cheby_f32";
     return h->has_support ? launch_tile<T, true, 3>(h, u, f, unew, 0.0, nm, d, lmax, kstep)
                           : launch_tile<T, false, 3>(h, u, f, unew, 0.0, nm, d, lmax, kstep);

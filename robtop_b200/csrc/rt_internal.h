@@ -57,9 +57,20 @@ struct rt_level {
     float* dvec32 = nullptr;
 };
 
+// launch shape of a finest-level operator kernel (chosen by rt_autotune)
+struct rt_tile_cfg {
+    int variant = 1;  // 0: shared-memory element tile (rt_fine_tile.cu), 1: register marching (rt_fine_march.cu)
+    int ty = 4;       // node rows per warp tile (marching kernel: 2, 4 or 8)
+    int zchunk = 16;  // node layers per tile
+};
+
 struct rt_hier {
     rt_ctx* ctx = nullptr;
     rt_params P;
+    rt_tile_cfg tune[2][4];          // [FP32, FP64][residual, applyK, jacobi, chebyshev]
+    double tune_us[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};  // measured time of the chosen shape
+    double* dinv64 = nullptr;        // [6][nv] inverted diagonal blocks of the finest level
+    float* dinv32 = nullptr;
     std::vector<rt_level> L;
     double KE[576];
     double* KE_dev = nullptr;
@@ -176,6 +187,10 @@ template <typename T>
 int st_cheby(rt_hier* h, int lvl, const T* u, const T* f, T* unew, T* d, const double* lmax, int kstep);
 int penalty_weights(rt_hier* h);
 int init_tile_kernels(rt_ctx* c);
+int fine_dinv(rt_hier* h);
+template <typename T, int MODE>
+int fine_march(rt_hier* h, const T* u, const T* f, T* out, double omega, T* dvec, const double* lmax, int kstep);
+int tile_zchunk_default(rt_ctx* c, int vx, int vy, int vz);
 // stencil levels
 template <typename T>
 int st_residual(rt_hier* h, int lvl, const T* u, const T* f, T* r);

@@ -311,6 +311,19 @@ class HierarchyGrid:
     def update_stencil(self):
         self._c(A.lib().rt_update_stencil(self._h))
 
+    def autotune(self, reps=5):
+        """Choose the finest-level kernel launch shapes (rt_autotune); returns them per kernel."""
+        self._c(A.lib().rt_autotune(self._h, reps))
+        out = {}
+        names = ["residual", "applyK", "jacobi", "chebyshev"]
+        for prec, pname in ((A.FP32, "f32"), (A.FP64, "f64")):
+            for m, mname in enumerate(names):
+                v, ty, zc, us = C.c_int(), C.c_int(), C.c_int(), C.c_double()
+                self._c(A.lib().rt_tuning_info(self._h, prec, m, C.byref(v), C.byref(ty), C.byref(zc), C.byref(us)))
+                out[f"{mname}_{pname}"] = {"variant": ["smem_tile", "register_march"][v.value], "rows": ty.value,
+                                           "zchunk": zc.value, "us": round(us.value, 2)}
+        return out
+
     def smoother_lmax(self, level):
         v = C.c_double()
         self._c(A.lib().rt_smoother_lmax(self._h, level, C.byref(v)))

@@ -95,6 +95,52 @@ def test_fine_smoothers(pair, smoother):
     assert rel_err(G[0].getDisplacement(), uo) < 1e-10
 
 
+@pytest.mark.parametrize("variant,ty,zc", [(0, 4, 8), (1, 2, 4), (1, 4, 16), (1, 8, 7), (1, 4, 1)])
+def test_fine_kernel_variants(pair, variant, ty, zc):
+    """Every launch shape of both finest-level kernels (shared-memory tile, register
+    marching) gives the oracle's residual, K u, Jacobi and Chebyshev results."""
+    cfg, ctx, G, H = pair
+    import ctypes as C
+
+    for m in range(4):
+        rb._capi.check(rb.lib().rt_set_tuning(G.handle, rb.FP64, m, variant, ty, zc), ctx.handle)
+    u, f = _rand_vec(G, 0, 210), _rand_vec(G, 0, 211)
+    G[0].setDisplacement(u)
+    G[0].setForce(f)
+    G[0].update_residual()
+    r_or = np.zeros_like(u)
+    O.lib().or_fine_residual(H.lv(0), O.ptr(H.KE), O.ptr(u), O.ptr(f), O.ptr(r_or))
+    assert rel_err(G[0].getResidual(), r_or) < FP64_TOL
+    assert rel_err(G[0].applyK(u), H.applyK(u)) < FP64_TOL
+    G[0].smooth(rb.SMOOTH_JACOBI, 1, 0.6)
+    uo, tmp = u.copy(), np.zeros_like(u)
+    O.lib().or_fine_jacobi(H.lv(0), O.ptr(H.KE), O.ptr(uo), O.ptr(f), 0.6, O.ptr(tmp))
+    assert rel_err(G[0].getDisplacement(), uo) < 1e-10
+    H.set_lmax([G.smoother_lmax(i) for i in range(H.nlev - 1)])
+    G[0].setDisplacement(u)
+    G[0].smooth(rb.SMOOTH_CHEBY, 2)
+    uo, un, d = u.copy(), np.zeros_like(u), np.zeros_like(u)
+    for k in range(2):
+        O.lib().or_fine_cheby(H.lv(0), O.ptr(H.KE), O.ptr(uo), O.ptr(f), O.ptr(un), O.ptr(d), k)
+        uo, un = un, uo
+    assert rel_err(G[0].getDisplacement(), uo) < 1e-9
+    for m in range(4):  # back to the default shape
+        rb._capi.check(rb.lib().rt_set_tuning(G.handle, rb.FP64, m, 1, 4, 16), ctx.handle)
+
+
+def test_autotune_keeps_results(pair):
+    cfg, ctx, G, H = pair
+    shapes = G.autotune(reps=2)
+    assert set(shapes) >= {"residual_f32", "chebyshev_f64"}
+    u, f = _rand_vec(G, 0, 220), _rand_vec(G, 0, 221)
+    G[0].setDisplacement(u)
+    G[0].setForce(f)
+    G[0].update_residual()
+    r_or = np.zeros_like(u)
+    O.lib().or_fine_residual(H.lv(0), O.ptr(H.KE), O.ptr(u), O.ptr(f), O.ptr(r_or))
+    assert rel_err(G[0].getResidual(), r_or) < FP64_TOL
+
+
 def test_galerkin_stencils(pair):
     cfg, ctx, G, H = pair
     for i in range(1, H.nlev):
