@@ -300,6 +300,19 @@ def run_kernel(args):
     u = np.random.default_rng(0).standard_normal(3 * G[0].nv) * np.tile(G[0].getVact(), 3)
     G[0].setDisplacement(u)
     G[0].setForce(u[::-1].copy())
+    if args.kernel in ("fine_cheby_f32", "fine_residual_f64", "fine_applyK_f64", "fine_residual_f32"):
+        # one finest-level kernel at the autotuned launch shape, timed by the library (CUDA events)
+        shapes = G.autotune()
+        prec = rb.FP32 if args.kernel.endswith("f32") else rb.FP64
+        mode = {"fine_residual": 0, "fine_applyK": 1, "fine_cheby": 3}[args.kernel.rsplit("_", 1)[0]]
+        us = C.c_double()
+        rb._capi.check(rb.lib().rt_bench_fine_kernel(G.handle, prec, mode, args.warmup, C.byref(us)), ctx.handle)
+        rb._capi.check(rb.lib().rt_bench_fine_kernel(G.handle, prec, mode, args.steps, C.byref(us)), ctx.handle)
+        key = {0: "residual", 1: "applyK", 3: "chebyshev"}[mode] + ("_f32" if prec == rb.FP32 else "_f64")
+        print(json.dumps({"kernel": args.kernel, "us_per_call": us.value, "nodes": G[0].nv, "shape": shapes[key]}))
+        G.close()
+        ctx.close()
+        return 0
     ops = {"fine_residual": lambda: G[0].update_residual(),
            "fine_jacobi": lambda: G[0].smooth(rb.SMOOTH_JACOBI, 1, 0.6),
            "st_residual": lambda: G[1].update_residual()}
@@ -325,7 +338,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--kernel", default=None, choices=["fine_residual", "fine_jacobi", "st_residual"])
+    ap.add_argument("--kernel", default=None, choices=["fine_residual", "fine_jacobi", "st_residual", "fine_cheby_f32",
+                                                      "fine_residual_f64", "fine_applyK_f64", "fine_residual_f32"])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

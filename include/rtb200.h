@@ -207,6 +207,9 @@ int rt_autotune(rt_hier* h, int reps);
 int rt_tuning_info(rt_hier* h, int precision, int mode, int* variant, int* ty, int* zchunk, double* us);
 /* set a finest-level kernel's launch shape explicitly (ty: 2, 4 or 8 rows for variant 1) */
 int rt_set_tuning(rt_hier* h, int precision, int mode, int variant, int ty, int zchunk);
+/* time reps launches of one finest-level kernel at its current shape on random data
+ * (device time per launch in microseconds, CUDA events on the context stream) */
+int rt_bench_fine_kernel(rt_hier* h, int precision, int mode, int reps, double* us_per_launch);
 
 /* ---- solvers -------------------------------------------------------------- */
 /* MG-preconditioned CG on level 0: u <- K^-1 f to ||r||/||f|| <= tol (solveFEM's role,

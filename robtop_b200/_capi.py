@@ -102,6 +102,7 @@ SIGNATURES = {
     "rt_autotune": (I, [P, I]),
     "rt_tuning_info": (I, [P, I, I, C.POINTER(I), C.POINTER(I), C.POINTER(I), C.POINTER(D)]),
     "rt_set_tuning": (I, [P, I, I, I, I, I]),
+    "rt_bench_fine_kernel": (I, [P, I, I, I, C.POINTER(D)]),
     "rt_pcg": (I, [P, D, I, C.POINTER(SolveInfo)]),
     "rt_worst_case": (I, [P, I, I, D, C.c_uint64, C.POINTER(D), C.POINTER(SolveInfo)]),
     "rt_sensitivity": (I, [P, I]),

@@ -1702,3 +1702,23 @@ extern "C" int rt_set_tuning(rt_hier* h, int precision, int mode, int variant, i
     h->graph_epoch++;
     return RT_OK;
 }
+
+extern "C" int rt_bench_fine_kernel(rt_hier* h, int precision, int mode, int reps, double* us_per_launch) {
+    if (!h || precision < 0 || precision > 1 || mode < 0 || mode > 3 || reps < 1) return RT_EINVAL;
+    rt_ctx* c = h->ctx;
+    rt_level& L = h->L[0];
+    const long n = 3 * L.nv;
+    RT_CHECK(refresh_fine(h));
+    RT_CHECK(rtk::rng_uniform(h, 0xbe7c, n, h->x));
+    RT_CHECK(rtk::rng_uniform(h, 0xbe7d, n, h->q));
+    RT_CHECK(rtk::d2f(h, n, h->x, L.u32));
+    RT_CHECK(rtk::d2f(h, n, h->q, L.f32));
+    if (!h->stencil_ready) {
+        const double two = 2.0;
+        RT_CUDA(c, cudaMemcpyAsync(h->scal + 299, &two, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    }
+    const double t = time_fine_kernel(h, precision == RT_FP64 ? 1 : 0, mode, reps);
+    if (t >= 1e30) return rt_fail(c, RT_ECUDA, "kernel launch failed");
+    if (us_per_launch) *us_per_launch = t;
+    return RT_OK;
+}
