@@ -99,8 +99,9 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def build_problem(rb, configs, ctx, precision):
-    cfg = configs.worst_case_box(WORKLOAD["nx"], WORKLOAD["ny"], WORKLOAD["nz"], seed=WORKLOAD["seed"])
+def build_problem(rb, configs, ctx, precision, dims=None):
+    nx, ny, nz = dims or (WORKLOAD["nx"], WORKLOAD["ny"], WORKLOAD["nz"])
+    cfg = configs.worst_case_box(nx, ny, nz, seed=WORKLOAD["seed"])
     params = rb.default_params(mode=cfg["mode"], youngs_modulus=1e6, poisson_ratio=0.4, power_penalty=3.0,
                                min_rho=1e-3, precision=precision, smoother=rb.SMOOTH_SGS, pre_sweeps=1,
                                post_sweeps=1)
@@ -295,16 +296,24 @@ def run_kernel(args):
     from robtop_b200 import configs
 
     ctx = rb.Context(0)
-    cfg, G = build_problem(rb, configs, ctx, rb.FP64)
+    dims = tuple(int(v) for v in args.size.split("x")) if args.size else None
+    cfg, G = build_problem(rb, configs, ctx, rb.FP64, dims)
     G.update_stencil()
     u = np.random.default_rng(0).standard_normal(3 * G[0].nv) * np.tile(G[0].getVact(), 3)
     G[0].setDisplacement(u)
     G[0].setForce(u[::-1].copy())
     if args.kernel in ("fine_cheby_f32", "fine_residual_f64", "fine_applyK_f64", "fine_residual_f32"):
-        # one finest-level kernel at the autotuned launch shape, timed by the library (CUDA events)
-        shapes = G.autotune()
+        # one finest-level kernel at the autotuned (or a given) launch shape, timed by the library (CUDA events)
         prec = rb.FP32 if args.kernel.endswith("f32") else rb.FP64
         mode = {"fine_residual": 0, "fine_applyK": 1, "fine_cheby": 3}[args.kernel.rsplit("_", 1)[0]]
+        if args.shape:
+            variant, ty, zc = (int(v) for v in args.shape.split(","))
+            rb._capi.check(rb.lib().rt_set_tuning(G.handle, prec, mode, variant, ty, zc), ctx.handle)
+            names = ["residual", "applyK", "jacobi", "chebyshev"]
+            shapes = {f"{names[mode]}_{'f32' if prec == rb.FP32 else 'f64'}":
+                      {"variant": ["smem_tile", "register_march"][variant], "rows": ty, "zchunk": zc}}
+        else:
+            shapes = G.autotune()
         us = C.c_double()
         rb._capi.check(rb.lib().rt_bench_fine_kernel(G.handle, prec, mode, args.warmup, C.byref(us)), ctx.handle)
         rb._capi.check(rb.lib().rt_bench_fine_kernel(G.handle, prec, mode, args.steps, C.byref(us)), ctx.handle)
@@ -338,8 +347,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--forms", default="both", choices=["both", "mixed"],
+                    help="mixed: time only the mixed form (short command for launch-list captures)")
     ap.add_argument("--kernel", default=None, choices=["fine_residual", "fine_jacobi", "st_residual", "fine_cheby_f32",
                                                       "fine_residual_f64", "fine_applyK_f64", "fine_residual_f32"])
+    ap.add_argument("--size", default=None, help="kernel mode: grid NXxNYxNZ (default: the bench workload)")
+    ap.add_argument("--shape", default=None, help="kernel mode: launch shape variant,rows,zchunk (default: autotune)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -373,7 +386,7 @@ def main():
     G.update_stencil()
     tuning = G.autotune()
     results = {}
-    for prec in (rb.FP64, rb.FP32):
+    for prec in ((rb.FP64, rb.FP32) if args.forms == "both" else (rb.FP32,)):
         form = FORMS["plain" if prec == rb.FP64 else "mixed"]
         p = G.params
         p.precision = prec
@@ -408,11 +421,11 @@ def main():
     # end to end through the public API with host buffers
     e2e_ms, h2d, d2h = e2e_steps(rb, ctx, G, cfg, args.steps)
 
-    r32, r64 = results[rb.FP32], results[rb.FP64]
+    r32, r64 = results[rb.FP32], results.get(rb.FP64)
     ms_step = r32["ms"] / args.steps
     value = ws * args.steps / (r32["ms"] * 1e-3)
     lam32 = float(np.mean(r32["lams"]))
-    lam64 = float(np.mean(r64["lams"]))
+    lam64 = float(np.mean(r64["lams"])) if r64 else None
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -421,12 +434,12 @@ def main():
                                "wsff), Lanczos k=16, inner MG-PCG to 1e-6, stencil assembly included",
                    "form": "mixed: FP32 V-cycle (Chebyshev(4) smoothing) inside FP64 flexible CG, one CUDA "
                            "graph per solve; plain (fp64_ms_per_step): FP64 symmetric-GS V-cycle",
-                   "fp64_ms_per_step": r64["ms"] / args.steps,
-                   "speedup_vs_fp64": r64["ms"] / r32["ms"],
+                   "fp64_ms_per_step": r64["ms"] / args.steps if r64 else None,
+                   "speedup_vs_fp64": r64["ms"] / r32["ms"] if r64 else None,
                    "lambda_mixed": lam32, "lambda_fp64": lam64,
-                   "lambda_rel_diff": abs(lam32 - lam64) / abs(lam64),
+                   "lambda_rel_diff": abs(lam32 - lam64) / abs(lam64) if r64 else None,
                    "inner_pcg_iterations": r32["infos"][0]["inner_iterations"],
-                   "inner_pcg_iterations_fp64": r64["infos"][0]["inner_iterations"],
+                   "inner_pcg_iterations_fp64": r64["infos"][0]["inner_iterations"] if r64 else None,
                    "l2": "working set ~0.4 GB of vectors and stencils > 126 MB L2 per step",
                    "parallelism": f"replicas x{ws}",
                    "tile_shapes": tuning},

@@ -61,7 +61,7 @@ enum rt_layout { RT_LAYOUT_DENSE = 0, RT_LAYOUT_REF_GS = 1 };
 enum rt_field { RT_FIELD_U = 0, RT_FIELD_F = 1, RT_FIELD_R = 2, RT_FIELD_RHO = 3, RT_FIELD_SENS = 4,
                 RT_FIELD_STENCIL = 5, RT_FIELD_VACT = 6, RT_FIELD_EACT = 7, RT_FIELD_VFIX = 8,
                 RT_FIELD_PENALTY = 9 /* level-0 element weights powf(rho, p), FP32, refreshed by rt_update_stencil */ };
-enum rt_worst_method { RT_WORST_MODPM = 0, RT_WORST_LANCZOS = 1 };
+enum rt_worst_method { RT_WORST_MODPM = 0, RT_WORST_LANCZOS = 1, RT_WORST_BLOCK_LANCZOS = 2 };
 
 /* Parameter block: optimization/optimization.h:11-22 plus the solver knobs the
  * reference hard-codes (GS 1/1 sweeps, optimization/optimization.cpp:169). */
@@ -221,6 +221,27 @@ int rt_pcg(rt_hier* h, double tol, int maxit, rt_solve_info* info);
  * On return level-0 f holds the worst-case load and u = K^-1 f. */
 int rt_worst_case(rt_hier* h, int method, int k, double inner_tol, uint64_t seed, double* lambda,
                   rt_solve_info* info);
+/* RT_WORST_BLOCK_LANCZOS (rt_worst_case with k = Krylov dimension, block size 8) or this call:
+ * block Lanczos with block_size starting loads and n_blocks block steps; each step's
+ * block_size inner MG-PCG solves run concurrently as one batched CUDA graph (rt_pcg_batch)
+ * on solve workspaces the hierarchy keeps.  Replaces the same role as rt_worst_case
+ * (modifiedPM, optimization/optimization.cpp:123-261); no reference counterpart for the block form. */
+int rt_worst_case_block(rt_hier* h, int block_size, int n_blocks, double inner_tol, uint64_t seed,
+                        double* lambda, rt_solve_info* info);
+
+/* ---- independent solves in one launch ------------------------------------- */
+/* A solve workspace of `parent`: its own u/f/r and solver vectors on every level, the
+ * parent's operator (densities, supports, stencils, coarsest inverse, launch shapes).
+ * It accepts rt_put/rt_get of U, F, R, the level operators, rt_vcycle, rt_pcg and
+ * rt_pcg_batch; calls that change the operator return RT_ESTATE.  Destroy it (with
+ * rt_hier_destroy) before its parent.  No reference counterpart: the reference keeps one
+ * global hierarchy (optimization/optimization.cpp:10). */
+int rt_hier_workspace_create(rt_hier* parent, rt_hier** out);
+/* rt_pcg on n hierarchies or workspaces of one context in ONE graph launch: every
+ * instance's set-up and its WHILE-conditional PCG loop are independent branches of a
+ * captured CUDA graph (cached per instance set), so the GPU runs them concurrently.
+ * infos[i] as rt_pcg's; seconds is the whole batch. */
+int rt_pcg_batch(rt_hier* const* hs, int n, double tol, int maxit, rt_solve_info* infos);
 
 /* ---- optimisation step (optimization/optimization.cu) --------------------- */
 /* computeSensitivity (optimization/optimization.cu:109-133) including the filter */

@@ -10,7 +10,8 @@ reference's interfaces:
 """
 from . import _capi  # noqa: F401
 from ._capi import (FP32, FP64, LAYOUT_DENSE, LAYOUT_REF_GS, MODE_NSCF, MODE_NSFF, MODE_WSCF, MODE_WSFF,  # noqa: F401
-                    SMOOTH_CHEBY, SMOOTH_GS, SMOOTH_JACOBI, SMOOTH_SGS, WORST_LANCZOS, WORST_MODPM, RTError, lib)
-from .grid import Context, Grid, HierarchyGrid, default_params  # noqa: F401
+                    SMOOTH_CHEBY, SMOOTH_GS, SMOOTH_JACOBI, SMOOTH_SGS, WORST_BLOCK_LANCZOS, WORST_LANCZOS, WORST_MODPM,
+                    RTError, lib)
+from .grid import Context, Grid, HierarchyGrid, default_params, pcg_batch  # noqa: F401
 
-__all__ = ["Context", "Grid", "HierarchyGrid", "default_params", "lib", "RTError"]
+__all__ = ["Context", "Grid", "HierarchyGrid", "default_params", "pcg_batch", "lib", "RTError"]

@@ -20,7 +20,7 @@ FP64, FP32 = 0, 1
 LAYOUT_DENSE, LAYOUT_REF_GS = 0, 1
 FIELD_U, FIELD_F, FIELD_R, FIELD_RHO, FIELD_SENS, FIELD_STENCIL, FIELD_VACT, FIELD_EACT, FIELD_VFIX, \
     FIELD_PENALTY = range(10)
-WORST_MODPM, WORST_LANCZOS = 0, 1
+WORST_MODPM, WORST_LANCZOS, WORST_BLOCK_LANCZOS = 0, 1, 2
 
 
 class Params(C.Structure):
@@ -105,6 +105,9 @@ SIGNATURES = {
     "rt_bench_fine_kernel": (I, [P, I, I, I, C.POINTER(D)]),
     "rt_pcg": (I, [P, D, I, C.POINTER(SolveInfo)]),
     "rt_worst_case": (I, [P, I, I, D, C.c_uint64, C.POINTER(D), C.POINTER(SolveInfo)]),
+    "rt_worst_case_block": (I, [P, I, I, D, C.c_uint64, C.POINTER(D), C.POINTER(SolveInfo)]),
+    "rt_hier_workspace_create": (I, [P, C.POINTER(P)]),
+    "rt_pcg_batch": (I, [C.POINTER(P), I, D, I, C.POINTER(SolveInfo)]),
     "rt_sensitivity": (I, [P, I]),
     "rt_filter_sensitivity": (I, [P, F]),
     "rt_oc_update": (I, [P, F, C.POINTER(F), C.POINTER(I)]),

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -124,6 +125,10 @@ extern "C" void rt_ctx_destroy(rt_ctx* c) {
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     profile_drain(c);
+    for (auto& bg : c->batch_graphs) {
+        if (bg.exec) cudaGraphExecDestroy(bg.exec);
+        if (bg.graph) cudaGraphDestroy(bg.graph);
+    }
     for (auto e : c->ev_pool) cudaEventDestroy(e);
     if (c->hscal) cudaFreeHost(c->hscal);
     if (c->own_stream) cudaStreamDestroy(c->stream);
@@ -237,6 +242,11 @@ static void template_matrix(double E, double nu, double h, double* KE) {
 // ---------------------------------------------------------------------------
 // hierarchy
 // ---------------------------------------------------------------------------
+static uint64_t next_uid() {
+    static std::atomic<uint64_t> counter{1};
+    return counter.fetch_add(1);
+}
+
 template <typename T>
 static int dalloc(rt_ctx* c, T** p, size_t n) {
     if (n == 0) n = 1;
@@ -247,8 +257,47 @@ static int dalloc(rt_ctx* c, T** p, size_t n) {
     return RT_OK;
 }
 
+// drop the context's batched graphs that reference hierarchy uid (its buffers are going away)
+static void purge_batch_graphs(rt_ctx* c, uint64_t uid) {
+    auto& v = c->batch_graphs;
+    for (size_t i = 0; i < v.size();) {
+        if (std::find(v[i].uids.begin(), v[i].uids.end(), uid) != v[i].uids.end()) {
+            if (v[i].exec) cudaGraphExecDestroy(v[i].exec);
+            if (v[i].graph) cudaGraphDestroy(v[i].graph);
+            v.erase(v.begin() + i);
+        } else {
+            i++;
+        }
+    }
+}
+
+static void free_hier(rt_hier* h);
+
+// a workspace frees only the solve buffers it allocated (rt_hier_workspace_create)
+static void free_workspace(rt_hier* w) {
+    for (auto& L : w->L) {
+        cudaFree(L.u); cudaFree(L.f); cudaFree(L.r); cudaFree(L.u32); cudaFree(L.f32); cudaFree(L.r32);
+        cudaFree(L.d); cudaFree(L.d32); cudaFree(L.dvec); cudaFree(L.dvec32);
+    }
+    cudaFree(w->x); cudaFree(w->rr); cudaFree(w->z); cudaFree(w->p); cudaFree(w->q); cudaFree(w->rold);
+    cudaFree(w->partials); cudaFree(w->scal);
+    if (w->pcg_exec) cudaGraphExecDestroy(w->pcg_exec);
+    if (w->pcg_graph) cudaGraphDestroy(w->pcg_graph);
+    delete w;
+}
+
 static void free_hier(rt_hier* h) {
     if (!h) return;
+    if (h->ctx) purge_batch_graphs(h->ctx, h->uid);
+    for (rt_hier* w : h->wspool) {
+        purge_batch_graphs(h->ctx, w->uid);
+        free_workspace(w);
+    }
+    h->wspool.clear();
+    if (h->parent) {
+        free_workspace(h);
+        return;
+    }
     for (auto& L : h->L) {
         cudaFree(L.vact); cudaFree(L.eact); cudaFree(L.u); cudaFree(L.f); cudaFree(L.r);
         cudaFree(L.u32); cudaFree(L.f32); cudaFree(L.r32); cudaFree(L.st); cudaFree(L.st32);
@@ -265,6 +314,40 @@ static void free_hier(rt_hier* h) {
     delete h;
 }
 
+// refresh a workspace's copy of its parent's operator (buffers, settings, launch shapes)
+static void ws_sync(rt_hier* w) {
+    const rt_hier* p = w->parent;
+    if (!p) return;
+    w->P = p->P;
+    memcpy(w->tune, p->tune, sizeof(w->tune));
+    memcpy(w->tune_us, p->tune_us, sizeof(w->tune_us));
+    w->dinv64 = p->dinv64; w->dinv32 = p->dinv32;
+    for (size_t i = 0; i < w->L.size(); i++) {
+        rt_level& a = w->L[i];
+        const rt_level& b = p->L[i];
+        a.vact = b.vact; a.eact = b.eact; a.st = b.st; a.st32 = b.st32;
+        a.na = b.na; a.aidx = b.aidx; a.ainv = b.ainv; a.ainv32 = b.ainv32;
+        a.n_act_nodes = b.n_act_nodes; a.n_act_elems = b.n_act_elems;
+    }
+    memcpy(w->KE, p->KE, sizeof(w->KE));
+    w->KE_dev = p->KE_dev; w->KE32_dev = p->KE32_dev;
+    w->rho = p->rho; w->w = p->w; w->vfix = p->vfix; w->has_support = p->has_support;
+    w->sens = p->sens; w->ftmp = p->ftmp; w->eshell = p->eshell;
+    w->nload = p->nload; w->load_nodes = p->load_nodes; w->load_normal = p->load_normal; w->Rd = p->Rd;
+    w->nrig = p->nrig; w->Ru = p->Ru;
+    w->stencil_ready = p->stencil_ready;
+    w->Qgal = p->Qgal; w->Qgal_ratio = p->Qgal_ratio;
+    w->use_graphs = p->use_graphs;
+    w->graph_epoch = p->graph_epoch;
+}
+
+#define RT_NOT_WORKSPACE(h)                                                                                   \
+    do {                                                                                                      \
+        if ((h)->parent)                                                                                      \
+            return rt_fail((h)->ctx, RT_ESTATE, "%s changes or reads the operator's own state: call it on the " \
+                                                "parent hierarchy, not on a solve workspace", __func__);      \
+    } while (0)
+
 static int upload_KE(rt_hier* h) {
     template_matrix(h->P.youngs_modulus, h->P.poisson_ratio, h->P.element_length, h->KE);
     float ke32[576];
@@ -280,6 +363,7 @@ static int upload_KE(rt_hier* h) {
 static int build_hier(rt_ctx* c, const rt_params* p, int nx, int ny, int nz, uint8_t* eact_dev, rt_hier** out) {
     rt_hier* h = new rt_hier();
     h->ctx = c;
+    h->uid = next_uid();
     h->P = *p;
     *out = h;  // the caller releases a partially built hierarchy on failure
     // level chain on the device: halve while more than 400 elements are solid (grid/Grid.cpp:488)
@@ -314,6 +398,10 @@ static int build_hier(rt_ctx* c, const rt_params* p, int nx, int ny, int nz, uin
     if (chain.size() == 1) {
         cudaFree(chain[0].e);
         return rt_fail(c, RT_EINVAL, "grid too small for multigrid (<= 400 solid elements)");
+    }
+    if (idx.size() > RT_MAX_LEVELS) {
+        for (Chain& ch : chain) cudaFree(ch.e);
+        return rt_fail(c, RT_EINVAL, "more than 15 multigrid levels");
     }
     for (size_t k = 0; k < idx.size(); k++) {
         Chain& ch = chain[idx[k]];
@@ -463,6 +551,7 @@ extern "C" int rt_hier_get_params(rt_hier* h, rt_params* p) {
 
 extern "C" int rt_hier_set_params(rt_hier* h, const rt_params* p) {
     if (!h || !p) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
     const bool ke = p->youngs_modulus != h->P.youngs_modulus || p->poisson_ratio != h->P.poisson_ratio ||
                     p->element_length != h->P.element_length;
     if (p->skip_layer1 != h->P.skip_layer1)
@@ -533,6 +622,7 @@ extern "C" int rt_surface_nodes(rt_hier* h, uint8_t* surf) {
 
 extern "C" int rt_set_support(rt_hier* h, const uint8_t* vfix) {
     if (!h || !vfix) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
     rt_level& L = h->L[0];
     long cnt = 0;
     for (long v = 0; v < L.nv; v++) cnt += vfix[v] != 0;
@@ -601,6 +691,7 @@ static int load_rigid_basis(rt_hier* h, const int* nodes, const double* normals)
 
 extern "C" int rt_set_load_nodes(rt_hier* h, int nload, const int* nodes, const double* normals) {
     if (!h || nload < 0 || (nload > 0 && (!nodes || !normals))) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
     rt_ctx* c = h->ctx;
     rt_level& L = h->L[0];
     for (int i = 0; i < nload; i++)
@@ -638,6 +729,7 @@ extern "C" int rt_set_load_nodes(rt_hier* h, int nload, const int* nodes, const 
 // ---------------------------------------------------------------------------
 static int field_ptr(rt_hier* h, int field, int lvl, void** ptr, size_t* bytes) {
     if (lvl < 0 || lvl >= (int)h->L.size()) return RT_EINVAL;
+    ws_sync(h);
     rt_level& L = h->L[lvl];
     switch (field) {
         case RT_FIELD_U: *ptr = L.u; *bytes = sizeof(double) * 3 * L.nv; return RT_OK;
@@ -763,6 +855,8 @@ static int convert_layout(rt_hier* h, int field, int lvl, bool to_ref, const voi
 
 extern "C" int rt_put(rt_hier* h, int field, int lvl, int layout, const void* src) {
     if (!h || !src) return RT_EINVAL;
+    if (h->parent && field != RT_FIELD_U && field != RT_FIELD_F && field != RT_FIELD_R)
+        return rt_fail(h->ctx, RT_ESTATE, "a solve workspace takes only displacement, force and residual fields");
     void* d;
     size_t bytes;
     RT_CHECK(field_ptr(h, field, lvl, &d, &bytes));
@@ -797,6 +891,8 @@ extern "C" int rt_get(rt_hier* h, int field, int lvl, int layout, void* dst) {
 
 extern "C" int rt_put_dev(rt_hier* h, int field, int lvl, const void* src) {
     if (!h || !src) return RT_EINVAL;
+    if (h->parent && field != RT_FIELD_U && field != RT_FIELD_F && field != RT_FIELD_R)
+        return rt_fail(h->ctx, RT_ESTATE, "a solve workspace takes only displacement, force and residual fields");
     void* d;
     size_t bytes;
     RT_CHECK(field_ptr(h, field, lvl, &d, &bytes));
@@ -821,6 +917,7 @@ __global__ void k_fill_rho(long ne, const uint8_t* __restrict__ eact, float v, f
 
 extern "C" int rt_init_density(rt_hier* h, float rho) {
     if (!h) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
     rt_level& L = h->L[0];
     h->stencil_ready = false;
     return rt_launch(h->ctx, "init_density", [&] {
@@ -836,12 +933,17 @@ static int estimate_lmax(rt_hier* h, int lvl);
 
 // element weights rho^p and the inverted diagonal blocks of the finest level
 static int refresh_fine(rt_hier* h) {
+    if (h->parent) {  // weights and diagonal blocks belong to the parent (refreshed by its own calls)
+        ws_sync(h);
+        return RT_OK;
+    }
     RT_CHECK(rtk::penalty_weights(h));
     return rtk::fine_dinv(h);
 }
 
 extern "C" int rt_update_stencil(rt_hier* h) {
     if (!h) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
     RT_CUDA(h->ctx, cudaSetDevice(h->ctx->device));
     RT_CHECK(refresh_fine(h));
     const int nl = (int)h->L.size();
@@ -859,6 +961,7 @@ extern "C" int rt_update_stencil(rt_hier* h) {
 
 extern "C" int rt_smoother_lmax(rt_hier* h, int lvl, double* lmax) {
     if (!h || !lmax || lvl < 0 || lvl + 1 >= (int)h->L.size()) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
     if (!h->stencil_ready) return rt_fail(h->ctx, RT_ESTATE, "rt_update_stencil has not run");
     RT_CUDA(h->ctx, cudaMemcpyAsync(h->ctx->hscal, h->scal + RT_SCAL_LMAX + lvl, sizeof(double),
                                     cudaMemcpyDeviceToHost, h->ctx->stream));
@@ -884,9 +987,19 @@ struct LvlVec<float> {
     static float* d(rt_level& L) { return L.d32; }
 };
 
-__global__ void k_sqrt_slot(const double* __restrict__ src, double* __restrict__ dst) {
-    if (threadIdx.x == 0) dst[0] = sqrt(src[0]);
+// lmax = sqrt(|x|^2) after the power steps, then the level's Chebyshev coefficient table
+__global__ void k_lmax_finish(const double* __restrict__ xx, double* __restrict__ lmax, double* __restrict__ table) {
+    if (threadIdx.x == 0 && xx) lmax[0] = sqrt(xx[0]);
+    __syncthreads();
+    if (threadIdx.x < RT_CHEBY_MAXK) {
+        double a, b;
+        rt_cheby_coef(lmax[0], threadIdx.x, a, b);
+        table[2 * threadIdx.x] = a;
+        table[2 * threadIdx.x + 1] = b;
+    }
 }
+
+static double* cheby_table(rt_hier* h, int lvl) { return h->scal + RT_SCAL_CHEB + 2 * RT_CHEBY_MAXK * lvl; }
 
 // lmax(D^-1 A) of a level by 15 power steps (D^-1 A v = v - jacobi(v; f = 0, omega = 1)),
 // left on the device for the Chebyshev kernels
@@ -904,8 +1017,8 @@ static int estimate_lmax(rt_hier* h, int lvl) {
         RT_CHECK(rtk::axpy(h, n, -1.0, z, x));
     }
     RT_CHECK(rtk::dot(h, n, x, x, h->scal + 291));
-    return rt_launch(h->ctx, "lmax_sqrt", [&] {
-        k_sqrt_slot<<<1, 32, 0, h->ctx->stream>>>(h->scal + 291, h->scal + RT_SCAL_LMAX + lvl);
+    return rt_launch(h->ctx, "lmax_finish", [&] {
+        k_lmax_finish<<<1, 32, 0, h->ctx->stream>>>(h->scal + 291, h->scal + RT_SCAL_LMAX + lvl, cheby_table(h, lvl));
     });
 }
 
@@ -922,7 +1035,9 @@ static int level_smooth(rt_hier* h, int lvl, int smoother, int sweeps, double om
     T* u = LvlVec<T>::u(L);
     T* f = LvlVec<T>::f(L);
     T* tmp = LvlVec<T>::r(L);
-    const double* lmax = h->scal + RT_SCAL_LMAX + lvl;
+    const double* coef = cheby_table(h, lvl);
+    if (smoother == RT_SMOOTH_CHEBY && sweeps > RT_CHEBY_MAXK)
+        return rt_fail(h->ctx, RT_EINVAL, "Chebyshev smoothing takes at most 16 steps");
     for (int s = 0; s < sweeps; s++) {
         if (smoother == RT_SMOOTH_JACOBI || smoother == RT_SMOOTH_CHEBY) {
             // ping-pong u -> tmp -> u
@@ -930,8 +1045,8 @@ static int level_smooth(rt_hier* h, int lvl, int smoother, int sweeps, double om
             T* dst = (s % 2 == 0) ? tmp : u;
             if (smoother == RT_SMOOTH_CHEBY) {
                 T* d = LvlVec<T>::d(L);
-                if (lvl == 0) RT_CHECK(rtk::fine_cheby<T>(h, src, f, dst, d, lmax, s));
-                else RT_CHECK(rtk::st_cheby<T>(h, lvl, src, f, dst, d, lmax, s));
+                if (lvl == 0) RT_CHECK(rtk::fine_cheby<T>(h, src, f, dst, d, coef, s));
+                else RT_CHECK(rtk::st_cheby<T>(h, lvl, src, f, dst, d, coef, s));
             } else {
                 if (lvl == 0) RT_CHECK(rtk::fine_jacobi<T>(h, src, f, dst, omega));
                 else RT_CHECK(rtk::st_jacobi<T>(h, lvl, src, f, dst, omega));
@@ -979,6 +1094,7 @@ static int read_scalars(rt_hier* h, int first, int count, double* out) {
 }
 
 static int need_stencil(rt_hier* h) {
+    ws_sync(h);
     if (!h->stencil_ready) return rt_fail(h->ctx, RT_ESTATE, "rt_update_stencil must run after the density or supports change");
     return RT_OK;
 }
@@ -1015,11 +1131,13 @@ extern "C" int rt_smooth(rt_hier* h, int lvl, int smoother, int sweeps, double o
 
 extern "C" int rt_restrict_residual(rt_hier* h, int lvl) {
     if (!h || lvl < 1 || lvl >= (int)h->L.size()) return RT_EINVAL;
+    ws_sync(h);
     return rtk::restrict_<double>(h, lvl, h->L[lvl - 1].r, h->L[lvl].f);
 }
 
 extern "C" int rt_prolongate_correction(rt_hier* h, int lvl) {
     if (!h || lvl < 0 || lvl + 1 >= (int)h->L.size()) return RT_EINVAL;
+    ws_sync(h);
     return rtk::prolong_add<double>(h, lvl, h->L[lvl + 1].u, h->L[lvl].u);
 }
 
@@ -1183,18 +1301,23 @@ static int pcg_graph_run(rt_hier* h, double* x, double* r, bool no_support) {
     return RT_OK;
 }
 
-static int pcg_core(rt_hier* h, double* x, const double* b, double tol, int maxit, rt_solve_info* info, int* vcycles) {
+// r = b - K x (identity rows on supports), rold = 0, scal[22] = b.b, scal[21] = r.r (graph-capturable)
+static int pcg_prologue(rt_hier* h, double* x, const double* b) {
     rt_level& L = h->L[0];
     const long n = 3 * L.nv;
     double* r = h->rr;
-    // r = b - K x (identity rows on supports), rold = 0
     RT_CHECK(rtk::fine_applyK<double>(h, x, h->q));
     RT_CUDA(h->ctx, cudaMemcpyAsync(r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->ctx->stream));
     RT_CHECK(rtk::axpy(h, n, -1.0, h->q, r));
     RT_CHECK(rtk::mask_copy(h, n, r, r));
     RT_CUDA(h->ctx, cudaMemsetAsync(h->rold, 0, sizeof(double) * n, h->ctx->stream));
     RT_CHECK(rtk::dot(h, n, b, b, h->scal + 22));
-    RT_CHECK(rtk::dot(h, n, r, r, h->scal + 21));
+    return rtk::dot(h, n, r, r, h->scal + 21);
+}
+
+static int pcg_core(rt_hier* h, double* x, const double* b, double tol, int maxit, rt_solve_info* info, int* vcycles) {
+    double* r = h->rr;
+    RT_CHECK(pcg_prologue(h, x, b));
     double s[2];
     RT_CHECK(read_scalars(h, 21, 2, s));
     const double bn = std::sqrt(s[1]) > 0 ? std::sqrt(s[1]) : 1.0;
@@ -1516,9 +1639,13 @@ static int modified_pm(rt_hier* h, int maxit, uint64_t seed, double* lambda, rt_
     return RT_OK;
 }
 
+static int block_lanczos(rt_hier* h, int bs, int nblk, double inner_tol, uint64_t seed, double* lambda,
+                         rt_solve_info* info);
+
 extern "C" int rt_worst_case(rt_hier* h, int method, int k, double inner_tol, uint64_t seed, double* lambda,
                              rt_solve_info* info) {
     if (!h || !lambda) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
     RT_CHECK(need_stencil(h));
     rt_solve_info loc;
     memset(&loc, 0, sizeof(loc));
@@ -1528,6 +1655,7 @@ extern "C" int rt_worst_case(rt_hier* h, int method, int k, double inner_tol, ui
     cudaEventRecord(a, h->ctx->stream);
     int s;
     if (method == RT_WORST_LANCZOS) s = lanczos(h, k, inner_tol, seed, lambda, &loc);
+    else if (method == RT_WORST_BLOCK_LANCZOS) s = block_lanczos(h, 8, std::max(1, (k + 7) / 8), inner_tol, seed, lambda, &loc);
     else if (method == RT_WORST_MODPM) s = modified_pm(h, k > 0 ? k : 500, seed, lambda, &loc);
     else s = RT_EINVAL;
     cudaEventRecord(b, h->ctx->stream);
@@ -1546,11 +1674,13 @@ extern "C" int rt_worst_case(rt_hier* h, int method, int k, double inner_tol, ui
 // ---------------------------------------------------------------------------
 extern "C" int rt_filter_sensitivity(rt_hier* h, float radius) {
     if (!h || radius <= 0) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
     return rtk::filter(h, radius);
 }
 
 extern "C" int rt_sensitivity(rt_hier* h, int filt) {
     if (!h) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
     RT_CHECK(rtk::sensitivity(h, h->L[0].u));
     if (filt) RT_CHECK(rtk::filter(h, h->P.filter_radius));
     return RT_OK;
@@ -1558,6 +1688,7 @@ extern "C" int rt_sensitivity(rt_hier* h, int filt) {
 
 extern "C" int rt_oc_update(rt_hier* h, float vgoal, float* lambda_out, int* trials_out) {
     if (!h) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
     rt_level& L = h->L[0];
     RT_CHECK(rtk::oc_maxabs(h, nullptr));
     double gmax;
@@ -1585,6 +1716,7 @@ extern "C" int rt_oc_update(rt_hier* h, float vgoal, float* lambda_out, int* tri
 extern "C" int rt_oc_iteration(rt_hier* h, int method, int k, double inner_tol, uint64_t seed, float vgoal,
                                double* compliance_out) {
     if (!h) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
     RT_CHECK(rt_update_stencil(h));
     double lam = 0;
     rt_solve_info info;
@@ -1598,13 +1730,22 @@ extern "C" int rt_oc_iteration(rt_hier* h, int method, int k, double inner_tol, 
 // ---------------------------------------------------------------------------
 // launch-shape autotuner for the finest-level kernels
 // ---------------------------------------------------------------------------
+// a Chebyshev table for lmax = 2 (slot 299) so the fine kernels can be timed before any stencil exists
+static int spare_cheby_table(rt_hier* h) {
+    const double two = 2.0;
+    RT_CUDA(h->ctx, cudaMemcpyAsync(h->scal + 299, &two, sizeof(double), cudaMemcpyHostToDevice, h->ctx->stream));
+    return rt_launch(h->ctx, "lmax_finish", [&] {
+        k_lmax_finish<<<1, 32, 0, h->ctx->stream>>>(nullptr, h->scal + 299, h->scal + RT_SCAL_CHEB_SPARE);
+    });
+}
+
 static double time_fine_kernel(rt_hier* h, int prec, int mode, int reps) {
     rt_ctx* c = h->ctx;
     rt_level& L = h->L[0];
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
-    const double* lmax = h->stencil_ready ? h->scal + RT_SCAL_LMAX : h->scal + 299;
+    const double* coef = h->stencil_ready ? cheby_table(h, 0) : h->scal + RT_SCAL_CHEB_SPARE;
     auto run = [&]() -> int {
         if (prec == 1) {
             double *u = h->x, *f = h->q, *o = h->z, *d = h->p;
@@ -1612,7 +1753,7 @@ static double time_fine_kernel(rt_hier* h, int prec, int mode, int reps) {
                 case 0: return rtk::fine_residual<double>(h, u, f, o);
                 case 1: return rtk::fine_applyK<double>(h, u, o);
                 case 2: return rtk::fine_jacobi<double>(h, u, f, o, 0.6);
-                default: return rtk::fine_cheby<double>(h, u, f, o, d, lmax, 1);
+                default: return rtk::fine_cheby<double>(h, u, f, o, d, coef, 1);
             }
         }
         float *u = L.u32, *f = L.f32, *o = L.r32, *d = L.d32;
@@ -1620,7 +1761,7 @@ static double time_fine_kernel(rt_hier* h, int prec, int mode, int reps) {
             case 0: return rtk::fine_residual<float>(h, u, f, o);
             case 1: return rtk::fine_applyK<float>(h, u, o);
             case 2: return rtk::fine_jacobi<float>(h, u, f, o, 0.6);
-            default: return rtk::fine_cheby<float>(h, u, f, o, d, lmax, 1);
+            default: return rtk::fine_cheby<float>(h, u, f, o, d, coef, 1);
         }
     };
     double best = 1e30;
@@ -1641,6 +1782,7 @@ static double time_fine_kernel(rt_hier* h, int prec, int mode, int reps) {
 
 extern "C" int rt_autotune(rt_hier* h, int reps) {
     if (!h) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
     if (reps <= 0) reps = 5;
     rt_ctx* c = h->ctx;
     rt_level& L = h->L[0];
@@ -1655,10 +1797,7 @@ extern "C" int rt_autotune(rt_hier* h, int reps) {
     RT_CHECK(rtk::d2f(h, n, h->q, L.f32));
     RT_CUDA(c, cudaMemsetAsync(h->p, 0, sizeof(double) * n, c->stream));
     RT_CUDA(c, cudaMemsetAsync(L.d32, 0, sizeof(float) * n, c->stream));
-    if (!h->stencil_ready) {
-        const double one = 2.0;
-        RT_CUDA(c, cudaMemcpyAsync(h->scal + 299, &one, sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    }
+    if (!h->stencil_ready) RT_CHECK(spare_cheby_table(h));
     std::vector<rt_tile_cfg> cands;
     for (int ty : {2, 4, 8})
         for (int zc : {4, 8, 16, 32, 64}) cands.push_back(rt_tile_cfg{1, ty, zc});
@@ -1696,6 +1835,7 @@ extern "C" int rt_tuning_info(rt_hier* h, int precision, int mode, int* variant,
 extern "C" int rt_set_tuning(rt_hier* h, int precision, int mode, int variant, int ty, int zchunk) {
     if (!h || precision < 0 || precision > 1 || mode < 0 || mode > 3 || variant < 0 || variant > 1 || zchunk < 1)
         return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
     if (variant == 1 && ty != 2 && ty != 4 && ty != 8) return rt_fail(h->ctx, RT_EINVAL, "rows per tile must be 2, 4 or 8");
     const int pr = precision == RT_FP64 ? 1 : 0;
     h->tune[pr][mode] = rt_tile_cfg{variant, variant == 1 ? ty : 4, zchunk};
@@ -1705,6 +1845,7 @@ extern "C" int rt_set_tuning(rt_hier* h, int precision, int mode, int variant, i
 
 extern "C" int rt_bench_fine_kernel(rt_hier* h, int precision, int mode, int reps, double* us_per_launch) {
     if (!h || precision < 0 || precision > 1 || mode < 0 || mode > 3 || reps < 1) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
     rt_ctx* c = h->ctx;
     rt_level& L = h->L[0];
     const long n = 3 * L.nv;
@@ -1713,12 +1854,470 @@ extern "C" int rt_bench_fine_kernel(rt_hier* h, int precision, int mode, int rep
     RT_CHECK(rtk::rng_uniform(h, 0xbe7d, n, h->q));
     RT_CHECK(rtk::d2f(h, n, h->x, L.u32));
     RT_CHECK(rtk::d2f(h, n, h->q, L.f32));
-    if (!h->stencil_ready) {
-        const double two = 2.0;
-        RT_CUDA(c, cudaMemcpyAsync(h->scal + 299, &two, sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    }
+    if (!h->stencil_ready) RT_CHECK(spare_cheby_table(h));
     const double t = time_fine_kernel(h, precision == RT_FP64 ? 1 : 0, mode, reps);
     if (t >= 1e30) return rt_fail(c, RT_ECUDA, "kernel launch failed");
     if (us_per_launch) *us_per_launch = t;
     return RT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// solve workspaces and batched MG-PCG: many independent solves in one CUDA graph
+// ---------------------------------------------------------------------------
+static int make_workspace(rt_hier* p, rt_hier** out) {
+    rt_ctx* c = p->ctx;
+    rt_hier* w = new rt_hier();
+    *out = w;  // the caller frees a partially built workspace
+    w->ctx = c;
+    w->uid = next_uid();
+    w->parent = p;
+    w->L.resize(p->L.size());
+    for (size_t i = 0; i < p->L.size(); i++) {
+        rt_level& a = w->L[i];
+        const rt_level& b = p->L[i];
+        a.nx = b.nx; a.ny = b.ny; a.nz = b.nz; a.vx = b.vx; a.vy = b.vy; a.vz = b.vz;
+        a.nv = b.nv; a.ne = b.ne; a.ratio = b.ratio;
+        const size_t n = 3 * (size_t)a.nv;
+        RT_CHECK(dalloc(c, &a.u, n)); RT_CHECK(dalloc(c, &a.f, n)); RT_CHECK(dalloc(c, &a.r, n));
+        RT_CHECK(dalloc(c, &a.d, n));
+        RT_CHECK(dalloc(c, &a.u32, n)); RT_CHECK(dalloc(c, &a.f32, n)); RT_CHECK(dalloc(c, &a.r32, n));
+        RT_CHECK(dalloc(c, &a.d32, n));
+        RT_CUDA(c, cudaMemsetAsync(a.u, 0, sizeof(double) * n, c->stream));
+        RT_CUDA(c, cudaMemsetAsync(a.f, 0, sizeof(double) * n, c->stream));
+        RT_CUDA(c, cudaMemsetAsync(a.r, 0, sizeof(double) * n, c->stream));
+        if (i + 1 == p->L.size()) {
+            RT_CHECK(dalloc(c, &a.dvec, 3 * (size_t)b.na));
+            RT_CHECK(dalloc(c, &a.dvec32, 3 * (size_t)b.na));
+        }
+    }
+    const size_t n3 = 3 * (size_t)p->L[0].nv;
+    RT_CHECK(dalloc(c, &w->x, n3)); RT_CHECK(dalloc(c, &w->rr, n3)); RT_CHECK(dalloc(c, &w->z, n3));
+    RT_CHECK(dalloc(c, &w->p, n3)); RT_CHECK(dalloc(c, &w->q, n3)); RT_CHECK(dalloc(c, &w->rold, n3));
+    RT_CHECK(dalloc(c, &w->partials, RT_PARTIALS));
+    RT_CHECK(dalloc(c, &w->scal, RT_NSCAL));
+    RT_CUDA(c, cudaMemsetAsync(w->scal, 0, sizeof(double) * RT_NSCAL, c->stream));
+    ws_sync(w);
+    return RT_OK;
+}
+
+extern "C" int rt_hier_workspace_create(rt_hier* parent, rt_hier** out) {
+    if (!parent || !out) return RT_EINVAL;
+    *out = nullptr;
+    RT_NOT_WORKSPACE(parent);
+    RT_CUDA(parent->ctx, cudaSetDevice(parent->ctx->device));
+    rt_hier* w = nullptr;
+    const int s = make_workspace(parent, &w);
+    if (s != RT_OK) {
+        if (w) free_workspace(w);
+        return s;
+    }
+    *out = w;
+    return RT_OK;
+}
+
+// start of one instance's loop in a batched graph: iteration state, and whether to iterate at all
+__global__ void k_pcg_start(double* __restrict__ scal, double tol, double maxit, cudaGraphConditionalHandle cond) {
+    if (threadIdx.x != 0) return;
+    scal[24] = 0.0;
+    scal[25] = tol;
+    scal[26] = maxit;
+    const double rr = scal[21], bb = scal[22] > 0 ? scal[22] : 1.0;
+    const bool go = isfinite(rr) && sqrt(rr) > tol * sqrt(bb) && maxit > 0;
+    cudaGraphSetConditional(cond, go ? 1u : 0u);
+}
+
+static bool no_support_mode(const rt_hier* h) { return h->P.mode == RT_MODE_NSCF || h->P.mode == RT_MODE_NSFF; }
+
+// one graph: per instance, prologue (child graph) -> k_pcg_start -> WHILE(one PCG iteration);
+// the instances share no node, so the device runs their kernels concurrently
+static int build_batch_graph(rt_ctx* c, rt_hier* const* hs, int n, double tol, int maxit, cudaGraph_t* out) {
+    cudaGraph_t g;
+    RT_CUDA(c, cudaGraphCreate(&g, 0));
+    for (int i = 0; i < n; i++) {
+        rt_hier* h = hs[i];
+        double* x = h->L[0].u;
+        const double* b = h->L[0].f;
+        cudaGraphConditionalHandle cond;
+        cudaError_t e = cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault);
+        cudaGraph_t pg = nullptr;
+        int s = RT_OK;
+        if (e == cudaSuccess) e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            s = pcg_prologue(h, x, b);
+            e = cudaStreamEndCapture(c->stream, &pg);
+        }
+        cudaGraphNode_t n1 = nullptr, n2 = nullptr, n3 = nullptr;
+        if (e == cudaSuccess && s == RT_OK) e = cudaGraphAddChildGraphNode(&n1, g, nullptr, 0, pg);
+        if (pg) cudaGraphDestroy(pg);
+        if (e == cudaSuccess && s == RT_OK) {
+            double* scal = h->scal;
+            double tl = tol, mi = (double)maxit;
+            void* args[] = {(void*)&scal, (void*)&tl, (void*)&mi, (void*)&cond};
+            cudaKernelNodeParams kp = {};
+            kp.func = (void*)k_pcg_start;
+            kp.gridDim = dim3(1);
+            kp.blockDim = dim3(32);
+            kp.kernelParams = args;
+            e = cudaGraphAddKernelNode(&n2, g, &n1, 1, &kp);
+        }
+        cudaGraph_t body = nullptr;
+        if (e == cudaSuccess && s == RT_OK) {
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = cond;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            e = cudaGraphAddNode(&n3, g, &n2, 1, &cp);
+            body = cp.conditional.phGraph_out[0];
+        }
+        if (e == cudaSuccess && s == RT_OK)
+            e = cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess && s == RT_OK) {
+            s = pcg_body(h, x, h->rr, no_support_mode(h), cond, 1);
+            cudaGraph_t captured = nullptr;
+            e = cudaStreamEndCapture(c->stream, &captured);
+        }
+        if (s != RT_OK || e != cudaSuccess) {
+            cudaGraphDestroy(g);
+            if (s != RT_OK) return s;
+            return rt_fail(c, RT_ECUDA, "batched PCG graph (instance %d): %s", i, cudaGetErrorString(e));
+        }
+    }
+    *out = g;
+    return RT_OK;
+}
+
+// key of a batched graph: the instances, their operator epochs and solver settings, tol, maxit
+static uint64_t batch_key(rt_hier* const* hs, int n, double tol, int maxit) {
+    uint64_t k = 1469598103934665603ull;
+    auto mix = [&](uint64_t v) { k = (k ^ v) * 1099511628211ull; };
+    for (int i = 0; i < n; i++) {
+        const rt_hier* h = hs[i];
+        mix(h->uid);
+        mix(h->graph_epoch);
+        mix((uint64_t)h->P.precision | ((uint64_t)h->P.smoother << 4) | ((uint64_t)h->P.pre_sweeps << 8) |
+            ((uint64_t)h->P.post_sweeps << 16) | ((uint64_t)h->P.mode << 24));
+        uint64_t om;
+        memcpy(&om, &h->P.jacobi_omega, 8);
+        mix(om);
+    }
+    uint64_t tb;
+    memcpy(&tb, &tol, 8);
+    mix(tb);
+    mix((uint64_t)maxit);
+    return k;
+}
+
+static int pcg_batch_core(rt_hier* const* hs, int n, double tol, int maxit, rt_solve_info* infos) {
+    rt_ctx* c = hs[0]->ctx;
+    for (int i = 0; i < n; i++) {
+        rt_hier* h = hs[i];
+        if (h->ctx != c) return rt_fail(c, RT_EINVAL, "batched solves must share one context");
+        for (int j = 0; j < i; j++)
+            if (hs[j] == h) return rt_fail(c, RT_EINVAL, "instance %d appears twice in the batch", i);
+        RT_CHECK(need_stencil(h));
+        if (no_support_mode(h) && h->Ru == nullptr) {
+            rt_hier* owner = h->parent ? h->parent : h;
+            RT_CHECK(rtk::rigid_nodes(owner));
+            ws_sync(h);
+        }
+    }
+    cudaEvent_t ea, eb;
+    cudaEventCreate(&ea);
+    cudaEventCreate(&eb);
+    cudaEventRecord(ea, c->stream);
+    if (c->profile || !hs[0]->use_graphs) {
+        // per-kernel events cannot sit inside a graph: run the instances one after the other
+        for (int i = 0; i < n; i++) {
+            rt_solve_info si;
+            memset(&si, 0, sizeof(si));
+            int vc = 0;
+            RT_CHECK(pcg_core(hs[i], hs[i]->L[0].u, hs[i]->L[0].f, tol, maxit, &si, &vc));
+        }
+    } else {
+        const uint64_t key = batch_key(hs, n, tol, maxit);
+        rt_ctx::BatchGraph* bg = nullptr;
+        for (auto& e : c->batch_graphs)
+            if (e.key == key) bg = &e;
+        if (!bg) {
+            rt_ctx::BatchGraph nb;
+            nb.key = key;
+            for (int i = 0; i < n; i++) nb.uids.push_back(hs[i]->uid);
+            RT_CHECK(build_batch_graph(c, hs, n, tol, maxit, &nb.graph));
+            cudaError_t e = cudaGraphInstantiate(&nb.exec, nb.graph, 0);
+            if (e != cudaSuccess) {
+                cudaGraphDestroy(nb.graph);
+                return rt_fail(c, RT_ECUDA, "batched PCG graph instantiation failed: %s", cudaGetErrorString(e));
+            }
+            if (c->batch_graphs.size() >= 4) {  // keep the four most recent batches
+                cudaGraphExecDestroy(c->batch_graphs.front().exec);
+                cudaGraphDestroy(c->batch_graphs.front().graph);
+                c->batch_graphs.erase(c->batch_graphs.begin());
+            }
+            c->batch_graphs.push_back(nb);
+            bg = &c->batch_graphs.back();
+        }
+        RT_CUDA(c, cudaGraphLaunch(bg->exec, c->stream));
+        c->launches += 1;
+    }
+    cudaEventRecord(eb, c->stream);
+    cudaEventSynchronize(eb);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ea, eb);
+    cudaEventDestroy(ea);
+    cudaEventDestroy(eb);
+    RT_CUDA(c, cudaGetLastError());
+    for (int i = 0; i < n; i++) {
+        rt_hier* h = hs[i];
+        double sc[4];
+        RT_CHECK(read_scalars(h, 21, 4, sc));  // r.r, b.b, (unused), iterations
+        const double bn = sc[1] > 0 ? std::sqrt(sc[1]) : 1.0;
+        const double rel = std::sqrt(sc[0]) / bn;
+        if (!std::isfinite(sc[0])) return rt_fail(c, RT_ENAN, "NaN in batched PCG instance %d", i);
+        if (infos) {
+            rt_solve_info& si = infos[i];
+            memset(&si, 0, sizeof(si));
+            si.iterations = (int)sc[3];
+            si.vcycles = (int)sc[3];
+            si.rel_residual = rel;
+            si.status = rel <= tol ? RT_OK : RT_ENOCONV;
+            si.seconds = ms * 1e-3;
+            RT_CHECK(rtk::dot(h, 3 * h->L[0].nv, h->L[0].f, h->L[0].u, h->scal + 2));
+            RT_CHECK(read_scalars(h, 2, 1, &si.value));
+        }
+    }
+    return RT_OK;
+}
+
+extern "C" int rt_pcg_batch(rt_hier* const* hs, int n, double tol, int maxit, rt_solve_info* infos) {
+    if (!hs || n < 1 || tol <= 0 || maxit < 0) return RT_EINVAL;
+    for (int i = 0; i < n; i++)
+        if (!hs[i]) return RT_EINVAL;
+    RT_CUDA(hs[0]->ctx, cudaSetDevice(hs[0]->ctx->device));
+    return pcg_batch_core(hs, n, tol, maxit, infos);
+}
+
+// ---------------------------------------------------------------------------
+// block Lanczos on the load-space compliance operator A = P S K^-1 S^T P:
+// block size bs, nblk block steps, full CGS2 re-orthogonalisation, Rayleigh-Ritz on
+// the projected (nblk bs)^2 matrix; each block step's bs inner solves run as one
+// batched graph on bs solve workspaces
+// ---------------------------------------------------------------------------
+
+// cyclic Jacobi eigen-decomposition of a symmetric n x n matrix (row-major, overwritten);
+// returns the largest eigenvalue and its unit eigenvector
+static double sym_max_eig(int n, std::vector<double>& A, std::vector<double>& vec) {
+    std::vector<double> V((size_t)n * n, 0.0);
+    for (int i = 0; i < n; i++) V[(size_t)i * n + i] = 1.0;
+    for (int sweep = 0; sweep < 100; sweep++) {
+        double off = 0, tot = 0;
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                const double a = A[(size_t)i * n + j] * A[(size_t)i * n + j];
+                tot += a;
+                if (i != j) off += a;
+            }
+        if (off <= 1e-30 * tot || off == 0) break;
+        for (int p = 0; p < n - 1; p++)
+            for (int q = p + 1; q < n; q++) {
+                const double apq = A[(size_t)p * n + q];
+                if (apq == 0) continue;
+                const double app = A[(size_t)p * n + p], aqq = A[(size_t)q * n + q];
+                // rotation angle zeroing A[p][q]: tan(2 phi) = 2 apq / (aqq - app)
+                const double theta = (aqq - app) / (2 * apq);
+                const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1));
+                const double cs = 1 / std::sqrt(t * t + 1), sn = t * cs;
+                for (int k = 0; k < n; k++) {  // A <- A J (columns p, q)
+                    const double akp = A[(size_t)k * n + p], akq = A[(size_t)k * n + q];
+                    A[(size_t)k * n + p] = cs * akp - sn * akq;
+                    A[(size_t)k * n + q] = sn * akp + cs * akq;
+                }
+                for (int k = 0; k < n; k++) {  // A <- J^T A (rows p, q)
+                    const double apk = A[(size_t)p * n + k], aqk = A[(size_t)q * n + k];
+                    A[(size_t)p * n + k] = cs * apk - sn * aqk;
+                    A[(size_t)q * n + k] = sn * apk + cs * aqk;
+                }
+                for (int k = 0; k < n; k++) {  // V <- V J
+                    const double vkp = V[(size_t)k * n + p], vkq = V[(size_t)k * n + q];
+                    V[(size_t)k * n + p] = cs * vkp - sn * vkq;
+                    V[(size_t)k * n + q] = sn * vkp + cs * vkq;
+                }
+            }
+    }
+    int best = 0;
+    for (int i = 1; i < n; i++)
+        if (A[(size_t)i * n + i] > A[(size_t)best * n + best]) best = i;
+    vec.resize(n);
+    for (int k = 0; k < n; k++) vec[k] = V[(size_t)k * n + best];
+    return A[(size_t)best * n + best];
+}
+
+// w -= sum_c (Q_c . w) Q_c over columns [0, m), twice (CGS2); coef[c] accumulates both passes
+static int cgs2(rt_hier* h, long nl, int m, const double* Q, double* w, double* dcoef, std::vector<double>& coef) {
+    rt_ctx* c = h->ctx;
+    coef.assign(m, 0.0);
+    for (int pass = 0; pass < 2; pass++) {
+        for (int c0 = 0; c0 < m; c0 += 64) {
+            const int mm = std::min(64, m - c0);
+            const double* Qc = Q + (long)c0 * nl;
+            RT_CHECK(multidot(h, nl, mm, Qc, w, dcoef));
+            RT_CHECK(rt_launch(c, "lanczos_sub", [&] {
+                k_sub_multi<<<(unsigned)std::min<long>((nl + 255) / 256, c->sm_count * 8), 256, 0, c->stream>>>(
+                    nl, mm, Qc, dcoef, w);
+            }));
+            RT_CUDA(c, cudaMemcpyAsync(c->hscal, dcoef, sizeof(double) * mm, cudaMemcpyDeviceToHost, c->stream));
+            RT_CUDA(c, cudaStreamSynchronize(c->stream));
+            for (int k = 0; k < mm; k++) coef[c0 + k] += c->hscal[k];
+        }
+    }
+    return RT_OK;
+}
+
+// |w| into the host, then w /= |w|
+static int normalize(rt_hier* h, long nl, double* w, double* norm) {
+    RT_CHECK(rtk::dot(h, nl, w, w, h->scal + 34));
+    double s;
+    RT_CHECK(read_scalars(h, 34, 1, &s));
+    *norm = std::sqrt(s);
+    if (!(*norm > 0) || !std::isfinite(*norm)) return RT_OK;
+    return rtk::scale(h, nl, w, h->scal + 34, true);
+}
+
+static int block_lanczos(rt_hier* h, int bs, int nblk, double inner_tol, uint64_t seed, double* lambda,
+                         rt_solve_info* info) {
+    rt_ctx* c = h->ctx;
+    rt_level& L = h->L[0];
+    const long n = 3 * L.nv, nl = 3L * h->nload;
+    if (h->nload == 0) return rt_fail(c, RT_ESTATE, "no load nodes");
+    if (bs < 1 || bs > 16 || nblk < 1 || (long)bs * nblk > 128)
+        return rt_fail(c, RT_EINVAL, "block Lanczos needs 1 <= block size <= 16 and block size x steps <= 128");
+    const int mcap = (nblk + 1) * bs;
+    if (h->Qcap < mcap) {
+        cudaFree(h->Q);
+        h->Q = nullptr;
+        RT_CHECK(dalloc(c, &h->Q, (size_t)mcap * nl));
+        h->Qcap = mcap;
+    }
+    while ((int)h->wspool.size() < bs) {
+        rt_hier* w = nullptr;
+        const int s = make_workspace(h, &w);
+        if (s != RT_OK) {
+            if (w) free_workspace(w);
+            return s;
+        }
+        h->wspool.push_back(w);
+    }
+    if (no_support_mode(h) && h->Ru == nullptr) RT_CHECK(rtk::rigid_nodes(h));
+    double* Q = h->Q;
+    double* dcoef = h->scal + 240;  // [64]
+    const int m = nblk * bs;        // Krylov dimension
+    std::vector<double> H((size_t)m * m, 0.0), coef;
+    int inner = 0, vcycles = 0;
+    // starting block: bs projected random loads, orthonormalised
+    int ncol = 0;
+    for (int i = 0; i < bs; i++) {
+        double* qi = Q + (long)i * nl;
+        RT_CHECK(rtk::rng_uniform(h, seed + 0x9e3779b97f4a7c15ull * (uint64_t)i, n, L.f));
+        RT_CHECK(rtk::project_load(h, L.f));
+        RT_CHECK(rtk::gather_load(h, L.f, qi));
+        if (i > 0) RT_CHECK(cgs2(h, nl, i, Q, qi, dcoef, coef));
+        double nr;
+        RT_CHECK(normalize(h, nl, qi, &nr));
+        if (!(nr > 0)) return rt_fail(c, RT_ENAN, "block Lanczos: degenerate starting block");
+        ncol++;
+    }
+    std::vector<rt_hier*> ws(h->wspool.begin(), h->wspool.begin() + bs);
+    std::vector<rt_solve_info> si(bs);
+    int done_blocks = 0;
+    for (int j = 0; j < nblk; j++) {
+        // A Q_j: scatter each column into its workspace's right-hand side, solve all bs at once
+        for (int i = 0; i < bs; i++) {
+            rt_hier* w = ws[i];
+            ws_sync(w);
+            RT_CUDA(c, cudaMemsetAsync(w->L[0].f, 0, sizeof(double) * n, c->stream));
+            RT_CHECK(rtk::scatter_load(w, Q + (long)(j * bs + i) * nl, w->L[0].f));
+            RT_CUDA(c, cudaMemsetAsync(w->L[0].u, 0, sizeof(double) * n, c->stream));
+        }
+        RT_CHECK(pcg_batch_core(ws.data(), bs, inner_tol, 500, si.data()));
+        for (int i = 0; i < bs; i++) {
+            inner += si[i].iterations;
+            vcycles += si[i].vcycles;
+        }
+        // new columns: orthogonalise against every earlier column; the coefficients and the
+        // norm are column j bs + i of the projected matrix H = Q^T A Q
+        bool breakdown = false;
+        for (int i = 0; i < bs; i++) {
+            const int col = (j + 1) * bs + i;
+            double* wv = Q + (long)col * nl;
+            RT_CUDA(c, cudaMemcpyAsync(h->z, ws[i]->L[0].u, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+            RT_CHECK(rtk::project_load(h, h->z));
+            RT_CHECK(rtk::gather_load(h, h->z, wv));
+            RT_CHECK(cgs2(h, nl, col, Q, wv, dcoef, coef));
+            double nr;
+            RT_CHECK(normalize(h, nl, wv, &nr));
+            const int hc = j * bs + i;
+            for (int r = 0; r < std::min(col, m); r++) H[(size_t)r * m + hc] = coef[r];
+            if (col < m) H[(size_t)col * m + hc] = nr;
+            if (!std::isfinite(nr)) return rt_fail(c, RT_ENAN, "NaN in block Lanczos");
+            if (nr <= 1e-13 * std::fabs(H[(size_t)hc * m + hc])) breakdown = true;
+        }
+        done_blocks = j + 1;
+        if (breakdown) break;  // invariant subspace: the Ritz values are exact
+    }
+    const int mk = done_blocks * bs;
+    std::vector<double> T((size_t)mk * mk), y;
+    for (int r = 0; r < mk; r++)
+        for (int q = 0; q < mk; q++) T[(size_t)r * mk + q] = 0.5 * (H[(size_t)r * m + q] + H[(size_t)q * m + r]);
+    const double theta = sym_max_eig(mk, T, y);
+    // worst-case load f = Q y on the load set, u = K^-1 f
+    double* dy = nullptr;
+    RT_CHECK(dalloc(c, &dy, mk));
+    RT_CUDA(c, cudaMemcpyAsync(dy, y.data(), sizeof(double) * mk, cudaMemcpyHostToDevice, c->stream));
+    int st = rt_launch(c, "lanczos_combine", [&] {
+        k_combine<<<(unsigned)std::min<long>((nl + 255) / 256, c->sm_count * 8), 256, 0, c->stream>>>(nl, mk, Q, dy,
+                                                                                                      h->fs_old);
+    });
+    RT_CUDA(c, cudaStreamSynchronize(c->stream));
+    cudaFree(dy);
+    RT_CHECK(st);
+    RT_CUDA(c, cudaMemsetAsync(L.f, 0, sizeof(double) * n, c->stream));
+    RT_CHECK(rtk::scatter_load(h, h->fs_old, L.f));
+    RT_CUDA(c, cudaMemsetAsync(L.u, 0, sizeof(double) * n, c->stream));
+    rt_solve_info fin;
+    memset(&fin, 0, sizeof(fin));
+    RT_CHECK(pcg_core(h, L.u, L.f, inner_tol, 500, &fin, &vcycles));
+    inner += fin.iterations;
+    *lambda = theta;
+    if (info) {
+        info->iterations = done_blocks;
+        info->inner_iterations = inner;
+        info->vcycles = vcycles;
+        info->rel_residual = fin.rel_residual;
+        info->value = theta;
+        info->status = RT_OK;
+    }
+    return RT_OK;
+}
+
+extern "C" int rt_worst_case_block(rt_hier* h, int block_size, int n_blocks, double inner_tol, uint64_t seed,
+                                   double* lambda, rt_solve_info* info) {
+    if (!h || !lambda || inner_tol <= 0) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
+    RT_CHECK(need_stencil(h));
+    rt_solve_info loc;
+    memset(&loc, 0, sizeof(loc));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, h->ctx->stream);
+    const int s = block_lanczos(h, block_size, n_blocks, inner_tol, seed, lambda, &loc);
+    cudaEventRecord(b, h->ctx->stream);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    loc.seconds = ms * 1e-3;
+    if (info) *info = loc;
+    return s;
 }

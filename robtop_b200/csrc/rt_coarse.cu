@@ -136,12 +136,11 @@ template <typename T, int MODE>
 __global__ void __launch_bounds__(ST_BS) k_st_split4(int nx, int ny, int nz, const uint8_t* __restrict__ vact,
                                                       const T* __restrict__ st, const T* __restrict__ u,
                                                       const T* __restrict__ f, T* __restrict__ out,
-                                                      T* __restrict__ d, T omega, const double* __restrict__ lmax,
+                                                      T* __restrict__ d, T omega, const double* __restrict__ coef,
                                                       int kstep) {
     T ca = T(0), cb = T(0);
     if (MODE == 3) {
-        double a_, b_;
-        rt_cheby_coef(lmax[0], kstep, a_, b_);
+        const double a_ = coef[2 * kstep], b_ = coef[2 * kstep + 1];
         ca = (T)a_;
         cb = (T)b_;
     }
@@ -256,14 +255,13 @@ __global__ void __launch_bounds__(ST_BS) k_restrict4_split8(int fnx, int fny, in
     }
 }
 
-// Chebyshev step on an assembled-stencil level (see rt_cheby_coef)
+// Chebyshev step on an assembled-stencil level (coefficients a_k, b_k from the level's table, see rt_cheby_coef)
 template <typename T>
 __global__ void __launch_bounds__(ST_BS) k_st_cheby(int nx, int ny, int nz, const uint8_t* __restrict__ vact,
                                                      const T* __restrict__ st, const T* __restrict__ u,
                                                      const T* __restrict__ f, T* __restrict__ unew,
-                                                     T* __restrict__ d, const double* __restrict__ lmax, int kstep) {
-    double ca, cb;
-    rt_cheby_coef(lmax[0], kstep, ca, cb);
+                                                     T* __restrict__ d, const double* __restrict__ coef, int kstep) {
+    const double ca = coef[2 * kstep], cb = coef[2 * kstep + 1];
     const T a = (T)ca, b = (T)cb;
     const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
     const long nv = (long)vx * vy * vz;
@@ -599,11 +597,11 @@ int st_jacobi(rt_hier* h, int lvl, const T* u, const T* f, T* unew, double omega
 }
 
 template <typename T>
-int st_cheby(rt_hier* h, int lvl, const T* u, const T* f, T* unew, T* d, const double* lmax, int kstep) {
+int st_cheby(rt_hier* h, int lvl, const T* u, const T* f, T* unew, T* d, const double* coef, int kstep) {
     rt_level& L = h->L[lvl];
     return rt_launch(h->ctx, sizeof(T) == 8 ? "st_cheby_f64" : "st_cheby_f32", [&] {
         k_st_split4<T, 3><<<grid_for(h->ctx, 4 * L.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(
-            L.nx, L.ny, L.nz, L.vact, stp<T>(L), u, f, unew, d, T(0), lmax, kstep);
+            L.nx, L.ny, L.nz, L.vact, stp<T>(L), u, f, unew, d, T(0), coef, kstep);
     });
 }
 template int st_cheby<double>(rt_hier*, int, const double*, const double*, double*, double*, const double*, int);

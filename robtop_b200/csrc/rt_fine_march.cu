@@ -69,24 +69,23 @@ __global__ void k_fine_dinv(int nx, int ny, int nz, const uint8_t* __restrict__ 
 }
 
 // MODE 0: r = f - K u (fixed rows: r = f)     MODE 1: out = K u (fixed rows: u)
-// MODE 2: unew = u + omega D^-1 (f - K u)     MODE 3: Chebyshev step kstep (see rt_cheby_coef)
+// MODE 2: unew = u + omega D^-1 (f - K u)     MODE 3: Chebyshev step kstep (coefficients a_k, b_k from the level's table, see rt_cheby_coef)
 // (fixed nodes in MODE 2/3: unew = f / n_e, d = 0)
 template <typename T, bool WS, int MODE, int TY>
-__global__ void __launch_bounds__(MARCH_BS) k_fine_march(int nx, int ny, int nz, int ntx, int nty, int nch,
+__global__ void __launch_bounds__(MARCH_BS, sizeof(T) == 4 ? 4 : 2) k_fine_march(int nx, int ny, int nz, int ntx, int nty, int nch,
                                                           int zchunk, const uint8_t* __restrict__ vact,
                                                           const float* __restrict__ wgt,
                                                           const uint8_t* __restrict__ vfix, const rte::KtVals<T> kt,
                                                           const T* __restrict__ u, const T* __restrict__ f,
                                                           T* __restrict__ out, T omega, T* __restrict__ dvec,
-                                                          const double* __restrict__ lmax, int kstep,
+                                                          const double* __restrict__ coef, int kstep,
                                                           const T* __restrict__ dinv) {
     const int lane = threadIdx.x & 31;
     const long wid = (long)blockIdx.x * MARCH_WARPS + (threadIdx.x >> 5);
     if (wid >= (long)ntx * nty * nch) return;  // whole warp leaves together
     T cheb_a = T(0), cheb_b = T(0);
     if (MODE == 3) {
-        double ca, cb;
-        rt_cheby_coef(lmax[0], kstep, ca, cb);
+        const double ca = coef[2 * kstep], cb = coef[2 * kstep + 1];
         cheb_a = (T)ca;
         cheb_b = (T)cb;
     }
@@ -177,6 +176,7 @@ __global__ void __launch_bounds__(MARCH_BS) k_fine_march(int nx, int ny, int nz,
 #pragma unroll
                         for (int c = 0; c < 3; c++) out[c * nv + v] = act ? (fixed ? u[c * nv + v] : fin[c]) : T(0);
                     } else {
+                        // u of this (non-fixed) node is ub[r]: node layer ez, node row Y0 - 1 + r == ey
                         T nu[3] = {T(0), T(0), T(0)}, dn[3] = {T(0), T(0), T(0)};
                         if (act) {
                             const T d00 = dinv[v], d01 = dinv[nv + v], d02 = dinv[2 * nv + v];
@@ -193,12 +193,12 @@ __global__ void __launch_bounds__(MARCH_BS) k_fine_march(int nx, int ny, int nz,
                                 for (int c = 0; c < 3; c++) nu[c] = zz[c];
                             } else if (MODE == 2) {
 #pragma unroll
-                                for (int c = 0; c < 3; c++) nu[c] = u[c * nv + v] + omega * zz[c];
+                                for (int c = 0; c < 3; c++) nu[c] = ub[r][c] + omega * zz[c];
                             } else {
 #pragma unroll
                                 for (int c = 0; c < 3; c++) {
                                     dn[c] = (kstep == 0 ? T(0) : cheb_a * dvec[c * nv + v]) + cheb_b * zz[c];
-                                    nu[c] = u[c * nv + v] + dn[c];
+                                    nu[c] = ub[r][c] + dn[c];
                                 }
                             }
                         }
@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(MARCH_BS) k_fine_march(int nx, int ny, int nz,
 
 template <typename T, bool WS, int MODE, int TY>
 int launch_march_ty(rt_hier* h, int zc, const T* u, const T* f, T* out, double omega, const char* name, T* dvec,
-                    const double* lmax, int kstep, const T* dinv) {
+                    const double* coef, int kstep, const T* dinv) {
     rt_level& L = h->L[0];
     const int ntx = (L.vx + MARCH_NX - 1) / MARCH_NX, nty = (L.vy + TY - 1) / TY, nch = (L.vz + zc - 1) / zc;
     const long nwarps = (long)ntx * nty * nch;
@@ -233,20 +233,20 @@ int launch_march_ty(rt_hier* h, int zc, const T* u, const T* f, T* out, double o
     const rte::KtVals<T> kt = rte::make_kt<T>(h);
     return rt_launch(h->ctx, name, [&] {
         k_fine_march<T, WS, MODE, TY><<<blocks, MARCH_BS, 0, h->ctx->stream>>>(
-            L.nx, L.ny, L.nz, ntx, nty, nch, zc, L.vact, h->w, h->vfix, kt, u, f, out, (T)omega, dvec, lmax, kstep,
+            L.nx, L.ny, L.nz, ntx, nty, nch, zc, L.vact, h->w, h->vfix, kt, u, f, out, (T)omega, dvec, coef, kstep,
             dinv);
     });
 }
 
 template <typename T, bool WS, int MODE>
 int launch_march(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name, T* dvec,
-                 const double* lmax, int kstep) {
+                 const double* coef, int kstep) {
     const rt_tile_cfg& tc = h->tune[sizeof(T) == 8 ? 1 : 0][MODE];
     const T* dinv = sizeof(T) == 8 ? (const T*)h->dinv64 : (const T*)h->dinv32;
     switch (tc.ty) {
-        case 2: return launch_march_ty<T, WS, MODE, 2>(h, tc.zchunk, u, f, out, omega, name, dvec, lmax, kstep, dinv);
-        case 8: return launch_march_ty<T, WS, MODE, 8>(h, tc.zchunk, u, f, out, omega, name, dvec, lmax, kstep, dinv);
-        default: return launch_march_ty<T, WS, MODE, 4>(h, tc.zchunk, u, f, out, omega, name, dvec, lmax, kstep, dinv);
+        case 2: return launch_march_ty<T, WS, MODE, 2>(h, tc.zchunk, u, f, out, omega, name, dvec, coef, kstep, dinv);
+        case 8: return launch_march_ty<T, WS, MODE, 8>(h, tc.zchunk, u, f, out, omega, name, dvec, coef, kstep, dinv);
+        default: return launch_march_ty<T, WS, MODE, 4>(h, tc.zchunk, u, f, out, omega, name, dvec, coef, kstep, dinv);
     }
 }
 
@@ -269,12 +269,12 @@ int fine_dinv(rt_hier* h) {
 }
 
 template <typename T, int MODE>
-int fine_march(rt_hier* h, const T* u, const T* f, T* out, double omega, T* dvec, const double* lmax, int kstep) {
+int fine_march(rt_hier* h, const T* u, const T* f, T* out, double omega, T* dvec, const double* coef, int kstep) {
     static const char* names[2][4] = {{"fine_residual_f32", "fine_applyK_f32", "fine_jacobi_f32", "fine_cheby_f32"},
                                       {"fine_residual_f64", "fine_applyK_f64", "fine_jacobi_f64", "fine_cheby_f64"}};
     const char* nm = names[sizeof(T) == 8 ? 1 : 0][MODE];
-    return h->has_support ? launch_march<T, true, MODE>(h, u, f, out, omega, nm, dvec, lmax, kstep)
-                          : launch_march<T, false, MODE>(h, u, f, out, omega, nm, dvec, lmax, kstep);
+    return h->has_support ? launch_march<T, true, MODE>(h, u, f, out, omega, nm, dvec, coef, kstep)
+                          : launch_march<T, false, MODE>(h, u, f, out, omega, nm, dvec, coef, kstep);
 }
 
 #define RT_INST_MARCH(T)                                                                                       \

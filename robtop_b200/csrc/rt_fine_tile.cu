@@ -51,13 +51,12 @@ __global__ void __launch_bounds__(TILE_BS, sizeof(T) == 8 ? 2 : 4) k_fine_tile(i
                                                         const uint8_t* __restrict__ vfix, const rte::KtVals<T> kt,
                                                         const T* __restrict__ u, const T* __restrict__ f,
                                                         T* __restrict__ out, T omega, T* __restrict__ dvec,
-                                                        const double* __restrict__ lmax, int kstep) {
+                                                        const double* __restrict__ coef, int kstep) {
     extern __shared__ __align__(16) unsigned char smraw[];
     TileSmem<T>& S = *reinterpret_cast<TileSmem<T>*>(smraw);
     T cheb_a = T(0), cheb_b = T(0);
     if (MODE == 3) {
-        double ca, cb;
-        rt_cheby_coef(lmax[0], kstep, ca, cb);
+        const double ca = coef[2 * kstep], cb = coef[2 * kstep + 1];
         cheb_a = (T)ca;
         cheb_b = (T)cb;
     }
@@ -291,7 +290,7 @@ __global__ void __launch_bounds__(TILE_BS, sizeof(T) == 8 ? 2 : 4) k_fine_tile(i
 
 template <typename T, bool WS, int MODE>
 int launch_tile(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name, T* dvec = nullptr,
-                const double* lmax = nullptr, int kstep = 0) {
+                const double* coef = nullptr, int kstep = 0) {
     rt_level& L = h->L[0];
     const size_t smem = sizeof(TileSmem<T>);
     auto kern = k_fine_tile<T, WS, MODE>;
@@ -300,7 +299,7 @@ int launch_tile(rt_hier* h, const T* u, const T* f, T* out, double omega, const 
     const rte::KtVals<T> kt = rte::make_kt<T>(h);
     return rt_launch(h->ctx, name, [&] {
         kern<<<grid, TILE_BS, smem, h->ctx->stream>>>(L.nx, L.ny, L.nz, zc, L.vact, h->w, h->vfix, kt, u, f, out,
-                                                      (T)omega, dvec, lmax, kstep);
+                                                      (T)omega, dvec, coef, kstep);
     });
 }
 
@@ -374,11 +373,11 @@ int fine_jacobi(rt_hier* h, const T* u, const T* f, T* unew, double omega) {
 }
 
 template <typename T>
-int fine_cheby(rt_hier* h, const T* u, const T* f, T* unew, T* d, const double* lmax, int kstep) {
-    if (use_march<T>(h, 3)) return fine_march<T, 3>(h, u, f, unew, 0.0, d, lmax, kstep);
+int fine_cheby(rt_hier* h, const T* u, const T* f, T* unew, T* d, const double* coef, int kstep) {
+    if (use_march<T>(h, 3)) return fine_march<T, 3>(h, u, f, unew, 0.0, d, coef, kstep);
     const char* nm = sizeof(T) == 8 ? "fine_cheby_f64" : "fine_cheby_f32";
-    return h->has_support ? launch_tile<T, true, 3>(h, u, f, unew, 0.0, nm, d, lmax, kstep)
-                          : launch_tile<T, false, 3>(h, u, f, unew, 0.0, nm, d, lmax, kstep);
+    return h->has_support ? launch_tile<T, true, 3>(h, u, f, unew, 0.0, nm, d, coef, kstep)
+                          : launch_tile<T, false, 3>(h, u, f, unew, 0.0, nm, d, coef, kstep);
 }
 
 template int fine_cheby<double>(rt_hier*, const double*, const double*, double*, double*, const double*, int);

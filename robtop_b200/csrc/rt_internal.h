@@ -33,6 +33,14 @@ struct rt_ctx {
     std::vector<Pending> pending;
     // host-pinned scalar mailbox
     double* hscal = nullptr;
+    // instantiated batched-PCG graphs (rt_pcg_batch), newest last
+    struct BatchGraph {
+        uint64_t key = 0;
+        std::vector<uint64_t> uids;  // hierarchies whose buffers the graph references
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+    };
+    std::vector<BatchGraph> batch_graphs;
 };
 
 struct rt_level {
@@ -66,6 +74,11 @@ struct rt_tile_cfg {
 
 struct rt_hier {
     rt_ctx* ctx = nullptr;
+    uint64_t uid = 0;            // unique per hierarchy / workspace of the process (graph cache keys)
+    // a solve workspace (rt_hier_workspace_create) owns only its solve vectors and scalars;
+    // every operator buffer and setting is the parent's, refreshed by ws_sync before each use
+    rt_hier* parent = nullptr;
+    std::vector<rt_hier*> wspool;  // workspaces this hierarchy made for its own block solves
     rt_params P;
     rt_tile_cfg tune[2][4];          // [FP32, FP64][residual, applyK, jacobi, chebyshev]
     double tune_us[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};  // measured time of the chosen shape
@@ -113,7 +126,7 @@ struct rt_hier {
 
 #define RT_RED_BLOCKS 296
 #define RT_PARTIALS (148 * 64)  // block partial sums: up to 64 values from 148 blocks
-#define RT_NSCAL 512            // device scalar slots
+#define RT_NSCAL 1024           // device scalar slots
 
 // error helpers -------------------------------------------------------------
 int rt_fail(rt_ctx* c, int code, const char* fmt, ...);
@@ -156,6 +169,12 @@ static inline unsigned rt_blocks(long n, int bs) { return (unsigned)((n + bs - 1
 #define RT_CHEBY_LO_FRAC (1.0 / 30.0)
 #define RT_CHEBY_HI_FRAC 1.1
 #define RT_SCAL_LMAX 300  // device scalar slots holding lmax(D^-1 A) per level
+// (a_k, b_k), k < RT_CHEBY_MAXK, per level at RT_SCAL_CHEB + 2 RT_CHEBY_MAXK lvl (levels 0..14);
+// the 16th table serves kernel timing before any stencil exists
+#define RT_CHEBY_MAXK 16
+#define RT_SCAL_CHEB 512
+#define RT_SCAL_CHEB_SPARE (RT_SCAL_CHEB + 2 * RT_CHEBY_MAXK * 15)
+#define RT_MAX_LEVELS 15
 __host__ __device__ inline void rt_cheby_coef(double lmax, int k, double& a, double& b) {
     const double hi = RT_CHEBY_HI_FRAC * lmax, lo = RT_CHEBY_LO_FRAC * lmax;
     const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
@@ -182,14 +201,14 @@ int fine_gs(rt_hier* h, T* u, const T* f, bool backward);
 template <typename T>
 int fine_jacobi(rt_hier* h, const T* u, const T* f, T* unew, double omega);
 template <typename T>
-int fine_cheby(rt_hier* h, const T* u, const T* f, T* unew, T* d, const double* lmax, int kstep);
+int fine_cheby(rt_hier* h, const T* u, const T* f, T* unew, T* d, const double* coef, int kstep);
 template <typename T>
-int st_cheby(rt_hier* h, int lvl, const T* u, const T* f, T* unew, T* d, const double* lmax, int kstep);
+int st_cheby(rt_hier* h, int lvl, const T* u, const T* f, T* unew, T* d, const double* coef, int kstep);
 int penalty_weights(rt_hier* h);
 int init_tile_kernels(rt_ctx* c);
 int fine_dinv(rt_hier* h);
 template <typename T, int MODE>
-int fine_march(rt_hier* h, const T* u, const T* f, T* out, double omega, T* dvec, const double* lmax, int kstep);
+int fine_march(rt_hier* h, const T* u, const T* f, T* out, double omega, T* dvec, const double* coef, int kstep);
 int tile_zchunk_default(rt_ctx* c, int vx, int vy, int vz);
 // stencil levels
 template <typename T>

@@ -238,6 +238,7 @@ class HierarchyGrid:
         self.params = params if params is not None else default_params()
         self._h = C.c_void_p()
         self._grids = []
+        self._children = []
 
     @property
     def handle(self):
@@ -347,7 +348,27 @@ class HierarchyGrid:
         self._c(A.lib().rt_worst_case(self._h, method, k, inner_tol, seed, C.byref(lam), C.byref(info)))
         return lam.value, info
 
+    def worst_case_block(self, block_size=8, n_blocks=2, inner_tol=1e-8, seed=0):
+        """Block Lanczos (rt_worst_case_block): each block step's inner solves run as one graph."""
+        lam = C.c_double()
+        info = A.SolveInfo()
+        self._c(A.lib().rt_worst_case_block(self._h, block_size, n_blocks, inner_tol, seed, C.byref(lam),
+                                            C.byref(info)))
+        return lam.value, info
+
+    def workspace(self):
+        """A solve workspace sharing this hierarchy's operator (rt_hier_workspace_create)."""
+        ws = HierarchyGrid(self.ctx, self.params)
+        self._c(A.lib().rt_hier_workspace_create(self._h, C.byref(ws._h)))
+        ws._init_levels()
+        ws._parent = self  # destroyed before the parent
+        self._children.append(ws)
+        return ws
+
     def close(self):
+        for ws in getattr(self, "_children", []):
+            ws.close()
+        self._children = []
         if self._h:
             A.lib().rt_hier_destroy(self._h)
             self._h = C.c_void_p()
@@ -357,3 +378,13 @@ class HierarchyGrid:
             self.close()
         except Exception:
             pass
+
+
+def pcg_batch(grids, tol=1e-6, maxit=500):
+    """rt_pcg_batch: u <- K^-1 f on every hierarchy / workspace in one graph launch."""
+    hs = (C.c_void_p * len(grids))(*[g.handle.value for g in grids])
+    infos = (A.SolveInfo * len(grids))()
+    st = A.lib().rt_pcg_batch(hs, len(grids), tol, maxit, infos)
+    if st not in (A.RT_OK, A.RT_ENOCONV):
+        check(st, grids[0].ctx.handle)
+    return list(infos)
