@@ -103,6 +103,7 @@ typedef struct rt_level_info {
 
 typedef struct rt_ctx rt_ctx;
 typedef struct rt_hier rt_hier;
+typedef struct rt_unet rt_unet;
 
 /* ---- context ------------------------------------------------------------ */
 int rt_ctx_create(int device, void* cuda_stream /* NULL: own stream */, rt_ctx** out);
@@ -254,6 +255,42 @@ int rt_oc_update(rt_hier* h, float vgoal, float* lambda_out, int* trials_out);
  * update_stencil, worst-case solve, sensitivity+filter, OC update */
 int rt_oc_iteration(rt_hier* h, int method, int k, double inner_tol, uint64_t seed, float vgoal,
                     double* compliance_out);
+
+/* ---- learned preconditioner (3D U-Net, BF16 activations, FP32 accumulation) ---- */
+/* No reference counterpart.  One 3x3x3 convolution (zero padding 1) on the tensor cores:
+ * out[v][n] (+)= bias[n] + sum_{tap,c} w[n][tap][c] in[v + offset(tap)][c], optional ReLU.
+ * Device pointers; activations channels-last [v][stride] (v = x + X (y + Y z)), bf16;
+ * w bf16 [cout][27][cin] with tap = 9 (dz+1) + 3 (dy+1) + (dx+1); out bf16 or float
+ * (out_f32), accumulate only for float.  cin, cout multiples of 16 in [16, 128]. */
+int rt_unet_conv3(rt_ctx* c, const void* in, int in_stride, int cin, const void* w, const float* bias, int cout,
+                  void* out, int out_stride, int out_f32, int relu, int accumulate, int X, int Y, int Z);
+
+/* The U-Net (levels of 16/32/48/64 channels, two 3x3x3 convolutions + ReLU per level and side,
+ * 2x2x2 average pooling, nearest upsampling with skip concatenation, 1x1x1 head to 3
+ * channels; 684,851 parameters) over an X x Y x Z node box; weights He-initialised from seed. */
+int rt_unet_create(rt_ctx* c, int X, int Y, int Z, uint64_t seed, rt_unet** out);
+void rt_unet_destroy(rt_unet* u);
+long long rt_unet_n_params(rt_unet* u);
+/* FP32 master parameters (host arrays of rt_unet_n_params floats) */
+int rt_unet_get_params(rt_unet* u, float* host);
+int rt_unet_set_params(rt_unet* u, const float* host);
+/* forward pass: in bf16 [V][16] and out float [V][3] device buffers (V = X Y Z) */
+int rt_unet_forward(rt_unet* u, const void* in, float* out);
+/* mean-squared-error gradients of one sample (no update); grads_host may be null */
+int rt_unet_gradients(rt_unet* u, const void* in, const float* tgt, double* loss, float* grads_host);
+/* one Adam step (b1 0.9, b2 0.999) on a batch of device samples in [batch][V][16], tgt [batch][V][3] */
+int rt_unet_train_step(rt_unet* u, int batch, const void* in, const float* tgt, float lr, double* loss);
+/* output unit of the network (rms of the scaled targets, fixed by the first harvest) */
+double rt_unet_output_scale(rt_unet* u);
+int rt_unet_set_output_scale(rt_unet* u, double oscale);
+/* one (density, residual, MG-error) training sample from hierarchy h (node box = the network's):
+ * a random load, k_iter plain MG-PCG iterations give the residual r; input = packed (log density,
+ * r / rms(r), support flag), target = (K^-1 r - Vcycle(r)) / rms(r) / output unit */
+int rt_unet_harvest(rt_hier* h, rt_unet* u, int k_iter, uint64_t seed, void* in_out, float* tgt_out);
+/* use the network inside rt_pcg / rt_worst_case: z = Vcycle(r) + N(rho, r); the correction is
+ * switched off for the rest of a solve once an iteration fails to reduce ||r|| below
+ * fallback_ratio x its previous value (the plain V-cycle is the fallback).  u = null detaches. */
+int rt_hier_set_learned(rt_hier* h, rt_unet* u, double fallback_ratio);
 
 #ifdef __cplusplus
 }

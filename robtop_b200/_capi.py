@@ -108,6 +108,19 @@ SIGNATURES = {
     "rt_worst_case_block": (I, [P, I, I, D, C.c_uint64, C.POINTER(D), C.POINTER(SolveInfo)]),
     "rt_hier_workspace_create": (I, [P, C.POINTER(P)]),
     "rt_pcg_batch": (I, [C.POINTER(P), I, D, I, C.POINTER(SolveInfo)]),
+    "rt_unet_conv3": (I, [P, P, I, I, P, P, I, P, I, I, I, I, I, I, I]),
+    "rt_unet_create": (I, [P, I, I, I, C.c_uint64, C.POINTER(P)]),
+    "rt_unet_destroy": (None, [P]),
+    "rt_unet_n_params": (C.c_longlong, [P]),
+    "rt_unet_get_params": (I, [P, P]),
+    "rt_unet_set_params": (I, [P, P]),
+    "rt_unet_forward": (I, [P, P, P]),
+    "rt_unet_gradients": (I, [P, P, P, C.POINTER(D), P]),
+    "rt_unet_train_step": (I, [P, I, P, P, F, C.POINTER(D)]),
+    "rt_unet_output_scale": (D, [P]),
+    "rt_unet_set_output_scale": (I, [P, D]),
+    "rt_unet_harvest": (I, [P, P, I, C.c_uint64, P, P]),
+    "rt_hier_set_learned": (I, [P, P, D]),
     "rt_sensitivity": (I, [P, I]),
     "rt_filter_sensitivity": (I, [P, F]),
     "rt_oc_update": (I, [P, F, C.POINTER(F), C.POINTER(I)]),

@@ -11,10 +11,12 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
 #include "rt_internal.h"
+#include "rt_unet.h"
 
 // ---------------------------------------------------------------------------
 // errors, launch accounting
@@ -339,6 +341,7 @@ static void ws_sync(rt_hier* w) {
     w->Qgal = p->Qgal; w->Qgal_ratio = p->Qgal_ratio;
     w->use_graphs = p->use_graphs;
     w->graph_epoch = p->graph_epoch;
+    w->unet = nullptr;  // the network's activation buffers cannot be shared by concurrent solves
 }
 
 #define RT_NOT_WORKSPACE(h)                                                                                   \
@@ -365,6 +368,8 @@ static int build_hier(rt_ctx* c, const rt_params* p, int nx, int ny, int nz, uin
     h->ctx = c;
     h->uid = next_uid();
     h->P = *p;
+    // RT_GRAPHS=0 runs the PCG loop as individual launches (same kernels; for per-launch profilers)
+    if (const char* g = std::getenv("RT_GRAPHS")) h->use_graphs = std::atoi(g) != 0;
     *out = h;  // the caller releases a partially built hierarchy on failure
     // level chain on the device: halve while more than 400 elements are solid (grid/Grid.cpp:488)
     struct Chain { int nx, ny, nz; uint8_t* e; long cnt; };
@@ -1207,6 +1212,8 @@ static int precondition(rt_hier* h, const double* r, double* z, const double* rr
         L.u = saved_u;
         RT_CHECK(s);
     }
+    // learned correction z += N(rho, r), switched off on the device by the gate in scal[28]
+    if (h->unet) RT_CHECK(rtu::correct(h->unet, h, r, rr_dev, h->scal + 28, z));
     return RT_OK;
 }
 
@@ -1226,6 +1233,10 @@ __global__ void k_pcg_tail(double* __restrict__ scal, cudaGraphConditionalHandle
     const double it = scal[24] + 1.0;
     scal[24] = it;
     scal[12] = scal[10];
+    // learned-correction fallback: off for the rest of the solve once an iteration's residual
+    // norm did not drop below ratio x the previous one
+    if (scal[28] != 0.0 && scal[29] > 0.0 && !(scal[21] <= scal[27] * scal[27] * scal[29])) scal[28] = 0.0;
+    scal[29] = scal[21];
     if (use_cond) {
         const double rr = scal[21], bb = scal[22] > 0 ? scal[22] : 1.0;
         const bool go = isfinite(rr) && sqrt(rr) > scal[25] * sqrt(bb) && it < scal[26];
@@ -1261,7 +1272,8 @@ static int pcg_graph_run(rt_hier* h, double* x, double* r, bool no_support) {
     const uint64_t key = ((uint64_t)(uintptr_t)x * 1315423911ull) ^ ((uint64_t)h->P.precision << 1) ^
                          ((uint64_t)h->P.smoother << 3) ^ ((uint64_t)h->P.pre_sweeps << 6) ^
                          ((uint64_t)h->P.post_sweeps << 11) ^ ((uint64_t)no_support << 16) ^
-                         ((uint64_t)(h->P.jacobi_omega * 1e6) << 20) ^ ((uint64_t)h->graph_epoch << 40);
+                         ((uint64_t)(h->P.jacobi_omega * 1e6) << 20) ^ ((uint64_t)h->graph_epoch << 40) ^
+                         ((uint64_t)(uintptr_t)h->unet * 2654435761ull);
     if (!h->pcg_exec || h->pcg_key != key) {
         if (h->pcg_exec) { cudaGraphExecDestroy(h->pcg_exec); h->pcg_exec = nullptr; }
         if (h->pcg_graph) { cudaGraphDestroy(h->pcg_graph); h->pcg_graph = nullptr; }
@@ -1327,8 +1339,9 @@ static int pcg_core(rt_hier* h, double* x, const double* b, double tol, int maxi
     const bool no_support = (h->P.mode == RT_MODE_NSCF || h->P.mode == RT_MODE_NSFF);
     if (no_support && h->Ru == nullptr) RT_CHECK(rtk::rigid_nodes(h));
     if (rel > tol && maxit > 0) {
-        // loop state on the device: scal[24] iteration count, scal[25] tol, scal[26] maxit
-        double st[3] = {0.0, tol, (double)maxit};
+        // loop state on the device: scal[24] iteration count, scal[25] tol, scal[26] maxit,
+        // scal[27..29] learned-correction fallback ratio, gate, previous r.r
+        double st[6] = {0.0, tol, (double)maxit, h->unet_fallback, h->unet ? 1.0 : 0.0, s[0]};
         memcpy(h->ctx->hscal + 8, st, sizeof(st));
         RT_CUDA(h->ctx, cudaMemcpyAsync(h->scal + 24, h->ctx->hscal + 8, sizeof(st), cudaMemcpyHostToDevice,
                                         h->ctx->stream));
@@ -1921,6 +1934,8 @@ __global__ void k_pcg_start(double* __restrict__ scal, double tol, double maxit,
     scal[24] = 0.0;
     scal[25] = tol;
     scal[26] = maxit;
+    scal[28] = 0.0;  // batched instances run without the learned correction
+    scal[29] = scal[21];
     const double rr = scal[21], bb = scal[22] > 0 ? scal[22] : 1.0;
     const bool go = isfinite(rr) && sqrt(rr) > tol * sqrt(bb) && maxit > 0;
     cudaGraphSetConditional(cond, go ? 1u : 0u);
@@ -2320,4 +2335,85 @@ extern "C" int rt_worst_case_block(rt_hier* h, int block_size, int n_blocks, dou
     loc.seconds = ms * 1e-3;
     if (info) *info = loc;
     return s;
+}
+
+// ---------------------------------------------------------------------------
+// learned preconditioner: attach a network, harvest training samples
+// ---------------------------------------------------------------------------
+extern "C" int rt_hier_set_learned(rt_hier* h, rt_unet* u, double fallback_ratio) {
+    if (!h) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
+    if (u && !rtu::box_matches(u, h))
+        return rt_fail(h->ctx, RT_EINVAL, "the network's box must equal the finest level's node box");
+    if (u && !(fallback_ratio > 0)) return rt_fail(h->ctx, RT_EINVAL, "fallback ratio must be positive");
+    h->unet = u;
+    h->unet_fallback = fallback_ratio;
+    h->graph_epoch++;
+    return RT_OK;
+}
+
+__global__ void k_zero_fixed(long n, long nv, const uint8_t* __restrict__ vact, const uint8_t* __restrict__ vfix,
+                             int ws, double* __restrict__ f) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const long v = i % nv;
+        if (!vact[v] || (ws && vfix[v])) f[i] = 0.0;
+    }
+}
+
+// one training sample from the solver: a random load on the free nodes, k PCG iterations
+// (plain V-cycle) from zero give the residual r; the input packs (density, r), the target is
+// the V-cycle's error on r: K^-1 r (PCG to 1e-10) minus one V-cycle applied to r
+extern "C" int rt_unet_harvest(rt_hier* h, rt_unet* u, int k_iter, uint64_t seed, void* in_out, float* tgt_out) {
+    if (!h || !u || !in_out || !tgt_out || k_iter < 0) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
+    RT_CHECK(need_stencil(h));
+    rt_ctx* c = h->ctx;
+    if (!rtu::box_matches(u, h)) return rt_fail(c, RT_EINVAL, "the network's box must equal the finest node box");
+    if (no_support_mode(h)) return rt_fail(c, RT_EINVAL, "training samples need a supported structure");
+    rt_level& L = h->L[0];
+    const long n = 3 * L.nv;
+    rt_unet* saved = h->unet;
+    h->unet = nullptr;
+    double* zv = nullptr;
+    int s = RT_OK;
+    auto step = [&](int st) { if (s == RT_OK) s = st; return s == RT_OK; };
+    if (cudaMallocAsync(&zv, sizeof(double) * n, c->stream) != cudaSuccess) {
+        h->unet = saved;
+        return rt_fail(c, RT_ENOMEM, "harvest scratch");
+    }
+    step(rtk::rng_uniform(h, seed, n, L.f));
+    if (s == RT_OK)
+        step(rt_launch(c, "zero_fixed", [&] {
+            k_zero_fixed<<<(unsigned)std::min<long>((n + 255) / 256, c->sm_count * 16L), 256, 0, c->stream>>>(
+                n, L.nv, L.vact, h->vfix, h->has_support ? 1 : 0, L.f);
+        }));
+    if (s == RT_OK) cudaMemsetAsync(L.u, 0, sizeof(double) * n, c->stream);
+    if (s == RT_OK) step(pcg_prologue(h, L.u, L.f));
+    if (s == RT_OK) {
+        const double st[6] = {0.0, 0.0, (double)k_iter, 1.0, 0.0, 0.0};
+        memcpy(c->hscal + 8, st, sizeof(st));
+        cudaMemcpyAsync(h->scal + 24, c->hscal + 8, sizeof(st), cudaMemcpyHostToDevice, c->stream);
+    }
+    for (int i = 0; i < k_iter && s == RT_OK; i++) step(pcg_body(h, L.u, h->rr, false, 0, 0));
+    // r_k becomes the right-hand side; r.r in scal[35]
+    if (s == RT_OK) cudaMemcpyAsync(L.f, h->rr, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream);
+    if (s == RT_OK) step(rtk::dot(h, n, L.f, L.f, h->scal + 35));
+    if (s == RT_OK) step(rtu::pack(u, h, L.f, h->scal + 35));
+    if (s == RT_OK)
+        cudaMemcpyAsync(in_out, rtu::input(u), sizeof(__nv_bfloat16) * 16 * rtu::voxels(u), cudaMemcpyDeviceToDevice,
+                        c->stream);
+    if (s == RT_OK) step(precondition(h, L.f, zv, h->scal + 35));
+    rt_solve_info si;
+    memset(&si, 0, sizeof(si));
+    int vc = 0;
+    if (s == RT_OK) cudaMemsetAsync(L.u, 0, sizeof(double) * n, c->stream);
+    if (s == RT_OK) step(pcg_core(h, L.u, L.f, 1e-10, 2000, &si, &vc));
+    if (s == RT_OK) step(rtu::target(u, h, L.u, zv, h->scal + 35, tgt_out));
+    cudaFreeAsync(zv, c->stream);
+    const cudaError_t e = cudaStreamSynchronize(c->stream);
+    h->unet = saved;
+    if (s != RT_OK) return s;
+    if (e != cudaSuccess) return rt_fail(c, RT_ECUDA, "harvest: %s", cudaGetErrorString(e));
+    if (si.status != RT_OK) return rt_fail(c, RT_ENOCONV, "harvest: the exact-error solve did not converge");
+    return RT_OK;
 }

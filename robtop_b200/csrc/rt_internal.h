@@ -122,6 +122,10 @@ struct rt_hier {
     cudaGraphExec_t pcg_exec = nullptr;
     uint64_t pcg_key = 0;
     uint64_t graph_epoch = 0;  // bumped whenever captured pointers may change
+    // learned correction added to the V-cycle inside PCG (rt_hier_set_learned); scal[27] holds the
+    // fallback ratio, scal[28] the gate (1 while active), scal[29] the previous iteration's r.r
+    struct rt_unet* unet = nullptr;
+    double unet_fallback = 1.0;
 };
 
 #define RT_RED_BLOCKS 296

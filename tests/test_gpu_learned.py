@@ -1,0 +1,101 @@
+"""The learned preconditioner end to end (GPU): samples harvested from the solver, training
+on the library's own forward/backward kernels, and MG-PCG with z = Vcycle(r) + N(rho, r)
+on a held-out density, against the same PCG without the network.
+
+What the network gains is measured and written to ``learned_gain.json`` in the pytest
+temporary directory; the tests assert what must hold whatever the gain: training lowers the
+loss, the learned PCG converges to the same tolerance and solution, and the fallback gate
+turns the correction off when the residual stops dropping.
+"""
+import json
+
+import numpy as np
+import pytest
+
+import robtop_b200 as rb
+from robtop_b200 import configs, learned
+
+pytestmark = pytest.mark.gpu
+
+DIMS = (24, 16, 16)
+
+
+def _grid(ctx, cfg, precision=rb.FP64, smoother=rb.SMOOTH_SGS, sweeps=1):
+    params = rb.default_params(mode=cfg["mode"], youngs_modulus=1e6, poisson_ratio=0.4, power_penalty=3.0,
+                               min_rho=1e-3, precision=precision, smoother=smoother, pre_sweeps=sweeps,
+                               post_sweeps=sweeps)
+    G = rb.HierarchyGrid(ctx, params)
+    G.genFromBox(cfg["eact"])
+    G[0].setRho(cfg["rho"].ravel())
+    G.set_support(cfg["vfix"])
+    G.update_stencil()
+    return G
+
+
+def _load(G, cfg, seed):
+    free = G[0].getVact().astype(np.float64) * (1.0 - cfg["vfix"].ravel().astype(np.float64))
+    return np.random.default_rng(seed).standard_normal(3 * G[0].nv) * np.tile(free, 3)
+
+
+@pytest.fixture(scope="module")
+def trained():
+    ctx = rb.Context(0)
+    grids = [_grid(ctx, configs.worst_case_box(*DIMS, seed=s)) for s in range(4)]
+    net = learned.UNet.for_grid(grids[0], seed=1)
+    samples = []
+    for i, G in enumerate(grids):
+        for k in (1, 3, 8):
+            samples.append(learned.harvest(G, net, k, seed=100 * i + k))
+    assert net.output_scale > 0
+    losses = learned.train(net, samples, steps=200, batch=4, lr=2e-3, seed=0)
+    for G in grids:
+        G.close()
+    yield ctx, net, losses
+    net.close()
+    ctx.close()
+
+
+def test_training_lowers_the_loss(trained):
+    _, _, losses = trained
+    assert np.all(np.isfinite(losses))
+    assert np.mean(losses[-20:]) < 0.7 * np.mean(losses[:5])
+
+
+def test_learned_pcg_converges_and_reports_gain(trained, tmp_path):
+    ctx, net, losses = trained
+    cfg = configs.worst_case_box(*DIMS, seed=9)
+    G = _grid(ctx, cfg)
+    f = _load(G, cfg, 5)
+    G[0].setForce(f)
+    G[0].setDisplacement(np.zeros_like(f))
+    plain = G.pcg(1e-6, 500)
+    u_plain = G[0].getDisplacement()
+    learned.attach(G, net, fallback_ratio=1.0)
+    G[0].setDisplacement(np.zeros_like(f))
+    lrn = G.pcg(1e-6, 500)
+    u_lrn = G[0].getDisplacement()
+    assert plain.status == rb._capi.RT_OK and lrn.status == rb._capi.RT_OK
+    assert lrn.rel_residual <= 1e-6
+    assert np.linalg.norm(u_lrn - u_plain) <= 1e-4 * np.linalg.norm(u_plain)
+    # the gate: a ratio no iteration can meet turns the correction off after one iteration
+    learned.attach(G, net, fallback_ratio=1e-12)
+    G[0].setDisplacement(np.zeros_like(f))
+    gated = G.pcg(1e-6, 500)
+    assert gated.status == rb._capi.RT_OK
+    assert abs(gated.iterations - plain.iterations) <= 3
+    learned.attach(G, None)
+    (tmp_path / "learned_gain.json").write_text(json.dumps({
+        "plain_iterations": plain.iterations, "learned_iterations": lrn.iterations,
+        "plain_seconds": plain.seconds, "learned_seconds": lrn.seconds,
+        "iteration_gain": plain.iterations / max(lrn.iterations, 1),
+        "final_loss": float(np.mean(losses[-20:])), "initial_loss": float(np.mean(losses[:5]))}))
+    print("learned preconditioner:", plain.iterations, "->", lrn.iterations, "PCG iterations")
+    G.close()
+
+
+def test_network_box_must_match(trained):
+    ctx, net, _ = trained
+    G = _grid(ctx, configs.worst_case_box(20, 16, 16, seed=2))
+    with pytest.raises(rb.RTError):
+        learned.attach(G, net)
+    G.close()
