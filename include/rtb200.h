@@ -107,6 +107,8 @@ typedef struct rt_unet rt_unet;
 
 /* ---- context ------------------------------------------------------------ */
 int rt_ctx_create(int device, void* cuda_stream /* NULL: own stream */, rt_ctx** out);
+/* releases the caller's handle (call once); hierarchies, workspaces and networks made on the
+ * context keep it alive until they are destroyed, in any order */
 void rt_ctx_destroy(rt_ctx* ctx);
 const char* rt_last_error(rt_ctx* ctx);
 int rt_ctx_sync(rt_ctx* ctx);

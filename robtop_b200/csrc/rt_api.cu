@@ -122,8 +122,20 @@ extern "C" int rt_ctx_create(int device, void* stream, rt_ctx** out) {
     return RT_OK;
 }
 
-extern "C" void rt_ctx_destroy(rt_ctx* c) {
-    if (!c) return;
+void rt_ctx_retain(rt_ctx* c) {
+    if (c) c->refs++;
+}
+
+static void ctx_free(rt_ctx* c);
+
+void rt_ctx_release(rt_ctx* c) {
+    if (c && --c->refs == 0) ctx_free(c);
+}
+
+// the caller's reference: the context lives on until its last hierarchy, workspace or network is destroyed
+extern "C" void rt_ctx_destroy(rt_ctx* c) { rt_ctx_release(c); }
+
+static void ctx_free(rt_ctx* c) {
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     profile_drain(c);
@@ -285,7 +297,9 @@ static void free_workspace(rt_hier* w) {
     cudaFree(w->partials); cudaFree(w->scal);
     if (w->pcg_exec) cudaGraphExecDestroy(w->pcg_exec);
     if (w->pcg_graph) cudaGraphDestroy(w->pcg_graph);
+    rt_ctx* c = w->ctx;
     delete w;
+    rt_ctx_release(c);
 }
 
 static void free_hier(rt_hier* h) {
@@ -313,7 +327,9 @@ static void free_hier(rt_hier* h) {
     cudaFree(h->scal); cudaFree(h->Qgal); cudaFree(h->dinv64); cudaFree(h->dinv32);
     if (h->pcg_exec) cudaGraphExecDestroy(h->pcg_exec);
     if (h->pcg_graph) cudaGraphDestroy(h->pcg_graph);
+    rt_ctx* c = h->ctx;
     delete h;
+    rt_ctx_release(c);
 }
 
 // refresh a workspace's copy of its parent's operator (buffers, settings, launch shapes)
@@ -366,6 +382,7 @@ static int upload_KE(rt_hier* h) {
 static int build_hier(rt_ctx* c, const rt_params* p, int nx, int ny, int nz, uint8_t* eact_dev, rt_hier** out) {
     rt_hier* h = new rt_hier();
     h->ctx = c;
+    rt_ctx_retain(c);
     h->uid = next_uid();
     h->P = *p;
     // RT_GRAPHS=0 runs the PCG loop as individual launches (same kernels; for per-launch profilers)
@@ -1004,7 +1021,10 @@ __global__ void k_lmax_finish(const double* __restrict__ xx, double* __restrict_
     }
 }
 
-static double* cheby_table(rt_hier* h, int lvl) { return h->scal + RT_SCAL_CHEB + 2 * RT_CHEBY_MAXK * lvl; }
+// the tables belong to the operator: a workspace reads its parent's
+static double* cheby_table(rt_hier* h, int lvl) {
+    return (h->parent ? h->parent->scal : h->scal) + RT_SCAL_CHEB + 2 * RT_CHEBY_MAXK * lvl;
+}
 
 // lmax(D^-1 A) of a level by 15 power steps (D^-1 A v = v - jacobi(v; f = 0, omega = 1)),
 // left on the device for the Chebyshev kernels
@@ -1882,6 +1902,7 @@ static int make_workspace(rt_hier* p, rt_hier** out) {
     rt_hier* w = new rt_hier();
     *out = w;  // the caller frees a partially built workspace
     w->ctx = c;
+    rt_ctx_retain(c);
     w->uid = next_uid();
     w->parent = p;
     w->L.resize(p->L.size());

@@ -18,6 +18,9 @@ struct rt_kstat {
 };
 
 struct rt_ctx {
+    // references: the caller's handle plus every hierarchy, workspace and network made on the
+    // context; rt_ctx_destroy drops the caller's, the last release frees the context
+    int refs = 1;
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -131,6 +134,9 @@ struct rt_hier {
 #define RT_RED_BLOCKS 296
 #define RT_PARTIALS (148 * 64)  // block partial sums: up to 64 values from 148 blocks
 #define RT_NSCAL 1024           // device scalar slots
+
+void rt_ctx_retain(rt_ctx* c);
+void rt_ctx_release(rt_ctx* c);
 
 // error helpers -------------------------------------------------------------
 int rt_fail(rt_ctx* c, int code, const char* fmt, ...);

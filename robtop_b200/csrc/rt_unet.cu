@@ -113,7 +113,9 @@ static void unet_free(rt_unet* u) {
                     u->out, u->g_out, u->g_d0, u->g_x, u->g_cat0, u->g_cat1, u->g_cat2, u->g_y, u->g_p, u->gpre,
                     u->dloss, u->err, u->dscal};
     for (void* p : ptrs) cudaFree(p);
+    rt_ctx* c = u->ctx;
     delete u;
+    rt_ctx_release(c);
 }
 
 static unsigned ew_blocks(rt_ctx* c, long n) {
@@ -353,6 +355,7 @@ extern "C" int rt_unet_create(rt_ctx* c, int X, int Y, int Z, uint64_t seed, rt_
     }
     rt_unet* u = new rt_unet();
     u->ctx = c;
+    rt_ctx_retain(c);
     u->X[0] = X; u->Y[0] = Y; u->Z[0] = Z;
     for (int l = 1; l < 4; l++) {
         u->X[l] = (u->X[l - 1] + 1) / 2;

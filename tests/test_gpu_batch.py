@@ -149,8 +149,25 @@ def test_block_lanczos_parity(name):
     u = G[0].getDisplacement()
     assert abs(np.linalg.norm(f) - 1) < 1e-9
     assert abs(f @ u - lam_b) <= 1e-6 * lam_b
-    # the rt_worst_case entry (block size 8, Krylov dimension rounded up to a multiple of 8)
-    lam_w, _ = G.worst_case(rb.WORST_BLOCK_LANCZOS, 32, 1e-10, seed=21)
+    # the rt_worst_case entry (block size 8, Krylov dimension rounded up to a multiple of 8): 8 block
+    # steps, so that the block Krylov polynomial has the degree of the 4 x 8 call above
+    lam_w, _ = G.worst_case(rb.WORST_BLOCK_LANCZOS, 64, 1e-10, seed=21)
     assert abs(lam_w - lo[0]) <= 1e-6 * abs(lo[0])
     G.close()
     ctx.close()
+
+
+def test_context_outlives_its_hierarchies():
+    # destroying the context first (as a garbage collector may) leaves its hierarchies usable
+    cfg = CONFIGS["worstcase"]()
+    ctx = rb.Context(0)
+    G = _grid(ctx, cfg, _params(cfg))
+    W = G.workspace()
+    rb.lib().rt_ctx_destroy(ctx.handle)
+    ctx._h = type(ctx._h)()  # the Python wrapper no longer owns the handle
+    f = _rhs(G, cfg, 3)
+    W[0].setForce(f)
+    W[0].setDisplacement(np.zeros_like(f))
+    assert W.pcg(1e-6, 500).status == rb._capi.RT_OK
+    W.close()
+    G.close()
