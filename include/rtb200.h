@@ -266,6 +266,9 @@ int rt_oc_iteration(rt_hier* h, int method, int k, double inner_tol, uint64_t se
  * (out_f32), accumulate only for float.  cin, cout multiples of 16 in [16, 128]. */
 int rt_unet_conv3(rt_ctx* c, const void* in, int in_stride, int cin, const void* w, const float* bias, int cout,
                   void* out, int out_stride, int out_f32, int relu, int accumulate, int X, int Y, int Z);
+/* kernel of every convolution in this process: 1 (default) halo tile (the input patch of P
+ * z-planes read once into shared memory, every tap a shifted descriptor), 0 per-tap gather */
+int rt_unet_set_conv_variant(int variant);
 
 /* The U-Net (levels of 16/32/48/64 channels, two 3x3x3 convolutions + ReLU per level and side,
  * 2x2x2 average pooling, nearest upsampling with skip concatenation, 1x1x1 head to 3

@@ -109,6 +109,7 @@ SIGNATURES = {
     "rt_hier_workspace_create": (I, [P, C.POINTER(P)]),
     "rt_pcg_batch": (I, [C.POINTER(P), I, D, I, C.POINTER(SolveInfo)]),
     "rt_unet_conv3": (I, [P, P, I, I, P, P, I, P, I, I, I, I, I, I, I]),
+    "rt_unet_set_conv_variant": (I, [I]),
     "rt_unet_create": (I, [P, I, I, I, C.c_uint64, C.POINTER(P)]),
     "rt_unet_destroy": (None, [P]),
     "rt_unet_n_params": (C.c_longlong, [P]),

@@ -103,6 +103,19 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
-__host__ __device__ constexpr uint32_t tmem_cols(int n) { return n <= 32 ? 32u : n <= 64 ? 64u : n <= 128 ? 128u : 256u; }
+// TMEM allocation size (a power of two >= 32) for n FP32 columns, n <= 512
+__host__ __device__ constexpr uint32_t tmem_cols(int n) {
+    return n <= 32 ? 32u : n <= 64 ? 64u : n <= 128 ? 128u : n <= 256 ? 256u : 512u;
+}
 
+}  // namespace rttc
+
+namespace rttc {
+// 16-byte global -> shared copy, zero-filled when src_bytes == 0 (Ampere-style asynchronous copy)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(smem)), "l"(gmem), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 }  // namespace rttc

@@ -51,6 +51,12 @@ extern "C" int rt_unet_conv3(rt_ctx* c, const void* in, int in_stride, int cin, 
     return RT_OK;
 }
 
+extern "C" int rt_unet_set_conv_variant(int variant) {
+    if (variant < 0 || variant > 1) return RT_EINVAL;
+    rtu::conv3_set_variant(variant);
+    return RT_OK;
+}
+
 // ---------------------------------------------------------------------------
 // the U-Net: 4 levels, 16/32/48/64 channels, two 3x3x3 convolutions (+ReLU) per level and
 // side, 2x2x2 average pooling, nearest upsampling with skip concatenation, 1x1x1 head

@@ -29,6 +29,7 @@ struct ConvArgs {
 int conv3_init(rt_ctx* c);
 int conv3(rt_ctx* c, const ConvArgs& a);
 size_t conv3_smem_bytes(int cin, int cout);
+void conv3_set_variant(int v);  // 1: halo tile (default), 0: per-tap gather
 
 }  // namespace rtu
 

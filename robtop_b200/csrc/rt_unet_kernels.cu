@@ -139,6 +139,167 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3_tc(ConvArgs a) {
     if (warp == 0) rttc::tmem_dealloc(tmem, ncols);
 }
 
+// ---------------------------------------------------------------------------
+// k_conv3_halo: the same convolution with the input read once per CTA.  A CTA owns an
+// 8 x 16 voxel patch over P consecutive z-planes; the patch's (P+2) x 18 x 10 halo is copied
+// into shared memory as [16-byte channel chunk][plane][y][x], which is the no-swizzle K-major
+// core-matrix layout of every tap's A operand at once: row m = x + 8 y of the patch is 16 B
+// after row m-1 within a patch row (8-row core matrix) and 160 B (one halo row) further per
+// patch row (SBO), the next channel chunk is one chunk plane further (LBO), and a tap
+// (dx, dy, dz) only moves the descriptor's start address.  Taps run outer: a tap's weights
+// are loaded once (two stages) and applied to all P planes, whose accumulators sit side by
+// side in TMEM (P x Cout columns).
+// ---------------------------------------------------------------------------
+constexpr int HALO_X = 10, HALO_Y = 18, HALO_V = HALO_X * HALO_Y;
+
+__global__ void __launch_bounds__(CONV_THREADS) k_conv3_halo(ConvArgs a, int P) {
+    extern __shared__ __align__(128) uint8_t sm[];
+    const int cin = a.cin, cout = a.cout, kch = cin / 8, npl = P + 2;
+    const uint32_t plane_b = HALO_V * 16;           // one plane of one channel chunk
+    const uint32_t lboA = (uint32_t)npl * plane_b;  // channel-chunk stride
+    const uint32_t halo_bytes = (uint32_t)kch * lboA;
+    const uint32_t wbytes = (uint32_t)cout * cin * 2;
+    uint8_t* sH = sm;
+    uint8_t* sW[2] = {sm + halo_bytes, sm + halo_bytes + wbytes};
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + halo_bytes + 2 * wbytes);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int x0 = blockIdx.x * 8, y0 = blockIdx.y * 16, z0 = blockIdx.z * P;
+    const uint32_t ncols = rttc::tmem_cols(P * cout);
+    if (tid == 0) {
+        rttc::mbar_init(&bar[0], 1);
+        rttc::mbar_init(&bar[1], 1);
+        rttc::fence_mbar_init();
+    }
+    if (warp == 0) rttc::tmem_alloc(tslot, ncols);
+    // halo planes z0-1 .. z0+P (zero outside the box); chunk index fastest for coalescing
+    const int nh = npl * HALO_V * kch;
+    for (int idx = tid; idx < nh; idx += CONV_THREADS) {
+        const int j = idx % kch, rest = idx / kch;
+        const int hv = rest % HALO_V, pl = rest / HALO_V;
+        const int gx = x0 - 1 + hv % HALO_X, gy = y0 - 1 + hv / HALO_X, gz = z0 - 1 + pl;
+        const bool inb = gx >= 0 && gx < a.X && gy >= 0 && gy < a.Y && gz >= 0 && gz < a.Z;
+        const __nv_bfloat16* src =
+            inb ? a.in + ((long)gx + (long)a.X * (gy + (long)a.Y * gz)) * a.in_stride + j * 8 : a.in;
+        rttc::cp_async16(sH + j * lboA + pl * plane_b + hv * 16, src, inb ? 16u : 0u);
+    }
+    // weights of a tap in the K-major layout: [chunk][out-channel group][8 rows][16 B]
+    const uint32_t lboB = (uint32_t)(cout / 8) * 128;
+    auto load_w = [&](int t, uint8_t* dst) {
+        for (int idx = tid; idx < cout * kch; idx += CONV_THREADS) {
+            const int n = idx / kch, j = idx - n * kch;
+            rttc::cp_async16(dst + j * lboB + (n >> 3) * 128 + (n & 7) * 16, a.w + ((long)n * 27 + t) * cin + j * 8,
+                             16u);
+        }
+    };
+    load_w(0, sW[0]);
+    rttc::cp_async_commit();
+    rttc::cp_async_wait_all();
+    rttc::fence_async_smem();
+    rttc::tc_fence_before();
+    __syncthreads();
+    rttc::tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const uint32_t idesc = rttc::idesc_bf16(CONV_TM, cout, 0, 0);
+    const uint32_t h0 = rttc::smem_u32(sH);
+    bool ok = true;
+    int last = -1;
+    for (int t = 0; t < 27; t++) {
+        const int b = t & 1;
+        if (tid == 0) {
+            rttc::tc_fence_after();
+            const int dx = t % 3 - 1, dy = (t / 3) % 3 - 1, dz = t / 9 - 1;
+            const uint32_t w0 = rttc::smem_u32(sW[b]);
+            for (int p = 0; p < P; p++) {
+                const uint32_t a0 = h0 + (uint32_t)(p + 1 + dz) * plane_b + (uint32_t)((1 + dy) * HALO_X + 1 + dx) * 16;
+                for (int kk = 0; kk < cin / 16; kk++) {
+                    const uint64_t ad = rttc::sdesc(a0 + 2 * kk * lboA, lboA, HALO_X * 16);
+                    const uint64_t bd = rttc::sdesc(w0 + 2 * kk * lboB, lboB, 128);
+                    rttc::mma_bf16(tmem + (uint32_t)(p * cout), ad, bd, idesc, (t > 0 || kk > 0) ? 1u : 0u);
+                }
+            }
+            rttc::mma_commit(&bar[b]);
+        }
+        last = t;
+        if (t + 1 < 27) {
+            // the other weight stage was read by tap t-1's MMAs
+            if (t >= 1) {
+                const bool w = rttc::mbar_wait(&bar[b ^ 1], ((t - 1) >> 1) & 1);
+                if (!__syncthreads_and(w)) {
+                    ok = false;
+                    break;
+                }
+            }
+            load_w(t + 1, sW[b ^ 1]);
+            rttc::cp_async_commit();
+            rttc::cp_async_wait_all();
+            rttc::fence_async_smem();
+            __syncthreads();
+        }
+    }
+    bool done = rttc::mbar_wait(&bar[last & 1], (last >> 1) & 1);
+    done = __syncthreads_and(done) != 0;
+    if (!ok || !done) {
+        if (tid == 0 && a.err) atomicExch(a.err, 1);
+    } else {
+        rttc::tc_fence_after();
+        const int x = x0 + (tid & 7), y = y0 + (tid >> 3);
+        for (int p = 0; p < P; p++) {
+            const int z = z0 + p;
+            const bool mv = x < a.X && y < a.Y && z < a.Z;
+            const long m = (long)x + (long)a.X * (y + (long)a.Y * z);
+            for (int c0 = 0; c0 < cout; c0 += 16) {
+                float v[16];
+                rttc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(p * cout + c0), v);
+                if (!mv) continue;
+#pragma unroll
+                for (int i = 0; i < 16; i++) {
+                    const float s = v[i] + (a.bias ? a.bias[c0 + i] : 0.f);
+                    v[i] = a.relu ? fmaxf(s, 0.f) : s;
+                }
+                if (a.out_f32) {
+                    float4* o = reinterpret_cast<float4*>(reinterpret_cast<float*>(a.out) + m * a.out_stride + c0);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        float4 val = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                        if (a.accumulate) {
+                            const float4 old = o[q];
+                            val.x += old.x; val.y += old.y; val.z += old.z; val.w += old.w;
+                        }
+                        o[q] = val;
+                    }
+                } else {
+                    __align__(16) __nv_bfloat162 pk[8];
+#pragma unroll
+                    for (int q = 0; q < 8; q++) pk[q] = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+                    uint4* o = reinterpret_cast<uint4*>(reinterpret_cast<__nv_bfloat16*>(a.out) + m * a.out_stride + c0);
+                    o[0] = *reinterpret_cast<const uint4*>(&pk[0]);
+                    o[1] = *reinterpret_cast<const uint4*>(&pk[4]);
+                }
+            }
+        }
+    }
+    rttc::tc_fence_before();
+    __syncthreads();
+    if (warp == 0) rttc::tmem_dealloc(tmem, ncols);
+}
+
+// planes per CTA and shared memory of k_conv3_halo (P = 0: the layer does not fit)
+static int halo_planes(int cin, int cout, size_t* smem) {
+    for (int P = 8; P >= 1; P /= 2) {
+        const size_t need = (size_t)(P + 2) * HALO_V * cin * 2 + 2 * (size_t)cout * cin * 2 + 32;
+        if (need <= 200 * 1024 && P * cout <= 512) {
+            const size_t maxc = 512 / rttc::tmem_cols(P * cout);
+            const size_t floor_b = 233472 / (maxc + 1);
+            *smem = need > floor_b ? need : floor_b;
+            return P;
+        }
+    }
+    return 0;
+}
+
+static int g_conv_variant = 1;  // 1: halo tile (default), 0: per-tap gather
+
 size_t conv3_smem_bytes(int cin, int cout) {
     const size_t need = 2 * (size_t)CONV_TM * cin * 2 + 2 * (size_t)cout * cin * 2 + 32;
     // keep the CTAs an SM can hold within its 512 TMEM columns: more than 512 / ncols of
@@ -149,16 +310,26 @@ size_t conv3_smem_bytes(int cin, int cout) {
 }
 
 int conv3_init(rt_ctx* c) {
-    const cudaError_t e = cudaFuncSetAttribute(k_conv3_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaError_t e = cudaFuncSetAttribute(k_conv3_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_conv3_halo, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
     if (e != cudaSuccess) return rt_fail(c, RT_ECUDA, "conv3 smem attribute: %s", cudaGetErrorString(e));
     return RT_OK;
 }
+
+void conv3_set_variant(int v) { g_conv_variant = v ? 1 : 0; }
 
 int conv3(rt_ctx* c, const ConvArgs& a) {
     if (a.cin % 16 || a.cout % 16 || a.cin < 16 || a.cout < 16 || a.cin > 128 || a.cout > 128 || a.in_stride % 8 ||
         a.out_stride % (a.out_f32 ? 4 : 8))
         return rt_fail(c, RT_EINVAL, "conv3: channel counts must be multiples of 16 in [16, 128] (got %d -> %d)",
                        a.cin, a.cout);
+    size_t hsmem = 0;
+    const int P = g_conv_variant ? halo_planes(a.cin, a.cout, &hsmem) : 0;
+    if (P > 0) {
+        const dim3 grid((unsigned)((a.X + 7) / 8), (unsigned)((a.Y + 15) / 16), (unsigned)((a.Z + P - 1) / P));
+        return rt_launch(c, "unet_conv3_halo", [&] { k_conv3_halo<<<grid, CONV_THREADS, hsmem, c->stream>>>(a, P); });
+    }
     const long V = (long)a.X * a.Y * a.Z;
     const unsigned blocks = (unsigned)((V + CONV_TM - 1) / CONV_TM);
     const size_t smem = conv3_smem_bytes(a.cin, a.cout);

@@ -26,9 +26,11 @@ def _ref_conv(inp, w, bias, X, Y, Z, cin, cout, relu):
 
 
 @pytest.mark.parametrize("cin,cout,dims", [(16, 16, (19, 13, 11)), (48, 32, (9, 17, 10)), (112, 48, (8, 8, 7)),
-                                           (32, 112, (16, 16, 3)), (64, 64, (40, 5, 6))])
+                                           (32, 112, (16, 16, 3)), (64, 64, (40, 5, 6)), (16, 64, (21, 35, 19))])
 @pytest.mark.parametrize("relu", [0, 1])
-def test_conv3_tc_matches_torch(cin, cout, dims, relu):
+@pytest.mark.parametrize("variant", [1, 0])
+def test_conv3_tc_matches_torch(cin, cout, dims, relu, variant):
+    rb.lib().rt_unet_set_conv_variant(variant)
     X, Y, Z = dims
     V = X * Y * Z
     g = torch.Generator().manual_seed(cin * 1000 + cout + relu)
@@ -61,6 +63,7 @@ def test_conv3_tc_matches_torch(cin, cout, dims, relu):
                                           None, cout, C.c_void_p(acc.data_ptr()), cout, 1, 0, 1, X, Y, Z), ctx.handle)
     ref_nb = _ref_conv(inp, w, None, X, Y, Z, cin, cout, 0)
     assert (acc.cpu() - 1.0 - ref_nb).abs().max().item() <= 2e-5 * scale + 1e-5
+    rb.lib().rt_unet_set_conv_variant(1)
     ctx.close()
 
 
