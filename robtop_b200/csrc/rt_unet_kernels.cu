@@ -152,16 +152,18 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3_tc(ConvArgs a) {
 // ---------------------------------------------------------------------------
 constexpr int HALO_X = 10, HALO_Y = 18, HALO_V = HALO_X * HALO_Y;
 
-__global__ void __launch_bounds__(CONV_THREADS) k_conv3_halo(ConvArgs a, int P) {
+__global__ void __launch_bounds__(CONV_THREADS) k_conv3_halo(ConvArgs a, int P, int G) {
     extern __shared__ __align__(128) uint8_t sm[];
     const int cin = a.cin, cout = a.cout, kch = cin / 8, npl = P + 2;
+    const int ngroups = 27 / G, nstage = ngroups > 1 ? 2 : 1;
     const uint32_t plane_b = HALO_V * 16;           // one plane of one channel chunk
     const uint32_t lboA = (uint32_t)npl * plane_b;  // channel-chunk stride
     const uint32_t halo_bytes = (uint32_t)kch * lboA;
-    const uint32_t wbytes = (uint32_t)cout * cin * 2;
+    const uint32_t wtap = (uint32_t)cout * cin * 2;  // one tap's weights
+    const uint32_t wstage = (uint32_t)G * wtap;      // one stage: G taps
     uint8_t* sH = sm;
-    uint8_t* sW[2] = {sm + halo_bytes, sm + halo_bytes + wbytes};
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + halo_bytes + 2 * wbytes);
+    uint8_t* sW[2] = {sm + halo_bytes, sm + halo_bytes + (nstage > 1 ? wstage : 0)};
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + halo_bytes + nstage * wstage);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2);
     const int tid = threadIdx.x, warp = tid >> 5;
     const int x0 = blockIdx.x * 8, y0 = blockIdx.y * 16, z0 = blockIdx.z * P;
@@ -183,13 +185,15 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3_halo(ConvArgs a, int P) 
             inb ? a.in + ((long)gx + (long)a.X * (gy + (long)a.Y * gz)) * a.in_stride + j * 8 : a.in;
         rttc::cp_async16(sH + j * lboA + pl * plane_b + hv * 16, src, inb ? 16u : 0u);
     }
-    // weights of a tap in the K-major layout: [chunk][out-channel group][8 rows][16 B]
+    // the weights of taps [g G, (g+1) G), each in the K-major layout [chunk][out-channel group][8 rows][16 B]
     const uint32_t lboB = (uint32_t)(cout / 8) * 128;
-    auto load_w = [&](int t, uint8_t* dst) {
-        for (int idx = tid; idx < cout * kch; idx += CONV_THREADS) {
-            const int n = idx / kch, j = idx - n * kch;
-            rttc::cp_async16(dst + j * lboB + (n >> 3) * 128 + (n & 7) * 16, a.w + ((long)n * 27 + t) * cin + j * 8,
-                             16u);
+    auto load_w = [&](int g, uint8_t* dst) {
+        const int n_all = G * cout * kch;
+        for (int idx = tid; idx < n_all; idx += CONV_THREADS) {
+            const int tt = idx / (cout * kch), r = idx - tt * (cout * kch);
+            const int n = r / kch, j = r - n * kch;
+            rttc::cp_async16(dst + tt * wtap + j * lboB + (n >> 3) * 128 + (n & 7) * 16,
+                             a.w + ((long)n * 27 + g * G + tt) * cin + j * 8, 16u);
         }
     };
     load_w(0, sW[0]);
@@ -204,33 +208,42 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3_halo(ConvArgs a, int P) 
     const uint32_t h0 = rttc::smem_u32(sH);
     bool ok = true;
     int last = -1;
-    for (int t = 0; t < 27; t++) {
-        const int b = t & 1;
+    for (int g = 0; g < ngroups; g++) {
+        const int b = g & 1;
         if (tid == 0) {
             rttc::tc_fence_after();
-            const int dx = t % 3 - 1, dy = (t / 3) % 3 - 1, dz = t / 9 - 1;
-            const uint32_t w0 = rttc::smem_u32(sW[b]);
-            for (int p = 0; p < P; p++) {
-                const uint32_t a0 = h0 + (uint32_t)(p + 1 + dz) * plane_b + (uint32_t)((1 + dy) * HALO_X + 1 + dx) * 16;
-                for (int kk = 0; kk < cin / 16; kk++) {
-                    const uint64_t ad = rttc::sdesc(a0 + 2 * kk * lboA, lboA, HALO_X * 16);
-                    const uint64_t bd = rttc::sdesc(w0 + 2 * kk * lboB, lboB, 128);
-                    rttc::mma_bf16(tmem + (uint32_t)(p * cout), ad, bd, idesc, (t > 0 || kk > 0) ? 1u : 0u);
+            // a descriptor's start field is (address >> 4): moving the operand is an integer add
+            const uint64_t ad0 = rttc::sdesc(h0, lboA, HALO_X * 16);
+            const uint64_t bd0 = rttc::sdesc(rttc::smem_u32(sW[b]), lboB, 128);
+            const uint32_t a_kk = (2 * lboA) >> 4, b_kk = (2 * lboB) >> 4, a_pl = plane_b >> 4;
+            const int nk = cin / 16;
+            for (int tt = 0; tt < G; tt++) {
+                const int t = g * G + tt;
+                const int dx = t % 3 - 1, dy = (t / 3) % 3 - 1, dz = t / 9 - 1;
+                const uint64_t at = ad0 + (((uint32_t)(1 + dz) * plane_b + (uint32_t)((1 + dy) * HALO_X + 1 + dx) * 16) >> 4);
+                const uint64_t bt = bd0 + ((uint32_t)tt * wtap >> 4);
+                const uint32_t acc0 = t > 0 ? 1u : 0u;
+                for (int p = 0; p < P; p++) {
+                    const uint64_t ap = at + (uint64_t)p * a_pl;
+                    const uint32_t dcol = tmem + (uint32_t)(p * cout);
+                    for (int kk = 0; kk < nk; kk++)
+                        rttc::mma_bf16(dcol, ap + (uint64_t)kk * a_kk, bt + (uint64_t)kk * b_kk, idesc,
+                                       (acc0 | (uint32_t)kk) ? 1u : 0u);
                 }
             }
             rttc::mma_commit(&bar[b]);
         }
-        last = t;
-        if (t + 1 < 27) {
-            // the other weight stage was read by tap t-1's MMAs
-            if (t >= 1) {
-                const bool w = rttc::mbar_wait(&bar[b ^ 1], ((t - 1) >> 1) & 1);
+        last = g;
+        if (g + 1 < ngroups) {
+            // the other stage was read by group g-1's MMAs
+            if (g >= 1) {
+                const bool w = rttc::mbar_wait(&bar[b ^ 1], ((g - 1) >> 1) & 1);
                 if (!__syncthreads_and(w)) {
                     ok = false;
                     break;
                 }
             }
-            load_w(t + 1, sW[b ^ 1]);
+            load_w(g + 1, sW[b ^ 1]);
             rttc::cp_async_commit();
             rttc::cp_async_wait_all();
             rttc::fence_async_smem();
@@ -284,15 +297,27 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3_halo(ConvArgs a, int P) 
     if (warp == 0) rttc::tmem_dealloc(tmem, ncols);
 }
 
-// planes per CTA and shared memory of k_conv3_halo (P = 0: the layer does not fit)
-static int halo_planes(int cin, int cout, size_t* smem) {
-    for (int P = 8; P >= 1; P /= 2) {
-        const size_t need = (size_t)(P + 2) * HALO_V * cin * 2 + 2 * (size_t)cout * cin * 2 + 32;
-        if (need <= 200 * 1024 && P * cout <= 512) {
-            const size_t maxc = 512 / rttc::tmem_cols(P * cout);
-            const size_t floor_b = 233472 / (maxc + 1);
-            *smem = need > floor_b ? need : floor_b;
-            return P;
+// planes per CTA (P), taps per weight stage (G) and shared memory of k_conv3_halo: the largest
+// P, then the largest G, whose halo and weight stages fit in 200 KB; P = 0 if nothing fits
+static int halo_plan(int cin, int cout, int* G, size_t* smem) {
+    static const int gs[4] = {27, 9, 3, 1};
+    // first pass: plans that leave two CTAs per SM (one loads its halo while the other multiplies);
+    // second pass: anything within 200 KB
+    const size_t budgets[2] = {233472 / 2 - 1024, 200 * 1024};
+    for (int pass = 0; pass < 2; pass++) {
+        for (int P = 8; P >= 1; P /= 2) {
+            if (P * cout > 512 || (pass == 0 && 2 * rttc::tmem_cols(P * cout) > 512)) continue;
+            for (int gi = 0; gi < 4; gi++) {
+                const int nst = gs[gi] == 27 ? 1 : 2;
+                const size_t need =
+                    (size_t)(P + 2) * HALO_V * cin * 2 + (size_t)nst * gs[gi] * cout * cin * 2 + 32;
+                if (need > budgets[pass]) continue;
+                const size_t maxc = 512 / rttc::tmem_cols(P * cout);
+                const size_t floor_b = 233472 / (maxc + 1);
+                *smem = need > floor_b ? need : floor_b;
+                *G = gs[gi];
+                return P;
+            }
         }
     }
     return 0;
@@ -325,10 +350,12 @@ int conv3(rt_ctx* c, const ConvArgs& a) {
         return rt_fail(c, RT_EINVAL, "conv3: channel counts must be multiples of 16 in [16, 128] (got %d -> %d)",
                        a.cin, a.cout);
     size_t hsmem = 0;
-    const int P = g_conv_variant ? halo_planes(a.cin, a.cout, &hsmem) : 0;
+    int G = 1;
+    const int P = g_conv_variant ? halo_plan(a.cin, a.cout, &G, &hsmem) : 0;
     if (P > 0) {
         const dim3 grid((unsigned)((a.X + 7) / 8), (unsigned)((a.Y + 15) / 16), (unsigned)((a.Z + P - 1) / P));
-        return rt_launch(c, "unet_conv3_halo", [&] { k_conv3_halo<<<grid, CONV_THREADS, hsmem, c->stream>>>(a, P); });
+        return rt_launch(c, "unet_conv3_halo",
+                         [&] { k_conv3_halo<<<grid, CONV_THREADS, hsmem, c->stream>>>(a, P, G); });
     }
     const long V = (long)a.X * a.Y * a.Z;
     const unsigned blocks = (unsigned)((V + CONV_TM - 1) / CONV_TM);
