@@ -468,6 +468,104 @@ def run_batched(args):
     return 0
 
 
+def run_learned(args):
+    """Learned preconditioner: (density, residual, MG-error) samples harvested from 128^3 worst-case
+    boxes with random densities (k = 2, 6, 14 plain MG-PCG iterations each), the U-Net trained by
+    the library's kernels on random 33^3 crops of them, then used inside flexible MG-PCG on the
+    256x256x128 box (z = Vcycle(r) + N(rho, r), plain V-cycle as fallback) against the same PCG
+    without it.  Step = one solve of a top-face load to 1e-6 from zero, timed per form."""
+    import torch
+
+    import robtop_b200 as rb
+    from robtop_b200 import configs, learned
+
+    ws_, rank, lrank = dist_env()
+    ctx = make_ctx(rb, lrank)
+    stream = torch.cuda.ExternalStream(ctx_stream_handle(ctx))
+
+    def grid(cfg):
+        p = rb.default_params(mode=cfg["mode"], youngs_modulus=1e6, poisson_ratio=0.4, power_penalty=3.0,
+                              min_rho=1e-3, precision=rb.FP32, smoother=rb.SMOOTH_CHEBY, pre_sweeps=4, post_sweeps=4)
+        G = rb.HierarchyGrid(ctx, p)
+        G.genFromBox(cfg["eact"])
+        G[0].setRho(cfg["rho"].ravel())
+        G.set_support(cfg["vfix"])
+        G.update_stencil()
+        return G
+
+    n_train, iters, crop, n_crops = 8, (2, 6, 14), (33, 33, 33), 24
+    rng = np.random.default_rng(11)
+    t0 = time.perf_counter()
+    samples, hnet = [], None
+    for i in range(n_train):
+        G = grid(configs.worst_case_box(128, 128, 128, seed=100 + i))
+        if hnet is None:
+            hnet = learned.UNet.for_grid(G, seed=0)
+        for k in iters:
+            inp, tgt = learned.harvest(G, hnet, k, seed=1000 * i + k)
+            samples += learned.crops(inp, tgt, hnet.dims, crop, n_crops, rng)
+        G.close()
+    t_harvest = time.perf_counter() - t0
+    net = learned.UNet(ctx, *crop, seed=1)
+    net.output_scale = hnet.output_scale
+    hnet.close()
+    t0 = time.perf_counter()
+    losses = learned.train(net, samples, steps=1200, batch=8, lr=1e-3, seed=0)
+    t_train = time.perf_counter() - t0
+    del samples
+    torch.cuda.empty_cache()
+    cfg = configs.worst_case_box(256, 256, 128, seed=0)
+    G = grid(cfg)
+    G.autotune(reps=2)
+    enet = learned.UNet.for_grid(G)
+    learned.transfer(net, enet)
+    f = np.zeros(3 * G[0].nv)
+    for c in range(3):
+        f[c * G[0].nv + cfg["load_nodes"]] = np.random.default_rng(5).standard_normal(cfg["load_nodes"].size)
+    G[0].setForce(f)
+    zeros = torch.zeros(3 * G[0].nv, dtype=torch.float64, device="cuda")
+
+    def solve():
+        rb._capi.check(rb.lib().rt_put_dev(G.handle, rb._capi.FIELD_U, 0, C.c_void_p(zeros.data_ptr())), ctx.handle)
+        ctx.sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        info = G.pcg(WORKLOAD["tol"], 1000)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), info
+
+    res = {}
+    for name, net_ in (("plain", None), ("learned", enet)):
+        learned.attach(G, net_, fallback_ratio=1.0)
+        for _ in range(max(args.warmup, 1)):
+            solve()
+        ms = [solve() for _ in range(args.steps)]
+        res[name] = (sum(m for m, _ in ms) / len(ms), ms[-1][1])
+    learned.attach(G, None)
+    pl_ms, pl = res["plain"]
+    ln_ms, ln = res["learned"]
+    line = {"metric": "learned+mixed vs mixed MG-PCG, time to rel. residual 1e-6 on 256x256x128",
+            "value": 1e3 / ln_ms, "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": max(args.warmup, 1), "ms_per_step": ln_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64+f32+bf16", "data": "synthetic",
+            "config": {"workload": "worst-case box 256x256x128 (seed 0), random top-face load; U-Net trained on "
+                                   f"{n_train * len(iters) * n_crops} crops {crop} of {n_train * len(iters)} samples "
+                                   "harvested from 128^3 boxes (seeds 100-107)",
+                       "plain_ms_per_solve": pl_ms, "learned_over_plain_speed": pl_ms / ln_ms,
+                       "plain_iterations": pl.iterations, "learned_iterations": ln.iterations,
+                       "learned_rel_residual": ln.rel_residual, "loss_first": float(np.mean(losses[:10])),
+                       "loss_last": float(np.mean(losses[-50:])), "harvest_s": t_harvest, "train_s": t_train}}
+    if rank == 0:
+        print(json.dumps(line))
+    enet.close()
+    net.close()
+    G.close()
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -475,7 +573,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="worstcase", choices=["worstcase", "batched"],
+    ap.add_argument("--workload", default="worstcase", choices=["worstcase", "batched", "learned"],
                     help="batched: the 12-instance + 8-RHS batched-solve configuration instead of the headline one")
     ap.add_argument("--forms", default="both", choices=["both", "mixed"],
                     help="mixed: time only the mixed form (short command for launch-list captures)")
@@ -490,6 +588,8 @@ def main():
         return run_kernel(args)
     if args.workload == "batched":
         return run_batched(args)
+    if args.workload == "learned":
+        return run_learned(args)
 
     import torch
 

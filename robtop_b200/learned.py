@@ -125,3 +125,26 @@ def train(net, samples, steps, batch=4, lr=1e-3, seed=0):
                               device=ins.device)
         losses.append(net.train_step(ins[idx], tgts[idx], lr))
     return losses
+
+
+def crops(inp, tgt, dims, crop, n, rng):
+    """n random crops (each a box of ``crop`` node dims) of one full-box sample, as contiguous
+    [v, 16] / [v, 3] tensors; the residual scaling of the full box is kept."""
+    X, Y, Z = dims
+    cx, cy, cz = crop
+    a = inp.view(Z, Y, X, 16)
+    t = tgt.view(Z, Y, X, 3)
+    out = []
+    for _ in range(n):
+        x0 = int(rng.integers(0, X - cx + 1))
+        y0 = int(rng.integers(0, Y - cy + 1))
+        z0 = int(rng.integers(0, Z - cz + 1))
+        out.append((a[z0:z0 + cz, y0:y0 + cy, x0:x0 + cx].reshape(-1, 16).contiguous(),
+                    t[z0:z0 + cz, y0:y0 + cy, x0:x0 + cx].reshape(-1, 3).contiguous()))
+    return out
+
+
+def transfer(src, dst):
+    """Copy the weights and the output unit of one network to another (any box)."""
+    dst.set_params(src.get_params())
+    dst.output_scale = src.output_scale
