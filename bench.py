@@ -323,7 +323,8 @@ def run_kernel(args):
             rb._capi.check(rb.lib().rt_set_tuning(G.handle, prec, mode, variant, ty, zc), ctx.handle)
             names = ["residual", "applyK", "jacobi", "chebyshev"]
             shapes = {f"{names[mode]}_{'f32' if prec == rb.FP32 else 'f64'}":
-                      {"variant": ["smem_tile", "register_march"][variant], "rows": ty, "zchunk": zc}}
+                      {"variant": ["smem_tile", "register_march", "register_march_prefetch"][variant], "rows": ty,
+                       "zchunk": zc}}
         else:
             shapes = G.autotune()
         us = C.c_double()

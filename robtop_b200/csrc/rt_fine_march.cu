@@ -71,8 +71,11 @@ __global__ void k_fine_dinv(int nx, int ny, int nz, const uint8_t* __restrict__ 
 // MODE 0: r = f - K u (fixed rows: r = f)     MODE 1: out = K u (fixed rows: u)
 // MODE 2: unew = u + omega D^-1 (f - K u)     MODE 3: Chebyshev step kstep (coefficients a_k, b_k from the level's table, see rt_cheby_coef)
 // (fixed nodes in MODE 2/3: unew = f / n_e, d = 0)
-template <typename T, bool WS, int MODE, int TY>
-__global__ void __launch_bounds__(MARCH_BS, sizeof(T) == 4 ? 4 : 2) k_fine_march(int nx, int ny, int nz, int ntx, int nty, int nch,
+// PF: load each layer's output-stage inputs (flags, f, inverted diagonal block, Chebyshev
+// direction) at the top of the layer iteration, so that their latency overlaps the element
+// arithmetic (more registers: 3 blocks per SM for FP32 instead of 4)
+template <typename T, bool WS, int MODE, int TY, bool PF>
+__global__ void __launch_bounds__(MARCH_BS, sizeof(T) == 4 ? (PF ? 3 : 4) : 2) k_fine_march(int nx, int ny, int nz, int ntx, int nty, int nch,
                                                           int zchunk, const uint8_t* __restrict__ vact,
                                                           const float* __restrict__ wgt,
                                                           const uint8_t* __restrict__ vfix, const rte::KtVals<T> kt,
@@ -123,6 +126,25 @@ __global__ void __launch_bounds__(MARCH_BS, sizeof(T) == 4 ? 4 : 2) k_fine_march
 #pragma unroll
         for (int r = 0; r < TY + 2; r++) load_u(Y0 - 1 + r, ez + 1, ut[r]);
         const bool ez_ok = ez >= 0 && ez < nz;
+        bool pact[TY], pfix[TY];
+        T pf[TY][3], pd[TY][6], pdv[TY][3];
+        if (PF) {
+#pragma unroll
+            for (int ri = 0; ri < TY; ri++) {
+                const int ey = Y0 + ri;
+                const bool own = own_x && ez >= Z0 && ey < vy;
+                const long v = own ? cx + (long)vx * ey + plane * ez : 0;
+                pact[ri] = own && vact[v];
+                pfix[ri] = WS && pact[ri] && vfix[v];
+#pragma unroll
+                for (int c = 0; c < 3; c++) pf[ri][c] = (MODE != 1 && pact[ri]) ? f[c * nv + v] : T(0);
+#pragma unroll
+                for (int q = 0; q < 6; q++) pd[ri][q] = (MODE >= 2 && pact[ri]) ? dinv[q * nv + v] : T(0);
+#pragma unroll
+                for (int c = 0; c < 3; c++)
+                    pdv[ri][c] = (MODE == 3 && pact[ri] && kstep != 0) ? dvec[c * nv + v] : T(0);
+            }
+        }
         T ycb[3] = {T(0), T(0), T(0)}, yct[3] = {T(0), T(0), T(0)};
 #pragma unroll
         for (int r = 0; r <= TY; r++) {
@@ -166,12 +188,12 @@ __global__ void __launch_bounds__(MARCH_BS, sizeof(T) == 4 ? 4 : 2) k_fine_march
                 }
                 if (own_x && ez >= Z0 && ey < vy) {
                     const long v = cx + (long)vx * ey + plane * ez;
-                    const bool act = vact[v];
-                    const bool fixed = WS && act && vfix[v];
+                    const bool act = PF ? pact[ri] : (bool)vact[v];
+                    const bool fixed = PF ? pfix[ri] : (WS && act && vfix[v]);
+                    auto fv = [&](int c) { return PF ? pf[ri][c] : f[c * nv + v]; };
                     if (MODE == 0) {
 #pragma unroll
-                        for (int c = 0; c < 3; c++)
-                            out[c * nv + v] = act ? (fixed ? f[c * nv + v] : f[c * nv + v] - fin[c]) : T(0);
+                        for (int c = 0; c < 3; c++) out[c * nv + v] = act ? (fixed ? fv(c) : fv(c) - fin[c]) : T(0);
                     } else if (MODE == 1) {
 #pragma unroll
                         for (int c = 0; c < 3; c++) out[c * nv + v] = act ? (fixed ? u[c * nv + v] : fin[c]) : T(0);
@@ -179,11 +201,12 @@ __global__ void __launch_bounds__(MARCH_BS, sizeof(T) == 4 ? 4 : 2) k_fine_march
                         // u of this (non-fixed) node is ub[r]: node layer ez, node row Y0 - 1 + r == ey
                         T nu[3] = {T(0), T(0), T(0)}, dn[3] = {T(0), T(0), T(0)};
                         if (act) {
-                            const T d00 = dinv[v], d01 = dinv[nv + v], d02 = dinv[2 * nv + v];
-                            const T d11 = dinv[3 * nv + v], d12 = dinv[4 * nv + v], d22 = dinv[5 * nv + v];
+                            const T d00 = PF ? pd[ri][0] : dinv[v], d01 = PF ? pd[ri][1] : dinv[nv + v];
+                            const T d02 = PF ? pd[ri][2] : dinv[2 * nv + v], d11 = PF ? pd[ri][3] : dinv[3 * nv + v];
+                            const T d12 = PF ? pd[ri][4] : dinv[4 * nv + v], d22 = PF ? pd[ri][5] : dinv[5 * nv + v];
                             T rr[3];
 #pragma unroll
-                            for (int c = 0; c < 3; c++) rr[c] = fixed ? f[c * nv + v] : f[c * nv + v] - fin[c];
+                            for (int c = 0; c < 3; c++) rr[c] = fixed ? fv(c) : fv(c) - fin[c];
                             const T z0 = d00 * rr[0] + d01 * rr[1] + d02 * rr[2];
                             const T z1 = d01 * rr[0] + d11 * rr[1] + d12 * rr[2];
                             const T z2 = d02 * rr[0] + d12 * rr[1] + d22 * rr[2];
@@ -197,7 +220,8 @@ __global__ void __launch_bounds__(MARCH_BS, sizeof(T) == 4 ? 4 : 2) k_fine_march
                             } else {
 #pragma unroll
                                 for (int c = 0; c < 3; c++) {
-                                    dn[c] = (kstep == 0 ? T(0) : cheb_a * dvec[c * nv + v]) + cheb_b * zz[c];
+                                    dn[c] = (kstep == 0 ? T(0) : cheb_a * (PF ? pdv[ri][c] : dvec[c * nv + v])) +
+                                            cheb_b * zz[c];
                                     nu[c] = ub[r][c] + dn[c];
                                 }
                             }
@@ -223,7 +247,7 @@ __global__ void __launch_bounds__(MARCH_BS, sizeof(T) == 4 ? 4 : 2) k_fine_march
     }
 }
 
-template <typename T, bool WS, int MODE, int TY>
+template <typename T, bool WS, int MODE, int TY, bool PF>
 int launch_march_ty(rt_hier* h, int zc, const T* u, const T* f, T* out, double omega, const char* name, T* dvec,
                     const double* coef, int kstep, const T* dinv) {
     rt_level& L = h->L[0];
@@ -232,7 +256,7 @@ int launch_march_ty(rt_hier* h, int zc, const T* u, const T* f, T* out, double o
     const unsigned blocks = (unsigned)((nwarps + MARCH_WARPS - 1) / MARCH_WARPS);
     const rte::KtVals<T> kt = rte::make_kt<T>(h);
     return rt_launch(h->ctx, name, [&] {
-        k_fine_march<T, WS, MODE, TY><<<blocks, MARCH_BS, 0, h->ctx->stream>>>(
+        k_fine_march<T, WS, MODE, TY, PF><<<blocks, MARCH_BS, 0, h->ctx->stream>>>(
             L.nx, L.ny, L.nz, ntx, nty, nch, zc, L.vact, h->w, h->vfix, kt, u, f, out, (T)omega, dvec, coef, kstep,
             dinv);
     });
@@ -243,10 +267,16 @@ int launch_march(rt_hier* h, const T* u, const T* f, T* out, double omega, const
                  const double* coef, int kstep) {
     const rt_tile_cfg& tc = h->tune[sizeof(T) == 8 ? 1 : 0][MODE];
     const T* dinv = sizeof(T) == 8 ? (const T*)h->dinv64 : (const T*)h->dinv32;
+    if (tc.variant == 2) {
+        switch (tc.ty) {
+            case 2: return launch_march_ty<T, WS, MODE, 2, true>(h, tc.zchunk, u, f, out, omega, name, dvec, coef, kstep, dinv);
+            default: return launch_march_ty<T, WS, MODE, 4, true>(h, tc.zchunk, u, f, out, omega, name, dvec, coef, kstep, dinv);
+        }
+    }
     switch (tc.ty) {
-        case 2: return launch_march_ty<T, WS, MODE, 2>(h, tc.zchunk, u, f, out, omega, name, dvec, coef, kstep, dinv);
-        case 8: return launch_march_ty<T, WS, MODE, 8>(h, tc.zchunk, u, f, out, omega, name, dvec, coef, kstep, dinv);
-        default: return launch_march_ty<T, WS, MODE, 4>(h, tc.zchunk, u, f, out, omega, name, dvec, coef, kstep, dinv);
+        case 2: return launch_march_ty<T, WS, MODE, 2, false>(h, tc.zchunk, u, f, out, omega, name, dvec, coef, kstep, dinv);
+        case 8: return launch_march_ty<T, WS, MODE, 8, false>(h, tc.zchunk, u, f, out, omega, name, dvec, coef, kstep, dinv);
+        default: return launch_march_ty<T, WS, MODE, 4, false>(h, tc.zchunk, u, f, out, omega, name, dvec, coef, kstep, dinv);
     }
 }
 

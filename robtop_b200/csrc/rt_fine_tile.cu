@@ -346,7 +346,7 @@ int tile_zchunk_default(rt_ctx* c, int vx, int vy, int vz) {
 
 template <typename T>
 static bool use_march(rt_hier* h, int mode) {
-    return h->tune[sizeof(T) == 8 ? 1 : 0][mode].variant == 1;
+    return h->tune[sizeof(T) == 8 ? 1 : 0][mode].variant >= 1;  // 1: marching, 2: marching with prefetch
 }
 
 template <typename T>

@@ -70,7 +70,8 @@ struct rt_level {
 
 // launch shape of a finest-level operator kernel (chosen by rt_autotune)
 struct rt_tile_cfg {
-    int variant = 1;  // 0: shared-memory element tile (rt_fine_tile.cu), 1: register marching (rt_fine_march.cu)
+    int variant = 1;  // 0: shared-memory element tile (rt_fine_tile.cu), 1: register marching (rt_fine_march.cu),
+                      // 2: register marching with the output-stage loads issued ahead
     int ty = 4;       // node rows per warp tile (marching kernel: 2, 4 or 8)
     int zchunk = 16;  // node layers per tile
 };
