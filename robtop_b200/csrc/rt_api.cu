@@ -1026,24 +1026,46 @@ static double* cheby_table(rt_hier* h, int lvl) {
     return (h->parent ? h->parent->scal : h->scal) + RT_SCAL_CHEB + 2 * RT_CHEBY_MAXK * lvl;
 }
 
-// lmax(D^-1 A) of a level by 15 power steps (D^-1 A v = v - jacobi(v; f = 0, omega = 1)),
-// left on the device for the Chebyshev kernels
+// Rayleigh quotient of the A-inner-product power method: lmax = (A x)^T D^-1 (A x) / x^T A x from
+// rz = r.(D^-1 r) and xr = x.r with r = -A x (kept when x^T A x is not positive)
+__global__ void k_rayleigh(const double* __restrict__ rz, const double* __restrict__ xr, double* __restrict__ lmax) {
+    if (threadIdx.x == 0 && -xr[0] > 0.0) lmax[0] = rz[0] / -xr[0];
+}
+
+#define RT_LMAX_STEPS 30
+
+// lmax(D^-1 A) of a smoothed level by RT_LMAX_STEPS power steps; D^-1 A is self-adjoint in the
+// A inner product, so its Rayleigh quotient there is a lower bound converging at twice the rate of
+// the iterate (a 2-norm ratio |D^-1 A x| is not a bound when the diagonal blocks span decades).
+// r = f - A x with f = 0 gives -A x; one Jacobi step from u = 0 (omega = 1) gives D^-1 r;
+// supported rows drop out (r = f = 0 there).  The value and the level's Chebyshev table stay
+// on the device.
 static int estimate_lmax(rt_hier* h, int lvl) {
     rt_level& L = h->L[lvl];
     const long n = 3 * L.nv;
-    double *x = h->x, *z = h->z, *zero = h->q;
+    double *x = h->x, *r = h->rold, *z = h->q, *zero = h->p;
+    double* lmax = h->scal + RT_SCAL_LMAX + lvl;
     RT_CUDA(h->ctx, cudaMemsetAsync(zero, 0, sizeof(double) * n, h->ctx->stream));
+    RT_CUDA(h->ctx, cudaMemsetAsync(lmax, 0, sizeof(double), h->ctx->stream));
     RT_CHECK(rtk::rng_uniform(h, 0x51ab + lvl, n, x));
-    for (int it = 0; it < 15; it++) {
+    for (int it = 0; it < RT_LMAX_STEPS; it++) {
         RT_CHECK(rtk::dot(h, n, x, x, h->scal + 290));
         RT_CHECK(rtk::scale(h, n, x, h->scal + 290, true));
-        if (lvl == 0) RT_CHECK(rtk::fine_jacobi<double>(h, x, zero, z, 1.0));
-        else RT_CHECK(rtk::st_jacobi<double>(h, lvl, x, zero, z, 1.0));
-        RT_CHECK(rtk::axpy(h, n, -1.0, z, x));
+        if (lvl == 0) {
+            RT_CHECK(rtk::fine_residual<double>(h, x, zero, r));
+            RT_CHECK(rtk::fine_jacobi<double>(h, zero, r, z, 1.0));
+        } else {
+            RT_CHECK(rtk::st_residual<double>(h, lvl, x, zero, r));
+            RT_CHECK(rtk::st_jacobi<double>(h, lvl, zero, r, z, 1.0));
+        }
+        RT_CHECK(rtk::dot(h, n, r, z, h->scal + 292));
+        RT_CHECK(rtk::dot(h, n, x, r, h->scal + 293));
+        RT_CHECK(rt_launch(h->ctx, "lmax_rayleigh",
+                           [&] { k_rayleigh<<<1, 32, 0, h->ctx->stream>>>(h->scal + 292, h->scal + 293, lmax); }));
+        RT_CUDA(h->ctx, cudaMemcpyAsync(x, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->ctx->stream));
     }
-    RT_CHECK(rtk::dot(h, n, x, x, h->scal + 291));
     return rt_launch(h->ctx, "lmax_finish", [&] {
-        k_lmax_finish<<<1, 32, 0, h->ctx->stream>>>(h->scal + 291, h->scal + RT_SCAL_LMAX + lvl, cheby_table(h, lvl));
+        k_lmax_finish<<<1, 32, 0, h->ctx->stream>>>(nullptr, lmax, cheby_table(h, lvl));
     });
 }
 
