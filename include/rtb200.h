@@ -81,6 +81,8 @@ typedef struct rt_params {
     int pre_sweeps, post_sweeps;
     double jacobi_omega;
     int precision;          /* rt_precision of the V-cycle inside rt_pcg / rt_worst_case */
+    int coarsest_elements;  /* halve while more elements than this are solid (the reference: 400,
+                               grid/Grid.cpp:488); the coarsest level is solved densely (<= 12288 DOF) */
 } rt_params;
 
 typedef struct rt_solve_info {

@@ -21,7 +21,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "liboracle.so")
 
 SMOOTH_GS, SMOOTH_SGS, SMOOTH_JACOBI, SMOOTH_CHEBY = 0, 1, 2, 3
-LMAX_STEPS = 30  # power steps of the Chebyshev bound estimate (the library uses the same count)
+LMAX_STEPS = 30  # Lanczos steps of the Chebyshev bound estimate (the library uses the same count)
 
 
 def build() -> str:
@@ -301,7 +301,7 @@ class Hierarchy:
         rc = lib().or_coarsest_setup(self.lv(self.nlev - 1), 1 if self.no_support else 0)
         if not getattr(self, "_lmax_fixed", False):
             for i in range(self.nlev - 1):
-                work = np.zeros(4 * self.arrs[i]["u"].size)
+                work = np.zeros(6 * self.arrs[i]["u"].size)
                 self.LA[i].lmax = lib().or_lambda_max(self.lv(i), 1 if i == 0 else 0, ptr(self.KE), 0x51AB + i,
                                                       LMAX_STEPS, ptr(work))
         if rc != 0:

@@ -612,28 +612,40 @@ void or_st_cheby(const or_level* L, const double* u, const double* f, double* un
 
 /* largest eigenvalue of D^-1 A by power steps (D^-1 A v = v - jacobi(v; f = 0, omega = 1)) */
 double or_lambda_max(or_level* L, int is_fine, const double* KE, uint64_t seed, int iters, double* work) {
-    /* power method on D^-1 A with the Rayleigh quotient in the A inner product, in which D^-1 A
-     * is self-adjoint: lambda ~ (A x)^T D^-1 (A x) / x^T A x, a lower bound that converges at twice
-     * the rate of the iterate.  r = f - A x with f = 0 gives -A x, one Jacobi step from u = 0
-     * with omega = 1 gives D^-1 r; supported rows drop out (r = f = 0 there).  work: 4 n doubles */
+    /* lambda_max(D^-1 A) by `iters` Lanczos steps in the A inner product, in which M = D^-1 A is
+     * self-adjoint (no re-orthogonalisation: only the extreme Ritz value is used).  r = f - A v with
+     * f = 0 gives -A v; one Jacobi step from u = 0 (omega = 1) gives D^-1 r = -M v.  Step j, with
+     * v_j and r_j = -A v_j:  w = -D^-1 r_j;  alpha_j = r_j . D^-1 r_j;  w -= alpha_j v_j + beta_{j-1} v_{j-1};
+     * beta_j = |w|_A;  v_{j+1} = w / beta_j.  Supported rows drop out (r = f = 0 there).
+     * work: 6 n doubles */
     long nv = (long)(L->nx + 1) * (L->ny + 1) * (L->nz + 1), n = 3 * nv;
-    double *x = work, *r = work + n, *z = work + 2 * n, *zero = work + 3 * n;
+    double *vp = work, *v = work + n, *r = work + 2 * n, *w = work + 3 * n, *r2 = work + 4 * n, *zero = work + 5 * n;
+    double alpha[64], beta[64];
+    if (iters > 64) iters = 64;
     memset(zero, 0, sizeof(double) * n);
-    or_rng_uniform(seed, n, x);
-    double lam = 0;
+    memset(vp, 0, sizeof(double) * n);
+    or_rng_uniform(seed, n, v);
+    if (is_fine) or_fine_residual(L, KE, v, zero, r);
+    else or_st_residual(L, v, zero, r);
+    double an = sqrt(fmax(-or_dot(n, v, r), 1e-300));
+    for (long i = 0; i < n; i++) { v[i] /= an; r[i] /= an; }
+    int k = 0;
     for (int it = 0; it < iters; it++) {
-        double nn = sqrt(or_dot(n, x, x));
-        for (long i = 0; i < n; i++) x[i] /= nn;
-        if (is_fine) or_fine_residual(L, KE, x, zero, r);
-        else or_st_residual(L, x, zero, r);
-        memset(z, 0, sizeof(double) * n);
-        if (is_fine) or_fine_jacobi(L, KE, z, r, 1.0, L->r);
-        else or_st_jacobi(L, z, r, 1.0, L->r);
-        double num = or_dot(n, r, z), den = -or_dot(n, x, r);
-        if (den > 0) lam = num / den;
-        memcpy(x, z, sizeof(double) * n);
+        memset(w, 0, sizeof(double) * n);
+        if (is_fine) or_fine_jacobi(L, KE, w, r, 1.0, L->r);
+        else or_st_jacobi(L, w, r, 1.0, L->r);
+        const double a = or_dot(n, r, w);
+        const double bp = it > 0 ? beta[it - 1] : 0.0;
+        for (long i = 0; i < n; i++) w[i] = -w[i] - a * v[i] - bp * vp[i];
+        if (is_fine) or_fine_residual(L, KE, w, zero, r2);
+        else or_st_residual(L, w, zero, r2);
+        const double b = sqrt(fmax(-or_dot(n, w, r2), 1e-300));
+        alpha[it] = a;
+        beta[it] = b;
+        k = it + 1;
+        for (long i = 0; i < n; i++) { vp[i] = v[i]; v[i] = w[i] / b; r[i] = r2[i] / b; }
     }
-    return lam;
+    return or_tridiag_max_eig(k, alpha, beta);
 }
 
 /* ------------------------------------------------------------------------ */

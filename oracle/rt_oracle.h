@@ -54,7 +54,7 @@ void or_cheby_coef(double lmax, int k, double* a, double* b);
 void or_fine_cheby(const or_level* L, const double* KE, const double* u, const double* f, double* unew, double* d,
                    int k);
 void or_st_cheby(const or_level* L, const double* u, const double* f, double* unew, double* d, int k);
-double or_lambda_max(or_level* L, int is_fine, const double* KE, uint64_t seed, int iters, double* work /*[4][3nv]*/);
+double or_lambda_max(or_level* L, int is_fine, const double* KE, uint64_t seed, int iters, double* work /*[6][3nv]*/);
 
 /* element template (element/templateMatrix.cpp:15-124) */
 void or_template_matrix(double E, double nu, double h, double* KE /* [576] row-major */);

@@ -210,6 +210,7 @@ extern "C" void rt_params_default(rt_params* p) {
     p->post_sweeps = 1;
     p->jacobi_omega = 0.6;
     p->precision = RT_FP64;
+    p->coarsest_elements = 400;
 }
 
 // ---------------------------------------------------------------------------
@@ -402,7 +403,8 @@ static int build_hier(rt_ctx* c, const rt_params* p, int nx, int ny, int nz, uin
         RT_CUDA(c, cudaMemcpyAsync(&hc, dcnt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         RT_CUDA(c, cudaStreamSynchronize(c->stream));
         last.cnt = (long)hc;
-        if (last.cnt <= 400 || (last.nx <= 1 && last.ny <= 1 && last.nz <= 1)) break;
+        const long stop = p->coarsest_elements > 0 ? p->coarsest_elements : 400;
+        if (last.cnt <= stop || (last.nx <= 1 && last.ny <= 1 && last.nz <= 1)) break;
         Chain nxt{(last.nx + 1) / 2, (last.ny + 1) / 2, (last.nz + 1) / 2, nullptr, 0};
         RT_CHECK(dalloc(c, &nxt.e, (size_t)nxt.nx * nxt.ny * nxt.nz));
         RT_CHECK(rtk::coarsen_elements(c, last.nx, last.ny, last.nz, 2, last.e, nxt.e));
@@ -419,7 +421,7 @@ static int build_hier(rt_ctx* c, const rt_params* p, int nx, int ny, int nz, uin
     }
     if (chain.size() == 1) {
         cudaFree(chain[0].e);
-        return rt_fail(c, RT_EINVAL, "grid too small for multigrid (<= 400 solid elements)");
+        return rt_fail(c, RT_EINVAL, "grid too small for multigrid (no level above the coarsest-size limit)");
     }
     if (idx.size() > RT_MAX_LEVELS) {
         for (Chain& ch : chain) cudaFree(ch.e);
@@ -467,7 +469,7 @@ static int build_hier(rt_ctx* c, const rt_params* p, int nx, int ny, int nz, uin
                 if (va[v]) aidx.push_back((int)v);
             L.na = (int)aidx.size();
             const size_t n = 3 * (size_t)L.na;
-            if (n > 6000) return rt_fail(c, RT_EINVAL, "coarsest level too large for the dense solve (%zu DOF)", n);
+            if (n > 12288) return rt_fail(c, RT_EINVAL, "coarsest level too large for the dense solve (%zu DOF)", n);
             RT_CHECK(dalloc(c, &L.aidx, L.na));
             RT_CUDA(c, cudaMemcpyAsync(L.aidx, aidx.data(), sizeof(int) * L.na, cudaMemcpyHostToDevice, c->stream));
             RT_CHECK(dalloc(c, &L.ainv, n * n));
@@ -1026,46 +1028,75 @@ static double* cheby_table(rt_hier* h, int lvl) {
     return (h->parent ? h->parent->scal : h->scal) + RT_SCAL_CHEB + 2 * RT_CHEBY_MAXK * lvl;
 }
 
-// Rayleigh quotient of the A-inner-product power method: lmax = (A x)^T D^-1 (A x) / x^T A x from
-// rz = r.(D^-1 r) and xr = x.r with r = -A x (kept when x^T A x is not positive)
-__global__ void k_rayleigh(const double* __restrict__ rz, const double* __restrict__ xr, double* __restrict__ lmax) {
-    if (threadIdx.x == 0 && -xr[0] > 0.0) lmax[0] = rz[0] / -xr[0];
+// v /= s and r /= s with s = sqrt(max(-v.r, tiny)) in slot out (the A-norm of v when r = -A v)
+__global__ void k_anorm_scale(long n, const double* __restrict__ vr, double* __restrict__ out, double* __restrict__ v,
+                              double* __restrict__ r) {
+    const double s = sqrt(fmax(-vr[0], 1e-300));
+    if (blockIdx.x == 0 && threadIdx.x == 0 && out) out[0] = s;
+    const double is = 1.0 / s;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        v[i] *= is;
+        r[i] *= is;
+    }
+}
+
+// Lanczos step update: w = -w - alpha v - beta_prev vp
+__global__ void k_lanczos_w(long n, double* __restrict__ w, const double* __restrict__ v,
+                            const double* __restrict__ vp, const double* __restrict__ alpha,
+                            const double* __restrict__ beta_prev) {
+    const double a = alpha[0], b = beta_prev ? beta_prev[0] : 0.0;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        w[i] = -w[i] - a * v[i] - b * vp[i];
 }
 
 #define RT_LMAX_STEPS 30
 
-// lmax(D^-1 A) of a smoothed level by RT_LMAX_STEPS power steps; D^-1 A is self-adjoint in the
-// A inner product, so its Rayleigh quotient there is a lower bound converging at twice the rate of
-// the iterate (a 2-norm ratio |D^-1 A x| is not a bound when the diagonal blocks span decades).
-// r = f - A x with f = 0 gives -A x; one Jacobi step from u = 0 (omega = 1) gives D^-1 r;
-// supported rows drop out (r = f = 0 there).  The value and the level's Chebyshev table stay
-// on the device.
+// lmax(D^-1 A) of a smoothed level by RT_LMAX_STEPS Lanczos steps in the A inner product, in which
+// M = D^-1 A is self-adjoint (no re-orthogonalisation: only the extreme Ritz value is used).
+// r = f - A v with f = 0 gives -A v; one Jacobi step from u = 0 (omega = 1) gives D^-1 r = -M v.
+// Step j, with v_j and r_j = -A v_j: w = -D^-1 r_j, alpha_j = r_j . D^-1 r_j,
+// w -= alpha_j v_j + beta_{j-1} v_{j-1}, beta_j = |w|_A, v_{j+1} = w / beta_j.  Supported rows
+// drop out (r = f = 0 there).  The largest eigenvalue of the tridiagonal matrix and the level's
+// Chebyshev table stay on the device.
 static int estimate_lmax(rt_hier* h, int lvl) {
     rt_level& L = h->L[lvl];
+    rt_ctx* c = h->ctx;
     const long n = 3 * L.nv;
-    double *x = h->x, *r = h->rold, *z = h->q, *zero = h->p;
-    double* lmax = h->scal + RT_SCAL_LMAX + lvl;
-    RT_CUDA(h->ctx, cudaMemsetAsync(zero, 0, sizeof(double) * n, h->ctx->stream));
-    RT_CUDA(h->ctx, cudaMemsetAsync(lmax, 0, sizeof(double), h->ctx->stream));
-    RT_CHECK(rtk::rng_uniform(h, 0x51ab + lvl, n, x));
+    double *vp = h->x, *v = h->rold, *r = h->q, *w = h->z, *r2 = h->rr, *zero = h->p;
+    double* alpha = h->scal + 100;  // [RT_LMAX_STEPS] (the Lanczos eigen-solve's slots; not in use here)
+    double* beta = h->scal + 164;
+    const unsigned g = (unsigned)std::min<long>((n + 255) / 256, (long)c->sm_count * 16);
+    auto residual = [&](const double* x, double* out) {
+        return lvl == 0 ? rtk::fine_residual<double>(h, x, zero, out) : rtk::st_residual<double>(h, lvl, x, zero, out);
+    };
+    auto jacobi = [&](const double* f, double* out) {
+        return lvl == 0 ? rtk::fine_jacobi<double>(h, zero, f, out, 1.0) : rtk::st_jacobi<double>(h, lvl, zero, f, out, 1.0);
+    };
+    RT_CUDA(c, cudaMemsetAsync(zero, 0, sizeof(double) * n, c->stream));
+    RT_CUDA(c, cudaMemsetAsync(vp, 0, sizeof(double) * n, c->stream));
+    RT_CHECK(rtk::rng_uniform(h, 0x51ab + lvl, n, v));
+    RT_CHECK(residual(v, r));
+    RT_CHECK(rtk::dot(h, n, v, r, h->scal + 292));
+    RT_CHECK(rt_launch(c, "lmax_anorm", [&] { k_anorm_scale<<<g, 256, 0, c->stream>>>(n, h->scal + 292, nullptr, v, r); }));
     for (int it = 0; it < RT_LMAX_STEPS; it++) {
-        RT_CHECK(rtk::dot(h, n, x, x, h->scal + 290));
-        RT_CHECK(rtk::scale(h, n, x, h->scal + 290, true));
-        if (lvl == 0) {
-            RT_CHECK(rtk::fine_residual<double>(h, x, zero, r));
-            RT_CHECK(rtk::fine_jacobi<double>(h, zero, r, z, 1.0));
-        } else {
-            RT_CHECK(rtk::st_residual<double>(h, lvl, x, zero, r));
-            RT_CHECK(rtk::st_jacobi<double>(h, lvl, zero, r, z, 1.0));
-        }
-        RT_CHECK(rtk::dot(h, n, r, z, h->scal + 292));
-        RT_CHECK(rtk::dot(h, n, x, r, h->scal + 293));
-        RT_CHECK(rt_launch(h->ctx, "lmax_rayleigh",
-                           [&] { k_rayleigh<<<1, 32, 0, h->ctx->stream>>>(h->scal + 292, h->scal + 293, lmax); }));
-        RT_CUDA(h->ctx, cudaMemcpyAsync(x, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->ctx->stream));
+        RT_CHECK(jacobi(r, w));
+        RT_CHECK(rtk::dot(h, n, r, w, alpha + it));
+        RT_CHECK(rt_launch(c, "lmax_lanczos_w", [&] {
+            k_lanczos_w<<<g, 256, 0, c->stream>>>(n, w, v, vp, alpha + it, it > 0 ? beta + it - 1 : nullptr);
+        }));
+        RT_CHECK(residual(w, r2));
+        RT_CHECK(rtk::dot(h, n, w, r2, h->scal + 292));
+        RT_CHECK(rt_launch(c, "lmax_anorm",
+                           [&] { k_anorm_scale<<<g, 256, 0, c->stream>>>(n, h->scal + 292, beta + it, w, r2); }));
+        // rotate: v_{j-1} <- v_j, v_j <- w, r_j <- r2
+        std::swap(vp, v);
+        std::swap(v, w);
+        std::swap(r, r2);
     }
-    return rt_launch(h->ctx, "lmax_finish", [&] {
-        k_lmax_finish<<<1, 32, 0, h->ctx->stream>>>(nullptr, lmax, cheby_table(h, lvl));
+    double* lmax = h->scal + RT_SCAL_LMAX + lvl;
+    RT_CHECK(rtk::tridiag_max_eig(h, RT_LMAX_STEPS, alpha, beta, lmax));
+    return rt_launch(c, "lmax_finish", [&] {
+        k_lmax_finish<<<1, 32, 0, c->stream>>>(nullptr, lmax, cheby_table(h, lvl));
     });
 }
 

@@ -273,10 +273,10 @@ def test_vcycle_and_pcg_converge():
 
 
 def test_chebyshev_bound_estimate_matches_dense_spectrum():
-    """The smoother bound lambda_max(D^-1 A) of the finest and first coarse level, estimated by
-    the power method with the A-inner-product Rayleigh quotient, is a lower bound within 2 % of
-    the dense spectrum's maximum, on a high-contrast density (the 2-norm ratio |D^-1 A x| that
-    a plain power method reports is not a bound there)."""
+    """The smoother bound lambda_max(D^-1 A) of the smoothed levels, estimated by 30 Lanczos steps
+    in the A inner product, is a lower bound within 0.5 % of the dense spectrum's maximum on a
+    high-contrast density (the 2-norm ratio |D^-1 A x| of a plain power method is not a bound
+    there, and its convergence at the dense top of the spectrum is slow)."""
     cfg = configs.worst_case_box(10, 8, 6, seed=4)
     H = O.Hierarchy(cfg["eact"], cfg["rho"], cfg["vfix"], p=3, E=1e6, nu=0.4)
     H.update_stencil()
@@ -305,7 +305,7 @@ def test_chebyshev_bound_estimate_matches_dense_spectrum():
         lam = np.max(np.linalg.eigvals(M).real)
         est = H.LA[lvl].lmax
         assert est <= lam * (1 + 1e-9), (lvl, est, lam)
-        assert est >= 0.98 * lam, (lvl, est, lam)
+        assert est >= 0.995 * lam, (lvl, est, lam)
 
 
 def test_surface_rule_numpy_and_c_agree():
