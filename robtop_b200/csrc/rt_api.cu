@@ -292,7 +292,7 @@ static void free_hier(rt_hier* h);
 static void free_workspace(rt_hier* w) {
     for (auto& L : w->L) {
         cudaFree(L.u); cudaFree(L.f); cudaFree(L.r); cudaFree(L.u32); cudaFree(L.f32); cudaFree(L.r32);
-        cudaFree(L.d); cudaFree(L.d32); cudaFree(L.dvec); cudaFree(L.dvec32);
+        cudaFree(L.d); cudaFree(L.d32); cudaFree(L.dvec);
     }
     cudaFree(w->x); cudaFree(w->rr); cudaFree(w->z); cudaFree(w->p); cudaFree(w->q); cudaFree(w->rold);
     cudaFree(w->partials); cudaFree(w->scal);
@@ -319,7 +319,7 @@ static void free_hier(rt_hier* h) {
         cudaFree(L.vact); cudaFree(L.eact); cudaFree(L.u); cudaFree(L.f); cudaFree(L.r);
         cudaFree(L.u32); cudaFree(L.f32); cudaFree(L.r32); cudaFree(L.st); cudaFree(L.st32);
         cudaFree(L.d); cudaFree(L.d32);
-        cudaFree(L.aidx); cudaFree(L.ainv); cudaFree(L.ainv32); cudaFree(L.dvec); cudaFree(L.dvec32);
+        cudaFree(L.aidx); cudaFree(L.ainv); cudaFree(L.dvec);
     }
     cudaFree(h->KE_dev); cudaFree(h->KE32_dev); cudaFree(h->rho); cudaFree(h->w); cudaFree(h->vfix);
     cudaFree(h->sens); cudaFree(h->ftmp); cudaFree(h->eshell); cudaFree(h->load_nodes); cudaFree(h->load_normal);
@@ -345,7 +345,7 @@ static void ws_sync(rt_hier* w) {
         rt_level& a = w->L[i];
         const rt_level& b = p->L[i];
         a.vact = b.vact; a.eact = b.eact; a.st = b.st; a.st32 = b.st32;
-        a.na = b.na; a.aidx = b.aidx; a.ainv = b.ainv; a.ainv32 = b.ainv32;
+        a.na = b.na; a.aidx = b.aidx; a.ainv = b.ainv;
         a.n_act_nodes = b.n_act_nodes; a.n_act_elems = b.n_act_elems;
     }
     memcpy(w->KE, p->KE, sizeof(w->KE));
@@ -473,9 +473,7 @@ static int build_hier(rt_ctx* c, const rt_params* p, int nx, int ny, int nz, uin
             RT_CHECK(dalloc(c, &L.aidx, L.na));
             RT_CUDA(c, cudaMemcpyAsync(L.aidx, aidx.data(), sizeof(int) * L.na, cudaMemcpyHostToDevice, c->stream));
             RT_CHECK(dalloc(c, &L.ainv, n * n));
-            RT_CHECK(dalloc(c, &L.ainv32, n * n));
             RT_CHECK(dalloc(c, &L.dvec, n));
-            RT_CHECK(dalloc(c, &L.dvec32, n));
             RT_CUDA(c, cudaStreamSynchronize(c->stream));
         }
     }
@@ -1977,7 +1975,6 @@ static int make_workspace(rt_hier* p, rt_hier** out) {
         RT_CUDA(c, cudaMemsetAsync(a.r, 0, sizeof(double) * n, c->stream));
         if (i + 1 == p->L.size()) {
             RT_CHECK(dalloc(c, &a.dvec, 3 * (size_t)b.na));
-            RT_CHECK(dalloc(c, &a.dvec32, 3 * (size_t)b.na));
         }
     }
     const size_t n3 = 3 * (size_t)p->L[0].nv;

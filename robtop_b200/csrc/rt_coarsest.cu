@@ -123,19 +123,19 @@ __global__ void k_add_rrt_dev(int n, int nr, const double* __restrict__ R, const
     }
 }
 
-template <typename T>
-__global__ void k_gather_active(int na, long nv, const int* __restrict__ aidx, const T* __restrict__ f,
-                                T* __restrict__ d) {
+template <typename TI, typename TO>
+__global__ void k_gather_active(int na, long nv, const int* __restrict__ aidx, const TI* __restrict__ f,
+                                TO* __restrict__ d) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x) {
         const int v = aidx[i];
-        d[3 * i] = f[v]; d[3 * i + 1] = f[nv + v]; d[3 * i + 2] = f[2 * nv + v];
+        d[3 * i] = (TO)f[v]; d[3 * i + 1] = (TO)f[nv + v]; d[3 * i + 2] = (TO)f[2 * nv + v];
     }
 }
 
 // u = Ainv d, one warp per row, scattered back to the node box (u zeroed first by the caller)
-template <typename T>
+template <typename T, typename TU>
 __global__ void k_gemv_scatter(int na, long nv, const int* __restrict__ aidx, const T* __restrict__ Ainv,
-                               const T* __restrict__ d, T* __restrict__ u) {
+                               const T* __restrict__ d, TU* __restrict__ u) {
     const int n = 3 * na;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -145,7 +145,7 @@ __global__ void k_gemv_scatter(int na, long nv, const int* __restrict__ aidx, co
         for (int j = lane; j < n; j += 32) s += row[j] * d[j];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-        if (lane == 0) u[(long)(i % 3) * nv + aidx[i / 3]] = s;
+        if (lane == 0) u[(long)(i % 3) * nv + aidx[i / 3]] = (TU)s;
     }
 }
 
@@ -235,24 +235,24 @@ int coarsest_setup(rt_hier* h) {
     RT_CUDA(c, cudaFreeAsync(status, c->stream));
     RT_CUDA(c, cudaStreamSynchronize(c->stream));
     if (st_h != 0) return rt_fail(c, RT_ENAN, "coarsest matrix not positive definite (pivot %d)", st_h - 1);
-    RT_CHECK(d2f(h, (long)n * n, L.ainv, L.ainv32));
     return RT_OK;
 }
 
+// u = A^-1 f on the coarsest level.  The inverse and the product are FP64 in both precisions
+// of the V-cycle: the coarse operator's conditioning (the stiffness contrast survives the
+// averaging) would amplify the rounding of an FP32 copy of the inverse.
 template <typename T>
 int coarsest_solve(rt_hier* h, const T* f, T* u) {
     rt_ctx* c = h->ctx;
     rt_level& L = h->L.back();
-    T* d = sizeof(T) == 8 ? (T*)L.dvec : (T*)L.dvec32;
-    const T* Ainv = sizeof(T) == 8 ? (const T*)L.ainv : (const T*)L.ainv32;
     RT_CHECK(rt_launch(c, sizeof(T) == 8 ? "coarsest_gather_f64" : "coarsest_gather_f32", [&] {
-        k_gather_active<T><<<(L.na + 255) / 256, 256, 0, c->stream>>>(L.na, L.nv, L.aidx, f, d);
+        k_gather_active<T, double><<<(L.na + 255) / 256, 256, 0, c->stream>>>(L.na, L.nv, L.aidx, f, L.dvec);
     }));
     RT_CUDA(c, cudaMemsetAsync(u, 0, sizeof(T) * 3 * L.nv, c->stream));
     const int n = 3 * L.na;
     return rt_launch(c, sizeof(T) == 8 ? "coarsest_gemv_f64" : "coarsest_gemv_f32", [&] {
         unsigned g = (unsigned)std::min<long>(((long)n * 32 + 255) / 256, (long)c->sm_count * 8);
-        k_gemv_scatter<T><<<g, 256, 0, c->stream>>>(L.na, L.nv, L.aidx, Ainv, d, u);
+        k_gemv_scatter<double, T><<<g, 256, 0, c->stream>>>(L.na, L.nv, L.aidx, L.ainv, L.dvec, u);
     });
 }
 

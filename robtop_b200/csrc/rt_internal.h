@@ -63,9 +63,7 @@ struct rt_level {
     int na = 0;
     int* aidx = nullptr;
     double* ainv = nullptr;  // [3na][3na]
-    float* ainv32 = nullptr;
     double* dvec = nullptr;  // [3na] gather buffer
-    float* dvec32 = nullptr;
 };
 
 // launch shape of a finest-level operator kernel (chosen by rt_autotune)
