@@ -56,7 +56,8 @@ enum rt_mode {
  * D^-1 A of degree pre/post_sweeps on [lmax/30, 1.1 lmax], lmax estimated per
  * level by rt_update_stencil (one fused element-tile / stencil kernel per step). */
 enum rt_smoother { RT_SMOOTH_GS = 0, RT_SMOOTH_SGS = 1, RT_SMOOTH_JACOBI = 2, RT_SMOOTH_CHEBY = 3 };
-enum rt_precision { RT_FP64 = 0, RT_FP32 = 1 };
+/* RT_FP64_FINE: the finest level's smoothing and residual in FP64, every coarser level in FP32 */
+enum rt_precision { RT_FP64 = 0, RT_FP32 = 1, RT_FP64_FINE = 2 };
 enum rt_layout { RT_LAYOUT_DENSE = 0, RT_LAYOUT_REF_GS = 1 };
 enum rt_field { RT_FIELD_U = 0, RT_FIELD_F = 1, RT_FIELD_R = 2, RT_FIELD_RHO = 3, RT_FIELD_SENS = 4,
                 RT_FIELD_STENCIL = 5, RT_FIELD_VACT = 6, RT_FIELD_EACT = 7, RT_FIELD_VFIX = 8,

@@ -9,7 +9,7 @@ reference's interfaces:
 * :mod:`robtop_b200.configs` — seeded synthetic domains of the benchmark configurations
 """
 from . import _capi  # noqa: F401
-from ._capi import (FP32, FP64, LAYOUT_DENSE, LAYOUT_REF_GS, MODE_NSCF, MODE_NSFF, MODE_WSCF, MODE_WSFF,  # noqa: F401
+from ._capi import (FP32, FP64, FP64_FINE, LAYOUT_DENSE, LAYOUT_REF_GS, MODE_NSCF, MODE_NSFF, MODE_WSCF, MODE_WSFF,  # noqa: F401
                     SMOOTH_CHEBY, SMOOTH_GS, SMOOTH_JACOBI, SMOOTH_SGS, WORST_BLOCK_LANCZOS, WORST_LANCZOS, WORST_MODPM,
                     RTError, lib)
 from .grid import Context, Grid, HierarchyGrid, default_params, pcg_batch  # noqa: F401

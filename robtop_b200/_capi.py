@@ -16,7 +16,7 @@ STATUS_NAMES = {0: "RT_OK", 1: "RT_EINVAL", 2: "RT_ECUDA", 3: "RT_ENOCONV", 4: "
                 6: "RT_ENOMEM", 7: "RT_ESTATE"}
 MODE_NSCF, MODE_NSFF, MODE_WSCF, MODE_WSFF = range(4)
 SMOOTH_GS, SMOOTH_SGS, SMOOTH_JACOBI, SMOOTH_CHEBY = range(4)
-FP64, FP32 = 0, 1
+FP64, FP32, FP64_FINE = 0, 1, 2
 LAYOUT_DENSE, LAYOUT_REF_GS = 0, 1
 FIELD_U, FIELD_F, FIELD_R, FIELD_RHO, FIELD_SENS, FIELD_STENCIL, FIELD_VACT, FIELD_EACT, FIELD_VFIX, \
     FIELD_PENALTY = range(10)

@@ -578,6 +578,10 @@ extern "C" int rt_hier_set_params(rt_hier* h, const rt_params* p) {
                     p->element_length != h->P.element_length;
     if (p->skip_layer1 != h->P.skip_layer1)
         return rt_fail(h->ctx, RT_EINVAL, "skip_layer1 is fixed when the hierarchy is built");
+    auto coarsest = [](int v) { return v > 0 ? v : 400; };
+    if (coarsest(p->coarsest_elements) != coarsest(h->P.coarsest_elements))
+        return rt_fail(h->ctx, RT_EINVAL, "coarsest_elements is fixed when the hierarchy is built");
+    if (p->precision < RT_FP64 || p->precision > RT_FP64_FINE) return rt_fail(h->ctx, RT_EINVAL, "unknown precision");
     h->P = *p;
     if (ke) RT_CHECK(upload_KE(h));
     h->stencil_ready = false;
@@ -1138,23 +1142,24 @@ static int level_smooth(rt_hier* h, int lvl, int smoother, int sweeps, double om
 }
 
 // HierarchyGrid::v_cycle (grid/Grid.cpp:1068-1113) over the real levels
+// levels l0 .. coarsest (level l0's u is the caller's initial guess)
 template <typename T>
-static int vcycle_T(rt_hier* h, int smoother, int pre, int post, double omega) {
+static int vcycle_T(rt_hier* h, int smoother, int pre, int post, double omega, int l0 = 0) {
     const int nl = (int)h->L.size();
-    for (int i = 0; i < nl; i++) {
-        if (i > 0) {
+    for (int i = l0; i < nl; i++) {
+        if (i > l0) {
             RT_CHECK(level_residual<T>(h, i - 1));
             RT_CHECK(rtk::restrict_<T>(h, i, LvlVec<T>::r(h->L[i - 1]), LvlVec<T>::f(h->L[i])));
         }
         if (i < nl - 1) {
-            if (i > 0)
+            if (i > l0)
                 RT_CUDA(h->ctx, cudaMemsetAsync(LvlVec<T>::u(h->L[i]), 0, sizeof(T) * 3 * h->L[i].nv, h->ctx->stream));
             RT_CHECK(level_smooth<T>(h, i, smoother, pre, omega, false));
         } else {
             RT_CHECK(rtk::coarsest_solve<T>(h, LvlVec<T>::f(h->L[i]), LvlVec<T>::u(h->L[i])));
         }
     }
-    for (int i = nl - 2; i >= 0; i--) {
+    for (int i = nl - 2; i >= l0; i--) {
         RT_CHECK(rtk::prolong_add<T>(h, i, LvlVec<T>::u(h->L[i + 1]), LvlVec<T>::u(h->L[i])));
         RT_CHECK(level_smooth<T>(h, i, smoother, post, omega, smoother == RT_SMOOTH_SGS));
     }
@@ -1271,6 +1276,33 @@ static int precondition(rt_hier* h, const double* r, double* z, const double* rr
         RT_CUDA(h->ctx, cudaMemsetAsync(L.u32, 0, sizeof(float) * n, h->ctx->stream));
         RT_CHECK(vcycle_T<float>(h, h->P.smoother, h->P.pre_sweeps, h->P.post_sweeps, h->P.jacobi_omega));
         RT_CHECK(rtk::f2d_scaled(h, n, L.u32, z, rr_dev));
+    } else if (h->P.precision == RT_FP64_FINE && h->L.size() > 1) {
+        // FP64 smoothing and residual on the finest level (on r / z themselves), the coarse
+        // V-cycle in FP32 on the restricted residual scaled by 1 / |r|, its correction added back
+        double* saved_f = L.f;
+        double* saved_u = L.u;
+        L.f = const_cast<double*>(r);
+        L.u = z;
+        rt_level& L1 = h->L[1];
+        int s = RT_OK;
+        auto step = [&](int st) { if (s == RT_OK) s = st; };
+        if (cudaMemsetAsync(z, 0, sizeof(double) * n, h->ctx->stream) != cudaSuccess) s = RT_ECUDA;
+        step(level_smooth<double>(h, 0, h->P.smoother, h->P.pre_sweeps, h->P.jacobi_omega, false));
+        step(level_residual<double>(h, 0));
+        step(rtk::d2f_scaled(h, n, L.r, L.r32, rr_dev));
+        step(rtk::restrict_<float>(h, 1, L.r32, L1.f32));
+        if (s == RT_OK && cudaMemsetAsync(L1.u32, 0, sizeof(float) * 3 * L1.nv, h->ctx->stream) != cudaSuccess)
+            s = RT_ECUDA;
+        step(vcycle_T<float>(h, h->P.smoother, h->P.pre_sweeps, h->P.post_sweeps, h->P.jacobi_omega, 1));
+        if (s == RT_OK && cudaMemsetAsync(L.u32, 0, sizeof(float) * n, h->ctx->stream) != cudaSuccess) s = RT_ECUDA;
+        step(rtk::prolong_add<float>(h, 0, L1.u32, L.u32));
+        step(rtk::f2d_scaled_add(h, n, L.u32, z, rr_dev));
+        step(level_smooth<double>(h, 0, h->P.smoother, h->P.post_sweeps, h->P.jacobi_omega,
+                                  h->P.smoother == RT_SMOOTH_SGS));
+        L.f = saved_f;
+        L.u = saved_u;
+        if (s == RT_ECUDA) return rt_fail(h->ctx, RT_ECUDA, "hybrid V-cycle memset failed");
+        RT_CHECK(s);
     } else {
         // run the FP64 V-cycle on level-0 f/u, using r/z as the level-0 vectors
         double* saved_f = L.f;

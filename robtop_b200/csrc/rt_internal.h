@@ -245,6 +245,7 @@ int d2f(rt_hier* h, long n, const double* a, float* b);
 int f2d(rt_hier* h, long n, const float* a, double* b);
 int d2f_scaled(rt_hier* h, long n, const double* a, float* b, const double* s_dev);
 int f2d_scaled(rt_hier* h, long n, const float* a, double* b, const double* s_dev);
+int f2d_scaled_add(rt_hier* h, long n, const float* a, double* b, const double* s_dev);
 int pcg_update_xr(rt_hier* h, long n, const double* scal_alpha_num, const double* scal_alpha_den, double* x,
                   double* r, const double* p, const double* q, double* rold);
 int pcg_update_p(rt_hier* h, long n, const double* s_num, const double* s_den, double* p, const double* z,

@@ -103,6 +103,14 @@ __global__ void k_f2d_scaled(long n, const float* __restrict__ a, double* __rest
         b[i] = (double)a[i] * sc;
 }
 
+// b += a * sqrt(s) (a coarse correction computed on a right-hand side scaled by 1 / sqrt(s))
+__global__ void k_f2d_scaled_add(long n, const float* __restrict__ a, double* __restrict__ b,
+                                 const double* __restrict__ s) {
+    const double sc = sqrt(fmax(s[0], 1e-300));
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        b[i] += (double)a[i] * sc;
+}
+
 // x += alpha p, r -= alpha q, rold = r(before);  alpha = num / den read on the device
 __global__ void k_pcg_xr(long n, const double* __restrict__ num, const double* __restrict__ den, double* __restrict__ x,
                          double* __restrict__ r, const double* __restrict__ p, const double* __restrict__ q,
@@ -469,6 +477,11 @@ int d2f_scaled(rt_hier* h, long n, const double* a, float* b, const double* s) {
 
 int f2d_scaled(rt_hier* h, long n, const float* a, double* b, const double* s) {
     return rt_launch(h->ctx, "f2d_scaled", [&] { k_f2d_scaled<<<gridN(h->ctx, n), 256, 0, h->ctx->stream>>>(n, a, b, s); });
+}
+
+int f2d_scaled_add(rt_hier* h, long n, const float* a, double* b, const double* s) {
+    return rt_launch(h->ctx, "f2d_scaled_add",
+                     [&] { k_f2d_scaled_add<<<gridN(h->ctx, n), 256, 0, h->ctx->stream>>>(n, a, b, s); });
 }
 
 int pcg_update_xr(rt_hier* h, long n, const double* num, const double* den, double* x, double* r, const double* p,

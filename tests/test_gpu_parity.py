@@ -235,7 +235,9 @@ def test_vcycle_sequence(pair):
 
 @pytest.mark.parametrize("precision,smoother,sweeps", [(rb.FP64, rb.SMOOTH_SGS, 1), (rb.FP32, rb.SMOOTH_SGS, 1),
                                                        (rb.FP32, rb.SMOOTH_CHEBY, 4),
-                                                       (rb.FP64, rb.SMOOTH_JACOBI, 2)])
+                                                       (rb.FP64, rb.SMOOTH_JACOBI, 2),
+                                                       (rb.FP64_FINE, rb.SMOOTH_CHEBY, 4),
+                                                       (rb.FP64_FINE, rb.SMOOTH_SGS, 1)])
 def test_pcg_to_1e6(pair, precision, smoother, sweeps):
     cfg, ctx, G, H = pair
     b = _rand_vec(G, 0, 80)
