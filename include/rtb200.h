@@ -84,6 +84,8 @@ typedef struct rt_params {
     int precision;          /* rt_precision of the V-cycle inside rt_pcg / rt_worst_case */
     int coarsest_elements;  /* halve while more elements than this are solid (the reference: 400,
                                grid/Grid.cpp:488); the coarsest level is solved densely (<= 12288 DOF) */
+    int cycle_gamma;        /* coarse corrections per visit of levels >= 1: 1 V-cycle (the reference), 2 W */
+    int coarse_sweeps;      /* smoothing steps on levels >= 1 (0: pre_sweeps / post_sweeps as on the finest) */
 } rt_params;
 
 typedef struct rt_solve_info {

@@ -31,7 +31,7 @@ class Params(C.Structure):
         ("youngs_modulus", C.c_double), ("poisson_ratio", C.c_double), ("element_length", C.c_double),
         ("mode", C.c_int), ("skip_layer1", C.c_int), ("smoother", C.c_int), ("pre_sweeps", C.c_int),
         ("post_sweeps", C.c_int), ("jacobi_omega", C.c_double), ("precision", C.c_int),
-        ("coarsest_elements", C.c_int),
+        ("coarsest_elements", C.c_int), ("cycle_gamma", C.c_int), ("coarse_sweeps", C.c_int),
     ]
 
 

@@ -211,6 +211,8 @@ extern "C" void rt_params_default(rt_params* p) {
     p->jacobi_omega = 0.6;
     p->precision = RT_FP64;
     p->coarsest_elements = 400;
+    p->cycle_gamma = 1;
+    p->coarse_sweeps = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -1141,29 +1143,33 @@ static int level_smooth(rt_hier* h, int lvl, int smoother, int sweeps, double om
     return RT_OK;
 }
 
-// HierarchyGrid::v_cycle (grid/Grid.cpp:1068-1113) over the real levels
-// levels l0 .. coarsest (level l0's u is the caller's initial guess)
+// the multigrid cycle from level i down (level i's u is the caller's initial guess): smoothing,
+// the coarse correction (cycle_gamma times on levels >= 1 unless the next level is the coarsest,
+// whose solve is exact: gamma = 2 is the W-cycle), smoothing; pre/post mirror each other, so the
+// cycle is symmetric when the smoother is (SGS, Jacobi, Chebyshev)
+template <typename T>
+static int mg_cycle(rt_hier* h, int i, int smoother, int pre, int post, double omega) {
+    const int nl = (int)h->L.size();
+    if (i == nl - 1) return rtk::coarsest_solve<T>(h, LvlVec<T>::f(h->L[i]), LvlVec<T>::u(h->L[i]));
+    const int cs = h->P.coarse_sweeps;
+    const int npre = (i > 0 && cs > 0) ? cs : pre, npost = (i > 0 && cs > 0) ? cs : post;
+    RT_CHECK(level_smooth<T>(h, i, smoother, npre, omega, false));
+    const int reps = (i > 0 && i + 1 < nl - 1 && h->P.cycle_gamma > 1) ? h->P.cycle_gamma : 1;
+    for (int g = 0; g < reps; g++) {
+        RT_CHECK(level_residual<T>(h, i));
+        RT_CHECK(rtk::restrict_<T>(h, i + 1, LvlVec<T>::r(h->L[i]), LvlVec<T>::f(h->L[i + 1])));
+        RT_CUDA(h->ctx,
+                cudaMemsetAsync(LvlVec<T>::u(h->L[i + 1]), 0, sizeof(T) * 3 * h->L[i + 1].nv, h->ctx->stream));
+        RT_CHECK(mg_cycle<T>(h, i + 1, smoother, pre, post, omega));
+        RT_CHECK(rtk::prolong_add<T>(h, i, LvlVec<T>::u(h->L[i + 1]), LvlVec<T>::u(h->L[i])));
+    }
+    return level_smooth<T>(h, i, smoother, npost, omega, smoother == RT_SMOOTH_SGS);
+}
+
+// HierarchyGrid::v_cycle (grid/Grid.cpp:1068-1113) over levels l0 .. coarsest
 template <typename T>
 static int vcycle_T(rt_hier* h, int smoother, int pre, int post, double omega, int l0 = 0) {
-    const int nl = (int)h->L.size();
-    for (int i = l0; i < nl; i++) {
-        if (i > l0) {
-            RT_CHECK(level_residual<T>(h, i - 1));
-            RT_CHECK(rtk::restrict_<T>(h, i, LvlVec<T>::r(h->L[i - 1]), LvlVec<T>::f(h->L[i])));
-        }
-        if (i < nl - 1) {
-            if (i > l0)
-                RT_CUDA(h->ctx, cudaMemsetAsync(LvlVec<T>::u(h->L[i]), 0, sizeof(T) * 3 * h->L[i].nv, h->ctx->stream));
-            RT_CHECK(level_smooth<T>(h, i, smoother, pre, omega, false));
-        } else {
-            RT_CHECK(rtk::coarsest_solve<T>(h, LvlVec<T>::f(h->L[i]), LvlVec<T>::u(h->L[i])));
-        }
-    }
-    for (int i = nl - 2; i >= l0; i--) {
-        RT_CHECK(rtk::prolong_add<T>(h, i, LvlVec<T>::u(h->L[i + 1]), LvlVec<T>::u(h->L[i])));
-        RT_CHECK(level_smooth<T>(h, i, smoother, post, omega, smoother == RT_SMOOTH_SGS));
-    }
-    return RT_OK;
+    return mg_cycle<T>(h, l0, smoother, pre, post, omega);
 }
 
 static int read_scalars(rt_hier* h, int first, int count, double* out) {
@@ -1376,7 +1382,8 @@ static int pcg_graph_run(rt_hier* h, double* x, double* r, bool no_support) {
                          ((uint64_t)h->P.smoother << 3) ^ ((uint64_t)h->P.pre_sweeps << 6) ^
                          ((uint64_t)h->P.post_sweeps << 11) ^ ((uint64_t)no_support << 16) ^
                          ((uint64_t)(h->P.jacobi_omega * 1e6) << 20) ^ ((uint64_t)h->graph_epoch << 40) ^
-                         ((uint64_t)(uintptr_t)h->unet * 2654435761ull);
+                         ((uint64_t)(uintptr_t)h->unet * 2654435761ull) ^ ((uint64_t)h->P.cycle_gamma << 56) ^
+                         ((uint64_t)h->P.coarse_sweeps << 60);
     if (!h->pcg_exec || h->pcg_key != key) {
         if (h->pcg_exec) { cudaGraphExecDestroy(h->pcg_exec); h->pcg_exec = nullptr; }
         if (h->pcg_graph) { cudaGraphDestroy(h->pcg_graph); h->pcg_graph = nullptr; }
@@ -2117,7 +2124,8 @@ static uint64_t batch_key(rt_hier* const* hs, int n, double tol, int maxit) {
         mix(h->uid);
         mix(h->graph_epoch);
         mix((uint64_t)h->P.precision | ((uint64_t)h->P.smoother << 4) | ((uint64_t)h->P.pre_sweeps << 8) |
-            ((uint64_t)h->P.post_sweeps << 16) | ((uint64_t)h->P.mode << 24));
+            ((uint64_t)h->P.post_sweeps << 16) | ((uint64_t)h->P.mode << 24) | ((uint64_t)h->P.cycle_gamma << 32) |
+            ((uint64_t)h->P.coarse_sweeps << 40));
         uint64_t om;
         memcpy(&om, &h->P.jacobi_omega, 8);
         mix(om);
