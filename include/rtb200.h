@@ -86,6 +86,9 @@ typedef struct rt_params {
                                grid/Grid.cpp:488); the coarsest level is solved densely (<= 12288 DOF) */
     int cycle_gamma;        /* coarse corrections per visit of levels >= 1: 1 V-cycle (the reference), 2 W */
     int coarse_sweeps;      /* smoothing steps on levels >= 1 (0: pre_sweeps / post_sweeps as on the finest) */
+    int precision_fallback; /* N > 0: a PCG solve whose FP32 / FP64_FINE V-cycles stop reducing |r| (no halving
+                               within N iterations; default 100) continues from its iterate with FP64 V-cycles;
+                               0: off */
 } rt_params;
 
 typedef struct rt_solve_info {
@@ -224,6 +227,9 @@ int rt_bench_fine_kernel(rt_hier* h, int precision, int mode, int reps, double* 
 /* MG-preconditioned CG on level 0: u <- K^-1 f to ||r||/||f|| <= tol (solveFEM's role,
  * optimization/optimization.cpp:85-91).  Uses the precision/smoother in the params. */
 int rt_pcg(rt_hier* h, double tol, int maxit, rt_solve_info* info);
+/* number of solves on h (PCG, Lanczos inner solves, batched instances) that switched to FP64
+ * V-cycles after stalling (rt_params.precision_fallback); no reference counterpart */
+long long rt_hier_precision_fallbacks(rt_hier* h);
 /* worst-case load: largest eigenvalue of P K^-1 P on the load set.
  * RT_WORST_MODPM restates modifiedPM (optimization/optimization.cpp:123-261);
  * RT_WORST_LANCZOS runs k Lanczos steps with PCG inner solves to inner_tol.

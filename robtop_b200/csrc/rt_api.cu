@@ -213,6 +213,7 @@ extern "C" void rt_params_default(rt_params* p) {
     p->coarsest_elements = 400;
     p->cycle_gamma = 1;
     p->coarse_sweeps = 0;
+    p->precision_fallback = 100;
 }
 
 // ---------------------------------------------------------------------------
@@ -1346,9 +1347,21 @@ __global__ void k_pcg_tail(double* __restrict__ scal, cudaGraphConditionalHandle
     // norm did not drop below ratio x the previous one
     if (scal[28] != 0.0 && scal[29] > 0.0 && !(scal[21] <= scal[27] * scal[27] * scal[29])) scal[28] = 0.0;
     scal[29] = scal[21];
+    // precision fallback: the loop ends once |r| has not halved within scal[93] iterations (0: off);
+    // scal[90] is the last halving's r.r, scal[91] its iteration, scal[92] the flag
+    bool stalled = false;
+    if (scal[93] > 0.0) {
+        if (scal[21] <= 0.25 * scal[90]) {
+            scal[90] = scal[21];
+            scal[91] = it;
+        } else if (it - scal[91] >= scal[93]) {
+            scal[92] = 1.0;
+            stalled = true;
+        }
+    }
     if (use_cond) {
         const double rr = scal[21], bb = scal[22] > 0 ? scal[22] : 1.0;
-        const bool go = isfinite(rr) && sqrt(rr) > scal[25] * sqrt(bb) && it < scal[26];
+        const bool go = isfinite(rr) && sqrt(rr) > scal[25] * sqrt(bb) && it < scal[26] && !stalled;
         cudaGraphSetConditional(cond, go ? 1u : 0u);
     }
 }
@@ -1455,24 +1468,46 @@ static int pcg_core(rt_hier* h, double* x, const double* b, double tol, int maxi
         memcpy(h->ctx->hscal + 8, st, sizeof(st));
         RT_CUDA(h->ctx, cudaMemcpyAsync(h->scal + 24, h->ctx->hscal + 8, sizeof(st), cudaMemcpyHostToDevice,
                                         h->ctx->stream));
+        // scal[90..93]: stall detection of the reduced-precision V-cycles (see k_pcg_tail)
+        const bool fallback = h->P.precision != RT_FP64 && h->P.precision_fallback > 0;
+        double sd[4] = {s[0], 0.0, 0.0, fallback ? (double)h->P.precision_fallback : 0.0};
+        memcpy(h->ctx->hscal + 16, sd, sizeof(sd));
+        RT_CUDA(h->ctx, cudaMemcpyAsync(h->scal + 90, h->ctx->hscal + 16, sizeof(sd), cudaMemcpyHostToDevice,
+                                        h->ctx->stream));
         if (h->use_graphs && !h->ctx->profile) {
             RT_CHECK(pcg_graph_run(h, x, r, no_support));
         } else {
             for (int k = 0; k < maxit; k++) {
                 RT_CHECK(pcg_body(h, x, r, no_support, 0));
-                double s2[4];
+                double s2[4], stall = 0;
                 RT_CHECK(read_scalars(h, 21, 4, s2));
-                if (!std::isfinite(s2[0]) || std::sqrt(s2[0]) / bn <= tol) break;
+                RT_CHECK(read_scalars(h, 92, 1, &stall));
+                if (!std::isfinite(s2[0]) || std::sqrt(s2[0]) / bn <= tol || stall != 0.0) break;
             }
         }
-        double s3[4];
+        double s3[4], stall = 0;
         RT_CHECK(read_scalars(h, 21, 4, s3));  // rr, bb, (unused), it
+        RT_CHECK(read_scalars(h, 92, 1, &stall));
         if (!std::isfinite(s3[0])) {
             if (info) { info->status = RT_ENAN; info->iterations = (int)s3[3]; }
             return rt_fail(h->ctx, RT_ENAN, "NaN in PCG at iteration %d", (int)s3[3]);
         }
         rel = std::sqrt(s3[0]) / bn;
         it = (int)s3[3];
+        if (fallback && stall != 0.0 && rel > tol && it < maxit) {
+            // continue from the current iterate with FP64 V-cycles (flexible CG restarts)
+            const int saved = h->P.precision;
+            h->P.precision = RT_FP64;
+            rt_solve_info sub;
+            memset(&sub, 0, sizeof(sub));
+            int vc = 0;
+            const int st2 = pcg_core(h, x, b, tol, maxit - it, &sub, &vc);
+            h->P.precision = saved;
+            RT_CHECK(st2);
+            it += sub.iterations;
+            rel = sub.rel_residual;
+            h->fallbacks++;
+        }
     }
     *vcycles += it;
     if (info) {
@@ -2042,13 +2077,18 @@ extern "C" int rt_hier_workspace_create(rt_hier* parent, rt_hier** out) {
 }
 
 // start of one instance's loop in a batched graph: iteration state, and whether to iterate at all
-__global__ void k_pcg_start(double* __restrict__ scal, double tol, double maxit, cudaGraphConditionalHandle cond) {
+__global__ void k_pcg_start(double* __restrict__ scal, double tol, double maxit, double stall,
+                            cudaGraphConditionalHandle cond) {
     if (threadIdx.x != 0) return;
     scal[24] = 0.0;
     scal[25] = tol;
     scal[26] = maxit;
     scal[28] = 0.0;  // batched instances run without the learned correction
     scal[29] = scal[21];
+    scal[90] = scal[21];  // stall detection of reduced-precision V-cycles (k_pcg_tail)
+    scal[91] = 0.0;
+    scal[92] = 0.0;
+    scal[93] = stall;
     const double rr = scal[21], bb = scal[22] > 0 ? scal[22] : 1.0;
     const bool go = isfinite(rr) && sqrt(rr) > tol * sqrt(bb) && maxit > 0;
     cudaGraphSetConditional(cond, go ? 1u : 0u);
@@ -2080,7 +2120,8 @@ static int build_batch_graph(rt_ctx* c, rt_hier* const* hs, int n, double tol, i
         if (e == cudaSuccess && s == RT_OK) {
             double* scal = h->scal;
             double tl = tol, mi = (double)maxit;
-            void* args[] = {(void*)&scal, (void*)&tl, (void*)&mi, (void*)&cond};
+            double stall = (h->P.precision != RT_FP64 && h->P.precision_fallback > 0) ? (double)h->P.precision_fallback : 0.0;
+            void* args[] = {(void*)&scal, (void*)&tl, (void*)&mi, (void*)&stall, (void*)&cond};
             cudaKernelNodeParams kp = {};
             kp.func = (void*)k_pcg_start;
             kp.gridDim = dim3(1);
@@ -2125,7 +2166,7 @@ static uint64_t batch_key(rt_hier* const* hs, int n, double tol, int maxit) {
         mix(h->graph_epoch);
         mix((uint64_t)h->P.precision | ((uint64_t)h->P.smoother << 4) | ((uint64_t)h->P.pre_sweeps << 8) |
             ((uint64_t)h->P.post_sweeps << 16) | ((uint64_t)h->P.mode << 24) | ((uint64_t)h->P.cycle_gamma << 32) |
-            ((uint64_t)h->P.coarse_sweeps << 40));
+            ((uint64_t)h->P.coarse_sweeps << 40) | ((uint64_t)h->P.precision_fallback << 48));
         uint64_t om;
         memcpy(&om, &h->P.jacobi_omega, 8);
         mix(om);
@@ -2198,16 +2239,32 @@ static int pcg_batch_core(rt_hier* const* hs, int n, double tol, int maxit, rt_s
     RT_CUDA(c, cudaGetLastError());
     for (int i = 0; i < n; i++) {
         rt_hier* h = hs[i];
-        double sc[4];
+        double sc[4], stall = 0;
         RT_CHECK(read_scalars(h, 21, 4, sc));  // r.r, b.b, (unused), iterations
+        RT_CHECK(read_scalars(h, 92, 1, &stall));
         const double bn = sc[1] > 0 ? std::sqrt(sc[1]) : 1.0;
-        const double rel = std::sqrt(sc[0]) / bn;
+        double rel = std::sqrt(sc[0]) / bn;
+        int its = (int)sc[3];
         if (!std::isfinite(sc[0])) return rt_fail(c, RT_ENAN, "NaN in batched PCG instance %d", i);
+        if (stall != 0.0 && rel > tol && its < maxit) {
+            // this instance's reduced-precision V-cycles stalled: continue it alone with FP64 ones
+            const int saved = h->P.precision;
+            h->P.precision = RT_FP64;
+            rt_solve_info sub;
+            memset(&sub, 0, sizeof(sub));
+            int vc = 0;
+            const int st2 = pcg_core(h, h->L[0].u, h->L[0].f, tol, maxit - its, &sub, &vc);
+            h->P.precision = saved;
+            RT_CHECK(st2);
+            its += sub.iterations;
+            rel = sub.rel_residual;
+            h->fallbacks++;
+        }
         if (infos) {
             rt_solve_info& si = infos[i];
             memset(&si, 0, sizeof(si));
-            si.iterations = (int)sc[3];
-            si.vcycles = (int)sc[3];
+            si.iterations = its;
+            si.vcycles = its;
             si.rel_residual = rel;
             si.status = rel <= tol ? RT_OK : RT_ENOCONV;
             si.seconds = ms * 1e-3;
@@ -2531,3 +2588,5 @@ extern "C" int rt_unet_harvest(rt_hier* h, rt_unet* u, int k_iter, uint64_t seed
     if (si.status != RT_OK) return rt_fail(c, RT_ENOCONV, "harvest: the exact-error solve did not converge");
     return RT_OK;
 }
+
+extern "C" long long rt_hier_precision_fallbacks(rt_hier* h) { return h ? h->fallbacks : 0; }

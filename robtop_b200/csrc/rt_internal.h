@@ -128,6 +128,7 @@ struct rt_hier {
     // fallback ratio, scal[28] the gate (1 while active), scal[29] the previous iteration's r.r
     struct rt_unet* unet = nullptr;
     double unet_fallback = 1.0;
+    long long fallbacks = 0;  // PCG solves that continued with FP64 V-cycles after stalling
 };
 
 #define RT_RED_BLOCKS 296
