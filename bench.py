@@ -34,10 +34,10 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = dict(nx=128, ny=128, nz=64, seed=0, k=16, tol=1e-6)
 # plain: the reference's V-cycle made symmetric (8-colour GS, forward pre / backward post), all FP64
-# mixed: FP32 V-cycle with Chebyshev smoothing (degree 4 on the finest level, 8 on coarser ones) inside
-#        FP64 flexible CG, FP64 coarsest solve, FP64 V-cycles once the FP32 ones stall
+# mixed: FP32 V-cycle with Chebyshev(4) smoothing inside FP64 flexible CG, FP64 coarsest solve,
+#        FP64 V-cycles once the FP32 ones stall
 FORMS = {"plain": dict(precision="FP64", smoother="SMOOTH_SGS", sweeps=1, coarse_sweeps=0),
-         "mixed": dict(precision="FP32", smoother="SMOOTH_CHEBY", sweeps=4, coarse_sweeps=8)}
+         "mixed": dict(precision="FP32", smoother="SMOOTH_CHEBY", sweeps=4, coarse_sweeps=0)}
 METRIC = "worst-case solve (Lanczos k=16, MG-PCG inner solves to rel. residual 1e-6) on 128x128x64"
 
 
@@ -667,9 +667,9 @@ def main():
         "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
         "config": {"workload": "worst-case 128x128x64 (smoothed random density, z=0 clamped, top-face load set, "
                                "wsff), Lanczos k=16, inner MG-PCG to 1e-6, stencil assembly included",
-                   "form": "mixed: FP32 V-cycle (Chebyshev smoothing, degree 4 finest / 8 coarse, FP64 coarsest "
-                           "solve) inside FP64 flexible CG, one CUDA graph per solve; plain (fp64_ms_per_step): "
-                           "FP64 symmetric-GS V-cycle",
+                   "form": "mixed: FP32 V-cycle (Chebyshev(4) smoothing, FP64 coarsest solve) inside FP64 "
+                           "flexible CG, one CUDA graph per solve; plain (fp64_ms_per_step): FP64 symmetric-GS "
+                           "V-cycle",
                    "fp64_ms_per_step": r64["ms"] / args.steps if r64 else None,
                    "speedup_vs_fp64": r64["ms"] / r32["ms"] if r64 else None,
                    "lambda_mixed": lam32, "lambda_fp64": lam64,

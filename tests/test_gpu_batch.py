@@ -171,3 +171,25 @@ def test_context_outlives_its_hierarchies():
     assert W.pcg(1e-6, 500).status == rb._capi.RT_OK
     W.close()
     G.close()
+
+
+def test_precision_fallback_at_scale():
+    """On the 256x256x128 smoothed-random box (stiffness contrast 1e9) FP32 V-cycles stop reducing
+    the residual; the solve continues from its iterate with FP64 V-cycles and reaches 1e-6."""
+    from robtop_b200 import configs
+
+    cfg = configs.worst_case_box(256, 256, 128, seed=0)
+    ctx = rb.Context(0)
+    G = _grid(ctx, cfg, _params(cfg, rb.FP32, rb.SMOOTH_CHEBY, 4))
+    f = np.zeros(3 * G[0].nv)
+    rng = np.random.default_rng(5)
+    for c in range(3):
+        f[c * G[0].nv + cfg["load_nodes"]] = rng.standard_normal(cfg["load_nodes"].size)
+    G[0].setForce(f)
+    G[0].setDisplacement(np.zeros_like(f))
+    assert rb.lib().rt_hier_precision_fallbacks(G.handle) == 0
+    info = G.pcg(1e-6, 3000)
+    assert info.status == rb._capi.RT_OK and info.rel_residual <= 1e-6
+    assert rb.lib().rt_hier_precision_fallbacks(G.handle) == 1
+    G.close()
+    ctx.close()

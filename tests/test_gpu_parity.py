@@ -431,35 +431,3 @@ def test_errors_are_reported_not_fatal():
         G.set_load_nodes(np.array([10 ** 9]), np.zeros((1, 3)))
     G.close()
     ctx.close()
-
-
-def test_precision_fallback_continues_in_fp64(pair):
-    """A reduced-precision PCG whose residual stops halving continues from its iterate with FP64
-    V-cycles: a 2-iteration stall window forces the switch; the solution is the FP64 one."""
-    cfg, ctx, G, H = pair
-    b = _rand_vec(G, 0, 85)
-    if cfg["mode"] not in (rb.MODE_WSCF, rb.MODE_WSFF):
-        pytest.skip("supported structures only")
-    b[np.tile(cfg["vfix"].ravel().astype(bool), 3)] = 0
-    params = G.params
-    params.precision = rb.FP32
-    params.smoother = rb.SMOOTH_CHEBY
-    params.pre_sweeps = params.post_sweeps = 4
-    params.precision_fallback = 2
-    G.set_params(params)
-    G.update_stencil()
-    n0 = rb.lib().rt_hier_precision_fallbacks(G.handle)
-    G[0].setForce(b)
-    G[0].reset_displacement()
-    info = G.pcg(1e-8, 1000)
-    assert info.status == 0 and info.rel_residual <= 1e-8
-    assert rb.lib().rt_hier_precision_fallbacks(G.handle) == n0 + 1
-    x = G[0].getDisplacement()
-    r = (b - H.applyK(x)) * np.tile(H.arrs[0]["vact"], 3)
-    assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.01e-8
-    params.precision = rb.FP64
-    params.smoother = rb.SMOOTH_SGS
-    params.pre_sweeps = params.post_sweeps = 1
-    params.precision_fallback = 100
-    G.set_params(params)
-    G.update_stencil()
