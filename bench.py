@@ -568,6 +568,97 @@ def run_learned(args):
     return 0
 
 
+def run_c5(args):
+    """Worst-case optimisation on the 511x256x256 arch (solid box minus a radius-96 tunnel along x,
+    four 16x16 support pads at the bottom corners, top face loadable with normal-constrained loads,
+    wscf; rho = 0.4 to start, volume target 0.4, filter radius 2, move limit 0.06, damping 0.5,
+    p = 3).  A step is one OC iteration (stencil update, worst-case Lanczos k = 16 with MG-PCG inner
+    solves to 1e-6, sensitivity, filter, OC update) in the mixed form.  After the timed steps the
+    worst-case solve of the current design is timed in the mixed and the plain FP64 form and their
+    eigenvalues compared."""
+    import torch
+
+    import robtop_b200 as rb
+    from robtop_b200 import configs
+
+    ws_, rank, lrank = dist_env()
+    ctx = make_ctx(rb, lrank)
+    stream = torch.cuda.ExternalStream(ctx_stream_handle(ctx))
+    t0 = time.perf_counter()
+    cfg = configs.arch(511, 256, 256)
+    p = rb.default_params(mode=cfg["mode"], youngs_modulus=1e6, poisson_ratio=0.4, power_penalty=3.0, min_rho=1e-3,
+                          volume_ratio=0.4, design_step=0.06, damp_ratio=0.5, filter_radius=2.0,
+                          precision=rb.FP32, smoother=rb.SMOOTH_CHEBY, pre_sweeps=4, post_sweeps=4)
+    G = rb.HierarchyGrid(ctx, p)
+    G.genFromBox(cfg["eact"])
+    G[0].setRho(cfg["rho"].ravel())
+    G.set_support(cfg["vfix"])
+    G.set_load_nodes(cfg["load_nodes"], cfg["normals"])
+    G.update_stencil()
+    G.autotune(reps=2)
+    t_setup = time.perf_counter() - t0
+
+    def oc_step(seed):
+        lam = C.c_double()
+        rb._capi.check(rb.lib().rt_oc_iteration(G.handle, rb.WORST_LANCZOS, WORKLOAD["k"], WORKLOAD["tol"], seed,
+                                                0.4, C.byref(lam)), ctx.handle)
+        return lam.value
+
+    def timed(fn):
+        ctx.sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), out
+
+    for w in range(args.warmup):
+        oc_step(10 + w)
+    clocks = Clocks(lrank)
+    clocks.start()
+    l0 = ctx.launches()
+    ms_oc, lams = 0.0, []
+    for s_ in range(args.steps):
+        ms, lam = timed(lambda: oc_step(100 + s_))
+        ms_oc += ms
+        lams.append(lam)
+    launches = ctx.launches() - l0
+    clk = clocks.stop()
+    fb0 = int(rb.lib().rt_hier_precision_fallbacks(G.handle))
+    forms = {}
+    for name, prec, sm, sw in (("mixed", rb.FP32, rb.SMOOTH_CHEBY, 4), ("plain", rb.FP64, rb.SMOOTH_SGS, 1)):
+        q = G.params
+        q.precision, q.smoother, q.pre_sweeps, q.post_sweeps = prec, sm, sw, sw
+        G.set_params(q)
+        ms, (lam, info) = timed(lambda: step(rb, G, 7))
+        forms[name] = (ms, lam, info.inner_iterations)
+    m_ms, m_lam, m_it = forms["mixed"]
+    p_ms, p_lam, p_it = forms["plain"]
+    line = {"metric": "worst-case optimisation on the 511x256x256 arch: OC iterations (stencil update, Lanczos k=16 "
+                      "worst-case solve to 1e-6, sensitivity, filter, OC update)",
+            "value": args.steps / (ms_oc * 1e-3), "unit": "OC iterations/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_oc / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+            "config": {"workload": "arch 511x256x256 (tunnel radius 96, 16x16 pads), wscf, V 0.4, R 2, move 0.06, "
+                                   "eta 0.5, p 3, rho0 0.4",
+                       "worst_case_lambda_per_step": lams, "setup_s": t_setup,
+                       "worst_case_solve_ms_mixed": m_ms, "worst_case_solve_ms_plain_fp64": p_ms,
+                       "speedup_mixed_vs_plain": p_ms / m_ms,
+                       "lambda_mixed": m_lam, "lambda_plain": p_lam,
+                       "lambda_rel_diff": abs(m_lam - p_lam) / abs(p_lam),
+                       "inner_iterations_mixed": m_it, "inner_iterations_plain": p_it,
+                       "precision_fallbacks": int(rb.lib().rt_hier_precision_fallbacks(G.handle)),
+                       "precision_fallbacks_in_timed_steps": fb0},
+            "clocks": clk, "gpu_launches": launches}
+    if rank == 0:
+        print(json.dumps(line))
+    G.close()
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -575,7 +666,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="worstcase", choices=["worstcase", "batched", "learned"],
+    ap.add_argument("--workload", default="worstcase", choices=["worstcase", "batched", "learned", "c5"],
                     help="batched: the 12-instance + 8-RHS batched-solve configuration instead of the headline one")
     ap.add_argument("--forms", default="both", choices=["both", "mixed"],
                     help="mixed: time only the mixed form (short command for launch-list captures)")
@@ -592,6 +683,8 @@ def main():
         return run_batched(args)
     if args.workload == "learned":
         return run_learned(args)
+    if args.workload == "c5":
+        return run_c5(args)
 
     import torch
 
