@@ -301,6 +301,39 @@ def run_reference(args):
     return 0
 
 
+def run_conv(args):
+    """One U-Net convolution (rt_unet_conv3) on random bf16 data: --conv CIN,COUT --size XxYxZ
+    (voxels); prints its per-launch device time (library CUDA events) and TFLOP/s."""
+    import torch
+
+    import robtop_b200 as rb
+
+    cin, cout = (int(v) for v in args.conv.split(","))
+    X, Y, Z = (int(v) for v in (args.size or "257x257x129").split("x"))
+    V = X * Y * Z
+    ctx = rb.Context(0)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    inp = (torch.randn(V, cin, device="cuda", generator=g) * 0.3).to(torch.bfloat16)
+    w = (torch.randn(cout, 27, cin, device="cuda", generator=g) * 0.05).to(torch.bfloat16)
+    out = torch.empty(V, cout, device="cuda", dtype=torch.bfloat16)
+    argv = (ctx.handle, C.c_void_p(inp.data_ptr()), cin, cin, C.c_void_p(w.data_ptr()), None, cout,
+            C.c_void_p(out.data_ptr()), cout, 0, 1, 0, X, Y, Z)
+    for _ in range(args.warmup):
+        rb._capi.check(rb.lib().rt_unet_conv3(*argv), ctx.handle)
+    ctx.profile(True)
+    ctx.profile_reset()
+    for _ in range(args.steps):
+        rb._capi.check(rb.lib().rt_unet_conv3(*argv), ctx.handle)
+    st = ctx.profile_stats()
+    ctx.profile(False)
+    n, ms = [v for k, v in st.items() if k.startswith("unet_conv3") and v[0]][0]
+    us = ms / n * 1e3
+    print(json.dumps({"kernel": "conv3", "cin": cin, "cout": cout, "dims": [X, Y, Z], "us_per_call": us,
+                      "tflops": 2 * 27 * cin * cout * V / (us * 1e-6) / 1e12}))
+    ctx.close()
+    return 0
+
+
 def run_kernel(args):
     """Repeat one hot operator of the path on the bench workload (short command for
     ncu captures): fine_residual = rt_update_residual(level 0), fine_jacobi =
@@ -670,13 +703,17 @@ def main():
                     help="batched: the 12-instance + 8-RHS batched-solve configuration instead of the headline one")
     ap.add_argument("--forms", default="both", choices=["both", "mixed"],
                     help="mixed: time only the mixed form (short command for launch-list captures)")
-    ap.add_argument("--kernel", default=None, choices=["fine_residual", "fine_jacobi", "st_residual", "fine_cheby_f32",
+    ap.add_argument("--conv", default="16,16", help="--kernel conv3: input and output channels")
+    ap.add_argument("--kernel", default=None, choices=["conv3", "fine_residual", "fine_jacobi", "st_residual",
+                                                      "fine_cheby_f32",
                                                       "fine_residual_f64", "fine_applyK_f64", "fine_residual_f32"])
     ap.add_argument("--size", default=None, help="kernel mode: grid NXxNYxNZ (default: the bench workload)")
     ap.add_argument("--shape", default=None, help="kernel mode: launch shape variant,rows,zchunk (default: autotune)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.kernel == "conv3":
+        return run_conv(args)
     if args.kernel:
         return run_kernel(args)
     if args.workload == "batched":

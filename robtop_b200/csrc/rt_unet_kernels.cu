@@ -174,16 +174,17 @@ __global__ void __launch_bounds__(CONV_THREADS) k_conv3_halo(ConvArgs a, int P, 
         rttc::fence_mbar_init();
     }
     if (warp == 0) rttc::tmem_alloc(tslot, ncols);
-    // halo planes z0-1 .. z0+P (zero outside the box); chunk index fastest for coalescing
-    const int nh = npl * HALO_V * kch;
-    for (int idx = tid; idx < nh; idx += CONV_THREADS) {
-        const int j = idx % kch, rest = idx / kch;
-        const int hv = rest % HALO_V, pl = rest / HALO_V;
-        const int gx = x0 - 1 + hv % HALO_X, gy = y0 - 1 + hv / HALO_X, gz = z0 - 1 + pl;
+    // halo planes z0-1 .. z0+P (zero outside the box): one (plane, halo voxel) pair per thread
+    // and step (constant divisors), its channel chunks in an inner loop
+    const int npairs = npl * HALO_V;
+    for (int pr = tid; pr < npairs; pr += CONV_THREADS) {
+        const int pl = pr / HALO_V, hv = pr - pl * HALO_V;
+        const int hy = hv / HALO_X, hx = hv - hy * HALO_X;
+        const int gx = x0 - 1 + hx, gy = y0 - 1 + hy, gz = z0 - 1 + pl;
         const bool inb = gx >= 0 && gx < a.X && gy >= 0 && gy < a.Y && gz >= 0 && gz < a.Z;
-        const __nv_bfloat16* src =
-            inb ? a.in + ((long)gx + (long)a.X * (gy + (long)a.Y * gz)) * a.in_stride + j * 8 : a.in;
-        rttc::cp_async16(sH + j * lboA + pl * plane_b + hv * 16, src, inb ? 16u : 0u);
+        const __nv_bfloat16* src = inb ? a.in + ((long)gx + (long)a.X * (gy + (long)a.Y * gz)) * a.in_stride : a.in;
+        uint8_t* dst = sH + pl * plane_b + hv * 16;
+        for (int j = 0; j < kch; j++) rttc::cp_async16(dst + j * lboA, src + (inb ? j * 8 : 0), inb ? 16u : 0u);
     }
     // the weights of taps [g G, (g+1) G), each in the K-major layout [chunk][out-channel group][8 rows][16 B]
     const uint32_t lboB = (uint32_t)(cout / 8) * 128;
