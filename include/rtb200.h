@@ -214,7 +214,7 @@ int rt_compliance_noalloc(const double* f_dev, const double* u_dev, long long n,
  * fastest.  reps: timed launches per candidate (<= 0: 5). */
 int rt_autotune(rt_hier* h, int reps);
 /* chosen shape of a finest-level kernel; mode 0 residual, 1 applyK, 2 Jacobi, 3 Chebyshev;
- * variant 0 shared-memory element tile, 1 register-marching element kernel, 2 register marching with
+ * variant 0 shared-memory element tile (ty 2, 4 or 8 node rows), 1 register-marching element kernel, 2 register marching with
  * each layer's output-stage loads issued before its element arithmetic */
 int rt_tuning_info(rt_hier* h, int precision, int mode, int* variant, int* ty, int* zchunk, double* us);
 /* set a finest-level kernel's launch shape explicitly (ty: 2, 4 or 8 rows for variant 1, 2 or 4 for variant 2) */

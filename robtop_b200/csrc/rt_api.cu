@@ -1961,7 +1961,8 @@ extern "C" int rt_autotune(rt_hier* h, int reps) {
         for (int zc : {4, 8, 16, 32, 64}) cands.push_back(rt_tile_cfg{1, ty, zc});
     for (int ty : {2, 4})
         for (int zc : {8, 16, 32}) cands.push_back(rt_tile_cfg{2, ty, zc});
-    for (int zc : {8, 16, 32}) cands.push_back(rt_tile_cfg{0, 4, zc});
+    for (int ty : {2, 4, 8})
+        for (int zc : {8, 16, 32}) cands.push_back(rt_tile_cfg{0, ty, zc});
     for (int prec = 0; prec < 2; prec++)
         for (int mode = 0; mode < 4; mode++) {
             rt_tile_cfg best_cfg = h->tune[prec][mode];
@@ -1996,10 +1997,10 @@ extern "C" int rt_set_tuning(rt_hier* h, int precision, int mode, int variant, i
     if (!h || precision < 0 || precision > 1 || mode < 0 || mode > 3 || variant < 0 || variant > 2 || zchunk < 1)
         return RT_EINVAL;
     RT_NOT_WORKSPACE(h);
-    if (variant == 1 && ty != 2 && ty != 4 && ty != 8) return rt_fail(h->ctx, RT_EINVAL, "rows per tile must be 2, 4 or 8");
+    if (variant <= 1 && ty != 2 && ty != 4 && ty != 8) return rt_fail(h->ctx, RT_EINVAL, "rows per tile must be 2, 4 or 8");
     const int pr = precision == RT_FP64 ? 1 : 0;
     if (variant == 2 && ty != 2 && ty != 4) return rt_fail(h->ctx, RT_EINVAL, "prefetching rows per tile must be 2 or 4");
-    h->tune[pr][mode] = rt_tile_cfg{variant, variant >= 1 ? ty : 4, zchunk};
+    h->tune[pr][mode] = rt_tile_cfg{variant, ty, zchunk};
     h->graph_epoch++;
     return RT_OK;
 }

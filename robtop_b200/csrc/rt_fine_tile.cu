@@ -26,34 +26,47 @@
 
 namespace {
 
-constexpr int TX = 32, TY = 4;             // node tile
-constexpr int EXT = TX + 1, EYT = TY + 1;  // element tile (one halo element below in x and y)
-constexpr int UXT = TX + 2, UYT = TY + 2;  // node halo tile
-constexpr int NE_T = EXT * EYT;            // 165 elements per layer
-constexpr int NU_T = UXT * UYT;            // 204 nodes per layer
-constexpr int TILE_BS = 192;               // >= NE_T, multiple of 32
-constexpr int U_PER_T = (NU_T + TILE_BS - 1) / TILE_BS;  // halo nodes loaded per thread (2)
-
-template <typename T>
-struct TileSmem {
-    T u[2][3][NU_T];   // node layers ez, ez+1 (slot layer & 1)
-    T e[24][NE_T];     // element outputs of the current layer
-    float w[3][NE_T];  // element weights of layers ez-1, ez, ez+1 (slot (layer+3)%3)
+// tile of 32 x TY nodes (TY = 2, 4 or 8; rt_autotune chooses)
+template <int TY_>
+struct Tile {
+    static constexpr int TX = 32, TY = TY_;
+    static constexpr int EXT = TX + 1, EYT = TY + 1;  // element tile (one halo element below in x and y)
+    static constexpr int UXT = TX + 2, UYT = TY + 2;  // node halo tile
+    static constexpr int NE_T = EXT * EYT;            // elements per layer (165 for TY = 4)
+    static constexpr int NU_T = UXT * UYT;            // halo nodes per layer (204 for TY = 4)
+    static constexpr int BS = ((NE_T > TX * TY ? NE_T : TX * TY) + 31) / 32 * 32;  // threads (192 for TY = 4)
+    static constexpr int U_PER_T = (NU_T + BS - 1) / BS;                            // halo nodes per thread
 };
+
+template <typename T, int TY_>
+struct TileSmem {
+    T u[2][3][Tile<TY_>::NU_T];   // node layers ez, ez+1 (slot layer & 1)
+    T e[24][Tile<TY_>::NE_T];     // element outputs of the current layer
+    float w[3][Tile<TY_>::NE_T];  // element weights of layers ez-1, ez, ez+1 (slot (layer+3)%3)
+};
+
+// blocks per SM the register budget is sized for
+template <typename T, int TY_>
+constexpr int tile_min_blocks() {
+    return sizeof(T) == 8 ? (TY_ == 2 ? 3 : TY_ == 4 ? 2 : 1) : (TY_ == 2 ? 8 : TY_ == 4 ? 4 : 2);
+}
 
 // MODE 0: r = f - K u (fixed rows: r = f)     MODE 1: out = K u (fixed rows: u)
 // MODE 2: unew = u + omega D^-1 (f - K u) (fixed: f / n_e)
 // MODE 3: Chebyshev step kstep: d = a_k d + b_k D^-1 (f - K u), unew = u + d (fixed: f / n_e)
-template <typename T, bool WS, int MODE>
-__global__ void __launch_bounds__(TILE_BS, sizeof(T) == 8 ? 2 : 4) k_fine_tile(int nx, int ny, int nz, int zchunk,
+template <typename T, bool WS, int MODE, int TY_>
+__global__ void __launch_bounds__(Tile<TY_>::BS, tile_min_blocks<T, TY_>()) k_fine_tile(int nx, int ny, int nz, int zchunk,
                                                         const uint8_t* __restrict__ vact,
                                                         const float* __restrict__ wgt,
                                                         const uint8_t* __restrict__ vfix, const rte::KtVals<T> kt,
                                                         const T* __restrict__ u, const T* __restrict__ f,
                                                         T* __restrict__ out, T omega, T* __restrict__ dvec,
                                                         const double* __restrict__ coef, int kstep) {
+    using TS = Tile<TY_>;
+    constexpr int TX = TS::TX, TY = TS::TY, EXT = TS::EXT, UXT = TS::UXT, NE_T = TS::NE_T, NU_T = TS::NU_T;
+    constexpr int TILE_BS = TS::BS, U_PER_T = TS::U_PER_T;
     extern __shared__ __align__(16) unsigned char smraw[];
-    TileSmem<T>& S = *reinterpret_cast<TileSmem<T>*>(smraw);
+    TileSmem<T, TY_>& S = *reinterpret_cast<TileSmem<T, TY_>*>(smraw);
     T cheb_a = T(0), cheb_b = T(0);
     if (MODE == 3) {
         const double ca = coef[2 * kstep], cb = coef[2 * kstep + 1];
@@ -288,33 +301,42 @@ __global__ void __launch_bounds__(TILE_BS, sizeof(T) == 8 ? 2 : 4) k_fine_tile(i
 }
 
 
-template <typename T, bool WS, int MODE>
-int launch_tile(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name, T* dvec = nullptr,
-                const double* coef = nullptr, int kstep = 0) {
+template <typename T, bool WS, int MODE, int TY_>
+int launch_tile_ty(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name, T* dvec,
+                   const double* coef, int kstep) {
     rt_level& L = h->L[0];
-    const size_t smem = sizeof(TileSmem<T>);
-    auto kern = k_fine_tile<T, WS, MODE>;
+    const size_t smem = sizeof(TileSmem<T, TY_>);
     const int zc = h->tune[sizeof(T) == 8 ? 1 : 0][MODE].zchunk;
-    dim3 grid((L.vx + TX - 1) / TX, (L.vy + TY - 1) / TY, (L.vz + zc - 1) / zc);
+    dim3 grid((L.vx + Tile<TY_>::TX - 1) / Tile<TY_>::TX, (L.vy + TY_ - 1) / TY_, (L.vz + zc - 1) / zc);
     const rte::KtVals<T> kt = rte::make_kt<T>(h);
     return rt_launch(h->ctx, name, [&] {
-        kern<<<grid, TILE_BS, smem, h->ctx->stream>>>(L.nx, L.ny, L.nz, zc, L.vact, h->w, h->vfix, kt, u, f, out,
-                                                      (T)omega, dvec, coef, kstep);
+        k_fine_tile<T, WS, MODE, TY_><<<grid, Tile<TY_>::BS, smem, h->ctx->stream>>>(
+            L.nx, L.ny, L.nz, zc, L.vact, h->w, h->vfix, kt, u, f, out, (T)omega, dvec, coef, kstep);
     });
 }
 
 template <typename T, bool WS, int MODE>
-cudaError_t set_attr() {
-    return cudaFuncSetAttribute(k_fine_tile<T, WS, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sizeof(TileSmem<T>));
+int launch_tile(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name, T* dvec = nullptr,
+                const double* coef = nullptr, int kstep = 0) {
+    switch (h->tune[sizeof(T) == 8 ? 1 : 0][MODE].ty) {
+        case 2: return launch_tile_ty<T, WS, MODE, 2>(h, u, f, out, omega, name, dvec, coef, kstep);
+        case 8: return launch_tile_ty<T, WS, MODE, 8>(h, u, f, out, omega, name, dvec, coef, kstep);
+        default: return launch_tile_ty<T, WS, MODE, 4>(h, u, f, out, omega, name, dvec, coef, kstep);
+    }
 }
 
-template <typename T>
+template <typename T, bool WS, int MODE, int TY_>
+cudaError_t set_attr() {
+    return cudaFuncSetAttribute(k_fine_tile<T, WS, MODE, TY_>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(TileSmem<T, TY_>));
+}
+
+template <typename T, int TY_>
 cudaError_t set_attrs_T() {
     cudaError_t e = cudaSuccess;
-    cudaError_t r[8] = {set_attr<T, false, 0>(), set_attr<T, false, 1>(), set_attr<T, false, 2>(),
-                        set_attr<T, false, 3>(), set_attr<T, true, 0>(),  set_attr<T, true, 1>(),
-                        set_attr<T, true, 2>(),  set_attr<T, true, 3>()};
+    cudaError_t r[8] = {set_attr<T, false, 0, TY_>(), set_attr<T, false, 1, TY_>(), set_attr<T, false, 2, TY_>(),
+                        set_attr<T, false, 3, TY_>(), set_attr<T, true, 0, TY_>(),  set_attr<T, true, 1, TY_>(),
+                        set_attr<T, true, 2, TY_>(),  set_attr<T, true, 3, TY_>()};
     for (auto x : r)
         if (x != cudaSuccess) e = x;
     return e;
@@ -327,10 +349,10 @@ namespace rtk {
 // dynamic shared-memory limits of every tile-kernel variant, set once per device
 // (before any stream capture can include a launch)
 int init_tile_kernels(rt_ctx* c) {
-    cudaError_t e1 = set_attrs_T<double>(), e2 = set_attrs_T<float>();
-    if (e1 != cudaSuccess || e2 != cudaSuccess)
-        return rt_fail(c, RT_ECUDA, "tile kernel attributes: %s",
-                       cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+    cudaError_t es[6] = {set_attrs_T<double, 2>(), set_attrs_T<double, 4>(), set_attrs_T<double, 8>(),
+                         set_attrs_T<float, 2>(),  set_attrs_T<float, 4>(),  set_attrs_T<float, 8>()};
+    for (cudaError_t e : es)
+        if (e != cudaSuccess) return rt_fail(c, RT_ECUDA, "tile kernel attributes: %s", cudaGetErrorString(e));
     return RT_OK;
 }
 

@@ -95,8 +95,8 @@ def test_fine_smoothers(pair, smoother):
     assert rel_err(G[0].getDisplacement(), uo) < 1e-10
 
 
-@pytest.mark.parametrize("variant,ty,zc", [(0, 4, 8), (1, 2, 4), (1, 4, 16), (1, 8, 7), (1, 4, 1), (2, 2, 8),
-                                           (2, 4, 3)])
+@pytest.mark.parametrize("variant,ty,zc", [(0, 4, 8), (0, 2, 5), (0, 8, 3), (1, 2, 4), (1, 4, 16), (1, 8, 7),
+                                           (1, 4, 1), (2, 2, 8), (2, 4, 3)])
 def test_fine_kernel_variants(pair, variant, ty, zc):
     """Every launch shape of the finest-level kernels (shared-memory tile, register marching,
     register marching with prefetched output-stage loads) gives the oracle's residual, K u,
