@@ -48,7 +48,7 @@ struct TileSmem {
 // blocks per SM the register budget is sized for
 template <typename T, int TY_>
 constexpr int tile_min_blocks() {
-    return sizeof(T) == 8 ? (TY_ == 2 ? 3 : TY_ == 4 ? 2 : 1) : (TY_ == 2 ? 8 : TY_ == 4 ? 4 : 2);
+    return sizeof(T) == 8 ? (TY_ == 2 ? 3 : TY_ == 4 ? 2 : 1) : (TY_ == 2 ? 8 : TY_ == 4 ? 5 : 2);
 }
 
 // MODE 0: r = f - K u (fixed rows: r = f)     MODE 1: out = K u (fixed rows: u)
