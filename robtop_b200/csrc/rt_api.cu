@@ -1275,13 +1275,23 @@ extern "C" int rt_relative_residual(rt_hier* h, double* rel) {
 // MG-preconditioned flexible CG on level 0: x = L0.u (initial guess), b = L0.f
 // scal slots: 10..13 r.z / rold.z (two parities), 20 p.q, 21 r.r, 22 b.b
 // ---------------------------------------------------------------------------
-static int precondition(rt_hier* h, const double* r, double* z, const double* rr_dev) {
+// z = B r (the V-cycle, plus the learned correction when attached).  When dots is given and the
+// form allows it, the FP32 path also leaves (z.r, z.rold) in dots[0..1] (fused with the widening
+// of z) and returns with *dots_done set.
+static int precondition(rt_hier* h, const double* r, double* z, const double* rr_dev, double* dots = nullptr,
+                        bool* dots_done = nullptr) {
     rt_level& L = h->L[0];
     const long n = 3 * L.nv;
+    if (dots_done) *dots_done = false;
     if (h->P.precision == RT_FP32) {
         RT_CHECK(rtk::d2f_scaled(h, n, r, L.f32, rr_dev));
         RT_CUDA(h->ctx, cudaMemsetAsync(L.u32, 0, sizeof(float) * n, h->ctx->stream));
         RT_CHECK(vcycle_T<float>(h, h->P.smoother, h->P.pre_sweeps, h->P.post_sweeps, h->P.jacobi_omega));
+        if (dots && !h->unet) {
+            RT_CHECK(rtk::f2d_scaled_dot2(h, n, L.u32, z, rr_dev, r, h->rold, dots));
+            *dots_done = true;
+            return RT_OK;
+        }
         RT_CHECK(rtk::f2d_scaled(h, n, L.u32, z, rr_dev));
     } else if (h->P.precision == RT_FP64_FINE && h->L.size() > 1) {
         // FP64 smoothing and residual on the finest level (on r / z themselves), the coarse
@@ -1373,17 +1383,18 @@ static int pcg_body(rt_hier* h, double* x, double* r, bool no_support, cudaGraph
     rt_level& L = h->L[0];
     const long n = 3 * L.nv;
     rt_ctx* c = h->ctx;
-    RT_CHECK(precondition(h, r, h->z, h->scal + 21));
+    bool dots_done = false;
+    // the projection of z (no supports) must precede its dots: no fusion then
+    RT_CHECK(precondition(h, r, h->z, h->scal + 21, no_support ? nullptr : h->scal + 10, &dots_done));
     if (no_support) RT_CHECK(rtk::displacement_project(h, h->z));
-    RT_CHECK(rtk::dot2(h, n, h->z, r, h->rold, h->scal + 10));
+    if (!dots_done) RT_CHECK(rtk::dot2(h, n, h->z, r, h->rold, h->scal + 10));
     RT_CHECK(rt_launch(c, "pcg_update_p", [&] {
         k_pcg_p_it<<<(unsigned)std::min<long>((n + 255) / 256, (long)c->sm_count * 16), 256, 0, c->stream>>>(
             n, h->scal + 10, h->scal + 24, h->p, h->z);
     }));
     RT_CHECK(rtk::fine_applyK<double>(h, h->p, h->q));
     RT_CHECK(rtk::dot(h, n, h->p, h->q, h->scal + 20));
-    RT_CHECK(rtk::pcg_update_xr(h, n, h->scal + 10, h->scal + 20, x, r, h->p, h->q, h->rold));
-    RT_CHECK(rtk::dot(h, n, r, r, h->scal + 21));
+    RT_CHECK(rtk::pcg_update_xr_rr(h, n, h->scal + 10, h->scal + 20, x, r, h->p, h->q, h->rold, h->scal + 21));
     return rt_launch(c, "pcg_tail", [&] { k_pcg_tail<<<1, 32, 0, c->stream>>>(h->scal, cond, use_cond); });
 }
 

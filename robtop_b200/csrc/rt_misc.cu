@@ -124,6 +124,40 @@ __global__ void k_pcg_xr(long n, const double* __restrict__ num, const double* _
     }
 }
 
+// k_pcg_xr and r.r of the updated r in the same pass (partials as k_dot's: same grid, same order)
+__global__ void __launch_bounds__(RB) k_pcg_xr_rr(long n, const double* __restrict__ num, const double* __restrict__ den,
+                                                  double* __restrict__ x, double* __restrict__ r,
+                                                  const double* __restrict__ p, const double* __restrict__ q,
+                                                  double* __restrict__ rold, double* __restrict__ partials) {
+    const double alpha = den[0] != 0.0 ? num[0] / den[0] : 0.0;
+    double v[1] = {0};
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const double ri = r[i];
+        rold[i] = ri;
+        x[i] += alpha * p[i];
+        const double rn = ri - alpha * q[i];
+        r[i] = rn;
+        v[0] += rn * rn;
+    }
+    block_reduce_store<1>(v, partials);
+}
+
+// z = a * sqrt(s) widened to FP64, with (z.r, z.rold) in the same pass (partials as k_dot2's)
+__global__ void __launch_bounds__(RB) k_f2d_scaled_dot2(long n, const float* __restrict__ a, double* __restrict__ z,
+                                                        const double* __restrict__ s, const double* __restrict__ r,
+                                                        const double* __restrict__ rold,
+                                                        double* __restrict__ partials) {
+    const double sc = sqrt(fmax(s[0], 1e-300));
+    double v[2] = {0, 0};
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const double x = (double)a[i] * sc;
+        z[i] = x;
+        v[0] += x * r[i];
+        v[1] += x * rold[i];
+    }
+    block_reduce_store<2>(v, partials);
+}
+
 // p = z + beta p with flexible beta = (r.z - rold.z) / rz_old; scalars: s[0]=r.z, s[1]=rold.z, den=rz_old
 __global__ void k_pcg_p(long n, const double* __restrict__ s, const double* __restrict__ den, double* __restrict__ p,
                         const double* __restrict__ z, int first) {
@@ -488,6 +522,22 @@ int pcg_update_xr(rt_hier* h, long n, const double* num, const double* den, doub
                   const double* q, double* rold) {
     return rt_launch(h->ctx, "pcg_update_xr",
                      [&] { k_pcg_xr<<<gridN(h->ctx, n), 256, 0, h->ctx->stream>>>(n, num, den, x, r, p, q, rold); });
+}
+
+int pcg_update_xr_rr(rt_hier* h, long n, const double* num, const double* den, double* x, double* r, const double* p,
+                     const double* q, double* rold, double* rr_out) {
+    RT_CHECK(rt_launch(h->ctx, "pcg_update_xr", [&] {
+        k_pcg_xr_rr<<<RT_RED_BLOCKS, RB, 0, h->ctx->stream>>>(n, num, den, x, r, p, q, rold, h->partials);
+    }));
+    return final_sum(h, 1, rr_out);
+}
+
+int f2d_scaled_dot2(rt_hier* h, long n, const float* a, double* z, const double* s, const double* r,
+                    const double* rold, double* out) {
+    RT_CHECK(rt_launch(h->ctx, "f2d_scaled", [&] {
+        k_f2d_scaled_dot2<<<RT_RED_BLOCKS, RB, 0, h->ctx->stream>>>(n, a, z, s, r, rold, h->partials);
+    }));
+    return final_sum(h, 2, out);
 }
 
 int pcg_update_p(rt_hier* h, long n, const double* s, const double* den, double* p, const double* z, bool first) {
