@@ -357,7 +357,7 @@ def run_kernel(args):
             rb._capi.check(rb.lib().rt_set_tuning(G.handle, prec, mode, variant, ty, zc), ctx.handle)
             names = ["residual", "applyK", "jacobi", "chebyshev"]
             shapes = {f"{names[mode]}_{'f32' if prec == rb.FP32 else 'f64'}":
-                      {"variant": ["smem_tile", "register_march", "register_march_prefetch"][variant], "rows": ty,
+                      {"variant": ["smem_tile", "register_march", "register_march_prefetch", "smem_tile_pipelined"][variant], "rows": ty,
                        "zchunk": zc}}
         else:
             shapes = G.autotune()
@@ -366,6 +366,27 @@ def run_kernel(args):
         rb._capi.check(rb.lib().rt_bench_fine_kernel(G.handle, prec, mode, args.steps, C.byref(us)), ctx.handle)
         key = {0: "residual", 1: "applyK", 3: "chebyshev"}[mode] + ("_f32" if prec == rb.FP32 else "_f64")
         print(json.dumps({"kernel": args.kernel, "us_per_call": us.value, "nodes": G[0].nv, "shape": shapes[key]}))
+        G.close()
+        ctx.close()
+        return 0
+    if args.kernel.startswith("st_") and args.kernel != "st_residual":
+        # one stencil-level kernel on level --level, timed by the library (CUDA events)
+        base, form = args.kernel.rsplit("_", 1)
+        prec = rb.FP64 if form == "f64" else rb.FP32
+        mode = {"st_residual": 0, "st_jacobi": 2, "st_cheby": 3}[base]
+        if form == "bf16":
+            p = G.params
+            p.coarse_bf16 = 1
+            G.set_params(p)
+            G.update_stencil()
+        us = C.c_double()
+        rb._capi.check(rb.lib().rt_bench_level_kernel(G.handle, args.level, prec, mode, args.warmup, C.byref(us)),
+                       ctx.handle)
+        rb._capi.check(rb.lib().rt_bench_level_kernel(G.handle, args.level, prec, mode, args.steps, C.byref(us)),
+                       ctx.handle)
+        print(json.dumps({"kernel": args.kernel, "level": args.level, "us_per_call": us.value,
+                          "nodes": G[args.level].nv, "stencil_bytes": G[args.level].nv * 243 * {"f64": 8, "f32": 4,
+                                                                                               "bf16": 2}[form]}))
         G.close()
         ctx.close()
         return 0
@@ -705,9 +726,12 @@ def main():
                     help="mixed: time only the mixed form (short command for launch-list captures)")
     ap.add_argument("--conv", default="16,16", help="--kernel conv3: input and output channels")
     ap.add_argument("--kernel", default=None, choices=["conv3", "fine_residual", "fine_jacobi", "st_residual",
-                                                      "fine_cheby_f32",
-                                                      "fine_residual_f64", "fine_applyK_f64", "fine_residual_f32"])
+                                                       "st_residual_f32", "st_residual_f64", "st_cheby_f32",
+                                                       "st_cheby_bf16", "st_cheby_f64", "st_jacobi_f32",
+                                                       "fine_cheby_f32", "fine_residual_f64", "fine_applyK_f64",
+                                                       "fine_residual_f32"])
     ap.add_argument("--size", default=None, help="kernel mode: grid NXxNYxNZ (default: the bench workload)")
+    ap.add_argument("--level", type=int, default=1, help="kernel mode, st_* kernels: the stencil level")
     ap.add_argument("--shape", default=None, help="kernel mode: launch shape variant,rows,zchunk (default: autotune)")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -89,6 +89,9 @@ typedef struct rt_params {
     int precision_fallback; /* N > 0: a PCG solve whose FP32 / FP64_FINE V-cycles stop reducing |r| (no halving
                                within N iterations; default 100) continues from its iterate with FP64 V-cycles;
                                0: off */
+    int coarse_bf16;        /* 1: the FP32 smoother on levels >= 1 reads the stencils stored in BF16 (half the
+                               bytes of the FP32 copy); residuals, restriction and the coarsest solve keep FP32 /
+                               FP64 stencils.  0 (default): FP32 stencils */
 } rt_params;
 
 typedef struct rt_solve_info {
@@ -215,13 +218,18 @@ int rt_compliance_noalloc(const double* f_dev, const double* u_dev, long long n,
 int rt_autotune(rt_hier* h, int reps);
 /* chosen shape of a finest-level kernel; mode 0 residual, 1 applyK, 2 Jacobi, 3 Chebyshev;
  * variant 0 shared-memory element tile (ty 2, 4 or 8 node rows), 1 register-marching element kernel, 2 register marching with
- * each layer's output-stage loads issued before its element arithmetic */
+ * each layer's output-stage loads issued before its element arithmetic, 3 shared-memory element tile software-pipelined
+ * over z (element layer z+1 and node layer z share one barrier interval; ty 2, 4 or 8) */
 int rt_tuning_info(rt_hier* h, int precision, int mode, int* variant, int* ty, int* zchunk, double* us);
-/* set a finest-level kernel's launch shape explicitly (ty: 2, 4 or 8 rows for variant 1, 2 or 4 for variant 2) */
+/* set a finest-level kernel's launch shape explicitly (ty: 2, 4 or 8 rows for variants 0, 1, 3; 2 or 4 for variant 2) */
 int rt_set_tuning(rt_hier* h, int precision, int mode, int variant, int ty, int zchunk);
 /* time reps launches of one finest-level kernel at its current shape on random data
  * (device time per launch in microseconds, CUDA events on the context stream) */
 int rt_bench_fine_kernel(rt_hier* h, int precision, int mode, int reps, double* us_per_launch);
+/* the same for one stencil level lvl (1 .. coarsest-1): mode 0 residual, 2 Jacobi, 3 Chebyshev step;
+ * precision RT_FP64 or RT_FP32 (FP32 smoothing reads the BF16 stencils when rt_params.coarse_bf16 is set).
+ * Overwrites the level's vectors; needs rt_update_stencil. */
+int rt_bench_level_kernel(rt_hier* h, int lvl, int precision, int mode, int reps, double* us_per_launch);
 
 /* ---- solvers -------------------------------------------------------------- */
 /* MG-preconditioned CG on level 0: u <- K^-1 f to ||r||/||f|| <= tol (solveFEM's role,

@@ -32,7 +32,7 @@ class Params(C.Structure):
         ("mode", C.c_int), ("skip_layer1", C.c_int), ("smoother", C.c_int), ("pre_sweeps", C.c_int),
         ("post_sweeps", C.c_int), ("jacobi_omega", C.c_double), ("precision", C.c_int),
         ("coarsest_elements", C.c_int), ("cycle_gamma", C.c_int), ("coarse_sweeps", C.c_int),
-        ("precision_fallback", C.c_int),
+        ("precision_fallback", C.c_int), ("coarse_bf16", C.c_int),
     ]
 
 
@@ -105,6 +105,7 @@ SIGNATURES = {
     "rt_tuning_info": (I, [P, I, I, C.POINTER(I), C.POINTER(I), C.POINTER(I), C.POINTER(D)]),
     "rt_set_tuning": (I, [P, I, I, I, I, I]),
     "rt_bench_fine_kernel": (I, [P, I, I, I, C.POINTER(D)]),
+    "rt_bench_level_kernel": (I, [P, I, I, I, I, C.POINTER(D)]),
     "rt_pcg": (I, [P, D, I, C.POINTER(SolveInfo)]),
     "rt_hier_precision_fallbacks": (C.c_longlong, [P]),
     "rt_worst_case": (I, [P, I, I, D, C.c_uint64, C.POINTER(D), C.POINTER(SolveInfo)]),

@@ -214,6 +214,7 @@ extern "C" void rt_params_default(rt_params* p) {
     p->cycle_gamma = 1;
     p->coarse_sweeps = 0;
     p->precision_fallback = 100;
+    p->coarse_bf16 = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -320,7 +321,7 @@ static void free_hier(rt_hier* h) {
     }
     for (auto& L : h->L) {
         cudaFree(L.vact); cudaFree(L.eact); cudaFree(L.u); cudaFree(L.f); cudaFree(L.r);
-        cudaFree(L.u32); cudaFree(L.f32); cudaFree(L.r32); cudaFree(L.st); cudaFree(L.st32);
+        cudaFree(L.u32); cudaFree(L.f32); cudaFree(L.r32); cudaFree(L.st); cudaFree(L.st32); cudaFree(L.st16);
         cudaFree(L.d); cudaFree(L.d32);
         cudaFree(L.aidx); cudaFree(L.ainv); cudaFree(L.dvec);
     }
@@ -347,7 +348,7 @@ static void ws_sync(rt_hier* w) {
     for (size_t i = 0; i < w->L.size(); i++) {
         rt_level& a = w->L[i];
         const rt_level& b = p->L[i];
-        a.vact = b.vact; a.eact = b.eact; a.st = b.st; a.st32 = b.st32;
+        a.vact = b.vact; a.eact = b.eact; a.st = b.st; a.st32 = b.st32; a.st16 = b.st16;
         a.na = b.na; a.aidx = b.aidx; a.ainv = b.ainv;
         a.n_act_nodes = b.n_act_nodes; a.n_act_elems = b.n_act_elems;
     }
@@ -457,7 +458,7 @@ static int build_hier(rt_ctx* c, const rt_params* p, int nx, int ny, int nz, uin
         RT_CUDA(c, cudaMemsetAsync(L.r, 0, sizeof(double) * 3 * L.nv, c->stream));
         if (k > 0) {
             RT_CHECK(dalloc(c, &L.st, 243 * L.nv));
-            RT_CHECK(dalloc(c, &L.st32, 243 * L.nv));
+            RT_CHECK(dalloc(c, &L.st32, 243 * (size_t)((L.nv + 31) / 32 * 32)));
             RT_CUDA(c, cudaMemsetAsync(L.st, 0, sizeof(double) * 243 * L.nv, c->stream));
         }
         std::vector<uint8_t> va(L.nv);
@@ -979,7 +980,9 @@ extern "C" int rt_update_stencil(rt_hier* h) {
     for (int i = 1; i < nl; i++) {
         if (i == 1) RT_CHECK(rtk::galerkin_from_elements(h));
         else RT_CHECK(rtk::galerkin_from_stencil(h, i));
-        RT_CHECK(rtk::d2f(h, 243 * h->L[i].nv, h->L[i].st, h->L[i].st32));
+        if (h->P.coarse_bf16 && !h->L[i].st16)
+            RT_CHECK(dalloc(h->ctx, &h->L[i].st16, 252 * (size_t)((h->L[i].nv + 31) / 32 * 32)));
+        RT_CHECK(rtk::stencil_copies(h, i));
     }
     RT_CHECK(rtk::coarsest_setup(h));
     // spectral bound of D^-1 A per smoothed level, for the Chebyshev smoother
@@ -1974,6 +1977,8 @@ extern "C" int rt_autotune(rt_hier* h, int reps) {
         for (int zc : {8, 16, 32}) cands.push_back(rt_tile_cfg{2, ty, zc});
     for (int ty : {2, 4, 8})
         for (int zc : {8, 16, 32}) cands.push_back(rt_tile_cfg{0, ty, zc});
+    for (int ty : {2, 4, 8})
+        for (int zc : {8, 16, 32, 64}) cands.push_back(rt_tile_cfg{3, ty, zc});
     for (int prec = 0; prec < 2; prec++)
         for (int mode = 0; mode < 4; mode++) {
             rt_tile_cfg best_cfg = h->tune[prec][mode];
@@ -2005,10 +2010,10 @@ extern "C" int rt_tuning_info(rt_hier* h, int precision, int mode, int* variant,
 }
 
 extern "C" int rt_set_tuning(rt_hier* h, int precision, int mode, int variant, int ty, int zchunk) {
-    if (!h || precision < 0 || precision > 1 || mode < 0 || mode > 3 || variant < 0 || variant > 2 || zchunk < 1)
+    if (!h || precision < 0 || precision > 1 || mode < 0 || mode > 3 || variant < 0 || variant > 3 || zchunk < 1)
         return RT_EINVAL;
     RT_NOT_WORKSPACE(h);
-    if (variant <= 1 && ty != 2 && ty != 4 && ty != 8) return rt_fail(h->ctx, RT_EINVAL, "rows per tile must be 2, 4 or 8");
+    if (variant != 2 && ty != 2 && ty != 4 && ty != 8) return rt_fail(h->ctx, RT_EINVAL, "rows per tile must be 2, 4 or 8");
     const int pr = precision == RT_FP64 ? 1 : 0;
     if (variant == 2 && ty != 2 && ty != 4) return rt_fail(h->ctx, RT_EINVAL, "prefetching rows per tile must be 2 or 4");
     h->tune[pr][mode] = rt_tile_cfg{variant, ty, zchunk};
@@ -2031,6 +2036,54 @@ extern "C" int rt_bench_fine_kernel(rt_hier* h, int precision, int mode, int rep
     const double t = time_fine_kernel(h, precision == RT_FP64 ? 1 : 0, mode, reps);
     if (t >= 1e30) return rt_fail(c, RT_ECUDA, "kernel launch failed");
     if (us_per_launch) *us_per_launch = t;
+    return RT_OK;
+}
+
+// one stencil-level kernel (residual, Jacobi or a Chebyshev step) on random inputs, timed with
+// CUDA events on the context stream; the level's own vectors are overwritten
+extern "C" int rt_bench_level_kernel(rt_hier* h, int lvl, int precision, int mode, int reps, double* us_per_launch) {
+    if (!h || lvl < 1 || lvl + 1 >= (int)h->L.size() || precision < RT_FP64 || precision > RT_FP32 || mode < 0 ||
+        mode > 3 || mode == 1 || reps < 1)
+        return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
+    RT_CHECK(need_stencil(h));
+    rt_ctx* c = h->ctx;
+    rt_level& L = h->L[lvl];
+    const long n = 3 * L.nv;
+    RT_CHECK(rtk::rng_uniform(h, 0xbe7e, n, L.u));
+    RT_CHECK(rtk::rng_uniform(h, 0xbe7f, n, L.f));
+    RT_CHECK(rtk::d2f(h, n, L.u, L.u32));
+    RT_CHECK(rtk::d2f(h, n, L.f, L.f32));
+    const double* coef = cheby_table(h, lvl);
+    auto run = [&]() -> int {
+        if (precision == RT_FP64) {
+            switch (mode) {
+                case 0: return rtk::st_residual<double>(h, lvl, L.u, L.f, L.r);
+                case 2: return rtk::st_jacobi<double>(h, lvl, L.u, L.f, L.r, 0.6);
+                default: return rtk::st_cheby<double>(h, lvl, L.u, L.f, L.r, L.d, coef, 1);
+            }
+        }
+        switch (mode) {
+            case 0: return rtk::st_residual<float>(h, lvl, L.u32, L.f32, L.r32);
+            case 2: return rtk::st_jacobi<float>(h, lvl, L.u32, L.f32, L.r32, 0.6);
+            default: return rtk::st_cheby<float>(h, lvl, L.u32, L.f32, L.r32, L.d32, coef, 1);
+        }
+    };
+    RT_CHECK(run());
+    cudaEvent_t a, b;
+    RT_CUDA(c, cudaEventCreate(&a));
+    RT_CUDA(c, cudaEventCreate(&b));
+    cudaEventRecord(a, c->stream);
+    int st = RT_OK;
+    for (int i = 0; i < reps && st == RT_OK; i++) st = run();
+    cudaEventRecord(b, c->stream);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    RT_CHECK(st);
+    if (us_per_launch) *us_per_launch = ms * 1e3 / reps;
     return RT_OK;
 }
 
@@ -2179,6 +2232,7 @@ static uint64_t batch_key(rt_hier* const* hs, int n, double tol, int maxit) {
         mix((uint64_t)h->P.precision | ((uint64_t)h->P.smoother << 4) | ((uint64_t)h->P.pre_sweeps << 8) |
             ((uint64_t)h->P.post_sweeps << 16) | ((uint64_t)h->P.mode << 24) | ((uint64_t)h->P.cycle_gamma << 32) |
             ((uint64_t)h->P.coarse_sweeps << 40) | ((uint64_t)h->P.precision_fallback << 48));
+        mix((uint64_t)h->P.coarse_bf16);
         uint64_t om;
         memcpy(&om, &h->P.jacobi_omega, 8);
         mix(om);

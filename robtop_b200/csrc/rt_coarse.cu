@@ -10,6 +10,7 @@
 // Stencils are [27*9][nv]: entry (k*9 + 3*row + col)*nv + v couples node v to
 // neighbour v + d(k), d(k) = (k%3-1, k/3%3-1, k/9-1) — the reference's
 // GraftArray<double,27,9> layout over a dense node box.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include "rt_internal.h"
@@ -24,11 +25,45 @@ unsigned grid_for(rt_ctx* c, long n, int bs) {
     return (unsigned)(b < cap ? b : cap);
 }
 
-template <typename T, bool SKIPSELF>
+// ---------------------------------------------------------------------------
+// Stencil storage.  The assembled FP64 operator is row-major, row j = 9 k + 3 r + c
+// (neighbour k, block row r, column c) of all nodes: [243][nv].  The FP32 and BF16
+// copies the smoothers read are blocked by 32 nodes, [nv/32][RS][32]: the rows of 32
+// neighbouring nodes form one contiguous run (31 KB in FP32), so the loads of a warp
+// stay in one or two DRAM pages and TLB entries instead of touching 243 rows nv apart.
+// The BF16 copy has 9 more rows (RS = 252): the centre block is stored as hi + lo
+// BF16 pairs, and is shifted by the rounding error of the 26 off-centre blocks, so
+// the row sums of every 3x3 block row (the operator applied to the three rigid
+// translations) equal the FP64 operator's to ~2^-17 instead of ~2^-9.
+// ---------------------------------------------------------------------------
+template <typename S>
+struct StAddr {
+    static constexpr bool BLK = sizeof(S) < 8;
+    static constexpr int RS = sizeof(S) == 2 ? 252 : 243;
+    __device__ __forceinline__ static long base(long v) { return BLK ? (v >> 5) * (RS * 32L) + (v & 31) : v; }
+    __device__ __forceinline__ static long stride(long nv) { return BLK ? 32 : nv; }
+};
+
+// a stencil entry in the compute type: FP64 / FP32 as stored, BF16 bit patterns widened exactly
+template <typename T>
+__device__ __forceinline__ T st_val(const T* p) { return *p; }
+__device__ __forceinline__ float st_val(const uint16_t* p) { return __uint_as_float((uint32_t)*p << 16); }
+
+// entry (block row r, column c) of the centre block; sb = st + StAddr::base(v)
+template <typename T, typename S>
+__device__ __forceinline__ T st_centre(const S* sb, long rs, int rc) {
+    T x = (T)st_val(sb + (117 + rc) * rs);
+    if (sizeof(S) == 2) x += (T)st_val(sb + (243 + rc) * rs);
+    return x;
+}
+
+// sum over the 27 neighbours of A_vk u_k (SKIPSELF: without the centre block)
+template <typename T, typename S, bool SKIPSELF>
 __device__ __forceinline__ void st_node_sum(int x, int y, int z, int vx, int vy, int vz, long nv,
-                                            const uint8_t* __restrict__ vact, const T* __restrict__ st,
-                                            const T* __restrict__ u, long v, T Au[3]) {
+                                            const S* __restrict__ st, const T* __restrict__ u, long v, T Au[3]) {
     Au[0] = Au[1] = Au[2] = T(0);
+    const long rs = StAddr<S>::stride(nv);
+    const S* sb = st + StAddr<S>::base(v);
 #pragma unroll
     for (int k = 0; k < 27; k++) {
         if (SKIPSELF && k == 13) continue;
@@ -36,25 +71,17 @@ __device__ __forceinline__ void st_node_sum(int x, int y, int z, int vx, int vy,
         if (jx < 0 || jy < 0 || jz < 0 || jx >= vx || jy >= vy || jz >= vz) continue;
         const long nj = jx + (long)vx * (jy + (long)vy * jz);
         const T u0 = u[nj], u1 = u[nv + nj], u2 = u[2 * nv + nj];
-        const T* s = st + (long)(k * 9) * nv + v;
 #pragma unroll
-        for (int r = 0; r < 3; r++) Au[r] += s[(3 * r) * nv] * u0 + s[(3 * r + 1) * nv] * u1 + s[(3 * r + 2) * nv] * u2;
-    }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(ST_BS) k_st_residual(int nx, int ny, int nz, const uint8_t* __restrict__ vact,
-                                                        const T* __restrict__ st, const T* __restrict__ u,
-                                                        const T* __restrict__ f, T* __restrict__ r) {
-    const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
-    const long nv = (long)vx * vy * vz;
-    for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < nv; v += (long)gridDim.x * blockDim.x) {
-        const int x = (int)(v % vx), y = (int)((v / vx) % vy), z = (int)(v / ((long)vx * vy));
-        T Au[3] = {T(0), T(0), T(0)};
-        const bool act = vact[v];
-        if (act) st_node_sum<T, false>(x, y, z, vx, vy, vz, nv, vact, st, u, v, Au);
-#pragma unroll
-        for (int c = 0; c < 3; c++) r[c * nv + v] = act ? f[c * nv + v] - Au[c] : T(0);
+        for (int r = 0; r < 3; r++) {
+            T a0, a1, a2;
+            if (k == 13) {
+                a0 = st_centre<T>(sb, rs, 3 * r); a1 = st_centre<T>(sb, rs, 3 * r + 1); a2 = st_centre<T>(sb, rs, 3 * r + 2);
+            } else {
+                const S* s = sb + (long)(k * 9 + 3 * r) * rs;
+                a0 = (T)st_val(s); a1 = (T)st_val(s + rs); a2 = (T)st_val(s + 2 * rs);
+            }
+            Au[r] += a0 * u0 + a1 * u1 + a2 * u2;
+        }
     }
 }
 
@@ -64,6 +91,7 @@ __global__ void __launch_bounds__(ST_BS) k_st_gs(int nx, int ny, int nz, int col
                                                   T* __restrict__ u, const T* __restrict__ f) {
     const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
     const long nv = (long)vx * vy * vz;
+    const long rs = StAddr<T>::stride(nv);
     const int px = color & 1, py = (color >> 1) & 1, pz = (color >> 2) & 1;
     const int cx = (vx - px + 1) / 2, cy = (vy - py + 1) / 2, cz = (vz - pz + 1) / 2;
     const long nc = (long)cx * cy * cz;
@@ -72,10 +100,11 @@ __global__ void __launch_bounds__(ST_BS) k_st_gs(int nx, int ny, int nz, int col
         const long v = x + (long)vx * (y + (long)vy * z);
         if (!vact[v]) continue;
         T Au[3];
-        st_node_sum<T, true>(x, y, z, vx, vy, vz, nv, vact, st, u, v, Au);
+        st_node_sum<T, T, true>(x, y, z, vx, vy, vz, nv, st, u, v, Au);
         T S[9];
+        const T* sb = st + StAddr<T>::base(v);
 #pragma unroll
-        for (int i = 0; i < 9; i++) S[i] = st[(long)(13 * 9 + i) * nv + v];
+        for (int i = 0; i < 9; i++) S[i] = st_centre<T>(sb, rs, i);
         const T F[3] = {f[v], f[nv + v], f[2 * nv + v]};
         T uu[3] = {u[v], u[nv + v], u[2 * nv + v]};
         if (!backward) {
@@ -91,40 +120,6 @@ __global__ void __launch_bounds__(ST_BS) k_st_gs(int nx, int ny, int nz, int col
     }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(ST_BS) k_st_jacobi(int nx, int ny, int nz, T omega,
-                                                      const uint8_t* __restrict__ vact, const T* __restrict__ st,
-                                                      const T* __restrict__ u, const T* __restrict__ f,
-                                                      T* __restrict__ unew) {
-    const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
-    const long nv = (long)vx * vy * vz;
-    for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < nv; v += (long)gridDim.x * blockDim.x) {
-        const int x = (int)(v % vx), y = (int)((v / vx) % vy), z = (int)(v / ((long)vx * vy));
-        T nu[3] = {T(0), T(0), T(0)};
-        if (vact[v]) {
-            T Au[3];
-            st_node_sum<T, false>(x, y, z, vx, vy, vz, nv, vact, st, u, v, Au);
-            T S[9], I[9];
-#pragma unroll
-            for (int i = 0; i < 9; i++) S[i] = st[(long)(13 * 9 + i) * nv + v];
-            const T a = S[0], b = S[1], c = S[2], d = S[3], e = S[4], ff = S[5], g = S[6], hh = S[7], k = S[8];
-            const T A = e * k - ff * hh, B = -(d * k - ff * g), Cc = d * hh - e * g;
-            const T id = T(1) / (a * A + b * B + c * Cc);
-            I[0] = A * id; I[1] = -(b * k - c * hh) * id; I[2] = (b * ff - c * e) * id;
-            I[3] = B * id; I[4] = (a * k - c * g) * id; I[5] = -(a * ff - c * d) * id;
-            I[6] = Cc * id; I[7] = -(a * hh - b * g) * id; I[8] = (a * e - b * d) * id;
-            T rr[3];
-#pragma unroll
-            for (int q = 0; q < 3; q++) rr[q] = f[q * nv + v] - Au[q];
-#pragma unroll
-            for (int q = 0; q < 3; q++)
-                nu[q] = u[q * nv + v] + omega * (I[q * 3] * rr[0] + I[q * 3 + 1] * rr[1] + I[q * 3 + 2] * rr[2]);
-        }
-#pragma unroll
-        for (int q = 0; q < 3; q++) unew[q * nv + v] = nu[q];
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Lane-split stencil kernels: 4 lanes per node, lane q sums neighbours
 // k = q, q+4, ..., then the three row sums are combined with shuffles.  Coarse
@@ -132,9 +127,9 @@ __global__ void __launch_bounds__(ST_BS) k_st_jacobi(int nx, int ny, int nz, T o
 // a thread per node leaves most of the GPU idle on long dependent load chains.
 // MODE 0: r = f - A u;  MODE 2: Jacobi;  MODE 3: Chebyshev step.
 // ---------------------------------------------------------------------------
-template <typename T, int MODE>
-__global__ void __launch_bounds__(ST_BS) k_st_split4(int nx, int ny, int nz, const uint8_t* __restrict__ vact,
-                                                      const T* __restrict__ st, const T* __restrict__ u,
+template <typename T, int MODE, typename S = T>
+__global__ void __launch_bounds__(ST_BS, sizeof(T) == 8 ? 1 : 3) k_st_split4(int nx, int ny, int nz, const uint8_t* __restrict__ vact,
+                                                      const S* __restrict__ st, const T* __restrict__ u,
                                                       const T* __restrict__ f, T* __restrict__ out,
                                                       T* __restrict__ d, T omega, const double* __restrict__ coef,
                                                       int kstep) {
@@ -146,6 +141,7 @@ __global__ void __launch_bounds__(ST_BS) k_st_split4(int nx, int ny, int nz, con
     }
     const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
     const long nv = (long)vx * vy * vz;
+    const long rs = StAddr<S>::stride(nv);
     const int q = threadIdx.x & 3;
     const long ngroups = (long)gridDim.x * (blockDim.x >> 2);
     // every lane runs the same number of trips (the shuffles below use the full mask)
@@ -153,6 +149,7 @@ __global__ void __launch_bounds__(ST_BS) k_st_split4(int nx, int ny, int nz, con
     for (long v = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 2; v < vend; v += ngroups) {
         const bool inb = v < nv;
         const bool act = inb && vact[v];
+        const S* sb = st + StAddr<S>::base(inb ? v : 0);
         T Au[3] = {T(0), T(0), T(0)};
         if (act) {
             const int x = (int)(v % vx), y = (int)((v / vx) % vy), z = (int)(v / ((long)vx * vy));
@@ -164,10 +161,18 @@ __global__ void __launch_bounds__(ST_BS) k_st_split4(int nx, int ny, int nz, con
                 if (jx < 0 || jy < 0 || jz < 0 || jx >= vx || jy >= vy || jz >= vz) continue;
                 const long nj = jx + (long)vx * (jy + (long)vy * jz);
                 const T u0 = u[nj], u1 = u[nv + nj], u2 = u[2 * nv + nj];
-                const T* s = st + (long)(k * 9) * nv + v;
+                const S* s = sb + (long)(k * 9) * rs;
 #pragma unroll
-                for (int r = 0; r < 3; r++)
-                    Au[r] += s[(3 * r) * nv] * u0 + s[(3 * r + 1) * nv] * u1 + s[(3 * r + 2) * nv] * u2;
+                for (int r = 0; r < 3; r++) {
+                    T a0 = (T)st_val(s + (3 * r) * rs), a1 = (T)st_val(s + (3 * r + 1) * rs),
+                      a2 = (T)st_val(s + (3 * r + 2) * rs);
+                    if (sizeof(S) == 2 && k == 13) {  // low parts of the BF16 centre block
+                        a0 += (T)st_val(sb + (243 + 3 * r) * rs);
+                        a1 += (T)st_val(sb + (243 + 3 * r + 1) * rs);
+                        a2 += (T)st_val(sb + (243 + 3 * r + 2) * rs);
+                    }
+                    Au[r] += a0 * u0 + a1 * u1 + a2 * u2;
+                }
             }
         }
 #pragma unroll
@@ -184,17 +189,19 @@ __global__ void __launch_bounds__(ST_BS) k_st_split4(int nx, int ny, int nz, con
         }
         T res = T(0), dn = T(0);
         if (act) {
-            T S[9], I[9];
+            T S9[9];
 #pragma unroll
-            for (int i = 0; i < 9; i++) S[i] = st[(long)(13 * 9 + i) * nv + v];
-            const T a0 = S[0], b0 = S[1], c0 = S[2], d0 = S[3], e0 = S[4], f0 = S[5], g0 = S[6], h0 = S[7], k0 = S[8];
+            for (int i = 0; i < 9; i++) S9[i] = st_centre<T>(sb, rs, i);
+            const T a0 = S9[0], b0 = S9[1], c0 = S9[2], d0 = S9[3], e0 = S9[4], f0 = S9[5], g0 = S9[6], h0 = S9[7],
+                    k0 = S9[8];
             const T A = e0 * k0 - f0 * h0, B = -(d0 * k0 - f0 * g0), Cc = d0 * h0 - e0 * g0;
             const T id = T(1) / (a0 * A + b0 * B + c0 * Cc);
-            I[0] = A * id; I[1] = -(b0 * k0 - c0 * h0) * id; I[2] = (b0 * f0 - c0 * e0) * id;
-            I[3] = B * id; I[4] = (a0 * k0 - c0 * g0) * id; I[5] = -(a0 * f0 - c0 * d0) * id;
-            I[6] = Cc * id; I[7] = -(a0 * h0 - b0 * g0) * id; I[8] = (a0 * e0 - b0 * d0) * id;
+            // row q of the inverse (adjugate / determinant)
+            const T i0 = q == 0 ? A : (q == 1 ? B : Cc);
+            const T i1 = q == 0 ? -(b0 * k0 - c0 * h0) : (q == 1 ? (a0 * k0 - c0 * g0) : -(a0 * h0 - b0 * g0));
+            const T i2 = q == 0 ? (b0 * f0 - c0 * e0) : (q == 1 ? -(a0 * f0 - c0 * d0) : (a0 * e0 - b0 * d0));
             const T r0 = f[v] - Au[0], r1 = f[nv + v] - Au[1], r2 = f[2 * nv + v] - Au[2];
-            const T zq = I[q * 3] * r0 + I[q * 3 + 1] * r1 + I[q * 3 + 2] * r2;
+            const T zq = (i0 * id) * r0 + (i1 * id) * r1 + (i2 * id) * r2;
             if (MODE == 2) {
                 res = u[oq] + omega * zq;
             } else {
@@ -204,6 +211,47 @@ __global__ void __launch_bounds__(ST_BS) k_st_split4(int nx, int ny, int nz, con
         }
         out[oq] = res;
         if (MODE == 3) d[oq] = dn;
+    }
+}
+
+// smoother copies of level stencils (layout above); one thread per (node, row group)
+__global__ void k_st_to_f32(long nv, long nvpad, const double* __restrict__ st, float* __restrict__ out) {
+    const long n = nvpad * 243;
+    for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < n; o += (long)gridDim.x * blockDim.x) {
+        const long blk = o / (243 * 32);
+        const int j = (int)((o / 32) % 243), l = (int)(o & 31);
+        const long v = blk * 32 + l;
+        out[o] = v < nv ? (float)st[(long)j * nv + v] : 0.f;
+    }
+}
+
+__device__ __forceinline__ uint16_t bf16_bits(double x) { return __bfloat16_as_ushort(__double2bfloat16(x)); }
+
+// thread per (node, centre entry rc): the 26 off-centre entries of column rc are rounded, the
+// centre entry takes their summed rounding error, stored as hi + lo
+__global__ void k_st_to_bf16(long nv, long nvpad, const double* __restrict__ st, uint16_t* __restrict__ out) {
+    const long n = nvpad * 9;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+        const long v = t % nvpad;
+        const int rc = (int)(t / nvpad);
+        uint16_t* ob = out + (v >> 5) * (252 * 32L) + (v & 31);
+        if (v >= nv) {
+            for (int k = 0; k < 27; k++) ob[(k * 9 + rc) * 32] = 0;
+            ob[(243 + rc) * 32] = 0;
+            continue;
+        }
+        double err = 0;
+        for (int k = 0; k < 27; k++) {
+            if (k == 13) continue;
+            const double x = st[(long)(k * 9 + rc) * nv + v];
+            const uint16_t b = bf16_bits(x);
+            ob[(k * 9 + rc) * 32] = b;
+            err += x - (double)__uint_as_float((uint32_t)b << 16);
+        }
+        const double c = st[(long)(117 + rc) * nv + v] + err;
+        const uint16_t hi = bf16_bits(c);
+        ob[(117 + rc) * 32] = hi;
+        ob[(243 + rc) * 32] = bf16_bits(c - (double)__uint_as_float((uint32_t)hi << 16));
     }
 }
 
@@ -255,48 +303,6 @@ __global__ void __launch_bounds__(ST_BS) k_restrict4_split8(int fnx, int fny, in
     }
 }
 
-// Chebyshev step on an assembled-stencil level (coefficients a_k, b_k from the level's table, see rt_cheby_coef)
-template <typename T>
-__global__ void __launch_bounds__(ST_BS) k_st_cheby(int nx, int ny, int nz, const uint8_t* __restrict__ vact,
-                                                     const T* __restrict__ st, const T* __restrict__ u,
-                                                     const T* __restrict__ f, T* __restrict__ unew,
-                                                     T* __restrict__ d, const double* __restrict__ coef, int kstep) {
-    const double ca = coef[2 * kstep], cb = coef[2 * kstep + 1];
-    const T a = (T)ca, b = (T)cb;
-    const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
-    const long nv = (long)vx * vy * vz;
-    for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < nv; v += (long)gridDim.x * blockDim.x) {
-        const int x = (int)(v % vx), y = (int)((v / vx) % vy), z = (int)(v / ((long)vx * vy));
-        T nu[3] = {T(0), T(0), T(0)}, dn[3] = {T(0), T(0), T(0)};
-        if (vact[v]) {
-            T Au[3];
-            st_node_sum<T, false>(x, y, z, vx, vy, vz, nv, vact, st, u, v, Au);
-            T S[9], I[9];
-#pragma unroll
-            for (int i = 0; i < 9; i++) S[i] = st[(long)(13 * 9 + i) * nv + v];
-            const T a0 = S[0], b0 = S[1], c0 = S[2], d0 = S[3], e0 = S[4], f0 = S[5], g0 = S[6], h0 = S[7], k0 = S[8];
-            const T A = e0 * k0 - f0 * h0, B = -(d0 * k0 - f0 * g0), Cc = d0 * h0 - e0 * g0;
-            const T id = T(1) / (a0 * A + b0 * B + c0 * Cc);
-            I[0] = A * id; I[1] = -(b0 * k0 - c0 * h0) * id; I[2] = (b0 * f0 - c0 * e0) * id;
-            I[3] = B * id; I[4] = (a0 * k0 - c0 * g0) * id; I[5] = -(a0 * f0 - c0 * d0) * id;
-            I[6] = Cc * id; I[7] = -(a0 * h0 - b0 * g0) * id; I[8] = (a0 * e0 - b0 * d0) * id;
-            T rr[3];
-#pragma unroll
-            for (int q = 0; q < 3; q++) rr[q] = f[q * nv + v] - Au[q];
-#pragma unroll
-            for (int q = 0; q < 3; q++) {
-                const T zq = I[q * 3] * rr[0] + I[q * 3 + 1] * rr[1] + I[q * 3 + 2] * rr[2];
-                dn[q] = (kstep == 0 ? T(0) : a * d[q * nv + v]) + b * zq;
-                nu[q] = u[q * nv + v] + dn[q];
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 3; q++) {
-            unew[q * nv + v] = nu[q];
-            d[q * nv + v] = dn[q];
-        }
-    }
-}
 
 // f_c(X) = sum_{|d| < r} prod (r - |d|)/r * r_f(rX + d)
 template <typename T, int R>
@@ -552,9 +558,15 @@ __global__ void k_d2f(long n, const double* __restrict__ a, float* __restrict__ 
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) b[i] = (float)a[i];
 }
 
+
 }  // namespace
 
 namespace rtk {
+
+// stencil kernels on level 1 (the ratio-4 level, by far the largest) report under their own
+// name, so a profile separates them from the small levels below
+#define LVL_NAME(lvl, f64, base) \
+    ((lvl) == 1 ? ((f64) ? base "_f64_l1" : base "_f32_l1") : ((f64) ? base "_f64" : base "_f32"))
 
 template <typename T>
 static const T* stp(rt_level& L);
@@ -566,7 +578,7 @@ const float* stp<float>(rt_level& L) { return L.st32; }
 template <typename T>
 int st_residual(rt_hier* h, int lvl, const T* u, const T* f, T* r) {
     rt_level& L = h->L[lvl];
-    return rt_launch(h->ctx, sizeof(T) == 8 ? "st_residual_f64" : "st_residual_f32", [&] {
+    return rt_launch(h->ctx, LVL_NAME(lvl, sizeof(T) == 8, "st_residual"), [&] {
         k_st_split4<T, 0><<<grid_for(h->ctx, 4 * L.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(
             L.nx, L.ny, L.nz, L.vact, stp<T>(L), u, f, r, nullptr, T(0), nullptr, 0);
     });
@@ -579,7 +591,7 @@ int st_gs(rt_hier* h, int lvl, T* u, const T* f, bool backward) {
         int col = backward ? 7 - cc : cc;
         long ncol = (long)((L.vx - (col & 1) + 1) / 2) * ((L.vy - ((col >> 1) & 1) + 1) / 2) *
                     ((L.vz - ((col >> 2) & 1) + 1) / 2);
-        RT_CHECK(rt_launch(h->ctx, sizeof(T) == 8 ? "st_gs_f64" : "st_gs_f32", [&] {
+        RT_CHECK(rt_launch(h->ctx, LVL_NAME(lvl, sizeof(T) == 8, "st_gs"), [&] {
             k_st_gs<T><<<grid_for(h->ctx, ncol, ST_BS), ST_BS, 0, h->ctx->stream>>>(L.nx, L.ny, L.nz, col, backward,
                                                                                     L.vact, stp<T>(L), u, f);
         }));
@@ -587,10 +599,22 @@ int st_gs(rt_hier* h, int lvl, T* u, const T* f, bool backward) {
     return RT_OK;
 }
 
+// the FP32 smoother reads the BF16 stencil copy when rt_params.coarse_bf16 is set
+template <typename T>
+static bool use_bf16(rt_hier* h, rt_level& L) {
+    return sizeof(T) == 4 && h->P.coarse_bf16 && L.st16;
+}
+
 template <typename T>
 int st_jacobi(rt_hier* h, int lvl, const T* u, const T* f, T* unew, double omega) {
     rt_level& L = h->L[lvl];
-    return rt_launch(h->ctx, sizeof(T) == 8 ? "st_jacobi_f64" : "st_jacobi_f32", [&] {
+    if constexpr (sizeof(T) == 4)
+        if (use_bf16<T>(h, L))
+            return rt_launch(h->ctx, lvl == 1 ? "st_jacobi_bf16_l1" : "st_jacobi_bf16", [&] {
+                k_st_split4<T, 2, uint16_t><<<grid_for(h->ctx, 4 * L.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(
+                    L.nx, L.ny, L.nz, L.vact, L.st16, u, f, unew, nullptr, (T)omega, nullptr, 0);
+            });
+    return rt_launch(h->ctx, LVL_NAME(lvl, sizeof(T) == 8, "st_jacobi"), [&] {
         k_st_split4<T, 2><<<grid_for(h->ctx, 4 * L.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(
             L.nx, L.ny, L.nz, L.vact, stp<T>(L), u, f, unew, nullptr, (T)omega, nullptr, 0);
     });
@@ -599,7 +623,13 @@ int st_jacobi(rt_hier* h, int lvl, const T* u, const T* f, T* unew, double omega
 template <typename T>
 int st_cheby(rt_hier* h, int lvl, const T* u, const T* f, T* unew, T* d, const double* coef, int kstep) {
     rt_level& L = h->L[lvl];
-    return rt_launch(h->ctx, sizeof(T) == 8 ? "st_cheby_f64" : "st_cheby_f32", [&] {
+    if constexpr (sizeof(T) == 4)
+        if (use_bf16<T>(h, L))
+            return rt_launch(h->ctx, lvl == 1 ? "st_cheby_bf16_l1" : "st_cheby_bf16", [&] {
+                k_st_split4<T, 3, uint16_t><<<grid_for(h->ctx, 4 * L.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(
+                    L.nx, L.ny, L.nz, L.vact, L.st16, u, f, unew, d, T(0), coef, kstep);
+            });
+    return rt_launch(h->ctx, LVL_NAME(lvl, sizeof(T) == 8, "st_cheby"), [&] {
         k_st_split4<T, 3><<<grid_for(h->ctx, 4 * L.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(
             L.nx, L.ny, L.nz, L.vact, stp<T>(L), u, f, unew, d, T(0), coef, kstep);
     });
@@ -711,6 +741,19 @@ int galerkin_from_stencil(rt_hier* h, int lvl) {
 
 int d2f(rt_hier* h, long n, const double* a, float* b) {
     return rt_launch(h->ctx, "d2f", [&] { k_d2f<<<grid_for(h->ctx, n, 256), 256, 0, h->ctx->stream>>>(n, a, b); });
+}
+
+// the FP32 (and, with rt_params.coarse_bf16, BF16) smoother copies of level lvl's stencils
+int stencil_copies(rt_hier* h, int lvl) {
+    rt_level& L = h->L[lvl];
+    const long nvpad = (L.nv + 31) / 32 * 32;
+    RT_CHECK(rt_launch(h->ctx, "stencil_f32", [&] {
+        k_st_to_f32<<<grid_for(h->ctx, nvpad * 243, 256), 256, 0, h->ctx->stream>>>(L.nv, nvpad, L.st, L.st32);
+    }));
+    if (!h->P.coarse_bf16) return RT_OK;
+    return rt_launch(h->ctx, "stencil_bf16", [&] {
+        k_st_to_bf16<<<grid_for(h->ctx, nvpad * 9, 256), 256, 0, h->ctx->stream>>>(L.nv, nvpad, L.st, L.st16);
+    });
 }
 
 template int st_residual<double>(rt_hier*, int, const double*, const double*, double*);

@@ -51,6 +51,65 @@ constexpr int tile_min_blocks() {
     return sizeof(T) == 8 ? (TY_ == 2 ? 3 : TY_ == 4 ? 2 : 1) : (TY_ == 2 ? 8 : TY_ == 4 ? 5 : 2);
 }
 
+// smoothing update of one node (MODE 2: damped block Jacobi, MODE 3: Chebyshev step) from its
+// accumulated K u (acc), f, u and the Chebyshev direction; wz0 / wz1 are the element-weight rows of the
+// element layers below / above the node, el the row index of its (-x, -y) element.  The 3x3 diagonal
+// block of K at the node is sum_e w_e KE_vv, KE_vv = a I + b (s s^T - I) with s the node's vertex signs.
+template <typename T, int MODE, int EXT>
+__device__ __forceinline__ void node_smooth(const rte::KtVals<T>& kt, const float* wz0, const float* wz1, int el,
+                                            const T (&acc)[3], const T (&fv)[3], const T (&uo)[3],
+                                            const T (&dv)[3], bool act, bool fixed, T omega, T cheb_a, T cheb_b,
+                                            int kstep, T (&nu)[3], T (&dn)[3]) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) nu[c] = dn[c] = T(0);
+    if (!act) return;
+    T sw = T(0), sxy = T(0), sxz = T(0), syz = T(0);
+    int ne = 0;
+#pragma unroll
+    for (int dz = 0; dz < 2; dz++)
+#pragma unroll
+        for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+            for (int dx = 0; dx < 2; dx++) {
+                const float wv = (dz ? wz1 : wz0)[el + dy * EXT + dx];
+                if (wv != 0.f) ne++;
+                // node's vertex bits in that element: (1-dx, 1-dy, 1-dz)
+                const T sx = dx ? T(1) : T(-1), sy = dy ? T(1) : T(-1), sz = dz ? T(1) : T(-1);
+                sw += T(wv);
+                sxy += T(wv) * sx * sy;
+                sxz += T(wv) * sx * sz;
+                syz += T(wv) * sy * sz;
+            }
+    if (fixed) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) nu[c] = fv[c] / T(ne);
+        return;
+    }
+    const T A = kt.diag_a * sw, bxy = kt.diag_b * sxy, bxz = kt.diag_b * sxz, byz = kt.diag_b * syz;
+    // inverse of [[A,bxy,bxz],[bxy,A,byz],[bxz,byz,A]]
+    const T c00 = A * A - byz * byz, c01 = -(bxy * A - byz * bxz), c02 = bxy * byz - A * bxz;
+    const T c11 = A * A - bxz * bxz, c12 = -(A * byz - bxy * bxz), c22 = A * A - bxy * bxy;
+    const T id = T(1) / (A * c00 + bxy * c01 + bxz * c02);
+    T rr[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) rr[c] = fv[c] - acc[c];
+    T zz[3];
+    zz[0] = id * (c00 * rr[0] + c01 * rr[1] + c02 * rr[2]);
+    zz[1] = id * (c01 * rr[0] + c11 * rr[1] + c12 * rr[2]);
+    zz[2] = id * (c02 * rr[0] + c12 * rr[1] + c22 * rr[2]);
+    if (MODE == 2) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) nu[c] = uo[c] + omega * zz[c];
+    } else {
+        // Chebyshev step: d = ca d + cb D^-1 r, u += d
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            dn[c] = (kstep == 0 ? T(0) : cheb_a * dv[c]) + cheb_b * zz[c];
+            nu[c] = uo[c] + dn[c];
+        }
+    }
+}
+
 // MODE 0: r = f - K u (fixed rows: r = f)     MODE 1: out = K u (fixed rows: u)
 // MODE 2: unew = u + omega D^-1 (f - K u) (fixed: f / n_e)
 // MODE 3: Chebyshev step kstep: d = a_k d + b_k D^-1 (f - K u), unew = u + d (fixed: f / n_e)
@@ -226,57 +285,9 @@ __global__ void __launch_bounds__(Tile<TY_>::BS, tile_min_blocks<T, TY_>()) k_fi
 #pragma unroll
                     for (int c = 0; c < 3; c++) out[c * nv + v] = act ? (fixed ? uo[c] : acc[c]) : T(0);
                 } else {
-                    T nu[3] = {T(0), T(0), T(0)};
-                    T dn[3] = {T(0), T(0), T(0)};
-                    if (act) {
-                        // diagonal block from the 8 incident element weights
-                        T sw = T(0), sxy = T(0), sxz = T(0), syz = T(0);
-                        int ne = 0;
-#pragma unroll
-                        for (int dz = 0; dz < 2; dz++)
-#pragma unroll
-                            for (int dy = 0; dy < 2; dy++)
-#pragma unroll
-                                for (int dx = 0; dx < 2; dx++) {
-                                    const float wv = S.w[(ez + 2 + dz) % 3][(nyl + dy) * EXT + nxl + dx];
-                                    if (wv != 0.f) ne++;
-                                    // node's vertex bits in that element: (1-dx, 1-dy, 1-dz)
-                                    const T sx = dx ? T(1) : T(-1), sy = dy ? T(1) : T(-1), sz = dz ? T(1) : T(-1);
-                                    sw += T(wv);
-                                    sxy += T(wv) * sx * sy;
-                                    sxz += T(wv) * sx * sz;
-                                    syz += T(wv) * sy * sz;
-                                }
-                        if (fixed) {
-#pragma unroll
-                            for (int c = 0; c < 3; c++) nu[c] = fv[c] / T(ne);
-                        } else {
-                            const T A = kt.diag_a * sw, bxy = kt.diag_b * sxy, bxz = kt.diag_b * sxz,
-                                    byz = kt.diag_b * syz;
-                            // inverse of [[A,bxy,bxz],[bxy,A,byz],[bxz,byz,A]]
-                            const T c00 = A * A - byz * byz, c01 = -(bxy * A - byz * bxz), c02 = bxy * byz - A * bxz;
-                            const T c11 = A * A - bxz * bxz, c12 = -(A * byz - bxy * bxz), c22 = A * A - bxy * bxy;
-                            const T id = T(1) / (A * c00 + bxy * c01 + bxz * c02);
-                            T rr[3];
-#pragma unroll
-                            for (int c = 0; c < 3; c++) rr[c] = fv[c] - acc[c];
-                            T zz[3];
-                            zz[0] = id * (c00 * rr[0] + c01 * rr[1] + c02 * rr[2]);
-                            zz[1] = id * (c01 * rr[0] + c11 * rr[1] + c12 * rr[2]);
-                            zz[2] = id * (c02 * rr[0] + c12 * rr[1] + c22 * rr[2]);
-                            if (MODE == 2) {
-#pragma unroll
-                                for (int c = 0; c < 3; c++) nu[c] = uo[c] + omega * zz[c];
-                            } else {
-                                // Chebyshev step: d = ca d + cb D^-1 r, u += d
-#pragma unroll
-                                for (int c = 0; c < 3; c++) {
-                                    dn[c] = (kstep == 0 ? T(0) : cheb_a * dv[c]) + cheb_b * zz[c];
-                                    nu[c] = uo[c] + dn[c];
-                                }
-                            }
-                        }
-                    }
+                    T nu[3], dn[3];
+                    node_smooth<T, MODE, EXT>(kt, S.w[(ez + 2) % 3], S.w[ez % 3], nyl * EXT + nxl, acc, fv, uo, dv, act,
+                                         fixed, omega, cheb_a, cheb_b, kstep, nu, dn);
 #pragma unroll
                     for (int c = 0; c < 3; c++) out[c * nv + v] = nu[c];
                     if (MODE == 3)
@@ -301,34 +312,271 @@ __global__ void __launch_bounds__(Tile<TY_>::BS, tile_min_blocks<T, TY_>()) k_fi
 }
 
 
+// ---------------------------------------------------------------------------
+// software-pipelined tile kernel: one barrier per element layer instead of two.
+// Iteration t computes element layer t+1 (into one of two element-output buffers)
+// while the node phase of node layer t reads element layer t from the other, so
+// the element and node work of neighbouring layers share one barrier interval.
+// Node layers live in a ring of 3 shared slots (layer t+3 is stored at the top of
+// iteration t, into the slot of layer t, whose last readers ran before the
+// previous barrier), element weights in a ring of 4 (layers t-1 .. t+2).
+// ---------------------------------------------------------------------------
+template <typename T, int TY_>
+struct PipeSmem {
+    T u[3][3][Tile<TY_>::NU_T];   // node layer L in slot (L + 3) % 3
+    T e[2][24][Tile<TY_>::NE_T];  // element layer L in slot (L + 2) & 1
+    float w[4][Tile<TY_>::NE_T];  // element layer L in slot (L + 4) & 3
+};
+
+template <typename T, int TY_>
+constexpr int pipe_min_blocks() {
+    return sizeof(T) == 8 ? (TY_ == 2 ? 3 : TY_ == 4 ? 2 : 1) : (TY_ == 2 ? 8 : TY_ == 4 ? 5 : 3);
+}
+
 template <typename T, bool WS, int MODE, int TY_>
+__global__ void __launch_bounds__(Tile<TY_>::BS, pipe_min_blocks<T, TY_>()) k_fine_pipe(int nx, int ny, int nz, int zchunk,
+                                                        const uint8_t* __restrict__ vact,
+                                                        const float* __restrict__ wgt,
+                                                        const uint8_t* __restrict__ vfix, const rte::KtVals<T> kt,
+                                                        const T* __restrict__ u, const T* __restrict__ f,
+                                                        T* __restrict__ out, T omega, T* __restrict__ dvec,
+                                                        const double* __restrict__ coef, int kstep) {
+    using TS = Tile<TY_>;
+    constexpr int TX = TS::TX, TY = TS::TY, EXT = TS::EXT, UXT = TS::UXT, NE_T = TS::NE_T, NU_T = TS::NU_T;
+    constexpr int TILE_BS = TS::BS, U_PER_T = TS::U_PER_T;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    PipeSmem<T, TY_>& S = *reinterpret_cast<PipeSmem<T, TY_>*>(smraw);
+    T cheb_a = T(0), cheb_b = T(0);
+    if (MODE == 3) {
+        const double ca = coef[2 * kstep], cb = coef[2 * kstep + 1];
+        cheb_a = (T)ca;
+        cheb_b = (T)cb;
+    }
+    const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
+    const long nv = (long)vx * vy * vz;
+    const long plane = (long)vx * vy;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int zb = blockIdx.z * zchunk;
+    const int ze = min(zb + zchunk, vz);
+    const int tid = threadIdx.x;
+    const int nxl = tid % TX, nyl = tid / TX;
+    const int nxg = x0 + nxl, nyg = y0 + nyl;
+    const bool node_thread = tid < TX * TY && nxg < vx && nyg < vy;
+    const long vxy = node_thread ? nxg + (long)vx * nyg : 0;
+    const int exl = tid % EXT, eyl = tid / EXT;
+    const int exg = x0 - 1 + exl, eyg = y0 - 1 + eyl;
+    const bool elem_xy = tid < NE_T && exg >= 0 && eyg >= 0 && exg < nx && eyg < ny;
+    const long exy = elem_xy ? exg + (long)nx * eyg : 0;
+    long hxy[U_PER_T];
+    bool hok[U_PER_T];
+#pragma unroll
+    for (int j = 0; j < U_PER_T; j++) {
+        const int i = tid + j * TILE_BS;
+        const int xx = x0 - 1 + i % UXT, yy = y0 - 1 + i / UXT;
+        hok[j] = i < NU_T && xx >= 0 && yy >= 0 && xx < vx && yy < vy;
+        hxy[j] = hok[j] ? xx + (long)vx * yy : 0;
+    }
+
+    T pu[U_PER_T][3];
+    float pw = 0.f;
+    auto fetch_layer = [&](int L) {
+#pragma unroll
+        for (int j = 0; j < U_PER_T; j++) {
+            T a = T(0), b = T(0), c = T(0);
+            if (hok[j] && L >= 0 && L < vz) {
+                const long v = hxy[j] + plane * L;
+                if (!(WS && vfix[v])) {
+                    a = u[v];
+                    b = u[nv + v];
+                    c = u[2 * nv + v];
+                }
+            }
+            pu[j][0] = a;
+            pu[j][1] = b;
+            pu[j][2] = c;
+        }
+    };
+    auto stash_layer = [&](int L) {
+        T* dst = &S.u[(L + 3) % 3][0][0];
+#pragma unroll
+        for (int j = 0; j < U_PER_T; j++) {
+            const int i = tid + j * TILE_BS;
+            if (i < NU_T) {
+                dst[i] = pu[j][0];
+                dst[NU_T + i] = pu[j][1];
+                dst[2 * NU_T + i] = pu[j][2];
+            }
+        }
+    };
+    auto fetch_w = [&](int ez) {
+        pw = (elem_xy && ez >= 0 && ez < nz) ? wgt[exy + (long)nx * ny * ez] : 0.f;
+    };
+    auto stash_w = [&](int ez) {
+        if (tid < NE_T) S.w[(ez + 4) & 3][tid] = pw;
+    };
+    // element layer e (couples node layers e and e+1) into its output slot
+    auto element_phase = [&](int e) {
+        if (tid >= NE_T) return;
+        T a[24];
+        const float wv = S.w[(e + 4) & 3][tid];
+        if (wv != 0.f) {
+            const T* lo = &S.u[(e + 3) % 3][0][0];
+            const T* hi = &S.u[(e + 4) % 3][0][0];
+#pragma unroll
+            for (int vtx = 0; vtx < 8; vtx++) {
+                const T* src = (vtx & 4) ? hi : lo;
+                const int idx = (eyl + ((vtx >> 1) & 1)) * UXT + exl + (vtx & 1);
+                a[3 * vtx] = src[idx];
+                a[3 * vtx + 1] = src[NU_T + idx];
+                a[3 * vtx + 2] = src[2 * NU_T + idx];
+            }
+            rte::element_apply(a, kt, T(wv));
+        } else {
+#pragma unroll
+            for (int q = 0; q < 24; q++) a[q] = T(0);
+        }
+        T* dst = &S.e[(e + 2) & 1][0][0];
+#pragma unroll
+        for (int q = 0; q < 24; q++) dst[q * NE_T + tid] = a[q];
+    };
+
+    // prologue: node layers zb-1 .. zb+1 and weights of element layers zb-1, zb in shared
+    // memory, element layer zb-1 computed; registers then hold node layer zb+2 and the
+    // weights of element layer zb+1
+    fetch_layer(zb - 1);
+    stash_layer(zb - 1);
+    fetch_layer(zb);
+    stash_layer(zb);
+    fetch_layer(zb + 1);
+    stash_layer(zb + 1);
+    fetch_w(zb - 1);
+    stash_w(zb - 1);
+    fetch_w(zb);
+    stash_w(zb);
+    __syncthreads();
+    element_phase(zb - 1);
+    fetch_layer(zb + 2);
+    fetch_w(zb + 1);
+    __syncthreads();
+
+    T acc[3] = {T(0), T(0), T(0)};
+    for (int t = zb - 1; t < ze; t++) {
+        if (t + 3 <= ze) stash_layer(t + 3);
+        if (t + 2 < ze) stash_w(t + 2);
+        if (t + 4 <= ze) fetch_layer(t + 4);
+        if (t + 3 < ze) fetch_w(t + 3);
+        const bool out_layer = t >= zb;
+        T fv[3] = {T(0), T(0), T(0)}, uo[3] = {T(0), T(0), T(0)}, dv[3] = {T(0), T(0), T(0)};
+        bool act = false, fixed = false;
+        long vout = 0;
+        if (node_thread && out_layer) {
+            vout = vxy + plane * t;
+            act = vact[vout];
+            fixed = WS && act && vfix[vout];
+            if (MODE != 1)
+#pragma unroll
+                for (int c = 0; c < 3; c++) fv[c] = f[c * nv + vout];
+            if (MODE >= 1)
+#pragma unroll
+                for (int c = 0; c < 3; c++) uo[c] = u[c * nv + vout];
+            if (MODE == 3 && kstep > 0)
+#pragma unroll
+                for (int c = 0; c < 3; c++) dv[c] = dvec[c * nv + vout];
+        }
+        if (t + 1 < ze) element_phase(t + 1);
+        if (node_thread) {
+            const T* E = &S.e[(t + 2) & 1][0][0];
+            if (out_layer) {
+                // node layer t: bottom vertices (bit z = 0) of element layer t
+#pragma unroll
+                for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+                    for (int dx = 0; dx < 2; dx++) {
+                        const int el = (nyl + dy) * EXT + nxl + dx;
+                        const int vtx = (1 - dx) + 2 * (1 - dy);
+#pragma unroll
+                        for (int c = 0; c < 3; c++) acc[c] += E[(3 * vtx + c) * NE_T + el];
+                    }
+                const long v = vout;
+                if (MODE == 0) {
+#pragma unroll
+                    for (int c = 0; c < 3; c++) out[c * nv + v] = act ? (fixed ? fv[c] : fv[c] - acc[c]) : T(0);
+                } else if (MODE == 1) {
+#pragma unroll
+                    for (int c = 0; c < 3; c++) out[c * nv + v] = act ? (fixed ? uo[c] : acc[c]) : T(0);
+                } else {
+                    T nu[3], dn[3];
+                    node_smooth<T, MODE, EXT>(kt, S.w[(t + 3) & 3], S.w[(t + 4) & 3], nyl * EXT + nxl, acc, fv, uo,
+                                              dv, act, fixed, omega, cheb_a, cheb_b, kstep, nu, dn);
+#pragma unroll
+                    for (int c = 0; c < 3; c++) out[c * nv + v] = nu[c];
+                    if (MODE == 3)
+#pragma unroll
+                        for (int c = 0; c < 3; c++) dvec[c * nv + v] = dn[c];
+                }
+            }
+            // start node layer t+1 with the top vertices (bit z = 1) of element layer t
+#pragma unroll
+            for (int c = 0; c < 3; c++) acc[c] = T(0);
+#pragma unroll
+            for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+                for (int dx = 0; dx < 2; dx++) {
+                    const int el = (nyl + dy) * EXT + nxl + dx;
+                    const int vtx = (1 - dx) + 2 * (1 - dy) + 4;
+#pragma unroll
+                    for (int c = 0; c < 3; c++) acc[c] += E[(3 * vtx + c) * NE_T + el];
+                }
+        }
+        __syncthreads();
+    }
+}
+
+
+template <typename T, bool WS, int MODE, int TY_, bool PIPE>
 int launch_tile_ty(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name, T* dvec,
                    const double* coef, int kstep) {
     rt_level& L = h->L[0];
-    const size_t smem = sizeof(TileSmem<T, TY_>);
+    const size_t smem = PIPE ? sizeof(PipeSmem<T, TY_>) : sizeof(TileSmem<T, TY_>);
     const int zc = h->tune[sizeof(T) == 8 ? 1 : 0][MODE].zchunk;
     dim3 grid((L.vx + Tile<TY_>::TX - 1) / Tile<TY_>::TX, (L.vy + TY_ - 1) / TY_, (L.vz + zc - 1) / zc);
     const rte::KtVals<T> kt = rte::make_kt<T>(h);
     return rt_launch(h->ctx, name, [&] {
-        k_fine_tile<T, WS, MODE, TY_><<<grid, Tile<TY_>::BS, smem, h->ctx->stream>>>(
-            L.nx, L.ny, L.nz, zc, L.vact, h->w, h->vfix, kt, u, f, out, (T)omega, dvec, coef, kstep);
+        if (PIPE)
+            k_fine_pipe<T, WS, MODE, TY_><<<grid, Tile<TY_>::BS, smem, h->ctx->stream>>>(
+                L.nx, L.ny, L.nz, zc, L.vact, h->w, h->vfix, kt, u, f, out, (T)omega, dvec, coef, kstep);
+        else
+            k_fine_tile<T, WS, MODE, TY_><<<grid, Tile<TY_>::BS, smem, h->ctx->stream>>>(
+                L.nx, L.ny, L.nz, zc, L.vact, h->w, h->vfix, kt, u, f, out, (T)omega, dvec, coef, kstep);
     });
 }
 
+// variant 0: two barriers per element layer; 3: software-pipelined, one barrier per layer
 template <typename T, bool WS, int MODE>
 int launch_tile(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name, T* dvec = nullptr,
                 const double* coef = nullptr, int kstep = 0) {
-    switch (h->tune[sizeof(T) == 8 ? 1 : 0][MODE].ty) {
-        case 2: return launch_tile_ty<T, WS, MODE, 2>(h, u, f, out, omega, name, dvec, coef, kstep);
-        case 8: return launch_tile_ty<T, WS, MODE, 8>(h, u, f, out, omega, name, dvec, coef, kstep);
-        default: return launch_tile_ty<T, WS, MODE, 4>(h, u, f, out, omega, name, dvec, coef, kstep);
+    const rt_tile_cfg& tn = h->tune[sizeof(T) == 8 ? 1 : 0][MODE];
+    if (tn.variant == 3) {
+        switch (tn.ty) {
+            case 2: return launch_tile_ty<T, WS, MODE, 2, true>(h, u, f, out, omega, name, dvec, coef, kstep);
+            case 8: return launch_tile_ty<T, WS, MODE, 8, true>(h, u, f, out, omega, name, dvec, coef, kstep);
+            default: return launch_tile_ty<T, WS, MODE, 4, true>(h, u, f, out, omega, name, dvec, coef, kstep);
+        }
+    }
+    switch (tn.ty) {
+        case 2: return launch_tile_ty<T, WS, MODE, 2, false>(h, u, f, out, omega, name, dvec, coef, kstep);
+        case 8: return launch_tile_ty<T, WS, MODE, 8, false>(h, u, f, out, omega, name, dvec, coef, kstep);
+        default: return launch_tile_ty<T, WS, MODE, 4, false>(h, u, f, out, omega, name, dvec, coef, kstep);
     }
 }
 
 template <typename T, bool WS, int MODE, int TY_>
 cudaError_t set_attr() {
-    return cudaFuncSetAttribute(k_fine_tile<T, WS, MODE, TY_>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sizeof(TileSmem<T, TY_>));
+    cudaError_t e = cudaFuncSetAttribute(k_fine_tile<T, WS, MODE, TY_>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(TileSmem<T, TY_>));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_fine_pipe<T, WS, MODE, TY_>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(PipeSmem<T, TY_>));
 }
 
 template <typename T, int TY_>
@@ -368,7 +616,8 @@ int tile_zchunk_default(rt_ctx* c, int vx, int vy, int vz) {
 
 template <typename T>
 static bool use_march(rt_hier* h, int mode) {
-    return h->tune[sizeof(T) == 8 ? 1 : 0][mode].variant >= 1;  // 1: marching, 2: marching with prefetch
+    const int v = h->tune[sizeof(T) == 8 ? 1 : 0][mode].variant;
+    return v == 1 || v == 2;  // 1: marching, 2: marching with prefetch (0, 3: tile kernels)
 }
 
 template <typename T>

@@ -58,7 +58,8 @@ struct rt_level {
     double* d = nullptr;  // Chebyshev direction
     float* d32 = nullptr;
     double* st = nullptr;   // [243][nv]
-    float* st32 = nullptr;  // [243][nv]
+    float* st32 = nullptr;     // FP32 smoother copy, 32-node blocks [nv/32][243][32]
+    uint16_t* st16 = nullptr;  // BF16 copy [nv/32][252][32] (only once rt_params.coarse_bf16 was set)
     // coarsest level
     int na = 0;
     int* aidx = nullptr;
@@ -243,6 +244,7 @@ int dot(rt_hier* h, long n, const double* a, const double* b, double* out_dev);
 int dot2(rt_hier* h, long n, const double* a, const double* b, const double* c, double* out_dev);
 int axpy(rt_hier* h, long n, double a, const double* x, double* y);
 int d2f(rt_hier* h, long n, const double* a, float* b);
+int stencil_copies(rt_hier* h, int lvl);
 int f2d(rt_hier* h, long n, const float* a, double* b);
 int d2f_scaled(rt_hier* h, long n, const double* a, float* b, const double* s_dev);
 int f2d_scaled(rt_hier* h, long n, const float* a, double* b, const double* s_dev);

@@ -18,6 +18,7 @@
 namespace {
 
 constexpr int RB = 256;  // reduction block size
+constexpr int XR_U = 4;  // grid strides per trip in the fused update + reduction kernels
 
 unsigned gridN(rt_ctx* c, long n, int bs = 256) {
     long b = rt_blocks(n, bs);
@@ -131,13 +132,26 @@ __global__ void __launch_bounds__(RB) k_pcg_xr_rr(long n, const double* __restri
                                                   double* __restrict__ rold, double* __restrict__ partials) {
     const double alpha = den[0] != 0.0 ? num[0] / den[0] : 0.0;
     double v[1] = {0};
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        const double ri = r[i];
-        rold[i] = ri;
-        x[i] += alpha * p[i];
-        const double rn = ri - alpha * q[i];
-        r[i] = rn;
-        v[0] += rn * rn;
+    // the reduction grid is small (2 blocks per SM): XR_U grid strides per trip keep enough loads in
+    // flight; the sum still runs over each thread's elements in stride order, as in k_dot
+    const long st = (long)gridDim.x * blockDim.x;
+    for (long i0 = blockIdx.x * (long)blockDim.x + threadIdx.x; i0 < n; i0 += XR_U * st) {
+        double ri[XR_U], pi[XR_U], qi[XR_U], xi[XR_U];
+#pragma unroll
+        for (int k = 0; k < XR_U; k++) {
+            const long i = i0 + k * st;
+            if (i < n) { ri[k] = r[i]; pi[k] = p[i]; qi[k] = q[i]; xi[k] = x[i]; }
+        }
+#pragma unroll
+        for (int k = 0; k < XR_U; k++) {
+            const long i = i0 + k * st;
+            if (i >= n) break;
+            rold[i] = ri[k];
+            x[i] = xi[k] + alpha * pi[k];
+            const double rn = ri[k] - alpha * qi[k];
+            r[i] = rn;
+            v[0] += rn * rn;
+        }
     }
     block_reduce_store<1>(v, partials);
 }
@@ -149,11 +163,24 @@ __global__ void __launch_bounds__(RB) k_f2d_scaled_dot2(long n, const float* __r
                                                         double* __restrict__ partials) {
     const double sc = sqrt(fmax(s[0], 1e-300));
     double v[2] = {0, 0};
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        const double x = (double)a[i] * sc;
-        z[i] = x;
-        v[0] += x * r[i];
-        v[1] += x * rold[i];
+    const long st = (long)gridDim.x * blockDim.x;
+    for (long i0 = blockIdx.x * (long)blockDim.x + threadIdx.x; i0 < n; i0 += XR_U * st) {
+        float ai[XR_U];
+        double ri[XR_U], oi[XR_U];
+#pragma unroll
+        for (int k = 0; k < XR_U; k++) {
+            const long i = i0 + k * st;
+            if (i < n) { ai[k] = a[i]; ri[k] = r[i]; oi[k] = rold[i]; }
+        }
+#pragma unroll
+        for (int k = 0; k < XR_U; k++) {
+            const long i = i0 + k * st;
+            if (i >= n) break;
+            const double x = (double)ai[k] * sc;
+            z[i] = x;
+            v[0] += x * ri[k];
+            v[1] += x * oi[k];
+        }
     }
     block_reduce_store<2>(v, partials);
 }

@@ -321,7 +321,7 @@ class HierarchyGrid:
             for m, mname in enumerate(names):
                 v, ty, zc, us = C.c_int(), C.c_int(), C.c_int(), C.c_double()
                 self._c(A.lib().rt_tuning_info(self._h, prec, m, C.byref(v), C.byref(ty), C.byref(zc), C.byref(us)))
-                out[f"{mname}_{pname}"] = {"variant": ["smem_tile", "register_march", "register_march_prefetch"][v.value], "rows": ty.value,
+                out[f"{mname}_{pname}"] = {"variant": ["smem_tile", "register_march", "register_march_prefetch", "smem_tile_pipelined"][v.value], "rows": ty.value,
                                            "zchunk": zc.value, "us": round(us.value, 2)}
         return out
 

@@ -96,11 +96,12 @@ def test_fine_smoothers(pair, smoother):
 
 
 @pytest.mark.parametrize("variant,ty,zc", [(0, 4, 8), (0, 2, 5), (0, 8, 3), (1, 2, 4), (1, 4, 16), (1, 8, 7),
-                                           (1, 4, 1), (2, 2, 8), (2, 4, 3)])
+                                           (1, 4, 1), (2, 2, 8), (2, 4, 3), (3, 4, 8), (3, 2, 5), (3, 8, 3),
+                                           (3, 4, 1), (3, 2, 64)])
 def test_fine_kernel_variants(pair, variant, ty, zc):
     """Every launch shape of the finest-level kernels (shared-memory tile, register marching,
-    register marching with prefetched output-stage loads) gives the oracle's residual, K u,
-    Jacobi and Chebyshev results."""
+    register marching with prefetched output-stage loads, pipelined shared-memory tile) gives the
+    oracle's residual, K u, Jacobi and Chebyshev results."""
     cfg, ctx, G, H = pair
     import ctypes as C
 
@@ -128,6 +129,44 @@ def test_fine_kernel_variants(pair, variant, ty, zc):
     assert rel_err(G[0].getDisplacement(), uo) < 1e-9
     for m in range(4):  # back to the default shape
         rb._capi.check(rb.lib().rt_set_tuning(G.handle, rb.FP64, m, 1, 4, 16), ctx.handle)
+
+
+@pytest.mark.parametrize("variant,ty,zc", [(0, 4, 8), (1, 2, 8), (2, 4, 8), (3, 4, 8), (3, 8, 2)])
+def test_fp32_kernel_variants_in_pcg(pair, variant, ty, zc):
+    """The FP32 finest-level kernels of every variant drive the mixed-precision PCG (FP32 Chebyshev
+    V-cycles) to 1e-6 in the FP64 residual; FP32 rounding differs between variants, the iteration
+    count stays within one step of the default shape's."""
+    cfg, ctx, G, H = pair
+    b = _rand_vec(G, 0, 81)
+    if cfg["mode"] in (rb.MODE_WSCF, rb.MODE_WSFF):
+        b[np.tile(cfg["vfix"].ravel().astype(bool), 3)] = 0
+    else:
+        Ru = np.zeros(6 * b.size)
+        O.lib().or_rigid_nodes(H.lv(0), O.ptr(Ru))
+        O.lib().or_displacement_project(b.size // 3, O.ptr(Ru), O.ptr(b))
+    params = G.params
+    params.precision, params.smoother = rb.FP32, rb.SMOOTH_CHEBY
+    params.pre_sweeps = params.post_sweeps = 4
+    G.set_params(params)
+    G.update_stencil()
+    its = []
+    for shape in ((1, 4, 16), (variant, ty, zc)):
+        for m in range(4):
+            rb._capi.check(rb.lib().rt_set_tuning(G.handle, rb.FP32, m, *shape), ctx.handle)
+        G[0].setForce(b)
+        G[0].reset_displacement()
+        info = G.pcg(1e-6, 1000)
+        assert info.status == 0 and info.rel_residual <= 1e-6
+        r = (b - H.applyK(G[0].getDisplacement())) * np.tile(H.arrs[0]["vact"], 3)
+        assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.01e-6
+        its.append(info.iterations)
+    assert abs(its[1] - its[0]) <= 1, its
+    for m in range(4):
+        rb._capi.check(rb.lib().rt_set_tuning(G.handle, rb.FP32, m, 1, 4, 16), ctx.handle)
+    params.precision, params.smoother = rb.FP64, rb.SMOOTH_SGS
+    params.pre_sweeps = params.post_sweeps = 1
+    G.set_params(params)
+    G.update_stencil()
 
 
 def test_autotune_keeps_results(pair):
@@ -233,12 +272,17 @@ def test_vcycle_sequence(pair):
     assert rel_err(G[0].getDisplacement(), H.arrs[0]["u"]) < 1e-8
 
 
-@pytest.mark.parametrize("precision,smoother,sweeps", [(rb.FP64, rb.SMOOTH_SGS, 1), (rb.FP32, rb.SMOOTH_SGS, 1),
-                                                       (rb.FP32, rb.SMOOTH_CHEBY, 4),
-                                                       (rb.FP64, rb.SMOOTH_JACOBI, 2),
-                                                       (rb.FP64_FINE, rb.SMOOTH_CHEBY, 4),
-                                                       (rb.FP64_FINE, rb.SMOOTH_SGS, 1)])
-def test_pcg_to_1e6(pair, precision, smoother, sweeps):
+@pytest.mark.parametrize("precision,smoother,sweeps,bf16", [(rb.FP64, rb.SMOOTH_SGS, 1, 0),
+                                                            (rb.FP32, rb.SMOOTH_SGS, 1, 0),
+                                                            (rb.FP32, rb.SMOOTH_CHEBY, 4, 0),
+                                                            (rb.FP32, rb.SMOOTH_CHEBY, 4, 1),
+                                                            (rb.FP32, rb.SMOOTH_JACOBI, 2, 1),
+                                                            (rb.FP64, rb.SMOOTH_JACOBI, 2, 0),
+                                                            (rb.FP64_FINE, rb.SMOOTH_CHEBY, 4, 0),
+                                                            (rb.FP64_FINE, rb.SMOOTH_SGS, 1, 0)])
+def test_pcg_to_1e6(pair, precision, smoother, sweeps, bf16):
+    """MG-PCG to 1e-6 in every precision form; bf16=1 smooths levels >= 1 with BF16-stored stencils,
+    which changes the preconditioner only: the FP64 residual of the answer still meets the tolerance."""
     cfg, ctx, G, H = pair
     b = _rand_vec(G, 0, 80)
     if cfg["mode"] in (rb.MODE_WSCF, rb.MODE_WSFF):
@@ -253,11 +297,21 @@ def test_pcg_to_1e6(pair, precision, smoother, sweeps):
     params.smoother = smoother
     params.pre_sweeps = params.post_sweeps = sweeps
     params.jacobi_omega = 0.5
+    params.coarse_bf16 = bf16
     G.set_params(params)
     G.update_stencil()
     G[0].setForce(b)
     G[0].reset_displacement()
+    if bf16:
+        ctx.profile(True)
+        ctx.profile_reset()
     info = G.pcg(1e-6, 1000)
+    if bf16:
+        st = ctx.profile_stats()
+        ctx.profile(False)
+        if G.n_grid() > 2:  # a smoothed coarse level exists: its smoother read the BF16 stencils
+            assert sum(v[0] for k, v in st.items() if k.startswith("st_") and "_bf16" in k) > 0, st
+        assert not any(k.startswith("st_") and "_f32" in k and "residual" not in k for k in st), st
     assert info.status == 0 and info.rel_residual <= 1e-6
     x = G[0].getDisplacement()
     # FP64 residual check of the returned solution with the oracle operator
@@ -269,6 +323,7 @@ def test_pcg_to_1e6(pair, precision, smoother, sweeps):
     params.precision = rb.FP64
     params.smoother = rb.SMOOTH_SGS
     params.pre_sweeps = params.post_sweeps = 1
+    params.coarse_bf16 = 0
     G.set_params(params)
     G.update_stencil()
 
