@@ -379,12 +379,16 @@ def run_kernel(args):
             p.coarse_bf16 = 1
             G.set_params(p)
             G.update_stencil()
+        variant = None
+        if args.shape and prec == rb.FP32:  # 0 lane-split, 1 bulk-copy
+            variant = int(args.shape)
+            rb._capi.check(rb.lib().rt_set_level_kernel(G.handle, 1 if form == "bf16" else 0, variant), ctx.handle)
         us = C.c_double()
         rb._capi.check(rb.lib().rt_bench_level_kernel(G.handle, args.level, prec, mode, args.warmup, C.byref(us)),
                        ctx.handle)
         rb._capi.check(rb.lib().rt_bench_level_kernel(G.handle, args.level, prec, mode, args.steps, C.byref(us)),
                        ctx.handle)
-        print(json.dumps({"kernel": args.kernel, "level": args.level, "us_per_call": us.value,
+        print(json.dumps({"kernel": args.kernel, "level": args.level, "variant": variant, "us_per_call": us.value,
                           "nodes": G[args.level].nv, "stencil_bytes": G[args.level].nv * 243 * {"f64": 8, "f32": 4,
                                                                                                "bf16": 2}[form]}))
         G.close()

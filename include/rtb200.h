@@ -230,6 +230,12 @@ int rt_bench_fine_kernel(rt_hier* h, int precision, int mode, int reps, double* 
  * precision RT_FP64 or RT_FP32 (FP32 smoothing reads the BF16 stencils when rt_params.coarse_bf16 is set).
  * Overwrites the level's vectors; needs rt_update_stencil. */
 int rt_bench_level_kernel(rt_hier* h, int lvl, int precision, int mode, int reps, double* us_per_launch);
+/* the kernel variant of the FP32 smoother's stencil levels, per stencil copy (stencil_type 0 FP32,
+ * 1 BF16): 0 lane-split (4 lanes per node), 1 bulk-copy (each 32-node stencil run staged in shared
+ * memory by cp.async.bulk).  rt_autotune times both on level 1 (after rt_update_stencil) and keeps
+ * the faster; us_*: its measured Chebyshev-step times (0 before it ran). */
+int rt_level_kernel_info(rt_hier* h, int stencil_type, int* variant, double* us_lane_split, double* us_bulk);
+int rt_set_level_kernel(rt_hier* h, int stencil_type, int variant);
 
 /* ---- solvers -------------------------------------------------------------- */
 /* MG-preconditioned CG on level 0: u <- K^-1 f to ||r||/||f|| <= tol (solveFEM's role,

@@ -106,6 +106,8 @@ SIGNATURES = {
     "rt_set_tuning": (I, [P, I, I, I, I, I]),
     "rt_bench_fine_kernel": (I, [P, I, I, I, C.POINTER(D)]),
     "rt_bench_level_kernel": (I, [P, I, I, I, I, C.POINTER(D)]),
+    "rt_level_kernel_info": (I, [P, I, C.POINTER(I), C.POINTER(D), C.POINTER(D)]),
+    "rt_set_level_kernel": (I, [P, I, I]),
     "rt_pcg": (I, [P, D, I, C.POINTER(SolveInfo)]),
     "rt_hier_precision_fallbacks": (C.c_longlong, [P]),
     "rt_worst_case": (I, [P, I, I, D, C.c_uint64, C.POINTER(D), C.POINTER(SolveInfo)]),

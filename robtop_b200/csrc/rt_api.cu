@@ -344,6 +344,7 @@ static void ws_sync(rt_hier* w) {
     w->P = p->P;
     memcpy(w->tune, p->tune, sizeof(w->tune));
     memcpy(w->tune_us, p->tune_us, sizeof(w->tune_us));
+    memcpy(w->st_variant, p->st_variant, sizeof(w->st_variant));
     w->dinv64 = p->dinv64; w->dinv32 = p->dinv32;
     for (size_t i = 0; i < w->L.size(); i++) {
         rt_level& a = w->L[i];
@@ -506,6 +507,7 @@ static int build_hier(rt_ctx* c, const rt_params* p, int nx, int ny, int nz, uin
     RT_CUDA(c, cudaMemsetAsync(h->scal, 0, sizeof(double) * RT_NSCAL, c->stream));
     RT_CHECK(upload_KE(h));
     RT_CHECK(rtk::init_tile_kernels(c));
+    RT_CHECK(rtk::init_stencil_kernels(c));
     *out = h;
     return RT_OK;
 }
@@ -1464,6 +1466,18 @@ static int pcg_prologue(rt_hier* h, double* x, const double* b) {
     return rtk::dot(h, n, r, r, h->scal + 21);
 }
 
+// a solve that produced NaN: a stencil kernel whose bounded copy wait ran out writes NaN and
+// flags RT_SCAL_ERR, anything else is a numerical breakdown
+static int nan_fail(rt_hier* h, int it) {
+    double e = 0;
+    RT_CHECK(read_scalars(h, RT_SCAL_ERR, 1, &e));
+    if (e != 0.0) {
+        RT_CUDA(h->ctx, cudaMemsetAsync(h->scal + RT_SCAL_ERR, 0, sizeof(double), h->ctx->stream));
+        return rt_fail(h->ctx, RT_ECUDA, "a stencil-level kernel gave up waiting for its bulk copies (iteration %d)", it);
+    }
+    return rt_fail(h->ctx, RT_ENAN, "NaN in PCG at iteration %d", it);
+}
+
 static int pcg_core(rt_hier* h, double* x, const double* b, double tol, int maxit, rt_solve_info* info, int* vcycles) {
     double* r = h->rr;
     RT_CHECK(pcg_prologue(h, x, b));
@@ -1504,7 +1518,7 @@ static int pcg_core(rt_hier* h, double* x, const double* b, double tol, int maxi
         RT_CHECK(read_scalars(h, 92, 1, &stall));
         if (!std::isfinite(s3[0])) {
             if (info) { info->status = RT_ENAN; info->iterations = (int)s3[3]; }
-            return rt_fail(h->ctx, RT_ENAN, "NaN in PCG at iteration %d", (int)s3[3]);
+            return nan_fail(h, (int)s3[3]);
         }
         rel = std::sqrt(s3[0]) / bn;
         it = (int)s3[3];
@@ -1952,6 +1966,8 @@ static double time_fine_kernel(rt_hier* h, int prec, int mode, int reps) {
     return best;
 }
 
+static int autotune_level_kernels(rt_hier* h, int reps);
+
 extern "C" int rt_autotune(rt_hier* h, int reps) {
     if (!h) return RT_EINVAL;
     RT_NOT_WORKSPACE(h);
@@ -1992,6 +2008,7 @@ extern "C" int rt_autotune(rt_hier* h, int reps) {
             h->tune[prec][mode] = best_cfg;
             h->tune_us[prec][mode] = best;
         }
+    RT_CHECK(autotune_level_kernels(h, reps));
     cudaGetLastError();
     h->graph_epoch++;  // launch shapes are baked into captured graphs
     c->profile = was_profiling;
@@ -2040,20 +2057,16 @@ extern "C" int rt_bench_fine_kernel(rt_hier* h, int precision, int mode, int rep
 }
 
 // one stencil-level kernel (residual, Jacobi or a Chebyshev step) on random inputs, timed with
-// CUDA events on the context stream; the level's own vectors are overwritten
-extern "C" int rt_bench_level_kernel(rt_hier* h, int lvl, int precision, int mode, int reps, double* us_per_launch) {
-    if (!h || lvl < 1 || lvl + 1 >= (int)h->L.size() || precision < RT_FP64 || precision > RT_FP32 || mode < 0 ||
-        mode > 3 || mode == 1 || reps < 1)
-        return RT_EINVAL;
-    RT_NOT_WORKSPACE(h);
-    RT_CHECK(need_stencil(h));
+// CUDA events on the context stream.  FP32: random u, f through the fine-level scratch vectors into
+// the level's FP32 vectors (V-cycle scratch); FP64: the level's own u, f (overwritten).
+static double time_level_kernel(rt_hier* h, int lvl, int precision, int mode, int reps) {
     rt_ctx* c = h->ctx;
     rt_level& L = h->L[lvl];
     const long n = 3 * L.nv;
-    RT_CHECK(rtk::rng_uniform(h, 0xbe7e, n, L.u));
-    RT_CHECK(rtk::rng_uniform(h, 0xbe7f, n, L.f));
-    RT_CHECK(rtk::d2f(h, n, L.u, L.u32));
-    RT_CHECK(rtk::d2f(h, n, L.f, L.f32));
+    double* ru = precision == RT_FP64 ? L.u : h->x;
+    double* rf = precision == RT_FP64 ? L.f : h->q;
+    if (rtk::rng_uniform(h, 0xbe7e, n, ru) != RT_OK || rtk::rng_uniform(h, 0xbe7f, n, rf) != RT_OK) return 1e30;
+    if (precision != RT_FP64 && (rtk::d2f(h, n, ru, L.u32) != RT_OK || rtk::d2f(h, n, rf, L.f32) != RT_OK)) return 1e30;
     const double* coef = cheby_table(h, lvl);
     auto run = [&]() -> int {
         if (precision == RT_FP64) {
@@ -2069,10 +2082,10 @@ extern "C" int rt_bench_level_kernel(rt_hier* h, int lvl, int precision, int mod
             default: return rtk::st_cheby<float>(h, lvl, L.u32, L.f32, L.r32, L.d32, coef, 1);
         }
     };
-    RT_CHECK(run());
+    if (run() != RT_OK) return 1e30;
     cudaEvent_t a, b;
-    RT_CUDA(c, cudaEventCreate(&a));
-    RT_CUDA(c, cudaEventCreate(&b));
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
     cudaEventRecord(a, c->stream);
     int st = RT_OK;
     for (int i = 0; i < reps && st == RT_OK; i++) st = run();
@@ -2082,8 +2095,57 @@ extern "C" int rt_bench_level_kernel(rt_hier* h, int lvl, int precision, int mod
     cudaEventElapsedTime(&ms, a, b);
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    RT_CHECK(st);
-    if (us_per_launch) *us_per_launch = ms * 1e3 / reps;
+    return st == RT_OK ? ms * 1e3 / reps : 1e30;
+}
+
+extern "C" int rt_bench_level_kernel(rt_hier* h, int lvl, int precision, int mode, int reps, double* us_per_launch) {
+    if (!h || lvl < 1 || lvl + 1 >= (int)h->L.size() || precision < RT_FP64 || precision > RT_FP32 || mode < 0 ||
+        mode > 3 || mode == 1 || reps < 1)
+        return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
+    RT_CHECK(need_stencil(h));
+    const double t = time_level_kernel(h, lvl, precision, mode, reps);
+    if (t >= 1e30) return rt_fail(h->ctx, RT_ECUDA, "kernel launch failed");
+    if (us_per_launch) *us_per_launch = t;
+    return RT_OK;
+}
+
+// the lane-split / bulk-copy choice for the FP32 smoother's stencil kernels, timed on the largest
+// stencil level's Chebyshev step (FP32 stencils, and BF16 ones when they exist)
+static int autotune_level_kernels(rt_hier* h, int reps) {
+    if (!h->stencil_ready || h->L.size() < 3) return RT_OK;
+    for (int t = 0; t < 2; t++) {
+        if (t == 1 && !(h->P.coarse_bf16 && h->L[1].st16)) continue;
+        const int saved_bf16 = h->P.coarse_bf16;
+        h->P.coarse_bf16 = t;  // selects the stencil copy the FP32 smoother reads
+        double best = 1e30;
+        int best_v = h->st_variant[t];
+        for (int v = 0; v < 2; v++) {
+            h->st_variant[t] = v;
+            const double us = time_level_kernel(h, 1, RT_FP32, 3, reps);
+            h->st_us[t][v] = us;
+            if (us < best) { best = us; best_v = v; }
+        }
+        h->st_variant[t] = best_v;
+        h->P.coarse_bf16 = saved_bf16;
+    }
+    return RT_OK;
+}
+
+extern "C" int rt_level_kernel_info(rt_hier* h, int stencil_type, int* variant, double* us_lane_split,
+                                    double* us_bulk) {
+    if (!h || stencil_type < 0 || stencil_type > 1) return RT_EINVAL;
+    if (variant) *variant = h->st_variant[stencil_type];
+    if (us_lane_split) *us_lane_split = h->st_us[stencil_type][0];
+    if (us_bulk) *us_bulk = h->st_us[stencil_type][1];
+    return RT_OK;
+}
+
+extern "C" int rt_set_level_kernel(rt_hier* h, int stencil_type, int variant) {
+    if (!h || stencil_type < 0 || stencil_type > 1 || variant < 0 || variant > 1) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
+    h->st_variant[stencil_type] = variant;
+    h->graph_epoch++;
     return RT_OK;
 }
 
@@ -2311,7 +2373,7 @@ static int pcg_batch_core(rt_hier* const* hs, int n, double tol, int maxit, rt_s
         const double bn = sc[1] > 0 ? std::sqrt(sc[1]) : 1.0;
         double rel = std::sqrt(sc[0]) / bn;
         int its = (int)sc[3];
-        if (!std::isfinite(sc[0])) return rt_fail(c, RT_ENAN, "NaN in batched PCG instance %d", i);
+        if (!std::isfinite(sc[0])) return nan_fail(h, its);
         if (stall != 0.0 && rel > tol && its < maxit) {
             // this instance's reduced-precision V-cycles stalled: continue it alone with FP64 ones
             const int saved = h->P.precision;

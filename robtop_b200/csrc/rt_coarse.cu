@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include "rt_internal.h"
+#include "rt_tc.cuh"
 
 namespace {
 
@@ -211,6 +212,167 @@ __global__ void __launch_bounds__(ST_BS, sizeof(T) == 8 ? 1 : 3) k_st_split4(int
         }
         out[oq] = res;
         if (MODE == 3) d[oq] = dn;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Stencil kernel over the blocked FP32 / BF16 copies: the 31 KB (FP32) / 16 KB (BF16)
+// stencil run of a 32-node block is fetched with one bulk asynchronous copy
+// (cp.async.bulk, completion counted on an mbarrier) into a ring of NST shared-memory
+// stages, so the stencil stream needs no registers in flight and the copies of the
+// next blocks overlap the arithmetic of this one.  A CTA of 8 warps walks its blocks
+// (blockIdx.x, + gridDim.x, ...): warp w sums the neighbours k = w, w+8, ... of the
+// block's 32 nodes (lane = node, conflict-free stage reads), the eight partial sums
+// meet in shared memory, and warps 0..2 finish component q = warp of every node.
+// Every mbarrier wait is bounded: on a timeout the CTA waits (bounded) for its copies
+// still in flight, writes NaN to the outputs it did not produce and sets the level's
+// error slot, so the solve stops with an error instead of hanging.
+// ---------------------------------------------------------------------------
+constexpr int SB_BS = 256;
+constexpr int SB_WARPS = SB_BS / 32;
+
+template <typename S>
+__host__ __device__ constexpr int sb_stages() { return sizeof(S) == 2 ? 4 : 3; }
+template <typename T, typename S>
+constexpr size_t sb_smem() {
+    return 128 + (size_t)sb_stages<S>() * StAddr<S>::RS * 32 * sizeof(S) + SB_WARPS * 3 * 32 * sizeof(T);
+}
+template <typename S>
+constexpr int sb_ctas_per_sm() { return sizeof(S) == 2 ? 3 : 2; }
+
+template <typename T, int MODE, typename S>
+__global__ void __launch_bounds__(SB_BS) k_st_bulk(int nx, int ny, int nz, const uint8_t* __restrict__ vact,
+                                                    const S* __restrict__ st, const T* __restrict__ u,
+                                                    const T* __restrict__ f, T* __restrict__ out, T* __restrict__ d,
+                                                    T omega, const double* __restrict__ coef, int kstep,
+                                                    double* __restrict__ errslot) {
+    constexpr int RS = StAddr<S>::RS, NST = sb_stages<S>();
+    constexpr uint32_t BLK_BYTES = RS * 32 * sizeof(S);
+    constexpr long BLK_ELEMS = RS * 32;
+    extern __shared__ __align__(128) unsigned char sm[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
+    S* stg = reinterpret_cast<S*>(sm + 128);
+    T* red = reinterpret_cast<T*>(sm + 128 + NST * BLK_BYTES);
+    T ca = T(0), cb = T(0);
+    if (MODE == 3) {
+        const double a_ = coef[2 * kstep], b_ = coef[2 * kstep + 1];
+        ca = (T)a_;
+        cb = (T)b_;
+    }
+    const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
+    const long nv = (long)vx * vy * vz;
+    const long nblk = (nv + 31) / 32;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const long nmine = (long)blockIdx.x < nblk ? (nblk - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    if (tid == 0) {
+        for (int s = 0; s < NST; s++) rttc::mbar_init(&bar[s], 1);
+        rttc::fence_mbar_init();
+    }
+    __syncthreads();
+    // thread 0: the stencil run of this CTA's i-th block into stage i % NST
+    auto issue = [&](long i) {
+        const long b = blockIdx.x + i * (long)gridDim.x;
+        uint64_t* br = &bar[i % NST];
+        rttc::mbar_expect_tx(br, BLK_BYTES);
+        rttc::bulk_g2s(stg + (i % NST) * BLK_ELEMS, st + b * BLK_ELEMS, BLK_BYTES, br);
+    };
+    if (tid == 0)
+        for (long i = 0; i < NST - 1 && i < nmine; i++) issue(i);
+    long i = 0, issued = nmine < NST - 1 ? nmine : NST - 1;
+    bool ok = true;
+    for (; i < nmine; i++) {
+        // block i + NST - 1 goes into the stage block i - 1 used (released by the barrier ending iteration i - 1)
+        if (issued < nmine) {
+            if (tid == 0) issue(issued);
+            issued++;
+        }
+        const int s = (int)(i % NST);
+        const bool w = rttc::mbar_wait(&bar[s], (uint32_t)((i / NST) & 1));
+        if (!__syncthreads_and(w)) {
+            ok = false;
+            break;
+        }
+        const S* sb = stg + s * BLK_ELEMS + lane;  // row j of this lane's node at sb[32 j]
+        const long v = (blockIdx.x + i * (long)gridDim.x) * 32 + lane;
+        const bool inb = v < nv;
+        const bool act = inb && vact[v];
+        T Au[3] = {T(0), T(0), T(0)};
+        if (act) {
+            const int x = (int)(v % vx), y = (int)((v / vx) % vy), z = (int)(v / ((long)vx * vy));
+#pragma unroll
+            for (int kk = 0; kk < 4; kk++) {
+                const int k = warp + SB_WARPS * kk;
+                if (k >= 27) break;
+                const int jx = x + k % 3 - 1, jy = y + (k / 3) % 3 - 1, jz = z + k / 9 - 1;
+                if (jx < 0 || jy < 0 || jz < 0 || jx >= vx || jy >= vy || jz >= vz) continue;
+                const long nj = jx + (long)vx * (jy + (long)vy * jz);
+                const T u0 = u[nj], u1 = u[nv + nj], u2 = u[2 * nv + nj];
+                const S* sk = sb + k * 9 * 32;
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    T a0 = (T)st_val(sk + (3 * r) * 32), a1 = (T)st_val(sk + (3 * r + 1) * 32),
+                      a2 = (T)st_val(sk + (3 * r + 2) * 32);
+                    if (sizeof(S) == 2 && k == 13) {
+                        a0 += (T)st_val(sb + (243 + 3 * r) * 32);
+                        a1 += (T)st_val(sb + (243 + 3 * r + 1) * 32);
+                        a2 += (T)st_val(sb + (243 + 3 * r + 2) * 32);
+                    }
+                    Au[r] += a0 * u0 + a1 * u1 + a2 * u2;
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 3; r++) red[(warp * 3 + r) * 32 + lane] = Au[r];
+        __syncthreads();
+        if (warp < 3 && inb) {
+            const int q = warp;
+            T A3[3];
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                A3[r] = red[r * 32 + lane];
+#pragma unroll
+                for (int w2 = 1; w2 < SB_WARPS; w2++) A3[r] += red[(3 * w2 + r) * 32 + lane];
+            }
+            const long oq = (long)q * nv + v;
+            const T Aq = q == 0 ? A3[0] : (q == 1 ? A3[1] : A3[2]);
+            if (MODE == 0) {
+                out[oq] = act ? f[oq] - Aq : T(0);
+            } else {
+                T res = T(0), dn = T(0);
+                if (act) {
+                    T S9[9];
+#pragma unroll
+                    for (int e = 0; e < 9; e++) S9[e] = st_centre<T>(sb, 32, e);
+                    const T a0 = S9[0], b0 = S9[1], c0 = S9[2], d0 = S9[3], e0 = S9[4], f0 = S9[5], g0 = S9[6],
+                            h0 = S9[7], k0 = S9[8];
+                    const T A = e0 * k0 - f0 * h0, B = -(d0 * k0 - f0 * g0), Cc = d0 * h0 - e0 * g0;
+                    const T id = T(1) / (a0 * A + b0 * B + c0 * Cc);
+                    const T i0 = q == 0 ? A : (q == 1 ? B : Cc);
+                    const T i1 = q == 0 ? -(b0 * k0 - c0 * h0) : (q == 1 ? (a0 * k0 - c0 * g0) : -(a0 * h0 - b0 * g0));
+                    const T i2 = q == 0 ? (b0 * f0 - c0 * e0) : (q == 1 ? -(a0 * f0 - c0 * d0) : (a0 * e0 - b0 * d0));
+                    const T r0 = f[v] - A3[0], r1 = f[nv + v] - A3[1], r2 = f[2 * nv + v] - A3[2];
+                    const T zq = (i0 * id) * r0 + (i1 * id) * r1 + (i2 * id) * r2;
+                    if (MODE == 2) {
+                        res = u[oq] + omega * zq;
+                    } else {
+                        dn = (kstep == 0 ? T(0) : ca * d[oq]) + cb * zq;
+                        res = u[oq] + dn;
+                    }
+                }
+                out[oq] = res;
+                if (MODE == 3) d[oq] = dn;
+            }
+        }
+        __syncthreads();  // the reduction buffer and stage s are free again
+    }
+    if (!ok) {
+        for (long j = i; j < issued; j++) rttc::mbar_wait(&bar[j % NST], (uint32_t)((j / NST) & 1));
+        if (tid == 0) errslot[0] = 1.0;
+        for (long j = i; j < nmine; j++)
+            for (int t = tid; t < 96; t += SB_BS) {
+                const long v = (blockIdx.x + j * (long)gridDim.x) * 32 + (t & 31);
+                if (v < nv) out[(long)(t >> 5) * nv + v] = T(NAN);
+            }
     }
 }
 
@@ -575,10 +737,46 @@ const double* stp<double>(rt_level& L) { return L.st; }
 template <>
 const float* stp<float>(rt_level& L) { return L.st32; }
 
+// the FP32 level kernels: bulk-copy stencil kernel over the blocked FP32 (or BF16) copy
+template <int MODE, typename S>
+static int launch_bulk(rt_hier* h, int lvl, const char* name, const S* st, const float* u, const float* f, float* out,
+                       float* d, double omega, const double* coef, int kstep) {
+    rt_level& L = h->L[lvl];
+    const long nblk = (L.nv + 31) / 32;
+    const long cap = (long)h->ctx->sm_count * sb_ctas_per_sm<S>();
+    const unsigned grid = (unsigned)(nblk < cap ? nblk : cap);
+    return rt_launch(h->ctx, name, [&] {
+        k_st_bulk<float, MODE, S><<<grid, SB_BS, sb_smem<float, S>(), h->ctx->stream>>>(
+            L.nx, L.ny, L.nz, L.vact, st, u, f, out, d, (float)omega, coef, kstep, h->scal + RT_SCAL_ERR);
+    });
+}
+
+// the lane-split kernel on an FP32 / BF16 blocked copy
+template <int MODE, typename S>
+static int launch_split(rt_hier* h, int lvl, const char* name, const S* st, const float* u, const float* f, float* out,
+                        float* d, double omega, const double* coef, int kstep) {
+    rt_level& L = h->L[lvl];
+    return rt_launch(h->ctx, name, [&] {
+        k_st_split4<float, MODE, S><<<grid_for(h->ctx, 4 * L.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(
+            L.nx, L.ny, L.nz, L.vact, st, u, f, out, d, (float)omega, coef, kstep);
+    });
+}
+
+template <int MODE, typename S>
+static int launch_f32(rt_hier* h, int lvl, const char* name, const S* st, const float* u, const float* f, float* out,
+                      float* d, double omega, const double* coef, int kstep) {
+    if (h->st_variant[sizeof(S) == 2 ? 1 : 0] == 1)
+        return launch_bulk<MODE, S>(h, lvl, name, st, u, f, out, d, omega, coef, kstep);
+    return launch_split<MODE, S>(h, lvl, name, st, u, f, out, d, omega, coef, kstep);
+}
+
 template <typename T>
 int st_residual(rt_hier* h, int lvl, const T* u, const T* f, T* r) {
     rt_level& L = h->L[lvl];
-    return rt_launch(h->ctx, LVL_NAME(lvl, sizeof(T) == 8, "st_residual"), [&] {
+    if constexpr (sizeof(T) == 4)
+        return launch_f32<0, float>(h, lvl, LVL_NAME(lvl, false, "st_residual"), L.st32, u, f, r, nullptr, 0.0,
+                                    nullptr, 0);
+    return rt_launch(h->ctx, LVL_NAME(lvl, true, "st_residual"), [&] {
         k_st_split4<T, 0><<<grid_for(h->ctx, 4 * L.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(
             L.nx, L.ny, L.nz, L.vact, stp<T>(L), u, f, r, nullptr, T(0), nullptr, 0);
     });
@@ -608,13 +806,14 @@ static bool use_bf16(rt_hier* h, rt_level& L) {
 template <typename T>
 int st_jacobi(rt_hier* h, int lvl, const T* u, const T* f, T* unew, double omega) {
     rt_level& L = h->L[lvl];
-    if constexpr (sizeof(T) == 4)
+    if constexpr (sizeof(T) == 4) {
         if (use_bf16<T>(h, L))
-            return rt_launch(h->ctx, lvl == 1 ? "st_jacobi_bf16_l1" : "st_jacobi_bf16", [&] {
-                k_st_split4<T, 2, uint16_t><<<grid_for(h->ctx, 4 * L.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(
-                    L.nx, L.ny, L.nz, L.vact, L.st16, u, f, unew, nullptr, (T)omega, nullptr, 0);
-            });
-    return rt_launch(h->ctx, LVL_NAME(lvl, sizeof(T) == 8, "st_jacobi"), [&] {
+            return launch_f32<2, uint16_t>(h, lvl, lvl == 1 ? "st_jacobi_bf16_l1" : "st_jacobi_bf16", L.st16, u, f,
+                                           unew, nullptr, omega, nullptr, 0);
+        return launch_f32<2, float>(h, lvl, LVL_NAME(lvl, false, "st_jacobi"), L.st32, u, f, unew, nullptr, omega,
+                                    nullptr, 0);
+    }
+    return rt_launch(h->ctx, LVL_NAME(lvl, true, "st_jacobi"), [&] {
         k_st_split4<T, 2><<<grid_for(h->ctx, 4 * L.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(
             L.nx, L.ny, L.nz, L.vact, stp<T>(L), u, f, unew, nullptr, (T)omega, nullptr, 0);
     });
@@ -623,13 +822,14 @@ int st_jacobi(rt_hier* h, int lvl, const T* u, const T* f, T* unew, double omega
 template <typename T>
 int st_cheby(rt_hier* h, int lvl, const T* u, const T* f, T* unew, T* d, const double* coef, int kstep) {
     rt_level& L = h->L[lvl];
-    if constexpr (sizeof(T) == 4)
+    if constexpr (sizeof(T) == 4) {
         if (use_bf16<T>(h, L))
-            return rt_launch(h->ctx, lvl == 1 ? "st_cheby_bf16_l1" : "st_cheby_bf16", [&] {
-                k_st_split4<T, 3, uint16_t><<<grid_for(h->ctx, 4 * L.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(
-                    L.nx, L.ny, L.nz, L.vact, L.st16, u, f, unew, d, T(0), coef, kstep);
-            });
-    return rt_launch(h->ctx, LVL_NAME(lvl, sizeof(T) == 8, "st_cheby"), [&] {
+            return launch_f32<3, uint16_t>(h, lvl, lvl == 1 ? "st_cheby_bf16_l1" : "st_cheby_bf16", L.st16, u, f,
+                                           unew, d, 0.0, coef, kstep);
+        return launch_f32<3, float>(h, lvl, LVL_NAME(lvl, false, "st_cheby"), L.st32, u, f, unew, d, 0.0, coef,
+                                    kstep);
+    }
+    return rt_launch(h->ctx, LVL_NAME(lvl, true, "st_cheby"), [&] {
         k_st_split4<T, 3><<<grid_for(h->ctx, 4 * L.nv, ST_BS), ST_BS, 0, h->ctx->stream>>>(
             L.nx, L.ny, L.nz, L.vact, stp<T>(L), u, f, unew, d, T(0), coef, kstep);
     });
@@ -741,6 +941,24 @@ int galerkin_from_stencil(rt_hier* h, int lvl) {
 
 int d2f(rt_hier* h, long n, const double* a, float* b) {
     return rt_launch(h->ctx, "d2f", [&] { k_d2f<<<grid_for(h->ctx, n, 256), 256, 0, h->ctx->stream>>>(n, a, b); });
+}
+
+// dynamic shared-memory limits of the bulk-copy stencil kernels, set once per device
+int init_stencil_kernels(rt_ctx* c) {
+    cudaError_t e[5] = {
+        cudaFuncSetAttribute(k_st_bulk<float, 0, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sb_smem<float, float>()),
+        cudaFuncSetAttribute(k_st_bulk<float, 2, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sb_smem<float, float>()),
+        cudaFuncSetAttribute(k_st_bulk<float, 3, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sb_smem<float, float>()),
+        cudaFuncSetAttribute(k_st_bulk<float, 2, uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sb_smem<float, uint16_t>()),
+        cudaFuncSetAttribute(k_st_bulk<float, 3, uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sb_smem<float, uint16_t>())};
+    for (cudaError_t x : e)
+        if (x != cudaSuccess) return rt_fail(c, RT_ECUDA, "stencil kernel attributes: %s", cudaGetErrorString(x));
+    return RT_OK;
 }
 
 // the FP32 (and, with rt_params.coarse_bf16, BF16) smoother copies of level lvl's stencils

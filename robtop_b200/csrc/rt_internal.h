@@ -85,6 +85,10 @@ struct rt_hier {
     rt_params P;
     rt_tile_cfg tune[2][4];          // [FP32, FP64][residual, applyK, jacobi, chebyshev]
     double tune_us[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};  // measured time of the chosen shape
+    // stencil-level kernels of the FP32 smoother [FP32 stencils, BF16 stencils]: 0 lane-split
+    // (4 lanes per node, loads through L1), 1 bulk-copy (32-node stencil runs staged in shared memory)
+    int st_variant[2] = {0, 1};
+    double st_us[2][2] = {{0, 0}, {0, 0}};  // [stencil type][variant] level-1 Chebyshev step (rt_autotune)
     double* dinv64 = nullptr;        // [6][nv] inverted diagonal blocks of the finest level
     float* dinv32 = nullptr;
     std::vector<rt_level> L;
@@ -179,6 +183,7 @@ static inline unsigned rt_blocks(long n, int bs) { return (unsigned)((n + bs - 1
 // rho_k = 1/(2 sigma - rho_{k-1}), a_k = rho_k rho_{k-1}, b_k = 2 rho_k / delta.
 #define RT_CHEBY_LO_FRAC (1.0 / 30.0)
 #define RT_CHEBY_HI_FRAC 1.1
+#define RT_SCAL_ERR 295   // set to 1 by a stencil kernel whose bounded copy wait ran out
 #define RT_SCAL_LMAX 300  // device scalar slots holding lmax(D^-1 A) per level
 // (a_k, b_k), k < RT_CHEBY_MAXK, per level at RT_SCAL_CHEB + 2 RT_CHEBY_MAXK lvl (levels 0..14);
 // the 16th table serves kernel timing before any stencil exists
@@ -217,6 +222,7 @@ template <typename T>
 int st_cheby(rt_hier* h, int lvl, const T* u, const T* f, T* unew, T* d, const double* coef, int kstep);
 int penalty_weights(rt_hier* h);
 int init_tile_kernels(rt_ctx* c);
+int init_stencil_kernels(rt_ctx* c);
 int fine_dinv(rt_hier* h);
 template <typename T, int MODE>
 int fine_march(rt_hier* h, const T* u, const T* f, T* out, double omega, T* dvec, const double* coef, int kstep);

@@ -323,6 +323,13 @@ class HierarchyGrid:
                 self._c(A.lib().rt_tuning_info(self._h, prec, m, C.byref(v), C.byref(ty), C.byref(zc), C.byref(us)))
                 out[f"{mname}_{pname}"] = {"variant": ["smem_tile", "register_march", "register_march_prefetch", "smem_tile_pipelined"][v.value], "rows": ty.value,
                                            "zchunk": zc.value, "us": round(us.value, 2)}
+        for st, sname in ((0, "f32"), (1, "bf16")):
+            v, u0, u1 = C.c_int(), C.c_double(), C.c_double()
+            self._c(A.lib().rt_level_kernel_info(self._h, st, C.byref(v), C.byref(u0), C.byref(u1)))
+            if u0.value > 0:
+                out[f"stencil_chebyshev_{sname}"] = {"variant": ["lane_split", "bulk_copy"][v.value],
+                                                     "us": {"lane_split": round(u0.value, 2),
+                                                            "bulk_copy": round(u1.value, 2)}}
         return out
 
     def smoother_lmax(self, level):

@@ -169,6 +169,40 @@ def test_fp32_kernel_variants_in_pcg(pair, variant, ty, zc):
     G.update_stencil()
 
 
+@pytest.mark.parametrize("bf16,variant", [(0, 0), (0, 1), (1, 0), (1, 1)])
+def test_level_kernel_variants_in_pcg(pair, bf16, variant):
+    """Both stencil-level kernels of the FP32 smoother (lane-split, bulk-copy), on the FP32 and the
+    BF16 stencil copies, drive the mixed-precision PCG to 1e-6 in the FP64 residual."""
+    cfg, ctx, G, H = pair
+    b = _rand_vec(G, 0, 82)
+    if cfg["mode"] in (rb.MODE_WSCF, rb.MODE_WSFF):
+        b[np.tile(cfg["vfix"].ravel().astype(bool), 3)] = 0
+    else:
+        Ru = np.zeros(6 * b.size)
+        O.lib().or_rigid_nodes(H.lv(0), O.ptr(Ru))
+        O.lib().or_displacement_project(b.size // 3, O.ptr(Ru), O.ptr(b))
+    params = G.params
+    params.precision, params.smoother = rb.FP32, rb.SMOOTH_CHEBY
+    params.pre_sweeps = params.post_sweeps = 4
+    params.coarse_bf16 = bf16
+    G.set_params(params)
+    G.update_stencil()
+    rb._capi.check(rb.lib().rt_set_level_kernel(G.handle, bf16, variant), ctx.handle)
+    G[0].setForce(b)
+    G[0].reset_displacement()
+    info = G.pcg(1e-6, 1000)
+    assert info.status == 0 and info.rel_residual <= 1e-6
+    r = (b - H.applyK(G[0].getDisplacement())) * np.tile(H.arrs[0]["vact"], 3)
+    assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.01e-6
+    rb._capi.check(rb.lib().rt_set_level_kernel(G.handle, 0, 0), ctx.handle)
+    rb._capi.check(rb.lib().rt_set_level_kernel(G.handle, 1, 1), ctx.handle)
+    params.precision, params.smoother = rb.FP64, rb.SMOOTH_SGS
+    params.pre_sweeps = params.post_sweeps = 1
+    params.coarse_bf16 = 0
+    G.set_params(params)
+    G.update_stencil()
+
+
 def test_autotune_keeps_results(pair):
     cfg, ctx, G, H = pair
     shapes = G.autotune(reps=2)
