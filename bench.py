@@ -34,10 +34,36 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = dict(nx=128, ny=128, nz=64, seed=0, k=16, tol=1e-6)
 # plain: the reference's V-cycle made symmetric (8-colour GS, forward pre / backward post), all FP64
-# mixed: FP32 V-cycle with Chebyshev(4) smoothing inside FP64 flexible CG, FP64 coarsest solve,
-#        FP64 V-cycles once the FP32 ones stall
-FORMS = {"plain": dict(precision="FP64", smoother="SMOOTH_SGS", sweeps=1, coarse_sweeps=0),
-         "mixed": dict(precision="FP32", smoother="SMOOTH_CHEBY", sweeps=4, coarse_sweeps=0)}
+# mixed: FP32 V-cycle with Chebyshev(2) smoothing (8 steps on the coarse levels) inside FP64 flexible
+#        CG, FP64 coarsest solve, FP64 V-cycles once the FP32 ones stall
+FORMS = {"plain": dict(precision="FP64", smoother="SMOOTH_SGS", sweeps=1, coarse_sweeps=0, cycle_gamma=1,
+                       coarse_bf16=0),
+         "mixed": dict(precision="FP32", smoother="SMOOTH_CHEBY", sweeps=2, coarse_sweeps=8, cycle_gamma=1,
+                       coarse_bf16=0)}
+# on the 511x256x256 arch the W-cycle (coarse corrections twice per visit below level 1) wins
+FORMS_C5 = {"plain": FORMS["plain"],
+            "mixed": dict(precision="FP32", smoother="SMOOTH_CHEBY", sweeps=2, coarse_sweeps=0, cycle_gamma=2,
+                          coarse_bf16=0),
+            "fp64_same_cycle": dict(precision="FP64", smoother="SMOOTH_CHEBY", sweeps=2, coarse_sweeps=0,
+                                    cycle_gamma=2, coarse_bf16=0)}
+
+
+def apply_form(rb, G, form):
+    p = G.params
+    p.precision = getattr(rb, form["precision"])
+    p.smoother = getattr(rb, form["smoother"])
+    p.pre_sweeps = p.post_sweeps = form["sweeps"]
+    p.coarse_sweeps = form["coarse_sweeps"]
+    p.cycle_gamma = form["cycle_gamma"]
+    p.coarse_bf16 = form["coarse_bf16"]
+    G.set_params(p)
+
+
+def form_text(form):
+    return (f"{form['precision']} V-cycle{' (W below level 1)' if form['cycle_gamma'] == 2 else ''}, "
+            f"{form['smoother'][7:].lower()}({form['sweeps']}) smoothing"
+            f"{', ' + str(form['coarse_sweeps']) + ' steps on coarse levels' if form['coarse_sweeps'] else ''}"
+            f"{', BF16 coarse stencils' if form['coarse_bf16'] else ''}")
 METRIC = "worst-case solve (Lanczos k=16, MG-PCG inner solves to rel. residual 1e-6) on 128x128x64"
 
 
@@ -176,9 +202,12 @@ def algorithmic_bytes(name, nv, ne, s):
 
 
 # DRAM bytes (read + write) per launch from one ncu capture of the kernel on this workload,
-# per node (71.0 MB read + 3.3 MB written over 1,081,665 nodes, register-marching variant,
-# rows 2, z-chunk 8); none for variants without a valid capture
-NCU_TRAFFIC_PER_NODE = {("fine_cheby_f32", "register_march"): (71.0e6 + 3.3e6) / 1081665}
+# per node (1,081,665 nodes): register-marching variant (rows 2, z-chunk 8) 71.0 MB read +
+# 3.3 MB written; pipelined tile variant (rows 8, z-chunk 32) 45.3 MB read + 0.3 MB written
+# (its 26 MB of writes were still in L2 when the launch ended).  None for variants
+# without a capture.
+NCU_TRAFFIC_PER_NODE = {("fine_cheby_f32", "register_march"): (71.0e6 + 3.3e6) / 1081665,
+                        ("fine_cheby_f32", "smem_tile_pipelined"): (45.328e6 + 0.292e6) / 1081665}
 
 
 def roofline(ctx, stats, G, peaks, tuning=None):
@@ -357,7 +386,7 @@ def run_kernel(args):
             rb._capi.check(rb.lib().rt_set_tuning(G.handle, prec, mode, variant, ty, zc), ctx.handle)
             names = ["residual", "applyK", "jacobi", "chebyshev"]
             shapes = {f"{names[mode]}_{'f32' if prec == rb.FP32 else 'f64'}":
-                      {"variant": ["smem_tile", "register_march", "register_march_prefetch", "smem_tile_pipelined"][variant], "rows": ty,
+                      {"variant": ["smem_tile", "register_march", "register_march_prefetch", "smem_tile_pipelined", "smem_tile_pairs_f32"][variant], "rows": ty,
                        "zchunk": zc}}
         else:
             shapes = G.autotune()
@@ -416,7 +445,7 @@ def run_batched(args):
     """Batched solves: 12 cantilever instances with per-axis sizes drawn from {48..160} (seed 1),
     smoothed random densities (seeds 2+i), x=0 clamped with the bottom-edge tip load, plus 8
     right-hand sides (random top-face loads) on one 256x256x128 worst-case box, all 20 MG-PCG
-    solves (FP32 Chebyshev(4) V-cycles in FP64 CG, to 1e-6 from zero) in ONE graph launch
+    solves (the mixed form: FP32 Chebyshev V-cycles in FP64 CG, to 1e-6 from zero) in ONE graph launch
     (rt_pcg_batch), timed against the same 20 solves one after another (rt_pcg)."""
     import torch
 
@@ -437,6 +466,7 @@ def run_batched(args):
         cfg = configs.cantilever(nx, ny, nz)
         cfg["rho"] = configs.smoothed_density(cfg["eact"].shape, 2 + i)
         G = rb.HierarchyGrid(ctx, params(cfg["mode"]))
+        apply_form(rb, G, FORMS["mixed"])
         G.genFromBox(cfg["eact"])
         G[0].setRho(cfg["rho"].ravel())
         G.set_support(cfg["vfix"])
@@ -447,6 +477,7 @@ def run_batched(args):
         rhs.append(cfg["fload"].ravel())
     big_cfg = configs.worst_case_box(256, 256, 128, seed=0)
     big = rb.HierarchyGrid(ctx, params(big_cfg["mode"]))
+    apply_form(rb, big, FORMS["mixed"])
     big.genFromBox(big_cfg["eact"])
     big[0].setRho(big_cfg["rho"].ravel())
     big.set_support(big_cfg["vfix"])
@@ -513,7 +544,7 @@ def run_batched(args):
             "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
             "config": {"workload": "12 cantilevers (sizes " + ";".join("x".join(map(str, s)) for s in sizes) +
                                    ") + 8 top-face loads on the 256x256x128 worst-case box",
-                       "form": "FP32 Chebyshev(4) V-cycle in FP64 flexible CG, per-step reset of u on the device",
+                       "form": form_text(FORMS["mixed"]) + " in FP64 flexible CG, per-step reset of u on the device",
                        "sequential_ms_per_step": ts / args.steps, "batch_speedup": ts / tb,
                        "iterations": [i.iterations for i in infos_b],
                        "iterations_sequential": [i.iterations for i in infos_s],
@@ -648,6 +679,7 @@ def run_c5(args):
                           volume_ratio=0.4, design_step=0.06, damp_ratio=0.5, filter_radius=2.0,
                           precision=rb.FP32, smoother=rb.SMOOTH_CHEBY, pre_sweeps=4, post_sweeps=4)
     G = rb.HierarchyGrid(ctx, p)
+    apply_form(rb, G, FORMS_C5["mixed"])
     G.genFromBox(cfg["eact"])
     G[0].setRho(cfg["rho"].ravel())
     G.set_support(cfg["vfix"])
@@ -686,14 +718,13 @@ def run_c5(args):
     clk = clocks.stop()
     fb0 = int(rb.lib().rt_hier_precision_fallbacks(G.handle))
     forms = {}
-    for name, prec, sm, sw in (("mixed", rb.FP32, rb.SMOOTH_CHEBY, 4), ("plain", rb.FP64, rb.SMOOTH_SGS, 1)):
-        q = G.params
-        q.precision, q.smoother, q.pre_sweeps, q.post_sweeps = prec, sm, sw, sw
-        G.set_params(q)
+    for name in ("mixed", "plain", "fp64_same_cycle"):
+        apply_form(rb, G, FORMS_C5[name])
         ms, (lam, info) = timed(lambda: step(rb, G, 7))
         forms[name] = (ms, lam, info.inner_iterations)
     m_ms, m_lam, m_it = forms["mixed"]
     p_ms, p_lam, p_it = forms["plain"]
+    s_ms, s_lam, s_it = forms["fp64_same_cycle"]
     line = {"metric": "worst-case optimisation on the 511x256x256 arch: OC iterations (stencil update, Lanczos k=16 "
                       "worst-case solve to 1e-6, sensitivity, filter, OC update)",
             "value": args.steps / (ms_oc * 1e-3), "unit": "OC iterations/s", "n_gpus": 1, "steps": args.steps,
@@ -702,8 +733,12 @@ def run_c5(args):
             "config": {"workload": "arch 511x256x256 (tunnel radius 96, 16x16 pads), wscf, V 0.4, R 2, move 0.06, "
                                    "eta 0.5, p 3, rho0 0.4",
                        "worst_case_lambda_per_step": lams, "setup_s": t_setup,
+                       "form_mixed": form_text(FORMS_C5["mixed"]),
                        "worst_case_solve_ms_mixed": m_ms, "worst_case_solve_ms_plain_fp64": p_ms,
                        "speedup_mixed_vs_plain": p_ms / m_ms,
+                       "worst_case_solve_ms_fp64_same_cycle": s_ms, "speedup_mixed_vs_fp64_same_cycle": s_ms / m_ms,
+                       "inner_iterations_fp64_same_cycle": s_it,
+                       "lambda_rel_diff_fp64_same_cycle": abs(s_lam - p_lam) / abs(p_lam),
                        "lambda_mixed": m_lam, "lambda_plain": p_lam,
                        "lambda_rel_diff": abs(m_lam - p_lam) / abs(p_lam),
                        "inner_iterations_mixed": m_it, "inner_iterations_plain": p_it,
@@ -779,13 +814,7 @@ def main():
     tuning = G.autotune()
     results = {}
     for prec in ((rb.FP64, rb.FP32) if args.forms == "both" else (rb.FP32,)):
-        form = FORMS["plain" if prec == rb.FP64 else "mixed"]
-        p = G.params
-        p.precision = prec
-        p.smoother = getattr(rb, form["smoother"])
-        p.pre_sweeps = p.post_sweeps = form["sweeps"]
-        p.coarse_sweeps = form["coarse_sweeps"]
-        G.set_params(p)
+        apply_form(rb, G, FORMS["plain" if prec == rb.FP64 else "mixed"])
         for w in range(max(args.warmup, 3)):
             step(rb, G, 10 + w)
         if dist:
@@ -825,9 +854,8 @@ def main():
         "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
         "config": {"workload": "worst-case 128x128x64 (smoothed random density, z=0 clamped, top-face load set, "
                                "wsff), Lanczos k=16, inner MG-PCG to 1e-6, stencil assembly included",
-                   "form": "mixed: FP32 V-cycle (Chebyshev(4) smoothing, FP64 coarsest solve) inside FP64 "
-                           "flexible CG, one CUDA graph per solve; plain (fp64_ms_per_step): FP64 symmetric-GS "
-                           "V-cycle",
+                   "form": "mixed: " + form_text(FORMS["mixed"]) + ", FP64 coarsest solve, inside FP64 flexible "
+                           "CG, one CUDA graph per solve; plain (fp64_ms_per_step): FP64 symmetric-GS V-cycle",
                    "fp64_ms_per_step": r64["ms"] / args.steps if r64 else None,
                    "speedup_vs_fp64": r64["ms"] / r32["ms"] if r64 else None,
                    "lambda_mixed": lam32, "lambda_fp64": lam64,

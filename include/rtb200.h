@@ -226,6 +226,10 @@ int rt_set_tuning(rt_hier* h, int precision, int mode, int variant, int ty, int 
 /* time reps launches of one finest-level kernel at its current shape on random data
  * (device time per launch in microseconds, CUDA events on the context stream) */
 int rt_bench_fine_kernel(rt_hier* h, int precision, int mode, int reps, double* us_per_launch);
+/* run one FP32 finest-level kernel at its current shape on level 0's vectors (u, f rounded to FP32)
+ * and widen its result into level 0's residual vector: mode 0 f - K u, 1 K u, 2 a Jacobi step
+ * u + omega D^-1 (f - K u), 3 the first Chebyshev step (needs rt_update_stencil) */
+int rt_fine_kernel_f32(rt_hier* h, int mode, double omega);
 /* the same for one stencil level lvl (1 .. coarsest-1): mode 0 residual, 2 Jacobi, 3 Chebyshev step;
  * precision RT_FP64 or RT_FP32 (FP32 smoothing reads the BF16 stencils when rt_params.coarse_bf16 is set).
  * Overwrites the level's vectors; needs rt_update_stencil. */

@@ -591,6 +591,7 @@ extern "C" int rt_hier_set_params(rt_hier* h, const rt_params* p) {
     h->P = *p;
     if (ke) RT_CHECK(upload_KE(h));
     h->stencil_ready = false;
+    h->graph_epoch++;  // captured graphs bake in the settings and the stencil copies they read
     return RT_OK;
 }
 
@@ -1407,12 +1408,20 @@ static int pcg_body(rt_hier* h, double* x, double* r, bool no_support, cudaGraph
 // captured iteration; the body's last kernel decides whether to run again
 static int pcg_graph_run(rt_hier* h, double* x, double* r, bool no_support) {
     rt_ctx* c = h->ctx;
-    const uint64_t key = ((uint64_t)(uintptr_t)x * 1315423911ull) ^ ((uint64_t)h->P.precision << 1) ^
-                         ((uint64_t)h->P.smoother << 3) ^ ((uint64_t)h->P.pre_sweeps << 6) ^
-                         ((uint64_t)h->P.post_sweeps << 11) ^ ((uint64_t)no_support << 16) ^
-                         ((uint64_t)(h->P.jacobi_omega * 1e6) << 20) ^ ((uint64_t)h->graph_epoch << 40) ^
-                         ((uint64_t)(uintptr_t)h->unet * 2654435761ull) ^ ((uint64_t)h->P.cycle_gamma << 56) ^
-                         ((uint64_t)h->P.coarse_sweeps << 60);
+    // the captured graph depends on the vectors, the solver settings, the operator epoch (launch
+    // shapes, kernel variants, parameter changes) and the learned correction
+    uint64_t key = 1469598103934665603ull;
+    auto mix = [&](uint64_t v) { key = (key ^ v) * 1099511628211ull; };
+    mix((uint64_t)(uintptr_t)x);
+    mix((uint64_t)(uintptr_t)h->unet);
+    mix(h->graph_epoch);
+    mix((uint64_t)no_support);
+    mix((uint64_t)h->P.precision | ((uint64_t)h->P.smoother << 8) | ((uint64_t)h->P.pre_sweeps << 16) |
+        ((uint64_t)h->P.post_sweeps << 24) | ((uint64_t)h->P.cycle_gamma << 32) |
+        ((uint64_t)h->P.coarse_sweeps << 40) | ((uint64_t)h->P.coarse_bf16 << 48));
+    uint64_t om;
+    memcpy(&om, &h->P.jacobi_omega, 8);
+    mix(om);
     if (!h->pcg_exec || h->pcg_key != key) {
         if (h->pcg_exec) { cudaGraphExecDestroy(h->pcg_exec); h->pcg_exec = nullptr; }
         if (h->pcg_graph) { cudaGraphDestroy(h->pcg_graph); h->pcg_graph = nullptr; }
@@ -1995,12 +2004,15 @@ extern "C" int rt_autotune(rt_hier* h, int reps) {
         for (int zc : {8, 16, 32}) cands.push_back(rt_tile_cfg{0, ty, zc});
     for (int ty : {2, 4, 8})
         for (int zc : {8, 16, 32, 64}) cands.push_back(rt_tile_cfg{3, ty, zc});
+    for (int ty : {2, 4, 8})
+        for (int zc : {8, 16, 32, 64}) cands.push_back(rt_tile_cfg{4, ty, zc});  // FP32 only
     for (int prec = 0; prec < 2; prec++)
         for (int mode = 0; mode < 4; mode++) {
             rt_tile_cfg best_cfg = h->tune[prec][mode];
             double best = 1e30;
             for (const rt_tile_cfg& cfg : cands) {
                 if (cfg.zchunk > 2 * L.vz && cfg.zchunk != 4) continue;
+                if (cfg.variant == 4 && prec == 1) continue;
                 h->tune[prec][mode] = cfg;
                 const double t = time_fine_kernel(h, prec, mode, reps);
                 if (t < best) { best = t; best_cfg = cfg; }
@@ -2027,9 +2039,10 @@ extern "C" int rt_tuning_info(rt_hier* h, int precision, int mode, int* variant,
 }
 
 extern "C" int rt_set_tuning(rt_hier* h, int precision, int mode, int variant, int ty, int zchunk) {
-    if (!h || precision < 0 || precision > 1 || mode < 0 || mode > 3 || variant < 0 || variant > 3 || zchunk < 1)
+    if (!h || precision < 0 || precision > 1 || mode < 0 || mode > 3 || variant < 0 || variant > 4 || zchunk < 1)
         return RT_EINVAL;
     RT_NOT_WORKSPACE(h);
+    if (variant == 4 && precision == RT_FP64) return rt_fail(h->ctx, RT_EINVAL, "variant 4 (packed FP32 pairs) is FP32 only");
     if (variant != 2 && ty != 2 && ty != 4 && ty != 8) return rt_fail(h->ctx, RT_EINVAL, "rows per tile must be 2, 4 or 8");
     const int pr = precision == RT_FP64 ? 1 : 0;
     if (variant == 2 && ty != 2 && ty != 4) return rt_fail(h->ctx, RT_EINVAL, "prefetching rows per tile must be 2 or 4");
@@ -2054,6 +2067,26 @@ extern "C" int rt_bench_fine_kernel(rt_hier* h, int precision, int mode, int rep
     if (t >= 1e30) return rt_fail(c, RT_ECUDA, "kernel launch failed");
     if (us_per_launch) *us_per_launch = t;
     return RT_OK;
+}
+
+// one FP32 finest-level kernel at its current launch shape on level 0's vectors: u, f rounded to
+// FP32, the result (mode 0 residual f - K u, 1 K u, 2 Jacobi step, 3 first Chebyshev step) widened into r
+extern "C" int rt_fine_kernel_f32(rt_hier* h, int mode, double omega) {
+    if (!h || mode < 0 || mode > 3) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
+    RT_CHECK(refresh_fine(h));
+    if (mode == 3 && !h->stencil_ready) return rt_fail(h->ctx, RT_ESTATE, "rt_update_stencil has not run");
+    rt_level& L = h->L[0];
+    const long n = 3 * L.nv;
+    RT_CHECK(rtk::d2f(h, n, L.u, L.u32));
+    RT_CHECK(rtk::d2f(h, n, L.f, L.f32));
+    switch (mode) {
+        case 0: RT_CHECK(rtk::fine_residual<float>(h, L.u32, L.f32, L.r32)); break;
+        case 1: RT_CHECK(rtk::fine_applyK<float>(h, L.u32, L.r32)); break;
+        case 2: RT_CHECK(rtk::fine_jacobi<float>(h, L.u32, L.f32, L.r32, omega)); break;
+        default: RT_CHECK(rtk::fine_cheby<float>(h, L.u32, L.f32, L.r32, L.d32, cheby_table(h, 0), 0)); break;
+    }
+    return rtk::f2d(h, n, L.r32, L.r);
 }
 
 // one stencil-level kernel (residual, Jacobi or a Chebyshev step) on random inputs, timed with

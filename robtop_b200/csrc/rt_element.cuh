@@ -79,3 +79,44 @@ KtVals<T> make_kt(const rt_hier* h) {
 }
 
 }  // namespace rte
+
+namespace rte {
+
+// two elements at once in packed FP32 pairs (the .x / .y lanes are independent elements):
+// the same butterflies and 45 Kt products as element_apply<float>, as FADD2 / FFMA2 / FMUL2
+__device__ __forceinline__ float2 sub2(float2 p, float2 q) { return __ffma2_rn(q, make_float2(-1.f, -1.f), p); }
+
+__device__ __forceinline__ void hadamard8x2(float2* a, int c) {
+#pragma unroll
+    for (int bit = 1; bit < 8; bit <<= 1)
+#pragma unroll
+        for (int i = 0; i < 8; i++)
+            if (!(i & bit)) {
+                const float2 p = a[3 * i + c], q = a[3 * (i | bit) + c];
+                a[3 * i + c] = __fadd2_rn(p, q);
+                a[3 * (i | bit) + c] = sub2(p, q);
+            }
+}
+
+// a <- w * KE * a for two elements (w.x, w.y their weights)
+__device__ __forceinline__ void element_apply2(float2* a, const KtVals<float>& kt, float2 w) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) hadamard8x2(a, c);
+    float2 z[24];
+    // Kt's rows are sorted: the first product of a row initialises it
+#pragma unroll
+    for (int k = 0; k < 45; k++) {
+        const float2 kv = make_float2(kt.v[k], kt.v[k]);
+        if (k == 0 || KT_R[k - 1] != KT_R[k]) z[KT_R[k]] = __fmul2_rn(kv, a[KT_C[k]]);
+        else z[KT_R[k]] = __ffma2_rn(kv, a[KT_C[k]], z[KT_R[k]]);
+    }
+    // rows 0..2 (the rigid translations) of Kt are empty
+#pragma unroll
+    for (int i = 0; i < 3; i++) a[i] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int i = 3; i < 24; i++) a[i] = __fmul2_rn(w, z[i]);
+#pragma unroll
+    for (int c = 0; c < 3; c++) hadamard8x2(a, c);
+}
+
+}  // namespace rte

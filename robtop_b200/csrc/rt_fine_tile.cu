@@ -533,6 +533,247 @@ __global__ void __launch_bounds__(Tile<TY_>::BS, pipe_min_blocks<T, TY_>()) k_fi
 }
 
 
+// ---------------------------------------------------------------------------
+// FP32 pipelined tile kernel with element pairs: a thread applies KE to two x-neighbour
+// elements at once in packed FP32 pairs (FADD2 / FFMA2 / FMUL2), loading each pair of
+// vertex values with one 64-bit shared load.  The node layers are kept twice in shared
+// memory, as is and shifted by one node in x, so that both the (x, x+1) and the
+// (x+1, x+2) vertex pairs of an element pair are aligned 64-bit words.  Element rows
+// hold 34 slots (17 pairs; the 34th element is a zero-weight pad).  Otherwise the
+// schedule is k_fine_pipe's: element layer t+1 and node layer t per barrier interval.
+// ---------------------------------------------------------------------------
+template <int TY_>
+struct PTile {
+    static constexpr int TX = 32, TY = TY_;
+    static constexpr int EXP = 34, NEP = 17, EYT = TY + 1;  // element row pitch, pairs per row
+    static constexpr int NE2 = EXP * EYT;                   // element slots per layer
+    static constexpr int NPAIR = NEP * EYT;                 // element-pair threads
+    static constexpr int UXR = 34, UXP = 36, UYT = TY + 2;  // halo nodes per row, row pitch (zero pad)
+    static constexpr int NU_T = UXR * UYT;                  // halo nodes per layer
+    static constexpr int NU2 = UXP * UYT;                   // shared slots per layer and component
+    static constexpr int BS = ((NPAIR > TX * TY ? NPAIR : TX * TY) + 31) / 32 * 32;
+    static constexpr int U_PER_T = (NU_T + BS - 1) / BS;
+};
+
+template <int TY_>
+struct PairSmem {
+    float u[3][2][3][PTile<TY_>::NU2];  // node layer L in slot (L + 3) % 3; copy 1 = shifted by one node in x
+    float e[2][24][PTile<TY_>::NE2];    // element layer L in slot (L + 2) & 1
+    float w[4][PTile<TY_>::NE2];        // element layer L in slot (L + 4) & 3
+};
+
+template <int TY_>
+constexpr int pair_min_blocks() { return TY_ == 2 ? 7 : TY_ == 4 ? 4 : 2; }
+
+template <bool WS, int MODE, int TY_>
+__global__ void __launch_bounds__(PTile<TY_>::BS, pair_min_blocks<TY_>()) k_fine_pair(int nx, int ny, int nz, int zchunk,
+                                                        const uint8_t* __restrict__ vact,
+                                                        const float* __restrict__ wgt,
+                                                        const uint8_t* __restrict__ vfix, const rte::KtVals<float> kt,
+                                                        const float* __restrict__ u, const float* __restrict__ f,
+                                                        float* __restrict__ out, float omega, float* __restrict__ dvec,
+                                                        const double* __restrict__ coef, int kstep) {
+    using T = float;
+    using TS = PTile<TY_>;
+    constexpr int TX = TS::TX, TY = TS::TY, EXP = TS::EXP, NEP = TS::NEP, NE2 = TS::NE2, NPAIR = TS::NPAIR;
+    constexpr int UXR = TS::UXR, UXP = TS::UXP, NU_T = TS::NU_T, NU2 = TS::NU2, TILE_BS = TS::BS,
+                  U_PER_T = TS::U_PER_T;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    PairSmem<TY_>& S = *reinterpret_cast<PairSmem<TY_>*>(smraw);
+    T cheb_a = T(0), cheb_b = T(0);
+    if (MODE == 3) {
+        const double ca = coef[2 * kstep], cb = coef[2 * kstep + 1];
+        cheb_a = (T)ca;
+        cheb_b = (T)cb;
+    }
+    const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
+    const long nv = (long)vx * vy * vz;
+    const long plane = (long)vx * vy;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int zb = blockIdx.z * zchunk;
+    const int ze = min(zb + zchunk, vz);
+    const int tid = threadIdx.x;
+    const int nxl = tid % TX, nyl = tid / TX;
+    const int nxg = x0 + nxl, nyg = y0 + nyl;
+    const bool node_thread = tid < TX * TY && nxg < vx && nyg < vy;
+    const long vxy = node_thread ? nxg + (long)vx * nyg : 0;
+    // element pair of this thread: elements 2m, 2m+1 of element row prow (tile coordinates)
+    const int pm = tid % NEP, prow = tid / NEP;
+    const int ex0 = x0 - 1 + 2 * pm, eyg = y0 - 1 + prow;
+    const bool pair_thread = tid < NPAIR;
+    const bool ey_ok = pair_thread && eyg >= 0 && eyg < ny;
+    const bool e0_ok = ey_ok && ex0 >= 0 && ex0 < nx;                       // element 2m
+    const bool e1_ok = ey_ok && ex0 + 1 < nx && 2 * pm + 1 <= TX;           // element 2m+1 (2m+1 = 33: pad)
+    const long exy0 = e0_ok ? ex0 + (long)nx * eyg : 0;
+    long hxy[U_PER_T];
+    bool hok[U_PER_T];
+#pragma unroll
+    for (int j = 0; j < U_PER_T; j++) {
+        const int i = tid + j * TILE_BS;
+        const int xx = x0 - 1 + i % UXR, yy = y0 - 1 + i / UXR;
+        hok[j] = i < NU_T && xx >= 0 && yy >= 0 && xx < vx && yy < vy;
+        hxy[j] = hok[j] ? xx + (long)vx * yy : 0;
+    }
+    // zero the node-layer slots once: the pad columns are read by the pad element
+    for (int i = tid; i < 3 * 2 * 3 * NU2; i += TILE_BS) (&S.u[0][0][0][0])[i] = 0.f;
+
+    T pu[U_PER_T][3];
+    float2 pw = make_float2(0.f, 0.f);
+    auto fetch_layer = [&](int L) {
+#pragma unroll
+        for (int j = 0; j < U_PER_T; j++) {
+            T a = T(0), b = T(0), c = T(0);
+            if (hok[j] && L >= 0 && L < vz) {
+                const long v = hxy[j] + plane * L;
+                if (!(WS && vfix[v])) {
+                    a = u[v];
+                    b = u[nv + v];
+                    c = u[2 * nv + v];
+                }
+            }
+            pu[j][0] = a;
+            pu[j][1] = b;
+            pu[j][2] = c;
+        }
+    };
+    auto stash_layer = [&](int L) {
+        float(*dst)[3][NU2] = S.u[(L + 3) % 3];
+#pragma unroll
+        for (int j = 0; j < U_PER_T; j++) {
+            const int i = tid + j * TILE_BS;
+            if (i < NU_T) {
+                const int row = i / UXR, col = i % UXR;
+                const int o = row * UXP + col;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    dst[0][c][o] = pu[j][c];
+                    if (col >= 1) dst[1][c][o - 1] = pu[j][c];
+                }
+            }
+        }
+    };
+    auto fetch_w = [&](int ez) {
+        const bool zok = ez >= 0 && ez < nz;
+        const long base = (long)nx * ny * ez;
+        pw.x = (e0_ok && zok) ? wgt[exy0 + base] : 0.f;
+        pw.y = (e1_ok && zok) ? wgt[ex0 + 1 + (long)nx * eyg + base] : 0.f;
+    };
+    auto stash_w = [&](int ez) {
+        if (pair_thread) *reinterpret_cast<float2*>(&S.w[(ez + 4) & 3][prow * EXP + 2 * pm]) = pw;
+    };
+    auto element_phase = [&](int e) {
+        if (!pair_thread) return;
+        const float2 wv = *reinterpret_cast<const float2*>(&S.w[(e + 4) & 3][prow * EXP + 2 * pm]);
+        float2 a[24];
+        if (wv.x != 0.f || wv.y != 0.f) {
+            const float(*lo)[3][NU2] = S.u[(e + 3) % 3];
+            const float(*hi)[3][NU2] = S.u[(e + 4) % 3];
+#pragma unroll
+            for (int vtx = 0; vtx < 8; vtx++) {
+                const float(*src)[3][NU2] = (vtx & 4) ? hi : lo;
+                const int idx = (prow + ((vtx >> 1) & 1)) * UXP + 2 * pm;
+#pragma unroll
+                for (int c = 0; c < 3; c++) a[3 * vtx + c] = *reinterpret_cast<const float2*>(&src[vtx & 1][c][idx]);
+            }
+            rte::element_apply2(a, kt, wv);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 24; q++) a[q] = make_float2(0.f, 0.f);
+        }
+        float* dst = &S.e[(e + 2) & 1][0][0];
+#pragma unroll
+        for (int q = 0; q < 24; q++) *reinterpret_cast<float2*>(&dst[q * NE2 + prow * EXP + 2 * pm]) = a[q];
+    };
+
+    fetch_layer(zb - 1);
+    fetch_w(zb - 1);
+    __syncthreads();  // the zeroed slots before the first stores
+    stash_layer(zb - 1);
+    stash_w(zb - 1);
+    fetch_layer(zb);
+    stash_layer(zb);
+    fetch_layer(zb + 1);
+    stash_layer(zb + 1);
+    fetch_w(zb);
+    stash_w(zb);
+    __syncthreads();
+    element_phase(zb - 1);
+    fetch_layer(zb + 2);
+    fetch_w(zb + 1);
+    __syncthreads();
+
+    T acc[3] = {T(0), T(0), T(0)};
+    for (int t = zb - 1; t < ze; t++) {
+        if (t + 3 <= ze) stash_layer(t + 3);
+        if (t + 2 < ze) stash_w(t + 2);
+        if (t + 4 <= ze) fetch_layer(t + 4);
+        if (t + 3 < ze) fetch_w(t + 3);
+        const bool out_layer = t >= zb;
+        T fv[3] = {T(0), T(0), T(0)}, uo[3] = {T(0), T(0), T(0)}, dv[3] = {T(0), T(0), T(0)};
+        bool act = false, fixed = false;
+        long vout = 0;
+        if (node_thread && out_layer) {
+            vout = vxy + plane * t;
+            act = vact[vout];
+            fixed = WS && act && vfix[vout];
+            if (MODE != 1)
+#pragma unroll
+                for (int c = 0; c < 3; c++) fv[c] = f[c * nv + vout];
+            if (MODE >= 1)
+#pragma unroll
+                for (int c = 0; c < 3; c++) uo[c] = u[c * nv + vout];
+            if (MODE == 3 && kstep > 0)
+#pragma unroll
+                for (int c = 0; c < 3; c++) dv[c] = dvec[c * nv + vout];
+        }
+        if (t + 1 < ze) element_phase(t + 1);
+        if (node_thread) {
+            const T* E = &S.e[(t + 2) & 1][0][0];
+            if (out_layer) {
+#pragma unroll
+                for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+                    for (int dx = 0; dx < 2; dx++) {
+                        const int el = (nyl + dy) * EXP + nxl + dx;
+                        const int vtx = (1 - dx) + 2 * (1 - dy);
+#pragma unroll
+                        for (int c = 0; c < 3; c++) acc[c] += E[(3 * vtx + c) * NE2 + el];
+                    }
+                const long v = vout;
+                if (MODE == 0) {
+#pragma unroll
+                    for (int c = 0; c < 3; c++) out[c * nv + v] = act ? (fixed ? fv[c] : fv[c] - acc[c]) : T(0);
+                } else if (MODE == 1) {
+#pragma unroll
+                    for (int c = 0; c < 3; c++) out[c * nv + v] = act ? (fixed ? uo[c] : acc[c]) : T(0);
+                } else {
+                    T nu[3], dn[3];
+                    node_smooth<T, MODE, EXP>(kt, S.w[(t + 3) & 3], S.w[(t + 4) & 3], nyl * EXP + nxl, acc, fv, uo,
+                                              dv, act, fixed, omega, cheb_a, cheb_b, kstep, nu, dn);
+#pragma unroll
+                    for (int c = 0; c < 3; c++) out[c * nv + v] = nu[c];
+                    if (MODE == 3)
+#pragma unroll
+                        for (int c = 0; c < 3; c++) dvec[c * nv + v] = dn[c];
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 3; c++) acc[c] = T(0);
+#pragma unroll
+            for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+                for (int dx = 0; dx < 2; dx++) {
+                    const int el = (nyl + dy) * EXP + nxl + dx;
+                    const int vtx = (1 - dx) + 2 * (1 - dy) + 4;
+#pragma unroll
+                    for (int c = 0; c < 3; c++) acc[c] += E[(3 * vtx + c) * NE2 + el];
+                }
+        }
+        __syncthreads();
+    }
+}
+
+
 template <typename T, bool WS, int MODE, int TY_, bool PIPE>
 int launch_tile_ty(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name, T* dvec,
                    const double* coef, int kstep) {
@@ -551,11 +792,34 @@ int launch_tile_ty(rt_hier* h, const T* u, const T* f, T* out, double omega, con
     });
 }
 
-// variant 0: two barriers per element layer; 3: software-pipelined, one barrier per layer
+template <bool WS, int MODE, int TY_>
+int launch_pair_ty(rt_hier* h, const float* u, const float* f, float* out, double omega, const char* name, float* dvec,
+                   const double* coef, int kstep) {
+    rt_level& L = h->L[0];
+    const int zc = h->tune[0][MODE].zchunk;
+    dim3 grid((L.vx + 31) / 32, (L.vy + TY_ - 1) / TY_, (L.vz + zc - 1) / zc);
+    const rte::KtVals<float> kt = rte::make_kt<float>(h);
+    return rt_launch(h->ctx, name, [&] {
+        k_fine_pair<WS, MODE, TY_><<<grid, PTile<TY_>::BS, sizeof(PairSmem<TY_>), h->ctx->stream>>>(
+            L.nx, L.ny, L.nz, zc, L.vact, h->w, h->vfix, kt, u, f, out, (float)omega, dvec, coef, kstep);
+    });
+}
+
+// variant 0: two barriers per element layer; 3: software-pipelined, one barrier per layer;
+// 4 (FP32): pipelined with element pairs in packed FP32
 template <typename T, bool WS, int MODE>
 int launch_tile(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name, T* dvec = nullptr,
                 const double* coef = nullptr, int kstep = 0) {
     const rt_tile_cfg& tn = h->tune[sizeof(T) == 8 ? 1 : 0][MODE];
+    if constexpr (sizeof(T) == 4) {
+        if (tn.variant == 4) {
+            switch (tn.ty) {
+                case 2: return launch_pair_ty<WS, MODE, 2>(h, u, f, out, omega, name, dvec, coef, kstep);
+                case 8: return launch_pair_ty<WS, MODE, 8>(h, u, f, out, omega, name, dvec, coef, kstep);
+                default: return launch_pair_ty<WS, MODE, 4>(h, u, f, out, omega, name, dvec, coef, kstep);
+            }
+        }
+    }
     if (tn.variant == 3) {
         switch (tn.ty) {
             case 2: return launch_tile_ty<T, WS, MODE, 2, true>(h, u, f, out, omega, name, dvec, coef, kstep);
@@ -579,6 +843,23 @@ cudaError_t set_attr() {
                                 (int)sizeof(PipeSmem<T, TY_>));
 }
 
+template <bool WS, int MODE, int TY_>
+cudaError_t set_attr_pair() {
+    return cudaFuncSetAttribute(k_fine_pair<WS, MODE, TY_>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(PairSmem<TY_>));
+}
+
+template <int TY_>
+cudaError_t set_attrs_pair() {
+    cudaError_t e = cudaSuccess;
+    cudaError_t r[8] = {set_attr_pair<false, 0, TY_>(), set_attr_pair<false, 1, TY_>(), set_attr_pair<false, 2, TY_>(),
+                        set_attr_pair<false, 3, TY_>(), set_attr_pair<true, 0, TY_>(),  set_attr_pair<true, 1, TY_>(),
+                        set_attr_pair<true, 2, TY_>(),  set_attr_pair<true, 3, TY_>()};
+    for (auto x : r)
+        if (x != cudaSuccess) e = x;
+    return e;
+}
+
 template <typename T, int TY_>
 cudaError_t set_attrs_T() {
     cudaError_t e = cudaSuccess;
@@ -597,8 +878,9 @@ namespace rtk {
 // dynamic shared-memory limits of every tile-kernel variant, set once per device
 // (before any stream capture can include a launch)
 int init_tile_kernels(rt_ctx* c) {
-    cudaError_t es[6] = {set_attrs_T<double, 2>(), set_attrs_T<double, 4>(), set_attrs_T<double, 8>(),
-                         set_attrs_T<float, 2>(),  set_attrs_T<float, 4>(),  set_attrs_T<float, 8>()};
+    cudaError_t es[9] = {set_attrs_T<double, 2>(), set_attrs_T<double, 4>(), set_attrs_T<double, 8>(),
+                         set_attrs_T<float, 2>(),  set_attrs_T<float, 4>(),  set_attrs_T<float, 8>(),
+                         set_attrs_pair<2>(),      set_attrs_pair<4>(),      set_attrs_pair<8>()};
     for (cudaError_t e : es)
         if (e != cudaSuccess) return rt_fail(c, RT_ECUDA, "tile kernel attributes: %s", cudaGetErrorString(e));
     return RT_OK;
@@ -617,7 +899,7 @@ int tile_zchunk_default(rt_ctx* c, int vx, int vy, int vz) {
 template <typename T>
 static bool use_march(rt_hier* h, int mode) {
     const int v = h->tune[sizeof(T) == 8 ? 1 : 0][mode].variant;
-    return v == 1 || v == 2;  // 1: marching, 2: marching with prefetch (0, 3: tile kernels)
+    return v == 1 || v == 2;  // 1: marching, 2: marching with prefetch (0, 3, 4: tile kernels)
 }
 
 template <typename T>

@@ -321,7 +321,7 @@ class HierarchyGrid:
             for m, mname in enumerate(names):
                 v, ty, zc, us = C.c_int(), C.c_int(), C.c_int(), C.c_double()
                 self._c(A.lib().rt_tuning_info(self._h, prec, m, C.byref(v), C.byref(ty), C.byref(zc), C.byref(us)))
-                out[f"{mname}_{pname}"] = {"variant": ["smem_tile", "register_march", "register_march_prefetch", "smem_tile_pipelined"][v.value], "rows": ty.value,
+                out[f"{mname}_{pname}"] = {"variant": ["smem_tile", "register_march", "register_march_prefetch", "smem_tile_pipelined", "smem_tile_pairs_f32"][v.value], "rows": ty.value,
                                            "zchunk": zc.value, "us": round(us.value, 2)}
         for st, sname in ((0, "f32"), (1, "bf16")):
             v, u0, u1 = C.c_int(), C.c_double(), C.c_double()

@@ -131,7 +131,42 @@ def test_fine_kernel_variants(pair, variant, ty, zc):
         rb._capi.check(rb.lib().rt_set_tuning(G.handle, rb.FP64, m, 1, 4, 16), ctx.handle)
 
 
-@pytest.mark.parametrize("variant,ty,zc", [(0, 4, 8), (1, 2, 8), (2, 4, 8), (3, 4, 8), (3, 8, 2)])
+FP32_TOL = 2e-6  # FP32 kernels against the FP64 oracle on random data (no cancellation)
+
+
+@pytest.mark.parametrize("variant,ty,zc", [(0, 4, 8), (1, 2, 8), (2, 4, 8), (3, 4, 8), (3, 8, 3), (4, 4, 8),
+                                           (4, 8, 16), (4, 2, 5), (4, 8, 1), (4, 4, 64)])
+def test_fp32_fine_kernels(pair, variant, ty, zc):
+    """Every FP32 finest-level kernel variant (including the packed-pair tile kernel) gives the
+    oracle's residual, K u, Jacobi and first Chebyshev step to FP32 accuracy."""
+    cfg, ctx, G, H = pair
+    for m in range(4):
+        rb._capi.check(rb.lib().rt_set_tuning(G.handle, rb.FP32, m, variant, ty, zc), ctx.handle)
+    u, f = _rand_vec(G, 0, 310), _rand_vec(G, 0, 311)
+    G[0].setDisplacement(u)
+    G[0].setForce(f)
+    lib = rb.lib()
+    rb._capi.check(lib.rt_fine_kernel_f32(G.handle, 0, 0.0), ctx.handle)
+    r_or = np.zeros_like(u)
+    O.lib().or_fine_residual(H.lv(0), O.ptr(H.KE), O.ptr(u), O.ptr(f), O.ptr(r_or))
+    assert rel_err(G[0].getResidual(), r_or) < FP32_TOL
+    rb._capi.check(lib.rt_fine_kernel_f32(G.handle, 1, 0.0), ctx.handle)
+    assert rel_err(G[0].getResidual(), H.applyK(u)) < FP32_TOL
+    rb._capi.check(lib.rt_fine_kernel_f32(G.handle, 2, 0.6), ctx.handle)
+    uo, tmp = u.copy(), np.zeros_like(u)
+    O.lib().or_fine_jacobi(H.lv(0), O.ptr(H.KE), O.ptr(uo), O.ptr(f), 0.6, O.ptr(tmp))
+    assert rel_err(G[0].getResidual(), uo) < FP32_TOL
+    H.set_lmax([G.smoother_lmax(i) for i in range(H.nlev - 1)])
+    rb._capi.check(lib.rt_fine_kernel_f32(G.handle, 3, 0.0), ctx.handle)
+    uc, un, d = u.copy(), np.zeros_like(u), np.zeros_like(u)
+    O.lib().or_fine_cheby(H.lv(0), O.ptr(H.KE), O.ptr(uc), O.ptr(f), O.ptr(un), O.ptr(d), 0)
+    assert rel_err(G[0].getResidual(), un) < FP32_TOL
+    for m in range(4):
+        rb._capi.check(rb.lib().rt_set_tuning(G.handle, rb.FP32, m, 1, 4, 16), ctx.handle)
+
+
+@pytest.mark.parametrize("variant,ty,zc", [(0, 4, 8), (1, 2, 8), (2, 4, 8), (3, 4, 8), (3, 8, 2), (4, 8, 16),
+                                           (4, 4, 8)])
 def test_fp32_kernel_variants_in_pcg(pair, variant, ty, zc):
     """The FP32 finest-level kernels of every variant drive the mixed-precision PCG (FP32 Chebyshev
     V-cycles) to 1e-6 in the FP64 residual; FP32 rounding differs between variants, the iteration
