@@ -203,11 +203,13 @@ def algorithmic_bytes(name, nv, ne, s):
 
 # DRAM bytes (read + write) per launch from one ncu capture of the kernel on this workload,
 # per node (1,081,665 nodes): register-marching variant (rows 2, z-chunk 8) 71.0 MB read +
-# 3.3 MB written; pipelined tile variant (rows 8, z-chunk 32) 45.3 MB read + 0.3 MB written
-# (its 26 MB of writes were still in L2 when the launch ended).  None for variants
-# without a capture.
+# 3.3 MB written; tile variant (rows 4, z-chunk 8) 45.33 MB read + 0.31 MB written;
+# pipelined tile variant (rows 8, z-chunk 8) 45.33 MB read + 0.26 MB written.  The tile
+# variants' 26 MB of writes are still in the 126 MB L2 when the launch ends.  None for
+# variants without a capture.
 NCU_TRAFFIC_PER_NODE = {("fine_cheby_f32", "register_march"): (71.0e6 + 3.3e6) / 1081665,
-                        ("fine_cheby_f32", "smem_tile_pipelined"): (45.328e6 + 0.292e6) / 1081665}
+                        ("fine_cheby_f32", "smem_tile"): (45.326e6 + 0.306e6) / 1081665,
+                        ("fine_cheby_f32", "smem_tile_pipelined"): (45.329e6 + 0.256e6) / 1081665}
 
 
 def roofline(ctx, stats, G, peaks, tuning=None):
@@ -236,9 +238,10 @@ def roofline(ctx, stats, G, peaks, tuning=None):
     return out
 
 
-def e2e_steps(rb, ctx, G, cfg, steps, seed0=500):
-    """Same step through the public API with host buffers: H2D of the density
-    each step, worst-case solve, D2H of the worst-case load field."""
+def e2e_steps(rb, ctx, G, cfg, steps, seed0=100):
+    """Same steps (same Lanczos start vectors as the device-timed ones) through the public
+    API with host buffers: H2D of the density each step, worst-case solve, D2H of the
+    worst-case load field."""
     import torch
 
     rho = np.ascontiguousarray(cfg["rho"].ravel(), np.float32)
@@ -466,8 +469,8 @@ def run_batched(args):
         cfg = configs.cantilever(nx, ny, nz)
         cfg["rho"] = configs.smoothed_density(cfg["eact"].shape, 2 + i)
         G = rb.HierarchyGrid(ctx, params(cfg["mode"]))
-        apply_form(rb, G, FORMS["mixed"])
         G.genFromBox(cfg["eact"])
+        apply_form(rb, G, FORMS["mixed"])
         G[0].setRho(cfg["rho"].ravel())
         G.set_support(cfg["vfix"])
         G.update_stencil()
@@ -477,8 +480,8 @@ def run_batched(args):
         rhs.append(cfg["fload"].ravel())
     big_cfg = configs.worst_case_box(256, 256, 128, seed=0)
     big = rb.HierarchyGrid(ctx, params(big_cfg["mode"]))
-    apply_form(rb, big, FORMS["mixed"])
     big.genFromBox(big_cfg["eact"])
+    apply_form(rb, big, FORMS["mixed"])
     big[0].setRho(big_cfg["rho"].ravel())
     big.set_support(big_cfg["vfix"])
     big.update_stencil()
@@ -679,8 +682,8 @@ def run_c5(args):
                           volume_ratio=0.4, design_step=0.06, damp_ratio=0.5, filter_radius=2.0,
                           precision=rb.FP32, smoother=rb.SMOOTH_CHEBY, pre_sweeps=4, post_sweeps=4)
     G = rb.HierarchyGrid(ctx, p)
-    apply_form(rb, G, FORMS_C5["mixed"])
     G.genFromBox(cfg["eact"])
+    apply_form(rb, G, FORMS_C5["mixed"])
     G[0].setRho(cfg["rho"].ravel())
     G.set_support(cfg["vfix"])
     G.set_load_nodes(cfg["load_nodes"], cfg["normals"])
