@@ -366,6 +366,92 @@ def run_conv(args):
     return 0
 
 
+def run_voxelize(args):
+    """Solid voxelisation (voxelize_mesh, voxelizer/voxelize_main.cpp:344-402) of a closed
+    mesh: an icosphere refined 7 times (327,680 triangles) merged with a rotated 256x128
+    torus (65,536 triangles), prefer_reso 511 -> a 512^3 bit grid.  value = cube cells per
+    second of device time (event pass + row pass, mesh resident); e2e = the same through
+    rt_voxelize_mesh with host arrays (mesh upload, bits download); the oracle's
+    restatement of the reference's CPU voxeliser is the CPU baseline."""
+    import robtop_b200 as rb
+    from robtop_b200 import configs
+
+    ctx = rb.Context(0)
+    sv, sf = configs.icosphere(7, (0.0, 0.0, 0.0), 1.0)
+    tv, tf = configs.torus(1.6, 0.3, 256, 128, (0.0, 0.0, 0.0))  # encircles the sphere, disjoint
+    v, f = configs.merge_meshes((sv, sf), (configs.rigid_transform(tv, 21), tf))
+    prefer = 511
+    R = rb.lib().rt_voxel_resolution(prefer)
+    vf = np.ascontiguousarray(v, np.float32).reshape(-1)
+    ff = np.ascontiguousarray(f, np.int32).reshape(-1)
+    us = C.c_double()
+    rb._capi.check(rb.lib().rt_bench_voxelize(ctx.handle, vf.ctypes.data, len(v), ff.ctypes.data, len(f), prefer,
+                                              max(args.warmup, 3), C.byref(us)), ctx.handle)
+    # one voxelisation takes well under a millisecond: time enough of them (about half a second)
+    # for the clock sampler to see the timed region
+    reps = max(args.steps, 6000)
+    clocks = Clocks(0)
+    clocks.start()
+    rb._capi.check(rb.lib().rt_bench_voxelize(ctx.handle, vf.ctypes.data, len(v), ff.ctypes.data, len(f), prefer,
+                                              reps, C.byref(us)), ctx.handle)
+    clk = clocks.stop()
+    # per-kernel split from the library's per-launch profile
+    ctx.profile(True)
+    ctx.profile_reset()
+    rb._capi.check(rb.lib().rt_bench_voxelize(ctx.handle, vf.ctypes.data, len(v), ff.ctypes.data, len(f), prefer,
+                                              args.steps, C.byref(us)), ctx.handle)
+    st = {k: v_ for k, v_ in ctx.profile_stats().items() if k.startswith("vox") and v_[0]}
+    ctx.profile(False)
+    # end to end with host arrays
+    import time as _t
+    t0 = _t.perf_counter()
+    for _ in range(args.steps):
+        bits, R2, box = rb.voxelize_mesh(ctx, v, f, prefer)
+    e2e_s = (_t.perf_counter() - t0) / args.steps
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    rows_n, rows_ms = st.get("vox_rows", (1, 0.0))
+    row_bytes = 2 * R ** 3 // 8  # each row pass reads and writes the R^3-bit grid once
+    ach = row_bytes / (rows_ms / max(rows_n, 1) * 1e-3) / 1e9 if rows_ms else None
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    ev_n, ev_ms = st.get("vox_events", (1, 0.0))
+    line = {"metric": "solid mesh voxelisation, 393,216-triangle closed mesh into a 512^3 bit grid",
+            "value": R ** 3 / (us.value * 1e-6), "unit": "cells/s", "n_gpus": 1, "steps": reps,
+            "warmup": max(args.warmup, 3), "ms_per_step": us.value * 1e-3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+u32", "data": "synthetic",
+            "config": {"workload": "icosphere(7) + rotated torus(256x128), prefer_reso 511, R 512",
+                       "triangles": int(len(f)), "solid_cells": int(_popcount_bits(bits)),
+                       "event_pass_ms": ev_ms / max(ev_n, 1), "row_pass_ms": rows_ms / max(rows_n, 1),
+                       "triangles_per_s": len(f) / (us.value * 1e-6)},
+            "roofline": {"kernel": "vox_rows", "bound": "hbm", "achieved": round(ach, 1) if ach else None,
+                         "peak": hbm, "unit": "GB/s", "frac": round(ach / hbm, 4) if ach else None, "traffic": None,
+                         "algorithmic_bytes": row_bytes},
+            "clocks": clk, "gpu_launches": 2 * reps,
+            "e2e": {"value": R ** 3 / e2e_s, "unit": "cells/s", "h2d_bytes_per_step": int(vf.nbytes + ff.nbytes),
+                    "d2h_bytes_per_step": int(bits.nbytes)}}
+    if not args.no_cpu_baseline:
+        import oracle as O
+
+        t0 = _t.perf_counter()
+        Ro, bmin, bmax, unit = O.voxel_box(v, prefer)
+        ob = O.voxelize_solid(v, f, Ro, bmin, unit)
+        t_cpu = _t.perf_counter() - t0
+        line["cpu_baseline"] = {"value": R ** 3 / t_cpu, "unit": "cells/s", "cores": 1, "kind": "port",
+                                "sample": "the oracle's single-threaded restatement of the reference's CPU solid "
+                                          "voxeliser on the same mesh and cube, one run"}
+        line["config"]["bit_exact_vs_oracle"] = bool(np.array_equal(ob, bits))
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
+def _popcount_bits(bits):
+    return int(np.unpackbits(np.ascontiguousarray(bits, np.uint32).view(np.uint8)).sum())
+
+
 def run_kernel(args):
     """Repeat one hot operator of the path on the bench workload (short command for
     ncu captures): fine_residual = rt_update_residual(level 0), fine_jacobi =
@@ -762,7 +848,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="worstcase", choices=["worstcase", "batched", "learned", "c5"],
+    ap.add_argument("--workload", default="worstcase", choices=["worstcase", "batched", "learned", "c5", "voxelize"],
                     help="batched: the 12-instance + 8-RHS batched-solve configuration instead of the headline one")
     ap.add_argument("--forms", default="both", choices=["both", "mixed"],
                     help="mixed: time only the mixed form (short command for launch-list captures)")
@@ -786,6 +872,8 @@ def main():
         return run_batched(args)
     if args.workload == "learned":
         return run_learned(args)
+    if args.workload == "voxelize":
+        return run_voxelize(args)
     if args.workload == "c5":
         return run_c5(args)
 

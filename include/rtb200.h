@@ -152,6 +152,28 @@ int rt_template_matrix(rt_hier* h, double* KE);
 int rt_cube_vertex_bits(rt_ctx* ctx, int reso, const uint32_t* ebits, uint32_t* vbits);
 int rt_cube_coarsen_bits(rt_ctx* ctx, int reso, const uint32_t* ebits_fine, uint32_t* ebits_coarse);
 
+/* ---- mesh voxeliser ------------------------------------------------------- */
+/* cube resolution the voxeliser uses for prefer_reso: the first power of two above it
+ * (padd2SatifyResolution, voxelizer/voxelize_main.cpp:312-340); 0 if prefer_reso is
+ * outside [1, 1023] */
+int rt_voxel_resolution(int prefer_reso);
+/* solid voxelisation of a closed triangle mesh (voxelize_mesh,
+ * voxelizer/voxelize_main.cpp:344-402; the solid kernel voxelizer/voxelize_solid.cu:80-150).
+ * vcoords [3 nvert] and tri_ids [3 ntri] are host arrays; every vertex index must lie in
+ * [0, nvert).  solid_bits (host, capacity_words >= R^3 / 32 with R = rt_voxel_resolution)
+ * receives bit x + y R + z R^2 of the padded cube, most significant bit first in each word
+ * as the reference's voxeliser writes it; out_reso = (R, R, R), out_box = (min xyz, max xyz) */
+int rt_voxelize_mesh(rt_ctx* ctx, const float* vcoords, long nvert, const int* tri_ids, long ntri, int prefer_reso,
+                     uint32_t* solid_bits, long capacity_words, int out_reso[3], float out_box[6]);
+/* HierarchyGrid::genFromMesh(pcoords, facevertices) (grid/Grid.cpp:184-205): voxelise, reverse
+ * the words to least significant bit first, build the hierarchy (rt_hier_create_from_bits).
+ * The reference's AABB tree of the surface (used for shell elements and normals) is not built. */
+int rt_hier_create_from_mesh(rt_ctx* ctx, const rt_params* p, const float* vcoords, long nvert, const int* tri_ids,
+                             long ntri, int prefer_reso, rt_hier** out);
+/* device time of one voxelisation (event and row passes, mesh already on the device) */
+int rt_bench_voxelize(rt_ctx* ctx, const float* vcoords, long nvert, const int* tri_ids, long ntri, int prefer_reso,
+                      int reps, double* us_per_call);
+
 /* ---- boundary conditions ------------------------------------------------- */
 /* surface nodes of level 0 (mark_surface_nodes_kernel, grid/Grid.cu:2005-2039), dense node order */
 int rt_surface_nodes(rt_hier* h, uint8_t* surf);

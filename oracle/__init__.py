@@ -26,8 +26,8 @@ LMAX_STEPS = 30  # Lanczos steps of the Chebyshev bound estimate (the library us
 
 def build() -> str:
     """Compile the oracle library in place (gcc + OpenMP)."""
-    src = os.path.join(_HERE, "rt_oracle.c")
-    if not os.path.exists(_LIB) or os.path.getmtime(_LIB) < os.path.getmtime(src):
+    srcs = [os.path.join(_HERE, f) for f in ("rt_oracle.c", "or_voxel.c", "rt_oracle.h")]
+    if not os.path.exists(_LIB) or os.path.getmtime(_LIB) < max(os.path.getmtime(s) for s in srcs):
         subprocess.check_call(["make", "-s", "-C", _HERE])
     return _LIB
 
@@ -98,6 +98,9 @@ def lib():
             "or_oc_try": (None, [C.c_long, P, P, P, P, C.c_float, C.c_float, C.c_float, C.c_float, P]),
             "or_oc_update": (C.c_float, [C.c_long, P, P, P, P, C.c_float, C.c_float, C.c_float, C.c_float,
                                          C.c_long, P, P]),
+            "or_voxel_box": (None, [P, C.c_long, C.c_int, P, P, P, P]),
+            "or_voxelize_solid": (None, [P, P, C.c_long, C.c_int, P, P, P]),
+            "or_word_reverse": (None, [C.c_long, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -336,3 +339,32 @@ def tridiag_max_eig(alpha, beta):
     a = np.ascontiguousarray(alpha, np.float64)
     b = np.ascontiguousarray(beta, np.float64)
     return lib().or_tridiag_max_eig(a.size, ptr(a), ptr(b))
+
+
+# ----------------------------------------------------------------------------
+# solid mesh voxeliser (voxelizer/voxelize_main.cpp:290-402, cpu_voxelizer.cpp:194-322)
+# ----------------------------------------------------------------------------
+def voxel_box(coords, prefer_reso):
+    """(reso, bmin, bmax, unit) of the padded power-of-two cube around the vertices."""
+    coords = np.ascontiguousarray(coords, np.float32).reshape(-1)
+    r = np.zeros(1, np.int32)
+    bmin, bmax, unit = (np.zeros(3, np.float32) for _ in range(3))
+    lib().or_voxel_box(ptr(coords), coords.size // 3, int(prefer_reso), ptr(r), ptr(bmin), ptr(bmax), ptr(unit))
+    return int(r[0]), bmin, bmax, unit
+
+
+def voxelize_solid(coords, tris, reso, bmin, unit):
+    """Solid bits of the mesh, reso^3, bit x + y*reso + z*reso^2, most significant bit first."""
+    coords = np.ascontiguousarray(coords, np.float32).reshape(-1)
+    tris = np.ascontiguousarray(tris, np.int32).reshape(-1)
+    bmin = np.ascontiguousarray(bmin, np.float32)
+    unit = np.ascontiguousarray(unit, np.float32)
+    bits = np.zeros((reso ** 3 + 31) // 32, np.uint32)
+    lib().or_voxelize_solid(ptr(coords), ptr(tris), tris.size // 3, int(reso), ptr(bmin), ptr(unit), ptr(bits))
+    return bits
+
+
+def word_reverse(bits):
+    out = np.array(bits, np.uint32, copy=True)
+    lib().or_word_reverse(out.size, ptr(out))
+    return out

@@ -135,4 +135,11 @@ float or_oc_update(long ne, const uint8_t* eact, const uint8_t* eshell, float* r
 #ifdef __cplusplus
 }
 #endif
+
+/* solid mesh voxeliser (or_voxel.c) */
+void or_voxel_box(const float* coords, long nvert, int prefer_reso, int* reso, float bmin[3], float bmax[3],
+                  float unit[3]);
+void or_voxelize_solid(const float* coords, const int* tris, long ntri, int reso, const float bmin[3],
+                       const float unit[3], uint32_t* bits);
+void or_word_reverse(long nwords, uint32_t* w);
 #endif

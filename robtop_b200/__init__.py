@@ -12,6 +12,6 @@ from . import _capi  # noqa: F401
 from ._capi import (FP32, FP64, FP64_FINE, LAYOUT_DENSE, LAYOUT_REF_GS, MODE_NSCF, MODE_NSFF, MODE_WSCF, MODE_WSFF,  # noqa: F401
                     SMOOTH_CHEBY, SMOOTH_GS, SMOOTH_JACOBI, SMOOTH_SGS, WORST_BLOCK_LANCZOS, WORST_LANCZOS, WORST_MODPM,
                     RTError, lib)
-from .grid import Context, Grid, HierarchyGrid, default_params, pcg_batch  # noqa: F401
+from .grid import Context, Grid, HierarchyGrid, default_params, pcg_batch, voxelize_mesh  # noqa: F401
 
-__all__ = ["Context", "Grid", "HierarchyGrid", "default_params", "pcg_batch", "lib", "RTError"]
+__all__ = ["Context", "Grid", "HierarchyGrid", "default_params", "pcg_batch", "voxelize_mesh", "lib", "RTError"]

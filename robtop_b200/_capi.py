@@ -107,6 +107,10 @@ SIGNATURES = {
     "rt_bench_fine_kernel": (I, [P, I, I, I, C.POINTER(D)]),
     "rt_bench_level_kernel": (I, [P, I, I, I, I, C.POINTER(D)]),
     "rt_fine_kernel_f32": (I, [P, I, D]),
+    "rt_voxel_resolution": (I, [I]),
+    "rt_voxelize_mesh": (I, [P, P, C.c_long, P, C.c_long, I, P, C.c_long, P, P]),
+    "rt_hier_create_from_mesh": (I, [P, C.POINTER(Params), P, C.c_long, P, C.c_long, I, C.POINTER(P)]),
+    "rt_bench_voxelize": (I, [P, P, C.c_long, P, C.c_long, I, I, C.POINTER(D)]),
     "rt_level_kernel_info": (I, [P, I, C.POINTER(I), C.POINTER(D), C.POINTER(D)]),
     "rt_set_level_kernel": (I, [P, I, I]),
     "rt_pcg": (I, [P, D, I, C.POINTER(SolveInfo)]),

@@ -125,3 +125,75 @@ def batch_instances(n=12, lo=48, hi=160, seed=1):
     rng = np.random.Generator(np.random.Philox(seed))
     sizes = rng.integers(lo, hi + 1, size=(n, 3))
     return [tuple(int(v) for v in s) for s in sizes]
+
+
+# ----------------------------------------------------------------------------
+# closed triangle meshes for the voxeliser (outward-facing, counter-clockwise)
+# ----------------------------------------------------------------------------
+def icosphere(subdiv=3, center=(0.0, 0.0, 0.0), radius=1.0):
+    """Icosahedron refined ``subdiv`` times, vertices pushed to the sphere: 20 * 4^subdiv triangles."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+         (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+         (8, 6, 7), (9, 8, 1)]
+    verts = np.array(v, np.float64)
+    verts /= np.linalg.norm(verts, axis=1, keepdims=True)
+    faces = np.array(f, np.int64)
+    for _ in range(subdiv):
+        edges = np.sort(np.concatenate([faces[:, [0, 1]], faces[:, [1, 2]], faces[:, [2, 0]]]), axis=1)
+        uniq, inv = np.unique(edges, axis=0, return_inverse=True)
+        mid = verts[uniq[:, 0]] + verts[uniq[:, 1]]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        base = verts.shape[0]
+        verts = np.concatenate([verts, mid])
+        nf = faces.shape[0]
+        m01, m12, m20 = (base + inv.reshape(-1)[k * nf:(k + 1) * nf] for k in range(3))
+        a, b, c = faces[:, 0], faces[:, 1], faces[:, 2]
+        faces = np.concatenate([np.stack([a, m01, m20], 1), np.stack([b, m12, m01], 1), np.stack([c, m20, m12], 1),
+                                np.stack([m01, m12, m20], 1)])
+    return (verts * radius + np.asarray(center, np.float64)).astype(np.float32), faces.astype(np.int32)
+
+
+def torus(R=1.0, r=0.35, n=48, m=24, center=(0.0, 0.0, 0.0)):
+    """Torus around the z axis, n x m quads split into 2 n m triangles."""
+    i, j = np.meshgrid(np.arange(n), np.arange(m), indexing="ij")
+    u, w = 2 * np.pi * i / n, 2 * np.pi * j / m
+    verts = np.stack([(R + r * np.cos(w)) * np.cos(u), (R + r * np.cos(w)) * np.sin(u), r * np.sin(w)], -1)
+    verts = verts.reshape(-1, 3) + np.asarray(center, np.float64)
+    idx = lambda a, b: (a % n) * m + (b % m)  # noqa: E731
+    q00, q10, q11, q01 = idx(i, j), idx(i + 1, j), idx(i + 1, j + 1), idx(i, j + 1)
+    faces = np.concatenate([np.stack([q00, q10, q11], -1).reshape(-1, 3), np.stack([q00, q11, q01], -1).reshape(-1, 3)])
+    return verts.astype(np.float32), faces.astype(np.int32)
+
+
+def box_mesh(lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0)):
+    """Axis-aligned box, 12 triangles."""
+    lo, hi = np.asarray(lo, np.float64), np.asarray(hi, np.float64)
+    c = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], np.float64)
+    verts = lo + c * (hi - lo)
+    faces = [(0, 2, 1), (0, 3, 2), (4, 5, 6), (4, 6, 7), (0, 1, 5), (0, 5, 4), (2, 3, 7), (2, 7, 6), (0, 4, 7),
+             (0, 7, 3), (1, 2, 6), (1, 6, 5)]
+    return verts.astype(np.float32), np.array(faces, np.int32)
+
+
+def rigid_transform(verts, seed, shift=(0.0, 0.0, 0.0)):
+    """A seeded random rotation of the vertices about their centroid, then a shift."""
+    rng = np.random.default_rng(seed)
+    q, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+    if np.linalg.det(q) < 0:
+        q[:, 0] = -q[:, 0]
+    v = np.asarray(verts, np.float64)
+    c = v.mean(0)
+    return ((v - c) @ q.T + c + np.asarray(shift, np.float64)).astype(np.float32)
+
+
+def merge_meshes(*meshes):
+    """Disjoint union of (verts, faces) pairs."""
+    vs, fs, base = [], [], 0
+    for v, f in meshes:
+        vs.append(np.asarray(v, np.float32))
+        fs.append(np.asarray(f, np.int32) + base)
+        base += len(v)
+    return np.concatenate(vs), np.concatenate(fs)

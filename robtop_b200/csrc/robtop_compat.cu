@@ -45,6 +45,26 @@ void HierarchyGrid::resetAllResidual(void) {
     for (auto g : _grids) g->reset_residual();
 }
 
+// HierarchyGrid::genFromMesh(pcoords, facevertices) (grid/Grid.cpp:184-205): solid voxelisation
+// on the device, word reverse to least significant bit first, then the bit-grid form
+void HierarchyGrid::genFromMesh(const std::vector<float>& pcoords, const std::vector<int>& facevertices) {
+    if (!_ctx) check(rt_ctx_create(0, nullptr, &_ctx), "rt_ctx_create");
+    const int R = rt_voxel_resolution(_prefer_reso);
+    if (R == 0) throw std::runtime_error("genFromMesh: prefer_reso must be in [1, 1023]");
+    std::vector<unsigned int> bits(((size_t)R * R * R + 31) / 32);
+    int reso[3];
+    float box[6];
+    check(rt_voxelize_mesh(_ctx, pcoords.data(), (long)pcoords.size() / 3, facevertices.data(),
+                           (long)facevertices.size() / 3, _prefer_reso, bits.data(), (long)bits.size(), reso, box),
+          "voxelize_mesh");
+    for (auto& w : bits) {  // most significant bit first -> least significant bit first
+        unsigned int r = 0;
+        for (int b = 0; b < 32; b++) r |= ((w >> b) & 1u) << (31 - b);
+        w = r;
+    }
+    genFromMesh(bits, reso);
+}
+
 // HierarchyGrid::genFromMesh(solid_bit, out_reso) (grid/Grid.cpp:455-712) plus the
 // support / load flags of Grid::computeProjectionMatrix (grid/Grid.cpp:1291-1403)
 void HierarchyGrid::genFromMesh(const std::vector<unsigned int>& solid_bit, int out_reso[3]) {
@@ -223,6 +243,12 @@ void Grid::v3_scale(double* v[3], double ampl) {
 // optimization/optimization.h free functions
 // ---------------------------------------------------------------------------
 static uint64_t g_pm_seed = 1;
+
+void buildGrids(const std::vector<float>& coords, const std::vector<int>& trifaces) {
+    grids.set_prefer_reso(params.gridreso);
+    grids.set_skip_layer(true);
+    grids.genFromMesh(coords, trifaces);
+}
 
 void buildGrids(const std::vector<unsigned int>& solid_bit, int reso) {
     grids.set_skip_layer(true);  // buildGrids always skips layer 1 (optimization/optimization.cpp:17)

@@ -82,6 +82,9 @@ public:
     HierarchyGrid(void);
     ~HierarchyGrid();
     void genFromMesh(const std::vector<unsigned int>& solid_bit, int out_reso[3]);
+    // grid/Grid.cpp:184-205: voxelise the closed triangle mesh at the preferred resolution
+    void genFromMesh(const std::vector<float>& pcoords, const std::vector<int>& facevertices);
+    void set_prefer_reso(int preferreso) { _prefer_reso = preferreso; }
     void update_stencil(void);
     double v_cycle(int pre_relax = 1, int post_relax = 1);
     void setMode(Mode mode);
@@ -110,6 +113,7 @@ private:
     rt_ctx* _ctx = nullptr;
     rt_hier* _h = nullptr;
     rt_params _params;
+    int _prefer_reso = 128;  // grid/Grid.h:541
     std::vector<Grid*> _grids;
     std::vector<int> _load_nodes;
     std::vector<double> _preload;  // [3*nload] load field at the load nodes
@@ -136,6 +140,8 @@ extern grid::HierarchyGrid grids;
 
 // optimization/optimization.h:28-82
 void buildGrids(const std::vector<unsigned int>& solid_bit, int reso);
+// optimization/optimization.cpp:14-19: the mesh form
+void buildGrids(const std::vector<float>& coords, const std::vector<int>& trifaces);
 void setParameters(float volRatio, float volDecrease, float designStep, float filterRadi, float dampRatio,
                    float powerPenal, float min_density, int gridreso, float youngs_modulu, float poisson_ratio,
                    float shell_width, bool logdensity, bool logcompliance);

@@ -256,6 +256,15 @@ class HierarchyGrid:
                                                  C.byref(self._h)))
         self._init_levels()
 
+    def genFromTriMesh(self, pcoords, facevertices, prefer_reso):
+        """HierarchyGrid::genFromMesh(pcoords, facevertices) (grid/Grid.cpp:184-205): solid
+        voxelisation of the closed triangle mesh on the device, then the hierarchy."""
+        v = np.ascontiguousarray(pcoords, np.float32).reshape(-1)
+        f = np.ascontiguousarray(facevertices, np.int32).reshape(-1)
+        self._c(A.lib().rt_hier_create_from_mesh(self.ctx.handle, C.byref(self.params), _p(v), v.size // 3, _p(f),
+                                                 f.size // 3, int(prefer_reso), C.byref(self._h)))
+        self._init_levels()
+
     def genFromBox(self, eact):
         """Dense element-activity box ``eact[nz, ny, nx]`` (x fastest)."""
         eact = np.ascontiguousarray(eact, np.uint8)
@@ -385,6 +394,23 @@ class HierarchyGrid:
             self.close()
         except Exception:
             pass
+
+
+def voxelize_mesh(ctx, pcoords, facevertices, prefer_reso):
+    """voxelize_mesh (voxelizer/voxelize_main.cpp:344-402) on the device: returns the solid
+    bits (most significant bit first in each word, bit x + y R + z R^2), R and the cube
+    ``[[min xyz], [max xyz]]``."""
+    v = np.ascontiguousarray(pcoords, np.float32).reshape(-1)
+    f = np.ascontiguousarray(facevertices, np.int32).reshape(-1)
+    R = A.lib().rt_voxel_resolution(int(prefer_reso))
+    if R == 0:
+        raise ValueError("prefer_reso must be in [1, 1023]")
+    bits = np.zeros((R ** 3 + 31) // 32, np.uint32)
+    reso = np.zeros(3, np.int32)
+    box = np.zeros(6, np.float32)
+    check(A.lib().rt_voxelize_mesh(ctx.handle, _p(v), v.size // 3, _p(f), f.size // 3, int(prefer_reso), _p(bits),
+                                   bits.size, _p(reso), _p(box)), ctx.handle)
+    return bits, int(reso[0]), box.reshape(2, 3)
 
 
 def pcg_batch(grids, tol=1e-6, maxit=500):

@@ -44,6 +44,17 @@ int main(int argc, char** argv) {
     double s = 0;
     for (float r : rho) s += r;
     printf("volume %.9g\n", s / rho.size());
+    // the mesh form of buildGrids (optimization/optimization.cpp:14-19): a 24 x 12 x 12 box
+    // of 12 triangles, voxelised at gridreso R - 1 (cube 32^3)
+    setParameters(0.4f, 0.0f, 0.03f, 2.0f, 0.5f, 3.0f, 1e-3f, R - 1, 1e6f, 0.4f, 0.0f, false, false);
+    const std::vector<float> coords = {0, 0, 0, 24, 0, 0, 24, 12, 0, 0, 12, 0, 0, 0, 12, 24, 0, 12, 24, 12, 12, 0, 12, 12};
+    const std::vector<int> faces = {0, 2, 1, 0, 3, 2, 4, 5, 6, 4, 6, 7, 0, 1, 5, 0, 5, 4,
+                                    2, 3, 7, 2, 7, 6, 0, 4, 7, 0, 7, 3, 1, 2, 6, 1, 6, 5};
+    buildGrids(coords, faces);
+    rt_level_info li;
+    rt_hier_level_info(getGrids().hier(), 0, &li);
+    printf("mesh_levels %d\n", getGrids().n_grid());
+    printf("mesh_elements %lld\n", li.n_active_elements);
     printf("ok 1\n");
     return 0;
 }

@@ -53,3 +53,10 @@ def test_compat_flow_matches_oracle():
     x, _, _ = H.pcg(b / np.linalg.norm(b), tol=1e-10)
     assert vals["worst_compliance"] >= (b / np.linalg.norm(b)) @ x * (1 - 1e-3)
     assert abs(vals["volume"] - 0.4) <= 2e-4
+    # buildGrids(coords, trifaces): the device voxeliser's solid cells = the oracle's
+    v = np.array([0, 0, 0, 24, 0, 0, 24, 12, 0, 0, 12, 0, 0, 0, 12, 24, 0, 12, 24, 12, 12, 0, 12, 12], np.float32)
+    f = np.array([0, 2, 1, 0, 3, 2, 4, 5, 6, 4, 6, 7, 0, 1, 5, 0, 5, 4, 2, 3, 7, 2, 7, 6, 0, 4, 7, 0, 7, 3, 1, 2, 6,
+                  1, 6, 5], np.int32)
+    R, bmin, bmax, unit = O.voxel_box(v, 31)
+    assert vals["mesh_elements"] == O.bits_total(O.voxelize_solid(v, f, R, bmin, unit)) > 0
+    assert vals["mesh_levels"] >= 2

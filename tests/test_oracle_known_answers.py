@@ -343,3 +343,42 @@ def test_gs_maps_padding_and_order():
     vl, gs_num, ngs = O.gs_maps(R + 1, vb)
     assert all(g % 32 == 0 for g in gs_num) and ngs == gs_num.sum()
     assert len(set(vl.tolist())) == vl.size
+
+
+def test_voxeliser_resolution_rule_and_volumes():
+    """The oracle voxeliser (voxelizer/cpu_voxelizer.cpp:245-322 restated): the cube resolution
+    is the first power of two above prefer_reso (voxelize_main.cpp:312-340), and the solid
+    voxel volume of closed meshes matches their enclosed volume."""
+    from robtop_b200 import configs
+
+    for prefer, R in ((1, 2), (7, 8), (31, 32), (63, 64), (64, 128), (200, 256)):
+        assert O.voxel_box(np.zeros((1, 3), np.float32) + [[0, 0, 0]], prefer)[0] == R
+    cases = {"sphere": (configs.icosphere(4), None), "torus": (configs.torus(1.0, 0.35, 64, 32), None),
+             "box": (configs.box_mesh((0, 0, 0), (1.0, 0.5, 0.7)), 0.35)}
+    for name, ((v, f), exact) in cases.items():
+        d = v.astype(np.float64)[f]
+        poly = abs(np.einsum("ij,ij->i", d[:, 0], np.cross(d[:, 1], d[:, 2])).sum()) / 6.0  # enclosed volume
+        if exact is not None:
+            assert abs(poly - exact) < 1e-6
+        R, bmin, bmax, unit = O.voxel_box(v, 127)
+        bits = O.voxelize_solid(v, f, R, bmin, unit)
+        vol = O.bits_total(bits) * float(unit[0]) ** 3
+        assert abs(vol - poly) < 0.02 * poly, (name, vol, poly)
+
+
+def test_voxeliser_word_reverse_and_bit_order():
+    """Bit id x + y R + z R^2 at bit 31 - id % 32 (most significant first); the word reverse
+    (wordReverse_g) gives the hierarchy's least-significant-first layout."""
+    from robtop_b200 import configs
+
+    v, f = configs.icosphere(2, (0.0, 0.0, 0.0), 1.0)
+    R, bmin, bmax, unit = O.voxel_box(v, 31)
+    msb = O.voxelize_solid(v, f, R, bmin, unit)
+    lsb = O.word_reverse(msb)
+    np.testing.assert_array_equal(O.word_reverse(lsb), msb)
+    # least-significant-first: bit id % 32 of word id / 32; the centred sphere fills the cube's
+    # centre, not its corner, and is mirror-symmetric in x up to a thin shell of boundary voxels
+    ids = np.arange(R ** 3)
+    vol = ((lsb[ids >> 5] >> (ids & 31)) & 1).reshape(R, R, R)  # [z][y][x]
+    assert vol[R // 2, R // 2, R // 2] == 1 and vol[0, 0, 0] == 0
+    assert np.count_nonzero(vol != vol[:, :, ::-1]) < 0.05 * vol.sum()
