@@ -83,20 +83,52 @@ def _rt_params(**kw):
                           mode=_state["mode"], skip_layer1=1, **kw)
 
 
-def buildGrids(solid_bit, reso, **solver):
-    """Builds the hierarchy from a cubic bit grid (HierarchyGrid::genFromMesh(solid_bit, out_reso),
-    grid/Grid.cpp:455) and applies the boundary predicates to the level-0 surface nodes
-    (Grid::computeProjectionMatrix, grid/Grid.cpp:1291-1403)."""
+def _word_reverse(words):
+    """Most-significant-bit-first words -> least-significant-bit-first (wordReverse_g)."""
+    b = np.ascontiguousarray(words, np.uint32).view(np.uint8).reshape(-1, 4)
+    rev = np.unpackbits(b, axis=1, bitorder="little")[:, ::-1]  # bit 31 .. 0 of each word
+    return np.packbits(rev, axis=1, bitorder="little").reshape(-1).view(np.uint32).copy()
+
+
+def _predicate(fn, pos):
+    """Applies a region predicate: vectorised (``contains``) or one position at a time."""
+    if fn is None:
+        return np.zeros(len(pos), bool)
+    if hasattr(fn, "contains"):
+        return np.asarray(fn.contains(pos), bool)
+    return np.array([bool(fn(p)) for p in pos], bool)
+
+
+def buildGrids(a, b, **solver):
+    """Builds the hierarchy and applies the boundary predicates to the level-0 surface nodes
+    (Grid::computeProjectionMatrix, grid/Grid.cpp:1291-1403).
+
+    ``buildGrids(coords, trifaces)`` (optimization/optimization.cpp:14-19): the closed triangle
+    mesh is voxelised on the device at ``params.gridreso`` and node positions are in the mesh
+    frame (cube corner + node index x element length).  ``buildGrids(solid_bit, reso)``: a
+    cubic bit grid (genFromMesh(solid_bit, out_reso), grid/Grid.cpp:455), least significant bit
+    first; node positions are the node indices."""
     G = HierarchyGrid(_ctx(), _rt_params(**solver))
-    G.genFromMesh(solid_bit, [reso, reso, reso])
+    if np.isscalar(b):
+        reso = int(b)
+        G.genFromMesh(a, [reso, reso, reso])
+        origin, h = np.zeros(3), np.ones(3)
+    else:
+        from .grid import voxelize_mesh
+
+        bits, reso, box = voxelize_mesh(_ctx(), a, b, params.gridreso)
+        G.genFromMesh(_word_reverse(bits), [reso, reso, reso])
+        origin = box[0].astype(np.float64)
+        h = (box[1].astype(np.float64) - origin) / reso
+        _state["box"] = box
     g0 = G[0]
     surf = G.surface_nodes().astype(bool) & g0.getVact().astype(bool)
     nv = g0.nv
     vx, vy = g0.nx + 1, g0.ny + 1
     ids = np.flatnonzero(surf)
-    pos = np.stack([ids % vx, (ids // vx) % vy, ids // (vx * vy)], 1).astype(np.float64)
-    fixed = np.array([bool(_state["fixed"](p)) for p in pos]) if _state["fixed"] else np.zeros(ids.size, bool)
-    loadm = np.array([bool(_state["load"](p)) for p in pos]) if _state["load"] else np.zeros(ids.size, bool)
+    pos = origin + np.stack([ids % vx, (ids // vx) % vy, ids // (vx * vy)], 1).astype(np.float64) * h
+    fixed = _predicate(_state["fixed"], pos)
+    loadm = _predicate(_state["load"], pos)
     loadm &= ~fixed
     vfix = np.zeros(nv, np.uint8)
     vfix[ids[fixed]] = 1
@@ -105,6 +137,7 @@ def buildGrids(solid_bit, reso, **solver):
     normals = np.tile([0.0, 0.0, 1.0], (load_ids.size, 1))
     G.set_load_nodes(load_ids, normals)
     _state["grids"] = G
+    _state["fixed_ids"] = ids[fixed]
     _state["load_ids"] = load_ids
     _state["load_pos"] = pos[loadm]
     return G
@@ -131,8 +164,12 @@ def solveFEM(tol=1e-4):
     G = getGrids()
     nv = G[0].nv
     f = np.zeros(3 * nv)
-    for i, p in zip(_state["load_ids"], _state["load_pos"]):
-        v = _state["field"](p) if _state["field"] else (0.0, 0.0, 0.0)
+    field = _state["field"]
+    if field is not None and hasattr(field, "force"):  # a parsed configuration's summed fields
+        vals = field.force(_state["load_pos"]) if len(_state["load_pos"]) else np.zeros((0, 3))
+    else:
+        vals = [field(p) if field else (0.0, 0.0, 0.0) for p in _state["load_pos"]]
+    for i, v in zip(_state["load_ids"], vals):
         f[i], f[nv + i], f[2 * nv + i] = v
     G[0].setForce(f)
     rel = 1.0
@@ -189,3 +226,27 @@ def optimization(max_iter=100, worst=modifiedPM):
         updateDensities(Vgoal)
     _state["records"] = rec
     return rec
+
+
+def run_config(jsonfile, meshfile=None, workmode="wsff", max_iter=100, worst=modifiedPM, **flags):
+    """The robtop.cpp flow driven by a benchmark configuration (config_parser_t::parse,
+    config_parser.cpp:485-498, then robtop.cpp:27-46): parse the regions and force fields,
+    read the mesh (the configuration's ``model`` unless ``meshfile`` is given), set the
+    parameters (``flags`` as setParameters' keywords), build the grids from the mesh and run
+    the optimisation.  Returns the compliance record."""
+    from .boundary import parse_config, read_mesh
+
+    cfg = parse_config(jsonfile)
+    path = meshfile or cfg.model_path()
+    if not path:
+        raise ValueError("no mesh: the configuration names no model and no meshfile was given")
+    v, f = read_mesh(path)
+    kw = dict(volRatio=0.3, volDecrease=0.02, designStep=0.03, filterRadi=2, dampRatio=0.5, powerPenal=3.0,
+              min_density=1e-3, gridreso=200, youngs_modulu=1e6, poisson_ratio=0.4)  # the reference's flag defaults
+    kw.update(flags)
+    setParameters(**kw)
+    setWorkMode(workmode)
+    setBoundaryCondition(cfg.fixed_area, cfg.load_area, cfg)
+    buildGrids(v, f)
+    uploadTemplateMatrix()
+    return optimization(max_iter=max_iter, worst=worst)
