@@ -175,6 +175,10 @@ int rt_bench_voxelize(rt_ctx* ctx, const float* vcoords, long nvert, const int* 
                       int reps, double* us_per_call);
 
 /* ---- boundary conditions ------------------------------------------------- */
+/* shell elements: eshell[ne] (dense level-0 element order) flags elements whose density the OC
+ * update holds at 1 (the reference marks those within shell_width elements of the mesh surface,
+ * HierarchyGrid::setSolidShellElement, grid/Grid.cpp:67-137); eshell = NULL clears them */
+int rt_set_shell(rt_hier* h, const uint8_t* eshell);
 /* surface nodes of level 0 (mark_surface_nodes_kernel, grid/Grid.cu:2005-2039), dense node order */
 int rt_surface_nodes(rt_hier* h, uint8_t* surf);
 /* support flags on level-0 nodes (Grid::computeProjectionMatrix, grid/Grid.cpp:1291-1403) */

@@ -107,6 +107,7 @@ SIGNATURES = {
     "rt_bench_fine_kernel": (I, [P, I, I, I, C.POINTER(D)]),
     "rt_bench_level_kernel": (I, [P, I, I, I, I, C.POINTER(D)]),
     "rt_fine_kernel_f32": (I, [P, I, D]),
+    "rt_set_shell": (I, [P, P]),
     "rt_voxel_resolution": (I, [I]),
     "rt_voxelize_mesh": (I, [P, P, C.c_long, P, C.c_long, I, P, C.c_long, P, P]),
     "rt_hier_create_from_mesh": (I, [P, C.POINTER(Params), P, C.c_long, P, C.c_long, I, C.POINTER(P)]),

@@ -300,3 +300,106 @@ def _read_stl(path):
     # weld identical vertices so shared edges are shared in the index list
     v, inv = np.unique(tris, axis=0, return_inverse=True)
     return v.astype(np.float32), inv.reshape(-1, 3).astype(np.int32)
+
+
+# ----------------------------------------------------------------------------
+# distances to the mesh surface: outward normals of load nodes, shell elements
+# ----------------------------------------------------------------------------
+def _closest_on_triangles(P, A, B, C):
+    """Closest points of points P[k] on triangles (A[k], B[k], C[k]) (Voronoi-region tests)."""
+    ab, ac, ap = B - A, C - A, P - A
+    d1, d2 = (ab * ap).sum(1), (ac * ap).sum(1)
+    bp = P - B
+    d3, d4 = (ab * bp).sum(1), (ac * bp).sum(1)
+    cp = P - C
+    d5, d6 = (ab * cp).sum(1), (ac * cp).sum(1)
+    va, vb, vc = d3 * d6 - d5 * d4, d5 * d2 - d1 * d6, d1 * d4 - d3 * d2
+    out = np.empty_like(P)
+    done = np.zeros(len(P), bool)
+
+    def put(mask, val):
+        m = mask & ~done
+        out[m] = val[m] if val.ndim == 2 else val
+        done[:] |= m
+
+    put((d1 <= 0) & (d2 <= 0), A)
+    put((d3 >= 0) & (d4 <= d3), B)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        put((vc <= 0) & (d1 >= 0) & (d3 <= 0), A + ab * (d1 / (d1 - d3))[:, None])
+        put((d6 >= 0) & (d5 <= d6), C)
+        put((vb <= 0) & (d2 >= 0) & (d6 <= 0), A + ac * (d2 / (d2 - d6))[:, None])
+        put((va <= 0) & ((d4 - d3) >= 0) & ((d5 - d6) >= 0),
+            B + (C - B) * ((d4 - d3) / ((d4 - d3) + (d5 - d6)))[:, None])
+        den = va + vb + vc
+        put(np.ones(len(P), bool), A + ab * (vb / den)[:, None] + ac * (vc / den)[:, None])
+    return out
+
+
+def closest_points(points, verts, faces):
+    """For each point: the closest point on the triangle mesh, its squared distance and the
+    triangle (the AABB-tree query of Grid::outwardNormal, grid/Grid.cpp:1404-1423).  Candidates
+    are the triangles whose centroid lies within (distance to the nearest centroid + the
+    largest centroid-to-vertex radius), found with a k-d tree."""
+    from scipy.spatial import cKDTree
+
+    P = np.atleast_2d(np.asarray(points, np.float64))
+    V = np.asarray(verts, np.float64)
+    F = np.asarray(faces, np.int64)
+    T = V[F]  # [m, 3, 3]
+    cen = T.mean(1)
+    rad = np.sqrt(((T - cen[:, None, :]) ** 2).sum(2).max(1)).max()
+    tree = cKDTree(cen)
+    d0, _ = tree.query(P)
+    best_q = np.zeros_like(P)
+    best_d = np.full(len(P), np.inf)
+    best_t = np.zeros(len(P), np.int64)
+    cands = tree.query_ball_point(P, d0 + rad + 1e-12)
+    idx_p = np.repeat(np.arange(len(P)), [len(c) for c in cands])
+    idx_t = np.fromiter((t for c in cands for t in c), np.int64, count=len(idx_p))
+    for s in range(0, len(idx_p), 1 << 20):
+        ip, it = idx_p[s:s + (1 << 20)], idx_t[s:s + (1 << 20)]
+        q = _closest_on_triangles(P[ip], T[it, 0], T[it, 1], T[it, 2])
+        d = ((q - P[ip]) ** 2).sum(1)
+        order = np.lexsort((d, ip))  # per point, smallest distance first
+        first = np.ones(len(order), bool)
+        first[1:] = ip[order][1:] != ip[order][:-1]
+        sel = order[first]
+        upd = d[sel] < best_d[ip[sel]]
+        tgt = ip[sel][upd]
+        best_d[tgt], best_q[tgt], best_t[tgt] = d[sel][upd], q[sel][upd], it[sel][upd]
+    return best_q, best_d, best_t
+
+
+def outward_normals(points, verts, faces):
+    """Grid::outwardNormal (grid/Grid.cpp:1404-1423): the unit vector from the point to its
+    closest surface point, oriented along that triangle's normal (the triangle's own normal
+    when the point lies on the surface, within 1e-6)."""
+    P = np.atleast_2d(np.asarray(points, np.float64))
+    q, d2, t = closest_points(P, verts, faces)
+    V = np.asarray(verts, np.float64)
+    F = np.asarray(faces, np.int64)[t]
+    tn = np.cross(V[F[:, 1]] - V[F[:, 0]], V[F[:, 2]] - V[F[:, 0]])
+    p2c = q - P
+    ln = np.sqrt(d2)
+    on = ln < 1e-6
+    sgn = np.where((p2c * tn).sum(1) < 0, -1.0, 1.0)
+    out = np.where(on[:, None], tn / np.linalg.norm(tn, axis=1, keepdims=True),
+                   p2c / np.where(on, 1.0, ln * sgn)[:, None])
+    return out
+
+
+def shell_elements(eact, origin, h, verts, faces, shell_width):
+    """HierarchyGrid::setSolidShellElement (grid/Grid.cpp:67-137): solid elements whose centre
+    lies within shell_width * h of the mesh surface.  ``eact[nz, ny, nx]`` dense level-0
+    activity, element (x, y, z) centred at origin + (x + 1/2, y + 1/2, z + 1/2) h."""
+    eact = np.asarray(eact)
+    z, y, x = np.nonzero(eact)
+    cen = np.asarray(origin, np.float64) + (np.stack([x, y, z], 1) + 0.5) * np.asarray(h, np.float64)
+    out = np.zeros(eact.shape, np.uint8)
+    if len(cen) == 0:
+        return out
+    w = float(shell_width) * float(np.max(h))
+    _, d2, _ = closest_points(cen, verts, faces)
+    inside = d2 < w * w
+    out[z[inside], y[inside], x[inside]] = 1
+    return out

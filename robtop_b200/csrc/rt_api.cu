@@ -667,6 +667,23 @@ extern "C" int rt_set_support(rt_hier* h, const uint8_t* vfix) {
     return RT_OK;
 }
 
+// shell elements (HierarchyGrid::setSolidShellElement, grid/Grid.cpp:67-137 marks them):
+// level-0 elements whose density the OC update holds at 1 (optimization/optimization.cu:136-162)
+extern "C" int rt_set_shell(rt_hier* h, const uint8_t* eshell) {
+    if (!h) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
+    rt_level& L = h->L[0];
+    if (!eshell) {
+        cudaFree(h->eshell);
+        h->eshell = nullptr;
+        return RT_OK;
+    }
+    if (!h->eshell) RT_CHECK(dalloc(h->ctx, &h->eshell, (size_t)L.ne));
+    RT_CUDA(h->ctx, cudaMemcpyAsync(h->eshell, eshell, L.ne, cudaMemcpyHostToDevice, h->ctx->stream));
+    RT_CUDA(h->ctx, cudaStreamSynchronize(h->ctx->stream));
+    return RT_OK;
+}
+
 // setLoadNodes (optimization/projection.cpp:129-269): rigid modes on the load set,
 // normal part only when the direction is constrained, Gram-Schmidt, degenerate dropped
 static int load_rigid_basis(rt_hier* h, const int* nodes, const double* normals) {

@@ -312,6 +312,14 @@ class HierarchyGrid:
         vfix = np.ascontiguousarray(vfix, np.uint8).ravel()
         self._c(A.lib().rt_set_support(self._h, _p(vfix)))
 
+    def set_shell(self, eshell):
+        """Shell elements (dense level-0 order) whose density the OC update holds at 1; None clears."""
+        if eshell is None:
+            self._c(A.lib().rt_set_shell(self._h, None))
+            return
+        e = np.ascontiguousarray(eshell, np.uint8)
+        self._c(A.lib().rt_set_shell(self._h, _p(e)))
+
     def set_load_nodes(self, nodes, normals):
         nodes = np.ascontiguousarray(nodes, np.int32)
         normals = np.ascontiguousarray(normals, np.float64).reshape(-1)

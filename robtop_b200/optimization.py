@@ -28,6 +28,7 @@ class Parameter:
     gridreso: int = 128
     youngs_modulu: float = 1e6
     poisson_ratio: float = 0.4
+    shell_width: float = 3.0  # elements within this many element lengths of the mesh surface stay solid
 
 
 params = Parameter()
@@ -58,6 +59,7 @@ def setParameters(volRatio, volDecrease, designStep, filterRadi, dampRatio, powe
     params.gridreso = gridreso
     params.youngs_modulu = youngs_modulu
     params.poisson_ratio = poisson_ratio
+    params.shell_width = shell_width
 
 
 def setWorkMode(modestr):
@@ -121,6 +123,7 @@ def buildGrids(a, b, **solver):
         origin = box[0].astype(np.float64)
         h = (box[1].astype(np.float64) - origin) / reso
         _state["box"] = box
+        _state["mesh"] = (np.asarray(a, np.float32).reshape(-1, 3), np.asarray(b, np.int32).reshape(-1, 3))
     g0 = G[0]
     surf = G.surface_nodes().astype(bool) & g0.getVact().astype(bool)
     nv = g0.nv
@@ -134,7 +137,18 @@ def buildGrids(a, b, **solver):
     vfix[ids[fixed]] = 1
     G.set_support(vfix)
     load_ids = ids[loadm]
-    normals = np.tile([0.0, 0.0, 1.0], (load_ids.size, 1))
+    if np.isscalar(b):
+        normals = np.tile([0.0, 0.0, 1.0], (load_ids.size, 1))
+    else:
+        # Grid::outwardNormal (closest surface point), and the shell elements of
+        # HierarchyGrid::setSolidShellElement (grid/Grid.cpp:67-137, 1404-1423)
+        from .boundary import outward_normals, shell_elements
+
+        mv, mf = _state["mesh"]
+        normals = outward_normals(pos[loadm], mv, mf) if load_ids.size else np.zeros((0, 3))
+        eact = g0.getEact().reshape(g0.nz, g0.ny, g0.nx)
+        if params.shell_width > 0:
+            G.set_shell(shell_elements(eact, origin, h, mv, mf, params.shell_width).ravel())
     G.set_load_nodes(load_ids, normals)
     _state["grids"] = G
     _state["fixed_ids"] = ids[fixed]
@@ -242,7 +256,8 @@ def run_config(jsonfile, meshfile=None, workmode="wsff", max_iter=100, worst=mod
         raise ValueError("no mesh: the configuration names no model and no meshfile was given")
     v, f = read_mesh(path)
     kw = dict(volRatio=0.3, volDecrease=0.02, designStep=0.03, filterRadi=2, dampRatio=0.5, powerPenal=3.0,
-              min_density=1e-3, gridreso=200, youngs_modulu=1e6, poisson_ratio=0.4)  # the reference's flag defaults
+              min_density=1e-3, gridreso=200, youngs_modulu=1e6, poisson_ratio=0.4,
+              shell_width=3.0)  # the reference's flag defaults
     kw.update(flags)
     setParameters(**kw)
     setWorkMode(workmode)

@@ -117,6 +117,27 @@ def test_mesh_readers_roundtrip(tmp_path):
         assert abs(vol(vs.astype(float), fs) - 2.0) < 1e-6
 
 
+def test_closest_points_normals_and_shell():
+    """Closest surface points against brute force, outward normals of a sphere mesh, and the
+    shell elements of a box: those within shell_width element lengths of the surface."""
+    v, f = configs.icosphere(2, (0, 0, 0), 1.0)
+    rng = np.random.default_rng(3)
+    P = rng.standard_normal((200, 3))
+    P *= (rng.random(200) * 1.6 + 0.2)[:, None] / np.linalg.norm(P, axis=1, keepdims=True)
+    q, d2, t = B.closest_points(P, v, f)
+    T = v.astype(np.float64)[f]
+    brute = np.full(len(P), np.inf)
+    for k in range(len(f)):
+        qq = B._closest_on_triangles(P, *(np.repeat(T[k:k + 1, j], len(P), 0) for j in range(3)))
+        brute = np.minimum(brute, ((qq - P) ** 2).sum(1))
+    np.testing.assert_allclose(d2, brute, atol=1e-12)
+    n = B.outward_normals(P, v, f)
+    assert ((n * P).sum(1) / np.linalg.norm(P, axis=1)).min() > 0.98  # outward, close to radial
+    bv, bf = configs.box_mesh((0, 0, 0), (10, 10, 10))
+    sh = B.shell_elements(np.ones((10, 10, 10), np.uint8), (0, 0, 0), (1.0, 1.0, 1.0), bv, bf, 3.0)
+    assert sh.sum() == 1000 - 4 ** 3 and sh[5, 5, 5] == 0 and sh[0, 5, 5] == 1
+
+
 @pytest.mark.gpu
 def test_build_grids_from_mesh_and_config(tmp_path):
     """buildGrids(coords, trifaces): voxelise, then flag surface nodes by the configuration's
@@ -147,3 +168,8 @@ def test_build_grids_from_mesh_and_config(tmp_path):
     x = float(bmin[0]) + (ids % vx) * ((float(bmax[0]) - float(bmin[0])) / R)  # buildGrids' positions
     assert set(OPT._state["fixed_ids"].tolist()) == set(ids[x <= 1.0].tolist())
     assert len(OPT._state["load_ids"]) > 0
+    # the shell (3 element lengths of the surface) stays solid through the OC updates
+    eact = g0.getEact().reshape(g0.nz, g0.ny, g0.nx)
+    h = (bmax.astype(np.float64) - bmin.astype(np.float64)) / R
+    sh = B.shell_elements(eact, bmin.astype(np.float64), h, v, f, 3.0).ravel().astype(bool)
+    assert sh.any() and np.all(g0.getRho()[sh] == 1.0)

@@ -481,6 +481,20 @@ def test_sensitivity_filter_oc(pair):
                                  0.5, 1e-3, int(H.arrs[0]["eact"].sum()), O.ptr(it), O.ptr(tmp))
     assert np.abs(G[0].getRho() - rho_o).max() <= 1e-4
     assert abs(lam.value - lam_o) <= 1e-3 * abs(lam_o)
+    # with shell elements (held at 1): the same update with the oracle's shell mask
+    shell = (np.random.default_rng(7).random(rho.size) < 0.2).astype(np.uint8) & H.arrs[0]["eact"].ravel()
+    G.set_shell(shell)
+    G[0].setSens(f_or)
+    G[0].setRho(rho)
+    rb._capi.check(rb.lib().rt_oc_update(G.handle, 0.4, C.byref(lam), C.byref(trials)), ctx.handle)
+    rho_s = rho.copy()
+    lam_s = O.lib().or_oc_update(rho_s.size, O.ptr(H.arrs[0]["eact"]), O.ptr(shell), O.ptr(rho_s), O.ptr(f_or), 0.4,
+                                 0.03, 0.5, 1e-3, int(H.arrs[0]["eact"].sum()), O.ptr(it), O.ptr(tmp))
+    got = G[0].getRho()
+    assert np.all(got[shell.astype(bool)] == 1.0)
+    assert np.abs(got - rho_s).max() <= 1e-4
+    assert abs(lam.value - lam_s) <= 1e-3 * abs(lam_s)
+    G.set_shell(None)
     G[0].setRho(rho)
     G.update_stencil()
 
