@@ -392,13 +392,20 @@ def shell_elements(eact, origin, h, verts, faces, shell_width):
     """HierarchyGrid::setSolidShellElement (grid/Grid.cpp:67-137): solid elements whose centre
     lies within shell_width * h of the mesh surface.  ``eact[nz, ny, nx]`` dense level-0
     activity, element (x, y, z) centred at origin + (x + 1/2, y + 1/2, z + 1/2) h."""
-    eact = np.asarray(eact)
-    z, y, x = np.nonzero(eact)
-    cen = np.asarray(origin, np.float64) + (np.stack([x, y, z], 1) + 0.5) * np.asarray(h, np.float64)
+    from scipy.ndimage import binary_erosion
+
+    eact = np.asarray(eact).astype(bool)
     out = np.zeros(eact.shape, np.uint8)
-    if len(cen) == 0:
+    if not eact.any():
         return out
-    w = float(shell_width) * float(np.max(h))
+    hv = np.asarray(h, np.float64)
+    w = float(shell_width) * float(np.max(hv))
+    # the mesh surface lies within a voxel of the solid's boundary: only elements within
+    # ceil(shell_width) + 2 cells of a void cell or the box edge can be closer than w to it
+    k = int(np.ceil(w / float(np.min(hv)))) + 2
+    core = binary_erosion(np.pad(eact, 1), iterations=k)[1:-1, 1:-1, 1:-1]
+    z, y, x = np.nonzero(eact & ~core)
+    cen = np.asarray(origin, np.float64) + (np.stack([x, y, z], 1) + 0.5) * hv
     _, d2, _ = closest_points(cen, verts, faces)
     inside = d2 < w * w
     out[z[inside], y[inside], x[inside]] = 1
