@@ -366,6 +366,150 @@ def run_conv(args):
     return 0
 
 
+def vcycle_bytes(G, s, smoother_sweeps, smoother_bytes_node):
+    """Algorithmic bytes of one V-cycle from the level sizes: per level its smoothing sweeps,
+    one residual, the restriction into and prolongation from the next level; s = bytes per
+    value.  Finest level matrix-free (u, f, r / unew 3 values each per node, 2 flag bytes,
+    4 B weight per element); stencil levels 243 values per node plus the vectors."""
+    total = 0
+    n = G.n_grid()
+    for i in range(n):
+        L = G[i]
+        nv, ne = L.nv, L.ne
+        if i == 0:
+            sweep = nv * (smoother_bytes_node * s + 2) + 4 * ne
+            resid = nv * (9 * s + 2) + 4 * ne
+        elif i < n - 1:
+            sweep = nv * (243 * s + smoother_bytes_node * s)
+            resid = nv * (243 * s + 9 * s)
+        else:  # the coarsest level: dense solve on the active nodes
+            total += (3 * nv) ** 2 // 64 * 8
+            continue
+        total += smoother_sweeps * sweep + resid
+        total += 2 * (3 * s * nv + 3 * s * G[i + 1].nv)  # restriction and prolongation
+    return total
+
+
+def run_c1(args):
+    """The plain method on the small cantilever: 64x32x32 elements, uniform density 0.4,
+    x = 0 clamped, total load 1 in -z spread over the bottom edge of the x = 64 face (wsff).
+    FP64 V-cycle PCG with 2 + 2 damped block-Jacobi sweeps to relative residual 1e-6, then
+    one OC step (sensitivity, filter radius 2, OC update to volume 0.4).  Every step starts
+    from the uniform density and zero displacement, so the steps are the same work.
+
+    The timed sweeps use omega 0.5.  With omega 0.6 the Jacobi step amplifies the top of
+    the spectrum: lambda_max(D^-1 K) is about 3.7 on the finest level, above 2 / 0.6.  PCG
+    then stalls near 6e-5; the oracle and the library agree on this, and the line records
+    that run beside the timed one.  The oracle runs the timed solve on the host cores as the
+    CPU baseline."""
+    import torch
+
+    import robtop_b200 as rb
+    from robtop_b200 import configs
+
+    ctx = make_ctx(rb, 0)
+    stream = torch.cuda.ExternalStream(ctx_stream_handle(ctx))
+    cfg = configs.cantilever(64, 32, 32)
+    p = rb.default_params(mode=cfg["mode"], youngs_modulus=1e6, poisson_ratio=0.4, power_penalty=3.0, min_rho=1e-3,
+                          precision=rb.FP64, smoother=rb.SMOOTH_JACOBI, pre_sweeps=2, post_sweeps=2,
+                          jacobi_omega=0.5, volume_ratio=0.4, design_step=0.03, damp_ratio=0.5, filter_radius=2.0)
+    G = rb.HierarchyGrid(ctx, p)
+    G.genFromBox(cfg["eact"])
+    G.set_support(cfg["vfix"])
+    G.set_load_nodes(cfg["load_nodes"], cfg["normals"])
+    rho0 = np.ascontiguousarray(cfg["rho"].ravel(), np.float32)
+    f = np.ascontiguousarray(cfg["fload"].ravel(), np.float64)
+    lam, trials = C.c_float(), C.c_int()
+    infos = []
+
+    def one_step(read_back=False):
+        G[0].setRho(rho0)
+        G.update_stencil()
+        G[0].setForce(f)
+        G[0].reset_displacement()
+        info = G.pcg(1e-6, 500)
+        rb._capi.check(rb.lib().rt_sensitivity(G.handle, 1), ctx.handle)
+        G[0].filterSensitivity(2.0)
+        rb._capi.check(rb.lib().rt_oc_update(G.handle, 0.4, C.byref(lam), C.byref(trials)), ctx.handle)
+        infos.append(info)
+        return G[0].getRho() if read_back else None
+
+    for _ in range(max(args.warmup, 3)):
+        one_step()
+    ctx.sync()
+    clocks = Clocks(0)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = ctx.launches()
+    e0.record(stream)
+    for _ in range(args.steps):
+        one_step()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = ctx.launches() - l0
+    # end to end with a device-to-host read of the updated density every step
+    e0.record(stream)
+    for _ in range(args.steps):
+        rho_out = one_step(read_back=True)
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    it = infos[-1].iterations
+    lmax0 = G.smoother_lmax(0)
+    # the same solve with omega 0.6, for the record
+    q = G.params
+    q.jacobi_omega = 0.6
+    G.set_params(q)
+    one_step()
+    bad = infos[-1]
+    q.jacobi_omega = 0.5
+    G.set_params(q)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    # per PCG iteration: one V-cycle, one FP64 K p (matrix-free) and ~10 vector passes of 24 B per node
+    nv0, ne0 = G[0].nv, G[0].ne
+    per_it = vcycle_bytes(G, 8, 4, 9) + nv0 * (6 * 8 + 2) + 4 * ne0 + 10 * 24 * nv0
+    solve_ms = ms / args.steps
+    line = {"metric": "plain MG-PCG solve to 1e-6 + one OC step, cantilever 64x32x32 (damped Jacobi 2+2)",
+            "value": args.steps / (ms * 1e-3), "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": solve_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "cantilever 64x32x32, rho 0.4, x=0 clamped, bottom-edge load, wsff, FP64 V-cycle "
+                                   "PCG (Jacobi 2+2, omega 0.5) to 1e-6, OC step (R 2, move 0.03, eta 0.5, V 0.4)",
+                       "levels": G.n_grid(), "pcg_iterations": it, "rel_residual": infos[-2].rel_residual,
+                       "smoother_lmax_level0": lmax0,
+                       "omega_0.6": {"pcg_iterations": bad.iterations, "rel_residual": bad.rel_residual,
+                                     "converged": bad.status == 0},
+                       "oc_multiplier": lam.value,
+                       "volume_after": float(rho_out.mean()),
+                       "algorithmic_bytes_per_pcg_iteration": int(per_it),
+                       "achieved_gbs_per_solve": per_it * it / (solve_ms * 1e-3) / 1e9,
+                       "hbm_peak_gbs": peaks.get("hbm_gbs")},
+            "clocks": clk, "gpu_launches": launches // max(args.steps, 1) * args.steps,
+            "e2e": {"value": args.steps / (e2e_ms * 1e-3), "unit": "solves/s",
+                    "h2d_bytes_per_step": int(rho0.nbytes + f.nbytes), "d2h_bytes_per_step": int(rho0.nbytes)}}
+    if not args.no_cpu_baseline:
+        import oracle as O
+
+        t0 = time.perf_counter()
+        H = O.Hierarchy(cfg["eact"], cfg["rho"], cfg["vfix"], p=3, E=1e6, nu=0.4)
+        H.update_stencil()
+        x, ito, rr = H.pcg(f, tol=1e-6, maxit=500, smoother=O.SMOOTH_JACOBI, npre=2, npost=2, omega=0.5)
+        t_cpu = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": "solves/s", "cores": os.cpu_count() or 1,
+                                "kind": "port", "sample": f"the oracle (OpenMP) stencil assembly + the same PCG solve "
+                                                          f"({ito} iterations), one run, without the OC step"}
+    print(json.dumps(line))
+    G.close()
+    ctx.close()
+    return 0
+
+
 def run_voxelize(args):
     """Solid voxelisation (voxelize_mesh, voxelizer/voxelize_main.cpp:344-402) of a closed
     mesh: an icosphere refined 7 times (327,680 triangles) merged with a rotated 256x128
@@ -848,7 +992,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="worstcase", choices=["worstcase", "batched", "learned", "c5", "voxelize"],
+    ap.add_argument("--workload", default="worstcase", choices=["worstcase", "batched", "learned", "c5", "voxelize", "c1"],
                     help="batched: the 12-instance + 8-RHS batched-solve configuration instead of the headline one")
     ap.add_argument("--forms", default="both", choices=["both", "mixed"],
                     help="mixed: time only the mixed form (short command for launch-list captures)")
@@ -874,6 +1018,8 @@ def main():
         return run_learned(args)
     if args.workload == "voxelize":
         return run_voxelize(args)
+    if args.workload == "c1":
+        return run_c1(args)
     if args.workload == "c5":
         return run_c5(args)
 

@@ -1301,13 +1301,19 @@ extern "C" int rt_relative_residual(rt_hier* h, double* rel) {
 // z = B r (the V-cycle, plus the learned correction when attached).  When dots is given and the
 // form allows it, the FP32 path also leaves (z.r, z.rold) in dots[0..1] (fused with the widening
 // of z) and returns with *dots_done set.
+// the FP32 right-hand side of the V-cycle comes out of the x / r update (scaled by the r.r
+// before that update, kept in scal[23]) instead of a separate conversion pass
+static bool fused_f32_rhs(const rt_hier* h) { return h->P.precision == RT_FP32 && !h->unet; }
+
+// z = M^-1 r.  rr_dev: the scale (r.r of the residual the FP32 copy was made from);
+// f32_ready: level 0's FP32 right-hand side already holds r / sqrt(rr_dev)
 static int precondition(rt_hier* h, const double* r, double* z, const double* rr_dev, double* dots = nullptr,
-                        bool* dots_done = nullptr) {
+                        bool* dots_done = nullptr, bool f32_ready = false) {
     rt_level& L = h->L[0];
     const long n = 3 * L.nv;
     if (dots_done) *dots_done = false;
     if (h->P.precision == RT_FP32) {
-        RT_CHECK(rtk::d2f_scaled(h, n, r, L.f32, rr_dev));
+        if (!f32_ready) RT_CHECK(rtk::d2f_scaled(h, n, r, L.f32, rr_dev));
         RT_CUDA(h->ctx, cudaMemsetAsync(L.u32, 0, sizeof(float) * n, h->ctx->stream));
         RT_CHECK(vcycle_T<float>(h, h->P.smoother, h->P.pre_sweeps, h->P.post_sweeps, h->P.jacobi_omega));
         if (dots && !h->unet) {
@@ -1407,8 +1413,9 @@ static int pcg_body(rt_hier* h, double* x, double* r, bool no_support, cudaGraph
     const long n = 3 * L.nv;
     rt_ctx* c = h->ctx;
     bool dots_done = false;
+    const bool fz = fused_f32_rhs(h);
     // the projection of z (no supports) must precede its dots: no fusion then
-    RT_CHECK(precondition(h, r, h->z, h->scal + 21, no_support ? nullptr : h->scal + 10, &dots_done));
+    RT_CHECK(precondition(h, r, h->z, h->scal + (fz ? 23 : 21), no_support ? nullptr : h->scal + 10, &dots_done, fz));
     if (no_support) RT_CHECK(rtk::displacement_project(h, h->z));
     if (!dots_done) RT_CHECK(rtk::dot2(h, n, h->z, r, h->rold, h->scal + 10));
     RT_CHECK(rt_launch(c, "pcg_update_p", [&] {
@@ -1417,7 +1424,8 @@ static int pcg_body(rt_hier* h, double* x, double* r, bool no_support, cudaGraph
     }));
     RT_CHECK(rtk::fine_applyK<double>(h, h->p, h->q));
     RT_CHECK(rtk::dot(h, n, h->p, h->q, h->scal + 20));
-    RT_CHECK(rtk::pcg_update_xr_rr(h, n, h->scal + 10, h->scal + 20, x, r, h->p, h->q, h->rold, h->scal + 21));
+    RT_CHECK(rtk::pcg_update_xr_rr(h, n, h->scal + 10, h->scal + 20, x, r, h->p, h->q, h->rold, h->scal + 21,
+                                   fz ? L.f32 : nullptr, h->scal + 23));
     return rt_launch(c, "pcg_tail", [&] { k_pcg_tail<<<1, 32, 0, c->stream>>>(h->scal, cond, use_cond); });
 }
 
@@ -1489,7 +1497,12 @@ static int pcg_prologue(rt_hier* h, double* x, const double* b) {
     RT_CHECK(rtk::mask_copy(h, n, r, r));
     RT_CUDA(h->ctx, cudaMemsetAsync(h->rold, 0, sizeof(double) * n, h->ctx->stream));
     RT_CHECK(rtk::dot(h, n, b, b, h->scal + 22));
-    return rtk::dot(h, n, r, r, h->scal + 21);
+    RT_CHECK(rtk::dot(h, n, r, r, h->scal + 21));
+    if (!fused_f32_rhs(h)) return RT_OK;
+    // the first iteration's FP32 right-hand side and its scale (later ones come from the x / r update)
+    RT_CHECK(rtk::d2f_scaled(h, n, r, L.f32, h->scal + 21));
+    RT_CUDA(h->ctx, cudaMemcpyAsync(h->scal + 23, h->scal + 21, sizeof(double), cudaMemcpyDeviceToDevice, h->ctx->stream));
+    return RT_OK;
 }
 
 // a solve that produced NaN: a stencil kernel whose bounded copy wait ran out writes NaN and

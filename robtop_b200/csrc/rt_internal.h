@@ -257,7 +257,7 @@ int f2d_scaled(rt_hier* h, long n, const float* a, double* b, const double* s_de
 int f2d_scaled_add(rt_hier* h, long n, const float* a, double* b, const double* s_dev);
 // fused passes of the PCG iteration: x, r update with r.r; widening of z with (z.r, z.rold)
 int pcg_update_xr_rr(rt_hier* h, long n, const double* num, const double* den, double* x, double* r, const double* p,
-                     const double* q, double* rold, double* rr_out);
+                     const double* q, double* rold, double* rr_out, float* r32 = nullptr, double* scale_out = nullptr);
 int f2d_scaled_dot2(rt_hier* h, long n, const float* a, double* z, const double* s_dev, const double* r,
                     const double* rold, double* out);
 int pcg_update_xr(rt_hier* h, long n, const double* scal_alpha_num, const double* scal_alpha_den, double* x,

@@ -126,11 +126,17 @@ __global__ void k_pcg_xr(long n, const double* __restrict__ num, const double* _
 }
 
 // k_pcg_xr and r.r of the updated r in the same pass (partials as k_dot's: same grid, same order)
+// r32 (optional): the new residual scaled by 1 / sqrt(rr_old) and rounded to FP32, the right-hand
+// side of the next FP32 V-cycle; rr_old (the r.r before this update) is kept in scale_out
 __global__ void __launch_bounds__(RB) k_pcg_xr_rr(long n, const double* __restrict__ num, const double* __restrict__ den,
                                                   double* __restrict__ x, double* __restrict__ r,
                                                   const double* __restrict__ p, const double* __restrict__ q,
-                                                  double* __restrict__ rold, double* __restrict__ partials) {
+                                                  double* __restrict__ rold, double* __restrict__ partials,
+                                                  float* __restrict__ r32, const double* __restrict__ rr_old,
+                                                  double* __restrict__ scale_out) {
     const double alpha = den[0] != 0.0 ? num[0] / den[0] : 0.0;
+    const double inv = r32 ? 1.0 / sqrt(fmax(rr_old[0], 1e-300)) : 0.0;
+    if (r32 && blockIdx.x == 0 && threadIdx.x == 0) scale_out[0] = rr_old[0];
     double v[1] = {0};
     // the reduction grid is small (2 blocks per SM): XR_U grid strides per trip keep enough loads in
     // flight; the sum still runs over each thread's elements in stride order, as in k_dot
@@ -150,6 +156,7 @@ __global__ void __launch_bounds__(RB) k_pcg_xr_rr(long n, const double* __restri
             x[i] = xi[k] + alpha * pi[k];
             const double rn = ri[k] - alpha * qi[k];
             r[i] = rn;
+            if (r32) r32[i] = (float)(rn * inv);
             v[0] += rn * rn;
         }
     }
@@ -552,9 +559,10 @@ int pcg_update_xr(rt_hier* h, long n, const double* num, const double* den, doub
 }
 
 int pcg_update_xr_rr(rt_hier* h, long n, const double* num, const double* den, double* x, double* r, const double* p,
-                     const double* q, double* rold, double* rr_out) {
+                     const double* q, double* rold, double* rr_out, float* r32, double* scale_out) {
     RT_CHECK(rt_launch(h->ctx, "pcg_update_xr", [&] {
-        k_pcg_xr_rr<<<RT_RED_BLOCKS, RB, 0, h->ctx->stream>>>(n, num, den, x, r, p, q, rold, h->partials);
+        k_pcg_xr_rr<<<RT_RED_BLOCKS, RB, 0, h->ctx->stream>>>(n, num, den, x, r, p, q, rold, h->partials, r32, rr_out,
+                                                               scale_out);
     }));
     return final_sum(h, 1, rr_out);
 }
