@@ -457,6 +457,8 @@ def run_c1(args):
     e2e_ms = e0.elapsed_time(e1)
     clk = clocks.stop()
     it = infos[-1].iterations
+    G[0].setRho(rho0)
+    G.update_stencil()
     lmax0 = G.smoother_lmax(0)
     # the same solve with omega 0.6, for the record
     q = G.params
