@@ -215,6 +215,7 @@ extern "C" void rt_params_default(rt_params* p) {
     p->coarse_sweeps = 0;
     p->precision_fallback = 100;
     p->coarse_bf16 = 0;
+    p->krylov_fp32 = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -302,6 +303,9 @@ static void free_workspace(rt_hier* w) {
     cudaFree(w->partials); cudaFree(w->scal);
     if (w->pcg_exec) cudaGraphExecDestroy(w->pcg_exec);
     if (w->pcg_graph) cudaGraphDestroy(w->pcg_graph);
+    if (w->pcg32_exec) cudaGraphExecDestroy(w->pcg32_exec);
+    if (w->pcg32_graph) cudaGraphDestroy(w->pcg32_graph);
+    cudaFree(w->p32k); cudaFree(w->q32k); cudaFree(w->d32k); cudaFree(w->ro32k);
     rt_ctx* c = w->ctx;
     delete w;
     rt_ctx_release(c);
@@ -332,6 +336,9 @@ static void free_hier(rt_hier* h) {
     cudaFree(h->scal); cudaFree(h->Qgal); cudaFree(h->dinv64); cudaFree(h->dinv32);
     if (h->pcg_exec) cudaGraphExecDestroy(h->pcg_exec);
     if (h->pcg_graph) cudaGraphDestroy(h->pcg_graph);
+    if (h->pcg32_exec) cudaGraphExecDestroy(h->pcg32_exec);
+    if (h->pcg32_graph) cudaGraphDestroy(h->pcg32_graph);
+    cudaFree(h->p32k); cudaFree(h->q32k); cudaFree(h->d32k); cudaFree(h->ro32k);
     rt_ctx* c = h->ctx;
     delete h;
     rt_ctx_release(c);
@@ -1303,7 +1310,7 @@ extern "C" int rt_relative_residual(rt_hier* h, double* rel) {
 // of z) and returns with *dots_done set.
 // the FP32 right-hand side of the V-cycle comes out of the x / r update (scaled by the r.r
 // before that update, kept in scal[23]) instead of a separate conversion pass
-static bool fused_f32_rhs(const rt_hier* h) { return h->P.precision == RT_FP32 && !h->unet; }
+static bool fused_f32_rhs(const rt_hier* h) { return h->P.precision == RT_FP32 && !h->unet && !h->P.krylov_fp32; }
 
 // z = M^-1 r.  rr_dev: the scale (r.r of the residual the FP32 copy was made from);
 // f32_ready: level 0's FP32 right-hand side already holds r / sqrt(rr_dev)
@@ -1517,8 +1524,180 @@ static int nan_fail(rt_hier* h, int it) {
     return rt_fail(h->ctx, RT_ENAN, "NaN in PCG at iteration %d", it);
 }
 
+// ---------------------------------------------------------------------------
+// FP32 Krylov form (rt_params.krylov_fp32 with precision RT_FP32): flexible CG whose vectors,
+// operator products and V-cycles are all FP32 (every dot product summed in FP64), solving
+// K d = r / |r| for the FP64 residual r = b - K x; x += |r| d, then the FP64 residual is
+// recomputed and the next inner solve starts from it (iterative refinement)
+// ---------------------------------------------------------------------------
+static int ensure_krylov32(rt_hier* h) {
+    if (h->p32k) return RT_OK;
+    const size_t n = 3 * (size_t)h->L[0].nv;
+    RT_CHECK(dalloc(h->ctx, &h->p32k, n));
+    RT_CHECK(dalloc(h->ctx, &h->q32k, n));
+    RT_CHECK(dalloc(h->ctx, &h->d32k, n));
+    return dalloc(h->ctx, &h->ro32k, n);
+}
+
+// one inner iteration: z = V(res) (res is level 0's FP32 right-hand side, z its FP32 solution),
+// flexible beta, p, q = K p, alpha, d += alpha p, res -= alpha q, then the loop test
+static int pcg32_body(rt_hier* h, cudaGraphConditionalHandle cond, int use_cond) {
+    rt_level& L = h->L[0];
+    const long n = 3 * L.nv;
+    rt_ctx* c = h->ctx;
+    RT_CUDA(c, cudaMemsetAsync(L.u32, 0, sizeof(float) * n, c->stream));
+    RT_CHECK(vcycle_T<float>(h, h->P.smoother, h->P.pre_sweeps, h->P.post_sweeps, h->P.jacobi_omega));
+    RT_CHECK(rtk::dot32_2(h, n, L.u32, L.f32, h->ro32k, h->scal + 10));
+    RT_CHECK(rtk::pcg32_update_p(h, n, h->scal + 10, h->scal + 24, h->p32k, L.u32));
+    RT_CHECK(rtk::fine_applyK<float>(h, h->p32k, h->q32k));
+    RT_CHECK(rtk::dot32(h, n, h->p32k, h->q32k, h->scal + 20));
+    RT_CHECK(rtk::pcg32_update_xr_rr(h, n, h->scal + 10, h->scal + 20, h->d32k, L.f32, h->p32k, h->q32k, h->ro32k,
+                                     h->scal + 21));
+    return rt_launch(c, "pcg_tail", [&] { k_pcg_tail<<<1, 32, 0, c->stream>>>(h->scal, cond, use_cond); });
+}
+
+// the inner loop as one graph with a WHILE conditional node (as pcg_graph_run)
+static int pcg32_graph_run(rt_hier* h) {
+    rt_ctx* c = h->ctx;
+    uint64_t key = 1469598103934665603ull;
+    auto mix = [&](uint64_t v) { key = (key ^ v) * 1099511628211ull; };
+    mix(h->graph_epoch);
+    mix((uint64_t)h->P.smoother | ((uint64_t)h->P.pre_sweeps << 8) | ((uint64_t)h->P.post_sweeps << 16) |
+        ((uint64_t)h->P.cycle_gamma << 24) | ((uint64_t)h->P.coarse_sweeps << 32) | ((uint64_t)h->P.coarse_bf16 << 40));
+    uint64_t om;
+    memcpy(&om, &h->P.jacobi_omega, 8);
+    mix(om);
+    if (!h->pcg32_exec || h->pcg32_key != key) {
+        if (h->pcg32_exec) { cudaGraphExecDestroy(h->pcg32_exec); h->pcg32_exec = nullptr; }
+        if (h->pcg32_graph) { cudaGraphDestroy(h->pcg32_graph); h->pcg32_graph = nullptr; }
+        cudaGraph_t g;
+        RT_CUDA(c, cudaGraphCreate(&g, 0));
+        cudaGraphConditionalHandle cond;
+        RT_CUDA(c, cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cond;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        RT_CUDA(c, cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        RT_CUDA(c, cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        int s = pcg32_body(h, cond, 1);
+        cudaGraph_t captured = nullptr;
+        cudaError_t e = cudaStreamEndCapture(c->stream, &captured);
+        if (s != RT_OK) { cudaGraphDestroy(g); return s; }
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(g);
+            return rt_fail(c, RT_ECUDA, "FP32 PCG graph capture failed: %s", cudaGetErrorString(e));
+        }
+        cudaGraphExec_t exec;
+        e = cudaGraphInstantiate(&exec, g, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(g);
+            return rt_fail(c, RT_ECUDA, "FP32 PCG graph instantiation failed: %s", cudaGetErrorString(e));
+        }
+        h->pcg32_graph = g;
+        h->pcg32_exec = exec;
+        h->pcg32_key = key;
+    }
+    RT_CUDA(c, cudaGraphLaunch(h->pcg32_exec, c->stream));
+    c->launches += 1;
+    return RT_OK;
+}
+
+static int pcg_core(rt_hier* h, double* x, const double* b, double tol, int maxit, rt_solve_info* info, int* vcycles);
+
+static int pcg32_core(rt_hier* h, double* x, const double* b, double tol, int maxit, rt_solve_info* info, int* vcycles) {
+    RT_CHECK(ensure_krylov32(h));
+    rt_ctx* c = h->ctx;
+    rt_level& L = h->L[0];
+    const long n = 3 * L.nv;
+    RT_CHECK(pcg_prologue(h, x, b));
+    double s[2];
+    RT_CHECK(read_scalars(h, 21, 2, s));
+    const double bn = std::sqrt(s[1]) > 0 ? std::sqrt(s[1]) : 1.0;
+    double rel = std::sqrt(s[0]) / bn;
+    int it = 0;
+    bool stalled = false;
+    const bool fallback = h->P.precision_fallback > 0;
+    while (rel > tol && it < maxit) {
+        // the inner solve aims at the outer target, no tighter than FP32 can hold it
+        const double tol_in = std::min(0.5, std::max(0.9 * tol / rel, 1e-4));
+        RT_CHECK(rtk::d2f_scaled(h, n, h->rr, L.f32, h->scal + 21));
+        RT_CUDA(c, cudaMemcpyAsync(h->scal + 23, h->scal + 21, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        RT_CUDA(c, cudaMemsetAsync(h->d32k, 0, sizeof(float) * n, c->stream));
+        RT_CUDA(c, cudaMemsetAsync(h->ro32k, 0, sizeof(float) * n, c->stream));
+        // inner loop state: scal[24..29] iteration count, tolerance, budget, no learned
+        // correction (ratio, gate, previous r.r); scal[21..22] the unit right-hand side's r.r
+        // and b.b; scal[90..93] stall detection as in pcg_core
+        const double st[6] = {0.0, tol_in, (double)(maxit - it), 0.0, 0.0, 1.0};
+        memcpy(c->hscal + 8, st, sizeof(st));
+        RT_CUDA(c, cudaMemcpyAsync(h->scal + 24, c->hscal + 8, sizeof(st), cudaMemcpyHostToDevice, c->stream));
+        const double unit[2] = {1.0, 1.0};
+        memcpy(c->hscal + 20, unit, sizeof(unit));
+        RT_CUDA(c, cudaMemcpyAsync(h->scal + 21, c->hscal + 20, sizeof(unit), cudaMemcpyHostToDevice, c->stream));
+        double sd[4] = {1.0, 0.0, 0.0, fallback ? (double)h->P.precision_fallback : 0.0};
+        memcpy(c->hscal + 16, sd, sizeof(sd));
+        RT_CUDA(c, cudaMemcpyAsync(h->scal + 90, c->hscal + 16, sizeof(sd), cudaMemcpyHostToDevice, c->stream));
+        if (h->use_graphs && !c->profile) {
+            RT_CHECK(pcg32_graph_run(h));
+        } else {
+            for (int k = 0; k < maxit - it; k++) {
+                RT_CHECK(pcg32_body(h, 0, 0));
+                double s2 = 0, stall = 0;
+                RT_CHECK(read_scalars(h, 21, 1, &s2));
+                RT_CHECK(read_scalars(h, 92, 1, &stall));
+                if (!std::isfinite(s2) || std::sqrt(s2) <= tol_in || stall != 0.0) break;
+            }
+        }
+        double s3[4], stall = 0;
+        RT_CHECK(read_scalars(h, 21, 4, s3));  // inner r.r, 1, |r|^2 of the outer residual, inner iterations
+        RT_CHECK(read_scalars(h, 92, 1, &stall));
+        if (!std::isfinite(s3[0])) {
+            if (info) { info->status = RT_ENAN; info->iterations = it + (int)s3[3]; }
+            return nan_fail(h, it + (int)s3[3]);
+        }
+        const int its_in = (int)s3[3];
+        RT_CHECK(rtk::axpy_f32_scaled(h, n, x, h->d32k, h->scal + 23));
+        RT_CHECK(pcg_prologue(h, x, b));
+        RT_CHECK(read_scalars(h, 21, 1, s));
+        rel = std::sqrt(s[0]) / bn;
+        it += its_in;
+        if (its_in == 0) break;
+        if (stall != 0.0) {
+            stalled = true;
+            break;
+        }
+    }
+    if (fallback && stalled && rel > tol && it < maxit) {
+        // the FP32 cycles stopped reducing |r|: continue from x with FP64 V-cycles and FP64 vectors
+        const int saved = h->P.precision;
+        h->P.precision = RT_FP64;
+        rt_solve_info sub;
+        memset(&sub, 0, sizeof(sub));
+        int vc = 0;
+        const int st2 = pcg_core(h, x, b, tol, maxit - it, &sub, &vc);
+        h->P.precision = saved;
+        RT_CHECK(st2);
+        it += sub.iterations;
+        rel = sub.rel_residual;
+        h->fallbacks++;
+    }
+    *vcycles += it;
+    if (info) {
+        info->iterations = it;
+        info->rel_residual = rel;
+        info->status = rel <= tol ? RT_OK : RT_ENOCONV;
+    }
+    return RT_OK;
+}
+
 static int pcg_core(rt_hier* h, double* x, const double* b, double tol, int maxit, rt_solve_info* info, int* vcycles) {
     double* r = h->rr;
+    if (h->P.precision == RT_FP32 && h->P.krylov_fp32 && !h->unet && h->P.mode != RT_MODE_NSCF &&
+        h->P.mode != RT_MODE_NSFF)
+        return pcg32_core(h, x, b, tol, maxit, info, vcycles);
     RT_CHECK(pcg_prologue(h, x, b));
     double s[2];
     RT_CHECK(read_scalars(h, 21, 2, s));

@@ -119,6 +119,11 @@ struct rt_hier {
     int Qcap = 0;
     // reductions
     double* partials = nullptr;  // [RT_RED_BLOCKS * 8]
+    // FP32 Krylov vectors of the refinement form (rt_params.krylov_fp32), allocated on first use
+    float *p32k = nullptr, *q32k = nullptr, *d32k = nullptr, *ro32k = nullptr;
+    cudaGraph_t pcg32_graph = nullptr;
+    cudaGraphExec_t pcg32_exec = nullptr;
+    uint64_t pcg32_key = 0;
     double* scal = nullptr;      // [64] device scalars
     bool stencil_ready = false;
     double* Qgal = nullptr;  // [R^3][576] cell Galerkin blocks P^T KE P (rebuilt when KE changes)
@@ -258,6 +263,12 @@ int f2d_scaled_add(rt_hier* h, long n, const float* a, double* b, const double* 
 // fused passes of the PCG iteration: x, r update with r.r; widening of z with (z.r, z.rold)
 int pcg_update_xr_rr(rt_hier* h, long n, const double* num, const double* den, double* x, double* r, const double* p,
                      const double* q, double* rold, double* rr_out, float* r32 = nullptr, double* scale_out = nullptr);
+int dot32(rt_hier* h, long n, const float* a, const float* b, double* out);
+int dot32_2(rt_hier* h, long n, const float* a, const float* b, const float* c, double* out);
+int pcg32_update_p(rt_hier* h, long n, const double* s, const double* it, float* p, const float* z);
+int pcg32_update_xr_rr(rt_hier* h, long n, const double* num, const double* den, float* d, float* r, const float* p,
+                       const float* q, float* rold, double* rr_out);
+int axpy_f32_scaled(rt_hier* h, long n, double* x, const float* d, const double* s);
 int f2d_scaled_dot2(rt_hier* h, long n, const float* a, double* z, const double* s_dev, const double* r,
                     const double* rold, double* out);
 int pcg_update_xr(rt_hier* h, long n, const double* scal_alpha_num, const double* scal_alpha_den, double* x,

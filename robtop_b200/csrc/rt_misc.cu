@@ -192,6 +192,73 @@ __global__ void __launch_bounds__(RB) k_f2d_scaled_dot2(long n, const float* __r
     block_reduce_store<2>(v, partials);
 }
 
+// ---- FP32 Krylov vectors (FP64 accumulation of every dot product) ----------------------
+__global__ void __launch_bounds__(RB) k_dot32(long n, const float* __restrict__ a, const float* __restrict__ b,
+                                              double* __restrict__ partials) {
+    double v[1] = {0};
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        v[0] += (double)a[i] * (double)b[i];
+    block_reduce_store<1>(v, partials);
+}
+
+__global__ void __launch_bounds__(RB) k_dot32_2(long n, const float* __restrict__ a, const float* __restrict__ b,
+                                                const float* __restrict__ c, double* __restrict__ partials) {
+    double v[2] = {0, 0};
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const double x = a[i];
+        v[0] += x * (double)b[i];
+        v[1] += x * (double)c[i];
+    }
+    block_reduce_store<2>(v, partials);
+}
+
+// p = z + beta p (flexible beta as k_pcg_p_it), FP32 vectors
+__global__ void k_pcg32_p(long n, const double* __restrict__ s, const double* __restrict__ it, float* __restrict__ p,
+                          const float* __restrict__ z) {
+    const bool first = it[0] == 0.0;
+    const double den = s[2];
+    const float beta = (first || den == 0.0) ? 0.f : (float)((s[0] - s[1]) / den);
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        p[i] = first ? z[i] : z[i] + beta * p[i];
+}
+
+// d += alpha p, rold = r, r -= alpha q, r.r (FP64 sum) with alpha = num / den
+__global__ void __launch_bounds__(RB) k_pcg32_xr_rr(long n, const double* __restrict__ num, const double* __restrict__ den,
+                                                    float* __restrict__ d, float* __restrict__ r,
+                                                    const float* __restrict__ p, const float* __restrict__ q,
+                                                    float* __restrict__ rold, double* __restrict__ partials) {
+    const float alpha = den[0] != 0.0 ? (float)(num[0] / den[0]) : 0.f;
+    double v[1] = {0};
+    const long st = (long)gridDim.x * blockDim.x;
+    for (long i0 = blockIdx.x * (long)blockDim.x + threadIdx.x; i0 < n; i0 += XR_U * st) {
+        float ri[XR_U], pi[XR_U], qi[XR_U], di[XR_U];
+#pragma unroll
+        for (int k = 0; k < XR_U; k++) {
+            const long i = i0 + k * st;
+            if (i < n) { ri[k] = r[i]; pi[k] = p[i]; qi[k] = q[i]; di[k] = d[i]; }
+        }
+#pragma unroll
+        for (int k = 0; k < XR_U; k++) {
+            const long i = i0 + k * st;
+            if (i >= n) break;
+            rold[i] = ri[k];
+            d[i] = di[k] + alpha * pi[k];
+            const float rn = ri[k] - alpha * qi[k];
+            r[i] = rn;
+            v[0] += (double)rn * (double)rn;
+        }
+    }
+    block_reduce_store<1>(v, partials);
+}
+
+// x += sqrt(s) d (the FP32 correction of a refinement step, scaled back to the FP64 residual)
+__global__ void k_axpy_f32_scaled(long n, double* __restrict__ x, const float* __restrict__ d,
+                                  const double* __restrict__ s) {
+    const double sc = sqrt(fmax(s[0], 0.0));
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        x[i] += sc * (double)d[i];
+}
+
 // p = z + beta p with flexible beta = (r.z - rold.z) / rz_old; scalars: s[0]=r.z, s[1]=rold.z, den=rz_old
 __global__ void k_pcg_p(long n, const double* __restrict__ s, const double* __restrict__ den, double* __restrict__ p,
                         const double* __restrict__ z, int first) {
@@ -573,6 +640,36 @@ int f2d_scaled_dot2(rt_hier* h, long n, const float* a, double* z, const double*
         k_f2d_scaled_dot2<<<RT_RED_BLOCKS, RB, 0, h->ctx->stream>>>(n, a, z, s, r, rold, h->partials);
     }));
     return final_sum(h, 2, out);
+}
+
+int dot32(rt_hier* h, long n, const float* a, const float* b, double* out) {
+    RT_CHECK(rt_launch(h->ctx, "dot32", [&] { k_dot32<<<RT_RED_BLOCKS, RB, 0, h->ctx->stream>>>(n, a, b, h->partials); }));
+    return final_sum(h, 1, out);
+}
+
+int dot32_2(rt_hier* h, long n, const float* a, const float* b, const float* c, double* out) {
+    RT_CHECK(rt_launch(h->ctx, "dot32_2", [&] {
+        k_dot32_2<<<RT_RED_BLOCKS, RB, 0, h->ctx->stream>>>(n, a, b, c, h->partials);
+    }));
+    return final_sum(h, 2, out);
+}
+
+int pcg32_update_p(rt_hier* h, long n, const double* s, const double* it, float* p, const float* z) {
+    return rt_launch(h->ctx, "pcg32_update_p",
+                     [&] { k_pcg32_p<<<gridN(h->ctx, n), 256, 0, h->ctx->stream>>>(n, s, it, p, z); });
+}
+
+int pcg32_update_xr_rr(rt_hier* h, long n, const double* num, const double* den, float* d, float* r, const float* p,
+                       const float* q, float* rold, double* rr_out) {
+    RT_CHECK(rt_launch(h->ctx, "pcg32_update_xr", [&] {
+        k_pcg32_xr_rr<<<RT_RED_BLOCKS, RB, 0, h->ctx->stream>>>(n, num, den, d, r, p, q, rold, h->partials);
+    }));
+    return final_sum(h, 1, rr_out);
+}
+
+int axpy_f32_scaled(rt_hier* h, long n, double* x, const float* d, const double* s) {
+    return rt_launch(h->ctx, "axpy_f32",
+                     [&] { k_axpy_f32_scaled<<<gridN(h->ctx, n), 256, 0, h->ctx->stream>>>(n, x, d, s); });
 }
 
 int pcg_update_p(rt_hier* h, long n, const double* s, const double* den, double* p, const double* z, bool first) {

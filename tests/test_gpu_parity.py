@@ -397,6 +397,38 @@ def test_pcg_to_1e6(pair, precision, smoother, sweeps, bf16):
     G.update_stencil()
 
 
+@pytest.mark.parametrize("gamma", [1, 2])
+def test_pcg_fp32_krylov_refinement(pair, gamma):
+    """FP32 Krylov vectors with FP64 iterative refinement (krylov_fp32): the answer meets 1e-6
+    in the FP64 residual computed by the oracle's operator; modes without supports take the
+    FP64-vector form."""
+    cfg, ctx, G, H = pair
+    b = _rand_vec(G, 0, 83)
+    if cfg["mode"] in (rb.MODE_WSCF, rb.MODE_WSFF):
+        b[np.tile(cfg["vfix"].ravel().astype(bool), 3)] = 0
+    else:
+        Ru = np.zeros(6 * b.size)
+        O.lib().or_rigid_nodes(H.lv(0), O.ptr(Ru))
+        O.lib().or_displacement_project(b.size // 3, O.ptr(Ru), O.ptr(b))
+    params = G.params
+    params.precision, params.smoother = rb.FP32, rb.SMOOTH_CHEBY
+    params.pre_sweeps = params.post_sweeps = 2
+    params.cycle_gamma, params.krylov_fp32 = gamma, 1
+    G.set_params(params)
+    G.update_stencil()
+    G[0].setForce(b)
+    G[0].reset_displacement()
+    info = G.pcg(1e-6, 1000)
+    assert info.status == 0 and info.rel_residual <= 1e-6
+    r = (b - H.applyK(G[0].getDisplacement())) * np.tile(H.arrs[0]["vact"], 3)
+    assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.01e-6
+    params.precision, params.smoother = rb.FP64, rb.SMOOTH_SGS
+    params.pre_sweeps = params.post_sweeps = 1
+    params.cycle_gamma, params.krylov_fp32 = 1, 0
+    G.set_params(params)
+    G.update_stencil()
+
+
 def test_modified_pm_parity(pair):
     cfg, ctx, G, H = pair
     lam, info = G.worst_case(rb.WORST_MODPM, 500, 0.0, seed=9)
