@@ -34,18 +34,22 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = dict(nx=128, ny=128, nz=64, seed=0, k=16, tol=1e-6)
 # plain: the reference's V-cycle made symmetric (8-colour GS, forward pre / backward post), all FP64
-# mixed: FP32 V-cycle with Chebyshev(2) smoothing (8 steps on the coarse levels) inside FP64 flexible
-#        CG, FP64 coarsest solve, FP64 V-cycles once the FP32 ones stall
+# mixed: FP32 V-cycle with Chebyshev(2) smoothing (8 steps on the coarse levels), FP64 coarsest solve,
+#        FP32 flexible-CG vectors restarted from FP64 residuals (iterative refinement), FP64 V-cycles
+#        once the FP32 ones stall
 FORMS = {"plain": dict(precision="FP64", smoother="SMOOTH_SGS", sweeps=1, coarse_sweeps=0, cycle_gamma=1,
-                       coarse_bf16=0),
+                       coarse_bf16=0, krylov_fp32=0),
          "mixed": dict(precision="FP32", smoother="SMOOTH_CHEBY", sweeps=2, coarse_sweeps=8, cycle_gamma=1,
-                       coarse_bf16=0)}
+                       coarse_bf16=0, krylov_fp32=2)}
+# the batched graph runs FP64-vector CG (the Krylov form is a single-solve path): the sequential
+# solves it is compared with use the same form
+FORMS_BATCH = dict(FORMS["mixed"], krylov_fp32=0)
 # on the 511x256x256 arch the W-cycle (coarse corrections twice per visit below level 1) wins
 FORMS_C5 = {"plain": FORMS["plain"],
             "mixed": dict(precision="FP32", smoother="SMOOTH_CHEBY", sweeps=2, coarse_sweeps=0, cycle_gamma=2,
-                          coarse_bf16=0),
+                          coarse_bf16=0, krylov_fp32=0),
             "fp64_same_cycle": dict(precision="FP64", smoother="SMOOTH_CHEBY", sweeps=2, coarse_sweeps=0,
-                                    cycle_gamma=2, coarse_bf16=0)}
+                                    cycle_gamma=2, coarse_bf16=0, krylov_fp32=0)}
 
 
 def apply_form(rb, G, form):
@@ -56,6 +60,7 @@ def apply_form(rb, G, form):
     p.coarse_sweeps = form["coarse_sweeps"]
     p.cycle_gamma = form["cycle_gamma"]
     p.coarse_bf16 = form["coarse_bf16"]
+    p.krylov_fp32 = form.get("krylov_fp32", 0)
     G.set_params(p)
 
 
@@ -63,7 +68,8 @@ def form_text(form):
     return (f"{form['precision']} V-cycle{' (W below level 1)' if form['cycle_gamma'] == 2 else ''}, "
             f"{form['smoother'][7:].lower()}({form['sweeps']}) smoothing"
             f"{', ' + str(form['coarse_sweeps']) + ' steps on coarse levels' if form['coarse_sweeps'] else ''}"
-            f"{', BF16 coarse stencils' if form['coarse_bf16'] else ''}")
+            f"{', BF16 coarse stencils' if form['coarse_bf16'] else ''}"
+            f"{', FP32 Krylov vectors with FP64 refinement' if form.get('krylov_fp32') else ''}")
 METRIC = "worst-case solve (Lanczos k=16, MG-PCG inner solves to rel. residual 1e-6) on 128x128x64"
 
 
@@ -702,7 +708,7 @@ def run_batched(args):
         cfg["rho"] = configs.smoothed_density(cfg["eact"].shape, 2 + i)
         G = rb.HierarchyGrid(ctx, params(cfg["mode"]))
         G.genFromBox(cfg["eact"])
-        apply_form(rb, G, FORMS["mixed"])
+        apply_form(rb, G, FORMS_BATCH)
         G[0].setRho(cfg["rho"].ravel())
         G.set_support(cfg["vfix"])
         G.update_stencil()
@@ -713,7 +719,7 @@ def run_batched(args):
     big_cfg = configs.worst_case_box(256, 256, 128, seed=0)
     big = rb.HierarchyGrid(ctx, params(big_cfg["mode"]))
     big.genFromBox(big_cfg["eact"])
-    apply_form(rb, big, FORMS["mixed"])
+    apply_form(rb, big, FORMS_BATCH)
     big[0].setRho(big_cfg["rho"].ravel())
     big.set_support(big_cfg["vfix"])
     big.update_stencil()
@@ -779,7 +785,7 @@ def run_batched(args):
             "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
             "config": {"workload": "12 cantilevers (sizes " + ";".join("x".join(map(str, s)) for s in sizes) +
                                    ") + 8 top-face loads on the 256x256x128 worst-case box",
-                       "form": form_text(FORMS["mixed"]) + " in FP64 flexible CG, per-step reset of u on the device",
+                       "form": form_text(FORMS_BATCH) + " in FP64 flexible CG, per-step reset of u on the device",
                        "sequential_ms_per_step": ts / args.steps, "batch_speedup": ts / tb,
                        "iterations": [i.iterations for i in infos_b],
                        "iterations_sequential": [i.iterations for i in infos_s],
@@ -1093,8 +1099,9 @@ def main():
         "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
         "config": {"workload": "worst-case 128x128x64 (smoothed random density, z=0 clamped, top-face load set, "
                                "wsff), Lanczos k=16, inner MG-PCG to 1e-6, stencil assembly included",
-                   "form": "mixed: " + form_text(FORMS["mixed"]) + ", FP64 coarsest solve, inside FP64 flexible "
-                           "CG, one CUDA graph per solve; plain (fp64_ms_per_step): FP64 symmetric-GS V-cycle",
+                   "form": "mixed: " + form_text(FORMS["mixed"]) + ", FP64 coarsest solve, FP64 residual "
+                           "recomputed at each refinement restart, one CUDA graph per inner solve; plain "
+                           "(fp64_ms_per_step): FP64 symmetric-GS V-cycle in FP64 flexible CG",
                    "fp64_ms_per_step": r64["ms"] / args.steps if r64 else None,
                    "speedup_vs_fp64": r64["ms"] / r32["ms"] if r64 else None,
                    "lambda_mixed": lam32, "lambda_fp64": lam64,

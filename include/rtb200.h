@@ -92,10 +92,11 @@ typedef struct rt_params {
     int coarse_bf16;        /* 1: the FP32 smoother on levels >= 1 reads the stencils stored in BF16 (half the
                                bytes of the FP32 copy); residuals, restriction and the coarsest solve keep FP32 /
                                FP64 stencils.  0 (default): FP32 stencils */
-    int krylov_fp32;        /* 1 (with precision RT_FP32, supported modes, no learned correction): the CG vectors
-                               and the operator product of rt_pcg are FP32 too (dot products summed in FP64); each
-                               inner solve of K d = r / |r| is followed by x += |r| d and a fresh FP64 residual
-                               (iterative refinement).  0 (default): FP64 flexible CG around the FP32 V-cycle */
+    int krylov_fp32;        /* k = 1..4 (with precision RT_FP32, supported modes, no learned correction): the CG
+                               vectors and the operator product of rt_pcg are FP32 too (dot products summed in
+                               FP64); each inner solve of K d = r / |r| (to the outer target, at most down to
+                               10^-(3+k)) is followed by x += |r| d and a fresh FP64 residual (iterative
+                               refinement).  0 (default): FP64 flexible CG around the FP32 V-cycle */
 } rt_params;
 
 typedef struct rt_solve_info {

@@ -1470,7 +1470,11 @@ static int pcg_graph_run(rt_hier* h, double* x, double* r, bool no_support) {
         RT_CUDA(c, cudaGraphAddNode(&node, g, nullptr, 0, &cp));
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         RT_CUDA(c, cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        // captured launches are counted when the graph runs, once per executed iteration
+        const long l0 = c->launches;
         int s = pcg_body(h, x, r, no_support, cond, 1);
+        h->pcg_iter_kernels = c->launches - l0;
+        c->launches = l0;
         cudaGraph_t captured = nullptr;
         cudaError_t e = cudaStreamEndCapture(c->stream, &captured);
         if (s != RT_OK) { cudaGraphDestroy(g); return s; }
@@ -1489,7 +1493,6 @@ static int pcg_graph_run(rt_hier* h, double* x, double* r, bool no_support) {
         h->pcg_key = key;
     }
     RT_CUDA(c, cudaGraphLaunch(h->pcg_exec, c->stream));
-    c->launches += 1;
     return RT_OK;
 }
 
@@ -1583,7 +1586,10 @@ static int pcg32_graph_run(rt_hier* h) {
         RT_CUDA(c, cudaGraphAddNode(&node, g, nullptr, 0, &cp));
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         RT_CUDA(c, cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        const long l0 = c->launches;
         int s = pcg32_body(h, cond, 1);
+        h->pcg32_iter_kernels = c->launches - l0;
+        c->launches = l0;
         cudaGraph_t captured = nullptr;
         cudaError_t e = cudaStreamEndCapture(c->stream, &captured);
         if (s != RT_OK) { cudaGraphDestroy(g); return s; }
@@ -1602,7 +1608,6 @@ static int pcg32_graph_run(rt_hier* h) {
         h->pcg32_key = key;
     }
     RT_CUDA(c, cudaGraphLaunch(h->pcg32_exec, c->stream));
-    c->launches += 1;
     return RT_OK;
 }
 
@@ -1622,8 +1627,9 @@ static int pcg32_core(rt_hier* h, double* x, const double* b, double tol, int ma
     bool stalled = false;
     const bool fallback = h->P.precision_fallback > 0;
     while (rel > tol && it < maxit) {
-        // the inner solve aims at the outer target, no tighter than FP32 can hold it
-        const double tol_in = std::min(0.5, std::max(0.9 * tol / rel, 1e-4));
+        // the inner solve aims at the outer target, no tighter than 10^-(3 + krylov_fp32)
+        const double floor_in = std::pow(10.0, -3.0 - std::min(std::max(h->P.krylov_fp32, 1), 4));
+        const double tol_in = std::min(0.5, std::max(0.9 * tol / rel, floor_in));
         RT_CHECK(rtk::d2f_scaled(h, n, h->rr, L.f32, h->scal + 21));
         RT_CUDA(c, cudaMemcpyAsync(h->scal + 23, h->scal + 21, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
         RT_CUDA(c, cudaMemsetAsync(h->d32k, 0, sizeof(float) * n, c->stream));
@@ -1640,7 +1646,8 @@ static int pcg32_core(rt_hier* h, double* x, const double* b, double tol, int ma
         double sd[4] = {1.0, 0.0, 0.0, fallback ? (double)h->P.precision_fallback : 0.0};
         memcpy(c->hscal + 16, sd, sizeof(sd));
         RT_CUDA(c, cudaMemcpyAsync(h->scal + 90, c->hscal + 16, sizeof(sd), cudaMemcpyHostToDevice, c->stream));
-        if (h->use_graphs && !c->profile) {
+        const bool graphed = h->use_graphs && !c->profile;
+        if (graphed) {
             RT_CHECK(pcg32_graph_run(h));
         } else {
             for (int k = 0; k < maxit - it; k++) {
@@ -1659,6 +1666,7 @@ static int pcg32_core(rt_hier* h, double* x, const double* b, double tol, int ma
             return nan_fail(h, it + (int)s3[3]);
         }
         const int its_in = (int)s3[3];
+        if (graphed) c->launches += h->pcg32_iter_kernels * its_in;
         RT_CHECK(rtk::axpy_f32_scaled(h, n, x, h->d32k, h->scal + 23));
         RT_CHECK(pcg_prologue(h, x, b));
         RT_CHECK(read_scalars(h, 21, 1, s));
@@ -1720,7 +1728,8 @@ static int pcg_core(rt_hier* h, double* x, const double* b, double tol, int maxi
         memcpy(h->ctx->hscal + 16, sd, sizeof(sd));
         RT_CUDA(h->ctx, cudaMemcpyAsync(h->scal + 90, h->ctx->hscal + 16, sizeof(sd), cudaMemcpyHostToDevice,
                                         h->ctx->stream));
-        if (h->use_graphs && !h->ctx->profile) {
+        const bool graphed = h->use_graphs && !h->ctx->profile;
+        if (graphed) {
             RT_CHECK(pcg_graph_run(h, x, r, no_support));
         } else {
             for (int k = 0; k < maxit; k++) {
@@ -1740,6 +1749,7 @@ static int pcg_core(rt_hier* h, double* x, const double* b, double tol, int maxi
         }
         rel = std::sqrt(s3[0]) / bn;
         it = (int)s3[3];
+        if (graphed) h->ctx->launches += h->pcg_iter_kernels * it;
         if (fallback && stall != 0.0 && rel > tol && it < maxit) {
             // continue from the current iterate with FP64 V-cycles (flexible CG restarts)
             const int saved = h->P.precision;
@@ -2467,10 +2477,14 @@ static bool no_support_mode(const rt_hier* h) { return h->P.mode == RT_MODE_NSCF
 
 // one graph: per instance, prologue (child graph) -> k_pcg_start -> WHILE(one PCG iteration);
 // the instances share no node, so the device runs their kernels concurrently
-static int build_batch_graph(rt_ctx* c, rt_hier* const* hs, int n, double tol, int maxit, cudaGraph_t* out) {
+static int build_batch_graph(rt_ctx* c, rt_hier* const* hs, int n, double tol, int maxit, cudaGraph_t* out,
+                             std::vector<long>* once_kernels, std::vector<long>* iter_kernels) {
     cudaGraph_t g;
     RT_CUDA(c, cudaGraphCreate(&g, 0));
+    // captured launches are counted when the graph runs (pcg_batch_core)
+    const long l0 = c->launches;
     for (int i = 0; i < n; i++) {
+        const long lp = c->launches;
         rt_hier* h = hs[i];
         double* x = h->L[0].u;
         const double* b = h->L[0].f;
@@ -2498,6 +2512,8 @@ static int build_batch_graph(rt_ctx* c, rt_hier* const* hs, int n, double tol, i
             kp.kernelParams = args;
             e = cudaGraphAddKernelNode(&n2, g, &n1, 1, &kp);
         }
+        once_kernels->push_back(c->launches - lp + 1);
+        const long lb = c->launches;
         cudaGraph_t body = nullptr;
         if (e == cudaSuccess && s == RT_OK) {
             cudaGraphNodeParams cp = {};
@@ -2515,12 +2531,15 @@ static int build_batch_graph(rt_ctx* c, rt_hier* const* hs, int n, double tol, i
             cudaGraph_t captured = nullptr;
             e = cudaStreamEndCapture(c->stream, &captured);
         }
+        iter_kernels->push_back(c->launches - lb);
         if (s != RT_OK || e != cudaSuccess) {
+            c->launches = l0;
             cudaGraphDestroy(g);
             if (s != RT_OK) return s;
             return rt_fail(c, RT_ECUDA, "batched PCG graph (instance %d): %s", i, cudaGetErrorString(e));
         }
     }
+    c->launches = l0;
     *out = g;
     return RT_OK;
 }
@@ -2566,6 +2585,7 @@ static int pcg_batch_core(rt_hier* const* hs, int n, double tol, int maxit, rt_s
     cudaEventCreate(&ea);
     cudaEventCreate(&eb);
     cudaEventRecord(ea, c->stream);
+    std::vector<long> batch_once, batch_iter;  // kernels of the graph run, per instance
     if (c->profile || !hs[0]->use_graphs) {
         // per-kernel events cannot sit inside a graph: run the instances one after the other
         for (int i = 0; i < n; i++) {
@@ -2583,7 +2603,7 @@ static int pcg_batch_core(rt_hier* const* hs, int n, double tol, int maxit, rt_s
             rt_ctx::BatchGraph nb;
             nb.key = key;
             for (int i = 0; i < n; i++) nb.uids.push_back(hs[i]->uid);
-            RT_CHECK(build_batch_graph(c, hs, n, tol, maxit, &nb.graph));
+            RT_CHECK(build_batch_graph(c, hs, n, tol, maxit, &nb.graph, &nb.once_kernels, &nb.iter_kernels));
             cudaError_t e = cudaGraphInstantiate(&nb.exec, nb.graph, 0);
             if (e != cudaSuccess) {
                 cudaGraphDestroy(nb.graph);
@@ -2598,7 +2618,8 @@ static int pcg_batch_core(rt_hier* const* hs, int n, double tol, int maxit, rt_s
             bg = &c->batch_graphs.back();
         }
         RT_CUDA(c, cudaGraphLaunch(bg->exec, c->stream));
-        c->launches += 1;
+        batch_once = bg->once_kernels;
+        batch_iter = bg->iter_kernels;
     }
     cudaEventRecord(eb, c->stream);
     cudaEventSynchronize(eb);
@@ -2615,6 +2636,7 @@ static int pcg_batch_core(rt_hier* const* hs, int n, double tol, int maxit, rt_s
         const double bn = sc[1] > 0 ? std::sqrt(sc[1]) : 1.0;
         double rel = std::sqrt(sc[0]) / bn;
         int its = (int)sc[3];
+        if (!batch_iter.empty()) c->launches += batch_once[i] + batch_iter[i] * its;
         if (!std::isfinite(sc[0])) return nan_fail(h, its);
         if (stall != 0.0 && rel > tol && its < maxit) {
             // this instance's reduced-precision V-cycles stalled: continue it alone with FP64 ones

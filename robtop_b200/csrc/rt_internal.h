@@ -42,6 +42,8 @@ struct rt_ctx {
         std::vector<uint64_t> uids;  // hierarchies whose buffers the graph references
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
+        // kernels per instance: prologue + start kernel, and one loop iteration
+        std::vector<long> once_kernels, iter_kernels;
     };
     std::vector<BatchGraph> batch_graphs;
 };
@@ -124,6 +126,7 @@ struct rt_hier {
     cudaGraph_t pcg32_graph = nullptr;
     cudaGraphExec_t pcg32_exec = nullptr;
     uint64_t pcg32_key = 0;
+    long pcg32_iter_kernels = 0;  // kernels in one iteration of the captured FP32 loop
     double* scal = nullptr;      // [64] device scalars
     bool stencil_ready = false;
     double* Qgal = nullptr;  // [R^3][576] cell Galerkin blocks P^T KE P (rebuilt when KE changes)
@@ -133,6 +136,7 @@ struct rt_hier {
     cudaGraph_t pcg_graph = nullptr;
     cudaGraphExec_t pcg_exec = nullptr;
     uint64_t pcg_key = 0;
+    long pcg_iter_kernels = 0;  // kernels in one iteration of the captured loop (launch accounting)
     uint64_t graph_epoch = 0;  // bumped whenever captured pointers may change
     // learned correction added to the V-cycle inside PCG (rt_hier_set_learned); scal[27] holds the
     // fallback ratio, scal[28] the gate (1 while active), scal[29] the previous iteration's r.r

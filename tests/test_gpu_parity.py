@@ -429,6 +429,35 @@ def test_pcg_fp32_krylov_refinement(pair, gamma):
     G.update_stencil()
 
 
+@pytest.mark.parametrize("krylov", [0, 2])
+def test_graph_launch_accounting(pair, krylov):
+    """A captured PCG loop adds its kernels to the launch count once per executed iteration:
+    the count equals that of the same solve run uncaptured, one launch per kernel (profiling
+    mode), with the same iteration count."""
+    cfg, ctx, G, H = pair
+    b = _rand_vec(G, 0, 85)
+    if cfg["mode"] not in (rb.MODE_WSCF, rb.MODE_WSFF):
+        return  # the projection of rigid modes is covered above; the accounting is mode independent
+    b[np.tile(cfg["vfix"].ravel().astype(bool), 3)] = 0
+    params = G.params
+    params.precision, params.smoother, params.krylov_fp32 = rb.FP32, rb.SMOOTH_CHEBY, krylov
+    G.set_params(params)
+    G.update_stencil()
+    runs = []
+    for prof in (False, True):
+        ctx.profile(prof)
+        G[0].setForce(b)
+        G[0].reset_displacement()
+        l0 = ctx.launches()
+        info = G.pcg(1e-6, 1000)
+        runs.append((ctx.launches() - l0, info.iterations, info.status))
+    ctx.profile(False)
+    assert runs[0] == runs[1] and runs[0][2] == 0 and runs[0][0] > 10 * runs[0][1]
+    params.precision, params.smoother, params.krylov_fp32 = rb.FP64, rb.SMOOTH_SGS, 0
+    G.set_params(params)
+    G.update_stencil()
+
+
 def test_modified_pm_parity(pair):
     cfg, ctx, G, H = pair
     lam, info = G.worst_case(rb.WORST_MODPM, 500, 0.0, seed=9)
