@@ -232,16 +232,54 @@ def roofline(ctx, stats, G, peaks, tuning=None):
         return out
     ach = b / avg_s / 1e9
     peak = peaks.get("hbm_gbs", 6650.0)
-    variant = None
+    variant, shape = None, None
     if tuning and name.startswith("fine_cheby"):
-        variant = tuning.get("chebyshev_" + name.rsplit("_", 1)[1], {}).get("variant")
+        t = tuning.get("chebyshev_" + name.rsplit("_", 1)[1], {})
+        variant, shape = t.get("variant"), (t.get("rows"), t.get("zchunk"))
     per_node = NCU_TRAFFIC_PER_NODE.get((name, variant))
     out.update({"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(ach / peak, 4), "traffic": int(per_node * nv) if per_node else None,
                 "traffic_source": "ncu capture of the same kernel variant on this workload" if per_node else None,
-                "variant": variant, "algorithmic_bytes": int(b),
+                "variant": variant, "rows_zchunk": shape, "algorithmic_bytes": int(b),
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"})
     return out
+
+
+# warp-instructions per node of the finest-level FP32 Chebyshev step (smsp__inst_executed.sum of one
+# ncu launch on 128x128x64 at the bench's launch shape, divided by its 1,081,665 nodes)
+NCU_INST_PER_NODE = {("fine_cheby_f32", "smem_tile", (4, 8)): 41640038 / 1081665}
+
+
+def simt_peaks(rb, ctx):
+    """FP32 FFMA, packed FFMA2 and FP64 DFMA throughput of this device (project microbenchmark)."""
+    out = {}
+    for kind, key in ((0, "fp32_tflops"), (1, "fp32x2_tflops"), (2, "fp64_tflops")):
+        t = C.c_double()
+        rb._capi.check(rb.lib().rt_bench_simt_peak(ctx.handle, kind, 5, C.byref(t)), ctx.handle)
+        out[key] = round(t.value, 2)
+    return out
+
+
+def issue_roofline(rb, ctx, G, roof, clk):
+    """The matrix-free finest-level kernel is bound by instruction issue, not HBM: next to the HBM
+    fraction, report its warp-instruction rate against 4 per SM per cycle at the measured SM clock,
+    and the measured SIMT peaks."""
+    import torch
+
+    roof["simt_peaks"] = simt_peaks(rb, ctx)
+    shape = tuple(roof["rows_zchunk"]) if roof.get("rows_zchunk") else None
+    ipn = NCU_INST_PER_NODE.get((roof.get("kernel"), roof.get("variant"), shape))
+    mhz = (clk or {}).get("sm_mhz")
+    if ipn is None or not mhz or not roof.get("avg_us"):
+        return
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    inst = ipn * G[0].nv
+    ach = inst / (roof["avg_us"] * 1e-6) / 1e9
+    peak = 4 * sms * mhz * 1e6 / 1e9
+    roof["issue"] = {"warp_inst_per_launch": int(inst), "achieved_ginst_s": round(ach, 1),
+                     "peak_ginst_s": round(peak, 1), "frac": round(ach / peak, 4),
+                     "source": "ncu smsp__inst_executed.sum of the same variant and shape; peak = 4 warp-"
+                               "instructions per SM per cycle at the median SM clock of the timed region"}
 
 
 def e2e_steps(rb, ctx, G, cfg, steps, seed0=100):
@@ -1012,6 +1050,12 @@ def main():
                                                        "fine_residual_f32"])
     ap.add_argument("--size", default=None, help="kernel mode: grid NXxNYxNZ (default: the bench workload)")
     ap.add_argument("--level", type=int, default=1, help="kernel mode, st_* kernels: the stencil level")
+    ap.add_argument("--tiles", default="autotune",
+                    help="finest-level launch shape of the worst-case bench: autotune, or variant,rows,zchunk for "
+                         "every finest-level kernel")
+    ap.add_argument("--fused", default="auto", choices=["auto", "on", "off"],
+                    help="FP32 Chebyshev sweeps of the stencil levels as one cooperative launch per smoothing: the "
+                         "autotuner's choice per level (auto), or on / off for every level")
     ap.add_argument("--shape", default=None, help="kernel mode: launch shape variant,rows,zchunk (default: autotune)")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -1054,9 +1098,14 @@ def main():
 
     ctx = make_ctx(rb, lrank)
     cfg, G = build_problem(rb, configs, ctx, rb.FP32)
-    # launch shapes of the finest-level kernels, chosen once by the library's autotuner
+    # launch shapes of the finest-level kernels, chosen once by the library's autotuner (or fixed by
+    # --tiles, e.g. for a profiler run, under which the autotuner's timings are distorted)
     G.update_stencil()
-    tuning = G.autotune()
+    tuning = G.autotune() if args.tiles == "autotune" else G.set_tiles(*map(int, args.tiles.split(",")))
+    if args.fused != "auto":  # fused Chebyshev sweeps on every stencil level, or on none
+        for lvl in range(1, G.n_grid() - 1):
+            rb._capi.check(rb.lib().rt_set_level_fused(G.handle, lvl, 1 if args.fused == "on" else 0), ctx.handle)
+        tuning = G.tuning()
     results = {}
     for prec in ((rb.FP64, rb.FP32) if args.forms == "both" else (rb.FP32,)):
         apply_form(rb, G, FORMS["plain" if prec == rb.FP64 else "mixed"])
@@ -1086,6 +1135,7 @@ def main():
     ctx.profile(False)
     stats = {k: v for k, v in stats.items() if v[0] > 0}
     roof = roofline(ctx, stats, G, peaks, tuning)
+    issue_roofline(rb, ctx, G, roof, results[rb.FP32]["clocks"])
     top = sorted(stats.items(), key=lambda kv: -kv[1][1])[:8]
 
     r32, r64 = results[rb.FP32], results.get(rb.FP64)

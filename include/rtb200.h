@@ -257,6 +257,21 @@ int rt_set_tuning(rt_hier* h, int precision, int mode, int variant, int ty, int 
 /* time reps launches of one finest-level kernel at its current shape on random data
  * (device time per launch in microseconds, CUDA events on the context stream) */
 int rt_bench_fine_kernel(rt_hier* h, int precision, int mode, int reps, double* us_per_launch);
+/* sweeps steps of the FP32 smoother (RT_SMOOTH_JACOBI or RT_SMOOTH_CHEBY) on level lvl (0 .. coarsest-1):
+ * the level's u, f rounded to FP32, smoothed with the kernels the mixed-precision V-cycle uses, u
+ * widened back.  Same smoothing rule as rt_smooth (grid/Grid.cu:1068-1111 for the reference's GS). */
+int rt_smooth_f32(rt_hier* h, int lvl, int smoother, int sweeps, double omega);
+/* FP32 Chebyshev smoothing of stencil level lvl (1 .. coarsest-1) as one cooperative launch per
+ * smoothing (the steps separated by a bounded grid barrier) instead of one launch per step.
+ * rt_autotune times both on sets of 8 steps, captured as graphs, and enables it per level where
+ * it is faster; batched solves always use separate launches (their instances run concurrently). */
+int rt_set_level_fused(rt_hier* h, int lvl, int on);
+int rt_level_fused_info(rt_hier* h, int lvl, int* on, double* us_separate, double* us_fused);
+/* SIMT arithmetic peak of the context's device in TFLOP/s, from a project microbenchmark (16
+ * independent FMA chains per thread, 8 blocks of 256 threads per SM, best of reps launches after one
+ * warm-up): kind 0 FP32 FFMA, 1 FP32 packed FFMA2, 2 FP64 DFMA.  The matrix-free finest-level
+ * operator is bound by this issue rate rather than by HBM.  No reference counterpart (measurement). */
+int rt_bench_simt_peak(rt_ctx* c, int kind, int reps, double* tflops);
 /* run one FP32 finest-level kernel at its current shape on level 0's vectors (u, f rounded to FP32)
  * and widen its result into level 0's residual vector: mode 0 f - K u, 1 K u, 2 a Jacobi step
  * u + omega D^-1 (f - K u), 3 the first Chebyshev step (needs rt_update_stencil) */

@@ -106,6 +106,10 @@ SIGNATURES = {
     "rt_set_tuning": (I, [P, I, I, I, I, I]),
     "rt_bench_fine_kernel": (I, [P, I, I, I, C.POINTER(D)]),
     "rt_bench_level_kernel": (I, [P, I, I, I, I, C.POINTER(D)]),
+    "rt_bench_simt_peak": (I, [P, I, I, C.POINTER(D)]),
+    "rt_set_level_fused": (I, [P, I, I]),
+    "rt_smooth_f32": (I, [P, I, I, I, D]),
+    "rt_level_fused_info": (I, [P, I, C.POINTER(I), C.POINTER(D), C.POINTER(D)]),
     "rt_fine_kernel_f32": (I, [P, I, D]),
     "rt_set_shell": (I, [P, P]),
     "rt_voxel_resolution": (I, [I]),

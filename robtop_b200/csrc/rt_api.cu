@@ -352,6 +352,7 @@ static void ws_sync(rt_hier* w) {
     memcpy(w->tune, p->tune, sizeof(w->tune));
     memcpy(w->tune_us, p->tune_us, sizeof(w->tune_us));
     memcpy(w->st_variant, p->st_variant, sizeof(w->st_variant));
+    w->cheby_fused = p->cheby_fused;
     w->dinv64 = p->dinv64; w->dinv32 = p->dinv32;
     for (size_t i = 0; i < w->L.size(); i++) {
         rt_level& a = w->L[i];
@@ -1151,6 +1152,13 @@ static int level_smooth(rt_hier* h, int lvl, int smoother, int sweeps, double om
     const double* coef = cheby_table(h, lvl);
     if (smoother == RT_SMOOTH_CHEBY && sweeps > RT_CHEBY_MAXK)
         return rt_fail(h->ctx, RT_EINVAL, "Chebyshev smoothing takes at most 16 steps");
+    if constexpr (sizeof(T) == 4) {
+        // all steps in one cooperative launch where rt_autotune found that faster (not inside a
+        // batched graph, whose instances run concurrently)
+        if (smoother == RT_SMOOTH_CHEBY && lvl > 0 && sweeps > 0 && ((h->cheby_fused >> lvl) & 1u) &&
+            !h->ctx->batch_capture)
+            return rtk::st_cheby_fused(h, lvl, u, f, tmp, LvlVec<T>::d(L), coef, sweeps);
+    }
     for (int s = 0; s < sweeps; s++) {
         if (smoother == RT_SMOOTH_JACOBI || smoother == RT_SMOOTH_CHEBY) {
             // ping-pong u -> tmp -> u
@@ -1245,6 +1253,27 @@ extern "C" int rt_smooth(rt_hier* h, int lvl, int smoother, int sweeps, double o
     if (lvl > 0) RT_CHECK(need_stencil(h));
     else RT_CHECK(refresh_fine(h));
     return level_smooth<double>(h, lvl, smoother, sweeps, omega, smoother == RT_SMOOTH_SGS);
+}
+
+static int nan_fail(rt_hier* h, int it);
+
+extern "C" int rt_smooth_f32(rt_hier* h, int lvl, int smoother, int sweeps, double omega) {
+    if (!h || lvl < 0 || lvl + 1 >= (int)h->L.size() || sweeps < 0) return RT_EINVAL;
+    if (smoother != RT_SMOOTH_JACOBI && smoother != RT_SMOOTH_CHEBY)
+        return rt_fail(h->ctx, RT_EINVAL, "FP32 smoothing: Jacobi or Chebyshev");
+    if (lvl > 0) RT_CHECK(need_stencil(h));
+    else RT_CHECK(refresh_fine(h));
+    if (smoother == RT_SMOOTH_CHEBY && !h->stencil_ready) return rt_fail(h->ctx, RT_ESTATE, "rt_update_stencil has not run");
+    rt_level& L = h->L[lvl];
+    const long n = 3 * L.nv;
+    RT_CHECK(rtk::d2f(h, n, L.u, L.u32));
+    RT_CHECK(rtk::d2f(h, n, L.f, L.f32));
+    RT_CHECK(level_smooth<float>(h, lvl, smoother, sweeps, omega, false));
+    RT_CHECK(rtk::f2d(h, n, L.u32, L.u));
+    double e = 0;
+    RT_CHECK(read_scalars(h, RT_SCAL_ERR, 1, &e));
+    if (e != 0.0) return nan_fail(h, 0);
+    return RT_OK;
 }
 
 extern "C" int rt_restrict_residual(rt_hier* h, int lvl) {
@@ -1522,7 +1551,10 @@ static int nan_fail(rt_hier* h, int it) {
     RT_CHECK(read_scalars(h, RT_SCAL_ERR, 1, &e));
     if (e != 0.0) {
         RT_CUDA(h->ctx, cudaMemsetAsync(h->scal + RT_SCAL_ERR, 0, sizeof(double), h->ctx->stream));
-        return rt_fail(h->ctx, RT_ECUDA, "a stencil-level kernel gave up waiting for its bulk copies (iteration %d)", it);
+        RT_CUDA(h->ctx, cudaMemsetAsync(h->scal + RT_SCAL_GBAR, 0, sizeof(double) * RT_MAX_LEVELS, h->ctx->stream));
+        return rt_fail(h->ctx, RT_ECUDA, e == 2.0 ? "a fused Chebyshev sweep gave up at its grid barrier (iteration %d)"
+                                                  : "a stencil-level kernel gave up waiting for its bulk copies (iteration %d)",
+                       it);
     }
     return rt_fail(h->ctx, RT_ENAN, "NaN in PCG at iteration %d", it);
 }
@@ -2364,8 +2396,68 @@ extern "C" int rt_bench_level_kernel(rt_hier* h, int lvl, int precision, int mod
 
 // the lane-split / bulk-copy choice for the FP32 smoother's stencil kernels, timed on the largest
 // stencil level's Chebyshev step (FP32 stencils, and BF16 ones when they exist)
+// a set of nsteps FP32 Chebyshev steps on stencil level lvl (random u, f), separate launches or one
+// fused launch, captured as a graph as the solver runs it; device time per set in microseconds
+static double time_level_sweeps(rt_hier* h, int lvl, bool fused, int nsteps, int reps) {
+    rt_ctx* c = h->ctx;
+    rt_level& L = h->L[lvl];
+    const long n = 3 * L.nv;
+    if (rtk::rng_uniform(h, 0xbe80, n, h->x) != RT_OK || rtk::rng_uniform(h, 0xbe81, n, h->q) != RT_OK) return 1e30;
+    if (rtk::d2f(h, n, h->x, L.u32) != RT_OK || rtk::d2f(h, n, h->q, L.f32) != RT_OK) return 1e30;
+    const uint32_t saved = h->cheby_fused;
+    h->cheby_fused = fused ? (saved | (1u << lvl)) : (saved & ~(1u << lvl));
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    double us = 1e30;
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        const int st = level_smooth<float>(h, lvl, RT_SMOOTH_CHEBY, nsteps, 0.0, false);
+        const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        if (st == RT_OK && e == cudaSuccess && cudaGraphInstantiate(&ge, g, 0) == cudaSuccess &&
+            cudaGraphLaunch(ge, c->stream) == cudaSuccess) {
+            cudaEvent_t a, b;
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            cudaEventRecord(a, c->stream);
+            bool ok = true;
+            for (int i = 0; i < reps && ok; i++) ok = cudaGraphLaunch(ge, c->stream) == cudaSuccess;
+            cudaEventRecord(b, c->stream);
+            cudaEventSynchronize(b);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, a, b);
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+            double err = 0;
+            if (ok && cudaStreamSynchronize(c->stream) == cudaSuccess && read_scalars(h, RT_SCAL_ERR, 1, &err) == RT_OK) {
+                if (err == 0.0) {
+                    us = ms * 1e3 / reps;
+                } else {  // a barrier wait ran out: not a candidate; clear the error and barrier words
+                    cudaMemsetAsync(h->scal + RT_SCAL_ERR, 0, sizeof(double), c->stream);
+                    cudaMemsetAsync(h->scal + RT_SCAL_GBAR, 0, sizeof(double) * RT_MAX_LEVELS, c->stream);
+                }
+            }
+        }
+    }
+    if (ge) cudaGraphExecDestroy(ge);
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    h->cheby_fused = saved;
+    return us;
+}
+
 static int autotune_level_kernels(rt_hier* h, int reps) {
     if (!h->stencil_ready || h->L.size() < 3) return RT_OK;
+    // fused Chebyshev sweeps (one cooperative launch per smoothing) per stencil level, timed on
+    // sets of 8 steps against the separate launches of the chosen lane-split / bulk variant
+    h->cheby_fused = 0;
+    if (rtk::st_cheby_fused_ok(h)) {
+        for (int lvl = 1; lvl + 1 < (int)h->L.size() && lvl < 15; lvl++) {
+            const double t0 = time_level_sweeps(h, lvl, false, 8, reps);
+            const double t1 = time_level_sweeps(h, lvl, true, 8, reps);
+            h->fused_us[lvl][0] = t0;
+            h->fused_us[lvl][1] = t1;
+            if (t1 < t0) h->cheby_fused |= 1u << lvl;
+        }
+    }
     for (int t = 0; t < 2; t++) {
         if (t == 1 && !(h->P.coarse_bf16 && h->L[1].st16)) continue;
         const int saved_bf16 = h->P.coarse_bf16;
@@ -2381,6 +2473,24 @@ static int autotune_level_kernels(rt_hier* h, int reps) {
         h->st_variant[t] = best_v;
         h->P.coarse_bf16 = saved_bf16;
     }
+    return RT_OK;
+}
+
+extern "C" int rt_set_level_fused(rt_hier* h, int lvl, int on) {
+    if (!h || lvl < 1 || lvl + 1 >= (int)h->L.size() || lvl >= 15) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
+    if (on && !rtk::st_cheby_fused_ok(h))
+        return rt_fail(h->ctx, RT_ECUDA, "the device cannot run the fused Chebyshev sweeps");
+    h->cheby_fused = on ? (h->cheby_fused | (1u << lvl)) : (h->cheby_fused & ~(1u << lvl));
+    h->graph_epoch++;
+    return RT_OK;
+}
+
+extern "C" int rt_level_fused_info(rt_hier* h, int lvl, int* on, double* us_separate, double* us_fused) {
+    if (!h || lvl < 1 || lvl + 1 >= (int)h->L.size() || lvl >= 15) return RT_EINVAL;
+    if (on) *on = (int)((h->cheby_fused >> lvl) & 1u);
+    if (us_separate) *us_separate = h->fused_us[lvl][0];
+    if (us_fused) *us_fused = h->fused_us[lvl][1];
     return RT_OK;
 }
 
@@ -2477,8 +2587,19 @@ static bool no_support_mode(const rt_hier* h) { return h->P.mode == RT_MODE_NSCF
 
 // one graph: per instance, prologue (child graph) -> k_pcg_start -> WHILE(one PCG iteration);
 // the instances share no node, so the device runs their kernels concurrently
+static int build_batch_graph_(rt_ctx* c, rt_hier* const* hs, int n, double tol, int maxit, cudaGraph_t* out,
+                              std::vector<long>* once_kernels, std::vector<long>* iter_kernels);
+
 static int build_batch_graph(rt_ctx* c, rt_hier* const* hs, int n, double tol, int maxit, cudaGraph_t* out,
                              std::vector<long>* once_kernels, std::vector<long>* iter_kernels) {
+    c->batch_capture = true;
+    const int s = build_batch_graph_(c, hs, n, tol, maxit, out, once_kernels, iter_kernels);
+    c->batch_capture = false;
+    return s;
+}
+
+static int build_batch_graph_(rt_ctx* c, rt_hier* const* hs, int n, double tol, int maxit, cudaGraph_t* out,
+                              std::vector<long>* once_kernels, std::vector<long>* iter_kernels) {
     cudaGraph_t g;
     RT_CUDA(c, cudaGraphCreate(&g, 0));
     // captured launches are counted when the graph runs (pcg_batch_core)

@@ -216,6 +216,254 @@ __global__ void __launch_bounds__(ST_BS, sizeof(T) == 8 ? 1 : 3) k_st_split4(int
 }
 
 // ---------------------------------------------------------------------------
+// Fused Chebyshev sweeps of a small stencil level: all nsteps steps in one cooperative
+// launch, the steps separated by a grid barrier instead of a kernel boundary.  The coarse
+// levels below the first are a few thousand nodes: a separate launch per step spends most
+// of its time in launch, ramp-up and drain, not in the 243-entry rows.  Same arithmetic and
+// thread layout as k_st_split4 (MODE 3); u is ping-ponged with tmp (u -> tmp -> u ...), so
+// after an odd step count a last barrier lets every thread copy its own entries back to u.
+// Values written by other blocks in the previous step are read through L2 (ld.global.cg):
+// L1 is not coherent across SMs.  The barrier is bounded: a block whose wait runs out sets
+// the error slot, poisons u[0] with NaN (the solve then stops on its NaN check) and returns.
+// ---------------------------------------------------------------------------
+constexpr long COOP_SPIN_LIMIT = 1L << 22;  // L2 polls (a few hundred ns each at most)
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// grid-wide barrier: bar[0] counts arrivals, bar[1] is the generation; gen is thread 0's copy
+__device__ __forceinline__ bool coop_grid_sync(unsigned* bar, unsigned& gen, int* s_ok) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        bool ok = true;
+        __threadfence();
+        const unsigned prev = atomicAdd(bar, 1u);
+        if (prev == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicExch(bar + 1, gen + 1);
+        } else {
+            long it = 0;
+            while (ld_acquire_u32(bar + 1) == gen) {
+                if (++it > COOP_SPIN_LIMIT) {
+                    ok = false;
+                    break;
+                }
+            }
+        }
+        __threadfence();
+        gen++;
+        *s_ok = ok ? 1 : 0;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+template <typename S>
+__global__ void __launch_bounds__(ST_BS, 3) k_st_cheby_coop(int nx, int ny, int nz, const uint8_t* __restrict__ vact,
+                                                             const S* __restrict__ st, float* u,
+                                                             const float* __restrict__ f, float* tmp, float* d,
+                                                             const double* __restrict__ coef, int nsteps,
+                                                             unsigned* bar, double* err) {
+    __shared__ int s_ok;
+    unsigned gen = 0;
+    if (threadIdx.x == 0) gen = ld_acquire_u32(bar + 1);
+    const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
+    const long nv = (long)vx * vy * vz;
+    const long rs = StAddr<S>::stride(nv);
+    const int q = threadIdx.x & 3;
+    const long ngroups = (long)gridDim.x * (blockDim.x >> 2);
+    const long vend = ((nv + ngroups - 1) / ngroups) * ngroups;
+    const long v0 = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 2;
+    for (int s = 0; s < nsteps; s++) {
+        const float* src = (s & 1) ? tmp : u;
+        float* dst = (s & 1) ? u : tmp;
+        const float ca = (float)coef[2 * s], cb = (float)coef[2 * s + 1];
+        for (long v = v0; v < vend; v += ngroups) {
+            const bool inb = v < nv;
+            const bool act = inb && vact[v];
+            const S* sb = st + StAddr<S>::base(inb ? v : 0);
+            float Au[3] = {0.f, 0.f, 0.f};
+            if (act) {
+                const int x = (int)(v % vx), y = (int)((v / vx) % vy), z = (int)(v / ((long)vx * vy));
+#pragma unroll
+                for (int kk = 0; kk < 7; kk++) {
+                    const int k = q + 4 * kk;
+                    if (k >= 27) break;
+                    const int jx = x + k % 3 - 1, jy = y + (k / 3) % 3 - 1, jz = z + k / 9 - 1;
+                    if (jx < 0 || jy < 0 || jz < 0 || jx >= vx || jy >= vy || jz >= vz) continue;
+                    const long nj = jx + (long)vx * (jy + (long)vy * jz);
+                    const float u0 = __ldcg(src + nj), u1 = __ldcg(src + nv + nj), u2 = __ldcg(src + 2 * nv + nj);
+                    const S* sk = sb + (long)(k * 9) * rs;
+#pragma unroll
+                    for (int r = 0; r < 3; r++) {
+                        float a0 = st_val(sk + (3 * r) * rs), a1 = st_val(sk + (3 * r + 1) * rs),
+                              a2 = st_val(sk + (3 * r + 2) * rs);
+                        if (sizeof(S) == 2 && k == 13) {  // low parts of the BF16 centre block
+                            a0 += st_val(sb + (243 + 3 * r) * rs);
+                            a1 += st_val(sb + (243 + 3 * r + 1) * rs);
+                            a2 += st_val(sb + (243 + 3 * r + 2) * rs);
+                        }
+                        Au[r] += a0 * u0 + a1 * u1 + a2 * u2;
+                    }
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                Au[r] += __shfl_xor_sync(0xffffffffu, Au[r], 1);
+                Au[r] += __shfl_xor_sync(0xffffffffu, Au[r], 2);
+            }
+            if (!inb || q == 3) continue;
+            const long oq = (long)q * nv + v;
+            float res = 0.f, dn = 0.f;
+            if (act) {
+                float S9[9];
+#pragma unroll
+                for (int i = 0; i < 9; i++) S9[i] = st_centre<float>(sb, rs, i);
+                const float a0 = S9[0], b0 = S9[1], c0 = S9[2], d0 = S9[3], e0 = S9[4], f0 = S9[5], g0 = S9[6],
+                            h0 = S9[7], k0 = S9[8];
+                const float A = e0 * k0 - f0 * h0, B = -(d0 * k0 - f0 * g0), Cc = d0 * h0 - e0 * g0;
+                const float id = 1.f / (a0 * A + b0 * B + c0 * Cc);
+                const float i0 = q == 0 ? A : (q == 1 ? B : Cc);
+                const float i1 = q == 0 ? -(b0 * k0 - c0 * h0) : (q == 1 ? (a0 * k0 - c0 * g0) : -(a0 * h0 - b0 * g0));
+                const float i2 = q == 0 ? (b0 * f0 - c0 * e0) : (q == 1 ? -(a0 * f0 - c0 * d0) : (a0 * e0 - b0 * d0));
+                const float r0 = f[v] - Au[0], r1 = f[nv + v] - Au[1], r2 = f[2 * nv + v] - Au[2];
+                const float zq = (i0 * id) * r0 + (i1 * id) * r1 + (i2 * id) * r2;
+                dn = (s == 0 ? 0.f : ca * d[oq]) + cb * zq;
+                res = __ldcg(src + oq) + dn;
+            }
+            dst[oq] = res;
+            d[oq] = dn;
+        }
+        if (s + 1 < nsteps || (nsteps & 1)) {
+            if (!coop_grid_sync(bar, gen, &s_ok)) {
+                if (threadIdx.x == 0) {
+                    *err = 2.0;
+                    u[0] = __int_as_float(0x7fc00000);
+                }
+                return;
+            }
+        }
+    }
+    if (nsteps & 1) {  // the last step wrote tmp: every thread copies back the entries it wrote
+        for (long v = v0; v < nv; v += ngroups)
+            if (q < 3) u[(long)q * nv + v] = __ldcg(tmp + (long)q * nv + v);
+    }
+}
+
+// Resident form of the fused sweeps, for levels whose 4-lane groups all fit on the device at
+// once (one group per node, 64 nodes per block): the stencil rows each lane multiplies are
+// read once into shared memory (63 x 256 floats, entries outside the box or of inactive
+// nodes zeroed so the step has no bounds branches), the inverse diagonal row, f and the
+// Chebyshev direction stay in registers, and a step moves only the neighbours' u through L2.
+constexpr int RES_ROWS = 63;  // 7 neighbours x 9 entries per lane
+constexpr size_t RES_SMEM = (size_t)RES_ROWS * ST_BS * sizeof(float);
+
+template <typename S>
+__global__ void __launch_bounds__(ST_BS, 3) k_st_cheby_res(int nx, int ny, int nz, const uint8_t* __restrict__ vact,
+                                                            const S* __restrict__ st, float* u,
+                                                            const float* __restrict__ f, float* tmp, float* d,
+                                                            const double* __restrict__ coef, int nsteps,
+                                                            unsigned* bar, double* err) {
+    extern __shared__ float srow[];  // [RES_ROWS][ST_BS]
+    __shared__ int s_ok;
+    unsigned gen = 0;
+    if (threadIdx.x == 0) gen = ld_acquire_u32(bar + 1);
+    const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
+    const long nv = (long)vx * vy * vz;
+    const long rs = StAddr<S>::stride(nv);
+    const int tid = threadIdx.x, q = tid & 3;
+    const long v = (blockIdx.x * (long)blockDim.x + tid) >> 2;
+    const bool inb = v < nv;
+    const bool act = inb && vact[v];
+    const S* sb = st + StAddr<S>::base(inb ? v : 0);
+    const int x = inb ? (int)(v % vx) : 0, y = inb ? (int)((v / vx) % vy) : 0,
+              z = inb ? (int)(v / ((long)vx * vy)) : 0;
+    long nj[7];
+#pragma unroll
+    for (int kk = 0; kk < 7; kk++) {
+        const int k = q + 4 * kk;
+        const int jx = x + k % 3 - 1, jy = y + (k / 3) % 3 - 1, jz = z + k / 9 - 1;
+        const bool ok = act && k < 27 && jx >= 0 && jy >= 0 && jz >= 0 && jx < vx && jy < vy && jz < vz;
+        nj[kk] = ok ? jx + (long)vx * (jy + (long)vy * jz) : (inb ? v : 0);
+        const S* sk = sb + (long)(k * 9) * rs;
+#pragma unroll
+        for (int e = 0; e < 9; e++) {
+            float a = 0.f;
+            if (ok) {
+                a = st_val(sk + e * rs);
+                if (sizeof(S) == 2 && k == 13) a += st_val(sb + (243 + e) * rs);  // BF16 centre low part
+            }
+            srow[(kk * 9 + e) * ST_BS + tid] = a;
+        }
+    }
+    // row q of the inverse centre block (scaled by 1 / det), f of the node, the direction d
+    float i0 = 0.f, i1 = 0.f, i2 = 0.f, f0 = 0.f, f1 = 0.f, f2 = 0.f, dq = 0.f;
+    if (act && q < 3) {
+        float S9[9];
+#pragma unroll
+        for (int i = 0; i < 9; i++) S9[i] = st_centre<float>(sb, rs, i);
+        const float a0 = S9[0], b0 = S9[1], c0 = S9[2], d0 = S9[3], e0 = S9[4], g0f = S9[5], g0 = S9[6], h0 = S9[7],
+                    k0 = S9[8];
+        const float A = e0 * k0 - g0f * h0, B = -(d0 * k0 - g0f * g0), Cc = d0 * h0 - e0 * g0;
+        const float id = 1.f / (a0 * A + b0 * B + c0 * Cc);
+        i0 = (q == 0 ? A : (q == 1 ? B : Cc)) * id;
+        i1 = (q == 0 ? -(b0 * k0 - c0 * h0) : (q == 1 ? (a0 * k0 - c0 * g0) : -(a0 * h0 - b0 * g0))) * id;
+        i2 = (q == 0 ? (b0 * g0f - c0 * e0) : (q == 1 ? -(a0 * g0f - c0 * d0) : (a0 * e0 - b0 * d0))) * id;
+        f0 = f[v];
+        f1 = f[nv + v];
+        f2 = f[2 * nv + v];
+    }
+    __syncthreads();
+    const long oq = (long)(q < 3 ? q : 0) * nv + (inb ? v : 0);
+    for (int s = 0; s < nsteps; s++) {
+        const float* src = (s & 1) ? tmp : u;
+        float* dst = (s & 1) ? u : tmp;
+        float Au[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int kk = 0; kk < 7; kk++) {
+            if (q + 4 * kk >= 27) break;
+            const float u0 = __ldcg(src + nj[kk]), u1 = __ldcg(src + nv + nj[kk]), u2 = __ldcg(src + 2 * nv + nj[kk]);
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+                Au[r] += srow[(kk * 9 + 3 * r) * ST_BS + tid] * u0 + srow[(kk * 9 + 3 * r + 1) * ST_BS + tid] * u1 +
+                         srow[(kk * 9 + 3 * r + 2) * ST_BS + tid] * u2;
+        }
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            Au[r] += __shfl_xor_sync(0xffffffffu, Au[r], 1);
+            Au[r] += __shfl_xor_sync(0xffffffffu, Au[r], 2);
+        }
+        if (inb && q < 3) {
+            float res = 0.f, dn = 0.f;
+            if (act) {
+                const float zq = i0 * (f0 - Au[0]) + i1 * (f1 - Au[1]) + i2 * (f2 - Au[2]);
+                dn = (s == 0 ? 0.f : (float)coef[2 * s] * dq) + (float)coef[2 * s + 1] * zq;
+                res = __ldcg(src + oq) + dn;
+            }
+            dst[oq] = res;
+            dq = dn;
+        }
+        if (s + 1 < nsteps || (nsteps & 1)) {
+            if (!coop_grid_sync(bar, gen, &s_ok)) {
+                if (threadIdx.x == 0) {
+                    *err = 2.0;
+                    u[0] = __int_as_float(0x7fc00000);
+                }
+                return;
+            }
+        }
+    }
+    if (inb && q < 3) {
+        d[oq] = dq;
+        if (nsteps & 1) u[oq] = __ldcg(tmp + oq);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Stencil kernel over the blocked FP32 / BF16 copies: the 31 KB (FP32) / 16 KB (BF16)
 // stencil run of a 32-node block is fetched with one bulk asynchronous copy
 // (cp.async.bulk, completion counted on an mbarrier) into a ring of NST shared-memory
@@ -834,6 +1082,87 @@ int st_cheby(rt_hier* h, int lvl, const T* u, const T* f, T* unew, T* d, const d
             L.nx, L.ny, L.nz, L.vact, stp<T>(L), u, f, unew, d, T(0), coef, kstep);
     });
 }
+// co-resident blocks per SM of the fused kernels (queried once per context): the streaming form
+// in coop_blocks_per_sm, the resident form (RES_SMEM of shared memory per block) in res_blocks_per_sm
+static int coop_blocks(rt_hier* h, bool resident = false) {
+    rt_ctx* c = h->ctx;
+    if (c->coop_blocks_per_sm < 0) {
+        int coop = 0, nb = 0, nr = 0;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);
+        if (coop) {
+            int a = 0, b = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_st_cheby_coop<float>, ST_BS, 0) == cudaSuccess &&
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_st_cheby_coop<uint16_t>, ST_BS, 0) == cudaSuccess)
+                nb = a < b ? a : b;
+            a = b = 0;
+            if (cudaFuncSetAttribute(k_st_cheby_res<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RES_SMEM) ==
+                    cudaSuccess &&
+                cudaFuncSetAttribute(k_st_cheby_res<uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)RES_SMEM) == cudaSuccess &&
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_st_cheby_res<float>, ST_BS, RES_SMEM) == cudaSuccess &&
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_st_cheby_res<uint16_t>, ST_BS, RES_SMEM) ==
+                    cudaSuccess)
+                nr = a < b ? a : b;
+        }
+        cudaGetLastError();
+        c->coop_blocks_per_sm = nb;
+        c->res_blocks_per_sm = nr;
+    }
+    return resident ? c->res_blocks_per_sm : c->coop_blocks_per_sm;
+}
+
+bool st_cheby_fused_ok(rt_hier* h) { return coop_blocks(h) > 0; }
+
+int st_cheby_fused(rt_hier* h, int lvl, float* u, const float* f, float* tmp, float* d, const double* coef,
+                   int nsteps) {
+    rt_level& L = h->L[lvl];
+    const int nb = coop_blocks(h);
+    if (nb <= 0) return rt_fail(h->ctx, RT_ECUDA, "the device cannot run the fused Chebyshev sweeps");
+    if (nsteps < 1 || nsteps > RT_CHEBY_MAXK) return rt_fail(h->ctx, RT_EINVAL, "fused Chebyshev: 1..16 steps");
+    // one 4-lane group per node: the resident form when all groups fit on the device at once,
+    // else the streaming form over a node loop
+    const long want = rt_blocks(4 * L.nv, ST_BS);
+    const long cap = (long)nb * h->ctx->sm_count;
+    const bool resident = want <= (long)coop_blocks(h, true) * h->ctx->sm_count;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(resident ? want : (want < cap ? want : cap)));
+    cfg.blockDim = dim3(ST_BS);
+    cfg.dynamicSmemBytes = resident ? RES_SMEM : 0;
+    cfg.stream = h->ctx->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    unsigned* bar = reinterpret_cast<unsigned*>(h->scal + RT_SCAL_GBAR + lvl);
+    double* err = h->scal + RT_SCAL_ERR;
+    const bool bf = use_bf16<float>(h, L);
+    cudaError_t e = cudaSuccess;
+    RT_CHECK(rt_launch(h->ctx, bf ? (lvl == 1 ? "st_cheby_fused_bf16_l1" : "st_cheby_fused_bf16")
+                                  : LVL_NAME(lvl, false, "st_cheby_fused"),
+                       [&] {
+                           if (resident && bf)
+                               e = cudaLaunchKernelEx(&cfg, k_st_cheby_res<uint16_t>, L.nx, L.ny, L.nz,
+                                                      (const uint8_t*)L.vact, (const uint16_t*)L.st16, u, f, tmp, d,
+                                                      coef, nsteps, bar, err);
+                           else if (resident)
+                               e = cudaLaunchKernelEx(&cfg, k_st_cheby_res<float>, L.nx, L.ny, L.nz,
+                                                      (const uint8_t*)L.vact, (const float*)L.st32, u, f, tmp, d,
+                                                      coef, nsteps, bar, err);
+                           else if (bf)
+                               e = cudaLaunchKernelEx(&cfg, k_st_cheby_coop<uint16_t>, L.nx, L.ny, L.nz,
+                                                      (const uint8_t*)L.vact, (const uint16_t*)L.st16, u, f, tmp, d,
+                                                      coef, nsteps, bar, err);
+                           else
+                               e = cudaLaunchKernelEx(&cfg, k_st_cheby_coop<float>, L.nx, L.ny, L.nz,
+                                                      (const uint8_t*)L.vact, (const float*)L.st32, u, f, tmp, d,
+                                                      coef, nsteps, bar, err);
+                       }));
+    if (e != cudaSuccess)
+        return rt_fail(h->ctx, RT_ECUDA, "fused Chebyshev launch failed: %s", cudaGetErrorString(e));
+    return RT_OK;
+}
+
 template int st_cheby<double>(rt_hier*, int, const double*, const double*, double*, double*, const double*, int);
 template int st_cheby<float>(rt_hier*, int, const float*, const float*, float*, float*, const double*, int);
 

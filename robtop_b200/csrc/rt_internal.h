@@ -29,6 +29,11 @@ struct rt_ctx {
     long long launches = 0;
     // profiling
     bool profile = false;
+    // set while a batched graph is captured: its instances run concurrently, so no cooperative
+    // (grid-synchronised) launch may be part of it
+    bool batch_capture = false;
+    int coop_blocks_per_sm = -1;  // co-resident blocks of the fused Chebyshev kernels (-1: not queried)
+    int res_blocks_per_sm = 0;
     std::vector<rt_kstat> kstats;
     std::unordered_map<const void*, int> kid_by_name;  // kernel-name literal -> kstats index
     std::vector<cudaEvent_t> ev_pool;
@@ -91,6 +96,10 @@ struct rt_hier {
     // (4 lanes per node, loads through L1), 1 bulk-copy (32-node stencil runs staged in shared memory)
     int st_variant[2] = {0, 1};
     double st_us[2][2] = {{0, 0}, {0, 0}};  // [stencil type][variant] level-1 Chebyshev step (rt_autotune)
+    // stencil levels whose FP32 Chebyshev sweeps run as one cooperative launch (bit lvl; rt_autotune),
+    // with the measured time of a sweep set [level][separate launches, one launch]
+    uint32_t cheby_fused = 0;
+    double fused_us[15][2] = {};
     double* dinv64 = nullptr;        // [6][nv] inverted diagonal blocks of the finest level
     float* dinv32 = nullptr;
     std::vector<rt_level> L;
@@ -194,6 +203,7 @@ static inline unsigned rt_blocks(long n, int bs) { return (unsigned)((n + bs - 1
 #define RT_CHEBY_HI_FRAC 1.1
 #define RT_SCAL_ERR 295   // set to 1 by a stencil kernel whose bounded copy wait ran out
 #define RT_SCAL_LMAX 300  // device scalar slots holding lmax(D^-1 A) per level
+#define RT_SCAL_GBAR 480  // per level: the grid barrier of the fused Chebyshev sweeps (arrivals, generation as 2 x u32)
 // (a_k, b_k), k < RT_CHEBY_MAXK, per level at RT_SCAL_CHEB + 2 RT_CHEBY_MAXK lvl (levels 0..14);
 // the 16th table serves kernel timing before any stencil exists
 #define RT_CHEBY_MAXK 16
@@ -229,6 +239,10 @@ template <typename T>
 int fine_cheby(rt_hier* h, const T* u, const T* f, T* unew, T* d, const double* coef, int kstep);
 template <typename T>
 int st_cheby(rt_hier* h, int lvl, const T* u, const T* f, T* unew, T* d, const double* coef, int kstep);
+// nsteps FP32 Chebyshev steps of stencil level lvl in one cooperative launch (u -> tmp -> u ...,
+// the result in u); false from st_cheby_fused_ok when the device cannot co-schedule the grid
+int st_cheby_fused(rt_hier* h, int lvl, float* u, const float* f, float* tmp, float* d, const double* coef, int nsteps);
+bool st_cheby_fused_ok(rt_hier* h);
 int penalty_weights(rt_hier* h);
 int init_tile_kernels(rt_ctx* c);
 int init_stencil_kernels(rt_ctx* c);

@@ -332,6 +332,18 @@ class HierarchyGrid:
     def autotune(self, reps=5):
         """Choose the finest-level kernel launch shapes (rt_autotune); returns them per kernel."""
         self._c(A.lib().rt_autotune(self._h, reps))
+        return self.tuning()
+
+    def set_tiles(self, variant, rows, zchunk):
+        """One launch shape for every finest-level kernel of both precisions (rt_set_tuning);
+        returns the shapes as tuning() reports them."""
+        for prec in (A.FP32, A.FP64):
+            for m in range(4):
+                self._c(A.lib().rt_set_tuning(self._h, prec, m, variant, rows, zchunk))
+        return self.tuning()
+
+    def tuning(self):
+        """The current launch shapes (and, after autotune, their measured times) per kernel."""
         out = {}
         names = ["residual", "applyK", "jacobi", "chebyshev"]
         for prec, pname in ((A.FP32, "f32"), (A.FP64, "f64")):
@@ -340,6 +352,12 @@ class HierarchyGrid:
                 self._c(A.lib().rt_tuning_info(self._h, prec, m, C.byref(v), C.byref(ty), C.byref(zc), C.byref(us)))
                 out[f"{mname}_{pname}"] = {"variant": ["smem_tile", "register_march", "register_march_prefetch", "smem_tile_pipelined", "smem_tile_pairs_f32"][v.value], "rows": ty.value,
                                            "zchunk": zc.value, "us": round(us.value, 2)}
+        for lvl in range(1, self.n_grid() - 1):
+            on, t0, t1 = C.c_int(), C.c_double(), C.c_double()
+            if A.lib().rt_level_fused_info(self._h, lvl, C.byref(on), C.byref(t0), C.byref(t1)) == A.RT_OK:
+                out[f"chebyshev_f32_level{lvl}"] = {"fused": bool(on.value),
+                                                    "us_8_steps": {"separate": round(t0.value, 2),
+                                                                   "fused": round(t1.value, 2)}}
         for st, sname in ((0, "f32"), (1, "bf16")):
             v, u0, u1 = C.c_int(), C.c_double(), C.c_double()
             self._c(A.lib().rt_level_kernel_info(self._h, st, C.byref(v), C.byref(u0), C.byref(u1)))

@@ -316,6 +316,69 @@ def test_chebyshev_bounds_and_steps(pair):
         assert rel_err(G[i].getDisplacement(), uo) < 1e-9, f"level {i}"
 
 
+@pytest.mark.parametrize("nsteps", [3, 8])
+def test_fused_chebyshev_sweeps(pair, nsteps):
+    """FP32 Chebyshev smoothing of every stencil level as one cooperative launch (grid barrier
+    between the steps) gives the separate launches' result, and both follow the oracle's FP64
+    steps to FP32 accuracy; odd step counts end with the copy back into u."""
+    cfg, ctx, G, H = pair
+    lm = [G.smoother_lmax(i) for i in range(H.nlev - 1)]
+    H.set_lmax(lm)
+    lib = rb.lib()
+    rb._capi.check(lib.rt_set_level_kernel(G.handle, 0, 0), ctx.handle)  # lane-split: same sums as fused
+    for i in range(1, H.nlev - 1):
+        u, f = _rand_vec(G, i, 130 + i), _rand_vec(G, i, 140 + i)
+        out = []
+        for fused in (0, 1):
+            rb._capi.check(lib.rt_set_level_fused(G.handle, i, fused), ctx.handle)
+            G[i].setDisplacement(u)
+            G[i].setForce(f)
+            rb._capi.check(lib.rt_smooth_f32(G.handle, i, rb.SMOOTH_CHEBY, nsteps, 0.0), ctx.handle)
+            out.append(G[i].getDisplacement())
+        rb._capi.check(lib.rt_set_level_fused(G.handle, i, 0), ctx.handle)
+        assert rel_err(out[1], out[0]) < 1e-6, f"level {i}"
+        uo, un, d = u.copy(), np.zeros_like(u), np.zeros_like(u)
+        for k in range(nsteps):
+            O.lib().or_st_cheby(H.lv(i), O.ptr(uo), O.ptr(f), O.ptr(un), O.ptr(d), k)
+            uo, un = un, uo
+        assert rel_err(out[1], uo) < 1e-3, f"level {i}"
+
+
+def test_fused_chebyshev_in_pcg(pair):
+    """The mixed-precision PCG with every stencil level's Chebyshev sweeps fused reaches 1e-6 in the
+    FP64 residual within one iteration of the separate launches' count."""
+    cfg, ctx, G, H = pair
+    b = _rand_vec(G, 0, 86)
+    if cfg["mode"] not in (rb.MODE_WSCF, rb.MODE_WSFF):
+        return  # the rigid-mode projection is covered by the other PCG tests
+    b[np.tile(cfg["vfix"].ravel().astype(bool), 3)] = 0
+    params = G.params
+    params.precision, params.smoother = rb.FP32, rb.SMOOTH_CHEBY
+    params.pre_sweeps = params.post_sweeps = 2
+    params.coarse_sweeps = 8
+    G.set_params(params)
+    G.update_stencil()
+    its = []
+    for fused in (0, 1):
+        for i in range(1, G.n_grid() - 1):
+            rb._capi.check(rb.lib().rt_set_level_fused(G.handle, i, fused), ctx.handle)
+        G[0].setForce(b)
+        G[0].reset_displacement()
+        info = G.pcg(1e-6, 1000)
+        assert info.status == 0 and info.rel_residual <= 1e-6
+        r = (b - H.applyK(G[0].getDisplacement())) * np.tile(H.arrs[0]["vact"], 3)
+        assert np.linalg.norm(r) / np.linalg.norm(b) <= 1.01e-6
+        its.append(info.iterations)
+    assert abs(its[1] - its[0]) <= 1
+    for i in range(1, G.n_grid() - 1):
+        rb._capi.check(rb.lib().rt_set_level_fused(G.handle, i, 0), ctx.handle)
+    params.precision, params.smoother = rb.FP64, rb.SMOOTH_SGS
+    params.pre_sweeps = params.post_sweeps = 1
+    params.coarse_sweeps = 0
+    G.set_params(params)
+    G.update_stencil()
+
+
 def test_coarsest_solve(pair):
     cfg, ctx, G, H = pair
     last = H.nlev - 1
