@@ -1055,7 +1055,7 @@ def main():
                          "every finest-level kernel")
     ap.add_argument("--fused", default="auto", choices=["auto", "on", "off"],
                     help="FP32 Chebyshev sweeps of the stencil levels as one cooperative launch per smoothing: the "
-                         "autotuner's choice per level (auto), or on / off for every level")
+                         "library's setting (auto: off unless enabled), or on / off for every level")
     ap.add_argument("--shape", default=None, help="kernel mode: launch shape variant,rows,zchunk (default: autotune)")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -263,8 +263,10 @@ int rt_bench_fine_kernel(rt_hier* h, int precision, int mode, int reps, double* 
 int rt_smooth_f32(rt_hier* h, int lvl, int smoother, int sweeps, double omega);
 /* FP32 Chebyshev smoothing of stencil level lvl (1 .. coarsest-1) as one cooperative launch per
  * smoothing (the steps separated by a bounded grid barrier) instead of one launch per step.
- * rt_autotune times both on sets of 8 steps, captured as graphs, and enables it per level where
- * it is faster; batched solves always use separate launches (their instances run concurrently). */
+ * Off by default.  rt_autotune times both forms on sets of 8 steps, captured as graphs, and
+ * reports the times here without switching: alone the fused sets are faster, but inside the
+ * solver's conditional-loop graphs whole solves measured slower with them.  Batched solves always
+ * use separate launches (their instances run concurrently). */
 int rt_set_level_fused(rt_hier* h, int lvl, int on);
 int rt_level_fused_info(rt_hier* h, int lvl, int* on, double* us_separate, double* us_fused);
 /* SIMT arithmetic peak of the context's device in TFLOP/s, from a project microbenchmark (16

@@ -2447,17 +2447,18 @@ static double time_level_sweeps(rt_hier* h, int lvl, bool fused, int nsteps, int
 static int autotune_level_kernels(rt_hier* h, int reps) {
     if (!h->stencil_ready || h->L.size() < 3) return RT_OK;
     // fused Chebyshev sweeps (one cooperative launch per smoothing) per stencil level, timed on
-    // sets of 8 steps against the separate launches of the chosen lane-split / bulk variant
-    h->cheby_fused = 0;
+    // sets of 8 steps against the separate launches of the chosen lane-split / bulk variant.
+    // The timings are recorded, the choice stays with the caller (rt_set_level_fused): alone the
+    // fused sets are faster, but inside the solver's conditional-loop graphs the whole solve
+    // measured slower with them
+    const uint32_t keep = h->cheby_fused;
     if (rtk::st_cheby_fused_ok(h)) {
         for (int lvl = 1; lvl + 1 < (int)h->L.size() && lvl < 15; lvl++) {
-            const double t0 = time_level_sweeps(h, lvl, false, 8, reps);
-            const double t1 = time_level_sweeps(h, lvl, true, 8, reps);
-            h->fused_us[lvl][0] = t0;
-            h->fused_us[lvl][1] = t1;
-            if (t1 < t0) h->cheby_fused |= 1u << lvl;
+            h->fused_us[lvl][0] = time_level_sweeps(h, lvl, false, 8, reps);
+            h->fused_us[lvl][1] = time_level_sweeps(h, lvl, true, 8, reps);
         }
     }
+    h->cheby_fused = keep;
     for (int t = 0; t < 2; t++) {
         if (t == 1 && !(h->P.coarse_bf16 && h->L[1].st16)) continue;
         const int saved_bf16 = h->P.coarse_bf16;
