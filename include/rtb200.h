@@ -263,6 +263,8 @@ int rt_bench_fine_kernel(rt_hier* h, int precision, int mode, int reps, double* 
 int rt_smooth_f32(rt_hier* h, int lvl, int smoother, int sweeps, double omega);
 /* FP32 Chebyshev smoothing of stencil level lvl (1 .. coarsest-1) as one cooperative launch per
  * smoothing (the steps separated by a bounded grid barrier) instead of one launch per step.
+ * on: 0 off, 1 on (the resident form when the level's nodes fit on the device at once, else the
+ * streaming form), 2 on with the streaming form at any size.
  * Off by default.  rt_autotune times both forms on sets of 8 steps, captured as graphs, and
  * reports the times here without switching: alone the fused sets are faster, but inside the
  * solver's conditional-loop graphs whole solves measured slower with them.  Batched solves always

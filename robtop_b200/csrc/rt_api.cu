@@ -353,6 +353,7 @@ static void ws_sync(rt_hier* w) {
     memcpy(w->tune_us, p->tune_us, sizeof(w->tune_us));
     memcpy(w->st_variant, p->st_variant, sizeof(w->st_variant));
     w->cheby_fused = p->cheby_fused;
+    w->cheby_stream = p->cheby_stream;
     w->dinv64 = p->dinv64; w->dinv32 = p->dinv32;
     for (size_t i = 0; i < w->L.size(); i++) {
         rt_level& a = w->L[i];
@@ -2478,11 +2479,12 @@ static int autotune_level_kernels(rt_hier* h, int reps) {
 }
 
 extern "C" int rt_set_level_fused(rt_hier* h, int lvl, int on) {
-    if (!h || lvl < 1 || lvl + 1 >= (int)h->L.size() || lvl >= 15) return RT_EINVAL;
+    if (!h || lvl < 1 || lvl + 1 >= (int)h->L.size() || lvl >= 15 || on < 0 || on > 2) return RT_EINVAL;
     RT_NOT_WORKSPACE(h);
     if (on && !rtk::st_cheby_fused_ok(h))
         return rt_fail(h->ctx, RT_ECUDA, "the device cannot run the fused Chebyshev sweeps");
     h->cheby_fused = on ? (h->cheby_fused | (1u << lvl)) : (h->cheby_fused & ~(1u << lvl));
+    h->cheby_stream = on == 2 ? (h->cheby_stream | (1u << lvl)) : (h->cheby_stream & ~(1u << lvl));
     h->graph_epoch++;
     return RT_OK;
 }

@@ -1123,7 +1123,7 @@ int st_cheby_fused(rt_hier* h, int lvl, float* u, const float* f, float* tmp, fl
     // else the streaming form over a node loop
     const long want = rt_blocks(4 * L.nv, ST_BS);
     const long cap = (long)nb * h->ctx->sm_count;
-    const bool resident = want <= (long)coop_blocks(h, true) * h->ctx->sm_count;
+    const bool resident = !((h->cheby_stream >> lvl) & 1u) && want <= (long)coop_blocks(h, true) * h->ctx->sm_count;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(resident ? want : (want < cap ? want : cap)));
     cfg.blockDim = dim3(ST_BS);

@@ -99,6 +99,7 @@ struct rt_hier {
     // stencil levels whose FP32 Chebyshev sweeps run as one cooperative launch (bit lvl; rt_autotune),
     // with the measured time of a sweep set [level][separate launches, one launch]
     uint32_t cheby_fused = 0;
+    uint32_t cheby_stream = 0;  // fused levels held to the streaming form (rt_set_level_fused on = 2)
     double fused_us[15][2] = {};
     double* dinv64 = nullptr;        // [6][nv] inverted diagonal blocks of the finest level
     float* dinv32 = nullptr;

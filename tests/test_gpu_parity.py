@@ -316,11 +316,12 @@ def test_chebyshev_bounds_and_steps(pair):
         assert rel_err(G[i].getDisplacement(), uo) < 1e-9, f"level {i}"
 
 
-@pytest.mark.parametrize("nsteps", [3, 8])
-def test_fused_chebyshev_sweeps(pair, nsteps):
+@pytest.mark.parametrize("nsteps,form", [(3, 1), (8, 1), (3, 2), (8, 2)])
+def test_fused_chebyshev_sweeps(pair, nsteps, form):
     """FP32 Chebyshev smoothing of every stencil level as one cooperative launch (grid barrier
-    between the steps) gives the separate launches' result, and both follow the oracle's FP64
-    steps to FP32 accuracy; odd step counts end with the copy back into u."""
+    between the steps), in the resident (form 1 on these small levels) and the streaming form
+    (2), gives the separate launches' result, and both follow the oracle's FP64 steps to FP32
+    accuracy; odd step counts end with the copy back into u."""
     cfg, ctx, G, H = pair
     lm = [G.smoother_lmax(i) for i in range(H.nlev - 1)]
     H.set_lmax(lm)
@@ -329,7 +330,7 @@ def test_fused_chebyshev_sweeps(pair, nsteps):
     for i in range(1, H.nlev - 1):
         u, f = _rand_vec(G, i, 130 + i), _rand_vec(G, i, 140 + i)
         out = []
-        for fused in (0, 1):
+        for fused in (0, form):
             rb._capi.check(lib.rt_set_level_fused(G.handle, i, fused), ctx.handle)
             G[i].setDisplacement(u)
             G[i].setForce(f)
