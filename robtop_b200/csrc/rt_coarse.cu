@@ -760,23 +760,30 @@ __global__ void __launch_bounds__(ST_BS) k_prolong(int fnx, int fny, int fnz, in
     const int cvx = cnx + 1, cvy = cny + 1, cvz = cnz + 1;
     const long nvf = (long)fvx * fvy * fvz, nvc = (long)cvx * cvy * cvz;
     for (long vf = blockIdx.x * (long)blockDim.x + threadIdx.x; vf < nvf; vf += (long)gridDim.x * blockDim.x) {
-        if (!fvact[vf]) continue;
+        // every load depends on the indices only: the activity flag, the fine values and the
+        // coarse corners are all in flight at once, and the flag decides only the store
+        const bool act = fvact[vf];
         const int x = (int)(vf % fvx), y = (int)((vf / fvx) % fvy), z = (int)(vf / ((long)fvx * fvy));
         const int X0 = x / R, Y0 = y / R, Z0 = z / R;
         const int ox = x - R * X0, oy = y - R * Y0, oz = z - R * Z0;
+        const T f0 = uf[vf], f1 = uf[nvf + vf], f2 = uf[2 * nvf + vf];
         T s[3] = {T(0), T(0), T(0)};
 #pragma unroll
         for (int i = 0; i < 8; i++) {
             const int a = i & 1, b = (i >> 1) & 1, c = i >> 2;
             const int wx = a ? ox : R - ox, wy = b ? oy : R - oy, wz = c ? oz : R - oz;
-            if (wx == 0 || wy == 0 || wz == 0) continue;
+            if (wx == 0 || wy == 0 || wz == 0) continue;  // also keeps the corner inside the coarse box
             const long vc = (X0 + a) + (long)cvx * ((Y0 + b) + (long)cvy * (Z0 + c));
             const T wgt = T(wx * wy * wz) * (T(1) / T(R * R * R));
             s[0] += wgt * uc[vc];
             s[1] += wgt * uc[nvc + vc];
             s[2] += wgt * uc[2 * nvc + vc];
         }
-        uf[vf] += s[0]; uf[nvf + vf] += s[1]; uf[2 * nvf + vf] += s[2];
+        if (act) {
+            uf[vf] = f0 + s[0];
+            uf[nvf + vf] = f1 + s[1];
+            uf[2 * nvf + vf] = f2 + s[2];
+        }
     }
 }
 
