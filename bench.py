@@ -73,6 +73,37 @@ def form_text(form):
 METRIC = "worst-case solve (Lanczos k=16, MG-PCG inner solves to rel. residual 1e-6) on 128x128x64"
 
 
+def init_replicas(ws, lrank, backend="nccl"):
+    """One process per GPU: the process group the replicas use for their barriers and the
+    max-over-ranks timing (no data-path collective: every replica solves its own problem).
+    Returns the torch.distributed module, or None for a single process."""
+    if ws <= 1:
+        return None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    if backend == "nccl":
+        torch.cuda.set_device(lrank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", lrank))
+    else:
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def max_over_ranks(dist, values, device="cuda"):
+    """Element-wise maximum of a list of timings over all ranks (the job's time is its slowest
+    replica's); the values unchanged for a single process."""
+    if dist is None:
+        return list(values)
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -1078,14 +1109,7 @@ def main():
     import torch
 
     ws, rank, lrank = dist_env()
-    dist = None
-    if ws > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        torch.cuda.set_device(lrank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", lrank))
+    dist = init_replicas(ws, lrank)
 
     import robtop_b200 as rb
     from robtop_b200 import configs
@@ -1121,10 +1145,10 @@ def main():
             # end to end through the public API with host buffers, under the same clock sampler
             e2e_ms, h2d, d2h = e2e_steps(rb, ctx, G, cfg, args.steps)
         clk = clocks.stop() if clocks else None
-        if dist:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        if prec == rb.FP32:
+            ms, e2e_ms = max_over_ranks(dist, [ms, e2e_ms])
+        else:
+            ms = max_over_ranks(dist, [ms])[0]
         results[prec] = dict(ms=ms, lams=lams, infos=[i.as_dict() for i in infos], launches=nlaunch, clocks=clk)
 
     # per-kernel device time over the same K steps (CUDA events around every launch; separate pass)
