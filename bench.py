@@ -111,8 +111,19 @@ def dist_env():
     return ws, rank, lrank
 
 
+def gpu_id(cuda_index):
+    """The id nvidia-smi should sample for CUDA device ``cuda_index``: its UUID.  nvidia-smi numbers
+    GPUs by NVML order and ignores CUDA_VISIBLE_DEVICES, so a CUDA ordinal can name another GPU."""
+    try:
+        import torch
+
+        return f"GPU-{torch.cuda.get_device_properties(cuda_index).uuid}"
+    except Exception:
+        return str(cuda_index)
+
+
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """nvidia-smi sampling during the timed region (``gpu`` is an id from gpu_id)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -160,7 +171,7 @@ class Clocks:
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "gpu": self.gpu}
 
 
 def build_problem(rb, configs, ctx, precision, dims=None):
@@ -249,7 +260,13 @@ NCU_TRAFFIC_PER_NODE = {("fine_cheby_f32", "register_march"): (71.0e6 + 3.3e6) /
                         ("fine_cheby_f32", "smem_tile_pipelined"): (45.329e6 + 0.256e6) / 1081665}
 
 
-def roofline(ctx, stats, G, peaks, tuning=None):
+# DRAM bytes per node of the finest-level kernels on the arch workload, from an ncu capture of the
+# same kernel variant on a smaller arch whose vectors exceed L2 (traffic grows with the nodes); empty
+# until captured
+NCU_TRAFFIC_ARCH = {}
+
+
+def roofline(ctx, stats, G, peaks, tuning=None, traffic_table=None):
     # dominant kernel by device time
     name, (n, ms) = max(stats.items(), key=lambda kv: kv[1][1])
     nv, ne = G[0].nv, G[0].ne
@@ -267,7 +284,7 @@ def roofline(ctx, stats, G, peaks, tuning=None):
     if tuning and name.startswith("fine_cheby"):
         t = tuning.get("chebyshev_" + name.rsplit("_", 1)[1], {})
         variant, shape = t.get("variant"), (t.get("rows"), t.get("zchunk"))
-    per_node = NCU_TRAFFIC_PER_NODE.get((name, variant))
+    per_node = (NCU_TRAFFIC_PER_NODE if traffic_table is None else traffic_table).get((name, variant))
     out.update({"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(ach / peak, 4), "traffic": int(per_node * nv) if per_node else None,
                 "traffic_source": "ncu capture of the same kernel variant on this workload" if per_node else None,
@@ -356,19 +373,71 @@ def cpu_baseline(gpu_inner_iters, gpu_vcycles, threads):
     x, it, rr = H.pcg(b, tol=1e-30, maxit=n_it, smoother=O.SMOOTH_SGS)
     t_it = (time.perf_counter() - t0) / n_it
     total = t_st + t_it * gpu_inner_iters
-    return {"value": 1.0 / total, "unit": "solves/s", "cores": threads, "kind": "port",
+    return {"value": 1.0 / total, "unit": "solves/s", "cores": threads, "kind": "port", "extrapolated": True,
             "sample": f"oracle FP64 stencil assembly ({t_st:.2f} s) + {n_it} MG-PCG iterations "
-                      f"({t_it:.3f} s each), extrapolated to the {gpu_inner_iters} PCG iterations of one GPU step",
+                      f"({t_it:.3f} s each), extrapolated to the plain method's {gpu_inner_iters} PCG iterations "
+                      "of one step on the GPU",
+            "sampled_wall_s": t_st + t_it * n_it, "scale_factor": total / (t_st + t_it * n_it),
             "seconds_per_step": total}
 
 
 def run_reference(args):
+    """The reference arm: the CPU restatement of the reference algorithm (oracle/, plain FP64 SGS
+    V-cycle PCG, OpenMP on all host cores) on the same workload as the default arm.  The
+    reference itself cannot be built here (its sources need Eigen, CGAL and OpenVDB).  A full step
+    on the 511x256x256 arch takes the oracle tens of minutes, so each step is a bounded sample: the
+    oracle runs stencil assembly and one inner solve to 1e-6 on the 127x64x64 arch, and the step
+    time is extrapolated to the full arch by node count and to the 17 inner solves of a step (k = 16
+    Lanczos solves + the displacement solve) at the sample's iterations per solve.  The line
+    carries the sampled wall seconds and the scale factor beside the extrapolated value."""
     ws, rank, lrank = dist_env()
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    # inner PCG iterations per step of the plain method on this workload (FP64, SGS V-cycle, measured
-    # by the oracle's own Lanczos on a bounded sample: 2 Lanczos steps, extrapolated to k=16)
+    if args.workload == "worstcase128":
+        return run_reference_128(args, threads)
+    dims = tuple(int(v) for v in args.size.split("x")) if args.size else ARCH["dims"]
+    solves = ARCH["k"] + 1
+    samples = []
+    for s_ in range(args.warmup + args.steps):
+        # iterations per solve from this sample (no GPU count on this arm)
+        smp = arch_cpu_sample(threads, dims, 0, solves)
+        its_full = solves * smp["sample_pcg_iterations"]
+        smp["plain_inner_iterations_full"] = its_full
+        smp["extrapolated_s_per_step"] = smp["node_scale_factor"] * (smp["sample_assembly_s"] +
+                                                                      smp["sample_s_per_iteration"] * its_full)
+        samples.append(smp)
+    tt = samples[args.warmup:]
+    sec = sum(t["extrapolated_s_per_step"] for t in tt) / len(tt)
+    wall = sum(t["sampled_wall_s"] for t in tt) / len(tt)
+    val = 1.0 / sec
+    last = tt[-1]
+    nx, ny, nz = dims
+    line = {"impl": "reference", "metric": METRIC_ARCH.replace(", learned+mixed form", ", plain FP64 method"),
+            "value": val, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"arch {nx}x{ny}x{nz}, worst-case solve (Lanczos k=16, inner PCG to 1e-6)",
+                       "threads": threads},
+            "extrapolated": True,
+            "sampled_wall_s_per_step": wall, "scale_factor": sec / wall,
+            "sample": {k: last[k] for k in ("sample_dims", "sample_nodes", "sample_assembly_s", "sample_pcg_iterations",
+                                            "sample_s_per_iteration", "node_scale_factor")},
+            "cpu_baseline": {"value": val, "unit": "solves/s", "cores": threads, "kind": "port", "extrapolated": True,
+                             "sample": "CPU restatement of the reference algorithm (the reference needs Eigen/CGAL/"
+                                       "OpenVDB and cannot be built here): stencil assembly + one inner solve to 1e-6 "
+                                       f"on the {'x'.join(map(str, last['sample_dims']))} arch per step "
+                                       f"({wall:.1f} s of CPU wall time), extrapolated by node count "
+                                       f"(x{last['node_scale_factor']:.1f}) and to {solves} inner solves "
+                                       f"(scale factor {sec / wall:.0f} overall)"},
+            "e2e": {"value": val, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_reference_128(args, threads):
+    """Reference arm of the 128x128x64 worst-case box: per step, stencil assembly + 2 of the 16
+    Lanczos inner solves by the oracle, the time scaled by 17/2."""
     import oracle as O
     from robtop_b200 import configs
 
@@ -377,32 +446,33 @@ def run_reference(args):
     H = O.Hierarchy(cfg["eact"], cfg["rho"], cfg["vfix"], p=3, E=1e6, nu=0.4)
     nv = H.arrs[0]["u"].size // 3
     nl = cfg["load_nodes"].size
-    times = []
+    times, walls = [], []
+    ksample = 2
+    scale_f = (WORKLOAD["k"] + 1) / ksample
     for s in range(args.warmup + args.steps):
         t0 = time.perf_counter()
         H.update_stencil()
-        ksample = 2
         work = np.zeros((ksample + 1) * 3 * nl + 10 * 3 * nv)
         lam = np.zeros(1)
-        inner = O.lib().or_lanczos(H.LA, H.nlev, O.ptr(H.KE), O.SMOOTH_SGS, 1, 1, 0.6, nl,
-                                   O.ptr(cfg["load_nodes"]), O.ptr(np.ascontiguousarray(cfg["normals"])), 0, 0, None,
-                                   100 + s, ksample, WORKLOAD["tol"], 500, O.ptr(lam), None, O.ptr(work))
+        O.lib().or_lanczos(H.LA, H.nlev, O.ptr(H.KE), O.SMOOTH_SGS, 1, 1, 0.6, nl, O.ptr(cfg["load_nodes"]),
+                           O.ptr(np.ascontiguousarray(cfg["normals"])), 0, 0, None, 100 + s, ksample, WORKLOAD["tol"],
+                           500, O.ptr(lam), None, O.ptr(work))
         dt = time.perf_counter() - t0
-        # the full step runs k Lanczos solves plus the final displacement solve
-        scale_f = (WORKLOAD["k"] + 1) / ksample
+        walls.append(dt)
         times.append(dt * scale_f)
     tt = times[args.warmup:]
     sec = sum(tt) / len(tt)
+    wall = sum(walls[args.warmup:]) / len(tt)
     val = 1.0 / sec
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "solves/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "worst-case 128x128x64 (z=0 clamped, top-face load set, wsff), Lanczos k=16",
                        "inner_tol": WORKLOAD["tol"], "threads": threads},
-            "cpu_baseline": {"value": val, "unit": "solves/s", "cores": threads, "kind": "port",
-                             "sample": "CPU restatement of the reference algorithm (the reference needs Eigen/CGAL/"
-                                       "OpenVDB and cannot be built here): stencil assembly + 2 of the 16 Lanczos "
-                                       "inner solves per step, time scaled by 17/2"},
+            "extrapolated": True, "sampled_wall_s_per_step": wall, "scale_factor": scale_f,
+            "cpu_baseline": {"value": val, "unit": "solves/s", "cores": threads, "kind": "port", "extrapolated": True,
+                             "sample": "CPU restatement of the reference algorithm: stencil assembly + 2 of the 16 "
+                                       "Lanczos inner solves per step, time scaled by 17/2"},
             "e2e": {"value": val, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -512,7 +582,7 @@ def run_c1(args):
     for _ in range(max(args.warmup, 3)):
         one_step()
     ctx.sync()
-    clocks = Clocks(0)
+    clocks = Clocks(gpu_id(0))
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     l0 = ctx.launches()
@@ -611,7 +681,7 @@ def run_voxelize(args):
     # one voxelisation takes well under a millisecond: time enough of them (about half a second)
     # for the clock sampler to see the timed region
     reps = max(args.steps, 6000)
-    clocks = Clocks(0)
+    clocks = Clocks(gpu_id(0))
     clocks.start()
     rb._capi.check(rb.lib().rt_bench_voxelize(ctx.handle, vf.ctypes.data, len(v), ff.ctypes.data, len(f), prefer,
                                               reps, C.byref(us)), ctx.handle)
@@ -696,7 +766,8 @@ def run_kernel(args):
             rb._capi.check(rb.lib().rt_set_tuning(G.handle, prec, mode, variant, ty, zc), ctx.handle)
             names = ["residual", "applyK", "jacobi", "chebyshev"]
             shapes = {f"{names[mode]}_{'f32' if prec == rb.FP32 else 'f64'}":
-                      {"variant": ["smem_tile", "register_march", "register_march_prefetch", "smem_tile_pipelined", "smem_tile_pairs_f32"][variant], "rows": ty,
+                      {"variant": ["smem_tile", "register_march", "register_march_prefetch", "smem_tile_pipelined",
+                                   "smem_tile_pairs_f32", "sum_factorised"][variant], "rows": ty,
                        "zchunk": zc}}
         else:
             shapes = G.autotune()
@@ -833,7 +904,7 @@ def run_batched(args):
     for _ in range(max(args.warmup, 3)):
         batch_step()
         seq_step()
-    clocks = Clocks(lrank)
+    clocks = Clocks(gpu_id(lrank))
     clocks.start()
     l0 = ctx.launches()
     tb, infos_b = 0.0, None
@@ -1016,7 +1087,7 @@ def run_c5(args):
 
     for w in range(args.warmup):
         oc_step(10 + w)
-    clocks = Clocks(lrank)
+    clocks = Clocks(gpu_id(lrank))
     clocks.start()
     l0 = ctx.launches()
     ms_oc, lams = 0.0, []
@@ -1062,6 +1133,372 @@ def run_c5(args):
     return 0
 
 
+# the default workload: the worst-case solve on the 511x256x256 arch, in the learned+mixed form
+ARCH = dict(dims=(511, 256, 256), k=16, tol=1e-6, design_iters=4, harvest_k=(1, 4, 12), crop=(33, 33, 33),
+            n_crops=32, train_steps=200, train_batch=8, vgoal=0.4)
+METRIC_ARCH = ("worst-case solve on the 511x256x256 arch (stencil assembly + Lanczos k=16 with MG-PCG inner solves "
+               "to rel. residual 1e-6 + the worst-case displacement solve), learned+mixed form")
+
+
+def arch_config(configs, dims):
+    """The arch of the given size; the tunnel radius (96 of 256) and the support pads (16 of 256)
+    scale with ny for the reduced sizes used by quick runs and the CPU baseline's sample."""
+    nx, ny, nz = dims
+    return configs.arch(nx, ny, nz, tunnel=int(round(96 * ny / 256)), pad=max(2, int(round(16 * ny / 256))))
+
+
+def arch_cpu_sample(threads, dims_full, plain_inner_its, solves, sample_dims=(127, 64, 64)):
+    """The oracle (plain FP64 SGS V-cycle PCG, OpenMP) on a reduced arch with the same shape: stencil
+    assembly plus one inner solve to 1e-6 of a top-face load.  Extrapolated to the full arch by node
+    count, to ``solves`` inner solves of ``plain_inner_its / solves`` iterations each (the plain
+    method's own iteration count on the full arch, measured on the GPU) plus one assembly."""
+    import oracle as O
+    from robtop_b200 import configs
+
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    cfg = arch_config(configs, sample_dims)
+    ws = cfg["vfix"] is not None
+    t0 = time.perf_counter()
+    H = O.Hierarchy(cfg["eact"], cfg["rho"], cfg["vfix"], p=3, E=1e6, nu=0.4)
+    H.update_stencil()
+    t_st = time.perf_counter() - t0
+    nv = H.arrs[0]["u"].size // 3
+    b = np.zeros(3 * nv)
+    b[2 * nv + cfg["load_nodes"]] = 1.0 / np.sqrt(cfg["load_nodes"].size)
+    t0 = time.perf_counter()
+    x, it, rr = H.pcg(b, tol=1e-6, maxit=200, smoother=O.SMOOTH_SGS)
+    t_pcg = time.perf_counter() - t0
+    t_it = t_pcg / max(it, 1)
+    nx, ny, nz = dims_full
+    scale = (nx + 1) * (ny + 1) * (nz + 1) / nv
+    total = scale * (t_st + t_it * plain_inner_its)
+    return {"sampled_wall_s": t_st + t_pcg, "sample_dims": list(sample_dims), "sample_nodes": int(nv),
+            "sample_assembly_s": t_st, "sample_pcg_iterations": int(it), "sample_s_per_iteration": t_it,
+            "node_scale_factor": scale, "extrapolated_s_per_step": total, "solves": solves,
+            "plain_inner_iterations_full": int(plain_inner_its), "ws": ws}
+
+
+def arch_design_and_network(rb, learned, ctx, G, design_iters, seed0=10, first_iter=0, on_iter=None):
+    """``design_iters`` OC iterations of the current form (worst-case Lanczos k = 16, sensitivity,
+    filter, OC update); after each, (density, residual, MG-error) samples harvested from the solver
+    are cropped; then the U-Net is trained on the crops by the library's kernels and its weights are
+    moved to a network over the full node box.  on_iter(i, lam) is called after iteration i."""
+    import torch
+
+    hnet = learned.UNet.for_grid(G, seed=0)
+    rng = np.random.default_rng(11)
+    samples, t_harvest = [], 0.0
+    lam_c = C.c_double()
+    for it in range(design_iters):
+        rb._capi.check(rb.lib().rt_oc_iteration(G.handle, rb.WORST_LANCZOS, ARCH["k"], ARCH["tol"], seed0 + it,
+                                                ARCH["vgoal"], C.byref(lam_c)), ctx.handle)
+        if on_iter:
+            on_iter(first_iter + it, lam_c.value)
+        G.update_stencil()
+        t0 = time.perf_counter()
+        for kk in ARCH["harvest_k"]:
+            inp, tgt = learned.harvest(G, hnet, kk, seed=1000 * it + kk)
+            samples += learned.crops(inp, tgt, hnet.dims, ARCH["crop"], ARCH["n_crops"] // len(ARCH["harvest_k"]), rng)
+            del inp, tgt
+        t_harvest += time.perf_counter() - t0
+    torch.cuda.empty_cache()
+    net = learned.UNet(ctx, *ARCH["crop"], seed=1)
+    net.output_scale = hnet.output_scale
+    t0 = time.perf_counter()
+    losses = learned.train(net, samples, steps=ARCH["train_steps"], batch=ARCH["train_batch"], lr=1e-3, seed=0)
+    t_train = time.perf_counter() - t0
+    learned.transfer(net, hnet)
+    net.close()
+    n = len(samples)
+    del samples
+    torch.cuda.empty_cache()
+    return hnet, {"losses": losses, "harvest_s": t_harvest, "train_s": t_train, "samples": n}
+
+
+def arch_attach_network(learned, G, cfg, hnet):
+    """Attach the network with the cost-aware fallback ratio: the plain V-cycle PCG's rate and
+    iteration time on this design (a unit top-face load, the second of two solves) against the
+    network's time."""
+    nv = G[0].nv
+    f = np.zeros(3 * nv)
+    f[2 * nv + cfg["load_nodes"]] = 1.0 / np.sqrt(cfg["load_nodes"].size)
+    learned.attach(G, None)
+    G[0].setForce(f)
+    for _ in range(2):
+        G[0].reset_displacement()
+        cal = G.pcg(ARCH["tol"], 500)
+    t_net = learned.forward_seconds(hnet)
+    ratio = learned.cost_aware_ratio(cal.iterations, cal.rel_residual, cal.seconds, t_net)
+    learned.attach(G, hnet, fallback_ratio=ratio)
+    return cal, t_net, ratio
+
+
+def run_c5_oc40(args):
+    """The 40-iteration worst-case optimisation of the 511x256x256 arch (volume 0.4, filter radius 2,
+    move 0.06, damping 0.5, p = 3): iterations 1-4 in the mixed form while training samples are
+    harvested, the U-Net trained, iterations 5-40 in the learned+mixed form.  Every 10 iterations
+    the design's worst-case eigenvalue and the compliance of a fixed unit top-face load are
+    recomputed with the plain FP64 method and compared with the learned+mixed values on the same
+    design.  Prints one JSON line with the per-iteration eigenvalues and the checks."""
+    import torch
+
+    import robtop_b200 as rb
+    from robtop_b200 import configs, learned
+
+    ws_, rank, lrank = dist_env()
+    dims = tuple(int(v) for v in args.size.split("x")) if args.size else ARCH["dims"]
+    n_iter = args.oc_iters
+    ctx = make_ctx(rb, lrank)
+    stream = torch.cuda.ExternalStream(ctx_stream_handle(ctx))
+    cfg = arch_config(configs, dims)
+    p = rb.default_params(mode=cfg["mode"], youngs_modulus=1e6, poisson_ratio=0.4, power_penalty=3.0, min_rho=1e-3,
+                          volume_ratio=ARCH["vgoal"], design_step=0.06, damp_ratio=0.5, filter_radius=2.0)
+    G = rb.HierarchyGrid(ctx, p)
+    G.genFromBox(cfg["eact"])
+    apply_form(rb, G, FORMS_C5["mixed"])
+    G[0].setRho(cfg["rho"].ravel())
+    G.set_support(cfg["vfix"])
+    G.set_load_nodes(cfg["load_nodes"], cfg["normals"])
+    G.update_stencil()
+    G.autotune(reps=2)
+    nv = G[0].nv
+    fload = np.zeros(3 * nv)
+    fload[2 * nv + cfg["load_nodes"]] = 1.0 / np.sqrt(cfg["load_nodes"].size)
+    lams, ms_iter, checks = [], [], []
+
+    def timed(fn):
+        ctx.sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), out
+
+    def compliance():
+        G[0].setForce(fload)
+        G[0].reset_displacement()
+        info = G.pcg(ARCH["tol"], 2000)
+        return float(fload @ G[0].getDisplacement()), info.iterations
+
+    def check(i):
+        # the current design in both forms (the stencil of the design before this OC update)
+        G.update_stencil()
+        lam_l, _ = G.worst_case(rb.WORST_LANCZOS, ARCH["k"], ARCH["tol"], seed=7)
+        c_l, it_l = compliance()
+        net_saved = G_net[0]
+        learned.attach(G, None)
+        apply_form(rb, G, FORMS_C5["plain"])
+        G.update_stencil()
+        ms_p, (lam_p, info_p) = timed(lambda: G.worst_case(rb.WORST_LANCZOS, ARCH["k"], ARCH["tol"], seed=7))
+        c_p, it_p = compliance()
+        apply_form(rb, G, FORMS_C5["mixed"])
+        G.update_stencil()
+        if net_saved is not None:
+            learned.attach(G, net_saved, fallback_ratio=G_net[1])
+        checks.append({"iteration": i, "lambda": lam_l, "lambda_plain_fp64": lam_p,
+                       "lambda_rel_diff": abs(lam_l - lam_p) / abs(lam_p), "compliance": c_l,
+                       "compliance_plain_fp64": c_p, "compliance_rel_diff": abs(c_l - c_p) / abs(c_p),
+                       "pcg_iterations": it_l, "pcg_iterations_plain_fp64": it_p, "plain_worst_case_ms": ms_p})
+
+    G_net = [None, 1.0]
+    t0 = time.perf_counter()
+    n_design = min(ARCH["design_iters"], n_iter)
+    hnet, tr = arch_design_and_network(rb, learned, ctx, G, n_design, seed0=10,
+                                       on_iter=lambda i, lam: lams.append(lam))
+    cal, t_net, ratio = arch_attach_network(learned, G, cfg, hnet)
+    G_net[0], G_net[1] = hnet, ratio
+    lam_c = C.c_double()
+    for it in range(n_design, n_iter):
+        if (it + 1) % 10 == 0 or it + 1 == n_iter:
+            check(it + 1)
+        ms, _ = timed(lambda: rb._capi.check(rb.lib().rt_oc_iteration(G.handle, rb.WORST_LANCZOS, ARCH["k"],
+                                                                        ARCH["tol"], 10 + it, ARCH["vgoal"],
+                                                                        C.byref(lam_c)), ctx.handle))
+        ms_iter.append(ms)
+        lams.append(lam_c.value)
+    wall = time.perf_counter() - t0
+    applied, off = learned.stats(G)
+    rho = G[0].getRho()
+    eact = cfg["eact"].ravel().astype(bool)
+    line = {"metric": "40-iteration worst-case optimisation of the 511x256x256 arch, learned+mixed form, checked "
+                      "against the plain FP64 method every 10 iterations",
+            "value": len(ms_iter) / (sum(ms_iter) * 1e-3) if ms_iter else None, "unit": "OC iterations/s",
+            "n_gpus": 1, "steps": len(ms_iter), "warmup": n_design, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64+f32+bf16", "data": "synthetic",
+            "config": {"workload": f"arch {'x'.join(map(str, dims))}, {n_iter} OC iterations (the first {n_design} "
+                                   "without the network, harvesting its training samples)",
+                       "lambda_per_iteration": lams, "ms_per_iteration": ms_iter, "checks": checks,
+                       "max_lambda_rel_diff": max((c["lambda_rel_diff"] for c in checks), default=None),
+                       "max_compliance_rel_diff": max((c["compliance_rel_diff"] for c in checks), default=None),
+                       "volume_fraction": float(rho[eact].mean()), "learned_corrections": applied,
+                       "learned_judged_off_at_end": off, "fallback_ratio": ratio, "network_ms": t_net * 1e3,
+                       "wall_s": wall}}
+    if rank == 0:
+        print(json.dumps(line))
+    hnet.close()
+    G.close()
+    ctx.close()
+    return 0
+
+
+def run_arch(args):
+    """Default workload.  A step is one worst-case solve of the current design of the 511x256x256
+    arch (solid box minus a radius-96 tunnel along x, four 16x16 support pads at the bottom corners,
+    top face loadable with normal-constrained loads, wscf, p = 3): Galerkin stencil assembly, the
+    largest eigenvalue of the load-space compliance operator by Lanczos (k = 16) whose inner MG-PCG
+    solves run to relative residual 1e-6, and the worst-case displacement solve.
+
+    Set-up (untimed): ``design_iters`` OC iterations (volume 0.4, filter radius 2, move 0.06,
+    damping 0.5) give the design; after each, (density, residual, MG-error) samples are harvested
+    from the solver and cropped; the U-Net is trained on the crops by the library's forward and
+    backward kernels and attached to the full-size hierarchy with the cost-aware fallback ratio.
+    ``value`` is the learned+mixed form (FP32 V-cycles inside FP64 flexible CG plus the network's
+    correction while it pays); the mixed form without the network and the plain FP64 method are
+    timed on the same design after the timed steps, with their eigenvalues."""
+    import torch
+
+    ws, rank, lrank = dist_env()
+    dist = init_replicas(ws, lrank)
+
+    import robtop_b200 as rb
+    from robtop_b200 import configs, learned
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    dims = tuple(int(v) for v in args.size.split("x")) if args.size else ARCH["dims"]
+    ctx = make_ctx(rb, lrank)
+    stream = torch.cuda.ExternalStream(ctx_stream_handle(ctx))
+    t_setup0 = time.perf_counter()
+    cfg = arch_config(configs, dims)
+    p = rb.default_params(mode=cfg["mode"], youngs_modulus=1e6, poisson_ratio=0.4, power_penalty=3.0, min_rho=1e-3,
+                          volume_ratio=ARCH["vgoal"], design_step=0.06, damp_ratio=0.5, filter_radius=2.0)
+    G = rb.HierarchyGrid(ctx, p)
+    G.genFromBox(cfg["eact"])
+    apply_form(rb, G, FORMS_C5["mixed"])
+    G[0].setRho(cfg["rho"].ravel())
+    G.set_support(cfg["vfix"])
+    G.set_load_nodes(cfg["load_nodes"], cfg["normals"])
+    G.update_stencil()
+    tuning = G.autotune(reps=2) if args.tiles == "autotune" else G.set_tiles(*map(int, args.tiles.split(",")))
+    nv = G[0].nv
+
+    # design iterations, harvesting training samples from the solver after each, then training
+    hnet, tr = arch_design_and_network(rb, learned, ctx, G, ARCH["design_iters"], seed0=10)
+    cal, t_net, ratio = arch_attach_network(learned, G, cfg, hnet)
+    losses, t_harvest, t_train, n_samples = tr["losses"], tr["harvest_s"], tr["train_s"], tr["samples"]
+    t_setup = time.perf_counter() - t_setup0
+    rho_design = G[0].getRho()
+
+    warm = max(args.warmup, 3)
+    for w in range(warm):
+        step(rb, G, 10 + w)
+    if dist:
+        dist.barrier()
+    applied0, _ = learned.stats(G)
+    clocks = Clocks(gpu_id(lrank))
+    clocks.start()
+    ms, lams, infos, nlaunch = time_steps(rb, ctx, G, args.steps)
+    applied1, judged_off = learned.stats(G)
+    # end to end through the public API with host buffers: H2D of the design density, the solve,
+    # D2H of the worst-case load field, every step
+    n_e2e = min(args.steps, 5)
+    e2e_ms, h2d, d2h = e2e_steps(rb, ctx, G, {"rho": rho_design}, n_e2e)
+    clk = clocks.stop()
+    ms, e2e_ms = max_over_ranks(dist, [ms, e2e_ms])
+
+    # the same design in the mixed form without the network and in the plain FP64 method
+    def timed(fn):
+        ctx.sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), out
+
+    learned.attach(G, None)
+    forms = {}
+    for name in ("mixed", "plain"):
+        apply_form(rb, G, FORMS_C5[name])
+        ms_f, (lam_f, info_f) = timed(lambda: step(rb, G, 100))
+        forms[name] = (ms_f, lam_f, info_f.inner_iterations)
+    apply_form(rb, G, FORMS_C5["mixed"])
+    learned.attach(G, hnet, fallback_ratio=ratio)
+
+    # per-kernel device time over one step (CUDA events around every launch; graphs off)
+    ctx.profile(True)
+    ctx.profile_reset()
+    time_steps(rb, ctx, G, 1)
+    stats = {k: v for k, v in ctx.profile_stats().items() if v[0] > 0}
+    ctx.profile(False)
+    roof = roofline(ctx, stats, G, peaks, tuning, traffic_table=NCU_TRAFFIC_ARCH)
+    top = sorted(stats.items(), key=lambda kv: -kv[1][1])[:10]
+
+    ms_step = ms / args.steps
+    lam = lams[0]
+    m_ms, m_lam, m_it = forms["mixed"]
+    p_ms, p_lam, p_it = forms["plain"]
+    nx, ny, nz = dims
+    line = {
+        "metric": METRIC_ARCH, "value": ws * args.steps / (ms * 1e-3), "unit": "solves/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": warm, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64+f32+bf16", "data": "synthetic",
+        "config": {"workload": f"arch {nx}x{ny}x{nz} (tunnel radius {int(round(96 * ny / 256))}, support pads, top "
+                               f"face loadable, wscf), design after {ARCH['design_iters']} OC iterations (V 0.4, R 2, "
+                               "move 0.06, eta 0.5, p 3); Lanczos k=16, inner MG-PCG to 1e-6, stencil assembly included",
+                   "form": "learned+mixed: " + form_text(FORMS_C5["mixed"]) + ", FP64 coarsest solve, FP64 flexible "
+                           "CG vectors and dots; U-Net correction z += N(rho, r, Vcycle(r)) under the cost-aware gate",
+                   "speedup_vs_plain_fp64": p_ms / ms_step, "speedup_vs_mixed_without_network": m_ms / ms_step,
+                   "plain_fp64_ms_per_step": p_ms, "mixed_ms_per_step": m_ms,
+                   "speedup_mixed_vs_plain_fp64": p_ms / m_ms,
+                   "lambda_learned_mixed": lam, "lambda_mixed": m_lam, "lambda_plain_fp64": p_lam,
+                   "lambda_rel_diff": abs(lam - p_lam) / abs(p_lam),
+                   "lambda_rel_diff_mixed": abs(m_lam - p_lam) / abs(p_lam),
+                   "inner_pcg_iterations": infos[0].inner_iterations, "inner_pcg_iterations_mixed": m_it,
+                   "inner_pcg_iterations_plain_fp64": p_it,
+                   "learned": {"fallback_ratio": ratio, "plain_rate_per_iteration":
+                               float(cal.rel_residual) ** (1.0 / max(cal.iterations, 1)),
+                               "plain_iteration_ms": cal.seconds * 1e3 / max(cal.iterations, 1),
+                               "network_ms": t_net * 1e3, "corrections_in_timed_steps": applied1 - applied0,
+                               "judged_off_at_end": judged_off, "train_steps": ARCH["train_steps"],
+                               "train_crops": n_samples,
+                               "loss_first": float(np.mean(losses[:10])), "loss_last": float(np.mean(losses[-20:])),
+                               "harvest_s": t_harvest, "train_s": t_train},
+                   "setup_s": t_setup, "e2e_steps": n_e2e,
+                   "l2": "working set several GB of vectors and stencils >> 126 MB L2 per step",
+                   "parallelism": f"replicas x{ws}", "tile_shapes": tuning},
+        "clocks": clk, "gpu_launches": nlaunch, "roofline": roof,
+        "kernel_top": {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in top},
+        "e2e": {"value": ws * n_e2e / (e2e_ms * 1e-3), "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        smp = arch_cpu_sample(threads, dims, p_it, ARCH["k"] + 1)
+        line["cpu_baseline"] = {"value": 1.0 / smp["extrapolated_s_per_step"], "unit": "solves/s", "cores": threads,
+                                "kind": "port", "extrapolated": True,
+                                "sample": f"oracle plain FP64 SGS V-cycle PCG on the {'x'.join(map(str, smp['sample_dims']))}"
+                                          f" arch: assembly + one solve to 1e-6 ({smp['sample_pcg_iterations']} iterations,"
+                                          f" {smp['sampled_wall_s']:.1f} s), scaled by node count x{smp['node_scale_factor']:.1f}"
+                                          f" and to the plain method's {p_it} inner iterations per step on the GPU",
+                                **smp}
+    if rank == 0:
+        print(json.dumps(line))
+    hnet.close()
+    G.close()
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1069,8 +1506,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="worstcase", choices=["worstcase", "batched", "learned", "c5", "voxelize", "c1"],
-                    help="batched: the 12-instance + 8-RHS batched-solve configuration instead of the headline one")
+    ap.add_argument("--workload", default="arch",
+                    choices=["arch", "worstcase128", "batched", "learned", "c5", "c5oc40", "voxelize", "c1"],
+                    help="arch (default): the worst-case solve on the 511x256x256 arch, learned+mixed vs mixed vs plain "
+                         "FP64; worstcase128: the 128x128x64 worst-case box; batched: the 12-instance + 8-RHS batched "
+                         "solves; c5: timed OC iterations of the arch; c5oc40: the 40-iteration arch optimisation with "
+                         "the plain FP64 check every 10")
     ap.add_argument("--forms", default="both", choices=["both", "mixed"],
                     help="mixed: time only the mixed form (short command for launch-list captures)")
     ap.add_argument("--conv", default="16,16", help="--kernel conv3: input and output channels")
@@ -1079,7 +1520,8 @@ def main():
                                                        "st_cheby_bf16", "st_cheby_f64", "st_jacobi_f32",
                                                        "fine_cheby_f32", "fine_residual_f64", "fine_applyK_f64",
                                                        "fine_residual_f32"])
-    ap.add_argument("--size", default=None, help="kernel mode: grid NXxNYxNZ (default: the bench workload)")
+    ap.add_argument("--size", default=None, help="kernel mode and arch workload: grid NXxNYxNZ (default: the bench "
+                                                  "workload)")
     ap.add_argument("--level", type=int, default=1, help="kernel mode, st_* kernels: the stencil level")
     ap.add_argument("--tiles", default="autotune",
                     help="finest-level launch shape of the worst-case bench: autotune, or variant,rows,zchunk for "
@@ -1088,6 +1530,7 @@ def main():
                     help="FP32 Chebyshev sweeps of the stencil levels as one cooperative launch per smoothing: the "
                          "library's setting (auto: off unless enabled), or on / off for every level")
     ap.add_argument("--shape", default=None, help="kernel mode: launch shape variant,rows,zchunk (default: autotune)")
+    ap.add_argument("--oc-iters", type=int, default=40, help="c5oc40 workload: OC iterations")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -1105,6 +1548,16 @@ def main():
         return run_c1(args)
     if args.workload == "c5":
         return run_c5(args)
+    if args.workload == "c5oc40":
+        return run_c5_oc40(args)
+    if args.workload == "arch":
+        return run_arch(args)
+    return run_worstcase128(args)
+
+
+def run_worstcase128(args):
+    """The worst-case solve on the 128x128x64 box (smoothed random density, z = 0 clamped, top face
+    loadable, wsff): mixed form timed, plain FP64 beside it."""
 
     import torch
 
@@ -1137,7 +1590,7 @@ def main():
             step(rb, G, 10 + w)
         if dist:
             dist.barrier()
-        clocks = Clocks(lrank) if prec == rb.FP32 else None
+        clocks = Clocks(gpu_id(lrank)) if prec == rb.FP32 else None
         if clocks:
             clocks.start()
         ms, lams, infos, nlaunch = time_steps(rb, ctx, G, args.steps)
@@ -1193,8 +1646,10 @@ def main():
                 "d2h_bytes_per_step": d2h},
     }
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(r32["infos"][0]["inner_iterations"], r32["infos"][0]["vcycles"],
-                                            os.cpu_count() or 1)
+        # the CPU runs the plain method: its time is extrapolated to the plain method's own inner
+        # iteration count on the GPU (the mixed form's count when the plain form was not run)
+        its_plain = r64["infos"][0]["inner_iterations"] if r64 else r32["infos"][0]["inner_iterations"]
+        line["cpu_baseline"] = cpu_baseline(its_plain, r32["infos"][0]["vcycles"], os.cpu_count() or 1)
     if rank == 0:
         print(json.dumps(line))
     G.close()

@@ -236,7 +236,10 @@ int rt_relative_residual(rt_hier* h, double* rel);
  * rejected with RT_EINVAL and a message on stderr.  The array's address is looked
  * up on the first call per device (make that call before any stream capture).
  * All calls share the array: calls that overlap on the GPU race.  Runs on
- * cuda_stream (NULL: the legacy default stream) of the current device. */
+ * cuda_stream (NULL: the legacy default stream) of the current device.  The
+ * address is cached with the id of the context it belongs to and looked up again
+ * when the current context changes (e.g. after cudaDeviceReset).  An error
+ * already pending on the calling thread is reported as RT_ECUDA, not cleared. */
 #define RT_NOALLOC_MAX_PARTIALS 65536
 #define RT_NOALLOC_MAX_N (65536LL * 4096LL)
 int rt_compliance_noalloc(const double* f_dev, const double* u_dev, long long n, double* out_dev,
@@ -250,9 +253,12 @@ int rt_autotune(rt_hier* h, int reps);
 /* chosen shape of a finest-level kernel; mode 0 residual, 1 applyK, 2 Jacobi, 3 Chebyshev;
  * variant 0 shared-memory element tile (ty 2, 4 or 8 node rows), 1 register-marching element kernel, 2 register marching with
  * each layer's output-stage loads issued before its element arithmetic, 3 shared-memory element tile software-pipelined
- * over z (element layer z+1 and node layer z share one barrier interval; ty 2, 4 or 8) */
+ * over z (element layer z+1 and node layer z share one barrier interval; ty 2, 4 or 8), 4 (FP32) variant 3 with
+ * two elements per thread in packed FP32, 5 sum-factorised row marching (the element grid's Hadamard stages shared between
+ * neighbouring elements, one warp per node row, one barrier per layer; ty 4, 8 or 16 node rows) */
 int rt_tuning_info(rt_hier* h, int precision, int mode, int* variant, int* ty, int* zchunk, double* us);
-/* set a finest-level kernel's launch shape explicitly (ty: 2, 4 or 8 rows for variants 0, 1, 3; 2 or 4 for variant 2) */
+/* set a finest-level kernel's launch shape explicitly (ty: 2, 4 or 8 rows for variants 0, 1, 3, 4; 2 or 4 for
+ * variant 2; 4, 8 or 16 for variant 5) */
 int rt_set_tuning(rt_hier* h, int precision, int mode, int variant, int ty, int zchunk);
 /* time reps launches of one finest-level kernel at its current shape on random data
  * (device time per launch in microseconds, CUDA events on the context stream) */
@@ -369,13 +375,20 @@ int rt_unet_train_step(rt_unet* u, int batch, const void* in, const float* tgt, 
 double rt_unet_output_scale(rt_unet* u);
 int rt_unet_set_output_scale(rt_unet* u, double oscale);
 /* one (density, residual, MG-error) training sample from hierarchy h (node box = the network's):
- * a random load, k_iter plain MG-PCG iterations give the residual r; input = packed (log density,
- * r / rms(r), support flag), target = (K^-1 r - Vcycle(r)) / rms(r) / output unit */
+ * a random load, k_iter plain MG-PCG iterations give the residual r and zv = Vcycle(r); input =
+ * packed (log density, r / rms(r), support flag, zv / rms(zv)), target = (K^-1 r - zv) / rms(zv) /
+ * output unit */
 int rt_unet_harvest(rt_hier* h, rt_unet* u, int k_iter, uint64_t seed, void* in_out, float* tgt_out);
-/* use the network inside rt_pcg / rt_worst_case: z = Vcycle(r) + N(rho, r); the correction is
- * switched off for the rest of a solve once an iteration fails to reduce ||r|| below
- * fallback_ratio x its previous value (the plain V-cycle is the fallback).  u = null detaches. */
+/* use the network inside rt_pcg / rt_worst_case: z = Vcycle(r) + N(rho, r, Vcycle(r)) (no
+ * reference counterpart).  The correction is switched off once an iteration fails to reduce
+ * ||r|| below fallback_ratio x its previous value (the plain V-cycle is the fallback and the
+ * judge); that verdict holds for the following solves until rt_update_stencil or the next
+ * rt_hier_set_learned.  Inside the captured PCG loop the correction is the body of an IF node,
+ * so a switched-off network costs no launches.  u = null detaches. */
 int rt_hier_set_learned(rt_hier* h, rt_unet* u, double fallback_ratio);
+/* corrections run since rt_hier_set_learned, and whether the gate has switched the network off
+ * for the current design */
+int rt_hier_learned_stats(rt_hier* h, long long* applied, int* judged_off);
 
 #ifdef __cplusplus
 }

@@ -138,6 +138,7 @@ SIGNATURES = {
     "rt_unet_set_output_scale": (I, [P, D]),
     "rt_unet_harvest": (I, [P, P, I, C.c_uint64, P, P]),
     "rt_hier_set_learned": (I, [P, P, D]),
+    "rt_hier_learned_stats": (I, [P, C.POINTER(C.c_longlong), C.POINTER(I)]),
     "rt_sensitivity": (I, [P, I]),
     "rt_filter_sensitivity": (I, [P, F]),
     "rt_oc_update": (I, [P, F, C.POINTER(F), C.POINTER(I)]),

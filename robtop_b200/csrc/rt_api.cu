@@ -146,6 +146,7 @@ static void ctx_free(rt_ctx* c) {
     for (auto e : c->ev_pool) cudaEventDestroy(e);
     if (c->hscal) cudaFreeHost(c->hscal);
     if (c->own_stream) cudaStreamDestroy(c->stream);
+    if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
     delete c;
 }
 
@@ -516,6 +517,7 @@ static int build_hier(rt_ctx* c, const rt_params* p, int nx, int ny, int nz, uin
     RT_CUDA(c, cudaMemsetAsync(h->scal, 0, sizeof(double) * RT_NSCAL, c->stream));
     RT_CHECK(upload_KE(h));
     RT_CHECK(rtk::init_tile_kernels(c));
+    RT_CHECK(rtk::init_sf_kernels(c));
     RT_CHECK(rtk::init_stencil_kernels(c));
     *out = h;
     return RT_OK;
@@ -1017,6 +1019,7 @@ extern "C" int rt_update_stencil(rt_hier* h) {
     // spectral bound of D^-1 A per smoothed level, for the Chebyshev smoother
     for (int i = 0; i + 1 < nl; i++) RT_CHECK(estimate_lmax(h, i));
     h->stencil_ready = true;
+    h->unet_off = false;  // a new design: the learned correction gets judged again
     return RT_OK;
 }
 
@@ -1340,7 +1343,65 @@ extern "C" int rt_relative_residual(rt_hier* h, double* rel) {
 // of z) and returns with *dots_done set.
 // the FP32 right-hand side of the V-cycle comes out of the x / r update (scaled by the r.r
 // before that update, kept in scal[23]) instead of a separate conversion pass
-static bool fused_f32_rhs(const rt_hier* h) { return h->P.precision == RT_FP32 && !h->unet && !h->P.krylov_fp32; }
+static bool fused_f32_rhs(const rt_hier* h) { return h->P.precision == RT_FP32 && !h->P.krylov_fp32; }
+
+// gate of the learned correction: counts the corrections run (scal[36]) and, inside a captured
+// loop, sets the IF node that holds them
+__global__ void k_learned_gate(const double* __restrict__ gate, double* __restrict__ count,
+                               cudaGraphConditionalHandle hc, int use_cond) {
+    if (threadIdx.x != 0) return;
+    const bool on = gate[0] != 0.0;
+    if (on) count[0] += 1.0;
+    if (use_cond) cudaGraphSetConditional(hc, on ? 1u : 0u);
+}
+
+// runs fn's launches only while the gate scal[28] is on.  Inside a stream capture they become
+// the body of an IF conditional node (captured on the context's auxiliary stream), so a loop
+// whose gate went off launches none of them; outside a capture the gate is read on the host.
+template <typename F>
+static int learned_if(rt_hier* h, F&& fn) {
+    rt_ctx* c = h->ctx;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    RT_CUDA(c, cudaStreamIsCapturing(c->stream, &cs));
+    if (cs != cudaStreamCaptureStatusActive) {
+        RT_CHECK(rt_launch(c, "learned_gate", [&] { k_learned_gate<<<1, 32, 0, c->stream>>>(h->scal + 28, h->scal + 36, 0, 0); }));
+        double g = 0;
+        RT_CHECK(read_scalars(h, 28, 1, &g));
+        return g != 0.0 ? fn() : RT_OK;
+    }
+    if (!c->aux_stream) return rt_fail(c, RT_ESTATE, "learned correction captured without an auxiliary stream");
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    RT_CUDA(c, cudaStreamGetCaptureInfo(c->stream, &cs, nullptr, &cg, &deps, &nd));
+    cudaGraphConditionalHandle hc;
+    RT_CUDA(c, cudaGraphConditionalHandleCreate(&hc, cg, 0, cudaGraphCondAssignDefault));
+    RT_CHECK(rt_launch(c, "learned_gate", [&] { k_learned_gate<<<1, 32, 0, c->stream>>>(h->scal + 28, h->scal + 36, hc, 1); }));
+    RT_CUDA(c, cudaStreamGetCaptureInfo(c->stream, &cs, nullptr, &cg, &deps, &nd));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = hc;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t ifn;
+    RT_CUDA(c, cudaGraphAddNode(&ifn, cg, deps, nd, &cp));
+    RT_CUDA(c, cudaStreamUpdateCaptureDependencies(c->stream, &ifn, 1, cudaStreamSetCaptureDependencies));
+    RT_CUDA(c, cudaStreamBeginCaptureToGraph(c->aux_stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                             cudaStreamCaptureModeThreadLocal));
+    cudaStream_t saved = c->stream;
+    c->stream = c->aux_stream;
+    const long l0 = c->launches;
+    const int st = fn();
+    // the body's kernels are counted when they run (scal[36] corrections), not per iteration
+    h->unet_kernels = c->launches - l0;
+    c->launches = l0;
+    c->stream = saved;
+    cudaGraph_t body = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->aux_stream, &body);
+    RT_CHECK(st);
+    if (e != cudaSuccess) return rt_fail(c, RT_ECUDA, "capture of the learned correction failed: %s", cudaGetErrorString(e));
+    return RT_OK;
+}
 
 // z = M^-1 r.  rr_dev: the scale (r.r of the residual the FP32 copy was made from);
 // f32_ready: level 0's FP32 right-hand side already holds r / sqrt(rr_dev)
@@ -1353,12 +1414,12 @@ static int precondition(rt_hier* h, const double* r, double* z, const double* rr
         if (!f32_ready) RT_CHECK(rtk::d2f_scaled(h, n, r, L.f32, rr_dev));
         RT_CUDA(h->ctx, cudaMemsetAsync(L.u32, 0, sizeof(float) * n, h->ctx->stream));
         RT_CHECK(vcycle_T<float>(h, h->P.smoother, h->P.pre_sweeps, h->P.post_sweeps, h->P.jacobi_omega));
-        if (dots && !h->unet) {
+        if (dots) {
             RT_CHECK(rtk::f2d_scaled_dot2(h, n, L.u32, z, rr_dev, r, h->rold, dots));
             *dots_done = true;
-            return RT_OK;
+        } else {
+            RT_CHECK(rtk::f2d_scaled(h, n, L.u32, z, rr_dev));
         }
-        RT_CHECK(rtk::f2d_scaled(h, n, L.u32, z, rr_dev));
     } else if (h->P.precision == RT_FP64_FINE && h->L.size() > 1) {
         // FP64 smoothing and residual on the finest level (on r / z themselves), the coarse
         // V-cycle in FP32 on the restricted residual scaled by 1 / |r|, its correction added back
@@ -1398,8 +1459,15 @@ static int precondition(rt_hier* h, const double* r, double* z, const double* rr
         L.u = saved_u;
         RT_CHECK(s);
     }
-    // learned correction z += N(rho, r), switched off on the device by the gate in scal[28]
-    if (h->unet) RT_CHECK(rtu::correct(h->unet, h, r, rr_dev, h->scal + 28, z));
+    // learned correction z += N(rho, r, z), run only while the gate in scal[28] is on; the dots
+    // the widening of z already produced are recomputed for the corrected z
+    if (h->unet)
+        RT_CHECK(learned_if(h, [&]() -> int {
+            RT_CHECK(rtk::dot(h, n, r, r, h->scal + 38));
+            RT_CHECK(rtk::dot(h, n, z, z, h->scal + 37));
+            RT_CHECK(rtu::correct(h->unet, h, r, h->scal + 38, h->scal + 37, h->scal + 28, z));
+            return (dots_done && *dots_done) ? rtk::dot2(h, n, z, r, h->rold, dots) : RT_OK;
+        }));
     return RT_OK;
 }
 
@@ -1487,6 +1555,7 @@ static int pcg_graph_run(rt_hier* h, double* x, double* r, bool no_support) {
     if (!h->pcg_exec || h->pcg_key != key) {
         if (h->pcg_exec) { cudaGraphExecDestroy(h->pcg_exec); h->pcg_exec = nullptr; }
         if (h->pcg_graph) { cudaGraphDestroy(h->pcg_graph); h->pcg_graph = nullptr; }
+        if (h->unet && !c->aux_stream) RT_CUDA(c, cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking));
         cudaGraph_t g;
         RT_CUDA(c, cudaGraphCreate(&g, 0));
         cudaGraphConditionalHandle cond;
@@ -1751,10 +1820,14 @@ static int pcg_core(rt_hier* h, double* x, const double* b, double tol, int maxi
     if (rel > tol && maxit > 0) {
         // loop state on the device: scal[24] iteration count, scal[25] tol, scal[26] maxit,
         // scal[27..29] learned-correction fallback ratio, gate, previous r.r
-        double st[6] = {0.0, tol, (double)maxit, h->unet_fallback, h->unet ? 1.0 : 0.0, s[0]};
+        const bool learned_on = h->unet && !h->unet_off;
+        double st[6] = {0.0, tol, (double)maxit, h->unet_fallback, learned_on ? 1.0 : 0.0, s[0]};
         memcpy(h->ctx->hscal + 8, st, sizeof(st));
         RT_CUDA(h->ctx, cudaMemcpyAsync(h->scal + 24, h->ctx->hscal + 8, sizeof(st), cudaMemcpyHostToDevice,
                                         h->ctx->stream));
+        // scal[36]: learned corrections run in this solve
+        RT_CUDA(h->ctx, cudaMemsetAsync(h->scal + 36, 0, sizeof(double), h->ctx->stream));
+        if (h->unet) RT_CHECK(rtu::refresh(h->unet));
         // scal[90..93]: stall detection of the reduced-precision V-cycles (see k_pcg_tail)
         const bool fallback = h->P.precision != RT_FP64 && h->P.precision_fallback > 0;
         double sd[4] = {s[0], 0.0, 0.0, fallback ? (double)h->P.precision_fallback : 0.0};
@@ -1783,6 +1856,14 @@ static int pcg_core(rt_hier* h, double* x, const double* b, double tol, int maxi
         rel = std::sqrt(s3[0]) / bn;
         it = (int)s3[3];
         if (graphed) h->ctx->launches += h->pcg_iter_kernels * it;
+        if (h->unet) {
+            double lg[9];
+            RT_CHECK(read_scalars(h, 28, 9, lg));  // scal[28] gate at the end, scal[36] corrections run
+            const long long applied = (long long)lg[8];
+            h->unet_applied += applied;
+            if (graphed) h->ctx->launches += h->unet_kernels * applied;
+            if (learned_on && lg[0] == 0.0) h->unet_off = true;
+        }
         if (fallback && stall != 0.0 && rel > tol && it < maxit) {
             // continue from the current iterate with FP64 V-cycles (flexible CG restarts)
             const int saved = h->P.precision;
@@ -2258,6 +2339,8 @@ extern "C" int rt_autotune(rt_hier* h, int reps) {
         for (int zc : {8, 16, 32, 64}) cands.push_back(rt_tile_cfg{3, ty, zc});
     for (int ty : {2, 4, 8})
         for (int zc : {8, 16, 32, 64}) cands.push_back(rt_tile_cfg{4, ty, zc});  // FP32 only
+    for (int ty : {4, 8, 16})
+        for (int zc : {16, 32, 64}) cands.push_back(rt_tile_cfg{5, ty, zc});  // ty 16: FP32 only
     for (int prec = 0; prec < 2; prec++)
         for (int mode = 0; mode < 4; mode++) {
             rt_tile_cfg best_cfg = h->tune[prec][mode];
@@ -2265,6 +2348,7 @@ extern "C" int rt_autotune(rt_hier* h, int reps) {
             for (const rt_tile_cfg& cfg : cands) {
                 if (cfg.zchunk > 2 * L.vz && cfg.zchunk != 4) continue;
                 if (cfg.variant == 4 && prec == 1) continue;
+                if (cfg.variant == 5 && cfg.ty == 16 && prec == 1) continue;
                 h->tune[prec][mode] = cfg;
                 const double t = time_fine_kernel(h, prec, mode, reps);
                 if (t < best) { best = t; best_cfg = cfg; }
@@ -2291,11 +2375,15 @@ extern "C" int rt_tuning_info(rt_hier* h, int precision, int mode, int* variant,
 }
 
 extern "C" int rt_set_tuning(rt_hier* h, int precision, int mode, int variant, int ty, int zchunk) {
-    if (!h || precision < 0 || precision > 1 || mode < 0 || mode > 3 || variant < 0 || variant > 4 || zchunk < 1)
+    if (!h || precision < 0 || precision > 1 || mode < 0 || mode > 3 || variant < 0 || variant > 5 || zchunk < 1)
         return RT_EINVAL;
     RT_NOT_WORKSPACE(h);
     if (variant == 4 && precision == RT_FP64) return rt_fail(h->ctx, RT_EINVAL, "variant 4 (packed FP32 pairs) is FP32 only");
-    if (variant != 2 && ty != 2 && ty != 4 && ty != 8) return rt_fail(h->ctx, RT_EINVAL, "rows per tile must be 2, 4 or 8");
+    if (variant == 5) {
+        if (ty != 4 && ty != 8 && ty != 16) return rt_fail(h->ctx, RT_EINVAL, "sum-factorised rows per tile must be 4, 8 or 16");
+    } else if (variant != 2 && ty != 2 && ty != 4 && ty != 8) {
+        return rt_fail(h->ctx, RT_EINVAL, "rows per tile must be 2, 4 or 8");
+    }
     const int pr = precision == RT_FP64 ? 1 : 0;
     if (variant == 2 && ty != 2 && ty != 4) return rt_fail(h->ctx, RT_EINVAL, "prefetching rows per tile must be 2 or 4");
     h->tune[pr][mode] = rt_tile_cfg{variant, ty, zchunk};
@@ -3035,7 +3123,16 @@ extern "C" int rt_hier_set_learned(rt_hier* h, rt_unet* u, double fallback_ratio
     if (u && !(fallback_ratio > 0)) return rt_fail(h->ctx, RT_EINVAL, "fallback ratio must be positive");
     h->unet = u;
     h->unet_fallback = fallback_ratio;
+    h->unet_off = false;
+    h->unet_applied = 0;
     h->graph_epoch++;
+    return RT_OK;
+}
+
+extern "C" int rt_hier_learned_stats(rt_hier* h, long long* applied, int* judged_off) {
+    if (!h) return RT_EINVAL;
+    if (applied) *applied = h->unet_applied;
+    if (judged_off) *judged_off = h->unet_off ? 1 : 0;
     return RT_OK;
 }
 
@@ -3048,8 +3145,8 @@ __global__ void k_zero_fixed(long n, long nv, const uint8_t* __restrict__ vact, 
 }
 
 // one training sample from the solver: a random load on the free nodes, k PCG iterations
-// (plain V-cycle) from zero give the residual r; the input packs (density, r), the target is
-// the V-cycle's error on r: K^-1 r (PCG to 1e-10) minus one V-cycle applied to r
+// (plain V-cycle) from zero give the residual r; the input packs (density, r, zv = one V-cycle
+// applied to r), the target is the V-cycle's error on r: K^-1 r (PCG to 1e-10) minus zv
 extern "C" int rt_unet_harvest(rt_hier* h, rt_unet* u, int k_iter, uint64_t seed, void* in_out, float* tgt_out) {
     if (!h || !u || !in_out || !tgt_out || k_iter < 0) return RT_EINVAL;
     RT_NOT_WORKSPACE(h);
@@ -3085,17 +3182,18 @@ extern "C" int rt_unet_harvest(rt_hier* h, rt_unet* u, int k_iter, uint64_t seed
     // r_k becomes the right-hand side; r.r in scal[35]
     if (s == RT_OK) cudaMemcpyAsync(L.f, h->rr, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream);
     if (s == RT_OK) step(rtk::dot(h, n, L.f, L.f, h->scal + 35));
-    if (s == RT_OK) step(rtu::pack(u, h, L.f, h->scal + 35));
+    if (s == RT_OK) step(precondition(h, L.f, zv, h->scal + 35));
+    if (s == RT_OK) step(rtk::dot(h, n, zv, zv, h->scal + 37));
+    if (s == RT_OK) step(rtu::pack(u, h, L.f, h->scal + 35, zv, h->scal + 37));
     if (s == RT_OK)
         cudaMemcpyAsync(in_out, rtu::input(u), sizeof(__nv_bfloat16) * 16 * rtu::voxels(u), cudaMemcpyDeviceToDevice,
                         c->stream);
-    if (s == RT_OK) step(precondition(h, L.f, zv, h->scal + 35));
     rt_solve_info si;
     memset(&si, 0, sizeof(si));
     int vc = 0;
     if (s == RT_OK) cudaMemsetAsync(L.u, 0, sizeof(double) * n, c->stream);
     if (s == RT_OK) step(pcg_core(h, L.u, L.f, 1e-10, 2000, &si, &vc));
-    if (s == RT_OK) step(rtu::target(u, h, L.u, zv, h->scal + 35, tgt_out));
+    if (s == RT_OK) step(rtu::target(u, h, L.u, zv, h->scal + 37, tgt_out));
     cudaFreeAsync(zv, c->stream);
     const cudaError_t e = cudaStreamSynchronize(c->stream);
     h->unet = saved;

@@ -806,11 +806,12 @@ int launch_pair_ty(rt_hier* h, const float* u, const float* f, float* out, doubl
 }
 
 // variant 0: two barriers per element layer; 3: software-pipelined, one barrier per layer;
-// 4 (FP32): pipelined with element pairs in packed FP32
+// 4 (FP32): pipelined with element pairs in packed FP32; 5: sum-factorised row marching (rt_fine_sf.cu)
 template <typename T, bool WS, int MODE>
 int launch_tile(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name, T* dvec = nullptr,
                 const double* coef = nullptr, int kstep = 0) {
     const rt_tile_cfg& tn = h->tune[sizeof(T) == 8 ? 1 : 0][MODE];
+    if (tn.variant == 5) return rtk::launch_sf<T, WS, MODE>(h, u, f, out, omega, name, dvec, coef, kstep);
     if constexpr (sizeof(T) == 4) {
         if (tn.variant == 4) {
             switch (tn.ty) {

@@ -41,6 +41,9 @@ struct rt_ctx {
     std::vector<Pending> pending;
     // host-pinned scalar mailbox
     double* hscal = nullptr;
+    // second stream, only ever used as a capture target: the body of a conditional node is
+    // captured on it while the context stream's own capture is still open
+    cudaStream_t aux_stream = nullptr;
     // instantiated batched-PCG graphs (rt_pcg_batch), newest last
     struct BatchGraph {
         uint64_t key = 0;
@@ -77,6 +80,7 @@ struct rt_level {
 // launch shape of a finest-level operator kernel (chosen by rt_autotune)
 struct rt_tile_cfg {
     int variant = 1;  // 0: shared-memory element tile (rt_fine_tile.cu), 1: register marching (rt_fine_march.cu),
+                      // 5: sum-factorised row marching (rt_fine_sf.cu; ty = node rows 4, 8 or 16),
                       // 2: register marching with the output-stage loads issued ahead
     int ty = 4;       // node rows per warp tile (marching kernel: 2, 4 or 8)
     int zchunk = 16;  // node layers per tile
@@ -152,6 +156,13 @@ struct rt_hier {
     // fallback ratio, scal[28] the gate (1 while active), scal[29] the previous iteration's r.r
     struct rt_unet* unet = nullptr;
     double unet_fallback = 1.0;
+    // the gate's verdict carries over from solve to solve: once an iteration with the network
+    // failed the ratio, the correction stays off until the design (rt_update_stencil) or the
+    // network changes.  unet_kernels: kernels of one correction (launch accounting of the IF node
+    // that runs it inside the captured loop); unet_applied: corrections run since attach
+    bool unet_off = false;
+    long unet_kernels = 0;
+    long long unet_applied = 0;
     long long fallbacks = 0;  // PCG solves that continued with FP64 V-cycles after stalling
 };
 
@@ -246,6 +257,10 @@ int st_cheby_fused(rt_hier* h, int lvl, float* u, const float* f, float* tmp, fl
 bool st_cheby_fused_ok(rt_hier* h);
 int penalty_weights(rt_hier* h);
 int init_tile_kernels(rt_ctx* c);
+int init_sf_kernels(rt_ctx* c);
+template <typename T, bool WS, int MODE>
+int launch_sf(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name, T* dvec, const double* coef,
+              int kstep);
 int init_stencil_kernels(rt_ctx* c);
 int fine_dinv(rt_hier* h);
 template <typename T, int MODE>

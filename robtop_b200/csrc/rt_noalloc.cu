@@ -18,7 +18,15 @@
 //    streams, or from several host threads without ordering) race;
 //  * the device address of the array is looked up once per device, on the
 //    first call made while that device is current.  That first call should be
-//    made before any stream capture begins.
+//    made before any stream capture begins.  The address belongs to the
+//    device's context, so it is cached together with that context's unique id
+//    (cuCtxGetId): after cudaDeviceReset the next call sees a new context id
+//    and looks the address up again instead of launching with a stale one;
+//  * errors left pending by earlier, unrelated work of the caller are not
+//    consumed: the launches are checked with cudaPeekAtLastError before and
+//    after, so a sticky error that was already there is reported as RT_ECUDA
+//    without being cleared.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -38,6 +46,34 @@ static __device__ __align__(256) double g_noalloc_partials[NA_MAX_PARTIALS];
 
 std::mutex g_setup_mutex;
 double* g_partials_addr[NA_MAX_DEVICES] = {nullptr};
+unsigned long long g_partials_ctx[NA_MAX_DEVICES] = {0};  // context id the cached address belongs to
+
+// unique id of the calling thread's current context (0 if none or unknown), through the
+// driver entry points the runtime exposes, so the library needs no link against libcuda
+unsigned long long current_context_id() {
+    using get_current_t = CUresult (*)(CUcontext*);
+    using get_id_t = CUresult (*)(CUcontext, unsigned long long*);
+    static get_current_t get_current = nullptr;
+    static get_id_t get_id = nullptr;
+    static bool resolved = false;
+    if (!resolved) {  // called with g_setup_mutex held
+        void* a = nullptr;
+        void* b = nullptr;
+        cudaDriverEntryPointQueryResult qa, qb;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) == cudaSuccess &&
+            qa == cudaDriverEntryPointSuccess && a)
+            get_current = (get_current_t)a;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) == cudaSuccess &&
+            qb == cudaDriverEntryPointSuccess && b)
+            get_id = (get_id_t)b;
+        resolved = true;
+    }
+    if (!get_current || !get_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 
 // block b sums a[i] * b[i] over its fixed chunk [b*CHUNK, (b+1)*CHUNK): the
 // summation order depends only on n, so repeated calls give identical results
@@ -94,20 +130,26 @@ extern "C" int rt_compliance_noalloc(const double* f_dev, const double* u_dev, l
     double* partials = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_setup_mutex);
-        if (g_partials_addr[dev] == nullptr) {
+        const unsigned long long id = current_context_id();
+        if (g_partials_addr[dev] == nullptr || id == 0 || id != g_partials_ctx[dev]) {
             void* p = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
             if (e != cudaSuccess) {
                 fprintf(stderr, "rt_compliance_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+                g_partials_addr[dev] = nullptr;
                 return RT_ECUDA;
             }
             g_partials_addr[dev] = (double*)p;
+            // the lookup made the device's context current if it was not yet
+            g_partials_ctx[dev] = id ? id : current_context_id();
         }
         partials = g_partials_addr[dev];
     }
+    // an error the caller left pending is theirs: report it, leave it in place, launch nothing
+    if (cudaPeekAtLastError() != cudaSuccess) return RT_ECUDA;
     cudaStream_t s = (cudaStream_t)cuda_stream;
     const int np = (int)((n + NA_CHUNK - 1) / NA_CHUNK);
     if (np > 0) k_dot_chunks<<<np, NA_THREADS, 0, s>>>(n, f_dev, u_dev, partials);
     k_sum_partials<<<1, NA_THREADS, 0, s>>>(np, partials, out_dev);
-    return cudaGetLastError() == cudaSuccess ? RT_OK : RT_ECUDA;
+    return cudaPeekAtLastError() == cudaSuccess ? RT_OK : RT_ECUDA;
 }

@@ -60,7 +60,8 @@ extern "C" int rt_unet_set_conv_variant(int variant) {
 // ---------------------------------------------------------------------------
 // the U-Net: 4 levels, 16/32/48/64 channels, two 3x3x3 convolutions (+ReLU) per level and
 // side, 2x2x2 average pooling, nearest upsampling with skip concatenation, 1x1x1 head
-// to 3 channels.  Input: 16 channels (log density, 3 scaled residual components, zeros).
+// to 3 channels.  Input: 16 channels (log density, 3 scaled residual components, the
+// support flag, 3 scaled components of the V-cycle's output for that residual, zeros).
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -519,10 +520,12 @@ namespace {
 // input channels: 0 log10 density feature mapped to [0, 1], 1-3 r * s, 4 support flag, rest 0
 __global__ void k_unet_pack(int nx, int ny, int nz, const uint8_t* __restrict__ vact, const uint8_t* __restrict__ vfix,
                             int ws, const float* __restrict__ w, const double* __restrict__ r,
-                            const double* __restrict__ rr, double nact, __nv_bfloat16* __restrict__ in) {
+                            const double* __restrict__ rr, const double* __restrict__ zv,
+                            const double* __restrict__ zz, double nact, __nv_bfloat16* __restrict__ in) {
     const int vx = nx + 1, vy = ny + 1;
     const long nv = (long)vx * vy * (nz + 1);
     const double s = sqrt(nact / fmax(rr[0], 1e-300));
+    const double sz = sqrt(nact / fmax(zz[0], 1e-300));
     for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < nv; v += (long)gridDim.x * blockDim.x) {
         const int x = (int)(v % vx), y = (int)((v / vx) % vy), z = (int)(v / ((long)vx * vy));
         float feat[16];
@@ -543,6 +546,9 @@ __global__ void k_unet_pack(int nx, int ny, int nz, const uint8_t* __restrict__ 
             feat[2] = (float)(r[nv + v] * s);
             feat[3] = (float)(r[2 * nv + v] * s);
             feat[4] = (ws && vfix[v]) ? 1.f : 0.f;
+            feat[5] = (float)(zv[v] * sz);
+            feat[6] = (float)(zv[nv + v] * sz);
+            feat[7] = (float)(zv[2 * nv + v] * sz);
         }
         uint4* o = reinterpret_cast<uint4*>(in + v * 16);
         __align__(16) __nv_bfloat162 pk[8];
@@ -553,14 +559,14 @@ __global__ void k_unet_pack(int nx, int ny, int nz, const uint8_t* __restrict__ 
     }
 }
 
-// z += gate * (oscale / s) * out on active, non-fixed nodes
+// z += gate * (oscale / sz) * out on active, non-fixed nodes (sz: the inverse rms of the V-cycle's z)
 __global__ void k_unet_correct(long nv, const uint8_t* __restrict__ vact, const uint8_t* __restrict__ vfix, int ws,
-                               const float* __restrict__ out, const double* __restrict__ rr, double nact,
+                               const float* __restrict__ out, const double* __restrict__ zz, double nact,
                                double oscale, const double* __restrict__ gate, double* __restrict__ z) {
     const double g = gate ? gate[0] : 1.0;
     if (g == 0.0) return;
-    const double s = sqrt(nact / fmax(rr[0], 1e-300));
-    const double f = g * oscale / s;
+    const double sz = sqrt(nact / fmax(zz[0], 1e-300));
+    const double f = g * oscale / sz;
     for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < nv; v += (long)gridDim.x * blockDim.x) {
         if (!vact[v] || (ws && vfix[v])) continue;
         z[v] += f * out[3 * v];
@@ -569,17 +575,17 @@ __global__ void k_unet_correct(long nv, const uint8_t* __restrict__ vact, const 
     }
 }
 
-// scaled target t = (e - zv) s on active non-fixed nodes: [V][3] float and its sum of squares
+// scaled target t = (e - zv) sz on active non-fixed nodes: [V][3] float and its sum of squares
 __global__ void k_unet_target(long nv, const uint8_t* __restrict__ vact, const uint8_t* __restrict__ vfix, int ws,
-                              const double* __restrict__ e, const double* __restrict__ zv, const double* __restrict__ rr,
+                              const double* __restrict__ e, const double* __restrict__ zv, const double* __restrict__ zz,
                               double nact, float* __restrict__ tgt, double* __restrict__ ss) {
     __shared__ double sh[256];
-    const double s = sqrt(nact / fmax(rr[0], 1e-300));
+    const double sz = sqrt(nact / fmax(zz[0], 1e-300));
     double acc = 0;
     for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < nv; v += (long)gridDim.x * blockDim.x) {
         const bool on = vact[v] && !(ws && vfix[v]);
         for (int c = 0; c < 3; c++) {
-            const double t = on ? (e[c * nv + v] - zv[c * nv + v]) * s : 0.0;
+            const double t = on ? (e[c * nv + v] - zv[c * nv + v]) * sz : 0.0;
             tgt[3 * v + c] = (float)t;
             acc += t * t;
         }
@@ -607,39 +613,42 @@ bool box_matches(const rt_unet* u, const rt_hier* h) {
     return u->X[0] == L.vx && u->Y[0] == L.vy && u->Z[0] == L.vz;
 }
 
-int pack(rt_unet* u, rt_hier* h, const double* r, const double* rr_dev) {
+int pack(rt_unet* u, rt_hier* h, const double* r, const double* rr_dev, const double* zv, const double* zz_dev) {
     rt_ctx* c = h->ctx;
     const rt_level& L = h->L[0];
     const int ws = h->has_support ? 1 : 0;
     return rt_launch(c, "unet_pack", [&] {
         k_unet_pack<<<ew_blocks(c, L.nv), 256, 0, c->stream>>>(L.nx, L.ny, L.nz, L.vact, h->vfix, ws, h->w, r, rr_dev,
-                                                               (double)L.n_act_nodes, u->in0);
+                                                               zv, zz_dev, (double)L.n_act_nodes, u->in0);
     });
 }
 
-// z += N(rho, r) correction (forward pass on the packed input), scaled back to solver units
-int correct(rt_unet* u, rt_hier* h, const double* r, const double* rr_dev, const double* gate, double* z) {
+int refresh(rt_unet* u) { return unet_refresh_w16(u); }
+
+// z += N(rho, r, z) correction (forward pass on the packed input), scaled back to solver units
+int correct(rt_unet* u, rt_hier* h, const double* r, const double* rr_dev, const double* zz_dev, const double* gate,
+            double* z) {
     rt_ctx* c = h->ctx;
     const rt_level& L = h->L[0];
-    RT_CHECK(pack(u, h, r, rr_dev));
+    RT_CHECK(pack(u, h, r, rr_dev, z, zz_dev));
     RT_CHECK(unet_forward(u));
     const int ws = h->has_support ? 1 : 0;
     const double osc = u->oscale > 0 ? u->oscale : 1.0;
     return rt_launch(c, "unet_correct", [&] {
-        k_unet_correct<<<ew_blocks(c, L.nv), 256, 0, c->stream>>>(L.nv, L.vact, h->vfix, ws, u->out, rr_dev,
+        k_unet_correct<<<ew_blocks(c, L.nv), 256, 0, c->stream>>>(L.nv, L.vact, h->vfix, ws, u->out, zz_dev,
                                                                   (double)L.n_act_nodes, osc, gate, z);
     });
 }
 
-// training target from the exact error e and the V-cycle's zv (both for residual r with r.r in rr_dev);
-// the first call fixes the output unit oscale to the target rms
-int target(rt_unet* u, rt_hier* h, const double* e, const double* zv, const double* rr_dev, float* tgt) {
+// training target from the exact error e and the V-cycle's zv (zv.zv in zz_dev); the first
+// call fixes the output unit oscale to the target rms
+int target(rt_unet* u, rt_hier* h, const double* e, const double* zv, const double* zz_dev, float* tgt) {
     rt_ctx* c = h->ctx;
     const rt_level& L = h->L[0];
     const int ws = h->has_support ? 1 : 0;
     RT_CUDA(c, cudaMemsetAsync(u->dscal, 0, sizeof(double), c->stream));
     RT_CHECK(rt_launch(c, "unet_target", [&] {
-        k_unet_target<<<ew_blocks(c, L.nv), 256, 0, c->stream>>>(L.nv, L.vact, h->vfix, ws, e, zv, rr_dev,
+        k_unet_target<<<ew_blocks(c, L.nv), 256, 0, c->stream>>>(L.nv, L.vact, h->vfix, ws, e, zv, zz_dev,
                                                                  (double)L.n_act_nodes, tgt, u->dscal);
     }));
     if (u->oscale <= 0) {

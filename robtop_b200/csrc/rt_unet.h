@@ -57,9 +57,16 @@ __global__ void k_mse(const float* out, const float* tgt, long n, float* gout, d
 struct rt_unet;
 namespace rtu {
 bool box_matches(const rt_unet* u, const rt_hier* h);
-int pack(rt_unet* u, rt_hier* h, const double* r, const double* rr_dev);
-int correct(rt_unet* u, rt_hier* h, const double* r, const double* rr_dev, const double* gate, double* z);
-int target(rt_unet* u, rt_hier* h, const double* e, const double* zv, const double* rr_dev, float* tgt);
+// input channels: 0 log density, 1-3 r / rms(r), 4 support flag, 5-7 zv / rms(zv) (zv = the
+// V-cycle's output for r); rr_dev = r.r, zz_dev = zv.zv
+int pack(rt_unet* u, rt_hier* h, const double* r, const double* rr_dev, const double* zv, const double* zz_dev);
+// z += gate * rms(z) * oscale * N(rho, r, z): z holds the V-cycle's output on entry
+int correct(rt_unet* u, rt_hier* h, const double* r, const double* rr_dev, const double* zz_dev, const double* gate,
+            double* z);
+// target (e - zv) / (rms(zv) oscale) from the exact error e and the V-cycle's zv
+int target(rt_unet* u, rt_hier* h, const double* e, const double* zv, const double* zz_dev, float* tgt);
+// convert the FP32 parameters to the BF16 copies the convolutions read, if they changed
+int refresh(rt_unet* u);
 const void* input(const rt_unet* u);
 long voxels(const rt_unet* u);
 }  // namespace rtu

@@ -107,9 +107,43 @@ def harvest(G, net, k_iter, seed):
 
 
 def attach(G, net, fallback_ratio=1.0):
-    """Use the network inside G's PCG (z = Vcycle(r) + N(rho, r)); net=None detaches."""
+    """Use the network inside G's PCG (z = Vcycle(r) + N(rho, r, Vcycle(r))); net=None detaches.
+    An iteration whose residual norm does not drop below ``fallback_ratio`` x the previous one
+    switches the correction off until the next stencil update."""
     check(A.lib().rt_hier_set_learned(G.handle, net.handle if net is not None else None, float(fallback_ratio)),
           G.ctx.handle)
+
+
+def stats(G):
+    """(corrections run since attach, whether the gate has switched the network off for this design)"""
+    n = C.c_longlong()
+    off = C.c_int()
+    check(A.lib().rt_hier_learned_stats(G.handle, C.byref(n), C.byref(off)), G.ctx.handle)
+    return int(n.value), bool(off.value)
+
+
+def forward_seconds(net, reps=3):
+    """Device time of one network application on the context stream (the forward pass on the
+    network's own input buffer; each call synchronises the stream)."""
+    import time
+
+    check(A.lib().rt_unet_forward(net.handle, None, None), net.ctx.handle)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        check(A.lib().rt_unet_forward(net.handle, None, None), net.ctx.handle)
+    return (time.perf_counter() - t0) / reps
+
+
+def cost_aware_ratio(plain_iterations, plain_rel_residual, plain_seconds, net_seconds):
+    """Fallback ratio under which a learned iteration pays for itself.  The plain V-cycle PCG
+    reduced the residual by q = rel_res^(1/its) per iteration in plain_seconds / its each; an
+    iteration with the network costs c = (that + net_seconds) / that as much, so it must reduce
+    the residual by q^c to reach the tolerance no later."""
+    its = max(int(plain_iterations), 1)
+    q = float(plain_rel_residual) ** (1.0 / its)
+    t_it = float(plain_seconds) / its
+    c = (t_it + float(net_seconds)) / t_it
+    return q ** c
 
 
 def train(net, samples, steps, batch=4, lr=1e-3, seed=0):
