@@ -1,0 +1,102 @@
+"""The reference's own code, compiled from its sources (test infrastructure only).
+
+``make -C oracle ref`` builds, from the reference tree (default /root/reference, present only
+where the reference is mounted), two libraries into oracle/_ref/:
+
+* libref_ke.so: element/templateMatrix.cpp:31-124 (initTemplateMatrix) on the host;
+* libref_kernels.so: applyK_OTFA_kernel (grid/Grid.cu:2439-2517), computeSensitivity_kernel and
+  trySensMultiplier_kernel (optimization/optimization.cu:44-162) and filterSensitivity_kernel
+  (grid/Grid.cu:2323-2409) for sm_100a, driven on dense element boxes (needs a GPU to run).
+
+The built files travel with the repository to GPU machines; the sources do not.  Nothing on the
+product path loads these libraries: the tests use them to pin the oracle and the CUDA path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(_HERE, "_ref")
+KE_LIB = os.path.join(REF_DIR, "libref_ke.so")
+KERNELS_LIB = os.path.join(REF_DIR, "libref_kernels.so")
+REFERENCE_TREE = os.environ.get("ROBTOP_REFERENCE", "/root/reference")
+
+
+def build() -> bool:
+    """Build oracle/_ref/ when the reference tree is present; True if both libraries exist."""
+    if os.path.isdir(REFERENCE_TREE):
+        subprocess.check_call(["make", "-s", "-C", _HERE, "ref", f"REF={REFERENCE_TREE}"])
+    return os.path.exists(KE_LIB) and os.path.exists(KERNELS_LIB)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def template_matrix(h=1.0, E=1.0, nu=0.3):
+    """KE (24x24) from the reference's initTemplateMatrix."""
+    L = C.CDLL(KE_LIB)
+    L.ref_template_matrix.argtypes = [C.c_double, C.c_double, C.c_double, C.c_void_p]
+    out = np.zeros(576)
+    L.ref_template_matrix(h, E, nu, _p(out))
+    return out.reshape(24, 24)
+
+
+class Kernels:
+    """The reference's CUDA kernels on a dense element box (arrays in the library's dense layout:
+    elements x fastest over (nz, ny, nx), node vectors [3][(nx+1)(ny+1)(nz+1)])."""
+
+    def __init__(self):
+        L = C.CDLL(KERNELS_LIB)
+        P, I, F = C.c_void_p, C.c_int, C.c_float
+        L.ref_apply_k.argtypes = [I, I, I, P, P, P, F, P, P, P]
+        L.ref_sensitivity.argtypes = [I, I, I, P, P, F, P, P, P]
+        L.ref_oc_try.argtypes = [I, I, I, P, P, P, P, F, F, F, F, P]
+        L.ref_filter.argtypes = [I, I, I, P, F, P, P]
+        self.L = L
+
+    @staticmethod
+    def _box(eact):
+        e = np.ascontiguousarray(eact, np.uint8)
+        nz, ny, nx = e.shape
+        return e, nx, ny, nz
+
+    def apply_k(self, eact, vfix, rho, p, KE, u):
+        e, nx, ny, nz = self._box(eact)
+        nv = (nx + 1) * (ny + 1) * (nz + 1)
+        f = np.zeros(3 * nv)
+        vf = None if vfix is None else np.ascontiguousarray(vfix, np.uint8).ravel()
+        st = self.L.ref_apply_k(nx, ny, nz, _p(e), _p(vf), _p(np.ascontiguousarray(rho, np.float32).ravel()), p,
+                                _p(np.ascontiguousarray(KE, np.float64).ravel()),
+                                _p(np.ascontiguousarray(u, np.float64)), _p(f))
+        assert st == 0
+        return f
+
+    def sensitivity(self, eact, rho, p, KE, u):
+        e, nx, ny, nz = self._box(eact)
+        s = np.zeros(nx * ny * nz, np.float32)
+        st = self.L.ref_sensitivity(nx, ny, nz, _p(e), _p(np.ascontiguousarray(rho, np.float32).ravel()), p,
+                                    _p(np.ascontiguousarray(KE, np.float64).ravel()),
+                                    _p(np.ascontiguousarray(u, np.float64)), _p(s))
+        assert st == 0
+        return s
+
+    def oc_try(self, eact, eshell, rho, sens, thres, step, damp, rhomin):
+        e, nx, ny, nz = self._box(eact)
+        out = np.zeros(nx * ny * nz, np.float32)
+        sh = None if eshell is None else np.ascontiguousarray(eshell, np.uint8).ravel()
+        st = self.L.ref_oc_try(nx, ny, nz, _p(e), _p(sh), _p(np.ascontiguousarray(rho, np.float32).ravel()),
+                               _p(np.ascontiguousarray(sens, np.float32).ravel()), thres, step, damp, rhomin, _p(out))
+        assert st == 0
+        return out
+
+    def filter(self, eact, radius, sens):
+        e, nx, ny, nz = self._box(eact)
+        out = np.zeros(nx * ny * nz, np.float32)
+        st = self.L.ref_filter(nx, ny, nz, _p(e), radius, _p(np.ascontiguousarray(sens, np.float32).ravel()), _p(out))
+        assert st == 0
+        return out

@@ -1,0 +1,55 @@
+"""Writes the fixtures that pin the oracle to the reference's own code:
+
+* ref_template_matrix.npz: KE from the reference's initTemplateMatrix
+  (element/templateMatrix.cpp:31-124, built into oracle/_ref/libref_ke.so by `make -C oracle ref`)
+  for three (h, E, nu);
+* ref_kernels.npz (only with --kernels, on a machine with a GPU): the outputs of the reference's
+  applyK_OTFA_kernel, computeSensitivity_kernel, trySensMultiplier_kernel and
+  filterSensitivity_kernel (oracle/_ref/libref_kernels.so) on the seeded inputs of
+  tests/golden/ref_inputs.py.
+
+Run from the repository root:  python tests/golden/make_ref_fixtures.py [--kernels] [--out DIR]
+"""
+import argparse
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, HERE)
+
+from oracle import reference  # noqa: E402
+from ref_inputs import CASES, FILTER_RADIUS, OC, P, inputs  # noqa: E402
+
+KE_PARAMS = [(1.0, 1e6, 0.4), (1.0, 1.0, 0.3), (0.5, 2e5, 0.25)]
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--kernels", action="store_true")
+    ap.add_argument("--out", default=HERE)
+    a = ap.parse_args()
+    os.makedirs(a.out, exist_ok=True)
+    if os.path.exists(reference.KE_LIB):
+        kes = np.stack([reference.template_matrix(h, E, nu) for h, E, nu in KE_PARAMS])
+        np.savez_compressed(os.path.join(a.out, "ref_template_matrix.npz"), params=np.array(KE_PARAMS), ke=kes)
+        print("template matrices written")
+    if a.kernels:
+        K = reference.Kernels()
+        out = {}
+        for name in CASES:
+            cfg, KE, u, sens, eshell, ws = inputs(name)
+            out[f"{name}/applyK"] = K.apply_k(cfg["eact"], cfg["vfix"] if ws else None, cfg["rho"], P, KE, u)
+            out[f"{name}/sensitivity"] = K.sensitivity(cfg["eact"], cfg["rho"], P, KE, u)
+            out[f"{name}/oc_try"] = K.oc_try(cfg["eact"], eshell, cfg["rho"], sens, OC["thres"], OC["step"],
+                                             OC["damp"], OC["rhomin"])
+            out[f"{name}/filter"] = K.filter(cfg["eact"], FILTER_RADIUS, sens)
+        np.savez_compressed(os.path.join(a.out, "ref_kernels.npz"), **out)
+        print("reference kernel outputs written:", sorted(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,71 @@
+"""The oracle pinned to the reference's own code (CPU part).
+
+* KE: the oracle's or_template_matrix against the reference's initTemplateMatrix
+  (element/templateMatrix.cpp:31-124), compiled from the reference sources into
+  oracle/_ref/libref_ke.so where the reference is present, and against the fixture
+  tests/golden/ref_template_matrix.npz that build wrote (tests/golden/make_ref_fixtures.py).
+* The oracle's applyK, sensitivity, OC trial and filter against the outputs of the reference's
+  own CUDA kernels (grid/Grid.cu:2439-2517, 2323-2409; optimization/optimization.cu:44-162) on
+  seeded inputs, stored in tests/golden/ref_kernels.npz by the same script on a GPU machine.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import oracle as O
+from oracle import reference
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+from ref_inputs import CASES, FILTER_RADIUS, OC, P, inputs  # noqa: E402
+
+KE_FIXTURE = os.path.join(HERE, "golden", "ref_template_matrix.npz")
+KERNEL_FIXTURE = os.path.join(HERE, "golden", "ref_kernels.npz")
+
+
+def test_template_matrix_matches_reference_fixture():
+    g = np.load(KE_FIXTURE)
+    for (h, E, nu), ke in zip(g["params"], g["ke"]):
+        assert np.array_equal(O.template_matrix(E, nu, h), ke), (h, E, nu)
+
+
+@pytest.mark.skipif(not os.path.exists(reference.KE_LIB), reason="oracle/_ref/libref_ke.so not built")
+def test_template_matrix_matches_reference_build():
+    for h, E, nu in [(1.0, 1e6, 0.4), (2.0, 3.0, 0.1), (0.25, 7e4, 0.45)]:
+        assert np.array_equal(O.template_matrix(E, nu, h), reference.template_matrix(h, E, nu)), (h, E, nu)
+
+
+def _oracle_outputs(name):
+    cfg, KE, u, sens, eshell, ws = inputs(name)
+    H = O.Hierarchy(cfg["eact"], cfg["rho"], cfg["vfix"] if ws else None, p=P, E=1e6, nu=0.4, no_support=not ws)
+    nz, ny, nx = cfg["eact"].shape
+    eact = np.ascontiguousarray(cfg["eact"].ravel(), np.uint8)
+    rho = np.ascontiguousarray(cfg["rho"].ravel(), np.float32)
+    s = np.zeros(rho.size, np.float32)
+    O.lib().or_sensitivity(nx, ny, nz, O.ptr(eact), O.ptr(rho), P, O.ptr(KE), O.ptr(u), O.ptr(s))
+    oc = np.zeros_like(rho)
+    O.lib().or_oc_try(rho.size, O.ptr(eact), O.ptr(eshell), O.ptr(rho), O.ptr(sens), OC["thres"], OC["step"],
+                      OC["damp"], OC["rhomin"], O.ptr(oc))
+    flt = np.zeros_like(rho)
+    O.lib().or_filter(nx, ny, nz, O.ptr(eact), FILTER_RADIUS, O.ptr(sens), O.ptr(flt))
+    return {"applyK": H.applyK(u), "sensitivity": s, "oc_try": oc, "filter": flt}, eact
+
+
+@pytest.mark.skipif(not os.path.exists(KERNEL_FIXTURE), reason="tests/golden/ref_kernels.npz not generated")
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_oracle_matches_reference_kernel_outputs(name):
+    g = np.load(KERNEL_FIXTURE)
+    mine, eact = _oracle_outputs(name)
+    ref = {k: g[f"{name}/{k}"] for k in ("applyK", "sensitivity", "oc_try", "filter")}
+    # K u: the same FP64 sums in another order
+    assert np.abs(mine["applyK"] - ref["applyK"]).max() <= 1e-12 * np.abs(ref["applyK"]).max()
+    # sensitivities: the reference adds FP32 partial sums with atomicAdd (order varies), the oracle
+    # sums in FP64 and rounds once
+    act = eact.astype(bool)
+    assert np.abs(mine["sensitivity"] - ref["sensitivity"]).max() <= 2e-6 * np.abs(ref["sensitivity"]).max()
+    # the OC trial: FP32 powf in both, one rounding apart at most
+    assert np.abs(mine["oc_try"][act] - ref["oc_try"][act]).max() <= 2e-6
+    # the filter: FP32 weights, FP64 sums in both
+    assert np.abs(mine["filter"][act] - ref["filter"][act]).max() <= 1e-6 * np.abs(ref["filter"]).max()
