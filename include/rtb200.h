@@ -128,6 +128,11 @@ int rt_ctx_create(int device, void* cuda_stream /* NULL: own stream */, rt_ctx**
 void rt_ctx_destroy(rt_ctx* ctx);
 const char* rt_last_error(rt_ctx* ctx);
 int rt_ctx_sync(rt_ctx* ctx);
+/* polls a device-side wait on other blocks may spend before it gives up (the grid barrier of the
+ * fused Chebyshev sweeps; default 1 << 22, polls <= 0 restores it).  No reference counterpart: a
+ * test lowers it so that a wait runs out and the call reports RT_ECUDA with the reason, leaving
+ * the context usable. */
+int rt_ctx_set_wait_limit(rt_ctx* ctx, long long polls);
 void rt_params_default(rt_params* p);
 /* per-kernel device-time accounting (CUDA events around each launch) */
 int rt_profile_enable(rt_ctx* ctx, int on);
@@ -225,6 +230,25 @@ int rt_apply_K_dev(rt_hier* h, const double* u_dev, double* out_dev);
 int rt_apply_K(rt_hier* h, const double* u, double* out);
 /* Grid::compliance (grid/Grid.cpp:1976-1979): f.u on level 0 */
 int rt_compliance(rt_hier* h, double* c);
+/* forceProject (optimization/projection.cu:165-231, projection.cpp:289-360): f_dev (dense [3][nv]
+ * device vector) <- P f: the load-node values projected onto the admissible loads of the work mode
+ * (wsff: unchanged; *scf: normal component only; ns*: minus the rigid-mode components), every other
+ * node set to zero */
+int rt_force_project(rt_hier* h, double* f_dev);
+/* getForceSupport (optimization/projection.cu:307-338): fs_dev [3][nload] (one array per component,
+ * load nodes in increasing dense id) <- the load-node values of f_dev */
+int rt_get_force_support(rt_hier* h, const double* f_dev, double* fs_dev);
+/* setForceSupport (optimization/projection.cu:340-369): f_dev <- 0, then the load nodes <- fs_dev */
+int rt_set_force_support(rt_hier* h, const double* fs_dev, double* f_dev);
+/* displacementProject (optimization/projection.cpp:374-392): u_dev minus its components along the
+ * orthonormalised rigid modes of the active nodes (no-support modes; a no-op with supports) */
+int rt_displacement_project(rt_hier* h, double* u_dev);
+/* getLoadNodes (optimization/projection.cpp:129-143): *n = number of load nodes; nodes (host,
+ * may be null) <- their dense level-0 node ids in increasing order */
+int rt_load_nodes(rt_hier* h, int* n, int* nodes);
+/* Grid::elementCompliance (grid/Grid.cu:3434-3480): ce_dev[ne] (dense element order, device)
+ * <- rho_e^p u_e.KE u_e for u_dev (dense [3][nv] device vector); 0 on inactive elements */
+int rt_element_compliance(rt_hier* h, const double* u_dev, float* ce_dev);
 /* Grid::relative_residual (grid/Grid.cu:1946-1951) */
 int rt_relative_residual(rt_hier* h, double* rel);
 /* Compliance f.u of two caller-owned FP64 device vectors of length n, written to

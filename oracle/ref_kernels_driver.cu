@@ -173,7 +173,7 @@ int finish() { return cudaDeviceSynchronize() == cudaSuccess && cudaGetLastError
 
 }  // namespace
 
-extern "C" int ref_apply_k(int nx, int ny, int nz, const uint8_t* eact, const uint8_t* vfix, const float* rho, float p,
+extern "C" __attribute__((visibility("default"))) int ref_apply_k(int nx, int ny, int nz, const uint8_t* eact, const uint8_t* vfix, const float* rho, float p,
                            const double* KE, const double* u, double* f_out) {
     RefBox b = make_box(nx, ny, nz, eact);
     Tables t = bind(b, vfix, nullptr, p, KE);
@@ -199,7 +199,7 @@ extern "C" int ref_apply_k(int nx, int ny, int nz, const uint8_t* eact, const ui
     return st;
 }
 
-extern "C" int ref_sensitivity(int nx, int ny, int nz, const uint8_t* eact, const float* rho, float p, const double* KE,
+extern "C" __attribute__((visibility("default"))) int ref_sensitivity(int nx, int ny, int nz, const uint8_t* eact, const float* rho, float p, const double* KE,
                                const double* u, float* sens_out) {
     RefBox b = make_box(nx, ny, nz, eact);
     Tables t = bind(b, nullptr, nullptr, p, KE);
@@ -218,7 +218,7 @@ extern "C" int ref_sensitivity(int nx, int ny, int nz, const uint8_t* eact, cons
     return st;
 }
 
-extern "C" int ref_oc_try(int nx, int ny, int nz, const uint8_t* eact, const uint8_t* eshell, const float* rho,
+extern "C" __attribute__((visibility("default"))) int ref_oc_try(int nx, int ny, int nz, const uint8_t* eact, const uint8_t* eshell, const float* rho,
                           const float* sens, float thres, float step, float damp, float rhomin, float* rho_out) {
     RefBox b = make_box(nx, ny, nz, eact);
     Tables t = bind(b, nullptr, eshell, 3.f, nullptr);
@@ -236,7 +236,7 @@ extern "C" int ref_oc_try(int nx, int ny, int nz, const uint8_t* eact, const uin
     return st;
 }
 
-extern "C" int ref_filter(int nx, int ny, int nz, const uint8_t* eact, float radius, const float* sens, float* out) {
+extern "C" __attribute__((visibility("default"))) int ref_filter(int nx, int ny, int nz, const uint8_t* eact, float radius, const float* sens, float* out) {
     RefBox b = make_box(nx, ny, nz, eact);
     const int R = nx > ny ? (nx > nz ? nx : nz) : (ny > nz ? ny : nz);
     const long nbits = (long)R * R * R;

@@ -139,6 +139,13 @@ SIGNATURES = {
     "rt_unet_harvest": (I, [P, P, I, C.c_uint64, P, P]),
     "rt_hier_set_learned": (I, [P, P, D]),
     "rt_hier_learned_stats": (I, [P, C.POINTER(C.c_longlong), C.POINTER(I)]),
+    "rt_force_project": (I, [P, P]),
+    "rt_ctx_set_wait_limit": (I, [P, C.c_longlong]),
+    "rt_get_force_support": (I, [P, P, P]),
+    "rt_set_force_support": (I, [P, P, P]),
+    "rt_displacement_project": (I, [P, P]),
+    "rt_load_nodes": (I, [P, C.POINTER(I), P]),
+    "rt_element_compliance": (I, [P, P, P]),
     "rt_sensitivity": (I, [P, I]),
     "rt_filter_sensitivity": (I, [P, F]),
     "rt_oc_update": (I, [P, F, C.POINTER(F), C.POINTER(I)]),

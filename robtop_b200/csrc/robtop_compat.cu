@@ -1,6 +1,7 @@
 // robtop_compat.cu — the reference's C++ entry points (robtop_compat.h) on the C ABI.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -11,6 +12,58 @@
 
 Parameter params;
 grid::HierarchyGrid grids;
+gpu_manager_t gpu_manager;
+
+// mem/gpu_manager_t.cu: named device buffers, freed with the manager
+void gpu_manager_t::upload_buf(void* dst, const void* src, size_t size) {
+    if (cudaMemcpy(dst, src, size, cudaMemcpyHostToDevice) != cudaSuccess) throw std::runtime_error("upload_buf failed");
+}
+void gpu_manager_t::download_buf(void* host_dst, const void* dev_src, size_t n) {
+    if (cudaMemcpy(host_dst, dev_src, n, cudaMemcpyDeviceToHost) != cudaSuccess)
+        throw std::runtime_error("download_buf failed");
+}
+void gpu_manager_t::initMem(void* pdata, size_t len, char value) {
+    if (cudaMemset(pdata, value, len) != cudaSuccess) throw std::runtime_error("initMem failed");
+}
+void* gpu_manager_t::add_buf(const std::string& name, size_t size, const void* src) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, size ? size : 1) != cudaSuccess) {
+        cudaGetLastError();
+        throw std::runtime_error("add_buf: cudaMalloc of " + std::to_string(size) + " bytes failed");
+    }
+    if (src) upload_buf(p, src, size);
+    _bufs.push_back(Buf{name, p, size});
+    return p;
+}
+void* gpu_manager_t::add_buf(size_t size, const void* src) {
+    return add_buf("anonymous_" + std::to_string(_anonymous++), size, src);
+}
+void gpu_manager_t::delete_buf(const std::string& name) {
+    for (size_t i = 0; i < _bufs.size(); i++)
+        if (_bufs[i].name == name) {
+            cudaFree(_bufs[i].p);
+            _bufs.erase(_bufs.begin() + i);
+            return;
+        }
+}
+void gpu_manager_t::delete_buf(void* pbuf) {
+    for (size_t i = 0; i < _bufs.size(); i++)
+        if (_bufs[i].p == pbuf) {
+            cudaFree(_bufs[i].p);
+            _bufs.erase(_bufs.begin() + i);
+            return;
+        }
+}
+size_t gpu_manager_t::size(void) {
+    size_t s = 0;
+    for (const Buf& b : _bufs) s += b.size;
+    return s;
+}
+gpu_manager_t::~gpu_manager_t() {
+    // at static destruction the runtime may already be gone
+    if (cudaFree(nullptr) == cudaSuccess)
+        for (const Buf& b : _bufs) cudaFree(b.p);
+}
 
 namespace grid {
 
@@ -237,6 +290,116 @@ void Grid::v3_scale(double* v[3], double ampl) {
     cudaStreamSynchronize(h->ctx->stream);
 }
 
+void Grid::v3_add(double* a[3], double alpha, double* b[3]) { v3_add(1.0, a, alpha, b); }
+
+void Grid::v3_add(double alpha, double* a[3], double beta, double* b[3]) {
+    rt_hier* h = _H->hier();
+    double ab[2] = {alpha, beta};
+    memcpy(h->ctx->hscal + 30, ab, sizeof(ab));
+    cudaMemcpyAsync(h->scal + 86, h->ctx->hscal + 30, sizeof(ab), cudaMemcpyHostToDevice, h->ctx->stream);
+    for (int c = 0; c < 3; c++) {
+        _H->check(rtk::scale(h, _nv, a[c], h->scal + 86, false), "v3_add");
+        _H->check(rtk::axpy(h, _nv, beta, b[c], a[c]), "v3_add");
+    }
+    cudaStreamSynchronize(h->ctx->stream);
+}
+
+void Grid::elementCompliance(double* u[3], float* ce) {
+    if (_layer != 0) throw std::runtime_error("elementCompliance is defined on the finest level");
+    rt_hier* h = _H->hier();
+    const double* uin = u[0];
+    if (!contiguous(u, _nv)) {
+        for (int c = 0; c < 3; c++)
+            cudaMemcpyAsync(h->x + c * _nv, u[c], sizeof(double) * _nv, cudaMemcpyDeviceToDevice, h->ctx->stream);
+        uin = h->x;
+    }
+    _H->check(rt_element_compliance(h, uin, ce), "elementCompliance");
+}
+
+// the support force arrays of level 0, allocated on first use
+static void ensure_support(grid::Grid* g, grid::HierarchyGrid* H, double* fs[3], double** scratch) {
+    if (fs[0]) return;
+    const int nl = (int)H->loadNodes().size();
+    double* p = nullptr;
+    H->check(cudaMalloc(&p, sizeof(double) * 6 * (nl > 0 ? nl : 1)) == cudaSuccess ? RT_OK : RT_ENOMEM,
+             "support force allocation");
+    cudaMemset(p, 0, sizeof(double) * 6 * (nl > 0 ? nl : 1));
+    for (int c = 0; c < 3; c++) fs[c] = p + c * nl;
+    *scratch = p + 3 * nl;
+    (void)g;
+}
+
+static double support_diff_norm(grid::HierarchyGrid* H, double* const fs_old[3], const double* fs_new, int nl) {
+    rt_hier* h = H->hier();
+    std::vector<double> a(3 * (size_t)nl), b(3 * (size_t)nl);
+    cudaMemcpyAsync(b.data(), fs_new, sizeof(double) * 3 * nl, cudaMemcpyDeviceToHost, h->ctx->stream);
+    cudaMemcpyAsync(a.data(), fs_old[0], sizeof(double) * 3 * nl, cudaMemcpyDeviceToHost, h->ctx->stream);
+    cudaStreamSynchronize(h->ctx->stream);
+    double s = 0;
+    for (size_t i = 0; i < a.size(); i++) s += (a[i] - b[i]) * (a[i] - b[i]);
+    return std::sqrt(s);
+}
+
+double Grid::supportForceCh(void) { return supportForceCh(_F); }
+
+double Grid::supportForceCh(double* f[3]) {
+    ensure_support(this, _H, _FS, &_FS_new);
+    const int nl = (int)_H->loadNodes().size();
+    double* fin[3] = {f[0], f[1], f[2]};
+    rt_hier* h = _H->hier();
+    const double* src = f[0];
+    if (!contiguous(fin, _nv)) {
+        for (int c = 0; c < 3; c++)
+            cudaMemcpyAsync(h->x + c * _nv, f[c], sizeof(double) * _nv, cudaMemcpyDeviceToDevice, h->ctx->stream);
+        src = h->x;
+    }
+    _H->check(rt_get_force_support(h, src, _FS_new), "supportForceCh");
+    return support_diff_norm(_H, _FS, _FS_new, nl);
+}
+
+double Grid::supportForceNorm(void) {
+    ensure_support(this, _H, _FS, &_FS_new);
+    const int nl = (int)_H->loadNodes().size();
+    rt_hier* h = _H->hier();
+    std::vector<double> a(3 * (size_t)nl);
+    cudaMemcpyAsync(a.data(), _FS[0], sizeof(double) * 3 * nl, cudaMemcpyDeviceToHost, h->ctx->stream);
+    cudaStreamSynchronize(h->ctx->stream);
+    double s = 0;
+    for (double v : a) s += v * v;
+    return std::sqrt(s);
+}
+
+// HierarchyGrid::writeDensity / readDensity (grid/Grid.cpp:727-764, 809-839) as raw files
+void HierarchyGrid::writeDensity(const std::string& filename) {
+    rt_level_info li;
+    check(rt_hier_level_info(_h, 0, &li), "level info");
+    std::vector<float> rho((size_t)li.nx * li.ny * li.nz);
+    check(rt_get(_h, RT_FIELD_RHO, 0, RT_LAYOUT_DENSE, rho.data()), "writeDensity");
+    FILE* fp = fopen(filename.c_str(), "wb");
+    if (!fp) throw std::runtime_error("writeDensity: cannot open " + filename);
+    const int32_t dims[3] = {li.nx, li.ny, li.nz};
+    const bool ok = fwrite("RTB200D1", 1, 8, fp) == 8 && fwrite(dims, sizeof(int32_t), 3, fp) == 3 &&
+                    fwrite(rho.data(), sizeof(float), rho.size(), fp) == rho.size();
+    fclose(fp);
+    if (!ok) throw std::runtime_error("writeDensity: short write to " + filename);
+}
+
+void HierarchyGrid::readDensity(const std::string& filename) {
+    rt_level_info li;
+    check(rt_hier_level_info(_h, 0, &li), "level info");
+    FILE* fp = fopen(filename.c_str(), "rb");
+    if (!fp) throw std::runtime_error("readDensity: cannot open " + filename);
+    char magic[8];
+    int32_t dims[3];
+    std::vector<float> rho((size_t)li.nx * li.ny * li.nz);
+    bool ok = fread(magic, 1, 8, fp) == 8 && memcmp(magic, "RTB200D1", 8) == 0 &&
+              fread(dims, sizeof(int32_t), 3, fp) == 3 && dims[0] == li.nx && dims[1] == li.ny && dims[2] == li.nz;
+    ok = ok && fread(rho.data(), sizeof(float), rho.size(), fp) == rho.size();
+    fclose(fp);
+    if (!ok) throw std::runtime_error("readDensity: " + filename + " is not a density file of this grid");
+    check(rt_put(_h, RT_FIELD_RHO, 0, RT_LAYOUT_DENSE, rho.data()), "readDensity");
+}
+
 }  // namespace grid
 
 // ---------------------------------------------------------------------------
@@ -329,10 +492,13 @@ void solveFEM(void) {
     }
 }
 
+void remember_worst_case(void);
+
 double modifiedPM(void) {
     double lam = 0;
     rt_solve_info info;
     grids.check(rt_worst_case(grids.hier(), RT_WORST_MODPM, 500, 0.0, g_pm_seed++, &lam, &info), "modifiedPM");
+    remember_worst_case();
     return lam;
 }
 
@@ -392,4 +558,257 @@ void test_rigid_displacement(void) {
         g->update_residual();
         printf("-- u_rigid %d res = %lf\n", k, g->residual());
     }
+}
+
+// ---------------------------------------------------------------------------
+// optimization/projection.h:16-65
+// ---------------------------------------------------------------------------
+static double* contiguous_copy(double* const v[3], long long nv, double* scratch) {
+    if (v[1] == v[0] + nv && v[2] == v[0] + 2 * nv) return v[0];
+    rt_hier* h = grids.hier();
+    for (int c = 0; c < 3; c++)
+        cudaMemcpyAsync(scratch + c * nv, v[c], sizeof(double) * nv, cudaMemcpyDeviceToDevice, h->ctx->stream);
+    return scratch;
+}
+
+static void copy_back(double* const v[3], long long nv, const double* src) {
+    if (src == v[0]) return;
+    rt_hier* h = grids.hier();
+    for (int c = 0; c < 3; c++)
+        cudaMemcpyAsync(v[c], src + c * nv, sizeof(double) * nv, cudaMemcpyDeviceToDevice, h->ctx->stream);
+}
+
+const std::vector<int>& getLoadNodes(void) { return grids.loadNodes(); }
+int n_loadnodes(void) { return (int)grids.loadNodes().size(); }
+
+void forceProject(double* f_dev[3]) {
+    const long long nv = grids[0]->n_box_nodes();
+    double* f = contiguous_copy(f_dev, nv, grids.hier()->x);
+    grids.check(rt_force_project(grids.hier(), f), "forceProject");
+    copy_back(f_dev, nv, f);
+}
+
+// host support-force vectors (one per component, the load nodes in order): scattered into a
+// device vector, projected, gathered back
+void forceProject(std::vector<double> fsupport[3]) {
+    rt_hier* h = grids.hier();
+    const int nl = n_loadnodes();
+    for (int c = 0; c < 3; c++)
+        if ((int)fsupport[c].size() != nl) throw std::invalid_argument("forceProject: support vectors of the wrong length");
+    std::vector<double> soa(3 * (size_t)nl);
+    for (int c = 0; c < 3; c++) std::copy(fsupport[c].begin(), fsupport[c].end(), soa.begin() + (size_t)c * nl);
+    double* d = nullptr;
+    grids.check(cudaMalloc(&d, sizeof(double) * 3 * (nl > 0 ? nl : 1)) == cudaSuccess ? RT_OK : RT_ENOMEM, "forceProject");
+    cudaMemcpyAsync(d, soa.data(), sizeof(double) * 3 * nl, cudaMemcpyHostToDevice, h->ctx->stream);
+    int st = rt_set_force_support(h, d, h->x);
+    if (st == RT_OK) st = rt_force_project(h, h->x);
+    if (st == RT_OK) st = rt_get_force_support(h, h->x, d);
+    if (st == RT_OK) cudaMemcpyAsync(soa.data(), d, sizeof(double) * 3 * nl, cudaMemcpyDeviceToHost, h->ctx->stream);
+    cudaStreamSynchronize(h->ctx->stream);
+    cudaFree(d);
+    grids.check(st, "forceProject");
+    for (int c = 0; c < 3; c++) std::copy(soa.begin() + (size_t)c * nl, soa.begin() + (size_t)(c + 1) * nl, fsupport[c].begin());
+}
+
+void getForceSupport(double const* const f_dev[3], double* fsup[3]) {
+    rt_hier* h = grids.hier();
+    const long long nv = grids[0]->n_box_nodes();
+    const int nl = n_loadnodes();
+    double* fv[3] = {const_cast<double*>(f_dev[0]), const_cast<double*>(f_dev[1]), const_cast<double*>(f_dev[2])};
+    const double* f = contiguous_copy(fv, nv, h->x);
+    const bool soa = fsup[1] == fsup[0] + nl && fsup[2] == fsup[0] + 2 * nl;
+    double* dst = soa ? fsup[0] : h->fs;  // h->fs holds 3 * nload doubles
+    grids.check(rt_get_force_support(h, f, dst), "getForceSupport");
+    if (!soa)
+        for (int c = 0; c < 3; c++)
+            cudaMemcpyAsync(fsup[c], dst + (size_t)c * nl, sizeof(double) * nl, cudaMemcpyDeviceToDevice, h->ctx->stream);
+    cudaStreamSynchronize(h->ctx->stream);
+}
+
+void getForceSupport(double const* const f_dev[3], std::vector<double> fs[3]) {
+    rt_hier* h = grids.hier();
+    const int nl = n_loadnodes();
+    double* p[3] = {h->fs, h->fs + nl, h->fs + 2 * nl};
+    getForceSupport(f_dev, p);
+    for (int c = 0; c < 3; c++) {
+        fs[c].resize(nl);
+        cudaMemcpy(fs[c].data(), p[c], sizeof(double) * nl, cudaMemcpyDeviceToHost);
+    }
+}
+
+void setForceSupport(double const* const fsup[3], double* f_dev[3]) {
+    rt_hier* h = grids.hier();
+    const long long nv = grids[0]->n_box_nodes();
+    const int nl = n_loadnodes();
+    const double* src = fsup[0];
+    if (!(fsup[1] == fsup[0] + nl && fsup[2] == fsup[0] + 2 * nl)) {
+        for (int c = 0; c < 3; c++)
+            cudaMemcpyAsync(h->fs + (size_t)c * nl, fsup[c], sizeof(double) * nl, cudaMemcpyDeviceToDevice, h->ctx->stream);
+        src = h->fs;
+    }
+    const bool contig = f_dev[1] == f_dev[0] + nv && f_dev[2] == f_dev[0] + 2 * nv;
+    double* dst = contig ? f_dev[0] : h->x;
+    grids.check(rt_set_force_support(h, src, dst), "setForceSupport");
+    copy_back(f_dev, nv, dst);
+    cudaStreamSynchronize(h->ctx->stream);
+}
+
+void displacementProject(double* u_dev[3]) {
+    const long long nv = grids[0]->n_box_nodes();
+    double* u = contiguous_copy(u_dev, nv, grids.hier()->x);
+    grids.check(rt_displacement_project(grids.hier(), u), "displacementProject");
+    copy_back(u_dev, nv, u);
+    cudaStreamSynchronize(grids.hier()->ctx->stream);
+}
+
+// ---------------------------------------------------------------------------
+// remaining optimization/optimization.h entry points
+// ---------------------------------------------------------------------------
+static std::string g_output_dir = ".";
+
+void setOutpurDir(const std::string& dirname) { g_output_dir = dirname; }
+const std::string& getOutputDir(void) { return g_output_dir; }
+
+// inCompleteModiPM (optimization/optimization.cpp:427-472): a random balanced unit load, then up to
+// 50 steps of one V-cycle on it, the displacement projected and normalised as the next load, until
+// the support force changes by less than fch_thres; returns the compliance f.u
+double inCompleteModiPM(double fch_thres) {
+    grid::Grid* g = grids[0];
+    g->randForce();
+    forceProject(g->getForce());
+    g->unitizeForce();
+    g->reset_displacement();
+    getForceSupport(g->getForce(), g->getSupportForce());
+    double fch = 1;
+    int itn = 0;
+    while (itn++ < 50 && fch > fch_thres) {
+        grids.v_cycle(1, 1);
+        g->v3_copy(g->getDisplacement(), g->getForce());
+        forceProject(g->getForce());
+        g->unitizeForce();
+        fch = g->supportForceCh() / g->supportForceNorm();
+        getForceSupport(g->getForce(), g->getSupportForce());
+    }
+    const double c = g->compliance();
+    if (!std::isfinite(c)) throw std::runtime_error("inCompleteModiPM: NaN compliance");
+    return c;
+}
+
+// MGPSOR (optimization/optimization.cpp:474-535): inCompleteModiPM, then preconditioned
+// eigen-iterations x <- x + Vcycle(P x - lambda K x) with lambda = |P x|^2 / x.K x
+double MGPSOR(void) {
+    grid::Grid* g = grids[0];
+    inCompleteModiPM();
+    rt_hier* h = grids.hier();
+    const long long nv = g->n_box_nodes();
+    double* xk_mem = nullptr;
+    grids.check(cudaMalloc(&xk_mem, sizeof(double) * 3 * nv) == cudaSuccess ? RT_OK : RT_ENOMEM, "MGPSOR");
+    double* xk[3] = {xk_mem, xk_mem + nv, xk_mem + 2 * nv};
+    double fch = 1, fsnorm = 1;
+    int itn = 0;
+    while ((itn++ < 200 && fch > 1e-4) || itn < 3) {
+        g->v3_copy(g->getDisplacement(), xk);
+        g->applyK(g->getDisplacement(), g->getForce());
+        const double c = g->v3_dot(g->getDisplacement(), g->getForce());
+        forceProject(g->getDisplacement());
+        fsnorm = g->v3_norm(g->getDisplacement());
+        const double lambda = fsnorm * fsnorm / c;
+        g->v3_add(-lambda, g->getForce(), 1, g->getDisplacement());
+        g->v3_scale(g->getDisplacement(), 1.0 / g->v3_norm(g->getDisplacement()));
+        fch = g->supportForceCh(g->getDisplacement());
+        getForceSupport(g->getDisplacement(), g->getSupportForce());
+        g->reset_displacement();
+        double rel_res = 1;
+        int vit = 0;
+        while (rel_res > 1e-1 && vit++ < 3) rel_res = grids.v_cycle();
+        g->v3_add(g->getDisplacement(), 1, xk);
+    }
+    cudaFree(xk_mem);
+    (void)h;
+    g->v3_scale(g->getDisplacement(), 1.0 / fsnorm);
+    g->applyK(g->getDisplacement(), g->getForce());
+    return g->v3_dot(g->getDisplacement(), g->getForce());
+}
+
+// RayleighGradient (optimization/optimization.cpp:385-398): for R(u) = |P u|^2 / u.K u, returns
+// (|P u|^2, u.K u) and g <- the gradient -2 P u / u.K u + 2 |P u|^2 K u / (u.K u)^2 (the
+// reference's sign convention); leaves K u in the force vector
+std::pair<double, double> RayleighGradient(double* u[3], double* g[3]) {
+    grid::Grid* G = grids[0];
+    G->v3_copy(u, g);
+    forceProject(g);
+    const double pnorm = G->v3_dot(g, g);
+    G->applyK(u, G->getForce());
+    const double knorm = G->v3_dot(u, G->getForce());
+    G->v3_add(-2.0 / knorm, g, 2.0 * pnorm / (knorm * knorm), G->getForce());
+    return {pnorm, knorm};
+}
+
+// Pnorm / Knorm (optimization/optimization.cpp:400-425)
+double Pnorm(double* u[3]) {
+    std::vector<double> fs[3];
+    getForceSupport(u, fs);
+    forceProject(fs);
+    double s = 0;
+    for (int c = 0; c < 3; c++)
+        for (double v : fs[c]) s += v * v;
+    return s;
+}
+
+double Knorm(double* u[3]) {
+    grid::Grid* G = grids[0];
+    G->applyK(u, G->getForce());
+    return G->v3_dot(u, G->getForce());
+}
+
+// checkAdjointVariable (optimization/optimization.cu:353-402): with the adjoint N^T lambda in the
+// displacement vector and the last worst-case pair (u_w, f_w = K u_w, compliance mu) from
+// modifiedPM, |2 f_w - K (N^T lambda) - 2 mu K f_w| on the free nodes must be below 1e-6
+// (relative to |f_w|); the displacement vector is left unchanged
+static std::vector<double> g_uworst, g_fworst;
+static double g_mu = 0;
+
+void remember_worst_case(void) {
+    rt_hier* h = grids.hier();
+    const long long nv = grids[0]->n_box_nodes();
+    g_uworst.resize(3 * nv);
+    g_fworst.resize(3 * nv);
+    grids.check(rt_get(h, RT_FIELD_U, 0, RT_LAYOUT_DENSE, g_uworst.data()), "worst-case displacement");
+    grids.check(rt_get(h, RT_FIELD_F, 0, RT_LAYOUT_DENSE, g_fworst.data()), "worst-case force");
+    g_mu = 0;
+    for (long long i = 0; i < 3 * nv; i++) g_mu += g_uworst[i] * g_fworst[i];
+}
+
+bool checkAdjointVariable(void) {
+    if (g_fworst.empty()) throw std::runtime_error("checkAdjointVariable: run modifiedPM first");
+    rt_hier* h = grids.hier();
+    const long long nv = grids[0]->n_box_nodes();
+    std::vector<double> adj(3 * nv), kadj(3 * nv), kkf(3 * nv);
+    std::vector<uint8_t> fix(nv, 0);
+    grids.check(rt_get(h, RT_FIELD_U, 0, RT_LAYOUT_DENSE, adj.data()), "adjoint");
+    grids.check(rt_apply_K(h, adj.data(), kadj.data()), "K adjoint");
+    grids.check(rt_apply_K(h, g_fworst.data(), kkf.data()), "K f_worst");
+    grids.check(rt_get(h, RT_FIELD_VFIX, 0, RT_LAYOUT_DENSE, fix.data()), "supports");
+    double r2 = 0, f2 = 0;
+    for (long long i = 0; i < 3 * nv; i++) {
+        if (fix[i % nv]) continue;  // resetDirchlet: rows of fixed nodes dropped
+        const double r = 2 * g_fworst[i] - kadj[i] - 2 * g_mu * kkf[i];
+        r2 += r * r;
+        f2 += g_fworst[i] * g_fworst[i];
+    }
+    return std::sqrt(r2) < 1e-6 * std::max(std::sqrt(f2), 1e-300);
+}
+
+// selfTest (optimization/optimization.cu:231-328): the reference checks its BitSAT and GraftArray
+// containers; here the equivalent checks of this library's structures: the rigid modes are in the
+// null space of the finest operator (test_rigid_displacement) and the template matrix is symmetric
+void selfTest(void) {
+    printf("-- Self testing...\n");
+    double ke[576];
+    grids.check(rt_template_matrix(grids.hier(), ke), "template matrix");
+    double asym = 0;
+    for (int i = 0; i < 24; i++)
+        for (int j = 0; j < 24; j++) asym = std::max(asym, std::fabs(ke[i * 24 + j] - ke[j * 24 + i]));
+    printf("-- template matrix asymmetry %g\n", asym);
+    test_rigid_displacement();
 }

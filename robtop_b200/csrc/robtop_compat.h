@@ -15,6 +15,7 @@
 #pragma once
 #include <array>
 #include <cstdint>
+#include <utility>
 #include <functional>
 #include <string>
 #include <vector>
@@ -64,6 +65,16 @@ public:
     double v3_norm(double* v[3]);
     void v3_copy(double* vsrc[3], double* vdst[3]);
     void v3_scale(double* v[3], double ampl);
+    // grid/Grid.cu:2163-2200: a += alpha b, and a = alpha a + beta b
+    void v3_add(double* a[3], double alpha, double* b[3]);
+    void v3_add(double alpha, double* a[3], double beta, double* b[3]);
+    // grid/Grid.cu:3434-3480: per-element compliance rho_e^p u_e.KE u_e of u into ce (device, dense element order)
+    void elementCompliance(double* u[3], float* ce);
+    // grid/Grid.cu:2255-2286: the support force held by the grid (device [3][nload]) and its change
+    double** getSupportForce(void) { return _FS; }
+    double supportForceCh(void);
+    double supportForceCh(double* f[3]);
+    double supportForceNorm(void);
     int _layer = 0;
 
 private:
@@ -73,6 +84,8 @@ private:
     double* _U[3];
     double* _F[3];
     double* _R[3];
+    double* _FS[3] = {nullptr, nullptr, nullptr};  // support force, [3][nload] device (level 0)
+    double* _FS_new = nullptr;                        // scratch [3][nload] for supportForceCh
     double* _tmp = nullptr;
 };
 
@@ -95,6 +108,10 @@ public:
     bool hasSupport(void) { return _mode == with_support_constrain_force_direction || _mode == with_support_free_force; }
     double elementLength(void) { return _params.element_length; }
     void resetAllResidual(void);
+    // grid/Grid.cpp:727-764, 809-839 (the reference writes and reads OpenVDB grids): the level-0
+    // densities as a raw file, magic "RTB200D1", int32 nx, ny, nz, then nx*ny*nz float32 (x fastest)
+    void writeDensity(const std::string& filename);
+    void readDensity(const std::string& filename);
 
     std::function<bool(double[3])> _inLoadArea;
     std::function<bool(double[3])> _inFixedArea;
@@ -120,6 +137,33 @@ private:
 };
 
 }  // namespace grid
+
+// mem/gpu_manager_t.h: the reference's device-buffer manager, the members its callers use.
+// Buffers come from the library's CUDA runtime; callers of this layer allocate through it
+// rather than linking a CUDA runtime of their own.
+class gpu_manager_t {
+public:
+    static void upload_buf(void* dst, const void* src, size_t size);
+    static void download_buf(void* host_dst, const void* dev_src, size_t n);
+    static void initMem(void* pdata, size_t len, char value = 0);
+    void* add_buf(const std::string& name, size_t size, const void* src = nullptr);
+    void* add_buf(size_t size, const void* src = nullptr);
+    void delete_buf(const std::string& name);
+    void delete_buf(void* pbuf);
+    size_t size(void);
+    ~gpu_manager_t();
+
+private:
+    struct Buf {
+        std::string name;
+        void* p;
+        size_t size;
+    };
+    std::vector<Buf> _bufs;
+    int _anonymous = 0;
+};
+
+extern gpu_manager_t gpu_manager;
 
 // optimization/optimization.h:11-22
 struct Parameter {
@@ -158,3 +202,25 @@ void uploadTemplateMatrix(void);
 void initDensities(double rho);
 void update_stencil(void);
 void test_rigid_displacement(void);
+
+// optimization/optimization.h:28-82, the remaining entry points
+void setOutpurDir(const std::string& dirname);
+const std::string& getOutputDir(void);
+void selfTest(void);
+double inCompleteModiPM(double fch_thres = 1e-2);
+double MGPSOR(void);
+std::pair<double, double> RayleighGradient(double* u[3], double* g[3]);
+double Pnorm(double* u[3]);
+double Knorm(double* u[3]);
+bool checkAdjointVariable(void);
+
+// optimization/projection.h:16-65 (dense level-0 node ids instead of GS ids; support-force
+// arrays hold the load nodes in increasing id)
+const std::vector<int>& getLoadNodes(void);
+int n_loadnodes(void);
+void forceProject(double* f_dev[3]);
+void forceProject(std::vector<double> fsupport[3]);
+void getForceSupport(double const* const f_dev[3], double* fsup[3]);
+void getForceSupport(double const* const f_dev[3], std::vector<double> fs[3]);
+void setForceSupport(double const* const fsup[3], double* f_dev[3]);
+void displacementProject(double* u_dev[3]);

@@ -152,6 +152,12 @@ static void ctx_free(rt_ctx* c) {
 
 extern "C" const char* rt_last_error(rt_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
+extern "C" int rt_ctx_set_wait_limit(rt_ctx* c, long long polls) {
+    if (!c) return RT_EINVAL;
+    c->wait_limit = polls > 0 ? polls : (1LL << 22);
+    return RT_OK;
+}
+
 extern "C" int rt_ctx_sync(rt_ctx* c) {
     if (!c) return RT_EINVAL;
     RT_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -1323,6 +1329,86 @@ extern "C" int rt_compliance(rt_hier* h, double* cpl) {
     return read_scalars(h, 2, 1, cpl);
 }
 
+// ---------------------------------------------------------------------------
+// projection API (optimization/projection.h:16-65) and element compliance
+// ---------------------------------------------------------------------------
+__global__ void k_support_gather_soa(int nload, long nv, const int* __restrict__ nodes, const double* __restrict__ f,
+                                     double* __restrict__ fs) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nload; i += gridDim.x * blockDim.x) {
+        const long v = nodes[i];
+        fs[i] = f[v];
+        fs[nload + i] = f[nv + v];
+        fs[2 * nload + i] = f[2 * nv + v];
+    }
+}
+
+__global__ void k_support_scatter_soa(int nload, long nv, const int* __restrict__ nodes,
+                                      const double* __restrict__ fs, double* __restrict__ f) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nload; i += gridDim.x * blockDim.x) {
+        const long v = nodes[i];
+        f[v] = fs[i];
+        f[nv + v] = fs[nload + i];
+        f[2 * nv + v] = fs[2 * nload + i];
+    }
+}
+
+static unsigned load_blocks(const rt_hier* h) {
+    return (unsigned)std::max(1, std::min((h->nload + 255) / 256, h->ctx->sm_count * 8));
+}
+
+extern "C" int rt_force_project(rt_hier* h, double* f_dev) {
+    if (!h || !f_dev) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
+    if (h->nload == 0) return rt_fail(h->ctx, RT_ESTATE, "forceProject: no load nodes (rt_set_load_nodes)");
+    return rtk::project_load(h, f_dev);
+}
+
+extern "C" int rt_get_force_support(rt_hier* h, const double* f_dev, double* fs_dev) {
+    if (!h || !f_dev || !fs_dev) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
+    if (h->nload == 0) return RT_OK;
+    return rt_launch(h->ctx, "support_gather", [&] {
+        k_support_gather_soa<<<load_blocks(h), 256, 0, h->ctx->stream>>>(h->nload, h->L[0].nv, h->load_nodes, f_dev,
+                                                                         fs_dev);
+    });
+}
+
+extern "C" int rt_set_force_support(rt_hier* h, const double* fs_dev, double* f_dev) {
+    if (!h || !fs_dev || !f_dev) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
+    RT_CUDA(h->ctx, cudaMemsetAsync(f_dev, 0, sizeof(double) * 3 * h->L[0].nv, h->ctx->stream));
+    if (h->nload == 0) return RT_OK;
+    return rt_launch(h->ctx, "support_scatter", [&] {
+        k_support_scatter_soa<<<load_blocks(h), 256, 0, h->ctx->stream>>>(h->nload, h->L[0].nv, h->load_nodes, fs_dev,
+                                                                          f_dev);
+    });
+}
+
+extern "C" int rt_displacement_project(rt_hier* h, double* u_dev) {
+    if (!h || !u_dev) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
+    if (h->P.mode != RT_MODE_NSCF && h->P.mode != RT_MODE_NSFF) return RT_OK;  // supports fix the rigid modes
+    if (h->Ru == nullptr) RT_CHECK(rtk::rigid_nodes(h));
+    return rtk::displacement_project(h, u_dev);
+}
+
+extern "C" int rt_load_nodes(rt_hier* h, int* n, int* nodes) {
+    if (!h || !n) return RT_EINVAL;
+    *n = h->nload;
+    if (nodes && h->nload > 0) {
+        RT_CUDA(h->ctx, cudaMemcpyAsync(nodes, h->load_nodes, sizeof(int) * h->nload, cudaMemcpyDeviceToHost,
+                                        h->ctx->stream));
+        RT_CUDA(h->ctx, cudaStreamSynchronize(h->ctx->stream));
+    }
+    return RT_OK;
+}
+
+extern "C" int rt_element_compliance(rt_hier* h, const double* u_dev, float* ce_dev) {
+    if (!h || !u_dev || !ce_dev) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
+    return rtk::element_compliance(h, u_dev, ce_dev);
+}
+
 extern "C" int rt_relative_residual(rt_hier* h, double* rel) {
     if (!h || !rel) return RT_EINVAL;
     rt_level& L = h->L[0];
@@ -1545,6 +1631,7 @@ static int pcg_graph_run(rt_hier* h, double* x, double* r, bool no_support) {
     mix((uint64_t)(uintptr_t)x);
     mix((uint64_t)(uintptr_t)h->unet);
     mix(h->graph_epoch);
+    mix((uint64_t)c->wait_limit);
     mix((uint64_t)no_support);
     mix((uint64_t)h->P.precision | ((uint64_t)h->P.smoother << 8) | ((uint64_t)h->P.pre_sweeps << 16) |
         ((uint64_t)h->P.post_sweeps << 24) | ((uint64_t)h->P.cycle_gamma << 32) |
@@ -1667,6 +1754,7 @@ static int pcg32_graph_run(rt_hier* h) {
     uint64_t key = 1469598103934665603ull;
     auto mix = [&](uint64_t v) { key = (key ^ v) * 1099511628211ull; };
     mix(h->graph_epoch);
+    mix((uint64_t)c->wait_limit);
     mix((uint64_t)h->P.smoother | ((uint64_t)h->P.pre_sweeps << 8) | ((uint64_t)h->P.post_sweeps << 16) |
         ((uint64_t)h->P.cycle_gamma << 24) | ((uint64_t)h->P.coarse_sweeps << 32) | ((uint64_t)h->P.coarse_bf16 << 40));
     uint64_t om;
@@ -1723,6 +1811,10 @@ static int pcg32_core(rt_hier* h, double* x, const double* b, double tol, int ma
     RT_CHECK(pcg_prologue(h, x, b));
     double s[2];
     RT_CHECK(read_scalars(h, 21, 2, s));
+    if (!std::isfinite(s[0]) || !std::isfinite(s[1])) {
+        if (info) { info->status = RT_ENAN; info->iterations = 0; }
+        return rt_fail(h->ctx, RT_ENAN, "PCG: the right-hand side or the initial residual is not finite");
+    }
     const double bn = std::sqrt(s[1]) > 0 ? std::sqrt(s[1]) : 1.0;
     double rel = std::sqrt(s[0]) / bn;
     int it = 0;
@@ -1811,6 +1903,10 @@ static int pcg_core(rt_hier* h, double* x, const double* b, double tol, int maxi
     RT_CHECK(pcg_prologue(h, x, b));
     double s[2];
     RT_CHECK(read_scalars(h, 21, 2, s));
+    if (!std::isfinite(s[0]) || !std::isfinite(s[1])) {
+        if (info) { info->status = RT_ENAN; info->iterations = 0; }
+        return rt_fail(h->ctx, RT_ENAN, "PCG: the right-hand side or the initial residual is not finite");
+    }
     const double bn = std::sqrt(s[1]) > 0 ? std::sqrt(s[1]) : 1.0;
     double rel = std::sqrt(s[0]) / bn;
     int it = 0;

@@ -226,7 +226,8 @@ __global__ void __launch_bounds__(ST_BS, sizeof(T) == 8 ? 1 : 3) k_st_split4(int
 // L1 is not coherent across SMs.  The barrier is bounded: a block whose wait runs out sets
 // the error slot, poisons u[0] with NaN (the solve then stops on its NaN check) and returns.
 // ---------------------------------------------------------------------------
-constexpr long COOP_SPIN_LIMIT = 1L << 22;  // L2 polls (a few hundred ns each at most)
+// the polls of a wait come from the context (rt_ctx_set_wait_limit; default 1 << 22, a few hundred
+// ns each at most)
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
     unsigned v;
@@ -235,7 +236,7 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
 }
 
 // grid-wide barrier: bar[0] counts arrivals, bar[1] is the generation; gen is thread 0's copy
-__device__ __forceinline__ bool coop_grid_sync(unsigned* bar, unsigned& gen, int* s_ok) {
+__device__ __forceinline__ bool coop_grid_sync(unsigned* bar, unsigned& gen, int* s_ok, long spin_limit) {
     __syncthreads();
     if (threadIdx.x == 0) {
         bool ok = true;
@@ -248,7 +249,7 @@ __device__ __forceinline__ bool coop_grid_sync(unsigned* bar, unsigned& gen, int
         } else {
             long it = 0;
             while (ld_acquire_u32(bar + 1) == gen) {
-                if (++it > COOP_SPIN_LIMIT) {
+                if (++it > spin_limit) {
                     ok = false;
                     break;
                 }
@@ -267,7 +268,7 @@ __global__ void __launch_bounds__(ST_BS, 3) k_st_cheby_coop(int nx, int ny, int 
                                                              const S* __restrict__ st, float* u,
                                                              const float* __restrict__ f, float* tmp, float* d,
                                                              const double* __restrict__ coef, int nsteps,
-                                                             unsigned* bar, double* err) {
+                                                             unsigned* bar, double* err, long spin_limit) {
     __shared__ int s_ok;
     unsigned gen = 0;
     if (threadIdx.x == 0) gen = ld_acquire_u32(bar + 1);
@@ -339,7 +340,7 @@ __global__ void __launch_bounds__(ST_BS, 3) k_st_cheby_coop(int nx, int ny, int 
             d[oq] = dn;
         }
         if (s + 1 < nsteps || (nsteps & 1)) {
-            if (!coop_grid_sync(bar, gen, &s_ok)) {
+            if (!coop_grid_sync(bar, gen, &s_ok, spin_limit)) {
                 if (threadIdx.x == 0) {
                     *err = 2.0;
                     u[0] = __int_as_float(0x7fc00000);
@@ -367,7 +368,7 @@ __global__ void __launch_bounds__(ST_BS, 3) k_st_cheby_res(int nx, int ny, int n
                                                             const S* __restrict__ st, float* u,
                                                             const float* __restrict__ f, float* tmp, float* d,
                                                             const double* __restrict__ coef, int nsteps,
-                                                            unsigned* bar, double* err) {
+                                                            unsigned* bar, double* err, long spin_limit) {
     extern __shared__ float srow[];  // [RES_ROWS][ST_BS]
     __shared__ int s_ok;
     unsigned gen = 0;
@@ -448,7 +449,7 @@ __global__ void __launch_bounds__(ST_BS, 3) k_st_cheby_res(int nx, int ny, int n
             dq = dn;
         }
         if (s + 1 < nsteps || (nsteps & 1)) {
-            if (!coop_grid_sync(bar, gen, &s_ok)) {
+            if (!coop_grid_sync(bar, gen, &s_ok, spin_limit)) {
                 if (threadIdx.x == 0) {
                     *err = 2.0;
                     u[0] = __int_as_float(0x7fc00000);
@@ -1143,6 +1144,7 @@ int st_cheby_fused(rt_hier* h, int lvl, float* u, const float* f, float* tmp, fl
     cfg.numAttrs = 1;
     unsigned* bar = reinterpret_cast<unsigned*>(h->scal + RT_SCAL_GBAR + lvl);
     double* err = h->scal + RT_SCAL_ERR;
+    const long spin = (long)h->ctx->wait_limit;
     const bool bf = use_bf16<float>(h, L);
     cudaError_t e = cudaSuccess;
     RT_CHECK(rt_launch(h->ctx, bf ? (lvl == 1 ? "st_cheby_fused_bf16_l1" : "st_cheby_fused_bf16")
@@ -1151,19 +1153,19 @@ int st_cheby_fused(rt_hier* h, int lvl, float* u, const float* f, float* tmp, fl
                            if (resident && bf)
                                e = cudaLaunchKernelEx(&cfg, k_st_cheby_res<uint16_t>, L.nx, L.ny, L.nz,
                                                       (const uint8_t*)L.vact, (const uint16_t*)L.st16, u, f, tmp, d,
-                                                      coef, nsteps, bar, err);
+                                                      coef, nsteps, bar, err, spin);
                            else if (resident)
                                e = cudaLaunchKernelEx(&cfg, k_st_cheby_res<float>, L.nx, L.ny, L.nz,
                                                       (const uint8_t*)L.vact, (const float*)L.st32, u, f, tmp, d,
-                                                      coef, nsteps, bar, err);
+                                                      coef, nsteps, bar, err, spin);
                            else if (bf)
                                e = cudaLaunchKernelEx(&cfg, k_st_cheby_coop<uint16_t>, L.nx, L.ny, L.nz,
                                                       (const uint8_t*)L.vact, (const uint16_t*)L.st16, u, f, tmp, d,
-                                                      coef, nsteps, bar, err);
+                                                      coef, nsteps, bar, err, spin);
                            else
                                e = cudaLaunchKernelEx(&cfg, k_st_cheby_coop<float>, L.nx, L.ny, L.nz,
                                                       (const uint8_t*)L.vact, (const float*)L.st32, u, f, tmp, d,
-                                                      coef, nsteps, bar, err);
+                                                      coef, nsteps, bar, err, spin);
                        }));
     if (e != cudaSuccess)
         return rt_fail(h->ctx, RT_ECUDA, "fused Chebyshev launch failed: %s", cudaGetErrorString(e));

@@ -122,6 +122,9 @@ __global__ void k_penalty(long ne, const uint8_t* __restrict__ eact, const float
 }
 
 // element compliance sensitivity s_e = -p rho^(p-1) u_e^T KE u_e, one thread per element
+// ELEM_C = false: s_e = -p rho^(p-1) u_e.KE u_e (computeSensitivity_kernel, optimization/optimization.cu:44-107);
+// ELEM_C = true: c_e = rho^p u_e.KE u_e (elementCompliance_kernel, grid/Grid.cu:3434-3480)
+template <bool ELEM_C>
 __global__ void __launch_bounds__(FINE_BS) k_sensitivity(int nx, int ny, int nz, const uint8_t* __restrict__ eact,
                                                           const float* __restrict__ rho, float p,
                                                           const double* __restrict__ KEg, const double* __restrict__ u,
@@ -148,8 +151,12 @@ __global__ void __launch_bounds__(FINE_BS) k_sensitivity(int nx, int ny, int nz,
             for (int j = 0; j < 24; j++) kr += sKE[i * 24 + j] * ue[j];
             s += ue[i] * kr;
         }
-        const double pen = (double)(p * powf(rho[e], p - 1.f));
-        sens[e] = (float)(-s * pen);
+        if (ELEM_C) {
+            sens[e] = (float)(s * (double)powf(rho[e], p));
+        } else {
+            const double pen = (double)(p * powf(rho[e], p - 1.f));
+            sens[e] = (float)(-s * pen);
+        }
     }
 }
 
@@ -202,9 +209,16 @@ int fine_gs(rt_hier* h, T* u, const T* f, bool backward) {
 int sensitivity(rt_hier* h, const double* u) {
     rt_level& L = h->L[0];
     return rt_launch(h->ctx, "sensitivity", [&] {
-        k_sensitivity<<<fine_grid(h->ctx, L.ne), FINE_BS, 0, h->ctx->stream>>>(L.nx, L.ny, L.nz, L.eact, h->rho,
-                                                                              h->P.power_penalty, h->KE_dev, u,
-                                                                              h->sens);
+        k_sensitivity<false><<<fine_grid(h->ctx, L.ne), FINE_BS, 0, h->ctx->stream>>>(
+            L.nx, L.ny, L.nz, L.eact, h->rho, h->P.power_penalty, h->KE_dev, u, h->sens);
+    });
+}
+
+int element_compliance(rt_hier* h, const double* u, float* out) {
+    rt_level& L = h->L[0];
+    return rt_launch(h->ctx, "element_compliance", [&] {
+        k_sensitivity<true><<<fine_grid(h->ctx, L.ne), FINE_BS, 0, h->ctx->stream>>>(
+            L.nx, L.ny, L.nz, L.eact, h->rho, h->P.power_penalty, h->KE_dev, u, out);
     });
 }
 

@@ -27,6 +27,9 @@ struct rt_ctx {
     std::string err;
     int sm_count = 148;
     long long launches = 0;
+    // polls of a bounded device wait on another block (the grid barrier of the fused sweeps);
+    // rt_ctx_set_wait_limit lowers it so a test can make a wait run out
+    long long wait_limit = 1LL << 22;
     // profiling
     bool profile = false;
     // set while a batched graph is captured: its instances run concurrently, so no cooperative
@@ -322,6 +325,7 @@ int scale(rt_hier* h, long n, double* x, const double* s_dev, bool inverse_sqrt)
 int tridiag_max_eig(rt_hier* h, int k, const double* alpha_dev, const double* beta_dev, double* out_dev);
 // optimisation
 int sensitivity(rt_hier* h, const double* u);
+int element_compliance(rt_hier* h, const double* u, float* out);
 int filter(rt_hier* h, float radius);
 int oc_try(rt_hier* h, float thr, float* out, double* vol_dev);
 int oc_maxabs(rt_hier* h, float* out_dev);

@@ -17,6 +17,11 @@ from . import _capi as A
 from ._capi import check
 
 
+def _dp(t):
+    """Device pointer of a torch CUDA tensor (plumbing only)."""
+    return C.c_void_p(t.data_ptr())
+
+
 def _p(a):
     assert a.flags["C_CONTIGUOUS"]
     return a.ctypes.data
@@ -27,6 +32,7 @@ class Context:
 
     def __init__(self, device=0, stream=None):
         self._h = C.c_void_p()
+        self.device = int(device)
         check(A.lib().rt_ctx_create(device, stream, C.byref(self._h)))
 
     @property
@@ -220,6 +226,18 @@ class Grid:
     def getEact(self):
         return self._get(A.FIELD_EACT, A.LAYOUT_DENSE, self.ne, np.uint8)
 
+    def elementCompliance(self, u):
+        """Grid::elementCompliance (grid/Grid.cu:3434-3480): rho_e^p u_e.KE u_e per element (dense
+        element order) for the level-0 displacement u."""
+        assert self._layer == 0
+        import torch
+
+        ud = torch.as_tensor(np.ascontiguousarray(u, np.float64), device=f"cuda:{self._H.ctx.device}")
+        ce = torch.zeros(self.ne, dtype=torch.float32, device=ud.device)
+        self._H._c(A.lib().rt_element_compliance(self._H.handle, _dp(ud), _dp(ce)))
+        self._H.ctx.sync()
+        return ce.cpu().numpy()
+
     def reset_displacement(self):
         self.setDisplacement(np.zeros(3 * self.nv))
 
@@ -398,6 +416,99 @@ class HierarchyGrid:
         self._c(A.lib().rt_worst_case_block(self._h, block_size, n_blocks, inner_tol, seed, C.byref(lam),
                                             C.byref(info)))
         return lam.value, info
+
+    # projection API (optimization/projection.h:16-65) ---------------------------------------
+    def _dev(self, a, dtype=np.float64):
+        import torch
+
+        return torch.as_tensor(np.ascontiguousarray(a, dtype), device=f"cuda:{self.ctx.device}")
+
+    def getLoadNodes(self):
+        """getLoadNodes (optimization/projection.cpp:129-143): dense level-0 ids, increasing."""
+        n = C.c_int()
+        self._c(A.lib().rt_load_nodes(self._h, C.byref(n), None))
+        ids = np.zeros(n.value, np.int32)
+        self._c(A.lib().rt_load_nodes(self._h, C.byref(n), _p(ids)))
+        return ids
+
+    def forceProject(self, f):
+        """forceProject (optimization/projection.cu:165-231): P f for a dense [3][nv] force."""
+        fd = self._dev(f)
+        self._c(A.lib().rt_force_project(self._h, _dp(fd)))
+        self.ctx.sync()
+        return fd.cpu().numpy()
+
+    def getForceSupport(self, f):
+        """getForceSupport (optimization/projection.cu:307-338): the load-node values, [3][nload]."""
+        fd = self._dev(f)
+        n = self.getLoadNodes().size
+        import torch
+
+        fs = torch.zeros(3 * n, dtype=torch.float64, device=fd.device)
+        self._c(A.lib().rt_get_force_support(self._h, _dp(fd), _dp(fs)))
+        self.ctx.sync()
+        return fs.cpu().numpy().reshape(3, n)
+
+    def setForceSupport(self, fs):
+        """setForceSupport (optimization/projection.cu:340-369): a dense force that is fs on the load
+        nodes and zero elsewhere."""
+        import torch
+
+        fsd = self._dev(np.asarray(fs).reshape(-1))
+        f = torch.zeros(3 * self[0].nv, dtype=torch.float64, device=fsd.device)
+        self._c(A.lib().rt_set_force_support(self._h, _dp(fsd), _dp(f)))
+        self.ctx.sync()
+        return f.cpu().numpy()
+
+    def displacementProject(self, u):
+        """displacementProject (optimization/projection.cpp:374-392): u minus its rigid-mode part
+        (no-support modes)."""
+        ud = self._dev(u)
+        self._c(A.lib().rt_displacement_project(self._h, _dp(ud)))
+        self.ctx.sync()
+        return ud.cpu().numpy()
+
+    # design state files (the reference writes OpenVDB grids, grid/Grid.cpp:727-839, and raw
+    # vectors, utils/binaryIO.h) -------------------------------------------------------------
+    def write_state(self, path, fields=("rho", "u", "f"), **meta):
+        """Writes the level-0 fields as .npy files into directory ``path`` with a manifest.json
+        (grid sizes, field files, the activity checksum and ``meta``: e.g. the iteration and the
+        worst-case eigenvalue).  Returns the manifest."""
+        import hashlib
+        import json
+        import os
+
+        os.makedirs(path, exist_ok=True)
+        g0 = self[0]
+        get = {"rho": g0.getRho, "u": g0.getDisplacement, "f": g0.getForce, "sens": g0.getSens}
+        files = {}
+        for name in fields:
+            np.save(os.path.join(path, f"{name}.npy"), get[name]())
+            files[name] = f"{name}.npy"
+        man = {"format": "robtop_b200 state 1", "dims": [g0.nx, g0.ny, g0.nz], "n_levels": self.n_grid(),
+               "mode": int(self.params.mode), "eact_sha1": hashlib.sha1(g0.getEact().tobytes()).hexdigest(),
+               "fields": files, "meta": meta}
+        with open(os.path.join(path, "manifest.json"), "w") as fp:
+            json.dump(man, fp, indent=1)
+        return man
+
+    def read_state(self, path):
+        """Loads a state written by write_state into this hierarchy (same grid); returns the manifest."""
+        import hashlib
+        import json
+        import os
+
+        with open(os.path.join(path, "manifest.json")) as fp:
+            man = json.load(fp)
+        g0 = self[0]
+        if man.get("format") != "robtop_b200 state 1" or man["dims"] != [g0.nx, g0.ny, g0.nz]:
+            raise ValueError(f"{path}: not a state of a {g0.nx}x{g0.ny}x{g0.nz} grid")
+        if man["eact_sha1"] != hashlib.sha1(g0.getEact().tobytes()).hexdigest():
+            raise ValueError(f"{path}: written for a different solid")
+        put = {"rho": g0.setRho, "u": g0.setDisplacement, "f": g0.setForce, "sens": g0.setSens}
+        for name, fn in man["fields"].items():
+            put[name](np.load(os.path.join(path, fn)))
+        return man
 
     def workspace(self):
         """A solve workspace sharing this hierarchy's operator (rt_hier_workspace_create)."""

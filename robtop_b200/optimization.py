@@ -219,13 +219,41 @@ def updateDensities(Vgoal):
     return lam.value
 
 
-def optimization(max_iter=100, worst=modifiedPM):
-    """optimization/optimization.cpp:583-673 without file output; returns the compliance record."""
-    initDensities(params.volume_ratio)
+def setOutpurDir(dirname):
+    """optimization/optimization.cpp (setOutpurDir): where optimization() writes its checkpoints."""
+    _state["outdir"] = dirname
+
+
+def writeDensity(path):
+    """The design state (densities, displacement, force) as .npy files with a manifest
+    (HierarchyGrid::writeDensity, grid/Grid.cpp:727-764, writes an OpenVDB grid instead)."""
+    return getGrids().write_state(path, iteration=_state.get("iteration", 0), records=_state["records"])
+
+
+def readDensity(path):
+    """Loads a state written by writeDensity (HierarchyGrid::readDensity, grid/Grid.cpp:809-839)."""
+    man = getGrids().read_state(path)
+    _state["records"] = list(man["meta"].get("records", []))
+    _state["iteration"] = int(man["meta"].get("iteration", 0))
+    return man
+
+
+def optimization(max_iter=100, worst=modifiedPM, checkpoint_every=0, resume=None):
+    """optimization/optimization.cpp:583-673; returns the compliance record.  With
+    ``checkpoint_every`` = n > 0 the state is written every n iterations into
+    <output dir>/iter_<k> (setOutpurDir); ``resume`` = such a directory continues from it."""
+    import os
+
+    rec, start = [], 1
+    if resume:
+        readDensity(resume)
+        rec, start = list(_state["records"]), _state["iteration"] + 1
+    else:
+        initDensities(params.volume_ratio)
     Vgoal = params.volume_ratio
-    rec = []
     small = 0
-    for itn in range(1, max_iter + 1):
+    for itn in range(start, max_iter + 1):
+        _state["iteration"] = itn
         Vgoal = max(Vgoal * (1 - params.volume_decrease), params.volume_ratio)
         update_stencil()
         c = worst()
@@ -238,6 +266,9 @@ def optimization(max_iter=100, worst=modifiedPM):
             break
         computeSensitivity()
         updateDensities(Vgoal)
+        _state["records"] = rec
+        if checkpoint_every and itn % checkpoint_every == 0:
+            writeDensity(os.path.join(_state.get("outdir", "."), f"iter_{itn}"))
     _state["records"] = rec
     return rec
 

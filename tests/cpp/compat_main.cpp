@@ -4,6 +4,7 @@
 // "key value" lines for tests/test_gpu_compat.py to compare with the oracle.
 #include <cmath>
 #include <cstdio>
+#include <string>
 #include <vector>
 
 #include "../../robtop_b200/csrc/robtop_compat.h"
@@ -36,6 +37,57 @@ int main(int argc, char** argv) {
     printf("rel_residual %.17g\n", getGrids()[0]->relative_residual());
     const double mu = modifiedPM();
     printf("worst_compliance %.17g\n", mu);
+    // the adjoint identity of checkAdjointVariable (optimization/optimization.cu:353-402) holds for
+    // N^T lambda = 2 u_w - 2 mu f_w; a zero vector fails it
+    grid::Grid* g0 = getGrids()[0];
+    g0->v3_add(2.0, g0->getDisplacement(), -2.0 * mu, g0->getForce());
+    printf("adjoint_ok %d\n", checkAdjointVariable() ? 1 : 0);
+    g0->reset_displacement();
+    printf("adjoint_zero_ok %d\n", checkAdjointVariable() ? 1 : 0);
+    // element compliance of the worst-case displacement sums to u.K u
+    const double mu2 = modifiedPM();
+    float* ce = (float*)gpu_manager.add_buf("element compliance", sizeof(float) * nx * ny * nz);
+    g0->elementCompliance(g0->getDisplacement(), ce);
+    std::vector<float> ceh((size_t)nx * ny * nz);
+    gpu_manager_t::download_buf(ceh.data(), ce, sizeof(float) * ceh.size());
+    gpu_manager.delete_buf(ce);
+    double csum = 0;
+    for (float v : ceh) csum += v;
+    printf("element_compliance_sum %.17g\n", csum);
+    printf("worst_compliance2 %.17g\n", mu2);
+    // projection API (wsff: the projection keeps the load-node values, zeroes every other node)
+    printf("n_loadnodes %d\n", n_loadnodes());
+    std::vector<double> fs[3];
+    getForceSupport(g0->getForce(), fs);
+    double fs2 = 0;
+    for (int c = 0; c < 3; c++)
+        for (double v : fs[c]) fs2 += v * v;
+    printf("support_norm2 %.17g\n", fs2);
+    printf("pnorm %.17g\n", Pnorm(g0->getForce()));
+    forceProject(g0->getForce());
+    printf("projected_norm2 %.17g\n", g0->v3_dot(g0->getForce(), g0->getForce()));
+    double* fsd = (double*)gpu_manager.add_buf(sizeof(double) * 3 * n_loadnodes());
+    double* fsp[3] = {fsd, fsd + n_loadnodes(), fsd + 2 * n_loadnodes()};
+    getForceSupport(g0->getForce(), fsp);
+    g0->reset_force();
+    setForceSupport(fsp, g0->getForce());
+    printf("restored_norm2 %.17g\n", g0->v3_dot(g0->getForce(), g0->getForce()));
+    gpu_manager.delete_buf(fsd);
+    // the Rayleigh quotient R(u) = |P u|^2 / u.K u of the worst-case displacement and its gradient
+    const long long nvb = g0->n_box_nodes();
+    double* gm = (double*)gpu_manager.add_buf("gradient", sizeof(double) * 3 * nvb);
+    double* gv[3] = {gm, gm + nvb, gm + 2 * nvb};
+    const double mu3 = modifiedPM();
+    const auto pk = RayleighGradient(g0->getDisplacement(), gv);
+    printf("rayleigh_pnorm %.17g\n", pk.first);
+    printf("rayleigh_knorm %.17g\n", pk.second);
+    printf("rayleigh_grad_norm %.17g\n", g0->v3_norm(gv));
+    printf("worst_compliance3 %.17g\n", mu3);
+    gpu_manager.delete_buf(gm);
+    // the incomplete power method and the preconditioned eigen-iteration
+    printf("incomplete_pm %.17g\n", inCompleteModiPM(1e-2));
+    printf("mgpsor %.17g\n", MGPSOR());
+    selfTest();
     computeSensitivity();
     const float g = updateDensities(0.4f);
     printf("oc_multiplier %.9g\n", g);
@@ -44,6 +96,15 @@ int main(int argc, char** argv) {
     double s = 0;
     for (float r : rho) s += r;
     printf("volume %.9g\n", s / rho.size());
+    // density file round trip (writeDensity / readDensity)
+    setOutpurDir("/tmp");
+    const std::string dfile = getOutputDir() + "/rtb200_density_test.bin";
+    getGrids().writeDensity(dfile);
+    initDensities(0.9);
+    getGrids().readDensity(dfile);
+    std::vector<float> rho2(rho.size());
+    rt_get(getGrids().hier(), RT_FIELD_RHO, 0, RT_LAYOUT_DENSE, rho2.data());
+    printf("density_roundtrip %d\n", rho2 == rho ? 1 : 0);
     // the mesh form of buildGrids (optimization/optimization.cpp:14-19): a 24 x 12 x 12 box
     // of 12 triangles, voxelised at gridreso R - 1 (cube 32^3)
     setParameters(0.4f, 0.0f, 0.03f, 2.0f, 0.5f, 3.0f, 1e-3f, R - 1, 1e6f, 0.4f, 0.0f, false, false);

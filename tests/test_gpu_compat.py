@@ -23,6 +23,8 @@ def run_driver():
         if line.startswith("-- u_rigid"):
             rigid.append(float(line.split("=")[1]))
             continue
+        if line.startswith("--"):
+            continue
         k, v = line.split()
         vals[k] = float(v)
     return vals, rigid
@@ -60,3 +62,28 @@ def test_compat_flow_matches_oracle():
     R, bmin, bmax, unit = O.voxel_box(v, 31)
     assert vals["mesh_elements"] == O.bits_total(O.voxelize_solid(v, f, R, bmin, unit)) > 0
     assert vals["mesh_levels"] >= 2
+
+
+def test_compat_remaining_entry_points():
+    """The projection API (optimization/projection.h:16-65), Grid::elementCompliance,
+    checkAdjointVariable, RayleighGradient, inCompleteModiPM, MGPSOR, selfTest and the density
+    file round trip, driven through the reference-signature layer."""
+    vals, rigid = run_driver()
+    assert vals["adjoint_ok"] == 1 and vals["adjoint_zero_ok"] == 0
+    # element compliances sum to u.K u = f.u of the worst-case pair
+    assert abs(vals["element_compliance_sum"] - vals["worst_compliance2"]) <= 1e-5 * vals["worst_compliance2"]
+    cfg = configs.cantilever(24, 12, 12)
+    assert vals["n_loadnodes"] == cfg["load_nodes"].size
+    # wsff: the support force of the unit worst-case load has norm 1 and P keeps it
+    assert abs(vals["support_norm2"] - 1.0) <= 1e-9
+    assert abs(vals["pnorm"] - 1.0) <= 1e-9
+    assert abs(vals["projected_norm2"] - 1.0) <= 1e-9
+    assert abs(vals["restored_norm2"] - 1.0) <= 1e-9
+    # at the worst-case displacement u = K^-1 f (|f| = 1): |P u|^2 / u.K u = lambda
+    lam = vals["worst_compliance3"]
+    assert abs(vals["rayleigh_pnorm"] / vals["rayleigh_knorm"] - lam) <= 1e-3 * lam
+    # the incomplete power method reaches the worst case to within its 1e-2 force-change threshold
+    assert 0.9 * lam <= vals["incomplete_pm"] <= lam * (1 + 1e-6)
+    assert abs(vals["mgpsor"] - lam) <= 1e-2 * lam
+    assert vals["density_roundtrip"] == 1
+    assert len(rigid) == 6

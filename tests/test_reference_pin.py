@@ -59,8 +59,9 @@ def test_oracle_matches_reference_kernel_outputs(name):
     g = np.load(KERNEL_FIXTURE)
     mine, eact = _oracle_outputs(name)
     ref = {k: g[f"{name}/{k}"] for k in ("applyK", "sensitivity", "oc_try", "filter")}
-    # K u: the same FP64 sums in another order
-    assert np.abs(mine["applyK"] - ref["applyK"]).max() <= 1e-12 * np.abs(ref["applyK"]).max()
+    # K u: the same FP64 sums in another order; the element weights rho^p come from C's powf here
+    # and CUDA's in the reference, which may differ by an ulp (2^-24) where rho varies
+    assert np.abs(mine["applyK"] - ref["applyK"]).max() <= 1e-6 * np.abs(ref["applyK"]).max()
     # sensitivities: the reference adds FP32 partial sums with atomicAdd (order varies), the oracle
     # sums in FP64 and rounds once
     act = eact.astype(bool)
