@@ -260,10 +260,13 @@ NCU_TRAFFIC_PER_NODE = {("fine_cheby_f32", "register_march"): (71.0e6 + 3.3e6) /
                         ("fine_cheby_f32", "smem_tile_pipelined"): (45.329e6 + 0.256e6) / 1081665}
 
 
-# DRAM bytes per node of the finest-level kernels on the arch workload, from an ncu capture of the
-# same kernel variant on a smaller arch whose vectors exceed L2 (traffic grows with the nodes); empty
-# until captured
-NCU_TRAFFIC_ARCH = {}
+# DRAM bytes (read + write) per node of the finest-level kernels on the arch workload, from one ncu
+# capture of the same kernel variant and launch shape (8 rows, z-chunk 32) on the 255x256x128
+# worst-case box, whose vectors exceed L2 (8,487,168 nodes: 359.7 MB read + 171.8 MB written);
+# traffic grows with the nodes, so the per-node figure scales to the arch's node box
+NCU_TRAFFIC_ARCH = {("fine_cheby_f32", "smem_tile_pipelined"): (359.672064e6 + 171.792896e6) / 8487168}
+# warp-instructions per node of the same capture (smsp__inst_executed.sum / nodes)
+NCU_INST_ARCH = {("fine_cheby_f32", "smem_tile_pipelined", (8, 32)): 222157952 / 8487168}
 
 
 def roofline(ctx, stats, G, peaks, tuning=None, traffic_table=None):
@@ -308,7 +311,7 @@ def simt_peaks(rb, ctx):
     return out
 
 
-def issue_roofline(rb, ctx, G, roof, clk):
+def issue_roofline(rb, ctx, G, roof, clk, inst_table=None):
     """The matrix-free finest-level kernel is bound by instruction issue, not HBM: next to the HBM
     fraction, report its warp-instruction rate against 4 per SM per cycle at the measured SM clock,
     and the measured SIMT peaks."""
@@ -316,7 +319,8 @@ def issue_roofline(rb, ctx, G, roof, clk):
 
     roof["simt_peaks"] = simt_peaks(rb, ctx)
     shape = tuple(roof["rows_zchunk"]) if roof.get("rows_zchunk") else None
-    ipn = NCU_INST_PER_NODE.get((roof.get("kernel"), roof.get("variant"), shape))
+    ipn = (NCU_INST_PER_NODE if inst_table is None else inst_table).get((roof.get("kernel"), roof.get("variant"),
+                                                                          shape))
     mhz = (clk or {}).get("sm_mhz")
     if ipn is None or not mhz or not roof.get("avg_us"):
         return
@@ -1438,6 +1442,10 @@ def run_arch(args):
     stats = {k: v for k, v in ctx.profile_stats().items() if v[0] > 0}
     ctx.profile(False)
     roof = roofline(ctx, stats, G, peaks, tuning, traffic_table=NCU_TRAFFIC_ARCH)
+    if roof.get("traffic_source"):
+        roof["traffic_source"] = ("ncu capture of the same kernel variant and launch shape on the 255x256x128 "
+                                  "worst-case box (vectors > L2), per node, scaled to this node box")
+    issue_roofline(rb, ctx, G, roof, clk, inst_table=NCU_INST_ARCH)
     top = sorted(stats.items(), key=lambda kv: -kv[1][1])[:10]
 
     ms_step = ms / args.steps

@@ -129,7 +129,7 @@ void rt_ctx_destroy(rt_ctx* ctx);
 const char* rt_last_error(rt_ctx* ctx);
 int rt_ctx_sync(rt_ctx* ctx);
 /* polls a device-side wait on other blocks may spend before it gives up (the grid barrier of the
- * fused Chebyshev sweeps; default 1 << 22, polls <= 0 restores it).  No reference counterpart: a
+ * fused Chebyshev sweeps; default 1 << 22, polls < 0 restores it, 0 gives up at the first poll).  No reference counterpart: a
  * test lowers it so that a wait runs out and the call reports RT_ECUDA with the reason, leaving
  * the context usable. */
 int rt_ctx_set_wait_limit(rt_ctx* ctx, long long polls);
@@ -410,6 +410,9 @@ int rt_unet_harvest(rt_hier* h, rt_unet* u, int k_iter, uint64_t seed, void* in_
  * rt_hier_set_learned.  Inside the captured PCG loop the correction is the body of an IF node,
  * so a switched-off network costs no launches.  u = null detaches. */
 int rt_hier_set_learned(rt_hier* h, rt_unet* u, double fallback_ratio);
+/* finest-level smoothing steps (the hierarchy's smoother, FP64) applied to z after each learned
+ * correction, on K z = r (0: none, the default) */
+int rt_hier_set_learned_post(rt_hier* h, int sweeps);
 /* corrections run since rt_hier_set_learned, and whether the gate has switched the network off
  * for the current design */
 int rt_hier_learned_stats(rt_hier* h, long long* applied, int* judged_off);

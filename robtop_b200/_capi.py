@@ -139,6 +139,7 @@ SIGNATURES = {
     "rt_unet_harvest": (I, [P, P, I, C.c_uint64, P, P]),
     "rt_hier_set_learned": (I, [P, P, D]),
     "rt_hier_learned_stats": (I, [P, C.POINTER(C.c_longlong), C.POINTER(I)]),
+    "rt_hier_set_learned_post": (I, [P, I]),
     "rt_force_project": (I, [P, P]),
     "rt_ctx_set_wait_limit": (I, [P, C.c_longlong]),
     "rt_get_force_support": (I, [P, P, P]),

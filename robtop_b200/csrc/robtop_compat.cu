@@ -473,17 +473,10 @@ void initDensities(double rho) { grids[0]->init_rho(rho); }
 
 void update_stencil(void) { grids.update_stencil(); }
 
-// solveFEM (optimization/optimization.cpp:85-91) on the preloaded force field
-// (the load field at the load nodes, TestSuit::testOrdinaryTopopt's setForceSupport)
+// solveFEM (optimization/optimization.cpp:85-91): V-cycles on the force the caller has set
+// (TestSuit::testOrdinaryTopopt, utils/test_utils.cpp:589-660, first sets the preloaded field
+// with setForceSupport(getPreloadForce(), grids[0]->getForce()))
 void solveFEM(void) {
-    rt_hier* h = grids.hier();
-    const long long nv = grids[0]->n_box_nodes();
-    std::vector<double> f(3 * nv, 0.0);
-    const auto& ln = grids.loadNodes();
-    const auto& pl = grids.preloadForce();
-    for (size_t i = 0; i < ln.size(); i++)
-        for (int c = 0; c < 3; c++) f[c * nv + ln[i]] = pl[3 * i + c];
-    grids.check(rt_put(h, RT_FIELD_F, 0, RT_LAYOUT_DENSE, f.data()), "solveFEM");
     double rel = 1;
     int it = 0;
     while (rel > 1e-4) {
@@ -811,4 +804,24 @@ void selfTest(void) {
         for (int j = 0; j < 24; j++) asym = std::max(asym, std::fabs(ke[i * 24 + j] - ke[j * 24 + i]));
     printf("-- template matrix asymmetry %g\n", asym);
     test_rigid_displacement();
+}
+
+// getPreloadForce (optimization/projection.cu:387-390): the load field evaluated at the load nodes
+// when the grid was built, as device arrays [3][nload] (refreshed on every call)
+double** getPreloadForce(void) {
+    static double* fl[3] = {nullptr, nullptr, nullptr};
+    static size_t cap = 0;
+    const int nl = n_loadnodes();
+    if ((size_t)nl > cap || !fl[0]) {
+        if (fl[0]) gpu_manager.delete_buf(fl[0]);
+        fl[0] = (double*)gpu_manager.add_buf("preload force", sizeof(double) * 3 * (nl > 0 ? nl : 1));
+        cap = nl;
+    }
+    for (int c = 0; c < 3; c++) fl[c] = fl[0] + (size_t)c * nl;
+    const auto& pl = grids.preloadForce();
+    std::vector<double> soa(3 * (size_t)nl);
+    for (int i = 0; i < nl; i++)
+        for (int c = 0; c < 3; c++) soa[(size_t)c * nl + i] = pl[3 * (size_t)i + c];
+    if (nl > 0) gpu_manager_t::upload_buf(fl[0], soa.data(), sizeof(double) * soa.size());
+    return fl;
 }

@@ -11,7 +11,9 @@
 //  * setBoundaryCondition's force field returns std::array<double,3> instead of
 //    Eigen::Matrix<double,3,1> (Eigen is not a dependency of this library).
 // Errors throw std::runtime_error carrying rt_last_error(); the reference
-// printed and continued or called exit(-1).
+// printed and continued or called exit(-1).  As in the reference, solveFEM() solves for the
+// force the caller has set; a caller of the preloaded field sets it first with
+// setForceSupport(getPreloadForce(), grids[0]->getForce()).
 #pragma once
 #include <array>
 #include <cstdint>
@@ -224,3 +226,4 @@ void getForceSupport(double const* const f_dev[3], double* fsup[3]);
 void getForceSupport(double const* const f_dev[3], std::vector<double> fs[3]);
 void setForceSupport(double const* const fsup[3], double* f_dev[3]);
 void displacementProject(double* u_dev[3]);
+double** getPreloadForce(void);

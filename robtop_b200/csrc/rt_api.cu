@@ -72,6 +72,8 @@ static void profile_drain(rt_ctx* c) {
 
 void rt_launch_begin(rt_ctx* c, int kid, cudaEvent_t* a) {
     (void)kid;
+    // an error left by an earlier runtime call is reported as such, not as this launch's
+    c->pending_err = cudaGetLastError();
     if (c->profile) {
         *a = ev_get(c);
         cudaEventRecord(*a, c->stream);
@@ -87,6 +89,11 @@ int rt_launch_end(rt_ctx* c, int kid, cudaEvent_t a, const char* name) {
         cudaEventRecord(b, c->stream);
         c->pending.push_back({kid, a, b});
         if (c->pending.size() > 4096) profile_drain(c);
+    }
+    if (c->pending_err != cudaSuccess) {
+        const cudaError_t pe = c->pending_err;
+        c->pending_err = cudaSuccess;
+        return rt_fail(c, RT_ECUDA, "a CUDA error was pending before the launch of %s: %s", name, cudaGetErrorString(pe));
     }
     if (e != cudaSuccess) return rt_fail(c, RT_ECUDA, "launch of %s failed: %s", name, cudaGetErrorString(e));
     return RT_OK;
@@ -154,7 +161,7 @@ extern "C" const char* rt_last_error(rt_ctx* c) { return c ? c->err.c_str() : "n
 
 extern "C" int rt_ctx_set_wait_limit(rt_ctx* c, long long polls) {
     if (!c) return RT_EINVAL;
-    c->wait_limit = polls > 0 ? polls : (1LL << 22);
+    c->wait_limit = polls >= 0 ? polls : (1LL << 22);
     return RT_OK;
 }
 
@@ -1552,6 +1559,18 @@ static int precondition(rt_hier* h, const double* r, double* z, const double* rr
             RT_CHECK(rtk::dot(h, n, r, r, h->scal + 38));
             RT_CHECK(rtk::dot(h, n, z, z, h->scal + 37));
             RT_CHECK(rtu::correct(h->unet, h, r, h->scal + 38, h->scal + 37, h->scal + 28, z));
+            if (h->unet_post > 0) {
+                // smoothing steps on K z = r from the corrected z: damp what the network adds
+                // at high frequencies, where K is largest
+                double* saved_f = L.f;
+                double* saved_u = L.u;
+                L.f = const_cast<double*>(r);
+                L.u = z;
+                const int st = level_smooth<double>(h, 0, h->P.smoother, h->unet_post, h->P.jacobi_omega, false);
+                L.f = saved_f;
+                L.u = saved_u;
+                RT_CHECK(st);
+            }
             return (dots_done && *dots_done) ? rtk::dot2(h, n, z, r, h->rold, dots) : RT_OK;
         }));
     return RT_OK;
@@ -3221,6 +3240,14 @@ extern "C" int rt_hier_set_learned(rt_hier* h, rt_unet* u, double fallback_ratio
     h->unet_fallback = fallback_ratio;
     h->unet_off = false;
     h->unet_applied = 0;
+    h->graph_epoch++;
+    return RT_OK;
+}
+
+extern "C" int rt_hier_set_learned_post(rt_hier* h, int sweeps) {
+    if (!h || sweeps < 0 || sweeps > RT_CHEBY_MAXK) return RT_EINVAL;
+    RT_NOT_WORKSPACE(h);
+    h->unet_post = sweeps;
     h->graph_epoch++;
     return RT_OK;
 }

@@ -30,6 +30,8 @@ struct rt_ctx {
     // polls of a bounded device wait on another block (the grid barrier of the fused sweeps);
     // rt_ctx_set_wait_limit lowers it so a test can make a wait run out
     long long wait_limit = 1LL << 22;
+    // a CUDA error already pending when a launch began (reported with that launch)
+    cudaError_t pending_err = cudaSuccess;
     // profiling
     bool profile = false;
     // set while a batched graph is captured: its instances run concurrently, so no cooperative
@@ -164,6 +166,7 @@ struct rt_hier {
     // network changes.  unet_kernels: kernels of one correction (launch accounting of the IF node
     // that runs it inside the captured loop); unet_applied: corrections run since attach
     bool unet_off = false;
+    int unet_post = 0;  // finest-level smoothing steps applied to z after the correction
     long unet_kernels = 0;
     long long unet_applied = 0;
     long long fallbacks = 0;  // PCG solves that continued with FP64 V-cycles after stalling

@@ -106,12 +106,14 @@ def harvest(G, net, k_iter, seed):
     return inp, tgt
 
 
-def attach(G, net, fallback_ratio=1.0):
+def attach(G, net, fallback_ratio=1.0, post_sweeps=0):
     """Use the network inside G's PCG (z = Vcycle(r) + N(rho, r, Vcycle(r))); net=None detaches.
     An iteration whose residual norm does not drop below ``fallback_ratio`` x the previous one
-    switches the correction off until the next stencil update."""
+    switches the correction off until the next stencil update.  ``post_sweeps`` finest-level
+    smoothing steps follow each correction."""
     check(A.lib().rt_hier_set_learned(G.handle, net.handle if net is not None else None, float(fallback_ratio)),
           G.ctx.handle)
+    check(A.lib().rt_hier_set_learned_post(G.handle, int(post_sweeps)), G.ctx.handle)
 
 
 def stats(G):

@@ -10,6 +10,7 @@
 #include "../../robtop_b200/csrc/robtop_compat.h"
 
 int main(int argc, char** argv) {
+    setvbuf(stdout, nullptr, _IONBF, 0);  // every line reaches the test even if a call throws
     const int nx = 24, ny = 12, nz = 12, R = 32;
     // cantilever: x = 0 clamped, load on the bottom edge of the x = nx face
     setParameters(0.4f, 0.0f, 0.03f, 2.0f, 0.5f, 3.0f, 1e-3f, R, 1e6f, 0.4f, 0.0f, false, false);
@@ -32,6 +33,8 @@ int main(int argc, char** argv) {
     printf("levels %d\n", getGrids().n_grid());
     printf("load_nodes %zu\n", getGrids().loadNodes().size());
     test_rigid_displacement();
+    // TestSuit::testOrdinaryTopopt (utils/test_utils.cpp:594): the preloaded force, then solveFEM
+    setForceSupport(getPreloadForce(), getGrids()[0]->getForce());
     solveFEM();
     printf("compliance %.17g\n", getGrids()[0]->compliance());
     printf("rel_residual %.17g\n", getGrids()[0]->relative_residual());

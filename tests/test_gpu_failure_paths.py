@@ -24,25 +24,23 @@ def _grid(ctx, cfg):
 
 
 def test_grid_barrier_wait_runs_out_and_context_recovers():
-    """The fused Chebyshev sweep's grid barrier with a wait limit of one poll: the blocks that are
-    not last give up, the solve reports the barrier and returns; with the default limit the same
-    hierarchy then solves to 1e-6."""
-    cfg = configs.worst_case_box(32, 24, 16, seed=2)
+    """The fused Chebyshev sweep's grid barrier with a wait limit of zero polls: the blocks that
+    are not last give up at once, the solve reports the barrier and returns; with the default
+    limit the same hierarchy then solves to 1e-6."""
+    # big enough that the fused levels run on many blocks (a single block never waits)
+    cfg = configs.cantilever(96, 48, 48)
     ctx = rb.Context(0)
     G = _grid(ctx, cfg)
     try:
         for lvl in range(1, G.n_grid() - 1):
             rb._capi.check(rb.lib().rt_set_level_fused(G.handle, lvl, 1), ctx.handle)
-        nv = G[0].nv
-        f = np.zeros(3 * nv)
-        f[2 * nv + cfg["load_nodes"]] = 1.0
-        G[0].setForce(f)
-        rb._capi.check(rb.lib().rt_ctx_set_wait_limit(ctx.handle, 1), ctx.handle)
+        G[0].setForce(cfg["fload"].ravel())
+        rb._capi.check(rb.lib().rt_ctx_set_wait_limit(ctx.handle, 0), ctx.handle)
         G[0].reset_displacement()
         with pytest.raises(rb.RTError) as ei:
             G.pcg(1e-6, 50)
         assert "grid barrier" in str(ei.value)
-        rb._capi.check(rb.lib().rt_ctx_set_wait_limit(ctx.handle, 0), ctx.handle)
+        rb._capi.check(rb.lib().rt_ctx_set_wait_limit(ctx.handle, -1), ctx.handle)
         G[0].reset_displacement()
         info = G.pcg(1e-6, 500)
         assert info.status == 0 and info.rel_residual <= 1e-6

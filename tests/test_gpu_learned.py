@@ -1,11 +1,17 @@
 """The learned preconditioner end to end (GPU): samples harvested from the solver, training
-on the library's own forward/backward kernels, and MG-PCG with z = Vcycle(r) + N(rho, r)
-on a held-out density, against the same PCG without the network.
+on the library's own forward/backward kernels, and MG-PCG with z = Vcycle(r) + N(rho, r, Vcycle(r))
+on held-out densities, against the same PCG without the network.
 
-What the network gains is measured and written to ``learned_gain.json`` in the pytest
-temporary directory; the tests assert what must hold whatever the gain: training lowers the
-loss, the learned PCG converges to the same tolerance and solution, and the fallback gate
-turns the correction off when the residual stops dropping.
+What the network gains is measured here, per held-out density, as the ratio of PCG iterations
+without and with it.  Measured on a B200 with this test's training and with larger runs (up to
+12 densities x 5 residual depths and 800 Adam steps, final loss 0.09-0.15 of the target
+variance on 24x16x16 and 32x32x32 boxes): the gain is below 1 (34 -> 36 iterations here).  Applied at
+every iteration with the gate held open, the correction alone keeps flexible CG from converging
+within 500 iterations: the network's error is small in the Euclidean norm it is trained in but
+not in the energy norm that CG measures.  So the test asserts what the gate guarantees instead
+of a gain: the gated learned PCG converges to the same tolerance and solution, and costs at most
+one iteration's worth of extra steps over the plain method.  The measured gains are printed and
+written to ``learned_gain.json`` in the pytest temporary directory.
 """
 import json
 
@@ -77,6 +83,10 @@ def test_learned_pcg_converges_and_reports_gain(trained, tmp_path):
     assert plain.status == rb._capi.RT_OK and lrn.status == rb._capi.RT_OK
     assert lrn.rel_residual <= 1e-6
     assert np.linalg.norm(u_lrn - u_plain) <= 1e-4 * np.linalg.norm(u_plain)
+    # the gate's bound: the network is switched off after the first iteration it does not pay
+    assert lrn.iterations <= plain.iterations + 3
+    applied, judged_off = learned.stats(G)
+    assert applied >= 1
     # the gate: a ratio no iteration can meet turns the correction off after one iteration
     learned.attach(G, net, fallback_ratio=1e-12)
     G[0].setDisplacement(np.zeros_like(f))
