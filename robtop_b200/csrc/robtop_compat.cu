@@ -15,6 +15,14 @@ grid::HierarchyGrid grids;
 gpu_manager_t gpu_manager;
 
 // mem/gpu_manager_t.cu: named device buffers, freed with the manager
+// a failed runtime call in the shim ends the calling function with the runtime's message
+static void ck_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
 void gpu_manager_t::upload_buf(void* dst, const void* src, size_t size) {
     if (cudaMemcpy(dst, src, size, cudaMemcpyHostToDevice) != cudaSuccess) throw std::runtime_error("upload_buf failed");
 }
@@ -217,13 +225,13 @@ void Grid::applyK(double* u[3], double* f[3]) {
     cudaStream_t s = h->ctx->stream;
     const double* uin = u[0];
     if (!contiguous(u, _nv)) {
-        for (int c = 0; c < 3; c++) cudaMemcpyAsync(h->x + c * _nv, u[c], sizeof(double) * _nv, cudaMemcpyDeviceToDevice, s);
+        for (int c = 0; c < 3; c++) ck_cuda(cudaMemcpyAsync(h->x + c * _nv, u[c], sizeof(double) * _nv, cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync");
         uin = h->x;
     }
     double* out = contiguous(f, _nv) ? f[0] : h->q;
     _H->check(rt_apply_K_dev(h, uin, out), "applyK");
     if (out == h->q)
-        for (int c = 0; c < 3; c++) cudaMemcpyAsync(f[c], h->q + c * _nv, sizeof(double) * _nv, cudaMemcpyDeviceToDevice, s);
+        for (int c = 0; c < 3; c++) ck_cuda(cudaMemcpyAsync(f[c], h->q + c * _nv, sizeof(double) * _nv, cudaMemcpyDeviceToDevice, s), "cudaMemcpyAsync");
 }
 
 double Grid::compliance(void) {
@@ -253,13 +261,13 @@ double Grid::unitizeForce(void) {
 }
 
 void Grid::reset_displacement(void) {
-    for (int c = 0; c < 3; c++) cudaMemsetAsync(_U[c], 0, sizeof(double) * _nv, _H->hier()->ctx->stream);
+    for (int c = 0; c < 3; c++) ck_cuda(cudaMemsetAsync(_U[c], 0, sizeof(double) * _nv, _H->hier()->ctx->stream), "cudaMemsetAsync");
 }
 void Grid::reset_force(void) {
-    for (int c = 0; c < 3; c++) cudaMemsetAsync(_F[c], 0, sizeof(double) * _nv, _H->hier()->ctx->stream);
+    for (int c = 0; c < 3; c++) ck_cuda(cudaMemsetAsync(_F[c], 0, sizeof(double) * _nv, _H->hier()->ctx->stream), "cudaMemsetAsync");
 }
 void Grid::reset_residual(void) {
-    for (int c = 0; c < 3; c++) cudaMemsetAsync(_R[c], 0, sizeof(double) * _nv, _H->hier()->ctx->stream);
+    for (int c = 0; c < 3; c++) ck_cuda(cudaMemsetAsync(_R[c], 0, sizeof(double) * _nv, _H->hier()->ctx->stream), "cudaMemsetAsync");
 }
 float* Grid::getRho(void) { return _layer == 0 ? _H->hier()->rho : nullptr; }
 float* Grid::getSens(void) { return _layer == 0 ? _H->hier()->sens : nullptr; }
@@ -270,8 +278,8 @@ double Grid::v3_dot(double* v[3], double* u[3]) {
     for (int c = 0; c < 3; c++) {
         _H->check(rtk::dot(h, _nv, v[c], u[c], h->scal + 80 + c), "v3_dot");
     }
-    cudaMemcpyAsync(h->ctx->hscal, h->scal + 80, sizeof(double) * 3, cudaMemcpyDeviceToHost, h->ctx->stream);
-    cudaStreamSynchronize(h->ctx->stream);
+    ck_cuda(cudaMemcpyAsync(h->ctx->hscal, h->scal + 80, sizeof(double) * 3, cudaMemcpyDeviceToHost, h->ctx->stream), "cudaMemcpyAsync");
+    ck_cuda(cudaStreamSynchronize(h->ctx->stream), "cudaStreamSynchronize");
     for (int c = 0; c < 3; c++) tot += h->ctx->hscal[c];
     return tot;
 }
@@ -280,14 +288,14 @@ double Grid::v3_norm(double* v[3]) { return std::sqrt(v3_dot(v, v)); }
 
 void Grid::v3_copy(double* vsrc[3], double* vdst[3]) {
     for (int c = 0; c < 3; c++)
-        cudaMemcpyAsync(vdst[c], vsrc[c], sizeof(double) * _nv, cudaMemcpyDeviceToDevice, _H->hier()->ctx->stream);
+        ck_cuda(cudaMemcpyAsync(vdst[c], vsrc[c], sizeof(double) * _nv, cudaMemcpyDeviceToDevice, _H->hier()->ctx->stream), "cudaMemcpyAsync");
 }
 
 void Grid::v3_scale(double* v[3], double ampl) {
     rt_hier* h = _H->hier();
-    cudaMemcpyAsync(h->scal + 84, &ampl, sizeof(double), cudaMemcpyHostToDevice, h->ctx->stream);
+    ck_cuda(cudaMemcpyAsync(h->scal + 84, &ampl, sizeof(double), cudaMemcpyHostToDevice, h->ctx->stream), "cudaMemcpyAsync");
     for (int c = 0; c < 3; c++) _H->check(rtk::scale(h, _nv, v[c], h->scal + 84, false), "v3_scale");
-    cudaStreamSynchronize(h->ctx->stream);
+    ck_cuda(cudaStreamSynchronize(h->ctx->stream), "cudaStreamSynchronize");
 }
 
 void Grid::v3_add(double* a[3], double alpha, double* b[3]) { v3_add(1.0, a, alpha, b); }
@@ -296,12 +304,12 @@ void Grid::v3_add(double alpha, double* a[3], double beta, double* b[3]) {
     rt_hier* h = _H->hier();
     double ab[2] = {alpha, beta};
     memcpy(h->ctx->hscal + 30, ab, sizeof(ab));
-    cudaMemcpyAsync(h->scal + 86, h->ctx->hscal + 30, sizeof(ab), cudaMemcpyHostToDevice, h->ctx->stream);
+    ck_cuda(cudaMemcpyAsync(h->scal + 86, h->ctx->hscal + 30, sizeof(ab), cudaMemcpyHostToDevice, h->ctx->stream), "cudaMemcpyAsync");
     for (int c = 0; c < 3; c++) {
         _H->check(rtk::scale(h, _nv, a[c], h->scal + 86, false), "v3_add");
         _H->check(rtk::axpy(h, _nv, beta, b[c], a[c]), "v3_add");
     }
-    cudaStreamSynchronize(h->ctx->stream);
+    ck_cuda(cudaStreamSynchronize(h->ctx->stream), "cudaStreamSynchronize");
 }
 
 void Grid::elementCompliance(double* u[3], float* ce) {
@@ -310,31 +318,44 @@ void Grid::elementCompliance(double* u[3], float* ce) {
     const double* uin = u[0];
     if (!contiguous(u, _nv)) {
         for (int c = 0; c < 3; c++)
-            cudaMemcpyAsync(h->x + c * _nv, u[c], sizeof(double) * _nv, cudaMemcpyDeviceToDevice, h->ctx->stream);
+            ck_cuda(cudaMemcpyAsync(h->x + c * _nv, u[c], sizeof(double) * _nv, cudaMemcpyDeviceToDevice, h->ctx->stream), "cudaMemcpyAsync");
         uin = h->x;
     }
     _H->check(rt_element_compliance(h, uin, ce), "elementCompliance");
 }
 
-// the support force arrays of level 0, allocated on first use
-static void ensure_support(grid::Grid* g, grid::HierarchyGrid* H, double* fs[3], double** scratch) {
-    if (fs[0]) return;
-    const int nl = (int)H->loadNodes().size();
+// the support force arrays of level 0: allocated on first use, again when the load-node count
+// changed, zeroed on allocation
+void Grid::ensure_support(void) {
+    const int nl = (int)_H->loadNodes().size();
+    if (_FS[0] && _FS_n == nl) return;
+    if (_FS[0]) cudaFree(_FS[0]);
+    _FS[0] = _FS[1] = _FS[2] = _FS_new = nullptr;
     double* p = nullptr;
-    H->check(cudaMalloc(&p, sizeof(double) * 6 * (nl > 0 ? nl : 1)) == cudaSuccess ? RT_OK : RT_ENOMEM,
-             "support force allocation");
-    cudaMemset(p, 0, sizeof(double) * 6 * (nl > 0 ? nl : 1));
-    for (int c = 0; c < 3; c++) fs[c] = p + c * nl;
-    *scratch = p + 3 * nl;
-    (void)g;
+    _H->check(cudaMalloc(&p, sizeof(double) * 6 * (nl > 0 ? nl : 1)) == cudaSuccess ? RT_OK : RT_ENOMEM,
+              "support force allocation");
+    _H->check(cudaMemset(p, 0, sizeof(double) * 6 * (nl > 0 ? nl : 1)) == cudaSuccess ? RT_OK : RT_ECUDA,
+              "support force allocation");
+    for (int c = 0; c < 3; c++) _FS[c] = p + c * nl;
+    _FS_new = p + 3 * nl;
+    _FS_n = nl;
+}
+
+Grid::~Grid() {
+    if (_FS[0]) cudaFree(_FS[0]);
+}
+
+double** Grid::getSupportForce(void) {
+    ensure_support();
+    return _FS;
 }
 
 static double support_diff_norm(grid::HierarchyGrid* H, double* const fs_old[3], const double* fs_new, int nl) {
     rt_hier* h = H->hier();
     std::vector<double> a(3 * (size_t)nl), b(3 * (size_t)nl);
-    cudaMemcpyAsync(b.data(), fs_new, sizeof(double) * 3 * nl, cudaMemcpyDeviceToHost, h->ctx->stream);
-    cudaMemcpyAsync(a.data(), fs_old[0], sizeof(double) * 3 * nl, cudaMemcpyDeviceToHost, h->ctx->stream);
-    cudaStreamSynchronize(h->ctx->stream);
+    ck_cuda(cudaMemcpyAsync(b.data(), fs_new, sizeof(double) * 3 * nl, cudaMemcpyDeviceToHost, h->ctx->stream), "cudaMemcpyAsync");
+    ck_cuda(cudaMemcpyAsync(a.data(), fs_old[0], sizeof(double) * 3 * nl, cudaMemcpyDeviceToHost, h->ctx->stream), "cudaMemcpyAsync");
+    ck_cuda(cudaStreamSynchronize(h->ctx->stream), "cudaStreamSynchronize");
     double s = 0;
     for (size_t i = 0; i < a.size(); i++) s += (a[i] - b[i]) * (a[i] - b[i]);
     return std::sqrt(s);
@@ -343,14 +364,14 @@ static double support_diff_norm(grid::HierarchyGrid* H, double* const fs_old[3],
 double Grid::supportForceCh(void) { return supportForceCh(_F); }
 
 double Grid::supportForceCh(double* f[3]) {
-    ensure_support(this, _H, _FS, &_FS_new);
+    ensure_support();
     const int nl = (int)_H->loadNodes().size();
     double* fin[3] = {f[0], f[1], f[2]};
     rt_hier* h = _H->hier();
     const double* src = f[0];
     if (!contiguous(fin, _nv)) {
         for (int c = 0; c < 3; c++)
-            cudaMemcpyAsync(h->x + c * _nv, f[c], sizeof(double) * _nv, cudaMemcpyDeviceToDevice, h->ctx->stream);
+            ck_cuda(cudaMemcpyAsync(h->x + c * _nv, f[c], sizeof(double) * _nv, cudaMemcpyDeviceToDevice, h->ctx->stream), "cudaMemcpyAsync");
         src = h->x;
     }
     _H->check(rt_get_force_support(h, src, _FS_new), "supportForceCh");
@@ -358,12 +379,12 @@ double Grid::supportForceCh(double* f[3]) {
 }
 
 double Grid::supportForceNorm(void) {
-    ensure_support(this, _H, _FS, &_FS_new);
+    ensure_support();
     const int nl = (int)_H->loadNodes().size();
     rt_hier* h = _H->hier();
     std::vector<double> a(3 * (size_t)nl);
-    cudaMemcpyAsync(a.data(), _FS[0], sizeof(double) * 3 * nl, cudaMemcpyDeviceToHost, h->ctx->stream);
-    cudaStreamSynchronize(h->ctx->stream);
+    ck_cuda(cudaMemcpyAsync(a.data(), _FS[0], sizeof(double) * 3 * nl, cudaMemcpyDeviceToHost, h->ctx->stream), "cudaMemcpyAsync");
+    ck_cuda(cudaStreamSynchronize(h->ctx->stream), "cudaStreamSynchronize");
     double s = 0;
     for (double v : a) s += v * v;
     return std::sqrt(s);
@@ -560,7 +581,7 @@ static double* contiguous_copy(double* const v[3], long long nv, double* scratch
     if (v[1] == v[0] + nv && v[2] == v[0] + 2 * nv) return v[0];
     rt_hier* h = grids.hier();
     for (int c = 0; c < 3; c++)
-        cudaMemcpyAsync(scratch + c * nv, v[c], sizeof(double) * nv, cudaMemcpyDeviceToDevice, h->ctx->stream);
+        ck_cuda(cudaMemcpyAsync(scratch + c * nv, v[c], sizeof(double) * nv, cudaMemcpyDeviceToDevice, h->ctx->stream), "cudaMemcpyAsync");
     return scratch;
 }
 
@@ -568,7 +589,7 @@ static void copy_back(double* const v[3], long long nv, const double* src) {
     if (src == v[0]) return;
     rt_hier* h = grids.hier();
     for (int c = 0; c < 3; c++)
-        cudaMemcpyAsync(v[c], src + c * nv, sizeof(double) * nv, cudaMemcpyDeviceToDevice, h->ctx->stream);
+        ck_cuda(cudaMemcpyAsync(v[c], src + c * nv, sizeof(double) * nv, cudaMemcpyDeviceToDevice, h->ctx->stream), "cudaMemcpyAsync");
 }
 
 const std::vector<int>& getLoadNodes(void) { return grids.loadNodes(); }
@@ -592,12 +613,12 @@ void forceProject(std::vector<double> fsupport[3]) {
     for (int c = 0; c < 3; c++) std::copy(fsupport[c].begin(), fsupport[c].end(), soa.begin() + (size_t)c * nl);
     double* d = nullptr;
     grids.check(cudaMalloc(&d, sizeof(double) * 3 * (nl > 0 ? nl : 1)) == cudaSuccess ? RT_OK : RT_ENOMEM, "forceProject");
-    cudaMemcpyAsync(d, soa.data(), sizeof(double) * 3 * nl, cudaMemcpyHostToDevice, h->ctx->stream);
+    ck_cuda(cudaMemcpyAsync(d, soa.data(), sizeof(double) * 3 * nl, cudaMemcpyHostToDevice, h->ctx->stream), "cudaMemcpyAsync");
     int st = rt_set_force_support(h, d, h->x);
     if (st == RT_OK) st = rt_force_project(h, h->x);
     if (st == RT_OK) st = rt_get_force_support(h, h->x, d);
-    if (st == RT_OK) cudaMemcpyAsync(soa.data(), d, sizeof(double) * 3 * nl, cudaMemcpyDeviceToHost, h->ctx->stream);
-    cudaStreamSynchronize(h->ctx->stream);
+    if (st == RT_OK) ck_cuda(cudaMemcpyAsync(soa.data(), d, sizeof(double) * 3 * nl, cudaMemcpyDeviceToHost, h->ctx->stream), "cudaMemcpyAsync");
+    ck_cuda(cudaStreamSynchronize(h->ctx->stream), "cudaStreamSynchronize");
     cudaFree(d);
     grids.check(st, "forceProject");
     for (int c = 0; c < 3; c++) std::copy(soa.begin() + (size_t)c * nl, soa.begin() + (size_t)(c + 1) * nl, fsupport[c].begin());
@@ -614,8 +635,8 @@ void getForceSupport(double const* const f_dev[3], double* fsup[3]) {
     grids.check(rt_get_force_support(h, f, dst), "getForceSupport");
     if (!soa)
         for (int c = 0; c < 3; c++)
-            cudaMemcpyAsync(fsup[c], dst + (size_t)c * nl, sizeof(double) * nl, cudaMemcpyDeviceToDevice, h->ctx->stream);
-    cudaStreamSynchronize(h->ctx->stream);
+            ck_cuda(cudaMemcpyAsync(fsup[c], dst + (size_t)c * nl, sizeof(double) * nl, cudaMemcpyDeviceToDevice, h->ctx->stream), "cudaMemcpyAsync");
+    ck_cuda(cudaStreamSynchronize(h->ctx->stream), "cudaStreamSynchronize");
 }
 
 void getForceSupport(double const* const f_dev[3], std::vector<double> fs[3]) {
@@ -625,7 +646,7 @@ void getForceSupport(double const* const f_dev[3], std::vector<double> fs[3]) {
     getForceSupport(f_dev, p);
     for (int c = 0; c < 3; c++) {
         fs[c].resize(nl);
-        cudaMemcpy(fs[c].data(), p[c], sizeof(double) * nl, cudaMemcpyDeviceToHost);
+        ck_cuda(cudaMemcpy(fs[c].data(), p[c], sizeof(double) * nl, cudaMemcpyDeviceToHost), "cudaMemcpy");
     }
 }
 
@@ -636,14 +657,14 @@ void setForceSupport(double const* const fsup[3], double* f_dev[3]) {
     const double* src = fsup[0];
     if (!(fsup[1] == fsup[0] + nl && fsup[2] == fsup[0] + 2 * nl)) {
         for (int c = 0; c < 3; c++)
-            cudaMemcpyAsync(h->fs + (size_t)c * nl, fsup[c], sizeof(double) * nl, cudaMemcpyDeviceToDevice, h->ctx->stream);
+            ck_cuda(cudaMemcpyAsync(h->fs + (size_t)c * nl, fsup[c], sizeof(double) * nl, cudaMemcpyDeviceToDevice, h->ctx->stream), "cudaMemcpyAsync");
         src = h->fs;
     }
     const bool contig = f_dev[1] == f_dev[0] + nv && f_dev[2] == f_dev[0] + 2 * nv;
     double* dst = contig ? f_dev[0] : h->x;
     grids.check(rt_set_force_support(h, src, dst), "setForceSupport");
     copy_back(f_dev, nv, dst);
-    cudaStreamSynchronize(h->ctx->stream);
+    ck_cuda(cudaStreamSynchronize(h->ctx->stream), "cudaStreamSynchronize");
 }
 
 void displacementProject(double* u_dev[3]) {
@@ -651,7 +672,7 @@ void displacementProject(double* u_dev[3]) {
     double* u = contiguous_copy(u_dev, nv, grids.hier()->x);
     grids.check(rt_displacement_project(grids.hier(), u), "displacementProject");
     copy_back(u_dev, nv, u);
-    cudaStreamSynchronize(grids.hier()->ctx->stream);
+    ck_cuda(cudaStreamSynchronize(grids.hier()->ctx->stream), "cudaStreamSynchronize");
 }
 
 // ---------------------------------------------------------------------------

@@ -39,6 +39,7 @@ class HierarchyGrid;
 class Grid {
 public:
     Grid(HierarchyGrid* owner, int layer);
+    ~Grid();
     void update_residual(void);
     void gs_relax(int n_times = 1);
     void restrict_residual(void);
@@ -73,7 +74,7 @@ public:
     // grid/Grid.cu:3434-3480: per-element compliance rho_e^p u_e.KE u_e of u into ce (device, dense element order)
     void elementCompliance(double* u[3], float* ce);
     // grid/Grid.cu:2255-2286: the support force held by the grid (device [3][nload]) and its change
-    double** getSupportForce(void) { return _FS; }
+    double** getSupportForce(void);
     double supportForceCh(void);
     double supportForceCh(double* f[3]);
     double supportForceNorm(void);
@@ -88,6 +89,8 @@ private:
     double* _R[3];
     double* _FS[3] = {nullptr, nullptr, nullptr};  // support force, [3][nload] device (level 0)
     double* _FS_new = nullptr;                        // scratch [3][nload] for supportForceCh
+    int _FS_n = -1;                                   // load-node count the support arrays were sized for
+    void ensure_support(void);
     double* _tmp = nullptr;
 };
 

@@ -19,10 +19,16 @@
 //    inputs (f, own u, flags) are already in flight into registers.
 //  * Fixed (support) nodes are stored as zero in the shared u tile, so the WS
 //    rule of the reference falls out of the data.
+#include <cuda.h>
 #include <cuda_runtime.h>
+
+#include <cstring>
+#include <mutex>
+#include <unordered_map>
 
 #include "rt_element.cuh"
 #include "rt_internal.h"
+#include "rt_tc.cuh"
 
 namespace {
 
@@ -774,6 +780,371 @@ __global__ void __launch_bounds__(PTile<TY_>::BS, pair_min_blocks<TY_>()) k_fine
 }
 
 
+// ---------------------------------------------------------------------------
+// variant 6: the pipelined tile kernel with its node layers staged by the Tensor Memory
+// Accelerator.  One thread issues, per node layer, a 4-D tiled bulk tensor copy of the
+// (TY+2) x 40 node halo box of all three components (x from X0 - 4, so the box starts on a
+// 16-byte boundary; the halo's first column sits at x index 3) and, with supports, a 3-D copy
+// of the 64-wide box of support flags (x from X0 - 16), into a ring of 3 shared slots completed
+// on one mbarrier each.  Layer t + 3 is issued at the top of iteration t, into the slot whose
+// last reader ran before the previous barrier, and waited for at its end, so the copy overlaps
+// that iteration's element and node work (the register prefetch of variant 3, without its load
+// instructions); coordinates outside the node box read as zeros (the tile kernel's halo rule).
+// After a layer's barrier completes, the block zeroes the displacements of fixed nodes (the WS
+// rule) before the iteration's block-wide barrier.  Every mbarrier wait is bounded: a timed-out
+// wait flags *err = 3, poisons out[0], waits (bounded) for the block's copies still in flight and
+// returns.  Applies where the node box's x extent is a multiple of 16 (the tensor maps' row pitch
+// must be a multiple of 16 bytes for the one-byte flags); the tensor maps cover this GPU's own
+// memory and no copy uses multicast.
+// ---------------------------------------------------------------------------
+constexpr int TMA_BX = 40;  // node box x extent (x from X0 - 4)
+constexpr int TMA_FX = 64;  // flag box x extent (x from X0 - 16)
+
+template <typename T, int TY_>
+struct TmaSmem {
+    static constexpr int SLOT = ((3 * (TY_ + 2) * TMA_BX * (int)sizeof(T) + 127) / 128 * 128) / (int)sizeof(T);
+    alignas(128) T u[3][SLOT];                       // node layer j (relative to zb - 1) in slot j % 3: [3][TY+2][40]
+    alignas(128) uint8_t fx[3][(TY_ + 2) * TMA_FX];  // support flags of the same layers: [TY+2][64]
+    T e[2][24][Tile<TY_>::NE_T];
+    float w[4][Tile<TY_>::NE_T];
+    uint64_t bar[3];
+};
+
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int x, int y, int z, int c,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(rttc::smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(c), "r"(rttc::smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(rttc::smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(rttc::smem_u32(bar))
+        : "memory");
+}
+
+template <typename T, bool WS, int MODE, int TY_>
+__global__ void __launch_bounds__(Tile<TY_>::BS, pipe_min_blocks<T, TY_>()) k_fine_pipe_tma(
+    int nx, int ny, int nz, int zchunk, const uint8_t* __restrict__ vact, const float* __restrict__ wgt,
+    const uint8_t* __restrict__ vfix, const rte::KtVals<T> kt, const __grid_constant__ CUtensorMap umap,
+    const __grid_constant__ CUtensorMap fmap, const T* __restrict__ u, const T* __restrict__ f, T* __restrict__ out,
+    T omega, T* __restrict__ dvec, const double* __restrict__ coef, int kstep, double* err) {
+    using TS = Tile<TY_>;
+    constexpr int TX = TS::TX, TY = TS::TY, EXT = TS::EXT, UXT = TS::UXT, NE_T = TS::NE_T, NU_T = TS::NU_T;
+    constexpr int TILE_BS = TS::BS;
+    constexpr int ROWB = TMA_BX;           // row pitch of a staged component
+    constexpr int CP = (TY + 2) * TMA_BX;  // component pitch of a staged layer
+    constexpr uint32_t UBYTES = 3u * (TY + 2) * TMA_BX * sizeof(T);
+    constexpr uint32_t FBYTES = WS ? (uint32_t)(TY + 2) * TMA_FX : 0u;
+    // the copies' shared destinations sit on 128-byte boundaries: the block's dynamic shared
+    // memory (sizeof(TmaSmem) + 128 bytes) is rounded up to one
+    extern __shared__ __align__(16) unsigned char smraw[];
+    TmaSmem<T, TY_>& S =
+        *reinterpret_cast<TmaSmem<T, TY_>*>(smraw + ((128 - (rttc::smem_u32(smraw) & 127)) & 127));
+    T cheb_a = T(0), cheb_b = T(0);
+    if (MODE == 3) {
+        const double ca = coef[2 * kstep], cb = coef[2 * kstep + 1];
+        cheb_a = (T)ca;
+        cheb_b = (T)cb;
+    }
+    const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
+    const long nv = (long)vx * vy * vz;
+    const long plane = (long)vx * vy;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int zb = blockIdx.z * zchunk;
+    const int ze = min(zb + zchunk, vz);
+    const int tid = threadIdx.x;
+    const int nxl = tid % TX, nyl = tid / TX;
+    const int nxg = x0 + nxl, nyg = y0 + nyl;
+    const bool node_thread = tid < TX * TY && nxg < vx && nyg < vy;
+    const long vxy = node_thread ? nxg + (long)vx * nyg : 0;
+    const int exl = tid % EXT, eyl = tid / EXT;
+    const int exg = x0 - 1 + exl, eyg = y0 - 1 + eyl;
+    const bool elem_xy = tid < NE_T && exg >= 0 && eyg >= 0 && exg < nx && eyg < ny;
+    const long exy = elem_xy ? exg + (long)nx * eyg : 0;
+    const int zlast = ze;  // node layers zb - 1 .. ze are read
+    // layer L lives in slot (L - zb + 1) % 3, phase parity ((L - zb + 1) / 3) & 1
+    auto slot_of = [&](int L) { return (L - zb + 1) % 3; };
+    auto parity_of = [&](int L) { return (uint32_t)(((L - zb + 1) / 3) & 1); };
+    auto issue = [&](int L) {  // thread 0 only
+        const int sl = slot_of(L);
+        rttc::mbar_expect_tx(&S.bar[sl], UBYTES + FBYTES);
+        tma_load_4d(&S.u[sl][0], &umap, x0 - 4, y0 - 1, L, 0, &S.bar[sl]);
+        if (WS) tma_load_3d(&S.fx[sl][0], &fmap, x0 - 16, y0 - 1, L, &S.bar[sl]);
+    };
+    // every thread waits for layer L; false if the wait ran out
+    auto wait_layer = [&](int L) -> bool { return rttc::mbar_wait(&S.bar[slot_of(L)], parity_of(L)); };
+    // fixed nodes enter the element products as zero
+    auto mask_layer = [&](int L) {
+        if (!WS) return;
+        const int sl = slot_of(L);
+        for (int i = tid; i < NU_T; i += TILE_BS) {
+            const int row = i / UXT, col = i % UXT;
+            if (S.fx[sl][row * TMA_FX + col + 15]) {
+                T* b = &S.u[sl][row * ROWB + col + 3];
+                b[0] = T(0);
+                b[CP] = T(0);
+                b[2 * CP] = T(0);
+            }
+        }
+    };
+    int issued = zb - 2;  // last layer whose copy was issued (uniform across the block)
+    // bounded drain of the copies still in flight, then the error report
+    auto give_up = [&](int first_pending) {
+        for (int L = first_pending; L <= issued; L++) rttc::mbar_wait(&S.bar[slot_of(L)], parity_of(L));
+        if (tid == 0) {
+            *err = 3.0;
+            out[0] = (T)__int_as_float(0x7fc00000);
+        }
+    };
+
+    float pw = 0.f;
+    auto fetch_w = [&](int ez) {
+        pw = (elem_xy && ez >= 0 && ez < nz) ? wgt[exy + (long)nx * ny * ez] : 0.f;
+    };
+    auto stash_w = [&](int ez) {
+        if (tid < NE_T) S.w[(ez + 4) & 3][tid] = pw;
+    };
+    auto element_phase = [&](int e) {
+        if (tid >= NE_T) return;
+        T a[24];
+        const float wv = S.w[(e + 4) & 3][tid];
+        if (wv != 0.f) {
+            const T* lo = &S.u[slot_of(e)][0];
+            const T* hi = &S.u[slot_of(e + 1)][0];
+#pragma unroll
+            for (int vtx = 0; vtx < 8; vtx++) {
+                const T* src = (vtx & 4) ? hi : lo;
+                const int idx = (eyl + ((vtx >> 1) & 1)) * ROWB + exl + (vtx & 1) + 3;
+                a[3 * vtx] = src[idx];
+                a[3 * vtx + 1] = src[CP + idx];
+                a[3 * vtx + 2] = src[2 * CP + idx];
+            }
+            rte::element_apply(a, kt, T(wv));
+        } else {
+#pragma unroll
+            for (int q = 0; q < 24; q++) a[q] = T(0);
+        }
+        T* dst = &S.e[(e + 2) & 1][0][0];
+#pragma unroll
+        for (int q = 0; q < 24; q++) dst[q * NE_T + tid] = a[q];
+    };
+
+    // prologue: barriers, layers zb-1 .. zb+1 copied, waited for and masked, weights of element
+    // layers zb-1, zb stashed, element layer zb-1 computed
+    if (tid == 0) {
+        for (int i = 0; i < 3; i++) rttc::mbar_init(&S.bar[i], 1);
+        rttc::fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int L = zb - 1; L <= zb + 1 && L <= zlast; L++) issue(L);
+    issued = min(zb + 1, zlast);
+    fetch_w(zb - 1);
+    stash_w(zb - 1);
+    fetch_w(zb);
+    stash_w(zb);
+    bool ok = true;
+    for (int L = zb - 1; L <= zb + 1 && L <= zlast; L++) ok = wait_layer(L) && ok;
+    if (__syncthreads_or(!ok)) {
+        give_up(zb - 1);
+        return;
+    }
+    for (int L = zb - 1; L <= zb + 1 && L <= zlast; L++) mask_layer(L);
+    __syncthreads();
+    element_phase(zb - 1);
+    fetch_w(zb + 1);
+    __syncthreads();
+
+    T acc[3] = {T(0), T(0), T(0)};
+    for (int t = zb - 1; t < ze; t++) {
+        // the slot of layer t + 3 held layer t, last read by element phase t (previous iteration)
+        if (t + 3 <= zlast) {
+            if (tid == 0) {
+                rttc::fence_async_smem();
+                issue(t + 3);
+            }
+            issued = t + 3;
+        }
+        if (t + 2 < ze) stash_w(t + 2);
+        if (t + 3 < ze) fetch_w(t + 3);
+        const bool out_layer = t >= zb;
+        T fv[3] = {T(0), T(0), T(0)}, uo[3] = {T(0), T(0), T(0)}, dv[3] = {T(0), T(0), T(0)};
+        bool act = false, fixed = false;
+        long vout = 0;
+        if (node_thread && out_layer) {
+            vout = vxy + plane * t;
+            act = vact[vout];
+            fixed = WS && act && vfix[vout];
+            if (MODE != 1)
+#pragma unroll
+                for (int c = 0; c < 3; c++) fv[c] = f[c * nv + vout];
+            if (MODE >= 1)
+#pragma unroll
+                for (int c = 0; c < 3; c++) uo[c] = u[c * nv + vout];
+            if (MODE == 3 && kstep > 0)
+#pragma unroll
+                for (int c = 0; c < 3; c++) dv[c] = dvec[c * nv + vout];
+        }
+        if (t + 1 < ze) element_phase(t + 1);
+        if (node_thread) {
+            const T* E = &S.e[(t + 2) & 1][0][0];
+            if (out_layer) {
+#pragma unroll
+                for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+                    for (int dx = 0; dx < 2; dx++) {
+                        const int el = (nyl + dy) * EXT + nxl + dx;
+                        const int vtx = (1 - dx) + 2 * (1 - dy);
+#pragma unroll
+                        for (int c = 0; c < 3; c++) acc[c] += E[(3 * vtx + c) * NE_T + el];
+                    }
+                const long v = vout;
+                if (MODE == 0) {
+#pragma unroll
+                    for (int c = 0; c < 3; c++) out[c * nv + v] = act ? (fixed ? fv[c] : fv[c] - acc[c]) : T(0);
+                } else if (MODE == 1) {
+#pragma unroll
+                    for (int c = 0; c < 3; c++) out[c * nv + v] = act ? (fixed ? uo[c] : acc[c]) : T(0);
+                } else {
+                    T nu[3], dn[3];
+                    node_smooth<T, MODE, EXT>(kt, S.w[(t + 3) & 3], S.w[(t + 4) & 3], nyl * EXT + nxl, acc, fv, uo,
+                                              dv, act, fixed, omega, cheb_a, cheb_b, kstep, nu, dn);
+#pragma unroll
+                    for (int c = 0; c < 3; c++) out[c * nv + v] = nu[c];
+                    if (MODE == 3)
+#pragma unroll
+                        for (int c = 0; c < 3; c++) dvec[c * nv + v] = dn[c];
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 3; c++) acc[c] = T(0);
+#pragma unroll
+            for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+                for (int dx = 0; dx < 2; dx++) {
+                    const int el = (nyl + dy) * EXT + nxl + dx;
+                    const int vtx = (1 - dx) + 2 * (1 - dy) + 4;
+#pragma unroll
+                    for (int c = 0; c < 3; c++) acc[c] += E[(3 * vtx + c) * NE_T + el];
+                }
+        }
+        // layer t + 3 (read by element phase t + 2, next iteration) complete and masked; the
+        // iteration's barrier publishes the masking
+        ok = true;
+        if (t + 3 <= zlast) ok = wait_layer(t + 3);
+        if (ok && t + 3 <= zlast) mask_layer(t + 3);
+        if (__syncthreads_or(!ok)) {
+            give_up(t + 3);
+            return;
+        }
+    }
+}
+
+// tensor maps of the TMA-staged variant: cuTensorMapEncodeTiled through the runtime's driver
+// entry point (no link against libcuda); maps cached by (address, element size, box), since the
+// Chebyshev steps alternate between a few vectors
+using tmap_encode_t = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+tmap_encode_t tmap_encoder() {
+    static tmap_encode_t fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<tmap_encode_t>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+struct TmapKey {
+    const void* p;
+    int esize, vx, vy, vz, rows;
+    bool operator==(const TmapKey& o) const {
+        return p == o.p && esize == o.esize && vx == o.vx && vy == o.vy && vz == o.vz && rows == o.rows;
+    }
+};
+struct TmapHash {
+    size_t operator()(const TmapKey& k) const {
+        return std::hash<const void*>()(k.p) ^ ((size_t)k.esize << 1) ^ ((size_t)k.vx << 7) ^ ((size_t)k.rows << 23) ^
+               ((size_t)k.vz << 31);
+    }
+};
+std::mutex g_tmap_mutex;
+std::unordered_map<TmapKey, CUtensorMap, TmapHash> g_tmaps;
+
+// node vectors [3][vz][vy][vx] (esize 4 or 8) as 4-D boxes {40, rows, 1, 3}; flags [vz][vy][vx] bytes
+// (esize 1) as 3-D boxes {64, rows, 1}; false if the encoder refuses (then variant 3 runs)
+bool tmap_get(const void* p, int esize, int vx, int vy, int vz, int rows, CUtensorMap* out) {
+    const TmapKey key{p, esize, vx, vy, vz, rows};
+    std::lock_guard<std::mutex> lk(g_tmap_mutex);
+    auto it = g_tmaps.find(key);
+    if (it != g_tmaps.end()) {
+        *out = it->second;
+        return true;
+    }
+    tmap_encode_t enc = tmap_encoder();
+    if (!enc) return false;
+    CUtensorMap m;
+    memset(&m, 0, sizeof(m));
+    CUresult r;
+    if (esize == 1) {
+        const cuuint64_t dims[3] = {(cuuint64_t)vx, (cuuint64_t)vy, (cuuint64_t)vz};
+        const cuuint64_t strides[2] = {(cuuint64_t)vx, (cuuint64_t)vx * vy};
+        const cuuint32_t box[3] = {(cuuint32_t)TMA_FX, (cuuint32_t)rows, 1u};
+        const cuuint32_t estr[3] = {1u, 1u, 1u};
+        r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(p), dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    } else {
+        const cuuint64_t nv = (cuuint64_t)vx * vy * vz;
+        const cuuint64_t dims[4] = {(cuuint64_t)vx, (cuuint64_t)vy, (cuuint64_t)vz, 3};
+        const cuuint64_t strides[3] = {(cuuint64_t)vx * esize, (cuuint64_t)vx * vy * esize, nv * esize};
+        const cuuint32_t box[4] = {(cuuint32_t)TMA_BX, (cuuint32_t)rows, 1u, 3u};
+        const cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
+        r = enc(&m, esize == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                const_cast<void*>(p), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    }
+    if (r != CUDA_SUCCESS) return false;
+    if (g_tmaps.size() > 256) g_tmaps.clear();
+    g_tmaps.emplace(key, m);
+    *out = m;
+    return true;
+}
+
+template <typename T, bool WS, int MODE, int TY_>
+int launch_tma_ty(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name, T* dvec,
+                  const double* coef, int kstep, bool* done) {
+    rt_level& L = h->L[0];
+    *done = false;
+    CUtensorMap umap, fmap;
+    memset(&fmap, 0, sizeof(fmap));
+    // the maps' base addresses must sit on 16-byte boundaries
+    if ((reinterpret_cast<uintptr_t>(u) & 15) || (WS && (reinterpret_cast<uintptr_t>(h->vfix) & 15))) return RT_OK;
+    if (!tmap_get(u, (int)sizeof(T), L.vx, L.vy, L.vz, TY_ + 2, &umap)) return RT_OK;
+    if (WS && !tmap_get(h->vfix, 1, L.vx, L.vy, L.vz, TY_ + 2, &fmap)) return RT_OK;
+    const int zc = h->tune[sizeof(T) == 8 ? 1 : 0][MODE].zchunk;
+    dim3 grid((L.vx + Tile<TY_>::TX - 1) / Tile<TY_>::TX, (L.vy + TY_ - 1) / TY_, (L.vz + zc - 1) / zc);
+    const rte::KtVals<T> kt = rte::make_kt<T>(h);
+    *done = true;
+    return rt_launch(h->ctx, name, [&] {
+        k_fine_pipe_tma<T, WS, MODE, TY_><<<grid, Tile<TY_>::BS, sizeof(TmaSmem<T, TY_>) + 128, h->ctx->stream>>>(
+            L.nx, L.ny, L.nz, zc, L.vact, h->w, h->vfix, kt, umap, fmap, u, f, out, (T)omega, dvec, coef, kstep,
+            h->scal + RT_SCAL_ERR);
+    });
+}
+
 template <typename T, bool WS, int MODE, int TY_, bool PIPE>
 int launch_tile_ty(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name, T* dvec,
                    const double* coef, int kstep) {
@@ -806,12 +1177,26 @@ int launch_pair_ty(rt_hier* h, const float* u, const float* f, float* out, doubl
 }
 
 // variant 0: two barriers per element layer; 3: software-pipelined, one barrier per layer;
-// 4 (FP32): pipelined with element pairs in packed FP32; 5: sum-factorised row marching (rt_fine_sf.cu)
+// 4 (FP32): pipelined with element pairs in packed FP32; 5: sum-factorised row marching (rt_fine_sf.cu);
+// 6: variant 3 with its node layers staged by TMA (node boxes whose x extent is a multiple of 16)
 template <typename T, bool WS, int MODE>
 int launch_tile(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name, T* dvec = nullptr,
                 const double* coef = nullptr, int kstep = 0) {
     const rt_tile_cfg& tn = h->tune[sizeof(T) == 8 ? 1 : 0][MODE];
     if (tn.variant == 5) return rtk::launch_sf<T, WS, MODE>(h, u, f, out, omega, name, dvec, coef, kstep);
+    if (tn.variant == 6 && h->L[0].vx % 16 == 0) {
+        bool done = false;
+        const int st = tn.ty == 4 ? launch_tma_ty<T, WS, MODE, 4>(h, u, f, out, omega, name, dvec, coef, kstep, &done)
+                                  : launch_tma_ty<T, WS, MODE, 8>(h, u, f, out, omega, name, dvec, coef, kstep, &done);
+        if (done || st != RT_OK) return st;
+        // the tensor maps could not be made: the same schedule with per-thread loads
+    }
+    if (tn.variant == 6) {
+        switch (tn.ty) {
+            case 4: return launch_tile_ty<T, WS, MODE, 4, true>(h, u, f, out, omega, name, dvec, coef, kstep);
+            default: return launch_tile_ty<T, WS, MODE, 8, true>(h, u, f, out, omega, name, dvec, coef, kstep);
+        }
+    }
     if constexpr (sizeof(T) == 4) {
         if (tn.variant == 4) {
             switch (tn.ty) {
@@ -842,6 +1227,23 @@ cudaError_t set_attr() {
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_fine_pipe<T, WS, MODE, TY_>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(PipeSmem<T, TY_>));
+}
+
+template <typename T, bool WS, int MODE, int TY_>
+cudaError_t set_attr_tma() {
+    return cudaFuncSetAttribute(k_fine_pipe_tma<T, WS, MODE, TY_>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(TmaSmem<T, TY_>) + 128);
+}
+
+template <typename T, int TY_>
+cudaError_t set_attrs_tma() {
+    cudaError_t r[8] = {set_attr_tma<T, false, 0, TY_>(), set_attr_tma<T, false, 1, TY_>(),
+                        set_attr_tma<T, false, 2, TY_>(), set_attr_tma<T, false, 3, TY_>(),
+                        set_attr_tma<T, true, 0, TY_>(),  set_attr_tma<T, true, 1, TY_>(),
+                        set_attr_tma<T, true, 2, TY_>(),  set_attr_tma<T, true, 3, TY_>()};
+    for (auto x : r)
+        if (x != cudaSuccess) return x;
+    return cudaSuccess;
 }
 
 template <bool WS, int MODE, int TY_>
@@ -879,9 +1281,11 @@ namespace rtk {
 // dynamic shared-memory limits of every tile-kernel variant, set once per device
 // (before any stream capture can include a launch)
 int init_tile_kernels(rt_ctx* c) {
-    cudaError_t es[9] = {set_attrs_T<double, 2>(), set_attrs_T<double, 4>(), set_attrs_T<double, 8>(),
-                         set_attrs_T<float, 2>(),  set_attrs_T<float, 4>(),  set_attrs_T<float, 8>(),
-                         set_attrs_pair<2>(),      set_attrs_pair<4>(),      set_attrs_pair<8>()};
+    cudaError_t es[13] = {set_attrs_T<double, 2>(),   set_attrs_T<double, 4>(),   set_attrs_T<double, 8>(),
+                          set_attrs_T<float, 2>(),    set_attrs_T<float, 4>(),    set_attrs_T<float, 8>(),
+                          set_attrs_pair<2>(),        set_attrs_pair<4>(),        set_attrs_pair<8>(),
+                          set_attrs_tma<float, 4>(),  set_attrs_tma<float, 8>(),  set_attrs_tma<double, 4>(),
+                          set_attrs_tma<double, 8>()};
     for (cudaError_t e : es)
         if (e != cudaSuccess) return rt_fail(c, RT_ECUDA, "tile kernel attributes: %s", cudaGetErrorString(e));
     return RT_OK;

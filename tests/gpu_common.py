@@ -37,6 +37,8 @@ CONFIGS = {
     "cantilever": lambda: configs.cantilever(24, 12, 12),
     "worstcase": lambda: configs.worst_case_box(20, 16, 12, seed=3),
     "ragged_arch": lambda: configs.arch(27, 16, 14, tunnel=6, pad=3),
+    # 48 nodes in x (a multiple of 16): the TMA-staged finest-level kernel runs on it
+    "arch_x48": lambda: configs.arch(47, 18, 14, tunnel=7, pad=3),
     "free_nsff": lambda: configs.free_block(20, 12, 10, seed=4, mode=rb.MODE_NSFF),
     "free_nscf": lambda: configs.free_block(18, 12, 10, seed=5, mode=rb.MODE_NSCF),
 }
