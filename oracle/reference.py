@@ -1,9 +1,12 @@
 """The reference's own code, compiled from its sources (test infrastructure only).
 
 ``make -C oracle ref`` builds, from the reference tree (default /root/reference, present only
-where the reference is mounted), two libraries into oracle/_ref/:
+where the reference is mounted), these libraries into oracle/_ref/:
 
 * libref_ke.so: element/templateMatrix.cpp:31-124 (initTemplateMatrix) on the host;
+* libref_stop.so, libref_stop_fabs.so: snippet::converge_criteria (utils/snippet.h:156-213), the
+  optimisation loop's stop test, on the host, with g++'s integer abs() of the change and with the
+  floating-point one;
 * libref_kernels.so: applyK_OTFA_kernel (grid/Grid.cu:2439-2517), computeSensitivity_kernel and
   trySensMultiplier_kernel (optimization/optimization.cu:44-162) and filterSensitivity_kernel
   (grid/Grid.cu:2323-2409) for sm_100a, driven on dense element boxes (needs a GPU to run).
@@ -23,6 +26,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(_HERE, "_ref")
 KE_LIB = os.path.join(REF_DIR, "libref_ke.so")
 KERNELS_LIB = os.path.join(REF_DIR, "libref_kernels.so")
+STOP_LIB = os.path.join(REF_DIR, "libref_stop.so")
+STOP_FABS_LIB = os.path.join(REF_DIR, "libref_stop_fabs.so")
 REFERENCE_TREE = os.environ.get("ROBTOP_REFERENCE", "/root/reference")
 
 
@@ -44,6 +49,20 @@ def template_matrix(h=1.0, E=1.0, nu=0.3):
     out = np.zeros(576)
     L.ref_template_matrix(h, E, nu, _p(out))
     return out.reshape(24, 24)
+
+
+def converge_run(n_constrain, max_counter, thres, values, constraints, float_abs=False):
+    """The reference's converge_criteria(n_constrain, max_counter, thres) fed the objective values
+    and the constraint rows in order; returns its update() results (1 = stop).  ``float_abs``
+    selects the build in which abs() of the change is the floating-point one (the header under
+    MSVC) instead of g++'s integer abs."""
+    L = C.CDLL(STOP_FABS_LIB if float_abs else STOP_LIB)
+    L.ref_converge_run.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    v = np.ascontiguousarray(values, np.float64)
+    g = np.ascontiguousarray(np.reshape(constraints, (v.size, n_constrain)), np.float64)
+    out = np.zeros(v.size, np.int32)
+    L.ref_converge_run(n_constrain, max_counter, thres, v.size, _p(v), _p(g), _p(out))
+    return out
 
 
 class Kernels:

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <cstdio>
 #include <cstring>
 #include <stdexcept>
@@ -525,25 +526,69 @@ float updateDensities(float Vgoal) {
     return lam;
 }
 
-// optimization() (optimization/optimization.cpp:583-673) without the file output
+// the stop test of optimization(): converge_criteria(n_constrain, max_counter, thres)
+// (utils/snippet.h:156-213).  The change of a recorded sequence h is
+// |h_k + h_{k-1} - h_{k-2} - h_{k-3}| / (h_{k-2} + h_{k-3}) (not a number before four values);
+// an update passes when the objective's change is below thres and no constraint's change exceeds
+// 1e-3, raising a counter (a failing update lowers it, not below 0); it reports convergence once
+// the counter exceeds max_counter.  The change is the floating-point one (the header's
+// behaviour under MSVC; under g++ its unqualified abs() truncates the change to an integer).
+namespace {
+class StopTest {
+public:
+    StopTest(int n_constrain, int max_counter, double thres)
+        : _n(n_constrain), _max(max_counter), _thres(thres), _g(n_constrain) {}
+    bool update(double value, const double* constraints) {
+        _c.push_back(value);
+        for (int i = 0; i < _n; i++) _g[i].push_back(constraints[i]);
+        bool ok = change(_c) < _thres;
+        for (int i = 0; i < _n && ok; i++)
+            if (change(_g[i]) > 1e-3) ok = false;
+        _counter = ok ? _counter + 1 : std::max(_counter - 1, 0);
+        return _counter > _max;
+    }
+
+private:
+    static double change(const std::vector<double>& h) {
+        const size_t k = h.size();
+        if (k < 4) return std::numeric_limits<double>::quiet_NaN();
+        return std::fabs(h[k - 1] + h[k - 2] - h[k - 3] - h[k - 4]) / (h[k - 3] + h[k - 4]);
+    }
+    int _n, _max, _counter = 0;
+    double _thres;
+    std::vector<double> _c;
+    std::vector<std::vector<double>> _g;
+};
+}  // namespace
+
+// optimization() (optimization/optimization.cpp:583-673) without the file output: the volume
+// goal shrinks by volume_decrease each iteration (the constraint value Vc is taken before the
+// goal is clamped to volume_ratio), and the loop ends when the stop test converges with the goal
+// at the volume ratio; the worst-case compliances and goals are kept (optimizationRecords)
+static std::vector<double> g_c_record, g_vol_record;
 void optimization(int max_iter) {
     initDensities(params.volume_ratio);
     float Vgoal = params.volume_ratio;
-    double last = 0;
-    int small = 0;
+    StopTest stop_check(1, 2, 5e-3);
+    g_c_record.clear();
+    g_vol_record.clear();
     for (int itn = 1; itn <= max_iter; itn++) {
         Vgoal *= (1 - params.volume_decrease);
+        double Vc = Vgoal - params.volume_ratio;
         if (Vgoal < params.volume_ratio) Vgoal = params.volume_ratio;
         update_stencil();
         const double c = modifiedPM();
-        // converge_criteria(1, 2, 5e-3) (utils/snippet.h:156-213): relative change below 5e-3 twice
-        if (itn > 1 && std::fabs(c - last) / std::fabs(last) < 5e-3) small++;
-        else small = 0;
-        last = c;
-        if (small >= 2 && Vgoal <= params.volume_ratio + 1e-3) break;
+        g_c_record.push_back(c);
+        g_vol_record.push_back(Vgoal);
+        if (stop_check.update(c, &Vc) && Vgoal <= params.volume_ratio + 1e-3) break;
         computeSensitivity();
         updateDensities(Vgoal);
     }
+}
+
+const std::vector<double>& optimizationRecords(std::vector<double>* volumes) {
+    if (volumes) *volumes = g_vol_record;
+    return g_c_record;
 }
 
 // test_rigid_displacement (optimization/optimization.cpp:697-709)
@@ -776,9 +821,9 @@ double Knorm(double* u[3]) {
 }
 
 // checkAdjointVariable (optimization/optimization.cu:353-402): with the adjoint N^T lambda in the
-// displacement vector and the last worst-case pair (u_w, f_w = K u_w, compliance mu) from
-// modifiedPM, |2 f_w - K (N^T lambda) - 2 mu K f_w| on the free nodes must be below 1e-6
-// (relative to |f_w|); the displacement vector is left unchanged
+// displacement vector and the last worst-case pair from modifiedPM (u_w, its compliance mu, and
+// f_w = K u_w, which the reference keeps in Fworst), |2 f_w - K (N^T lambda) - 2 mu K f_w| on the
+// free nodes must be below 1e-6 (relative to |f_w|); the displacement vector is left unchanged
 static std::vector<double> g_uworst, g_fworst;
 static double g_mu = 0;
 
@@ -787,10 +832,12 @@ void remember_worst_case(void) {
     const long long nv = grids[0]->n_box_nodes();
     g_uworst.resize(3 * nv);
     g_fworst.resize(3 * nv);
+    std::vector<double> f(3 * nv);
     grids.check(rt_get(h, RT_FIELD_U, 0, RT_LAYOUT_DENSE, g_uworst.data()), "worst-case displacement");
-    grids.check(rt_get(h, RT_FIELD_F, 0, RT_LAYOUT_DENSE, g_fworst.data()), "worst-case force");
+    grids.check(rt_get(h, RT_FIELD_F, 0, RT_LAYOUT_DENSE, f.data()), "worst-case force");
+    grids.check(rt_apply_K(h, g_uworst.data(), g_fworst.data()), "K u_worst");
     g_mu = 0;
-    for (long long i = 0; i < 3 * nv; i++) g_mu += g_uworst[i] * g_fworst[i];
+    for (long long i = 0; i < 3 * nv; i++) g_mu += g_uworst[i] * f[i];
 }
 
 bool checkAdjointVariable(void) {

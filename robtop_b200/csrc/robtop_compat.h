@@ -200,6 +200,9 @@ double modifiedPM(void);
 void computeSensitivity(void);
 float updateDensities(float Vgoal);
 void optimization(int max_iter = 100);
+// the worst-case compliance of each iteration of the last optimization() (the reference writes it
+// to the file "cworst"), and with volumes != nullptr the volume goals ("vrec")
+const std::vector<double>& optimizationRecords(std::vector<double>* volumes = nullptr);
 grid::HierarchyGrid& getGrids(void);
 void setBoundaryCondition(std::function<bool(double[3])> fixarea, std::function<bool(double[3])> loadarea,
                           std::function<std::array<double, 3>(double[3])> forcefield);

@@ -238,38 +238,93 @@ def readDensity(path):
     return man
 
 
+class ConvergeCriteria:
+    """snippet::converge_criteria (utils/snippet.h:156-213): the stop test of optimization().
+
+    Each update records the objective c_k and the constraint values g_k.  The objective change
+    fch = |c_k + c_{k-1} - c_{k-2} - c_{k-3}| / (c_{k-2} + c_{k-3}) (not a number while fewer
+    than four values exist) must be below ``stop_thres`` and each constraint's change, formed
+    the same way, must not exceed 1e-3.  A passing update raises a counter, a failing one lowers
+    it (not below 0); update returns True once the counter exceeds ``max_counter``.
+
+    ``integer_abs`` reproduces the header as g++ compiles it: its unqualified abs() of the
+    change resolves to the C library's int abs(int), so the numerator is truncated to an integer
+    first and every change below 1 reads as 0.  The default is the floating-point change (the
+    header under MSVC, and the test as it is written)."""
+
+    def __init__(self, n_constrain, max_counter, stop_thres, integer_abs=False):
+        self.n = int(n_constrain)
+        self.max_counter = int(max_counter)
+        self.thres = float(stop_thres)
+        self.integer_abs = bool(integer_abs)
+        self.values, self.constraints = [], []
+        self.counter = 0
+
+    def _change(self, h):
+        if len(h) < 4:
+            return float("nan")
+        a, b, c, d = h[-1], h[-2], h[-3], h[-4]
+        num, den = np.float64(a + b - c - d), np.float64(c + d)
+        if self.integer_abs and np.isfinite(num):
+            num = np.trunc(num)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            return float(np.abs(num) / den)
+
+    def update(self, value, constraints=()):
+        self.values.append(float(value))
+        self.constraints.append([float(g) for g in constraints][: self.n])
+        converged = self._change(self.values) < self.thres
+        for i in range(self.n):
+            if self._change([g[i] for g in self.constraints]) > 1e-3:
+                converged = False
+                break
+        self.counter = self.counter + 1 if converged else max(self.counter - 1, 0)
+        return self.counter > self.max_counter
+
+
 def optimization(max_iter=100, worst=modifiedPM, checkpoint_every=0, resume=None):
-    """optimization/optimization.cpp:583-673; returns the compliance record.  With
-    ``checkpoint_every`` = n > 0 the state is written every n iterations into
-    <output dir>/iter_<k> (setOutpurDir); ``resume`` = such a directory continues from it."""
+    """optimization/optimization.cpp:583-673; returns the worst-case compliance record.
+
+    Per iteration: the volume goal shrinks by volume_decrease (the constraint value Vc recorded
+    for the stop test is taken before the goal is clamped to volume_ratio), the stencils are
+    updated, the worst-case compliance is found, and the loop ends when
+    converge_criteria(1, 2, 5e-3) reports convergence with the goal at the volume ratio;
+    otherwise sensitivity, filter and OC update follow.  The volume goals are kept in
+    ``_state["volumes"]``.  With ``checkpoint_every`` = n > 0 the state is written every n
+    iterations into <output dir>/iter_<k> (setOutpurDir); ``resume`` = such a directory
+    continues from it (the stop test replays the recorded values)."""
     import os
 
-    rec, start = [], 1
+    rec, vols, start = [], [], 1
     if resume:
         readDensity(resume)
         rec, start = list(_state["records"]), _state["iteration"] + 1
     else:
         initDensities(params.volume_ratio)
+    stop = ConvergeCriteria(1, 2, 5e-3)
     Vgoal = params.volume_ratio
-    small = 0
+    for c in rec:  # a resumed run: the stop test and the goals of the recorded iterations
+        Vgoal *= 1 - params.volume_decrease
+        stop.update(c, [Vgoal - params.volume_ratio])
+        Vgoal = max(Vgoal, params.volume_ratio)
+        vols.append(Vgoal)
     for itn in range(start, max_iter + 1):
         _state["iteration"] = itn
-        Vgoal = max(Vgoal * (1 - params.volume_decrease), params.volume_ratio)
+        Vgoal *= 1 - params.volume_decrease
+        Vc = Vgoal - params.volume_ratio
+        Vgoal = max(Vgoal, params.volume_ratio)
         update_stencil()
         c = worst()
-        if rec and abs(c - rec[-1]) / abs(rec[-1]) < 5e-3:
-            small += 1
-        else:
-            small = 0
         rec.append(c)
-        if small >= 2 and Vgoal <= params.volume_ratio + 1e-3:
+        vols.append(Vgoal)
+        _state["records"], _state["volumes"] = rec, vols
+        if stop.update(c, [Vc]) and Vgoal <= params.volume_ratio + 1e-3:
             break
         computeSensitivity()
         updateDensities(Vgoal)
-        _state["records"] = rec
         if checkpoint_every and itn % checkpoint_every == 0:
             writeDensity(os.path.join(_state.get("outdir", "."), f"iter_{itn}"))
-    _state["records"] = rec
+    _state["records"], _state["volumes"] = rec, vols
     return rec
 
 

@@ -41,8 +41,9 @@ int main(int argc, char** argv) {
     const double mu = modifiedPM();
     printf("worst_compliance %.17g\n", mu);
     // the adjoint identity of checkAdjointVariable (optimization/optimization.cu:353-402) holds for
-    // N^T lambda = 2 u_w - 2 mu f_w; a zero vector fails it
+    // N^T lambda = 2 u_w - 2 mu K u_w; a zero vector fails it
     grid::Grid* g0 = getGrids()[0];
+    g0->applyK(g0->getDisplacement(), g0->getForce());
     g0->v3_add(2.0, g0->getDisplacement(), -2.0 * mu, g0->getForce());
     printf("adjoint_ok %d\n", checkAdjointVariable() ? 1 : 0);
     g0->reset_displacement();
@@ -108,6 +109,14 @@ int main(int argc, char** argv) {
     std::vector<float> rho2(rho.size());
     rt_get(getGrids().hier(), RT_FIELD_RHO, 0, RT_LAYOUT_DENSE, rho2.data());
     printf("density_roundtrip %d\n", rho2 == rho ? 1 : 0);
+    // the optimisation loop with its stop test (volume goal 0.4 throughout)
+    optimization(12);
+    std::vector<double> vols;
+    const std::vector<double>& crec = optimizationRecords(&vols);
+    printf("opt_iterations %zu\n", crec.size());
+    printf("opt_first_compliance %.17g\n", crec.front());
+    printf("opt_last_compliance %.17g\n", crec.back());
+    printf("opt_last_volume_goal %.9g\n", vols.back());
     // the mesh form of buildGrids (optimization/optimization.cpp:14-19): a 24 x 12 x 12 box
     // of 12 triangles, voxelised at gridreso R - 1 (cube 32^3)
     setParameters(0.4f, 0.0f, 0.03f, 2.0f, 0.5f, 3.0f, 1e-3f, R - 1, 1e6f, 0.4f, 0.0f, false, false);

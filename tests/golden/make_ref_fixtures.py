@@ -3,6 +3,9 @@
 * ref_template_matrix.npz: KE from the reference's initTemplateMatrix
   (element/templateMatrix.cpp:31-124, built into oracle/_ref/libref_ke.so by `make -C oracle ref`)
   for three (h, E, nu);
+* ref_stop.npz: the update() results of the reference's converge_criteria (utils/snippet.h:156-213,
+  oracle/_ref/libref_stop.so and libref_stop_fabs.so: integer and floating-point abs of the change)
+  on the seeded sequences of stop_sequences() below;
 * ref_kernels.npz (only with --kernels, on a machine with a GPU): the outputs of the reference's
   applyK_OTFA_kernel, computeSensitivity_kernel, trySensMultiplier_kernel and
   filterSensitivity_kernel (oracle/_ref/libref_kernels.so) on the seeded inputs of
@@ -27,6 +30,26 @@ from ref_inputs import CASES, FILTER_RADIUS, OC, P, inputs  # noqa: E402
 KE_PARAMS = [(1.0, 1e6, 0.4), (1.0, 1.0, 0.3), (0.5, 2e5, 0.25)]
 
 
+def stop_sequences():
+    """Objective / constraint sequences for the stop test: converging geometric tails, noisy
+    plateaus, a zero constraint (0 / 0 changes), a shrinking volume goal, and sequences of 1-3
+    values (changes not yet defined)."""
+    rng = np.random.default_rng(11)
+    seqs = []
+    for case in range(12):
+        n = int(rng.integers(1, 40))
+        c = 10.0 * (1 + rng.uniform(0.05, 0.5) * rng.uniform(0.3, 0.95) ** np.arange(n))
+        if case % 3 == 1:
+            c = c * (1 + rng.normal(0, 10 ** rng.uniform(-4, -2), n))
+        g = np.zeros(n) if case % 4 == 0 else -0.4 * 0.02 * np.ones(n)
+        if case % 4 == 3:
+            g = 0.4 * (0.98 ** np.arange(1, n + 1) - 1)
+        seqs.append((c, g))
+    for n in (1, 2, 3):
+        seqs.append((np.linspace(5, 4, n), np.zeros(n)))
+    return seqs
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--kernels", action="store_true")
@@ -37,6 +60,15 @@ def main():
         kes = np.stack([reference.template_matrix(h, E, nu) for h, E, nu in KE_PARAMS])
         np.savez_compressed(os.path.join(a.out, "ref_template_matrix.npz"), params=np.array(KE_PARAMS), ke=kes)
         print("template matrices written")
+    if os.path.exists(reference.STOP_LIB):
+        seqs = stop_sequences()
+        flat = {}
+        for i, (c, g) in enumerate(seqs):
+            flat[f"c{i}"], flat[f"g{i}"] = c, g
+            flat[f"stop{i}"] = reference.converge_run(1, 2, 5e-3, c, g)
+            flat[f"stop_fabs{i}"] = reference.converge_run(1, 2, 5e-3, c, g, float_abs=True)
+        np.savez_compressed(os.path.join(a.out, "ref_stop.npz"), n=len(seqs), **flat)
+        print("stop-test results written")
     if a.kernels:
         K = reference.Kernels()
         out = {}

@@ -87,3 +87,9 @@ def test_compat_remaining_entry_points():
     assert abs(vals["mgpsor"] - lam) <= 1e-2 * lam
     assert vals["density_roundtrip"] == 1
     assert len(rigid) == 6
+    # optimization(): at most the 12 iterations asked for, the goal at the volume ratio, finite
+    # compliances (the stop test needs at least four values before it can pass)
+    assert 1 <= vals["opt_iterations"] <= 12
+    assert vals["opt_iterations"] == 12 or vals["opt_iterations"] >= 6
+    assert abs(vals["opt_last_volume_goal"] - 0.4) <= 1e-6
+    assert 0 < vals["opt_first_compliance"] < 1e30 and 0 < vals["opt_last_compliance"] < 1e30

@@ -53,3 +53,50 @@ def test_density_after_oc_iterations():
     finally:
         G.close()
         ctx.close()
+
+
+def test_worst_case_oc_iterations():
+    """Four iterations of the worst-case optimisation (rt_oc_iteration: stencil update, Lanczos
+    worst-case load with k = 8 and inner solves to 1e-10, worst-case displacement, sensitivity,
+    filter radius 2, OC update to volume 0.4; optimization/optimization.cpp:611-656) on the
+    20x16x12 worst-case box against the same steps in the oracle: the eigenvalue of every
+    iteration within 1e-7 relative and the density within 1e-4 max-abs."""
+    cfg = CONFIGS["worstcase"]()
+    ctx, G, H = build_pair(cfg)
+    nz, ny, nx = cfg["eact"].shape
+    eact = np.ascontiguousarray(cfg["eact"].ravel(), np.uint8)
+    nact = int(eact.sum())
+    ln = np.ascontiguousarray(cfg["load_nodes"], np.int32)
+    normals = np.ascontiguousarray(cfg["normals"], np.float64)
+    rho_o = np.ascontiguousarray(cfg["rho"].ravel(), np.float32)
+    K, TOL = 8, 1e-10
+    lam_g = C.c_double()
+    try:
+        for it in range(4):
+            seed = 100 + it
+            rb._capi.check(rb.lib().rt_oc_iteration(G.handle, rb.WORST_LANCZOS, K, TOL, seed, 0.4, C.byref(lam_g)),
+                           ctx.handle)
+            rho_g = np.ascontiguousarray(G[0].getRho(), np.float32)
+            Ho = O.Hierarchy(cfg["eact"], rho_o.reshape(cfg["eact"].shape), cfg["vfix"], p=P, E=E, nu=NU)
+            Ho.update_stencil()
+            nv = Ho.arrs[0]["u"].size // 3
+            work = np.zeros((K + 1) * 3 * ln.size + 10 * 3 * nv)
+            lam, ritz = np.zeros(1), np.zeros(3 * nv)
+            O.lib().or_lanczos(Ho.LA, Ho.nlev, O.ptr(Ho.KE), O.SMOOTH_SGS, 1, 1, 0.6, ln.size, O.ptr(ln),
+                               O.ptr(normals), 0, 0, None, seed, K, TOL, 2000, O.ptr(lam), O.ptr(ritz), O.ptr(work))
+            assert abs(lam_g.value - lam[0]) <= 1e-7 * lam[0], (it, lam_g.value, lam[0])
+            x, _, rr = Ho.pcg(ritz, tol=TOL, maxit=2000)
+            assert rr <= TOL
+            s = np.zeros(rho_o.size, np.float32)
+            O.lib().or_sensitivity(nx, ny, nz, O.ptr(eact), O.ptr(rho_o), P, O.ptr(Ho.KE), O.ptr(x), O.ptr(s))
+            fs = np.zeros_like(s)
+            O.lib().or_filter(nx, ny, nz, O.ptr(eact), 2.0, O.ptr(s), O.ptr(fs))
+            tmp = np.zeros_like(rho_o)
+            its = np.zeros(1, np.int32)
+            O.lib().or_oc_update(rho_o.size, O.ptr(eact), None, O.ptr(rho_o), O.ptr(fs), 0.4, 0.03, 0.5, 1e-3, nact,
+                                 O.ptr(its), O.ptr(tmp))
+            assert np.abs(rho_g - rho_o).max() <= 1e-4, f"iteration {it}"
+        assert np.abs(rho_g - cfg["rho"].ravel()).max() > 1e-2  # the design moved
+    finally:
+        G.close()
+        ctx.close()

@@ -70,3 +70,37 @@ def test_oracle_matches_reference_kernel_outputs(name):
     assert np.abs(mine["oc_try"][act] - ref["oc_try"][act]).max() <= 2e-6
     # the filter: FP32 weights, FP64 sums in both
     assert np.abs(mine["filter"][act] - ref["filter"][act]).max() <= 1e-6 * np.abs(ref["filter"]).max()
+
+
+STOP_FIXTURE = os.path.join(HERE, "golden", "ref_stop.npz")
+
+
+def _stop_flags(c, g, integer_abs):
+    from robtop_b200.optimization import ConvergeCriteria
+
+    crit = ConvergeCriteria(1, 2, 5e-3, integer_abs=integer_abs)
+    return [int(crit.update(ci, [gi])) for ci, gi in zip(c, g)]
+
+
+def test_stop_test_matches_reference_fixture():
+    """optimization()'s stop test (ConvergeCriteria) gives the reference converge_criteria's
+    update() results on the fixture's sequences, stop for stop, in both builds of the header
+    (g++'s integer abs of the change, and the floating-point one)."""
+    d = np.load(STOP_FIXTURE)
+    for i in range(int(d["n"])):
+        assert _stop_flags(d[f"c{i}"], d[f"g{i}"], True) == d[f"stop{i}"].tolist(), i
+        assert _stop_flags(d[f"c{i}"], d[f"g{i}"], False) == d[f"stop_fabs{i}"].tolist(), i
+
+
+@pytest.mark.skipif(not (os.path.exists(reference.STOP_LIB) and os.path.exists(reference.STOP_FABS_LIB)),
+                    reason="oracle/_ref/libref_stop*.so not built")
+def test_stop_test_matches_reference_build():
+    rng = np.random.default_rng(5)
+    for case in range(60):
+        n = int(rng.integers(1, 30))
+        scale = 10.0 ** rng.uniform(-4, 2)  # compliances both below and above 1
+        c = scale * (3.0 + rng.uniform(0.01, 2.0) * rng.uniform(0.2, 0.97) ** np.arange(n))
+        c *= 1 + rng.normal(0, 10 ** rng.uniform(-5, -2), n)
+        g = [np.zeros(n), -0.4 * 0.05 * np.ones(n), 0.3 * (0.95 ** np.arange(1, n + 1) - 1)][case % 3]
+        assert _stop_flags(c, g, True) == reference.converge_run(1, 2, 5e-3, c, g).tolist(), case
+        assert _stop_flags(c, g, False) == reference.converge_run(1, 2, 5e-3, c, g, float_abs=True).tolist(), case
