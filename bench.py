@@ -771,7 +771,8 @@ def run_kernel(args):
             names = ["residual", "applyK", "jacobi", "chebyshev"]
             shapes = {f"{names[mode]}_{'f32' if prec == rb.FP32 else 'f64'}":
                       {"variant": ["smem_tile", "register_march", "register_march_prefetch", "smem_tile_pipelined",
-                                   "smem_tile_pairs_f32", "sum_factorised", "smem_tile_pipelined_tma"][variant],
+                                   "smem_tile_pairs_f32", "sum_factorised", "smem_tile_pipelined_tma",
+                                   "smem_tile_pipelined_tma_x31"][variant],
                        "rows": ty,
                        "zchunk": zc}}
         else:

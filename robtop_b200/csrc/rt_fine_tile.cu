@@ -95,7 +95,14 @@ __device__ __forceinline__ void node_smooth(const rte::KtVals<T>& kt, const floa
     // inverse of [[A,bxy,bxz],[bxy,A,byz],[bxz,byz,A]]
     const T c00 = A * A - byz * byz, c01 = -(bxy * A - byz * bxz), c02 = bxy * byz - A * bxz;
     const T c11 = A * A - bxz * bxz, c12 = -(A * byz - bxy * bxz), c22 = A * A - bxy * bxy;
-    const T id = T(1) / (A * c00 + bxy * c01 + bxz * c02);
+    // FP32: the reciprocal by the fast-division intrinsic (2 ulp; the block's determinant is far
+    // inside its range); FP64: IEEE division
+    const T det = A * c00 + bxy * c01 + bxz * c02;
+    T id;
+    if constexpr (sizeof(T) == 4)
+        id = __fdividef(1.0f, det);
+    else
+        id = T(1) / det;
     T rr[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) rr[c] = fv[c] - acc[c];
@@ -781,32 +788,55 @@ __global__ void __launch_bounds__(PTile<TY_>::BS, pair_min_blocks<TY_>()) k_fine
 
 
 // ---------------------------------------------------------------------------
-// variant 6: the pipelined tile kernel with its node layers staged by the Tensor Memory
+// variants 6 and 7: the pipelined tile kernel with its node layers staged by the Tensor Memory
 // Accelerator.  One thread issues, per node layer, a 4-D tiled bulk tensor copy of the
-// (TY+2) x 40 node halo box of all three components (x from X0 - 4, so the box starts on a
-// 16-byte boundary; the halo's first column sits at x index 3) and, with supports, a 3-D copy
-// of the 64-wide box of support flags (x from X0 - 16), into a ring of 3 shared slots completed
-// on one mbarrier each.  Layer t + 3 is issued at the top of iteration t, into the slot whose
-// last reader ran before the previous barrier, and waited for at its end, so the copy overlaps
-// that iteration's element and node work (the register prefetch of variant 3, without its load
-// instructions); coordinates outside the node box read as zeros (the tile kernel's halo rule).
-// After a layer's barrier completes, the block zeroes the displacements of fixed nodes (the WS
-// rule) before the iteration's block-wide barrier.  Every mbarrier wait is bounded: a timed-out
-// wait flags *err = 3, poisons out[0], waits (bounded) for the block's copies still in flight and
-// returns.  Applies where the node box's x extent is a multiple of 16 (the tensor maps' row pitch
-// must be a multiple of 16 bytes for the one-byte flags); the tensor maps cover this GPU's own
-// memory and no copy uses multicast.
+// (TY+2) x 40 node halo box of all three components (x from the halo's first column X0 - 1
+// rounded down to a 16-byte boundary, at most 3 columns earlier) and, with supports, a 3-D copy
+// of the 64-wide box of support flags (x rounded down to a multiple of 16), into a ring of 3
+// shared slots completed on one mbarrier each.  Layer t + 3 is issued at the top of iteration t,
+// into the slot of layer t, whose last reader (element phase t) ran before the previous barrier,
+// and waited for at its end, so the copy overlaps that iteration's element and node work (the
+// register prefetch of variant 3, without its load instructions).  (A fourth slot, which would
+// let the node phase read its own u from shared memory, costs a block per SM at 4 rows and was
+// slower.)  Coordinates outside the node box read as zeros (the tile kernel's halo rule).  After a layer's barrier completes, the block
+// zeroes the displacements of fixed nodes (the WS rule) before the iteration's block-wide
+// barrier.  Every mbarrier wait is bounded: a timed-out wait flags *err = 3, poisons out[0],
+// waits (bounded) for the block's copies still in flight and returns.  Applies where the node
+// box's x extent is a multiple of 16 (the tensor maps' row pitch must be a multiple of 16 bytes
+// for the one-byte flags); the tensor maps cover this GPU's own memory and no copy uses
+// multicast.  Variant 6 tiles 32 x TY nodes, variant 7 31 x TY (element rows of 32).
 // ---------------------------------------------------------------------------
-constexpr int TMA_BX = 40;  // node box x extent (x from X0 - 4)
-constexpr int TMA_FX = 64;  // flag box x extent (x from X0 - 16)
+constexpr int TMA_BX = 40;  // node box x extent (x from the halo's first column rounded down to 4)
+constexpr int TMA_FX = 64;  // flag box x extent (x from the same column rounded down to 16)
 
-template <typename T, int TY_>
+// tile of the TMA-staged kernel: TXN x TY nodes.  Node threads are laid out one warp per node row
+// (lane = x; with TXN = 31 the last lane of each row idles); element threads (TXN+1) x (TY+1).
+// TXN = 32 is variant 3's tile; TXN = 31 makes the element tile 32 x (TY+1), whole warps, where
+// the 33-wide rows of TXN = 32 leave a last warp with TY+1 of 32 lanes busy.
+template <int TY_, int TXN>
+struct TTile {
+    static constexpr int TX = TXN, TY = TY_;
+    static constexpr int EXT = TX + 1, EYT = TY + 1;  // element tile
+    static constexpr int UXT = TX + 2, UYT = TY + 2;  // node halo tile
+    static constexpr int NE_T = EXT * EYT;
+    static constexpr int NU_T = UXT * UYT;
+    static constexpr int NODE_T = 32 * TY;
+    static constexpr int BS = ((NE_T > NODE_T ? NE_T : NODE_T) + 31) / 32 * 32;
+};
+
+template <typename T, int TY_, int TXN>
+constexpr int tma_min_blocks() {
+    return sizeof(T) == 8 ? (TY_ == 4 ? 2 : 1) : (TY_ == 4 ? 5 : 3);
+}
+
+template <typename T, int TY_, int TXN>
 struct TmaSmem {
     static constexpr int SLOT = ((3 * (TY_ + 2) * TMA_BX * (int)sizeof(T) + 127) / 128 * 128) / (int)sizeof(T);
+    static constexpr int NE_T = TTile<TY_, TXN>::NE_T;
     alignas(128) T u[3][SLOT];                       // node layer j (relative to zb - 1) in slot j % 3: [3][TY+2][40]
     alignas(128) uint8_t fx[3][(TY_ + 2) * TMA_FX];  // support flags of the same layers: [TY+2][64]
-    T e[2][24][Tile<TY_>::NE_T];
-    float w[4][Tile<TY_>::NE_T];
+    T e[2][24][NE_T];
+    float w[4][NE_T];
     uint64_t bar[3];
 };
 
@@ -827,15 +857,15 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
-template <typename T, bool WS, int MODE, int TY_>
-__global__ void __launch_bounds__(Tile<TY_>::BS, pipe_min_blocks<T, TY_>()) k_fine_pipe_tma(
+template <typename T, bool WS, int MODE, int TY_, int TXN>
+__global__ void __launch_bounds__(TTile<TY_, TXN>::BS, tma_min_blocks<T, TY_, TXN>()) k_fine_pipe_tma(
     int nx, int ny, int nz, int zchunk, const uint8_t* __restrict__ vact, const float* __restrict__ wgt,
     const uint8_t* __restrict__ vfix, const rte::KtVals<T> kt, const __grid_constant__ CUtensorMap umap,
     const __grid_constant__ CUtensorMap fmap, const T* __restrict__ u, const T* __restrict__ f, T* __restrict__ out,
     T omega, T* __restrict__ dvec, const double* __restrict__ coef, int kstep, double* err) {
-    using TS = Tile<TY_>;
+    using TS = TTile<TY_, TXN>;
     constexpr int TX = TS::TX, TY = TS::TY, EXT = TS::EXT, UXT = TS::UXT, NE_T = TS::NE_T, NU_T = TS::NU_T;
-    constexpr int TILE_BS = TS::BS;
+    constexpr int TILE_BS = TS::BS, NODE_T = TS::NODE_T;
     constexpr int ROWB = TMA_BX;           // row pitch of a staged component
     constexpr int CP = (TY + 2) * TMA_BX;  // component pitch of a staged layer
     constexpr uint32_t UBYTES = 3u * (TY + 2) * TMA_BX * sizeof(T);
@@ -843,8 +873,8 @@ __global__ void __launch_bounds__(Tile<TY_>::BS, pipe_min_blocks<T, TY_>()) k_fi
     // the copies' shared destinations sit on 128-byte boundaries: the block's dynamic shared
     // memory (sizeof(TmaSmem) + 128 bytes) is rounded up to one
     extern __shared__ __align__(16) unsigned char smraw[];
-    TmaSmem<T, TY_>& S =
-        *reinterpret_cast<TmaSmem<T, TY_>*>(smraw + ((128 - (rttc::smem_u32(smraw) & 127)) & 127));
+    TmaSmem<T, TY_, TXN>& S =
+        *reinterpret_cast<TmaSmem<T, TY_, TXN>*>(smraw + ((128 - (rttc::smem_u32(smraw) & 127)) & 127));
     T cheb_a = T(0), cheb_b = T(0);
     if (MODE == 3) {
         const double ca = coef[2 * kstep], cb = coef[2 * kstep + 1];
@@ -858,23 +888,27 @@ __global__ void __launch_bounds__(Tile<TY_>::BS, pipe_min_blocks<T, TY_>()) k_fi
     const int zb = blockIdx.z * zchunk;
     const int ze = min(zb + zchunk, vz);
     const int tid = threadIdx.x;
-    const int nxl = tid % TX, nyl = tid / TX;
+    const int nxl = tid & 31, nyl = tid >> 5;
     const int nxg = x0 + nxl, nyg = y0 + nyl;
-    const bool node_thread = tid < TX * TY && nxg < vx && nyg < vy;
+    const bool node_thread = tid < NODE_T && nxl < TX && nxg < vx && nyg < vy;
     const long vxy = node_thread ? nxg + (long)vx * nyg : 0;
     const int exl = tid % EXT, eyl = tid / EXT;
     const int exg = x0 - 1 + exl, eyg = y0 - 1 + eyl;
     const bool elem_xy = tid < NE_T && exg >= 0 && eyg >= 0 && exg < nx && eyg < ny;
     const long exy = elem_xy ? exg + (long)nx * eyg : 0;
     const int zlast = ze;  // node layers zb - 1 .. ze are read
+    // the halo's first column x0 - 1, rounded down to the copies' 16-byte boundaries (4 or 2
+    // elements of the node vectors, 16 one-byte flags), and its index inside the staged boxes
+    const int xs = (x0 - 1) & ~3, xf = (x0 - 1) & ~15;
+    const int off = (x0 - 1) - xs, offf = (x0 - 1) - xf;
     // layer L lives in slot (L - zb + 1) % 3, phase parity ((L - zb + 1) / 3) & 1
     auto slot_of = [&](int L) { return (L - zb + 1) % 3; };
     auto parity_of = [&](int L) { return (uint32_t)(((L - zb + 1) / 3) & 1); };
     auto issue = [&](int L) {  // thread 0 only
         const int sl = slot_of(L);
         rttc::mbar_expect_tx(&S.bar[sl], UBYTES + FBYTES);
-        tma_load_4d(&S.u[sl][0], &umap, x0 - 4, y0 - 1, L, 0, &S.bar[sl]);
-        if (WS) tma_load_3d(&S.fx[sl][0], &fmap, x0 - 16, y0 - 1, L, &S.bar[sl]);
+        tma_load_4d(&S.u[sl][0], &umap, xs, y0 - 1, L, 0, &S.bar[sl]);
+        if (WS) tma_load_3d(&S.fx[sl][0], &fmap, xf, y0 - 1, L, &S.bar[sl]);
     };
     // every thread waits for layer L; false if the wait ran out
     auto wait_layer = [&](int L) -> bool { return rttc::mbar_wait(&S.bar[slot_of(L)], parity_of(L)); };
@@ -884,8 +918,8 @@ __global__ void __launch_bounds__(Tile<TY_>::BS, pipe_min_blocks<T, TY_>()) k_fi
         const int sl = slot_of(L);
         for (int i = tid; i < NU_T; i += TILE_BS) {
             const int row = i / UXT, col = i % UXT;
-            if (S.fx[sl][row * TMA_FX + col + 15]) {
-                T* b = &S.u[sl][row * ROWB + col + 3];
+            if (S.fx[sl][row * TMA_FX + col + offf]) {
+                T* b = &S.u[sl][row * ROWB + col + off];
                 b[0] = T(0);
                 b[CP] = T(0);
                 b[2 * CP] = T(0);
@@ -919,7 +953,7 @@ __global__ void __launch_bounds__(Tile<TY_>::BS, pipe_min_blocks<T, TY_>()) k_fi
 #pragma unroll
             for (int vtx = 0; vtx < 8; vtx++) {
                 const T* src = (vtx & 4) ? hi : lo;
-                const int idx = (eyl + ((vtx >> 1) & 1)) * ROWB + exl + (vtx & 1) + 3;
+                const int idx = (eyl + ((vtx >> 1) & 1)) * ROWB + exl + (vtx & 1) + off;
                 a[3 * vtx] = src[idx];
                 a[3 * vtx + 1] = src[CP + idx];
                 a[3 * vtx + 2] = src[2 * CP + idx];
@@ -1123,7 +1157,7 @@ bool tmap_get(const void* p, int esize, int vx, int vy, int vz, int rows, CUtens
     return true;
 }
 
-template <typename T, bool WS, int MODE, int TY_>
+template <typename T, bool WS, int MODE, int TY_, int TXN>
 int launch_tma_ty(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name, T* dvec,
                   const double* coef, int kstep, bool* done) {
     rt_level& L = h->L[0];
@@ -1135,11 +1169,12 @@ int launch_tma_ty(rt_hier* h, const T* u, const T* f, T* out, double omega, cons
     if (!tmap_get(u, (int)sizeof(T), L.vx, L.vy, L.vz, TY_ + 2, &umap)) return RT_OK;
     if (WS && !tmap_get(h->vfix, 1, L.vx, L.vy, L.vz, TY_ + 2, &fmap)) return RT_OK;
     const int zc = h->tune[sizeof(T) == 8 ? 1 : 0][MODE].zchunk;
-    dim3 grid((L.vx + Tile<TY_>::TX - 1) / Tile<TY_>::TX, (L.vy + TY_ - 1) / TY_, (L.vz + zc - 1) / zc);
+    dim3 grid((L.vx + TXN - 1) / TXN, (L.vy + TY_ - 1) / TY_, (L.vz + zc - 1) / zc);
     const rte::KtVals<T> kt = rte::make_kt<T>(h);
     *done = true;
     return rt_launch(h->ctx, name, [&] {
-        k_fine_pipe_tma<T, WS, MODE, TY_><<<grid, Tile<TY_>::BS, sizeof(TmaSmem<T, TY_>) + 128, h->ctx->stream>>>(
+        k_fine_pipe_tma<T, WS, MODE, TY_, TXN>
+            <<<grid, TTile<TY_, TXN>::BS, sizeof(TmaSmem<T, TY_, TXN>) + 128, h->ctx->stream>>>(
             L.nx, L.ny, L.nz, zc, L.vact, h->w, h->vfix, kt, umap, fmap, u, f, out, (T)omega, dvec, coef, kstep,
             h->scal + RT_SCAL_ERR);
     });
@@ -1178,20 +1213,26 @@ int launch_pair_ty(rt_hier* h, const float* u, const float* f, float* out, doubl
 
 // variant 0: two barriers per element layer; 3: software-pipelined, one barrier per layer;
 // 4 (FP32): pipelined with element pairs in packed FP32; 5: sum-factorised row marching (rt_fine_sf.cu);
-// 6: variant 3 with its node layers staged by TMA (node boxes whose x extent is a multiple of 16)
+// 6: variant 3 with its node layers staged by TMA (node boxes whose x extent is a multiple of 16);
+// 7: variant 6 on 31-node-wide tiles (element rows of 32: whole warps)
 template <typename T, bool WS, int MODE>
 int launch_tile(rt_hier* h, const T* u, const T* f, T* out, double omega, const char* name, T* dvec = nullptr,
                 const double* coef = nullptr, int kstep = 0) {
     const rt_tile_cfg& tn = h->tune[sizeof(T) == 8 ? 1 : 0][MODE];
     if (tn.variant == 5) return rtk::launch_sf<T, WS, MODE>(h, u, f, out, omega, name, dvec, coef, kstep);
-    if (tn.variant == 6 && h->L[0].vx % 16 == 0) {
+    if ((tn.variant == 6 || tn.variant == 7) && h->L[0].vx % 16 == 0) {
         bool done = false;
-        const int st = tn.ty == 4 ? launch_tma_ty<T, WS, MODE, 4>(h, u, f, out, omega, name, dvec, coef, kstep, &done)
-                                  : launch_tma_ty<T, WS, MODE, 8>(h, u, f, out, omega, name, dvec, coef, kstep, &done);
+        int st;
+        if (tn.variant == 6)
+            st = tn.ty == 4 ? launch_tma_ty<T, WS, MODE, 4, 32>(h, u, f, out, omega, name, dvec, coef, kstep, &done)
+                            : launch_tma_ty<T, WS, MODE, 8, 32>(h, u, f, out, omega, name, dvec, coef, kstep, &done);
+        else
+            st = tn.ty == 4 ? launch_tma_ty<T, WS, MODE, 4, 31>(h, u, f, out, omega, name, dvec, coef, kstep, &done)
+                            : launch_tma_ty<T, WS, MODE, 8, 31>(h, u, f, out, omega, name, dvec, coef, kstep, &done);
         if (done || st != RT_OK) return st;
         // the tensor maps could not be made: the same schedule with per-thread loads
     }
-    if (tn.variant == 6) {
+    if (tn.variant == 6 || tn.variant == 7) {
         switch (tn.ty) {
             case 4: return launch_tile_ty<T, WS, MODE, 4, true>(h, u, f, out, omega, name, dvec, coef, kstep);
             default: return launch_tile_ty<T, WS, MODE, 8, true>(h, u, f, out, omega, name, dvec, coef, kstep);
@@ -1229,21 +1270,27 @@ cudaError_t set_attr() {
                                 (int)sizeof(PipeSmem<T, TY_>));
 }
 
-template <typename T, bool WS, int MODE, int TY_>
+template <typename T, bool WS, int MODE, int TY_, int TXN>
 cudaError_t set_attr_tma() {
-    return cudaFuncSetAttribute(k_fine_pipe_tma<T, WS, MODE, TY_>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sizeof(TmaSmem<T, TY_>) + 128);
+    return cudaFuncSetAttribute(k_fine_pipe_tma<T, WS, MODE, TY_, TXN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(TmaSmem<T, TY_, TXN>) + 128);
+}
+
+template <typename T, int TY_, int TXN>
+cudaError_t set_attrs_tma_x() {
+    cudaError_t r[8] = {set_attr_tma<T, false, 0, TY_, TXN>(), set_attr_tma<T, false, 1, TY_, TXN>(),
+                        set_attr_tma<T, false, 2, TY_, TXN>(), set_attr_tma<T, false, 3, TY_, TXN>(),
+                        set_attr_tma<T, true, 0, TY_, TXN>(),  set_attr_tma<T, true, 1, TY_, TXN>(),
+                        set_attr_tma<T, true, 2, TY_, TXN>(),  set_attr_tma<T, true, 3, TY_, TXN>()};
+    for (auto x : r)
+        if (x != cudaSuccess) return x;
+    return cudaSuccess;
 }
 
 template <typename T, int TY_>
 cudaError_t set_attrs_tma() {
-    cudaError_t r[8] = {set_attr_tma<T, false, 0, TY_>(), set_attr_tma<T, false, 1, TY_>(),
-                        set_attr_tma<T, false, 2, TY_>(), set_attr_tma<T, false, 3, TY_>(),
-                        set_attr_tma<T, true, 0, TY_>(),  set_attr_tma<T, true, 1, TY_>(),
-                        set_attr_tma<T, true, 2, TY_>(),  set_attr_tma<T, true, 3, TY_>()};
-    for (auto x : r)
-        if (x != cudaSuccess) return x;
-    return cudaSuccess;
+    const cudaError_t a = set_attrs_tma_x<T, TY_, 32>();
+    return a != cudaSuccess ? a : set_attrs_tma_x<T, TY_, 31>();
 }
 
 template <bool WS, int MODE, int TY_>

@@ -369,7 +369,8 @@ class HierarchyGrid:
                 v, ty, zc, us = C.c_int(), C.c_int(), C.c_int(), C.c_double()
                 self._c(A.lib().rt_tuning_info(self._h, prec, m, C.byref(v), C.byref(ty), C.byref(zc), C.byref(us)))
                 out[f"{mname}_{pname}"] = {"variant": ["smem_tile", "register_march", "register_march_prefetch", "smem_tile_pipelined", "smem_tile_pairs_f32",
-                                                       "sum_factorised", "smem_tile_pipelined_tma"][v.value], "rows": ty.value,
+                                                       "sum_factorised", "smem_tile_pipelined_tma",
+                                                       "smem_tile_pipelined_tma_x31"][v.value], "rows": ty.value,
                                            "zchunk": zc.value, "us": round(us.value, 2)}
         for lvl in range(1, self.n_grid() - 1):
             on, t0, t1 = C.c_int(), C.c_double(), C.c_double()

@@ -58,6 +58,15 @@ int main(int argc, char** argv) {
     double csum = 0;
     for (float v : ceh) csum += v;
     printf("element_compliance_sum %.17g\n", csum);
+    {  // u.K u of the same displacement, by the operator (host copies; the force stays as it is)
+        const long long nvb0 = g0->n_box_nodes();
+        std::vector<double> uh(3 * nvb0), kuh(3 * nvb0);
+        rt_get(getGrids().hier(), RT_FIELD_U, 0, RT_LAYOUT_DENSE, uh.data());
+        rt_apply_K(getGrids().hier(), uh.data(), kuh.data());
+        double uku = 0;
+        for (long long i = 0; i < 3 * nvb0; i++) uku += uh[i] * kuh[i];
+        printf("worst_uKu %.17g\n", uku);
+    }
     printf("worst_compliance2 %.17g\n", mu2);
     // projection API (wsff: the projection keeps the load-node values, zeroes every other node)
     printf("n_loadnodes %d\n", n_loadnodes());

@@ -39,7 +39,8 @@ def test_compat_flow_matches_oracle():
     assert vals["levels"] == H.nlev
     # test_rigid_displacement: K u_rigid vanishes away from the supports; with supports the
     # residual is nonzero only through the clamped nodes, so compare with the oracle's value
-    assert len(rigid) == 6
+    # (six modes from the explicit call, six more from selfTest, which repeats it)
+    assert len(rigid) == 12 and np.allclose(rigid[:6], rigid[6:], rtol=1e-9, atol=0)
     # solveFEM: V-cycles to 1e-4 on the preloaded force
     b = cfg["fload"].ravel().copy()
     H.arrs[0]["f"][:] = b
@@ -70,8 +71,9 @@ def test_compat_remaining_entry_points():
     file round trip, driven through the reference-signature layer."""
     vals, rigid = run_driver()
     assert vals["adjoint_ok"] == 1 and vals["adjoint_zero_ok"] == 0
-    # element compliances sum to u.K u = f.u of the worst-case pair
-    assert abs(vals["element_compliance_sum"] - vals["worst_compliance2"]) <= 1e-5 * vals["worst_compliance2"]
+    # element compliances of the worst-case displacement sum to its u.K u (the modified power
+    # method's last displacement is one V-cycle from the last load, so f.u differs from it)
+    assert abs(vals["element_compliance_sum"] - vals["worst_uKu"]) <= 1e-5 * vals["worst_uKu"]
     cfg = configs.cantilever(24, 12, 12)
     assert vals["n_loadnodes"] == cfg["load_nodes"].size
     # wsff: the support force of the unit worst-case load has norm 1 and P keeps it
@@ -86,7 +88,6 @@ def test_compat_remaining_entry_points():
     assert 0.9 * lam <= vals["incomplete_pm"] <= lam * (1 + 1e-6)
     assert abs(vals["mgpsor"] - lam) <= 1e-2 * lam
     assert vals["density_roundtrip"] == 1
-    assert len(rigid) == 6
     # optimization(): at most the 12 iterations asked for, the goal at the volume ratio, finite
     # compliances (the stop test needs at least four values before it can pass)
     assert 1 <= vals["opt_iterations"] <= 12
