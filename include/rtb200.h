@@ -120,6 +120,7 @@ typedef struct rt_level_info {
 typedef struct rt_ctx rt_ctx;
 typedef struct rt_hier rt_hier;
 typedef struct rt_unet rt_unet;
+typedef struct rt_mma rt_mma;
 
 /* ---- context ------------------------------------------------------------ */
 int rt_ctx_create(int device, void* cuda_stream /* NULL: own stream */, rt_ctx** out);
@@ -367,6 +368,30 @@ int rt_oc_update(rt_hier* h, float vgoal, float* lambda_out, int* trials_out);
  * update_stencil, worst-case solve, sensitivity+filter, OC update */
 int rt_oc_iteration(rt_hier* h, int method, int k, double inner_tol, uint64_t seed, float vgoal,
                     double* compliance_out);
+
+/* ---- method of moving asymptotes, one inequality constraint (optimization/mma_t.h:159-273) ---- */
+/* mma_t(n, 1) + init(lower, upper) (optimization/mma_t.h:208-221, mma_t.cu:790-824): n design
+ * variables with bounds xmin / xmax (host arrays), or, when both pointers are null, the uniform
+ * bounds [uniform_min, uniform_max]; the design starts at the middle of its bounds */
+int rt_mma_create(rt_ctx* ctx, long long n, const double* xmin, const double* xmax, double uniform_min,
+                  double uniform_max, rt_mma** out);
+int rt_mma_destroy(rt_mma* m);
+/* mma_t::update (optimization/mma_t.cpp:18-51): one MMA step for min f0 s.t. f1 <= 0, from the
+ * objective gradient df_dev and the constraint gradient dg_dev (device, n floats each, as the
+ * reference's Scalar) and the constraint value g; the subproblem (a0 = 1, a = 0, c = 10, d = 1)
+ * is solved exactly through its one-multiplier dual; *stop = 1 once more than 10 steps were
+ * shorter than 1e-3 (the reference's stop rule); *lambda_out = the multiplier, *dxnorm_out = |dx|
+ * (each may be null) */
+int rt_mma_update(rt_mma* m, const float* df_dev, const float* dg_dev, double g, int* stop, double* lambda_out,
+                  double* dxnorm_out);
+/* mma_t::get_x: the design (device pointer owned by the state, n doubles), or a host copy */
+int rt_mma_x(rt_mma* m, const double** x_dev);
+int rt_mma_get_x(rt_mma* m, double* x_host);
+/* setDensity(mma.get_x()) (utils/test_utils.cpp:1672): the design as the finest level's densities
+ * (FP32, zero on inactive elements; n must be the element count of the dense finest level) */
+int rt_mma_set_density(rt_mma* m, rt_hier* h);
+/* dual-derivative evaluations run so far (each one pass over the design variables) */
+long long rt_mma_evaluations(rt_mma* m);
 
 /* ---- learned preconditioner (3D U-Net, BF16 activations, FP32 accumulation) ---- */
 /* No reference counterpart.  One 3x3x3 convolution (zero padding 1) on the tensor cores:

@@ -101,6 +101,8 @@ def lib():
             "or_voxel_box": (None, [P, C.c_long, C.c_int, P, P, P, P]),
             "or_voxelize_solid": (None, [P, P, C.c_long, C.c_int, P, P, P]),
             "or_word_reverse": (None, [C.c_long, P]),
+            "or_mma_init": (None, [C.c_long, P, P, P, P, P, P, P, P]),
+            "or_mma_update": (C.c_double, [C.c_long, P, P, C.c_double, P, P, P, P, P, P, P, P, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -368,3 +370,29 @@ def word_reverse(bits):
     out = np.array(bits, np.uint32, copy=True)
     lib().or_word_reverse(out.size, ptr(out))
     return out
+
+
+class MMA:
+    """The oracle's MMA state for one constraint (or_mma.c): bounds xmin, xmax (arrays or
+    scalars); update(df, dg, g) takes one step and returns the multiplier."""
+
+    def __init__(self, n, xmin, xmax):
+        self.n = int(n)
+        self.xmin = np.ascontiguousarray(np.broadcast_to(np.asarray(xmin, np.float64), (self.n,)))
+        self.xmax = np.ascontiguousarray(np.broadcast_to(np.asarray(xmax, np.float64), (self.n,)))
+        z = lambda: np.zeros(self.n)
+        self.x, self.low, self.upp, self.alpha, self.beta, self.lastdx = z(), z(), z(), z(), z(), z()
+        self.work = np.zeros(4 * self.n)
+        self.dxnorm = 0.0
+        lib().or_mma_init(self.n, ptr(self.xmin), ptr(self.xmax), ptr(self.x), ptr(self.low), ptr(self.upp),
+                          ptr(self.alpha), ptr(self.beta), ptr(self.lastdx))
+
+    def update(self, df, dg, g):
+        df = np.ascontiguousarray(df, np.float64)
+        dg = np.ascontiguousarray(dg, np.float64)
+        dn = np.zeros(1)
+        lam = lib().or_mma_update(self.n, ptr(df), ptr(dg), float(g), ptr(self.xmin), ptr(self.xmax), ptr(self.x),
+                                  ptr(self.low), ptr(self.upp), ptr(self.alpha), ptr(self.beta), ptr(self.lastdx),
+                                  ptr(dn), ptr(self.work))
+        self.dxnorm = float(dn[0])
+        return lam

@@ -151,6 +151,13 @@ SIGNATURES = {
     "rt_filter_sensitivity": (I, [P, F]),
     "rt_oc_update": (I, [P, F, C.POINTER(F), C.POINTER(I)]),
     "rt_oc_iteration": (I, [P, I, I, D, C.c_uint64, F, C.POINTER(D)]),
+    "rt_mma_create": (I, [P, C.c_longlong, P, P, D, D, C.POINTER(P)]),
+    "rt_mma_destroy": (I, [P]),
+    "rt_mma_update": (I, [P, P, P, D, C.POINTER(I), C.POINTER(D), C.POINTER(D)]),
+    "rt_mma_x": (I, [P, C.POINTER(P)]),
+    "rt_mma_get_x": (I, [P, P]),
+    "rt_mma_set_density": (I, [P, P]),
+    "rt_mma_evaluations": (C.c_longlong, [P]),
 }
 
 _lib = None

@@ -754,7 +754,8 @@ double inCompleteModiPM(double fch_thres) {
 }
 
 // MGPSOR (optimization/optimization.cpp:474-535): inCompleteModiPM, then preconditioned
-// eigen-iterations x <- x + Vcycle(P x - lambda K x) with lambda = |P x|^2 / x.K x
+// eigen-iterations x <- x + Vcycle(P x - lambda K x) with lambda = |P x|^2 / x.K x; like the
+// reference it returns u.K u for u = x / |P x|, i.e. 1 / lambda
 double MGPSOR(void) {
     grid::Grid* g = grids[0];
     inCompleteModiPM();
@@ -893,3 +894,81 @@ double** getPreloadForce(void) {
     if (nl > 0) gpu_manager_t::upload_buf(fl[0], soa.data(), sizeof(double) * soa.size());
     return fl;
 }
+
+// setDensity (utils/test_utils.cpp:1672) and Grid::volumeRatio
+void setDensity(const float* rho_dev) {
+    grids.check(rt_put_dev(grids.hier(), RT_FIELD_RHO, 0, rho_dev), "setDensity");
+}
+
+double volumeRatio(void) {
+    rt_hier* h = grids.hier();
+    rt_level_info li;
+    grids.check(rt_hier_level_info(h, 0, &li), "volumeRatio");
+    const size_t ne = (size_t)li.nx * li.ny * li.nz;
+    std::vector<float> rho(ne);
+    std::vector<uint8_t> act(ne);
+    grids.check(rt_get(h, RT_FIELD_RHO, 0, RT_LAYOUT_DENSE, rho.data()), "volumeRatio");
+    grids.check(rt_get(h, RT_FIELD_EACT, 0, RT_LAYOUT_DENSE, act.data()), "volumeRatio");
+    double s = 0;
+    long long na = 0;
+    for (size_t e = 0; e < ne; e++)
+        if (act[e]) {
+            s += rho[e];
+            na++;
+        }
+    return na ? s / (double)na : 0.0;
+}
+
+namespace MMA {
+namespace {
+__global__ void k_d2f(long long n, const double* __restrict__ x, float* __restrict__ y) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        y[i] = (float)x[i];
+}
+}  // namespace
+
+mma_t::mma_t(int ndim, int nConstrain, double) : _n(ndim) {
+    if (nConstrain != 1) throw std::invalid_argument("mma_t: this implementation takes exactly one constraint");
+    if (ndim < 1) throw std::invalid_argument("mma_t: no design variables");
+}
+
+mma_t::~mma_t() {
+    if (_m) rt_mma_destroy(_m);
+    if (_x32 && cudaFree(nullptr) == cudaSuccess) cudaFree(_x32);
+}
+
+void mma_t::init(float lower_bound, float upper_bound) {
+    if (_m) rt_mma_destroy(_m);
+    _m = nullptr;
+    grids.check(rt_mma_create(grids.ctx(), _n, nullptr, nullptr, lower_bound, upper_bound, &_m), "mma_t::init");
+}
+
+void mma_t::init(const float* lower_bound_host, const float* upper_bound_host) {
+    std::vector<double> lo(lower_bound_host, lower_bound_host + _n), hi(upper_bound_host, upper_bound_host + _n);
+    if (_m) rt_mma_destroy(_m);
+    _m = nullptr;
+    grids.check(rt_mma_create(grids.ctx(), _n, lo.data(), hi.data(), 0.0, 0.0, &_m), "mma_t::init");
+}
+
+bool mma_t::update(float* dev_df, float** dg, float* dev_g) {
+    if (!_m) throw std::runtime_error("mma_t::update: call init first");
+    float g = 0;
+    ck_cuda(cudaMemcpy(&g, dev_g, sizeof(float), cudaMemcpyDeviceToHost), "mma_t::update");
+    int stop = 0;
+    grids.check(rt_mma_update(_m, dev_df, dg[0], (double)g, &stop, nullptr, nullptr), "mma_t::update");
+    return stop != 0;
+}
+
+mma_t::XView mma_t::get_x(void) {
+    if (!_m) throw std::runtime_error("mma_t::get_x: call init first");
+    if (!_x32) ck_cuda(cudaMalloc(&_x32, sizeof(float) * (size_t)_n), "mma_t::get_x");
+    const double* x = nullptr;
+    grids.check(rt_mma_x(_m, &x), "mma_t::get_x");
+    rt_ctx* c = grids.hier()->ctx;
+    const unsigned nb = (unsigned)std::min<long long>((_n + 255) / 256, 1184);
+    grids.check(rt_launch(c, "mma_design_f32", [&] { k_d2f<<<nb, 256, 0, c->stream>>>(_n, x, _x32); }), "mma_t::get_x");
+    ck_cuda(cudaStreamSynchronize(c->stream), "mma_t::get_x");
+    return XView{_x32};
+}
+}  // namespace MMA
+

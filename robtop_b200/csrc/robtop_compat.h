@@ -233,3 +233,41 @@ void getForceSupport(double const* const f_dev[3], std::vector<double> fs[3]);
 void setForceSupport(double const* const fsup[3], double* f_dev[3]);
 void displacementProject(double* u_dev[3]);
 double** getPreloadForce(void);
+
+// setDensity (utils/test_utils.cpp:1672): densities of the dense finest level from a device
+// array (FP32); the volume ratio of the current densities over the active elements
+// (Grid::volumeRatio)
+void setDensity(const float* rho_dev);
+double volumeRatio(void);
+
+// optimization/mma_t.h:159-273: the method of moving asymptotes with one constraint (the
+// reference's TestSuit::test2011 / testtest2011 drive it with the volume constraint).  The
+// subproblem is solved exactly through its one-multiplier dual; the state is FP64, the
+// gradients and the design view FP32 device arrays, as the reference's Scalar.
+namespace MMA {
+class mma_t {
+public:
+    struct XView {
+        float* p;
+        float* data() { return p; }
+    };
+    mma_t(int ndim, int nConstrain, double err_tol = 1e-7);
+    ~mma_t();
+    mma_t(const mma_t&) = delete;
+    mma_t& operator=(const mma_t&) = delete;
+    void init(float lower_bound, float upper_bound);
+    void init(const float* lower_bound_host, const float* upper_bound_host);
+    // one step: df (device, n), dg[0] (device, n) and g (device, 1 value); true once the
+    // reference's stop rule fires (more than 10 steps shorter than 1e-3)
+    bool update(float* dev_df, float** dg, float* dev_g);
+    XView get_x(void);  // FP32 device copy of the design, valid until the next update
+    int n_dim(void) const { return _n; }
+    int n_constrain(void) const { return 1; }
+
+private:
+    int _n;
+    ::rt_mma* _m = nullptr;
+    float* _x32 = nullptr;
+};
+}  // namespace MMA
+

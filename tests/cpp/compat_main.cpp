@@ -126,6 +126,43 @@ int main(int argc, char** argv) {
     printf("opt_first_compliance %.17g\n", crec.front());
     printf("opt_last_compliance %.17g\n", crec.back());
     printf("opt_last_volume_goal %.9g\n", vols.back());
+    // TestSuit::testtest2011 (utils/test_utils.cpp:1750-1800): MMA steps on the densities with
+    // the volume constraint scaled by 1e3 and the sensitivity by 1e5
+    {
+        rt_level_info l0;
+        rt_hier_level_info(getGrids().hier(), 0, &l0);
+        const int ne = l0.nx * l0.ny * l0.nz;
+        std::vector<uint8_t> act(ne);
+        rt_get(getGrids().hier(), RT_FIELD_EACT, 0, RT_LAYOUT_DENSE, act.data());
+        long long na = 0;
+        for (uint8_t a : act) na += a;
+        std::vector<float> dvh(ne), sh(ne);
+        for (int e = 0; e < ne; e++) dvh[e] = act[e] ? 1e3f / (float)na : 0.f;
+        float* dv = (float*)gpu_manager.add_buf("mma dv", sizeof(float) * ne, dvh.data());
+        float* sdev = (float*)gpu_manager.add_buf("mma sens", sizeof(float) * ne);
+        float* vdev = (float*)gpu_manager.add_buf("mma v", sizeof(float));
+        MMA::mma_t mma(ne, 1);
+        mma.init(1e-3f, 1.0f);
+        double c_mma = 0;
+        for (int itn = 0; itn < 3; itn++) {
+            setDensity(mma.get_x().data());
+            update_stencil();
+            const float v = 1e3f * (float)(volumeRatio() - 0.4);
+            gpu_manager_t::upload_buf(vdev, &v, sizeof(float));
+            c_mma = modifiedPM();
+            computeSensitivity();
+            gpu_manager_t::download_buf(sh.data(), getGrids()[0]->getSens(), sizeof(float) * ne);
+            for (float& x : sh) x *= 1e5f;
+            gpu_manager_t::upload_buf(sdev, sh.data(), sizeof(float) * ne);
+            mma.update(sdev, &dv, vdev);
+        }
+        setDensity(mma.get_x().data());
+        printf("mma_volume %.9g\n", volumeRatio());
+        printf("mma_compliance %.17g\n", c_mma);
+        gpu_manager.delete_buf(dv);
+        gpu_manager.delete_buf(sdev);
+        gpu_manager.delete_buf(vdev);
+    }
     // the mesh form of buildGrids (optimization/optimization.cpp:14-19): a 24 x 12 x 12 box
     // of 12 triangles, voxelised at gridreso R - 1 (cube 32^3)
     setParameters(0.4f, 0.0f, 0.03f, 2.0f, 0.5f, 3.0f, 1e-3f, R - 1, 1e6f, 0.4f, 0.0f, false, false);

@@ -86,7 +86,9 @@ def test_compat_remaining_entry_points():
     assert abs(vals["rayleigh_pnorm"] / vals["rayleigh_knorm"] - lam) <= 1e-3 * lam
     # the incomplete power method reaches the worst case to within its 1e-2 force-change threshold
     assert 0.9 * lam <= vals["incomplete_pm"] <= lam * (1 + 1e-6)
-    assert abs(vals["mgpsor"] - lam) <= 1e-2 * lam
+    # MGPSOR (optimization/optimization.cpp:474-535) ends with u = x / |P x| and returns u.K u =
+    # x.K x / |P x|^2, the reciprocal of the Rayleigh quotient it converged: 1 / lambda
+    assert abs(vals["mgpsor"] * lam - 1.0) <= 1e-2
     assert vals["density_roundtrip"] == 1
     # optimization(): at most the 12 iterations asked for, the goal at the volume ratio, finite
     # compliances (the stop test needs at least four values before it can pass)
@@ -94,3 +96,7 @@ def test_compat_remaining_entry_points():
     assert vals["opt_iterations"] == 12 or vals["opt_iterations"] >= 6
     assert abs(vals["opt_last_volume_goal"] - 0.4) <= 1e-6
     assert 0 < vals["opt_first_compliance"] < 1e30 and 0 < vals["opt_last_compliance"] < 1e30
+    # three MMA steps (MMA::mma_t, the testtest2011 loop) from the middle of the bounds (0.5005)
+    # move the volume towards the 0.4 target
+    assert 0 < vals["mma_compliance"] < 1e30
+    assert 0.3 < vals["mma_volume"] < 0.5

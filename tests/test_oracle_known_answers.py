@@ -382,3 +382,33 @@ def test_voxeliser_word_reverse_and_bit_order():
     vol = ((lsb[ids >> 5] >> (ids & 31)) & 1).reshape(R, R, R)  # [z][y][x]
     assert vol[R // 2, R // 2, R // 2] == 1 and vol[0, 0, 0] == 0
     assert np.count_nonzero(vol != vol[:, :, ::-1]) < 0.05 * vol.sum()
+
+
+def test_mma_reaches_the_separable_optimum():
+    """The oracle's MMA (or_mma.c, optimization/mma_t.cu's method with one constraint) on
+    min sum c_j / x_j / n s.t. 1e3 (mean(x) - V) <= 0, 0.01 <= x <= 1: 80 steps reach the known
+    optimum x_j = V n sqrt(c_j) / sum sqrt(c) (inside the bounds here) to 1e-12, and each step's
+    design satisfies the subproblem's stationarity: between its move bounds, the derivative of
+    the approximated Lagrangian vanishes."""
+    rng = np.random.default_rng(0)
+    n, V = 1000, 0.3
+    c = rng.uniform(0.5, 2.0, n)
+    m = O.MMA(n, 0.01, 1.0)
+    for it in range(80):
+        x0, low, upp, a, b = m.x.copy(), m.low.copy(), m.upp.copy(), m.alpha.copy(), m.beta.copy()
+        df, dg = -c / x0 ** 2 / n, np.full(n, 1e3 / n)
+        lam = m.update(df, dg, 1e3 * (x0.mean() - V))
+        if it < 5:
+            # p, q of both functions at x0 (mma_t.cu:70-81), then d/dx of sum (p0 + lam p1) / (U - x)
+            # + (q0 + lam q1) / (x - L) at the new design, zero where it is strictly inside [a, b]
+            r = 1e-5 / 0.99
+            pq = lambda f: ((upp - x0) ** 2 * (1.001 * np.maximum(f, 0) + 0.001 * np.maximum(-f, 0) + r),
+                            (x0 - low) ** 2 * (0.001 * np.maximum(f, 0) + 1.001 * np.maximum(-f, 0) + r))
+            (p0, q0), (p1, q1) = pq(df), pq(dg)
+            xn = m.x
+            grad = (p0 + lam * p1) / (upp - xn) ** 2 - (q0 + lam * q1) / (xn - low) ** 2
+            inside = (xn > a + 1e-12) & (xn < b - 1e-12)
+            scale = np.abs((p0 + lam * p1) / (upp - xn) ** 2).max()
+            assert np.abs(grad[inside]).max() <= 1e-9 * scale, it
+    xs = V * n * np.sqrt(c) / np.sqrt(c).sum()
+    assert np.abs(m.x - xs).max() <= 1e-12
