@@ -2460,8 +2460,9 @@ extern "C" int rt_autotune(rt_hier* h, int reps) {
         for (int zc : {16, 32, 64}) cands.push_back(rt_tile_cfg{5, ty, zc});  // ty 16: FP32 only
     if (h->L[0].vx % 16 == 0)  // TMA-staged node layers: the flags' row pitch must be a multiple of 16 bytes
         for (int v : {6, 7})
-            for (int ty : {4, 8})
-                for (int zc : {8, 16, 32, 64}) cands.push_back(rt_tile_cfg{v, ty, zc});
+            for (int ty : {4, 6, 8})
+                for (int zc : {8, 16, 32, 64})
+                    if (ty != 6 || v == 7) cands.push_back(rt_tile_cfg{v, ty, zc});
     for (int prec = 0; prec < 2; prec++)
         for (int mode = 0; mode < 4; mode++) {
             rt_tile_cfg best_cfg = h->tune[prec][mode];
@@ -2503,7 +2504,8 @@ extern "C" int rt_set_tuning(rt_hier* h, int precision, int mode, int variant, i
     if (variant == 5) {
         if (ty != 4 && ty != 8 && ty != 16) return rt_fail(h->ctx, RT_EINVAL, "sum-factorised rows per tile must be 4, 8 or 16");
     } else if (variant == 6 || variant == 7) {
-        if (ty != 4 && ty != 8) return rt_fail(h->ctx, RT_EINVAL, "TMA-staged rows per tile must be 4 or 8");
+        if (ty != 4 && ty != 8 && !(variant == 7 && ty == 6))
+            return rt_fail(h->ctx, RT_EINVAL, "TMA-staged rows per tile must be 4 or 8 (6 as well on 31-wide tiles)");
     } else if (variant != 2 && ty != 2 && ty != 4 && ty != 8) {
         return rt_fail(h->ctx, RT_EINVAL, "rows per tile must be 2, 4 or 8");
     }

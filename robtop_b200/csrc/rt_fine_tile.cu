@@ -826,7 +826,7 @@ struct TTile {
 
 template <typename T, int TY_, int TXN>
 constexpr int tma_min_blocks() {
-    return sizeof(T) == 8 ? (TY_ == 4 ? 2 : 1) : (TY_ == 4 ? 5 : 3);
+    return sizeof(T) == 8 ? (TY_ == 4 ? 2 : 1) : (TY_ == 4 ? 5 : 3);  // TY 6 and 8: 3 (FP32), 1 (FP64)
 }
 
 template <typename T, int TY_, int TXN>
@@ -1226,9 +1226,12 @@ int launch_tile(rt_hier* h, const T* u, const T* f, T* out, double omega, const 
         if (tn.variant == 6)
             st = tn.ty == 4 ? launch_tma_ty<T, WS, MODE, 4, 32>(h, u, f, out, omega, name, dvec, coef, kstep, &done)
                             : launch_tma_ty<T, WS, MODE, 8, 32>(h, u, f, out, omega, name, dvec, coef, kstep, &done);
+        else if (tn.ty == 4)
+            st = launch_tma_ty<T, WS, MODE, 4, 31>(h, u, f, out, omega, name, dvec, coef, kstep, &done);
+        else if (tn.ty == 6)
+            st = launch_tma_ty<T, WS, MODE, 6, 31>(h, u, f, out, omega, name, dvec, coef, kstep, &done);
         else
-            st = tn.ty == 4 ? launch_tma_ty<T, WS, MODE, 4, 31>(h, u, f, out, omega, name, dvec, coef, kstep, &done)
-                            : launch_tma_ty<T, WS, MODE, 8, 31>(h, u, f, out, omega, name, dvec, coef, kstep, &done);
+            st = launch_tma_ty<T, WS, MODE, 8, 31>(h, u, f, out, omega, name, dvec, coef, kstep, &done);
         if (done || st != RT_OK) return st;
         // the tensor maps could not be made: the same schedule with per-thread loads
     }
@@ -1290,7 +1293,8 @@ cudaError_t set_attrs_tma_x() {
 template <typename T, int TY_>
 cudaError_t set_attrs_tma() {
     const cudaError_t a = set_attrs_tma_x<T, TY_, 32>();
-    return a != cudaSuccess ? a : set_attrs_tma_x<T, TY_, 31>();
+    const cudaError_t b = a != cudaSuccess ? a : set_attrs_tma_x<T, TY_, 31>();
+    return b != cudaSuccess || TY_ != 4 ? b : set_attrs_tma_x<T, 6, 31>();  // 6 rows: 31-wide tiles only
 }
 
 template <bool WS, int MODE, int TY_>

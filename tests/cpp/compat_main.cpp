@@ -2,6 +2,7 @@
 // points, in the order robtop.cpp:27-46 and TestSuit::testOrdinaryTopopt
 // (utils/test_utils.cpp:589-660) call them, and prints the results as
 // "key value" lines for tests/test_gpu_compat.py to compare with the oracle.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <string>
@@ -48,8 +49,29 @@ int main(int argc, char** argv) {
     printf("adjoint_ok %d\n", checkAdjointVariable() ? 1 : 0);
     g0->reset_displacement();
     printf("adjoint_zero_ok %d\n", checkAdjointVariable() ? 1 : 0);
-    // element compliance of the worst-case displacement sums to u.K u
+    // element compliance of the worst-case displacement sums to u.K u (on the displacement
+    // with its support nodes zeroed: K u has identity rows there, the element sums do not)
     const double mu2 = modifiedPM();
+    {
+        const long long nvb0 = g0->n_box_nodes();
+        std::vector<double> uh(3 * nvb0), kuh(3 * nvb0);
+        std::vector<uint8_t> fix(nvb0);
+        rt_get(getGrids().hier(), RT_FIELD_U, 0, RT_LAYOUT_DENSE, uh.data());
+        rt_get(getGrids().hier(), RT_FIELD_VFIX, 0, RT_LAYOUT_DENSE, fix.data());
+        double ufix = 0;
+        for (long long v = 0; v < nvb0; v++)
+            if (fix[v])
+                for (int c = 0; c < 3; c++) {
+                    ufix = std::max(ufix, std::fabs(uh[c * nvb0 + v]));
+                    uh[c * nvb0 + v] = 0;
+                }
+        printf("worst_u_support_max %.17g\n", ufix);
+        rt_put(getGrids().hier(), RT_FIELD_U, 0, RT_LAYOUT_DENSE, uh.data());
+        rt_apply_K(getGrids().hier(), uh.data(), kuh.data());
+        double uku = 0;
+        for (long long i = 0; i < 3 * nvb0; i++) uku += uh[i] * kuh[i];
+        printf("worst_uKu %.17g\n", uku);
+    }
     float* ce = (float*)gpu_manager.add_buf("element compliance", sizeof(float) * nx * ny * nz);
     g0->elementCompliance(g0->getDisplacement(), ce);
     std::vector<float> ceh((size_t)nx * ny * nz);
@@ -58,15 +80,6 @@ int main(int argc, char** argv) {
     double csum = 0;
     for (float v : ceh) csum += v;
     printf("element_compliance_sum %.17g\n", csum);
-    {  // u.K u of the same displacement, by the operator (host copies; the force stays as it is)
-        const long long nvb0 = g0->n_box_nodes();
-        std::vector<double> uh(3 * nvb0), kuh(3 * nvb0);
-        rt_get(getGrids().hier(), RT_FIELD_U, 0, RT_LAYOUT_DENSE, uh.data());
-        rt_apply_K(getGrids().hier(), uh.data(), kuh.data());
-        double uku = 0;
-        for (long long i = 0; i < 3 * nvb0; i++) uku += uh[i] * kuh[i];
-        printf("worst_uKu %.17g\n", uku);
-    }
     printf("worst_compliance2 %.17g\n", mu2);
     // projection API (wsff: the projection keeps the load-node values, zeroes every other node)
     printf("n_loadnodes %d\n", n_loadnodes());

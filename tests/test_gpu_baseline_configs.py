@@ -139,3 +139,62 @@ def test_c2_worst_case_eigenvalue_against_golden(form):
     finally:
         G.close()
         ctx.close()
+
+
+def test_c5_loop_checked_against_oracle_at_reduced_size():
+    """C5's loop (arch domain with the tunnel and support pads, wscf top-face load, V 0.4, R 2,
+    move 0.06, eta 0.5, p 3) at 63x32x32 elements, 12 OC iterations (rt_oc_iteration: Lanczos
+    k = 16, inner solves to 1e-6) in the mixed form (FP32 Chebyshev(2) cycles, W below level 1).
+    Every 4 iterations the design's worst-case eigenvalue and the compliance of a fixed unit
+    top-face load are checked against the FP64 oracle on the same densities: eigenvalue within
+    1e-5, compliance within 1e-6.  (At 511x256x256 the oracle would take about 40 minutes per
+    check on the host; the bench's c5oc40 workload checks against the plain FP64 GPU path.)"""
+    cfg = configs.arch(63, 32, 32, tunnel=12, pad=2)
+    ctx = rb.Context(0)
+    p = rb.default_params(mode=cfg["mode"], youngs_modulus=E, poisson_ratio=NU, power_penalty=P, min_rho=1e-3,
+                          precision=rb.FP32, smoother=rb.SMOOTH_CHEBY, pre_sweeps=2, post_sweeps=2,
+                          volume_ratio=0.4, design_step=0.06, damp_ratio=0.5, filter_radius=2.0)
+    p.cycle_gamma = 2
+    G = rb.HierarchyGrid(ctx, p)
+    ln = np.ascontiguousarray(cfg["load_nodes"], np.int32)
+    normals = np.ascontiguousarray(cfg["normals"], np.float64)
+    try:
+        G.genFromBox(cfg["eact"])
+        G[0].setRho(cfg["rho"].ravel())
+        G.set_support(cfg["vfix"])
+        G.set_load_nodes(cfg["load_nodes"], cfg["normals"])
+        nv = G[0].nv
+        fload = np.zeros(3 * nv)
+        fload[2 * nv + ln] = 1.0 / np.sqrt(ln.size)
+        lam_c = C.c_double()
+        checks = 0
+        for it in range(1, 13):
+            rb._capi.check(rb.lib().rt_oc_iteration(G.handle, rb.WORST_LANCZOS, 16, 1e-6, 7, 0.4, C.byref(lam_c)),
+                           ctx.handle)
+            if it % 4:
+                continue
+            G.update_stencil()
+            lam_g, _ = G.worst_case(rb.WORST_LANCZOS, 16, 1e-6, seed=7)
+            G[0].setForce(fload)
+            G[0].reset_displacement()
+            info = G.pcg(1e-8, 2000)
+            assert info.status == 0
+            c_g = float(fload @ G[0].getDisplacement())
+            rho = G[0].getRho().reshape(cfg["eact"].shape)
+            H = O.Hierarchy(cfg["eact"], rho, cfg["vfix"], p=P, E=E, nu=NU)
+            H.update_stencil()
+            nvo = H.arrs[0]["u"].size // 3
+            work = np.zeros(17 * 3 * ln.size + 10 * 3 * nvo)
+            lo = np.zeros(1)
+            O.lib().or_lanczos(H.LA, H.nlev, O.ptr(H.KE), O.SMOOTH_SGS, 1, 1, 0.6, ln.size, O.ptr(ln),
+                               O.ptr(normals), 1, 0, None, 7, 16, 1e-8, 3000, O.ptr(lo), None, O.ptr(work))
+            assert abs(lam_g - lo[0]) <= 1e-5 * lo[0], (it, lam_g, lo[0])
+            xo, _, rr = H.pcg(fload, tol=1e-10, maxit=3000)
+            assert rr <= 1e-10
+            c_o = float(fload @ xo)
+            assert abs(c_g - c_o) <= 1e-6 * abs(c_o), (it, c_g, c_o)
+            checks += 1
+        assert checks == 3
+    finally:
+        G.close()
+        ctx.close()

@@ -99,7 +99,7 @@ def test_fine_smoothers(pair, smoother):
                                            (1, 4, 1), (2, 2, 8), (2, 4, 3), (3, 4, 8), (3, 2, 5), (3, 8, 3),
                                            (3, 4, 1), (3, 2, 64), (5, 4, 8), (5, 8, 3), (5, 16, 1), (5, 4, 64),
                                            (5, 8, 5), (6, 4, 8), (6, 8, 3), (6, 4, 1), (6, 8, 64), (7, 4, 8),
-                                           (7, 8, 3), (7, 4, 1), (7, 8, 64)])
+                                           (7, 8, 3), (7, 4, 1), (7, 8, 64), (7, 6, 5), (7, 6, 32)])
 def test_fine_kernel_variants(pair, variant, ty, zc):
     """Every launch shape of the finest-level kernels (shared-memory tile, register marching,
     register marching with prefetched output-stage loads, pipelined shared-memory tile,
@@ -141,7 +141,8 @@ FP32_TOL = 2e-6  # FP32 kernels against the FP64 oracle on random data (no cance
 @pytest.mark.parametrize("variant,ty,zc", [(0, 4, 8), (1, 2, 8), (2, 4, 8), (3, 4, 8), (3, 8, 3), (4, 4, 8),
                                            (4, 8, 16), (4, 2, 5), (4, 8, 1), (4, 4, 64), (5, 4, 8), (5, 8, 16),
                                            (5, 16, 3), (5, 8, 1), (5, 4, 64), (6, 4, 8), (6, 8, 16), (6, 4, 1),
-                                           (6, 8, 64), (7, 4, 8), (7, 8, 16), (7, 4, 1), (7, 8, 64)])
+                                           (6, 8, 64), (7, 4, 8), (7, 8, 16), (7, 4, 1), (7, 8, 64),
+                                           (7, 6, 3), (7, 6, 32)])
 def test_fp32_fine_kernels(pair, variant, ty, zc):
     """Every FP32 finest-level kernel variant (including the packed-pair tile kernel) gives the
     oracle's residual, K u, Jacobi and first Chebyshev step to FP32 accuracy."""
@@ -173,7 +174,7 @@ def test_fp32_fine_kernels(pair, variant, ty, zc):
 
 @pytest.mark.parametrize("variant,ty,zc", [(0, 4, 8), (1, 2, 8), (2, 4, 8), (3, 4, 8), (3, 8, 2), (4, 8, 16),
                                            (4, 4, 8), (5, 8, 16), (5, 16, 32), (5, 4, 2), (6, 4, 8), (6, 8, 16),
-                                           (7, 4, 8), (7, 8, 16)])
+                                           (7, 4, 8), (7, 8, 16), (7, 6, 16)])
 def test_fp32_kernel_variants_in_pcg(pair, variant, ty, zc):
     """The FP32 finest-level kernels of every variant drive the mixed-precision PCG (FP32 Chebyshev
     V-cycles) to 1e-6 in the FP64 residual; FP32 rounding differs between variants, the iteration
