@@ -265,10 +265,12 @@ NCU_TRAFFIC_PER_NODE = {("fine_cheby_f32", "register_march"): (71.0e6 + 3.3e6) /
 # worst-case box, whose vectors exceed L2 (8,487,168 nodes: 359.7 MB read + 171.8 MB written);
 # traffic grows with the nodes, so the per-node figure scales to the arch's node box
 NCU_TRAFFIC_ARCH = {("fine_cheby_f32", "smem_tile_pipelined"): (359.672064e6 + 171.792896e6) / 8487168,
-                    ("fine_cheby_f32", "smem_tile_pipelined_tma"): (358.008320e6 + 168.810240e6) / 8487168}
+                    ("fine_cheby_f32", "smem_tile_pipelined_tma"): (358.008320e6 + 168.810240e6) / 8487168,
+                    ("fine_cheby_f32", "smem_tile_pipelined_tma_x31"): (358.434304e6 + 167.496448e6) / 8487168}
 # warp-instructions per node of the same captures (smsp__inst_executed.sum / nodes)
 NCU_INST_ARCH = {("fine_cheby_f32", "smem_tile_pipelined", (8, 32)): 222157952 / 8487168,
-                 ("fine_cheby_f32", "smem_tile_pipelined_tma", (4, 32)): 256982264 / 8487168}
+                 ("fine_cheby_f32", "smem_tile_pipelined_tma", (4, 32)): 256982264 / 8487168,
+                 ("fine_cheby_f32", "smem_tile_pipelined_tma_x31", (8, 32)): 232812378 / 8487168}
 
 
 def roofline(ctx, stats, G, peaks, tuning=None, traffic_table=None):
