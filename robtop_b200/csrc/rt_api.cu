@@ -317,6 +317,8 @@ static void free_workspace(rt_hier* w) {
     cudaFree(w->partials); cudaFree(w->scal);
     if (w->pcg_exec) cudaGraphExecDestroy(w->pcg_exec);
     if (w->pcg_graph) cudaGraphDestroy(w->pcg_graph);
+    if (w->pcg_exec_alt) cudaGraphExecDestroy(w->pcg_exec_alt);
+    if (w->pcg_graph_alt) cudaGraphDestroy(w->pcg_graph_alt);
     if (w->pcg32_exec) cudaGraphExecDestroy(w->pcg32_exec);
     if (w->pcg32_graph) cudaGraphDestroy(w->pcg32_graph);
     cudaFree(w->p32k); cudaFree(w->q32k); cudaFree(w->d32k); cudaFree(w->ro32k);
@@ -350,6 +352,8 @@ static void free_hier(rt_hier* h) {
     cudaFree(h->scal); cudaFree(h->Qgal); cudaFree(h->dinv64); cudaFree(h->dinv32);
     if (h->pcg_exec) cudaGraphExecDestroy(h->pcg_exec);
     if (h->pcg_graph) cudaGraphDestroy(h->pcg_graph);
+    if (h->pcg_exec_alt) cudaGraphExecDestroy(h->pcg_exec_alt);
+    if (h->pcg_graph_alt) cudaGraphDestroy(h->pcg_graph_alt);
     if (h->pcg32_exec) cudaGraphExecDestroy(h->pcg32_exec);
     if (h->pcg32_graph) cudaGraphDestroy(h->pcg32_graph);
     cudaFree(h->p32k); cudaFree(h->q32k); cudaFree(h->d32k); cudaFree(h->ro32k);
@@ -1553,8 +1557,10 @@ static int precondition(rt_hier* h, const double* r, double* z, const double* rr
         RT_CHECK(s);
     }
     // learned correction z += N(rho, r, z), run only while the gate in scal[28] is on; the dots
-    // the widening of z already produced are recomputed for the corrected z
-    if (h->unet)
+    // the widening of z already produced are recomputed for the corrected z.  Once the gate has
+    // judged the network off for this design, the loop is captured without it: a conditional
+    // node inside the captured loop body slows every iteration's launches, even when it skips
+    if (h->unet && !h->unet_off)
         RT_CHECK(learned_if(h, [&]() -> int {
             RT_CHECK(rtk::dot(h, n, r, r, h->scal + 38));
             RT_CHECK(rtk::dot(h, n, z, z, h->scal + 37));
@@ -1649,6 +1655,7 @@ static int pcg_graph_run(rt_hier* h, double* x, double* r, bool no_support) {
     auto mix = [&](uint64_t v) { key = (key ^ v) * 1099511628211ull; };
     mix((uint64_t)(uintptr_t)x);
     mix((uint64_t)(uintptr_t)h->unet);
+    mix((uint64_t)h->unet_off);
     mix(h->graph_epoch);
     mix((uint64_t)c->wait_limit);
     mix((uint64_t)no_support);
@@ -1658,9 +1665,22 @@ static int pcg_graph_run(rt_hier* h, double* x, double* r, bool no_support) {
     uint64_t om;
     memcpy(&om, &h->P.jacobi_omega, 8);
     mix(om);
+    if ((!h->pcg_exec || h->pcg_key != key) && h->pcg_exec_alt && h->pcg_key_alt == key) {
+        std::swap(h->pcg_exec, h->pcg_exec_alt);
+        std::swap(h->pcg_graph, h->pcg_graph_alt);
+        std::swap(h->pcg_key, h->pcg_key_alt);
+        std::swap(h->pcg_iter_kernels, h->pcg_iter_kernels_alt);
+    }
     if (!h->pcg_exec || h->pcg_key != key) {
-        if (h->pcg_exec) { cudaGraphExecDestroy(h->pcg_exec); h->pcg_exec = nullptr; }
-        if (h->pcg_graph) { cudaGraphDestroy(h->pcg_graph); h->pcg_graph = nullptr; }
+        // the current graph becomes the alternate one; the older alternate is released
+        if (h->pcg_exec_alt) cudaGraphExecDestroy(h->pcg_exec_alt);
+        if (h->pcg_graph_alt) cudaGraphDestroy(h->pcg_graph_alt);
+        h->pcg_exec_alt = h->pcg_exec;
+        h->pcg_graph_alt = h->pcg_graph;
+        h->pcg_key_alt = h->pcg_key;
+        h->pcg_iter_kernels_alt = h->pcg_iter_kernels;
+        h->pcg_exec = nullptr;
+        h->pcg_graph = nullptr;
         if (h->unet && !c->aux_stream) RT_CUDA(c, cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking));
         cudaGraph_t g;
         RT_CUDA(c, cudaGraphCreate(&g, 0));

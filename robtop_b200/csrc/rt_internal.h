@@ -156,6 +156,13 @@ struct rt_hier {
     cudaGraphExec_t pcg_exec = nullptr;
     uint64_t pcg_key = 0;
     long pcg_iter_kernels = 0;  // kernels in one iteration of the captured loop (launch accounting)
+    // the previously used PCG graph, kept so that two forms can alternate without re-capture (the
+    // loop with the learned correction for a design's first solve, without it once the gate
+    // judged the network off)
+    cudaGraph_t pcg_graph_alt = nullptr;
+    cudaGraphExec_t pcg_exec_alt = nullptr;
+    uint64_t pcg_key_alt = 0;
+    long pcg_iter_kernels_alt = 0;
     uint64_t graph_epoch = 0;  // bumped whenever captured pointers may change
     // learned correction added to the V-cycle inside PCG (rt_hier_set_learned); scal[27] holds the
     // fallback ratio, scal[28] the gate (1 while active), scal[29] the previous iteration's r.r
