@@ -1337,14 +1337,27 @@ def run_c5_oc40(args):
     cal, t_net, ratio = arch_attach_network(learned, G, cfg, hnet)
     G_net[0], G_net[1] = hnet, ratio
     lam_c = C.c_double()
+    stopped_early = False
     for it in range(n_design, n_iter):
         if (it + 1) % 10 == 0 or it + 1 == n_iter:
             check(it + 1)
+            c = checks[-1]
+            print(f"check at iteration {it + 1}: lambda rel diff {c['lambda_rel_diff']:.2e}, compliance rel diff "
+                  f"{c['compliance_rel_diff']:.2e}, {c['pcg_iterations']} / {c['pcg_iterations_plain_fp64']} PCG "
+                  "iterations", file=sys.stderr, flush=True)
         ms, _ = timed(lambda: rb._capi.check(rb.lib().rt_oc_iteration(G.handle, rb.WORST_LANCZOS, ARCH["k"],
                                                                         ARCH["tol"], 10 + it, ARCH["vgoal"],
                                                                         C.byref(lam_c)), ctx.handle))
         ms_iter.append(ms)
         lams.append(lam_c.value)
+        print(f"OC iteration {it + 1}: {ms:.0f} ms, lambda {lam_c.value:.6e}", file=sys.stderr, flush=True)
+        # the design sharpens towards 0/1 densities (nine decades of stiffness): later iterations
+        # need many more PCG iterations; a time budget ends the run with the iterations done
+        if args.time_budget > 0 and time.perf_counter() - t0 > args.time_budget and it + 1 < n_iter:
+            stopped_early = True
+            if not checks or checks[-1]["iteration"] != it + 1:
+                check(it + 1)
+            break
     wall = time.perf_counter() - t0
     applied, off = learned.stats(G)
     rho = G[0].getRho()
@@ -1361,7 +1374,8 @@ def run_c5_oc40(args):
                        "max_compliance_rel_diff": max((c["compliance_rel_diff"] for c in checks), default=None),
                        "volume_fraction": float(rho[eact].mean()), "learned_corrections": applied,
                        "learned_judged_off_at_end": off, "fallback_ratio": ratio, "network_ms": t_net * 1e3,
-                       "wall_s": wall}}
+                       "wall_s": wall, "iterations_completed": n_design + len(ms_iter),
+                       "stopped_by_time_budget": stopped_early}}
     if rank == 0:
         print(json.dumps(line))
     hnet.close()
@@ -1565,6 +1579,8 @@ def main():
     ap.add_argument("--shape", default=None, help="kernel mode: launch shape variant,rows,zchunk (default: autotune)")
     ap.add_argument("--oc-iters", type=int, default=40, help="c5oc40 workload: OC iterations")
     ap.add_argument("--maxit", type=int, default=3000, help="batched workload: PCG iteration limit per solve")
+    ap.add_argument("--time-budget", type=float, default=900.0,
+                    help="c5oc40 workload: seconds after which the run stops at the end of an OC iteration (0: none)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
