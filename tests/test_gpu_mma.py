@@ -144,3 +144,31 @@ def test_mma_density_loop_against_oracle():
         m.close()
         G.close()
         ctx.close()
+
+
+def test_mma_optimisation_loop_through_the_module():
+    """robtop_b200.mma.optimization_mma (TestSuit::testtest2011's loop) on the 24x12x12
+    cantilever built through the optimization module: four MMA iterations with the worst-case
+    eigenvalue by Lanczos; the eigenvalues are finite and positive and the design's volume
+    moves from the middle of the bounds towards the 0.4 target."""
+    from robtop_b200 import mma as M
+    from robtop_b200 import optimization as opt
+
+    opt.setParameters(0.4, 0.0, 0.03, 2, 0.5, 3.0, 1e-3, 32, 1e6, 0.4)
+    opt.setWorkMode("wsff")
+    nx, ny, nz, R = 24, 12, 12, 32
+    opt.setBoundaryCondition(lambda p: p[0] == 0.0, lambda p: p[0] == nx and p[2] == 0.0,
+                             lambda p: (0.0, 0.0, -1.0))
+    bits = np.zeros((R ** 3 + 31) // 32, np.uint32)
+    for z in range(nz):
+        for y in range(ny):
+            t = np.arange(nx) + R * (y + R * z)
+            np.bitwise_or.at(bits, t >> 5, (np.uint32(1) << (t & 31).astype(np.uint32)))
+    opt.buildGrids(bits, R)
+    opt.uploadTemplateMatrix()
+    rec = M.optimization_mma(max_iter=4, worst=lambda: opt.worstCaseLanczos(8, 1e-8, seed=3))
+    assert len(rec) == 4 and all(np.isfinite(c) and c > 0 for c in rec)
+    G = opt.getGrids()
+    eact = G[0].getEact() != 0
+    vol = float(G[0].getRho()[eact].mean())
+    assert vol < 0.5005 - 1e-3 and vol > 0.3
