@@ -97,6 +97,8 @@ typedef struct rt_params {
                                FP64); each inner solve of K d = r / |r| (to the outer target, at most down to
                                10^-(3+k)) is followed by x += |r| d and a fresh FP64 residual (iterative
                                refinement).  0 (default): FP64 flexible CG around the FP32 V-cycle */
+    int cycle_gamma_levels; /* with cycle_gamma > 1: the coarse correction repeats on levels 1 .. this level
+                               only (coarser levels are visited V-cycle fashion); 0 (default): on every level */
 } rt_params;
 
 typedef struct rt_solve_info {

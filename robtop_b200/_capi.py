@@ -33,6 +33,7 @@ class Params(C.Structure):
         ("post_sweeps", C.c_int), ("jacobi_omega", C.c_double), ("precision", C.c_int),
         ("coarsest_elements", C.c_int), ("cycle_gamma", C.c_int), ("coarse_sweeps", C.c_int),
         ("precision_fallback", C.c_int), ("coarse_bf16", C.c_int), ("krylov_fp32", C.c_int),
+        ("cycle_gamma_levels", C.c_int),
     ]
 
 

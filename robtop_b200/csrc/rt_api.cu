@@ -230,6 +230,7 @@ extern "C" void rt_params_default(rt_params* p) {
     p->precision_fallback = 100;
     p->coarse_bf16 = 0;
     p->krylov_fp32 = 0;
+    p->cycle_gamma_levels = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -1204,8 +1205,9 @@ static int level_smooth(rt_hier* h, int lvl, int smoother, int sweeps, double om
 }
 
 // the multigrid cycle from level i down (level i's u is the caller's initial guess): smoothing,
-// the coarse correction (cycle_gamma times on levels >= 1 unless the next level is the coarsest,
-// whose solve is exact: gamma = 2 is the W-cycle), smoothing; pre/post mirror each other, so the
+// the coarse correction (cycle_gamma times on levels 1 .. cycle_gamma_levels (all when 0) unless
+// the next level is the coarsest, whose solve is exact: gamma = 2 is the W-cycle), smoothing;
+// pre/post mirror each other, so the
 // cycle is symmetric when the smoother is (SGS, Jacobi, Chebyshev)
 template <typename T>
 static int mg_cycle(rt_hier* h, int i, int smoother, int pre, int post, double omega) {
@@ -1214,7 +1216,8 @@ static int mg_cycle(rt_hier* h, int i, int smoother, int pre, int post, double o
     const int cs = h->P.coarse_sweeps;
     const int npre = (i > 0 && cs > 0) ? cs : pre, npost = (i > 0 && cs > 0) ? cs : post;
     RT_CHECK(level_smooth<T>(h, i, smoother, npre, omega, false));
-    const int reps = (i > 0 && i + 1 < nl - 1 && h->P.cycle_gamma > 1) ? h->P.cycle_gamma : 1;
+    const int gl = h->P.cycle_gamma_levels;
+    const int reps = (i > 0 && i + 1 < nl - 1 && h->P.cycle_gamma > 1 && (gl <= 0 || i <= gl)) ? h->P.cycle_gamma : 1;
     for (int g = 0; g < reps; g++) {
         RT_CHECK(level_residual<T>(h, i));
         RT_CHECK(rtk::restrict_<T>(h, i + 1, LvlVec<T>::r(h->L[i]), LvlVec<T>::f(h->L[i + 1])));
@@ -1662,6 +1665,7 @@ static int pcg_graph_run(rt_hier* h, double* x, double* r, bool no_support) {
     mix((uint64_t)h->P.precision | ((uint64_t)h->P.smoother << 8) | ((uint64_t)h->P.pre_sweeps << 16) |
         ((uint64_t)h->P.post_sweeps << 24) | ((uint64_t)h->P.cycle_gamma << 32) |
         ((uint64_t)h->P.coarse_sweeps << 40) | ((uint64_t)h->P.coarse_bf16 << 48));
+    mix((uint64_t)(uint32_t)h->P.cycle_gamma_levels);
     uint64_t om;
     memcpy(&om, &h->P.jacobi_omega, 8);
     mix(om);
@@ -1798,6 +1802,7 @@ static int pcg32_graph_run(rt_hier* h) {
     mix((uint64_t)c->wait_limit);
     mix((uint64_t)h->P.smoother | ((uint64_t)h->P.pre_sweeps << 8) | ((uint64_t)h->P.post_sweeps << 16) |
         ((uint64_t)h->P.cycle_gamma << 24) | ((uint64_t)h->P.coarse_sweeps << 32) | ((uint64_t)h->P.coarse_bf16 << 40));
+    mix((uint64_t)(uint32_t)h->P.cycle_gamma_levels);
     uint64_t om;
     memcpy(&om, &h->P.jacobi_omega, 8);
     mix(om);
@@ -2913,6 +2918,7 @@ static uint64_t batch_key(rt_hier* const* hs, int n, double tol, int maxit) {
             ((uint64_t)h->P.post_sweeps << 16) | ((uint64_t)h->P.mode << 24) | ((uint64_t)h->P.cycle_gamma << 32) |
             ((uint64_t)h->P.coarse_sweeps << 40) | ((uint64_t)h->P.precision_fallback << 48));
         mix((uint64_t)h->P.coarse_bf16);
+        mix((uint64_t)(uint32_t)h->P.cycle_gamma_levels);
         uint64_t om;
         memcpy(&om, &h->P.jacobi_omega, 8);
         mix(om);
