@@ -433,9 +433,11 @@ int rt_unet_harvest(rt_hier* h, rt_unet* u, int k_iter, uint64_t seed, void* in_
 /* use the network inside rt_pcg / rt_worst_case: z = Vcycle(r) + N(rho, r, Vcycle(r)) (no
  * reference counterpart).  The correction is switched off once an iteration fails to reduce
  * ||r|| below fallback_ratio x its previous value (the plain V-cycle is the fallback and the
- * judge); that verdict holds for the following solves until rt_update_stencil or the next
- * rt_hier_set_learned.  Inside the captured PCG loop the correction is the body of an IF node,
- * so a switched-off network costs no launches.  u = null detaches. */
+ * judge); that verdict holds for the design it was made on: for the following solves, and
+ * across rt_update_stencil as long as the density, supports and parameters are unchanged, until
+ * the design changes or the next rt_hier_set_learned.  Inside the captured PCG loop the
+ * correction is the body of an IF node; once switched off, the loop is captured without it.
+ * u = null detaches. */
 int rt_hier_set_learned(rt_hier* h, rt_unet* u, double fallback_ratio);
 /* finest-level smoothing steps (the hierarchy's smoother, FP64) applied to z after each learned
  * correction, on K z = r (0: none, the default) */

@@ -620,6 +620,7 @@ extern "C" int rt_hier_set_params(rt_hier* h, const rt_params* p) {
     h->P = *p;
     if (ke) RT_CHECK(upload_KE(h));
     h->stencil_ready = false;
+    h->design_epoch++;
     h->graph_epoch++;  // captured graphs bake in the settings and the stencil copies they read
     return RT_OK;
 }
@@ -693,6 +694,7 @@ extern "C" int rt_set_support(rt_hier* h, const uint8_t* vfix) {
     h->has_support = cnt > 0;
     h->graph_epoch++;  // kernel variants depend on whether supports exist
     h->stencil_ready = false;
+    h->design_epoch++;
     return RT_OK;
 }
 
@@ -948,7 +950,10 @@ extern "C" int rt_put(rt_hier* h, int field, int lvl, int layout, const void* sr
         RT_CUDA(h->ctx, cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, h->ctx->stream));
         RT_CUDA(h->ctx, cudaStreamSynchronize(h->ctx->stream));
     }
-    if (field == RT_FIELD_RHO || field == RT_FIELD_VFIX || field == RT_FIELD_STENCIL) h->stencil_ready = false;
+    if (field == RT_FIELD_RHO || field == RT_FIELD_VFIX || field == RT_FIELD_STENCIL) {
+        h->stencil_ready = false;
+        h->design_epoch++;
+    }
     return RT_OK;
 }
 
@@ -976,7 +981,10 @@ extern "C" int rt_put_dev(rt_hier* h, int field, int lvl, const void* src) {
     size_t bytes;
     RT_CHECK(field_ptr(h, field, lvl, &d, &bytes));
     RT_CUDA(h->ctx, cudaMemcpyAsync(d, src, bytes, cudaMemcpyDeviceToDevice, h->ctx->stream));
-    if (field == RT_FIELD_RHO || field == RT_FIELD_VFIX) h->stencil_ready = false;
+    if (field == RT_FIELD_RHO || field == RT_FIELD_VFIX) {
+        h->stencil_ready = false;
+        h->design_epoch++;
+    }
     return RT_OK;
 }
 
@@ -999,6 +1007,7 @@ extern "C" int rt_init_density(rt_hier* h, float rho) {
     RT_NOT_WORKSPACE(h);
     rt_level& L = h->L[0];
     h->stencil_ready = false;
+    h->design_epoch++;
     return rt_launch(h->ctx, "init_density", [&] {
         k_fill_rho<<<(unsigned)std::min<long>((L.ne + 255) / 256, 148 * 16), 256, 0, h->ctx->stream>>>(L.ne, L.eact,
                                                                                                        rho, h->rho);
@@ -1037,7 +1046,9 @@ extern "C" int rt_update_stencil(rt_hier* h) {
     // spectral bound of D^-1 A per smoothed level, for the Chebyshev smoother
     for (int i = 0; i + 1 < nl; i++) RT_CHECK(estimate_lmax(h, i));
     h->stencil_ready = true;
-    h->unet_off = false;  // a new design: the learned correction gets judged again
+    // a new design: the learned correction gets judged again (the verdict stands while only the
+    // stencils of the same design are assembled again)
+    if (h->design_epoch != h->unet_verdict_epoch) h->unet_off = false;
     return RT_OK;
 }
 
@@ -2004,7 +2015,10 @@ static int pcg_core(rt_hier* h, double* x, const double* b, double tol, int maxi
             const long long applied = (long long)lg[8];
             h->unet_applied += applied;
             if (graphed) h->ctx->launches += h->unet_kernels * applied;
-            if (learned_on && lg[0] == 0.0) h->unet_off = true;
+            if (learned_on && lg[0] == 0.0) {
+                h->unet_off = true;
+                h->unet_verdict_epoch = h->design_epoch;
+            }
         }
         if (fallback && stall != 0.0 && rel > tol && it < maxit) {
             // continue from the current iterate with FP64 V-cycles (flexible CG restarts)
@@ -2378,6 +2392,7 @@ extern "C" int rt_oc_update(rt_hier* h, float vgoal, float* lambda_out, int* tri
     } while (std::fabs(V - vgoal) > 1e-4f && itn++ < 30);
     RT_CHECK(rtk::oc_try(h, thr, h->rho, h->scal + 51));
     h->stencil_ready = false;
+    h->design_epoch++;
     if (lambda_out) *lambda_out = thr;
     if (trials_out) *trials_out = trials;
     return RT_OK;
@@ -3275,6 +3290,7 @@ extern "C" int rt_hier_set_learned(rt_hier* h, rt_unet* u, double fallback_ratio
     h->unet = u;
     h->unet_fallback = fallback_ratio;
     h->unet_off = false;
+    h->unet_verdict_epoch = ~0ull;
     h->unet_applied = 0;
     h->graph_epoch++;
     return RT_OK;

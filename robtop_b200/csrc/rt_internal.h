@@ -173,6 +173,10 @@ struct rt_hier {
     // network changes.  unet_kernels: kernels of one correction (launch accounting of the IF node
     // that runs it inside the captured loop); unet_applied: corrections run since attach
     bool unet_off = false;
+    // bumped whenever the density, the supports, the stencil or the parameters change; the gate's
+    // verdict on the learned correction holds while the design it was made on is unchanged
+    uint64_t design_epoch = 0;
+    uint64_t unet_verdict_epoch = ~0ull;
     int unet_post = 0;  // finest-level smoothing steps applied to z after the correction
     long unet_kernels = 0;
     long long unet_applied = 0;

@@ -334,6 +334,7 @@ extern "C" int rt_mma_set_density(rt_mma* m, rt_hier* h) {
         return rt_fail(m->ctx, RT_EINVAL, "MMA state has %lld variables, the finest level %ld elements", m->n, L.ne);
     rt_ctx* c = m->ctx;
     h->stencil_ready = false;
+    h->design_epoch++;
     return rt_launch(c, "mma_set_density", [&] {
         k_mma_to_rho<<<nblocks(m), kBS, 0, c->stream>>>(m->n, m->x, L.eact, h->rho);
     });

@@ -93,6 +93,14 @@ def test_learned_pcg_converges_and_reports_gain(trained, tmp_path):
     gated = G.pcg(1e-6, 500)
     assert gated.status == rb._capi.RT_OK
     assert abs(gated.iterations - plain.iterations) <= 3
+    # the verdict holds for the design: assembling the same design's stencils again keeps the
+    # network off; a changed density brings it back for judgement
+    assert learned.stats(G)[1]
+    G.update_stencil()
+    assert learned.stats(G)[1]
+    G[0].setRho(G[0].getRho())
+    G.update_stencil()
+    assert not learned.stats(G)[1]
     learned.attach(G, None)
     (tmp_path / "learned_gain.json").write_text(json.dumps({
         "plain_iterations": plain.iterations, "learned_iterations": lrn.iterations,
