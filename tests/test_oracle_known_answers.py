@@ -412,3 +412,37 @@ def test_mma_reaches_the_separable_optimum():
             assert np.abs(grad[inside]).max() <= 1e-9 * scale, it
     xs = V * n * np.sqrt(c) / np.sqrt(c).sum()
     assert np.abs(m.x - xs).max() <= 1e-12
+
+
+def test_mma_step_solves_the_subproblem_the_reference_poses():
+    """One step of the oracle's MMA equals the optimum of the subproblem as the reference states
+    it (optimization/mma_t.cu:70-89, mma_t.h:229-237: a0 = 1, a = 0, c = 10, d = 1), solved here
+    by a general constrained optimiser over (x, y, z) instead of the one-multiplier dual: the
+    dual's design is feasible, its objective is not above the optimiser's (to 1e-9 relative),
+    and the designs agree to 1e-4, for an active and an inactive constraint."""
+    from scipy.optimize import minimize
+
+    rng = np.random.default_rng(4)
+    n = 40
+    for target in (0.3, 0.9):  # volume constraint active / inactive at the start design
+        m = O.MMA(n, 0.01, 1.0)
+        x0, low, upp, a, b = m.x.copy(), m.low.copy(), m.upp.copy(), m.alpha.copy(), m.beta.copy()
+        c = rng.uniform(0.5, 2.0, n)
+        df, dg = -c / x0 ** 2 / n, np.full(n, 1e3 / n)
+        g = 1e3 * (x0.mean() - target)
+        lam = m.update(df, dg, g)
+        r = 1e-5 / 0.99
+        pq = lambda f: ((upp - x0) ** 2 * (1.001 * np.maximum(f, 0) + 0.001 * np.maximum(-f, 0) + r),
+                        (x0 - low) ** 2 * (0.001 * np.maximum(f, 0) + 1.001 * np.maximum(-f, 0) + r))
+        (p0, q0), (p1, q1) = pq(df), pq(dg)
+        bb = np.sum(p1 / (upp - x0) + q1 / (x0 - low)) - g
+        f0 = lambda v: np.sum(p0 / (upp - v[:n]) + q0 / (v[:n] - low)) + v[n + 1] + 10 * v[n] + 0.5 * v[n] ** 2
+        con = {"type": "ineq", "fun": lambda v: bb - (np.sum(p1 / (upp - v[:n]) + q1 / (v[:n] - low)) - v[n])}
+        bounds = list(zip(a, b)) + [(0, None), (0, None)]
+        res = minimize(f0, np.concatenate([x0, [0.0, 0.0]]), method="SLSQP", bounds=bounds, constraints=[con],
+                       options={"ftol": 1e-12, "maxiter": 2000})
+        y = max(0.0, lam - 10.0)
+        mine = np.concatenate([m.x, [y, 0.0]])
+        assert con["fun"](mine) >= -1e-9 * abs(bb)
+        assert f0(mine) <= res.fun + 1e-9 * abs(res.fun), (target, f0(mine), res.fun)
+        assert np.abs(res.x[:n] - m.x).max() <= 1e-4, (target, np.abs(res.x[:n] - m.x).max())
