@@ -656,16 +656,14 @@ void forceProject(std::vector<double> fsupport[3]) {
         if ((int)fsupport[c].size() != nl) throw std::invalid_argument("forceProject: support vectors of the wrong length");
     std::vector<double> soa(3 * (size_t)nl);
     for (int c = 0; c < 3; c++) std::copy(fsupport[c].begin(), fsupport[c].end(), soa.begin() + (size_t)c * nl);
-    double* d = nullptr;
-    grids.check(cudaMalloc(&d, sizeof(double) * 3 * (nl > 0 ? nl : 1)) == cudaSuccess ? RT_OK : RT_ENOMEM, "forceProject");
+    if (nl == 0) return;
+    double* d = h->fs;  // the hierarchy's [3][nload] support-force scratch
     ck_cuda(cudaMemcpyAsync(d, soa.data(), sizeof(double) * 3 * nl, cudaMemcpyHostToDevice, h->ctx->stream), "cudaMemcpyAsync");
-    int st = rt_set_force_support(h, d, h->x);
-    if (st == RT_OK) st = rt_force_project(h, h->x);
-    if (st == RT_OK) st = rt_get_force_support(h, h->x, d);
-    if (st == RT_OK) ck_cuda(cudaMemcpyAsync(soa.data(), d, sizeof(double) * 3 * nl, cudaMemcpyDeviceToHost, h->ctx->stream), "cudaMemcpyAsync");
+    grids.check(rt_set_force_support(h, d, h->x), "forceProject");
+    grids.check(rt_force_project(h, h->x), "forceProject");
+    grids.check(rt_get_force_support(h, h->x, d), "forceProject");
+    ck_cuda(cudaMemcpyAsync(soa.data(), d, sizeof(double) * 3 * nl, cudaMemcpyDeviceToHost, h->ctx->stream), "cudaMemcpyAsync");
     ck_cuda(cudaStreamSynchronize(h->ctx->stream), "cudaStreamSynchronize");
-    cudaFree(d);
-    grids.check(st, "forceProject");
     for (int c = 0; c < 3; c++) std::copy(soa.begin() + (size_t)c * nl, soa.begin() + (size_t)(c + 1) * nl, fsupport[c].begin());
 }
 
