@@ -904,18 +904,17 @@ __global__ void __launch_bounds__(TTile<TY_, TXN>::BS, tma_min_blocks<T, TY_, TX
     // layer L lives in slot (L - zb + 1) % 3, phase parity ((L - zb + 1) / 3) & 1
     auto slot_of = [&](int L) { return (L - zb + 1) % 3; };
     auto parity_of = [&](int L) { return (uint32_t)(((L - zb + 1) / 3) & 1); };
-    auto issue = [&](int L) {  // thread 0 only
-        const int sl = slot_of(L);
+    auto issue_to = [&](int L, int sl) {  // thread 0 only
         rttc::mbar_expect_tx(&S.bar[sl], UBYTES + FBYTES);
         tma_load_4d(&S.u[sl][0], &umap, xs, y0 - 1, L, 0, &S.bar[sl]);
         if (WS) tma_load_3d(&S.fx[sl][0], &fmap, xf, y0 - 1, L, &S.bar[sl]);
     };
+    auto issue = [&](int L) { issue_to(L, slot_of(L)); };
     // every thread waits for layer L; false if the wait ran out
     auto wait_layer = [&](int L) -> bool { return rttc::mbar_wait(&S.bar[slot_of(L)], parity_of(L)); };
     // fixed nodes enter the element products as zero
-    auto mask_layer = [&](int L) {
+    auto mask_slot = [&](int sl) {
         if (!WS) return;
-        const int sl = slot_of(L);
         for (int i = tid; i < NU_T; i += TILE_BS) {
             const int row = i / UXT, col = i % UXT;
             if (S.fx[sl][row * TMA_FX + col + offf]) {
@@ -926,6 +925,7 @@ __global__ void __launch_bounds__(TTile<TY_, TXN>::BS, tma_min_blocks<T, TY_, TX
             }
         }
     };
+    auto mask_layer = [&](int L) { mask_slot(slot_of(L)); };
     int issued = zb - 2;  // last layer whose copy was issued (uniform across the block)
     // bounded drain of the copies still in flight, then the error report
     auto give_up = [&](int first_pending) {
@@ -943,13 +943,14 @@ __global__ void __launch_bounds__(TTile<TY_, TXN>::BS, tma_min_blocks<T, TY_, TX
     auto stash_w = [&](int ez) {
         if (tid < NE_T) S.w[(ez + 4) & 3][tid] = pw;
     };
-    auto element_phase = [&](int e) {
+    // element layer e from the node layers in slots slo (layer e) and shi (layer e + 1)
+    auto element_phase_s = [&](int e, int slo, int shi) {
         if (tid >= NE_T) return;
         T a[24];
         const float wv = S.w[(e + 4) & 3][tid];
         if (wv != 0.f) {
-            const T* lo = &S.u[slot_of(e)][0];
-            const T* hi = &S.u[slot_of(e + 1)][0];
+            const T* lo = &S.u[slo][0];
+            const T* hi = &S.u[shi][0];
 #pragma unroll
             for (int vtx = 0; vtx < 8; vtx++) {
                 const T* src = (vtx & 4) ? hi : lo;
@@ -967,6 +968,7 @@ __global__ void __launch_bounds__(TTile<TY_, TXN>::BS, tma_min_blocks<T, TY_, TX
 #pragma unroll
         for (int q = 0; q < 24; q++) dst[q * NE_T + tid] = a[q];
     };
+    auto element_phase = [&](int e) { element_phase_s(e, slot_of(e), slot_of(e + 1)); };
 
     // prologue: barriers, layers zb-1 .. zb+1 copied, waited for and masked, weights of element
     // layers zb-1, zb stashed, element layer zb-1 computed
@@ -995,12 +997,17 @@ __global__ void __launch_bounds__(TTile<TY_, TXN>::BS, tma_min_blocks<T, TY_, TX
     __syncthreads();
 
     T acc[3] = {T(0), T(0), T(0)};
+    // slots and phase parity carried from iteration to iteration instead of divisions by 3:
+    // r3 = slot of layers t and t + 3, (r3 + 1) % 3 of layer t + 1, (r3 + 2) % 3 of layer t + 2;
+    // q3 = (t + 3 - zb + 1) / 3, whose low bit is the parity of layer t + 3's phase
+    int r3 = 0, q3 = 1;
     for (int t = zb - 1; t < ze; t++) {
+        const int s1 = r3 == 2 ? 0 : r3 + 1, s2 = r3 == 0 ? 2 : r3 - 1;
         // the slot of layer t + 3 held layer t, last read by element phase t (previous iteration)
         if (t + 3 <= zlast) {
             if (tid == 0) {
                 rttc::fence_async_smem();
-                issue(t + 3);
+                issue_to(t + 3, r3);
             }
             issued = t + 3;
         }
@@ -1024,7 +1031,7 @@ __global__ void __launch_bounds__(TTile<TY_, TXN>::BS, tma_min_blocks<T, TY_, TX
 #pragma unroll
                 for (int c = 0; c < 3; c++) dv[c] = dvec[c * nv + vout];
         }
-        if (t + 1 < ze) element_phase(t + 1);
+        if (t + 1 < ze) element_phase_s(t + 1, s1, s2);
         if (node_thread) {
             const T* E = &S.e[(t + 2) & 1][0][0];
             if (out_layer) {
@@ -1070,8 +1077,12 @@ __global__ void __launch_bounds__(TTile<TY_, TXN>::BS, tma_min_blocks<T, TY_, TX
         // layer t + 3 (read by element phase t + 2, next iteration) complete and masked; the
         // iteration's barrier publishes the masking
         ok = true;
-        if (t + 3 <= zlast) ok = wait_layer(t + 3);
-        if (ok && t + 3 <= zlast) mask_layer(t + 3);
+        if (t + 3 <= zlast) ok = rttc::mbar_wait(&S.bar[r3], (uint32_t)(q3 & 1));
+        if (ok && t + 3 <= zlast) mask_slot(r3);
+        if (++r3 == 3) {
+            r3 = 0;
+            q3++;
+        }
         if (__syncthreads_or(!ok)) {
             give_up(t + 3);
             return;
