@@ -24,15 +24,22 @@ static void ck_cuda(cudaError_t e, const char* what) {
     }
 }
 
+// The reference's copies are cudaMemcpy / cudaMemset on the legacy default stream, which its
+// kernels share, so a copy always sees the kernels launched before it.  This library's kernels
+// run on a non-blocking stream per context, which the legacy stream does not wait for: each
+// copy first waits for the device, so that a caller reading a buffer the library just wrote
+// (or refilling one it is still reading) sees the same order as with the reference.
 void gpu_manager_t::upload_buf(void* dst, const void* src, size_t size) {
-    if (cudaMemcpy(dst, src, size, cudaMemcpyHostToDevice) != cudaSuccess) throw std::runtime_error("upload_buf failed");
+    if (cudaDeviceSynchronize() != cudaSuccess || cudaMemcpy(dst, src, size, cudaMemcpyHostToDevice) != cudaSuccess)
+        throw std::runtime_error("upload_buf failed");
 }
 void gpu_manager_t::download_buf(void* host_dst, const void* dev_src, size_t n) {
-    if (cudaMemcpy(host_dst, dev_src, n, cudaMemcpyDeviceToHost) != cudaSuccess)
+    if (cudaDeviceSynchronize() != cudaSuccess || cudaMemcpy(host_dst, dev_src, n, cudaMemcpyDeviceToHost) != cudaSuccess)
         throw std::runtime_error("download_buf failed");
 }
 void gpu_manager_t::initMem(void* pdata, size_t len, char value) {
-    if (cudaMemset(pdata, value, len) != cudaSuccess) throw std::runtime_error("initMem failed");
+    if (cudaDeviceSynchronize() != cudaSuccess || cudaMemset(pdata, value, len) != cudaSuccess)
+        throw std::runtime_error("initMem failed");
 }
 void* gpu_manager_t::add_buf(const std::string& name, size_t size, const void* src) {
     void* p = nullptr;
