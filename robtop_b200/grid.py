@@ -18,7 +18,12 @@ from ._capi import check
 
 
 def _dp(t):
-    """Device pointer of a torch CUDA tensor (plumbing only)."""
+    """Device pointer of a torch CUDA tensor (plumbing only).  The library runs on its context's
+    own stream, so torch's pending work on the tensor (the copy or fill that made it) is waited
+    for first."""
+    import torch
+
+    torch.cuda.current_stream(t.device).synchronize()
     return C.c_void_p(t.data_ptr())
 
 

@@ -15,6 +15,12 @@ from ._capi import check
 
 
 def _vp(t):
+    """Device pointer of a torch CUDA tensor for the library.  The library runs on its context's
+    own stream, so torch's pending work on the tensor (the copy or fill that made it) is waited
+    for first."""
+    import torch
+
+    torch.cuda.current_stream(t.device).synchronize()
     return C.c_void_p(t.data_ptr())
 
 
@@ -67,6 +73,7 @@ class UNet:
 
         out = torch.empty(self.V, 3, dtype=torch.float32, device=inp.device)
         self._c(A.lib().rt_unet_forward(self._u, _vp(inp.contiguous()), _vp(out)))
+        self.ctx.sync()  # out is written on the library's stream
         return out
 
     def gradients(self, inp, tgt):
@@ -103,6 +110,7 @@ def harvest(G, net, k_iter, seed):
     inp = torch.empty(net.V, 16, dtype=torch.bfloat16, device="cuda")
     tgt = torch.empty(net.V, 3, dtype=torch.float32, device="cuda")
     check(A.lib().rt_unet_harvest(G.handle, net.handle, int(k_iter), int(seed), _vp(inp), _vp(tgt)), G.ctx.handle)
+    G.ctx.sync()  # inp and tgt are written on the library's stream
     return inp, tgt
 
 
