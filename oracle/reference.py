@@ -7,6 +7,8 @@ where the reference is mounted), these libraries into oracle/_ref/:
 * libref_stop.so, libref_stop_fabs.so: snippet::converge_criteria (utils/snippet.h:156-213), the
   optimisation loop's stop test, on the host, with g++'s integer abs() of the change and with the
   floating-point one;
+* libref_vox.so: cpu_voxelizer::cpu_voxelize_mesh_solid (voxelizer/cpu_voxelizer.cpp:262-322),
+  the solid mesh voxeliser, on the host, against GLM / trimesh2 stand-ins;
 * libref_kernels.so: applyK_OTFA_kernel (grid/Grid.cu:2439-2517), computeSensitivity_kernel and
   trySensMultiplier_kernel (optimization/optimization.cu:44-162) and filterSensitivity_kernel
   (grid/Grid.cu:2323-2409) for sm_100a, driven on dense element boxes (needs a GPU to run).
@@ -28,6 +30,7 @@ KE_LIB = os.path.join(REF_DIR, "libref_ke.so")
 KERNELS_LIB = os.path.join(REF_DIR, "libref_kernels.so")
 STOP_LIB = os.path.join(REF_DIR, "libref_stop.so")
 STOP_FABS_LIB = os.path.join(REF_DIR, "libref_stop_fabs.so")
+VOX_LIB = os.path.join(REF_DIR, "libref_vox.so")
 REFERENCE_TREE = os.environ.get("ROBTOP_REFERENCE", "/root/reference")
 
 
@@ -63,6 +66,21 @@ def converge_run(n_constrain, max_counter, thres, values, constraints, float_abs
     out = np.zeros(v.size, np.int32)
     L.ref_converge_run(n_constrain, max_counter, thres, v.size, _p(v), _p(g), _p(out))
     return out
+
+
+def voxelize_solid(coords, tris, reso, bmin, bmax):
+    """The reference's CPU solid voxeliser (cpu_voxelizer::cpu_voxelize_mesh_solid) on the cube
+    [bmin, bmax] at reso^3: bits x + y reso + z reso^2, most significant bit first."""
+    L = C.CDLL(VOX_LIB)
+    P = C.c_void_p
+    L.ref_voxelize_solid.argtypes = [P, C.c_long, P, C.c_long, P, P, C.c_int, P]
+    v = np.ascontiguousarray(coords, np.float32).reshape(-1, 3)
+    f = np.ascontiguousarray(tris, np.int32).reshape(-1, 3)
+    lo = np.ascontiguousarray(bmin, np.float32)
+    hi = np.ascontiguousarray(bmax, np.float32)
+    bits = np.zeros((reso ** 3 + 31) // 32, np.uint32)
+    L.ref_voxelize_solid(_p(v), v.shape[0], _p(f), f.shape[0], _p(lo), _p(hi), int(reso), _p(bits))
+    return bits
 
 
 class Kernels:

@@ -6,6 +6,9 @@
 * ref_stop.npz: the update() results of the reference's converge_criteria (utils/snippet.h:156-213,
   oracle/_ref/libref_stop.so and libref_stop_fabs.so: integer and floating-point abs of the change)
   on the seeded sequences of stop_sequences() below;
+* ref_vox.npz: the solid bits of the reference's CPU voxeliser (voxelizer/cpu_voxelizer.cpp:262-322,
+  oracle/_ref/libref_vox.so) for the meshes of vox_meshes() below at preferred resolutions 7, 31
+  and 63, each on the cube the oracle's voxel_box gives;
 * ref_kernels.npz (only with --kernels, on a machine with a GPU): the outputs of the reference's
   applyK_OTFA_kernel, computeSensitivity_kernel, trySensMultiplier_kernel and
   filterSensitivity_kernel (oracle/_ref/libref_kernels.so) on the seeded inputs of
@@ -50,6 +53,26 @@ def stop_sequences():
     return seqs
 
 
+def vox_meshes():
+    """Closed meshes for the voxeliser pin (product mesh generators, deterministic)."""
+    from robtop_b200 import configs
+
+    s3 = configs.icosphere(3, radius=1.0)
+    t = configs.torus(1.0, 0.35, 40, 20)
+    return {
+        "sphere": configs.icosphere(4, radius=1.0),
+        "sphere_rotated": (configs.rigid_transform(s3[0], 11, (0.3, -0.2, 0.1)), s3[1]),
+        "torus_rotated": (configs.rigid_transform(t[0], 12), t[1]),
+        "box_half_voxel": configs.box_mesh((0.1, 0.1, 0.1), (0.9, 0.9, 0.9)),
+        "box_flat": configs.box_mesh((0.0, 0.0, 0.0), (1.0, 0.37, 0.61)),
+        "two_spheres": configs.merge_meshes(configs.icosphere(2, (0, 0, 0), 0.5),
+                                            configs.icosphere(3, (1.3, 0.2, 0.1), 0.6)),
+    }
+
+
+VOX_PREFER = (7, 31, 63)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--kernels", action="store_true")
@@ -69,6 +92,16 @@ def main():
             flat[f"stop_fabs{i}"] = reference.converge_run(1, 2, 5e-3, c, g, float_abs=True)
         np.savez_compressed(os.path.join(a.out, "ref_stop.npz"), n=len(seqs), **flat)
         print("stop-test results written")
+    if os.path.exists(reference.VOX_LIB):
+        import oracle as O
+
+        out = {}
+        for name, (v, f) in vox_meshes().items():
+            for prefer in VOX_PREFER:
+                R, bmin, bmax, _ = O.voxel_box(v, prefer)
+                out[f"{name}/{prefer}"] = reference.voxelize_solid(v, f, R, bmin, bmax)
+        np.savez_compressed(os.path.join(a.out, "ref_vox.npz"), **out)
+        print("voxeliser bits written")
     if a.kernels:
         K = reference.Kernels()
         out = {}

@@ -7,6 +7,9 @@
 * The oracle's applyK, sensitivity, OC trial and filter against the outputs of the reference's
   own CUDA kernels (grid/Grid.cu:2439-2517, 2323-2409; optimization/optimization.cu:44-162) on
   seeded inputs, stored in tests/golden/ref_kernels.npz by the same script on a GPU machine.
+* The optimisation loop's stop test against the reference's converge_criteria (utils/snippet.h)
+  in both of its builds, and the oracle's solid voxeliser against the reference's CPU voxeliser
+  (voxelizer/cpu_voxelizer.cpp), each as fixtures and against the live build.
 """
 import os
 import sys
@@ -104,3 +107,37 @@ def test_stop_test_matches_reference_build():
         g = [np.zeros(n), -0.4 * 0.05 * np.ones(n), 0.3 * (0.95 ** np.arange(1, n + 1) - 1)][case % 3]
         assert _stop_flags(c, g, True) == reference.converge_run(1, 2, 5e-3, c, g).tolist(), case
         assert _stop_flags(c, g, False) == reference.converge_run(1, 2, 5e-3, c, g, float_abs=True).tolist(), case
+
+
+VOX_FIXTURE = os.path.join(HERE, "golden", "ref_vox.npz")
+
+
+def test_voxeliser_matches_reference_fixture():
+    """The oracle's solid voxeliser gives the reference CPU voxeliser's bits
+    (voxelizer/cpu_voxelizer.cpp:262-322), bit for bit, on closed meshes (spheres, rotated
+    sphere and torus, boxes on voxel centres and flat, merged spheres) at resolutions 8, 32, 64."""
+    from make_ref_fixtures import VOX_PREFER, vox_meshes
+
+    g = np.load(VOX_FIXTURE)
+    for name, (v, f) in vox_meshes().items():
+        for prefer in VOX_PREFER:
+            R, bmin, bmax, unit = O.voxel_box(v, prefer)
+            assert np.array_equal(O.voxelize_solid(v, f, R, bmin, unit), g[f"{name}/{prefer}"]), (name, prefer)
+
+
+@pytest.mark.skipif(not os.path.exists(reference.VOX_LIB), reason="oracle/_ref/libref_vox.so not built")
+def test_voxeliser_matches_reference_build():
+    """The same against the live build, at 256^3 as well and on merged meshes of other sizes."""
+    from make_ref_fixtures import vox_meshes
+
+    from robtop_b200 import configs
+
+    meshes = dict(vox_meshes())
+    meshes["three_tori"] = configs.merge_meshes(configs.torus(1.0, 0.3, 48, 24),
+                                                (configs.rigid_transform(configs.torus(0.6, 0.2, 32, 16)[0], 5),
+                                                 configs.torus(0.6, 0.2, 32, 16)[1]))
+    for name, (v, f) in meshes.items():
+        for prefer in (15, 200):
+            R, bmin, bmax, unit = O.voxel_box(v, prefer)
+            assert np.array_equal(O.voxelize_solid(v, f, R, bmin, unit),
+                                  reference.voxelize_solid(v, f, R, bmin, bmax)), (name, prefer)
