@@ -18,7 +18,10 @@
  *    finest grid.  RT_LAYOUT_REF_GS selects the reference's Gauss-Seidel
  *    colour-ordered, 32-padded layout (grid/Grid.cpp:2045-2106) instead.
  *  - A context owns one CUDA stream (or borrows the caller's); every call is
- *    ordered on it.  Contexts and hierarchies are independent of each other
+ *    ordered on it.  The context's own stream is non-blocking: a caller that writes
+ *    an input _dev array on another stream, or reads an output one there, orders
+ *    that work with the context's stream first (or passes its own stream at
+ *    rt_ctx_create).  Contexts and hierarchies are independent of each other
  *    (the reference rebinds global __constant__ tables per level,
  *    grid/Grid.cu:48-75, and is not reentrant).
  */
