@@ -392,7 +392,9 @@ def cpu_baseline(gpu_inner_iters, gpu_vcycles, threads):
 def run_reference(args):
     """The reference arm: the CPU restatement of the reference algorithm (oracle/, plain FP64 SGS
     V-cycle PCG, OpenMP on all host cores) on the same workload as the default arm.  The
-    reference itself cannot be built here (its sources need Eigen, CGAL and OpenVDB).  A full step
+    reference's solve path cannot be built here (Grid.cpp and optimization.cpp need Eigen, CGAL and
+    OpenVDB; only its element template, four kernels, stop test and voxeliser compile, and those
+    pin the oracle).  A full step
     on the 511x256x256 arch takes the oracle tens of minutes, so each step is a bounded sample: the
     oracle runs stencil assembly and one inner solve to 1e-6 on the 127x64x64 arch, and the step
     time is extrapolated to the full arch by node count and to the 17 inner solves of a step (k = 16
@@ -432,8 +434,9 @@ def run_reference(args):
             "sample": {k: last[k] for k in ("sample_dims", "sample_nodes", "sample_assembly_s", "sample_pcg_iterations",
                                             "sample_s_per_iteration", "node_scale_factor")},
             "cpu_baseline": {"value": val, "unit": "solves/s", "cores": threads, "kind": "port", "extrapolated": True,
-                             "sample": "CPU restatement of the reference algorithm (the reference needs Eigen/CGAL/"
-                                       "OpenVDB and cannot be built here): stencil assembly + one inner solve to 1e-6 "
+                             "sample": "CPU restatement of the reference algorithm (the reference's solve path needs "
+                                       "Eigen/CGAL/OpenVDB and cannot be built here; the restatement is pinned to the "
+                                       "parts that can): stencil assembly + one inner solve to 1e-6 "
                                        f"on the {'x'.join(map(str, last['sample_dims']))} arch per step "
                                        f"({wall:.1f} s of CPU wall time), extrapolated by node count "
                                        f"(x{last['node_scale_factor']:.1f}) and to {solves} inner solves "
